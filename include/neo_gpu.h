@@ -1,0 +1,125 @@
+/*
+ * neo_gpu.h -- C ABI of the B200 (sm_100a) Neo fold-step prover core.
+ *
+ * Plain C types only.  F_q = canonical uint64 < q (q = 2^64 - 2^32 + 1);
+ * K = F_q[u]/(u^2 - 7) = two consecutive uint64 (re, im).  All buffers passed
+ * to these functions are HOST buffers owned by the caller; they are copied to
+ * and from the device inside the call.  Handles are opaque and freed by the
+ * matching *_destroy.  Every function returns a status (NEO_OK = 0) and never
+ * aborts; neo_gpu_last_error() gives the message of the last failure on a
+ * context.  A context is bound to one device and one CUDA stream; calls on one
+ * context must be serialized by the caller (one context per host thread).
+ *
+ * Each entry point cites the reference interface it replaces (path:line
+ * relative to the reference project root).
+ */
+#ifndef NEO_GPU_H
+#define NEO_GPU_H
+#include <stdint.h>
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum {
+    NEO_OK = 0,
+    NEO_ERR_ARG = 1,        /* bad argument or shape (reference: panic / InvalidInput) */
+    NEO_ERR_OOM = 2,        /* device allocation failed */
+    NEO_ERR_INVARIANT = 3,  /* protocol invariant failed (reference: ProtocolError) */
+    NEO_ERR_CUDA = 4,       /* CUDA runtime error */
+    NEO_ERR_UNSUPPORTED = 5 /* parameter outside what the kernels implement */
+};
+
+typedef struct neo_gpu_ctx neo_gpu_ctx;
+typedef struct neo_gpu_ccs_oracle neo_gpu_ccs_oracle;
+
+/* CCS structure (crates/neo-ccs/src/relations.rs:14-23).  Matrix j is the
+ * identity sentinel when is_identity[j] != 0, otherwise CSC
+ * (crates/neo-ccs/src/sparse.rs:19): column pointers col_ptr[j*(m+1) + c]
+ * index into row_idx/vals starting at nnz_off[j].  f is a sparse polynomial
+ * with n_terms terms: coefficient f_coeff[i], exponents f_exps[i*t + j]. */
+typedef struct neo_ccs_desc {
+    uint32_t n, m, t;
+    const uint8_t* is_identity;
+    const uint64_t* col_ptr;
+    const uint64_t* nnz_off;
+    const uint32_t* row_idx;
+    const uint64_t* vals;
+    uint32_t n_terms;
+    const uint64_t* f_coeff;
+    const uint32_t* f_exps;
+} neo_ccs_desc;
+
+/* ---- context -------------------------------------------------------- */
+int neo_gpu_ctx_create(int device, neo_gpu_ctx** out);
+int neo_gpu_ctx_destroy(neo_gpu_ctx* ctx);
+const char* neo_gpu_last_error(const neo_gpu_ctx* ctx);
+/* Number of kernels this context has launched so far (instrumentation). */
+uint64_t neo_gpu_kernel_launches(const neo_gpu_ctx* ctx);
+
+/* ---- Ajtai commitment (crates/neo-ajtai) ---------------------------- */
+/* Upload public parameters M in R_q^{kappa x m}: coeffs[(i*m + j)*54 + s] is
+ * coefficient s of M[i][j].  Replaces the PP registry load
+ * (crates/neo-ajtai/src/s_module.rs:23-222, types.rs:7-16). */
+int neo_gpu_pp_upload(neo_gpu_ctx* ctx, uint32_t kappa, uint64_t m, const uint64_t* coeffs);
+
+/* c = cf(M cf^{-1}(Z)) for n_vec digit matrices at once.
+ * digits[(v*54 + r)*m + j] = Z_v[r][j] (row-major d x m, values in [-128,127]);
+ * out[(v*kappa + i)*54 + r] = Commitment.data[i*54 + r] (column-major d x kappa,
+ * crates/neo-ajtai/src/types.rs:17-50).  Replaces SModuleHomomorphism::commit
+ * (crates/neo-ccs/src/traits.rs:8-14; crates/neo-ajtai/src/s_module.rs:335-377)
+ * and commit_row_major (crates/neo-ajtai/src/commit.rs:376-402, 679-744). */
+int neo_gpu_commit(neo_gpu_ctx* ctx, const int8_t* digits, uint32_t n_vec, uint64_t m, uint64_t* out);
+
+/* Balanced base-2 decomposition z in F_q^m -> Z in {-1,0,1}^{54 x m}
+ * row-major (crates/neo-ajtai/src/decomp.rs:118-158, DecompStyle::Balanced). */
+int neo_gpu_decomp_b2(neo_gpu_ctx* ctx, const uint64_t* z, uint64_t m, int8_t* Z);
+
+/* ---- Pi_RLC / Pi_DEC (crates/neo-reductions/src/common.rs) ---------- */
+/* Z_mix = sum_i rot(a_i) Z_i, a_i = rho_coeffs[i*54 .. ] in {-2..2}
+ * (common.rs:398-430 rot_from_coeffs; optimized_engine/common.rs:1221-1379).
+ * Zs[(i*54 + r)*m + c]; Zmix[r*m + c] exact small integers. count == 1 is the
+ * identity (common.rs:560-564). */
+int neo_gpu_rlc_mix(neo_gpu_ctx* ctx, const int8_t* rho_coeffs, const int8_t* Zs, uint32_t count,
+                    uint64_t m, int32_t* Zmix);
+
+/* Balanced base-b split into k planes with nonzero flags
+ * (common.rs:75-268 split_b_matrix_k_with_nonzero_flags).  Returns
+ * NEO_ERR_INVARIANT when an entry needs more than k digits. */
+int neo_gpu_split_b(neo_gpu_ctx* ctx, const int32_t* Zmix, uint64_t len, uint32_t k, uint32_t b,
+                    int8_t* planes, uint8_t* nonzero);
+
+/* y_j = Z (M_j^T chi_r) for every CCS matrix j, and y_scalars_j = sum_rho b^rho y_j[rho]
+ * (common.rs:582-650 compute_y_from_Z_and_r).  Z: n_w digit matrices [n_w][54][m];
+ * r: ell_n K points; y: [n_w][t][54] K; y_scalars: [n_w][t] K. */
+int neo_gpu_me_y(neo_gpu_ctx* ctx, const neo_ccs_desc* ccs, const int8_t* Z, uint32_t n_w,
+                 uint32_t ell_n, const uint64_t* r, uint32_t b, uint64_t* y, uint64_t* y_scalars);
+
+/* ---- Pi_CCS sum-check oracle (RoundOracle) -------------------------- */
+/* OptimizedOracle::new_with_sparse
+ * (crates/neo-reductions/src/engines/optimized_engine/oracle.rs:1597-1639,
+ * RowStreamState::build oracle.rs:82-414).  Z: [k][54][m] digits, MCS
+ * witnesses first then ME witnesses; alpha, beta_a: ell_d K; beta_r: ell_n K;
+ * gamma: 1 K; r_inputs: ell_n K or NULL.  Requires n == m == 2^ell_n and b == 2.
+ * The oracle keeps its own device copy of Z and the CCS. */
+int neo_gpu_ccs_oracle_create(neo_gpu_ctx* ctx, const neo_ccs_desc* ccs, const int8_t* Z, uint32_t k,
+                              uint32_t b, const uint64_t* alpha, const uint64_t* beta_a,
+                              const uint64_t* beta_r, const uint64_t* gamma, const uint64_t* r_inputs,
+                              uint32_t ell_d, uint32_t ell_n, uint32_t d_sc, neo_gpu_ccs_oracle** out);
+/* RoundOracle::evals_at (crates/neo-reductions/src/sumcheck.rs:17-34;
+ * oracle.rs:2087-2093): ys[i] = p_round(xs[i]). */
+int neo_gpu_ccs_oracle_evals(neo_gpu_ccs_oracle* o, const uint64_t* xs, uint32_t nx, uint64_t* ys);
+/* RoundOracle::fold (oracle.rs:2095-2103). */
+int neo_gpu_ccs_oracle_fold(neo_gpu_ccs_oracle* o, const uint64_t* r);
+uint32_t neo_gpu_ccs_oracle_num_rounds(const neo_gpu_ccs_oracle* o);
+uint32_t neo_gpu_ccs_oracle_degree_bound(const neo_gpu_ccs_oracle* o);
+/* build_me_outputs_from_ajtai_precomp (oracle.rs:1955-2072), after the
+ * ell_n row rounds: y [k][t][54] K digits and y_scalars [k][t] K. */
+int neo_gpu_ccs_oracle_me_outputs(neo_gpu_ccs_oracle* o, uint64_t* y, uint64_t* y_scalars);
+int neo_gpu_ccs_oracle_destroy(neo_gpu_ccs_oracle* o);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,980 @@
+// ccs_oracle.cu -- Pi_CCS sum-check oracle (RoundOracle) on sm_100a.
+//
+// Reference: OptimizedOracle / RowStreamState
+// (crates/neo-reductions/src/engines/optimized_engine/oracle.rs:82-503,
+// 1047-1178, 1597-2104).  Round polynomial of the row phase, for pairs
+// (2t, 2t+1) of every table (LSB-first binding):
+//   p(X) = sum_t eq_br(X) * ( f(M z1)(X) + sum_{i,rho} wg[i,rho] N(y_{i,rho}(X)) )
+//          + gamma^k * eq_rin(X) * eval(X),         N(y) = y^3 - y  (b = 2)
+// computed as coefficients (low -> high) and evaluated at the requested xs.
+//
+// Design:
+//  * Witness digit planes Z_i[rho][row] stay int8 in HBM.  For the first J
+//    rounds the folded value of a table entry after j bound variables is
+//    sum_b chi(r_0..r_{j-1})[b] * Z[rho][2^j t + b]: it is recomputed from the
+//    digits each round (adds only) instead of materialising 16-byte K tables.
+//  * Round J writes the K table T_J; later rounds read T_{j-1}, fold with
+//    r_{j-1}, write T_j (ping-pong) and evaluate, all in one pass.
+//  * The eq / f-variable / eval tables are folded the same way inside the
+//    round kernel.  Block partial coefficients are reduced by a second kernel
+//    in a fixed order, so results are deterministic (exact F_q arithmetic
+//    makes them order-independent anyway).
+#include "internal.cuh"
+#include <algorithm>
+#include <memory>
+
+using gl::K;
+
+namespace {
+
+constexpr int MAX_DEG = 8;    // deg_max + 1 <= 9 coefficients
+constexpr int MAX_TERMS = 8;
+constexpr int MAX_FVAR = 8;
+constexpr int RT = 256;       // threads per round block
+constexpr int JMAX = 4;       // rounds streamed from int8 digits (0..JMAX)
+
+struct FTerms {
+    int n_terms;
+    int n_vars[MAX_TERMS];
+    int var_pos[MAX_TERMS][4];
+    int var_exp[MAX_TERMS][4];
+    K coeff[MAX_TERMS];
+};
+
+struct RoundArgs {
+    // small tables [n_small][len]
+    const K* small_in;
+    K* small_out;
+    uint64_t small_len_in;
+    uint64_t small_len_out;
+    int fold;          // small_in must be folded by r first
+    K r;
+    int n_small;
+    int n_fvar;
+    int idx_eqrin;     // -1 when absent
+    int idx_eval;      // -1 when absent
+    K gamma_to_k;
+    FTerms f;
+    int deg_max;
+    // NC
+    const int8_t* Z;   // [nq][m]
+    uint64_t m;
+    const K* eqw;      // [2^j] chi of the bound prefix (streaming mode)
+    const K* nc_in;    // K-mode input [nq][nc_len_in]
+    uint64_t nc_len_in;
+    K* nc_out;         // written table [nq][nc_len_out] or null
+    uint64_t nc_len_out;
+    const K* wg;       // [nq]
+    int nq;
+    int q_per_block;
+    uint64_t pairs;
+    K* partials;       // [gridDim.x * gridDim.y][deg_max+1]
+};
+
+__device__ __forceinline__ K shfl_xor_k(K a, int o) {
+    K b;
+    b.re = __shfl_xor_sync(0xffffffffu, a.re, o);
+    b.im = __shfl_xor_sync(0xffffffffu, a.im, o);
+    return b;
+}
+
+__device__ __forceinline__ K ld_k(const K* p) {
+    ulonglong2 v = __ldg(reinterpret_cast<const ulonglong2*>(p));
+    return gl::kmk(v.x, v.y);
+}
+__device__ __forceinline__ void st_k(K* p, K a) {
+    *reinterpret_cast<ulonglong2*>(p) = make_ulonglong2(a.re, a.im);
+}
+
+// N(a + bX) coefficients accumulated with weight wg into inner[0..3]
+__device__ __forceinline__ void nc_accum_k(K wg, K a, K hi, K inner[4]) {
+    K bb = gl::ksub(hi, a);
+    K a2 = gl::ksqr(a);
+    K a3 = gl::kmul(a2, a);
+    K b2 = gl::ksqr(bb);
+    K b3 = gl::kmul(b2, bb);
+    K a2b = gl::kmul(a2, bb);
+    K ab2 = gl::kmul(a, b2);
+    K t0 = gl::ksub(a3, a);
+    K t1 = gl::ksub(gl::kadd(gl::kdbl(a2b), a2b), bb);
+    K t2 = gl::kadd(gl::kdbl(ab2), ab2);
+    inner[0] = gl::kadd(inner[0], gl::kmul(wg, t0));
+    inner[1] = gl::kadd(inner[1], gl::kmul(wg, t1));
+    inner[2] = gl::kadd(inner[2], gl::kmul(wg, t2));
+    inner[3] = gl::kadd(inner[3], gl::kmul(wg, b3));
+}
+
+// small-integer case (round 0): a = lo, hi are int8 digits, so every
+// coefficient of N(a + bX) is a small integer (|.| < 2^25).
+__device__ __forceinline__ void nc_accum_small(K wg, int a, int hi, K inner[4]) {
+    int bb = hi - a;
+    int t0 = a * a * a - a;             // 0 for a in {-1,0,1}
+    int t1 = bb * (3 * a * a - 1);
+    int t2 = 3 * a * bb * bb;
+    int t3 = bb * bb * bb;
+    if (t0) inner[0] = gl::kadd(inner[0], gl::kscale_small(wg, t0));
+    if (t1) inner[1] = gl::kadd(inner[1], gl::kscale_small(wg, t1));
+    if (t2) inner[2] = gl::kadd(inner[2], gl::kscale_small(wg, t2));
+    if (t3) inner[3] = gl::kadd(inner[3], gl::kscale_small(wg, t3));
+}
+
+template <int NB>  // bytes per row pair = 2^(j+1)
+__device__ __forceinline__ void load_digits(const int8_t* p, int8_t* d) {
+    if constexpr (NB == 2) {
+        char2 v = *reinterpret_cast<const char2*>(p);
+        d[0] = v.x; d[1] = v.y;
+    } else if constexpr (NB == 4) {
+        char4 v = *reinterpret_cast<const char4*>(p);
+        d[0] = v.x; d[1] = v.y; d[2] = v.z; d[3] = v.w;
+    } else if constexpr (NB == 8) {
+        int2 v = __ldg(reinterpret_cast<const int2*>(p));
+        memcpy(d, &v, 8);
+    } else {
+#pragma unroll
+        for (int o = 0; o < NB; o += 16) {
+            int4 v = __ldg(reinterpret_cast<const int4*>(p + o));
+            memcpy(d + o, &v, 16);
+        }
+    }
+}
+
+// MODE 0..JMAX: digit streaming at round j = MODE; MODE = JMAX + 1: K tables.
+template <int MODE>
+__global__ void __launch_bounds__(RT) ccs_round_kernel(const RoundArgs a) {
+    const uint64_t t = blockIdx.x * (uint64_t)RT + threadIdx.x;
+    const bool live = t < a.pairs;
+    const int dm = a.deg_max;
+    K coeffs[MAX_DEG + 1];
+#pragma unroll
+    for (int d = 0; d <= MAX_DEG; d++) coeffs[d] = gl::kzero();
+
+    __shared__ K s_wg[1024];
+    __shared__ K s_eqw[1 << JMAX];
+    const int q0 = blockIdx.y * a.q_per_block;
+    const int q1 = min(a.nq, q0 + a.q_per_block);
+    for (int q = q0 + threadIdx.x; q < q1; q += RT) s_wg[q - q0] = a.wg[q];
+    if constexpr (MODE <= JMAX) {
+        for (int b = threadIdx.x; b < (1 << MODE); b += RT) s_eqw[b] = a.eqw[b];
+    }
+    __syncthreads();
+
+    if (live) {
+        K inner[MAX_DEG + 1];
+#pragma unroll
+        for (int d = 0; d <= MAX_DEG; d++) inner[d] = gl::kzero();
+        // ---- small tables: eq_beta_r, f vars, eq_rin, eval (only y-block 0) ----
+        K e0 = gl::kzero(), e1 = gl::kzero();
+        if (blockIdx.y == 0) {
+            K lo_s[2 + MAX_FVAR + 2], hi_s[2 + MAX_FVAR + 2];
+            for (int s = 0; s < a.n_small; s++) {
+                K lo, hi;
+                if (a.fold) {
+                    const K* in = a.small_in + (uint64_t)s * a.small_len_in + 4 * t;
+                    K x0 = ld_k(in), x1 = ld_k(in + 1), x2 = ld_k(in + 2), x3 = ld_k(in + 3);
+                    lo = gl::klerp(x0, x1, a.r);
+                    hi = gl::klerp(x2, x3, a.r);
+                    if (a.small_out) {
+                        K* out = a.small_out + (uint64_t)s * a.small_len_out + 2 * t;
+                        st_k(out, lo);
+                        st_k(out + 1, hi);
+                    }
+                } else {
+                    const K* in = a.small_in + (uint64_t)s * a.small_len_in + 2 * t;
+                    lo = ld_k(in);
+                    hi = ld_k(in + 1);
+                }
+                lo_s[s] = lo;
+                hi_s[s] = hi;
+            }
+            e0 = lo_s[0];
+            e1 = gl::ksub(hi_s[0], e0);
+            // f(X) = sum_terms coeff * prod (a_v + b_v X)^exp, truncated to deg_max+1
+            for (int tt = 0; tt < a.f.n_terms; tt++) {
+                K tp[MAX_DEG + 1];
+#pragma unroll
+                for (int d = 0; d <= MAX_DEG; d++) tp[d] = gl::kzero();
+                tp[0] = a.f.coeff[tt];
+                for (int vv = 0; vv < a.f.n_vars[tt]; vv++) {
+                    int pos = a.f.var_pos[tt][vv];
+                    K av = lo_s[1 + pos];
+                    K bv = gl::ksub(hi_s[1 + pos], av);
+                    for (int e = 0; e < a.f.var_exp[tt][vv]; e++) {
+                        K prev = gl::kzero();
+#pragma unroll
+                        for (int d = 0; d <= MAX_DEG; d++) {
+                            if (d <= dm) {
+                                K old = tp[d];
+                                tp[d] = gl::kadd(gl::kmul(av, old), gl::kmul(bv, prev));
+                                prev = old;
+                            }
+                        }
+                    }
+                }
+#pragma unroll
+                for (int d = 0; d <= MAX_DEG; d++) inner[d] = gl::kadd(inner[d], tp[d]);
+            }
+            if (a.idx_eval >= 0) {
+                K r0 = lo_s[a.idx_eqrin], r1 = gl::ksub(hi_s[a.idx_eqrin], r0);
+                K v0 = lo_s[a.idx_eval], v1 = gl::ksub(hi_s[a.idx_eval], v0);
+                K g = a.gamma_to_k;
+                coeffs[0] = gl::kadd(coeffs[0], gl::kmul(g, gl::kmul(r0, v0)));
+                coeffs[1] = gl::kadd(coeffs[1], gl::kmul(g, gl::kadd(gl::kmul(r0, v1), gl::kmul(r1, v0))));
+                coeffs[2] = gl::kadd(coeffs[2], gl::kmul(g, gl::kmul(r1, v1)));
+            }
+        } else {
+            // NC-only blocks still need eq_beta_r at this pair
+            K lo, hi;
+            if (a.fold) {
+                const K* in = a.small_in + 4 * t;
+                lo = gl::klerp(ld_k(in), ld_k(in + 1), a.r);
+                hi = gl::klerp(ld_k(in + 2), ld_k(in + 3), a.r);
+            } else {
+                lo = ld_k(a.small_in + 2 * t);
+                hi = ld_k(a.small_in + 2 * t + 1);
+            }
+            e0 = lo;
+            e1 = gl::ksub(hi, lo);
+        }
+
+        // ---- NC block ----
+        K nc[4] = {gl::kzero(), gl::kzero(), gl::kzero(), gl::kzero()};
+        if constexpr (MODE == 0) {
+            for (int q = q0; q < q1; q++) {
+                int8_t d[2];
+                load_digits<2>(a.Z + (uint64_t)q * a.m + 2 * t, d);
+                if (a.nc_out) {
+                    K* out = a.nc_out + (uint64_t)q * a.nc_len_out + 2 * t;
+                    st_k(out, gl::kfq(gl::from_i64(d[0])));
+                    st_k(out + 1, gl::kfq(gl::from_i64(d[1])));
+                }
+                nc_accum_small(s_wg[q - q0], d[0], d[1], nc);
+            }
+        } else if constexpr (MODE <= JMAX) {
+            constexpr int HALF = 1 << MODE;
+            constexpr int NB = 2 * HALF;
+            for (int q = q0; q < q1; q++) {
+                int8_t d[NB];
+                load_digits<NB>(a.Z + (uint64_t)q * a.m + (uint64_t)NB * t, d);
+                K lo = gl::kzero(), hi = gl::kzero();
+#pragma unroll
+                for (int b = 0; b < HALF; b++) {
+                    if (d[b] == 1) lo = gl::kadd(lo, s_eqw[b]);
+                    else if (d[b] == -1) lo = gl::ksub(lo, s_eqw[b]);
+                    else if (d[b] != 0) lo = gl::kadd(lo, gl::kscale_small(s_eqw[b], d[b]));
+                    if (d[HALF + b] == 1) hi = gl::kadd(hi, s_eqw[b]);
+                    else if (d[HALF + b] == -1) hi = gl::ksub(hi, s_eqw[b]);
+                    else if (d[HALF + b] != 0) hi = gl::kadd(hi, gl::kscale_small(s_eqw[b], d[HALF + b]));
+                }
+                if (a.nc_out) {
+                    K* out = a.nc_out + (uint64_t)q * a.nc_len_out + 2 * t;
+                    st_k(out, lo);
+                    st_k(out + 1, hi);
+                }
+                nc_accum_k(s_wg[q - q0], lo, hi, nc);
+            }
+        } else {
+            for (int q = q0; q < q1; q++) {
+                const K* in = a.nc_in + (uint64_t)q * a.nc_len_in + 4 * t;
+                K x0 = ld_k(in), x1 = ld_k(in + 1), x2 = ld_k(in + 2), x3 = ld_k(in + 3);
+                K lo = gl::klerp(x0, x1, a.r);
+                K hi = gl::klerp(x2, x3, a.r);
+                if (a.nc_out) {
+                    K* out = a.nc_out + (uint64_t)q * a.nc_len_out + 2 * t;
+                    st_k(out, lo);
+                    st_k(out + 1, hi);
+                }
+                nc_accum_k(s_wg[q - q0], lo, hi, nc);
+            }
+        }
+#pragma unroll
+        for (int d = 0; d < 4; d++) inner[d] = gl::kadd(inner[d], nc[d]);
+        // coeffs += eq_br(X) * inner(X)
+        coeffs[0] = gl::kadd(coeffs[0], gl::kmul(e0, inner[0]));
+#pragma unroll
+        for (int d = 1; d <= MAX_DEG; d++)
+            if (d <= dm) coeffs[d] = gl::kadd(coeffs[d], gl::kadd(gl::kmul(e0, inner[d]), gl::kmul(e1, inner[d - 1])));
+    }
+
+    // ---- block reduction of coeffs[0..dm] ----
+    __shared__ K s_red[RT / 32][MAX_DEG + 1];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int d = 0; d <= MAX_DEG; d++) {
+        if (d <= dm) {
+            K v = coeffs[d];
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) v = gl::kadd(v, shfl_xor_k(v, o));
+            if (lane == 0) s_red[warp][d] = v;
+        }
+    }
+    __syncthreads();
+    if (threadIdx.x <= dm) {
+        K v = gl::kzero();
+        for (int w = 0; w < RT / 32; w++) v = gl::kadd(v, s_red[w][threadIdx.x]);
+        a.partials[((uint64_t)blockIdx.y * gridDim.x + blockIdx.x) * (dm + 1) + threadIdx.x] = v;
+    }
+}
+
+struct EvalArgs {
+    const K* partials;
+    uint32_t nblocks;
+    int ncoef;
+    int nx;
+    K xs[16];
+    K* coeffs_out;
+    K* ys_out;
+};
+
+__global__ void __launch_bounds__(256) reduce_eval_kernel(const EvalArgs a) {
+    __shared__ K s_c[MAX_DEG + 1];
+    __shared__ K s_red[8];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int d = 0; d < a.ncoef; d++) {
+        K v = gl::kzero();
+        for (uint32_t b = threadIdx.x; b < a.nblocks; b += blockDim.x) v = gl::kadd(v, a.partials[(uint64_t)b * a.ncoef + d]);
+        for (int o = 16; o > 0; o >>= 1) v = gl::kadd(v, shfl_xor_k(v, o));
+        if (lane == 0) s_red[warp] = v;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            K s = gl::kzero();
+            for (int w = 0; w < (int)(blockDim.x >> 5); w++) s = gl::kadd(s, s_red[w]);
+            s_c[d] = s;
+            a.coeffs_out[d] = s;
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x < a.nx) {
+        K x = a.xs[threadIdx.x];
+        K r = s_c[a.ncoef - 1];
+        for (int d = a.ncoef - 2; d >= 0; d--) r = gl::kadd(gl::kmul(r, x), s_c[d]);
+        a.ys_out[threadIdx.x] = r;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Table build kernels
+// ---------------------------------------------------------------------------
+// z1[c] = sum_rho b^rho Z_0[rho][c]  (oracle.rs:215-243)
+__global__ void z1_kernel(const int8_t* __restrict__ Z, uint64_t m, uint32_t b, uint64_t* __restrict__ z1) {
+    uint64_t c = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+    if (c >= m) return;
+    uint64_t acc = 0, pw = 1;
+    for (int rho = 0; rho < NEO_D; rho++) {
+        int z = Z[(uint64_t)rho * m + c];
+        if (z == 1) acc = gl::add(acc, pw);
+        else if (z == -1) acc = gl::sub(acc, pw);
+        else if (z) acc = gl::add(acc, gl::mul(pw, gl::from_i64(z)));
+        pw = gl::mul(pw, b);
+    }
+    z1[c] = acc;
+}
+
+// out[r] = (M x)[r] for base-field x (CSR), or x[r] for the identity (oracle.rs:245-285)
+__global__ void spmv_fq_kernel(const uint64_t* __restrict__ row_ptr, const uint32_t* __restrict__ col,
+                               const uint64_t* __restrict__ val, int is_identity, uint32_t n, uint32_t m,
+                               const uint64_t* __restrict__ x, uint64_t n_pad, K* __restrict__ out) {
+    uint64_t r = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+    if (r >= n_pad) return;
+    uint64_t acc = 0;
+    if (r < n) {
+        if (is_identity) {
+            acc = r < m ? x[r] : 0;
+        } else {
+            for (uint64_t k = row_ptr[r]; k < row_ptr[r + 1]; k++) acc = gl::add(acc, gl::mul(val[k], x[col[k]]));
+        }
+    }
+    out[r] = gl::kfq(acc);
+}
+
+// u[c] = sum_{i>=1} sum_rho gamma^i chi_alpha[rho] Z_i[rho][c]  (Eval table input, oracle.rs:320-390)
+__global__ void eval_u_kernel(const int8_t* __restrict__ Z, uint64_t m, uint32_t k, const K* __restrict__ w,
+                              K* __restrict__ u) {
+    uint64_t c = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+    if (c >= m) return;
+    K acc = gl::kzero();
+    for (uint32_t i = 1; i < k; i++)
+        for (int rho = 0; rho < NEO_D; rho++) {
+            int z = Z[((uint64_t)i * NEO_D + rho) * m + c];
+            if (z == 0) continue;
+            K x = w[i * NEO_D + rho];
+            acc = z == 1 ? gl::kadd(acc, x) : (z == -1 ? gl::ksub(acc, x) : gl::kadd(acc, gl::kscale_small(x, z)));
+        }
+    u[c] = acc;
+}
+
+// eval[r] = sum_j coef_j (M_j u)[r]
+__global__ void eval_tbl_kernel(const uint64_t* __restrict__ row_ptr, const uint32_t* __restrict__ col,
+                                const uint64_t* __restrict__ val, const uint64_t* __restrict__ nnz_off,
+                                const uint8_t* __restrict__ is_id, uint32_t t, uint32_t n, uint32_t m,
+                                const K* __restrict__ u, const K* __restrict__ coef, uint64_t n_pad,
+                                K* __restrict__ out) {
+    uint64_t r = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+    if (r >= n_pad) return;
+    K acc = gl::kzero();
+    if (r < n) {
+        for (uint32_t j = 0; j < t; j++) {
+            K mj = gl::kzero();
+            if (is_id[j]) {
+                if (r < m) mj = u[r];
+            } else {
+                const uint64_t* rp = row_ptr + (uint64_t)j * (n + 1);
+                uint64_t base = nnz_off[j];
+                for (uint64_t k = rp[r]; k < rp[r + 1]; k++)
+                    mj = gl::kadd(mj, gl::kscale(u[col[base + k]], val[base + k]));
+            }
+            acc = gl::kadd(acc, gl::kmul(coef[j], mj));
+        }
+    }
+    out[r] = acc;
+}
+
+// ---------------------------------------------------------------------------
+// Ajtai phase (oracle.rs:1812-1951): one block.
+// ---------------------------------------------------------------------------
+struct AjtaiArgs {
+    int k, t, ell_d, ell_n, j, nx, has_inputs;
+    K xs[16];
+    K alpha[8], beta_a[8], ajtai_chals[8];
+    K beta_r[32], r_in[32], row_chals[32];
+    K gamma;
+    FTerms f;
+    int fvar_j[MAX_FVAR];
+    const K* y;      // [k][t][54]
+    const K* ysc;    // [k][t]
+    K* ys_out;       // [nx]
+};
+
+__device__ K eq_lin_d(K a, K b) {
+    return gl::kadd(gl::kmul(gl::ksub(gl::kone(), a), gl::ksub(gl::kone(), b)), gl::kmul(a, b));
+}
+
+__global__ void __launch_bounds__(512) ajtai_round_kernel(const AjtaiArgs a) {
+    extern __shared__ K s_y[];            // [nvec][54] prefolded
+    __shared__ K s_wb[64], s_wa[64];
+    const int nvec = a.k * (1 + a.t);     // vector q < k: NC (y[i][0]); then eval (i, jm)
+    const int j = a.j;
+    // prefix fold of every vector by bits 0..j-1 (fold_bit_inplace semantics)
+    for (int q = threadIdx.x; q < nvec; q += blockDim.x) {
+        const K* src = q < a.k ? a.y + ((uint64_t)q * a.t + 0) * NEO_D
+                               : a.y + (uint64_t)(q - a.k) * NEO_D;
+        K* dst = s_y + q * NEO_D;
+        for (int r = 0; r < NEO_D; r++) dst[r] = src[r];
+        for (int bb = 0; bb < j; bb++) {
+            int stride = 1 << bb, step = stride << 1;
+            for (int base = 0; base < NEO_D; base += step)
+                for (int off = 0; off < stride; off++) {
+                    int i0 = base + off;
+                    if (i0 >= NEO_D) break;
+                    int i1 = i0 + stride;
+                    K lo = dst[i0], hi = i1 < NEO_D ? dst[i1] : gl::kzero();
+                    dst[i0] = gl::klerp(lo, hi, a.ajtai_chals[bb]);
+                }
+        }
+    }
+    // tail weights chi(beta_a[j+1..]), chi(alpha[j+1..])
+    const int ntail = a.ell_d - j - 1;
+    const int tail_len = 1 << ntail;
+    for (int tt = threadIdx.x; tt < tail_len; tt += blockDim.x) {
+        K wb = gl::kone(), wa = gl::kone();
+        for (int i = 0; i < ntail; i++) {
+            int bit = (tt >> i) & 1;
+            K b = a.beta_a[j + 1 + i], al = a.alpha[j + 1 + i];
+            wb = gl::kmul(wb, bit ? b : gl::ksub(gl::kone(), b));
+            wa = gl::kmul(wa, bit ? al : gl::ksub(gl::kone(), al));
+        }
+        s_wb[tt] = wb;
+        s_wa[tt] = wa;
+    }
+    __syncthreads();
+    const int hs = 1 << (j + 1), stride = 1 << j;
+    // per (x, vector) work item
+    __shared__ K s_val[16][160];
+    for (int w = threadIdx.x; w < a.nx * nvec; w += blockDim.x) {
+        int xi = w / nvec, q = w % nvec;
+        K x = a.xs[xi];
+        const K* v = s_y + q * NEO_D;
+        K acc = gl::kzero();
+        for (int tt = 0; tt < tail_len; tt++) {
+            int idx = tt * hs;
+            if (idx >= NEO_D) continue;
+            int i1 = idx + stride;
+            K lo = v[idx], hi = i1 < NEO_D ? v[i1] : gl::kzero();
+            K val = gl::klerp(lo, hi, x);
+            if (q < a.k) {
+                K y2 = gl::ksqr(val);
+                val = gl::kmul(val, gl::ksub(y2, gl::kone()));  // range product, b = 2
+                acc = gl::kadd(acc, gl::kmul(s_wb[tt], val));
+            } else {
+                acc = gl::kadd(acc, gl::kmul(s_wa[tt], val));
+            }
+        }
+        s_val[xi][q] = acc;
+    }
+    __syncthreads();
+    if (threadIdx.x < a.nx) {
+        const int xi = threadIdx.x;
+        K x = a.xs[xi];
+        // gamma^k, prefix eqs
+        K gk = gl::kone();
+        for (int i = 0; i < a.k; i++) gk = gl::kmul(gk, a.gamma);
+        K ebp = gl::kone(), eap = gl::kone();
+        for (int i = 0; i < j; i++) {
+            ebp = gl::kmul(ebp, eq_lin_d(a.ajtai_chals[i], a.beta_a[i]));
+            eap = gl::kmul(eap, eq_lin_d(a.ajtai_chals[i], a.alpha[i]));
+        }
+        K eq_br = gl::kone(), eq_ri = gl::kone();
+        for (int i = 0; i < a.ell_n; i++) {
+            eq_br = gl::kmul(eq_br, eq_lin_d(a.row_chals[i], a.beta_r[i]));
+            if (a.has_inputs) eq_ri = gl::kmul(eq_ri, eq_lin_d(a.row_chals[i], a.r_in[i]));
+        }
+        K eq_beta = gl::kmul(eq_br, gl::kmul(ebp, eq_lin_d(x, a.beta_a[j])));
+        K eq_ar = a.has_inputs ? gl::kmul(eq_ri, gl::kmul(eap, eq_lin_d(x, a.alpha[j]))) : gl::kzero();
+        // F' = f(m_vals), m_vals[j] = y_scalars[0][j] (z1 . v_j by linearity of recomposition)
+        K fprime = gl::kzero();
+        for (int tt = 0; tt < a.f.n_terms; tt++) {
+            K p = a.f.coeff[tt];
+            for (int vv = 0; vv < a.f.n_vars[tt]; vv++) {
+                K mv = a.ysc[a.fvar_j[a.f.var_pos[tt][vv]]];
+                for (int e = 0; e < a.f.var_exp[tt][vv]; e++) p = gl::kmul(p, mv);
+            }
+            fprime = gl::kadd(fprime, p);
+        }
+        K nc_sum = gl::kzero(), g = a.gamma;
+        for (int i = 0; i < a.k; i++) {
+            nc_sum = gl::kadd(nc_sum, gl::kmul(g, s_val[xi][i]));
+            g = gl::kmul(g, a.gamma);
+        }
+        K out = gl::kmul(eq_beta, gl::kadd(fprime, nc_sum));
+        if (a.k >= 2 && !gl::kiszero(eq_ar)) {
+            K inner = gl::kzero();
+            K gkj = gl::kone();
+            for (int jm = 0; jm < a.t; jm++) {
+                K gi = gl::kone();
+                for (int i = 1; i < a.k; i++) {
+                    gi = gl::kmul(gi, a.gamma);
+                    inner = gl::kadd(inner, gl::kmul(gl::kmul(gi, gkj), s_val[xi][a.k + i * a.t + jm]));
+                }
+                gkj = gl::kmul(gkj, gk);
+            }
+            out = gl::kadd(out, gl::kmul(eq_ar, gl::kmul(gk, inner)));
+        }
+        a.ys_out[xi] = out;
+    }
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// Oracle object
+// ---------------------------------------------------------------------------
+struct neo_gpu_ccs_oracle {
+    neo_gpu_ctx* ctx = nullptr;
+    uint32_t k = 0, b = 2, ell_d = 0, ell_n = 0, d_sc = 0, t = 0;
+    uint64_t n_pad = 0, m = 0;
+    DevCcs ccs;
+    DevBuf<int8_t> Z;
+    FTerms f{};
+    int n_fvar = 0;
+    int fvar_j[MAX_FVAR] = {0};
+    int deg_max = 4;
+    int n_small = 0, idx_eqrin = -1, idx_eval = -1;
+    DevBuf<K> small[2];
+    int small_cur = 0;
+    DevBuf<K> nc[2];
+    int nc_cur = 0;
+    int J = 0;
+    DevBuf<K> wg, eqw, partials, coeffs, ys, scratch_k;
+    K gamma{}, gamma_to_k{};
+    std::vector<K> alpha, beta_a, beta_r, r_in, row_chals, ajtai_chals;
+    bool has_inputs = false, has_eval = false;
+    uint32_t round_idx = 0;
+    bool coeffs_valid = false;
+    std::vector<K> h_coeffs;
+    // Ajtai-phase state
+    bool have_pre = false;
+    DevBuf<K> chi_r, vj, y_eval, y_sc;
+};
+
+static std::vector<K> load_k(const uint64_t* p, size_t n) {
+    std::vector<K> v(n);
+    for (size_t i = 0; i < n; i++) v[i] = gl::kmk(gl::canon(p[2 * i]), gl::canon(p[2 * i + 1]));
+    return v;
+}
+
+static K host_chi_mask(size_t mask, const std::vector<K>& pts) {
+    K p = gl::kone();
+    for (size_t i = 0; i < pts.size(); i++) p = gl::kmul(p, ((mask >> i) & 1) ? pts[i] : gl::ksub(gl::kone(), pts[i]));
+    return p;
+}
+
+extern "C" int neo_gpu_ccs_oracle_create(neo_gpu_ctx* ctx, const neo_ccs_desc* desc, const int8_t* Z, uint32_t k,
+                                         uint32_t b, const uint64_t* alpha, const uint64_t* beta_a,
+                                         const uint64_t* beta_r, const uint64_t* gamma, const uint64_t* r_inputs,
+                                         uint32_t ell_d, uint32_t ell_n, uint32_t d_sc, neo_gpu_ccs_oracle** out) {
+    if (!ctx) return NEO_ERR_ARG;
+    if (!out || !desc || !Z || !alpha || !beta_a || !beta_r || !gamma) return ctx->fail(NEO_ERR_ARG, "ccs_oracle: null argument");
+    *out = nullptr;
+    if (b != 2) return ctx->fail(NEO_ERR_UNSUPPORTED, "ccs_oracle: only b = 2 is implemented");
+    if (k == 0 || k > 18) return ctx->fail(NEO_ERR_ARG, "ccs_oracle: k must be in 1..18");
+    if (ell_d == 0 || ell_d > 8 || (1u << ell_d) < NEO_D) return ctx->fail(NEO_ERR_ARG, "ccs_oracle: ell_d");
+    if (ell_n < 1 || ell_n > 30) return ctx->fail(NEO_ERR_ARG, "ccs_oracle: ell_n");
+    if (desc->n != desc->m || desc->n != (1u << ell_n))
+        return ctx->fail(NEO_ERR_UNSUPPORTED, "ccs_oracle: requires n == m == 2^ell_n");
+    if (!desc->is_identity[0]) return ctx->fail(NEO_ERR_ARG, "ccs_oracle: CCS must be identity-first");
+    cudaSetDevice(ctx->device);
+    auto* o = new neo_gpu_ccs_oracle();
+    std::unique_ptr<neo_gpu_ccs_oracle> guard(o);
+    o->ctx = ctx;
+    o->k = k; o->b = b; o->ell_d = ell_d; o->ell_n = ell_n; o->d_sc = d_sc;
+    int rc = dev_ccs_upload(ctx, desc, o->ccs);
+    if (rc) return rc;
+    o->t = desc->t;
+    o->m = desc->m;
+    o->n_pad = 1ULL << ell_n;
+    o->alpha = load_k(alpha, ell_d);
+    o->beta_a = load_k(beta_a, ell_d);
+    o->beta_r = load_k(beta_r, ell_n);
+    o->gamma = load_k(gamma, 1)[0];
+    o->has_inputs = r_inputs != nullptr;
+    if (o->has_inputs) o->r_in = load_k(r_inputs, ell_n);
+    o->has_eval = o->has_inputs && k >= 2;
+
+    // compile f (oracle.rs:136-186)
+    const uint32_t t = o->t;
+    std::vector<int> pos_by_j(t, -1);
+    for (uint32_t j = 0; j < t; j++) {
+        bool used = false;
+        for (uint32_t tt = 0; tt < desc->n_terms; tt++) used |= desc->f_exps[tt * t + j] != 0;
+        if (used) {
+            if (o->n_fvar >= MAX_FVAR) return ctx->fail(NEO_ERR_UNSUPPORTED, "ccs_oracle: too many f variables");
+            pos_by_j[j] = o->n_fvar;
+            o->fvar_j[o->n_fvar++] = (int)j;
+        }
+    }
+    if (desc->n_terms > MAX_TERMS) return ctx->fail(NEO_ERR_UNSUPPORTED, "ccs_oracle: too many f terms");
+    int fmax = 0;
+    o->f.n_terms = (int)desc->n_terms;
+    for (uint32_t tt = 0; tt < desc->n_terms; tt++) {
+        int dg = 0, nv = 0;
+        o->f.coeff[tt] = gl::kfq(gl::canon(desc->f_coeff[tt]));
+        for (uint32_t j = 0; j < t; j++) {
+            uint32_t e = desc->f_exps[tt * t + j];
+            if (!e) continue;
+            if (nv >= 4) return ctx->fail(NEO_ERR_UNSUPPORTED, "ccs_oracle: term with more than 4 variables");
+            o->f.var_pos[tt][nv] = pos_by_j[j];
+            o->f.var_exp[tt][nv] = (int)e;
+            nv++;
+            dg += (int)e;
+        }
+        o->f.n_vars[tt] = nv;
+        fmax = std::max(fmax, dg);
+    }
+    o->deg_max = std::max(4, fmax + 1);
+    if (o->deg_max > MAX_DEG) return ctx->fail(NEO_ERR_UNSUPPORTED, "ccs_oracle: f degree too large");
+
+    const uint64_t n_pad = o->n_pad, m = o->m;
+    const uint32_t nq = k * NEO_D;
+    NEO_CK(ctx, o->Z.alloc((size_t)nq * m));
+    NEO_CK(ctx, cudaMemcpyAsync(o->Z.p, Z, o->Z.bytes(), cudaMemcpyHostToDevice, ctx->stream));
+
+    // small tables: [0] eq_beta_r, [1..n_fvar] f vars, then eq_rin, eval
+    o->n_small = 1 + o->n_fvar;
+    if (o->has_eval) {
+        o->idx_eqrin = o->n_small++;
+        o->idx_eval = o->n_small++;
+    }
+    NEO_CK(ctx, o->small[0].alloc((size_t)o->n_small * n_pad));
+    NEO_CK(ctx, o->small[1].alloc((size_t)o->n_small * n_pad / 2 + 1));
+    K* S = o->small[0].p;
+    DevBuf<K> dbits;
+    NEO_CK(ctx, dbits.alloc(ell_n));
+    NEO_CK(ctx, cudaMemcpyAsync(dbits.p, o->beta_r.data(), ell_n * 16, cudaMemcpyHostToDevice, ctx->stream));
+    if ((rc = launch_chi_table(ctx, dbits.p, ell_n, S))) return rc;
+    DevBuf<uint64_t> z1;
+    NEO_CK(ctx, z1.alloc(m));
+    z1_kernel<<<ceil_div(m, 256), 256, 0, ctx->stream>>>(o->Z.p, m, b, z1.p);
+    NEO_LAUNCHED(ctx);
+    for (int v = 0; v < o->n_fvar; v++) {
+        int j = o->fvar_j[v];
+        spmv_fq_kernel<<<ceil_div(n_pad, 256), 256, 0, ctx->stream>>>(
+            o->ccs.csr_ptr.p + (size_t)j * (desc->n + 1), o->ccs.csr_col.p + o->ccs.nnz_off[j],
+            o->ccs.csr_val.p + o->ccs.nnz_off[j], o->ccs.is_identity[j], desc->n, desc->m, z1.p, n_pad,
+            S + (size_t)(1 + v) * n_pad);
+        NEO_LAUNCHED(ctx);
+    }
+    // gamma^k, wg
+    o->gamma_to_k = gl::kone();
+    for (uint32_t i = 0; i < k; i++) o->gamma_to_k = gl::kmul(o->gamma_to_k, o->gamma);
+    std::vector<K> wg(nq);
+    {
+        K g = o->gamma;
+        for (uint32_t i = 0; i < k; i++) {
+            for (int rho = 0; rho < NEO_D; rho++) wg[i * NEO_D + rho] = gl::kmul(host_chi_mask(rho, o->beta_a), g);
+            g = gl::kmul(g, o->gamma);
+        }
+    }
+    NEO_CK(ctx, o->wg.alloc(nq));
+    NEO_CK(ctx, cudaMemcpyAsync(o->wg.p, wg.data(), nq * 16, cudaMemcpyHostToDevice, ctx->stream));
+    if (o->has_eval) {
+        NEO_CK(ctx, cudaMemcpyAsync(dbits.p, o->r_in.data(), ell_n * 16, cudaMemcpyHostToDevice, ctx->stream));
+        if ((rc = launch_chi_table(ctx, dbits.p, ell_n, S + (size_t)o->idx_eqrin * n_pad))) return rc;
+        // w[i*54+rho] = gamma^i chi_alpha[rho]
+        std::vector<K> w((size_t)nq), coef(t);
+        K gi = gl::kone();
+        for (uint32_t i = 0; i < k; i++) {
+            for (int rho = 0; rho < NEO_D; rho++) w[i * NEO_D + rho] = i ? gl::kmul(gi, host_chi_mask(rho, o->alpha)) : gl::kzero();
+            gi = gl::kmul(gi, o->gamma);
+        }
+        K gkj = gl::kone();
+        for (uint32_t j = 0; j < t; j++) { coef[j] = gkj; gkj = gl::kmul(gkj, o->gamma_to_k); }
+        DevBuf<K> dw, dcoef, du;
+        NEO_CK(ctx, dw.alloc(nq));
+        NEO_CK(ctx, dcoef.alloc(t));
+        NEO_CK(ctx, du.alloc(m));
+        NEO_CK(ctx, cudaMemcpyAsync(dw.p, w.data(), nq * 16, cudaMemcpyHostToDevice, ctx->stream));
+        NEO_CK(ctx, cudaMemcpyAsync(dcoef.p, coef.data(), t * 16, cudaMemcpyHostToDevice, ctx->stream));
+        eval_u_kernel<<<ceil_div(m, 256), 256, 0, ctx->stream>>>(o->Z.p, m, k, dw.p, du.p);
+        NEO_LAUNCHED(ctx);
+        DevBuf<uint8_t> isid;
+        NEO_CK(ctx, isid.alloc(t));
+        NEO_CK(ctx, cudaMemcpyAsync(isid.p, o->ccs.is_identity.data(), t, cudaMemcpyHostToDevice, ctx->stream));
+        DevBuf<uint64_t> nnzoff;
+        NEO_CK(ctx, nnzoff.alloc(t + 1));
+        NEO_CK(ctx, cudaMemcpyAsync(nnzoff.p, o->ccs.nnz_off.data(), (t + 1) * 8, cudaMemcpyHostToDevice, ctx->stream));
+        eval_tbl_kernel<<<ceil_div(n_pad, 256), 256, 0, ctx->stream>>>(
+            o->ccs.csr_ptr.p, o->ccs.csr_col.p, o->ccs.csr_val.p, nnzoff.p, isid.p, t, desc->n, desc->m, du.p,
+            dcoef.p, n_pad, S + (size_t)o->idx_eval * n_pad);
+        NEO_LAUNCHED(ctx);
+        NEO_CK(ctx, cudaStreamSynchronize(ctx->stream));
+    }
+    // streamed rounds and the materialised NC table
+    o->J = (int)std::min<uint32_t>(JMAX, ell_n - 1);
+    if ((uint32_t)o->J < ell_n - 1) {
+        uint64_t LJ = n_pad >> o->J;
+        NEO_CK(ctx, o->nc[0].alloc((size_t)nq * LJ));
+        NEO_CK(ctx, o->nc[1].alloc((size_t)nq * LJ / 2 + 1));
+    }
+    NEO_CK(ctx, o->eqw.alloc(1 << JMAX));
+    uint64_t max_blocks = (uint64_t)ceil_div(n_pad / 2, RT) * nq + 16;
+    NEO_CK(ctx, o->partials.alloc(max_blocks * (o->deg_max + 1)));
+    NEO_CK(ctx, o->coeffs.alloc(MAX_DEG + 1));
+    NEO_CK(ctx, o->ys.alloc(16));
+    NEO_CK(ctx, cudaStreamSynchronize(ctx->stream));
+    *out = guard.release();
+    return NEO_OK;
+}
+
+static int row_round(neo_gpu_ccs_oracle* o) {
+    neo_gpu_ctx* ctx = o->ctx;
+    const uint32_t j = o->round_idx;
+    const uint32_t nq = o->k * NEO_D;
+    RoundArgs a{};
+    a.pairs = o->n_pad >> (j + 1);
+    a.n_small = o->n_small;
+    a.n_fvar = o->n_fvar;
+    a.idx_eqrin = o->idx_eqrin;
+    a.idx_eval = o->idx_eval;
+    a.gamma_to_k = o->gamma_to_k;
+    a.f = o->f;
+    a.deg_max = o->deg_max;
+    a.wg = o->wg.p;
+    a.nq = (int)nq;
+    a.Z = o->Z.p;
+    a.m = o->m;
+    const bool last = j + 1 == o->ell_n;
+    // small tables
+    if (j == 0) {
+        a.small_in = o->small[0].p;
+        a.small_len_in = o->n_pad;
+        a.fold = 0;
+        a.small_out = nullptr;
+    } else {
+        a.small_in = o->small[o->small_cur].p;
+        a.small_len_in = o->n_pad >> (j - 1);
+        a.fold = 1;
+        a.r = o->row_chals[j - 1];
+        a.small_out = last ? nullptr : o->small[o->small_cur ^ 1].p;
+        a.small_len_out = o->n_pad >> j;
+    }
+    // NC source
+    const int J = o->J;
+    if ((int)j <= J) {
+        if (j > 0) {
+            std::vector<K> w(1u << j);
+            std::vector<K> pre(o->row_chals.begin(), o->row_chals.begin() + j);
+            for (uint32_t bsel = 0; bsel < (1u << j); bsel++) w[bsel] = host_chi_mask(bsel, pre);
+            NEO_CK(ctx, cudaMemcpyAsync(o->eqw.p, w.data(), w.size() * 16, cudaMemcpyHostToDevice, ctx->stream));
+        }
+        a.eqw = o->eqw.p;
+        if ((int)j == J && !last) {
+            a.nc_out = o->nc[0].p;
+            a.nc_len_out = o->n_pad >> j;
+            o->nc_cur = 0;
+        }
+    } else {
+        a.nc_in = o->nc[o->nc_cur].p;
+        a.nc_len_in = o->n_pad >> (j - 1);
+        a.r = o->row_chals[j - 1];
+        if (!last) {
+            a.nc_out = o->nc[o->nc_cur ^ 1].p;
+            a.nc_len_out = o->n_pad >> j;
+        }
+    }
+    // grid: x over pairs, y over q-chunks so that the GPU is filled
+    unsigned gx = ceil_div(a.pairs, RT);
+    unsigned target = 148 * 6;
+    unsigned gy = std::min<unsigned>(nq, std::max<unsigned>(1, (target + gx - 1) / gx));
+    int qpb = (int)ceil_div(nq, gy);
+    if (qpb > 1024) qpb = 1024;
+    gy = ceil_div(nq, qpb);
+    a.q_per_block = qpb;
+    a.partials = o->partials.p;
+    dim3 grid(gx, gy);
+    switch ((int)j <= J ? (int)j : JMAX + 1) {
+        case 0: ccs_round_kernel<0><<<grid, RT, 0, ctx->stream>>>(a); break;
+        case 1: ccs_round_kernel<1><<<grid, RT, 0, ctx->stream>>>(a); break;
+        case 2: ccs_round_kernel<2><<<grid, RT, 0, ctx->stream>>>(a); break;
+        case 3: ccs_round_kernel<3><<<grid, RT, 0, ctx->stream>>>(a); break;
+        case 4: ccs_round_kernel<4><<<grid, RT, 0, ctx->stream>>>(a); break;
+        default: ccs_round_kernel<JMAX + 1><<<grid, RT, 0, ctx->stream>>>(a); break;
+    }
+    NEO_LAUNCHED(ctx);
+    if (j > 0 && !last) o->small_cur ^= 1;
+    if ((int)j > J && !last) o->nc_cur ^= 1;
+    // reduce
+    EvalArgs e{};
+    e.partials = o->partials.p;
+    e.nblocks = gx * gy;
+    e.ncoef = o->deg_max + 1;
+    e.nx = 0;
+    e.coeffs_out = o->coeffs.p;
+    e.ys_out = o->ys.p;
+    reduce_eval_kernel<<<1, 256, 0, ctx->stream>>>(e);
+    NEO_LAUNCHED(ctx);
+    o->h_coeffs.resize(o->deg_max + 1);
+    NEO_CK(ctx, cudaMemcpyAsync(o->h_coeffs.data(), o->coeffs.p, (o->deg_max + 1) * 16, cudaMemcpyDeviceToHost, ctx->stream));
+    NEO_CK(ctx, cudaStreamSynchronize(ctx->stream));
+    o->coeffs_valid = true;
+    return NEO_OK;
+}
+
+static int ajtai_precompute(neo_gpu_ccs_oracle* o) {
+    neo_gpu_ctx* ctx = o->ctx;
+    NEO_CK(ctx, o->chi_r.alloc(o->n_pad));
+    NEO_CK(ctx, o->vj.alloc((size_t)o->t * o->m));
+    NEO_CK(ctx, o->y_eval.alloc((size_t)o->k * o->t * NEO_D));
+    NEO_CK(ctx, o->y_sc.alloc((size_t)o->k * o->t));
+    DevBuf<K> dbits;
+    NEO_CK(ctx, dbits.alloc(o->ell_n));
+    NEO_CK(ctx, cudaMemcpyAsync(dbits.p, o->row_chals.data(), o->ell_n * 16, cudaMemcpyHostToDevice, ctx->stream));
+    int rc = launch_chi_table(ctx, dbits.p, o->ell_n, o->chi_r.p);
+    if (rc) return rc;
+    rc = launch_me_y(ctx, o->ccs, o->Z.p, o->k, o->m, o->chi_r.p, o->ell_n, o->b, o->vj.p, o->y_eval.p, o->y_sc.p);
+    if (rc) return rc;
+    NEO_CK(ctx, cudaStreamSynchronize(ctx->stream));
+    o->have_pre = true;
+    return NEO_OK;
+}
+
+static int ajtai_round(neo_gpu_ccs_oracle* o, const uint64_t* xs, uint32_t nx, uint64_t* ys) {
+    neo_gpu_ctx* ctx = o->ctx;
+    if (!o->have_pre) {
+        int rc = ajtai_precompute(o);
+        if (rc) return rc;
+    }
+    if (nx > 16 || o->ell_n > 32 || o->ell_d > 8 || o->k * (1 + o->t) > 160)
+        return ctx->fail(NEO_ERR_UNSUPPORTED, "ccs_oracle: ajtai phase size limits");
+    AjtaiArgs a{};
+    a.k = (int)o->k; a.t = (int)o->t; a.ell_d = (int)o->ell_d; a.ell_n = (int)o->ell_n;
+    a.j = (int)(o->round_idx - o->ell_n);
+    a.nx = (int)nx;
+    a.has_inputs = o->has_inputs;
+    for (uint32_t i = 0; i < nx; i++) a.xs[i] = gl::kmk(gl::canon(xs[2 * i]), gl::canon(xs[2 * i + 1]));
+    for (uint32_t i = 0; i < o->ell_d; i++) { a.alpha[i] = o->alpha[i]; a.beta_a[i] = o->beta_a[i]; }
+    for (size_t i = 0; i < o->ajtai_chals.size(); i++) a.ajtai_chals[i] = o->ajtai_chals[i];
+    for (uint32_t i = 0; i < o->ell_n; i++) {
+        a.beta_r[i] = o->beta_r[i];
+        a.row_chals[i] = o->row_chals[i];
+        if (o->has_inputs) a.r_in[i] = o->r_in[i];
+    }
+    a.gamma = o->gamma;
+    a.f = o->f;
+    for (int v = 0; v < o->n_fvar; v++) a.fvar_j[v] = o->fvar_j[v];
+    a.y = o->y_eval.p;
+    a.ysc = o->y_sc.p;
+    a.ys_out = o->ys.p;
+    size_t smem = (size_t)o->k * (1 + o->t) * NEO_D * sizeof(K);
+    NEO_CK(ctx, cudaFuncSetAttribute(ajtai_round_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    ajtai_round_kernel<<<1, 512, smem, ctx->stream>>>(a);
+    NEO_LAUNCHED(ctx);
+    NEO_CK(ctx, cudaMemcpyAsync(ys, o->ys.p, nx * 16, cudaMemcpyDeviceToHost, ctx->stream));
+    NEO_CK(ctx, cudaStreamSynchronize(ctx->stream));
+    return NEO_OK;
+}
+
+extern "C" int neo_gpu_ccs_oracle_evals(neo_gpu_ccs_oracle* o, const uint64_t* xs, uint32_t nx, uint64_t* ys) {
+    if (!o) return NEO_ERR_ARG;
+    neo_gpu_ctx* ctx = o->ctx;
+    if (!xs || !ys || nx == 0 || nx > 16) return ctx->fail(NEO_ERR_ARG, "evals: bad args");
+    if (o->round_idx >= o->ell_n + o->ell_d) return ctx->fail(NEO_ERR_ARG, "evals: all rounds done");
+    cudaSetDevice(ctx->device);
+    if (o->round_idx < o->ell_n) {
+        if (!o->coeffs_valid) {
+            int rc = row_round(o);
+            if (rc) return rc;
+        }
+        // Horner at each x (sumcheck.rs:48-60)
+        for (uint32_t i = 0; i < nx; i++) {
+            K x = gl::kmk(gl::canon(xs[2 * i]), gl::canon(xs[2 * i + 1]));
+            K r = o->h_coeffs.back();
+            for (int d = (int)o->h_coeffs.size() - 2; d >= 0; d--) r = gl::kadd(gl::kmul(r, x), o->h_coeffs[d]);
+            ys[2 * i] = r.re;
+            ys[2 * i + 1] = r.im;
+        }
+        return NEO_OK;
+    }
+    return ajtai_round(o, xs, nx, ys);
+}
+
+extern "C" int neo_gpu_ccs_oracle_fold(neo_gpu_ccs_oracle* o, const uint64_t* r) {
+    if (!o) return NEO_ERR_ARG;
+    if (!r) return o->ctx->fail(NEO_ERR_ARG, "fold: null r");
+    K rr = gl::kmk(gl::canon(r[0]), gl::canon(r[1]));
+    if (o->round_idx < o->ell_n) {
+        o->row_chals.push_back(rr);
+        o->coeffs_valid = false;
+    } else if (o->round_idx < o->ell_n + o->ell_d) {
+        o->ajtai_chals.push_back(rr);
+    } else {
+        return o->ctx->fail(NEO_ERR_ARG, "fold: all rounds done");
+    }
+    o->round_idx++;
+    return NEO_OK;
+}
+
+extern "C" uint32_t neo_gpu_ccs_oracle_num_rounds(const neo_gpu_ccs_oracle* o) { return o ? o->ell_n + o->ell_d : 0; }
+extern "C" uint32_t neo_gpu_ccs_oracle_degree_bound(const neo_gpu_ccs_oracle* o) { return o ? o->d_sc : 0; }
+
+extern "C" int neo_gpu_ccs_oracle_me_outputs(neo_gpu_ccs_oracle* o, uint64_t* y, uint64_t* y_scalars) {
+    if (!o) return NEO_ERR_ARG;
+    neo_gpu_ctx* ctx = o->ctx;
+    if (!y || !y_scalars) return ctx->fail(NEO_ERR_ARG, "me_outputs: null output");
+    if (o->row_chals.size() != o->ell_n) return ctx->fail(NEO_ERR_ARG, "me_outputs: row challenges not finalized");
+    cudaSetDevice(ctx->device);
+    if (!o->have_pre) {
+        int rc = ajtai_precompute(o);
+        if (rc) return rc;
+    }
+    NEO_CK(ctx, cudaMemcpyAsync(y, o->y_eval.p, o->y_eval.bytes(), cudaMemcpyDeviceToHost, ctx->stream));
+    NEO_CK(ctx, cudaMemcpyAsync(y_scalars, o->y_sc.p, o->y_sc.bytes(), cudaMemcpyDeviceToHost, ctx->stream));
+    NEO_CK(ctx, cudaStreamSynchronize(ctx->stream));
+    return NEO_OK;
+}
+
+extern "C" int neo_gpu_ccs_oracle_destroy(neo_gpu_ccs_oracle* o) {
+    if (!o) return NEO_ERR_ARG;
+    cudaSetDevice(o->ctx->device);
+    cudaStreamSynchronize(o->ctx->stream);
+    delete o;
+    return NEO_OK;
+}

@@ -1,0 +1,136 @@
+// commit.cu -- Ajtai commitment c_i = sum_j M[i][j] * z_j in R_q = F_q[X]/Phi_81.
+//
+// Reference: commit_precomp_ct_row_major (crates/neo-ajtai/src/commit.rs:679-744)
+// computes c_i = sum_j rot(a_ij) Z[:, j] column by column.  Here the product
+// is taken modulo X^81 - 1 (Phi_81 divides X^81 - 1), i.e. a cyclic
+// convolution of length 81 whose matrix entries are the raw PP coefficients,
+// and the 81 coefficients are folded back to 54 with X^54 = -X^27 - 1 in the
+// epilogue.  This file holds the CUDA-core kernel: split-K over column
+// chunks, exact F_q accumulation, then a cross-chunk reduction.
+#include "internal.cuh"
+
+using gl::K;
+
+namespace {
+
+constexpr int CHUNK_COLS = 32;    // columns staged per shared-memory tile
+constexpr int COMMIT_THREADS = 96;  // >= 81 output coefficients
+
+// partial[(v*n_chunks + chunk)*kappa + i][r], r < 81
+__global__ void __launch_bounds__(COMMIT_THREADS)
+commit_partial_kernel(const uint64_t* __restrict__ pp, uint32_t kappa, uint64_t m, const int8_t* __restrict__ digits,
+                      uint32_t cols_per_block, uint64_t* __restrict__ partial) {
+    const uint32_t chunk = blockIdx.x, i = blockIdx.y, v = blockIdx.z;
+    const uint32_t n_chunks = gridDim.x;
+    __shared__ uint64_t s_a[CHUNK_COLS][NEO_D];
+    __shared__ int8_t s_z[CHUNK_COLS][NEO_D + 2];
+    const int r = threadIdx.x;
+    uint64_t acc = 0;
+    const uint64_t j_begin = (uint64_t)chunk * cols_per_block;
+    uint64_t j_end = j_begin + cols_per_block;
+    if (j_end > m) j_end = m;
+    const int8_t* Zv = digits + (uint64_t)v * NEO_D * m;
+    for (uint64_t j0 = j_begin; j0 < j_end; j0 += CHUNK_COLS) {
+        const int ncol = (int)((j_end - j0) < CHUNK_COLS ? (j_end - j0) : CHUNK_COLS);
+        __syncthreads();
+        for (int x = threadIdx.x; x < ncol * NEO_D; x += blockDim.x) {
+            int c = x / NEO_D, s = x % NEO_D;
+            s_a[c][s] = pp[((uint64_t)i * m + j0 + c) * NEO_D + s];
+        }
+        for (int x = threadIdx.x; x < ncol * NEO_D; x += blockDim.x) {
+            int t = x / ncol, c = x % ncol;
+            s_z[c][t] = Zv[(uint64_t)t * m + j0 + c];
+        }
+        __syncthreads();
+        if (r < 81) {
+            for (int c = 0; c < ncol; c++) {
+                // c'[r] += sum_s a[s] * z[(r - s) mod 81], z[p] = 0 for p >= 54
+#pragma unroll 6
+                for (int s = 0; s < NEO_D; s++) {
+                    int p = r - s;
+                    p += (p < 0) ? 81 : 0;
+                    if (p < NEO_D) {
+                        int z = s_z[c][p];
+                        if (z == 1) acc = gl::add(acc, s_a[c][s]);
+                        else if (z == -1) acc = gl::sub(acc, s_a[c][s]);
+                        else if (z != 0) acc = gl::add(acc, gl::mul(s_a[c][s], gl::from_i64(z)));
+                    }
+                }
+            }
+        }
+    }
+    if (r < 81) partial[(((uint64_t)v * n_chunks + chunk) * kappa + i) * 81 + r] = acc;
+}
+
+// sum partials over chunks, then fold 81 -> 54: c[r] = c'[r] - c'[r+27] (r>=27) - c'[r+54] (r<27)
+__global__ void commit_reduce_kernel(const uint64_t* __restrict__ partial, uint32_t n_chunks, uint32_t kappa,
+                                     uint32_t n_vec, uint64_t* __restrict__ out) {
+    const uint32_t vi = blockIdx.x;  // v*kappa + i
+    const uint32_t v = vi / kappa, i = vi % kappa;
+    __shared__ uint64_t s_c[81];
+    for (int r = threadIdx.x; r < 81; r += blockDim.x) {
+        uint64_t acc = 0;
+        for (uint32_t ch = 0; ch < n_chunks; ch++) acc = gl::add(acc, partial[(((uint64_t)v * n_chunks + ch) * kappa + i) * 81 + r]);
+        s_c[r] = acc;
+    }
+    __syncthreads();
+    for (int r = threadIdx.x; r < NEO_D; r += blockDim.x) {
+        uint64_t c = s_c[r];
+        c = gl::sub(c, r >= 27 ? s_c[r + 27] : s_c[r + 54]);
+        out[((uint64_t)v * kappa + i) * NEO_D + r] = c;
+    }
+}
+
+}  // namespace
+
+int launch_commit(neo_gpu_ctx* ctx, const int8_t* d_digits, uint32_t n_vec, uint64_t m, uint64_t* d_out) {
+    if (!ctx->d_pp || ctx->pp_m != m) return ctx->fail(NEO_ERR_ARG, "commit: PP not loaded for this m");
+    const uint32_t kappa = ctx->kappa;
+    // pick a chunking that fills the GPU: ~4 blocks per SM in total
+    uint32_t target_blocks = 148 * 8;
+    uint32_t per = (uint32_t)((uint64_t)kappa * n_vec);
+    uint32_t n_chunks = (target_blocks + per - 1) / per;
+    uint64_t cols_per_block = (m + n_chunks - 1) / n_chunks;
+    if (cols_per_block < CHUNK_COLS) cols_per_block = CHUNK_COLS;
+    n_chunks = (uint32_t)((m + cols_per_block - 1) / cols_per_block);
+    DevBuf<uint64_t> partial;
+    NEO_CK(ctx, partial.alloc((size_t)n_vec * n_chunks * kappa * 81));
+    dim3 grid(n_chunks, kappa, n_vec);
+    commit_partial_kernel<<<grid, COMMIT_THREADS, 0, ctx->stream>>>(ctx->d_pp, kappa, m, d_digits,
+                                                                     (uint32_t)cols_per_block, partial.p);
+    NEO_LAUNCHED(ctx);
+    commit_reduce_kernel<<<n_vec * kappa, 96, 0, ctx->stream>>>(partial.p, n_chunks, kappa, n_vec, d_out);
+    NEO_LAUNCHED(ctx);
+    // partial is freed at scope exit: make sure the kernels are done with it
+    NEO_CK(ctx, cudaStreamSynchronize(ctx->stream));
+    return NEO_OK;
+}
+
+extern "C" int neo_gpu_pp_upload(neo_gpu_ctx* ctx, uint32_t kappa, uint64_t m, const uint64_t* coeffs) {
+    if (!ctx) return NEO_ERR_ARG;
+    if (!coeffs || kappa == 0 || m == 0 || kappa > 64) return ctx->fail(NEO_ERR_ARG, "pp_upload: bad args");
+    cudaSetDevice(ctx->device);
+    if (ctx->d_pp) { cudaFree(ctx->d_pp); ctx->d_pp = nullptr; }
+    size_t n = (size_t)kappa * m * NEO_D;
+    NEO_CK(ctx, cudaMalloc(&ctx->d_pp, n * 8));
+    NEO_CK(ctx, cudaMemcpy(ctx->d_pp, coeffs, n * 8, cudaMemcpyHostToDevice));
+    ctx->kappa = kappa;
+    ctx->pp_m = m;
+    return NEO_OK;
+}
+
+extern "C" int neo_gpu_commit(neo_gpu_ctx* ctx, const int8_t* digits, uint32_t n_vec, uint64_t m, uint64_t* out) {
+    if (!ctx) return NEO_ERR_ARG;
+    if (!digits || !out || n_vec == 0 || m == 0) return ctx->fail(NEO_ERR_ARG, "commit: bad args");
+    cudaSetDevice(ctx->device);
+    DevBuf<int8_t> dZ;
+    DevBuf<uint64_t> dout;
+    NEO_CK(ctx, dZ.alloc((size_t)n_vec * NEO_D * m));
+    NEO_CK(ctx, dout.alloc((size_t)n_vec * ctx->kappa * NEO_D));
+    NEO_CK(ctx, cudaMemcpyAsync(dZ.p, digits, dZ.bytes(), cudaMemcpyHostToDevice, ctx->stream));
+    int rc = launch_commit(ctx, dZ.p, n_vec, m, dout.p);
+    if (rc) return rc;
+    NEO_CK(ctx, cudaMemcpyAsync(out, dout.p, dout.bytes(), cudaMemcpyDeviceToHost, ctx->stream));
+    NEO_CK(ctx, cudaStreamSynchronize(ctx->stream));
+    return NEO_OK;
+}

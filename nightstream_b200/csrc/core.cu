@@ -1,0 +1,423 @@
+// core.cu -- context, CCS upload, decomposition, Pi_RLC mix, Pi_DEC split and
+// ME evaluations y = Z (M^T chi_r).
+#include "internal.cuh"
+#include <algorithm>
+
+using gl::K;
+
+extern "C" int neo_gpu_ctx_create(int device, neo_gpu_ctx** out) {
+    if (!out) return NEO_ERR_ARG;
+    *out = nullptr;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return NEO_ERR_CUDA;
+    if (device < 0 || device >= ndev) return NEO_ERR_ARG;
+    if (cudaSetDevice(device) != cudaSuccess) return NEO_ERR_CUDA;
+    neo_gpu_ctx* c = new neo_gpu_ctx();
+    c->device = device;
+    if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) {
+        delete c;
+        return NEO_ERR_CUDA;
+    }
+    *out = c;
+    return NEO_OK;
+}
+
+extern "C" int neo_gpu_ctx_destroy(neo_gpu_ctx* ctx) {
+    if (!ctx) return NEO_ERR_ARG;
+    cudaSetDevice(ctx->device);
+    cudaStreamSynchronize(ctx->stream);
+    if (ctx->d_pp) cudaFree(ctx->d_pp);
+    if (ctx->d_pp_limbs) cudaFree(ctx->d_pp_limbs);
+    cudaStreamDestroy(ctx->stream);
+    delete ctx;
+    return NEO_OK;
+}
+
+extern "C" const char* neo_gpu_last_error(const neo_gpu_ctx* ctx) { return ctx ? ctx->err.c_str() : "null context"; }
+extern "C" uint64_t neo_gpu_kernel_launches(const neo_gpu_ctx* ctx) { return ctx ? ctx->launches : 0; }
+
+// ---------------------------------------------------------------------------
+// CCS upload: CSC as given, plus a CSR copy built on the host.
+// ---------------------------------------------------------------------------
+int dev_ccs_upload(neo_gpu_ctx* ctx, const neo_ccs_desc* d, DevCcs& o) {
+    if (!d || d->t == 0 || d->m == 0 || d->n == 0 || d->t > 16 || d->n_terms == 0 || d->n_terms > 16)
+        return ctx->fail(NEO_ERR_ARG, "ccs: bad dimensions");
+    o.n = d->n; o.m = d->m; o.t = d->t; o.n_terms = d->n_terms;
+    o.is_identity.assign(d->is_identity, d->is_identity + d->t);
+    o.f_coeff.assign(d->f_coeff, d->f_coeff + d->n_terms);
+    o.f_exps.assign(d->f_exps, d->f_exps + (size_t)d->n_terms * d->t);
+    o.nnz_off.assign(d->nnz_off, d->nnz_off + d->t + 1);
+    uint64_t nnz = o.nnz_off[d->t];
+    std::vector<uint64_t> csr_ptr((size_t)d->t * (d->n + 1), 0);
+    std::vector<uint32_t> csr_col(std::max<uint64_t>(nnz, 1));
+    std::vector<uint64_t> csr_val(std::max<uint64_t>(nnz, 1));
+    for (uint32_t j = 0; j < d->t; j++) {
+        if (o.is_identity[j]) continue;
+        const uint64_t* cp = d->col_ptr + (size_t)j * (d->m + 1);
+        uint64_t base = o.nnz_off[j];
+        uint64_t cnt = o.nnz_off[j + 1] - base;
+        if (cp[d->m] != cnt) return ctx->fail(NEO_ERR_ARG, "ccs: col_ptr inconsistent with nnz_off");
+        uint64_t* rp = csr_ptr.data() + (size_t)j * (d->n + 1);
+        for (uint64_t k = 0; k < cnt; k++) {
+            uint32_t r = d->row_idx[base + k];
+            if (r >= d->n) return ctx->fail(NEO_ERR_ARG, "ccs: row index out of range");
+            rp[r + 1]++;
+        }
+        for (uint32_t r = 0; r < d->n; r++) rp[r + 1] += rp[r];
+        std::vector<uint64_t> fill(rp, rp + d->n);
+        for (uint32_t c = 0; c < d->m; c++)
+            for (uint64_t k = cp[c]; k < cp[c + 1]; k++) {
+                uint32_t r = d->row_idx[base + k];
+                uint64_t pos = base + fill[r]++;
+                csr_col[pos] = c;
+                csr_val[pos] = gl::canon(d->vals[base + k]);
+            }
+    }
+    size_t nn = std::max<uint64_t>(nnz, 1);
+    NEO_CK(ctx, o.csr_ptr.alloc(csr_ptr.size()));
+    NEO_CK(ctx, o.csr_col.alloc(nn));
+    NEO_CK(ctx, o.csr_val.alloc(nn));
+    NEO_CK(ctx, o.csc_ptr.alloc((size_t)d->t * (d->m + 1)));
+    NEO_CK(ctx, o.csc_row.alloc(nn));
+    NEO_CK(ctx, o.csc_val.alloc(nn));
+    NEO_CK(ctx, cudaMemcpy(o.csr_ptr.p, csr_ptr.data(), csr_ptr.size() * 8, cudaMemcpyHostToDevice));
+    NEO_CK(ctx, cudaMemcpy(o.csr_col.p, csr_col.data(), nn * 4, cudaMemcpyHostToDevice));
+    NEO_CK(ctx, cudaMemcpy(o.csr_val.p, csr_val.data(), nn * 8, cudaMemcpyHostToDevice));
+    std::vector<uint64_t> csc_ptr((size_t)d->t * (d->m + 1), 0);
+    for (uint32_t j = 0; j < d->t; j++)
+        if (!o.is_identity[j]) memcpy(&csc_ptr[(size_t)j * (d->m + 1)], d->col_ptr + (size_t)j * (d->m + 1), (d->m + 1) * 8);
+    std::vector<uint64_t> csc_val(nn, 0);
+    if (nnz) for (uint64_t k = 0; k < nnz; k++) csc_val[k] = gl::canon(d->vals[k]);
+    NEO_CK(ctx, cudaMemcpy(o.csc_ptr.p, csc_ptr.data(), csc_ptr.size() * 8, cudaMemcpyHostToDevice));
+    if (nnz) {
+        NEO_CK(ctx, cudaMemcpy(o.csc_row.p, d->row_idx, nnz * 4, cudaMemcpyHostToDevice));
+        NEO_CK(ctx, cudaMemcpy(o.csc_val.p, csc_val.data(), nnz * 8, cudaMemcpyHostToDevice));
+    }
+    return NEO_OK;
+}
+
+// ---------------------------------------------------------------------------
+// chi table: w[mask] = prod_i (bit_i(mask) ? b_i : 1 - b_i)
+// (crates/neo-reductions/src/engines/optimized_engine/oracle.rs:1525-1540)
+// ---------------------------------------------------------------------------
+__global__ void chi_table_kernel(const K* __restrict__ bits, uint32_t nbits, K* __restrict__ out) {
+    uint64_t idx = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+    if (idx >= (1ULL << nbits)) return;
+    K w = gl::kone();
+    for (uint32_t i = 0; i < nbits; i++) {
+        K b = bits[i];
+        w = gl::kmul(w, ((idx >> i) & 1) ? b : gl::ksub(gl::kone(), b));
+    }
+    out[idx] = w;
+}
+
+int launch_chi_table(neo_gpu_ctx* ctx, const K* d_bits, uint32_t nbits, K* d_out) {
+    uint64_t len = 1ULL << nbits;
+    chi_table_kernel<<<ceil_div(len, 256), 256, 0, ctx->stream>>>(d_bits, nbits, d_out);
+    NEO_LAUNCHED(ctx);
+    return NEO_OK;
+}
+
+// ---------------------------------------------------------------------------
+// decomp_b (b = 2, balanced) (crates/neo-ajtai/src/decomp.rs:118-158)
+// ---------------------------------------------------------------------------
+__global__ void decomp_b2_kernel(const uint64_t* __restrict__ z, uint64_t m, int8_t* __restrict__ Z) {
+    uint64_t c = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+    if (c >= m) return;
+    uint64_t u = gl::canon(z[c]);
+    const uint64_t half = (GL_Q - 1) / 2;
+    int64_t a = u <= half ? (int64_t)u : -(int64_t)(GL_Q - u);
+#pragma unroll
+    for (int row = 0; row < NEO_D; row++) {
+        int64_t digit = (a & 1) == 0 ? 0 : (a >= 0 ? 1 : -1);
+        Z[(uint64_t)row * m + c] = (int8_t)digit;
+        a = (a - digit) >> 1;
+    }
+}
+
+extern "C" int neo_gpu_decomp_b2(neo_gpu_ctx* ctx, const uint64_t* z, uint64_t m, int8_t* Z) {
+    if (!ctx || !z || !Z || m == 0) return ctx ? ctx->fail(NEO_ERR_ARG, "decomp: bad args") : NEO_ERR_ARG;
+    cudaSetDevice(ctx->device);
+    DevBuf<uint64_t> dz;
+    DevBuf<int8_t> dZ;
+    NEO_CK(ctx, dz.alloc(m));
+    NEO_CK(ctx, dZ.alloc((size_t)NEO_D * m));
+    NEO_CK(ctx, cudaMemcpyAsync(dz.p, z, m * 8, cudaMemcpyHostToDevice, ctx->stream));
+    decomp_b2_kernel<<<ceil_div(m, 256), 256, 0, ctx->stream>>>(dz.p, m, dZ.p);
+    NEO_LAUNCHED(ctx);
+    NEO_CK(ctx, cudaMemcpyAsync(Z, dZ.p, (size_t)NEO_D * m, cudaMemcpyDeviceToHost, ctx->stream));
+    NEO_CK(ctx, cudaStreamSynchronize(ctx->stream));
+    return NEO_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Pi_RLC mix: Z_mix[:, c] = sum_i a_i(X) z_{i,c}(X) mod Phi_81 over the
+// integers (all entries are small, so this equals the F_q computation of
+// optimized_engine/common.rs:1221-1379 with rot_from_coeffs common.rs:398-430).
+// One thread per column; rot matrices live in shared memory as int8.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(128) rlc_mix_kernel(const int8_t* __restrict__ rot, const int8_t* __restrict__ Zs,
+                                                      uint32_t count, uint64_t m, int32_t* __restrict__ Zmix) {
+    extern __shared__ int8_t s_rot[];  // [count][54][54] row-major rot(a_i)[r][k]
+    for (uint32_t x = threadIdx.x; x < count * NEO_D * NEO_D; x += blockDim.x) s_rot[x] = rot[x];
+    __syncthreads();
+    uint64_t c = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+    if (c >= m) return;
+    int32_t acc[NEO_D];
+#pragma unroll
+    for (int r = 0; r < NEO_D; r++) acc[r] = 0;
+    for (uint32_t i = 0; i < count; i++) {
+        const int8_t* Zi = Zs + (uint64_t)i * NEO_D * m;
+        const int8_t* R = s_rot + i * NEO_D * NEO_D;
+        for (int k = 0; k < NEO_D; k++) {
+            int z = Zi[(uint64_t)k * m + c];
+            if (z == 0) continue;
+#pragma unroll
+            for (int r = 0; r < NEO_D; r++) acc[r] += z * (int)R[r * NEO_D + k];
+        }
+    }
+#pragma unroll
+    for (int r = 0; r < NEO_D; r++) Zmix[(uint64_t)r * m + c] = acc[r];
+}
+
+// integer rot(a): column t = a X^t mod Phi_81 (commit.rs:46-54 recurrence)
+static void rot_int8(const int8_t* a, int8_t* out) {
+    int32_t col[NEO_D], nxt[NEO_D];
+    for (int r = 0; r < NEO_D; r++) col[r] = a[r];
+    for (int t = 0; t < NEO_D; t++) {
+        for (int r = 0; r < NEO_D; r++) out[r * NEO_D + t] = (int8_t)col[r];
+        int32_t last = col[NEO_D - 1];
+        nxt[0] = -last;
+        for (int q = 1; q < NEO_D; q++) nxt[q] = col[q - 1];
+        nxt[27] -= last;
+        memcpy(col, nxt, sizeof col);
+    }
+}
+
+int rlc_mix_device(neo_gpu_ctx* ctx, const int8_t* rho_coeffs_host, const int8_t* d_Zs, uint32_t count, uint64_t m,
+                   int32_t* d_Zmix, int8_t* d_rot_scratch) {
+    std::vector<int8_t> rot((size_t)count * NEO_D * NEO_D);
+    for (uint32_t i = 0; i < count; i++) {
+        for (int r = 0; r < NEO_D; r++)
+            if (rho_coeffs_host[i * NEO_D + r] < -2 || rho_coeffs_host[i * NEO_D + r] > 2)
+                return ctx->fail(NEO_ERR_ARG, "rlc: rho coefficient outside {-2..2}");
+        if (count == 1) {
+            memset(rot.data(), 0, NEO_D * NEO_D);
+            for (int r = 0; r < NEO_D; r++) rot[r * NEO_D + r] = 1;  // identity (common.rs:560-564)
+        } else {
+            rot_int8(rho_coeffs_host + i * NEO_D, rot.data() + (size_t)i * NEO_D * NEO_D);
+        }
+    }
+    NEO_CK(ctx, cudaMemcpyAsync(d_rot_scratch, rot.data(), rot.size(), cudaMemcpyHostToDevice, ctx->stream));
+    size_t smem = rot.size();
+    if (smem > 48 * 1024) NEO_CK(ctx, cudaFuncSetAttribute(rlc_mix_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    rlc_mix_kernel<<<ceil_div(m, 128), 128, smem, ctx->stream>>>(d_rot_scratch, d_Zs, count, m, d_Zmix);
+    NEO_LAUNCHED(ctx);
+    return NEO_OK;
+}
+
+extern "C" int neo_gpu_rlc_mix(neo_gpu_ctx* ctx, const int8_t* rho_coeffs, const int8_t* Zs, uint32_t count,
+                               uint64_t m, int32_t* Zmix) {
+    if (!ctx) return NEO_ERR_ARG;
+    if (!rho_coeffs || !Zs || !Zmix || count == 0 || count > 64 || m == 0) return ctx->fail(NEO_ERR_ARG, "rlc: bad args");
+    cudaSetDevice(ctx->device);
+    DevBuf<int8_t> dZs, drot;
+    DevBuf<int32_t> dmix;
+    NEO_CK(ctx, dZs.alloc((size_t)count * NEO_D * m));
+    NEO_CK(ctx, drot.alloc((size_t)count * NEO_D * NEO_D));
+    NEO_CK(ctx, dmix.alloc((size_t)NEO_D * m));
+    NEO_CK(ctx, cudaMemcpyAsync(dZs.p, Zs, dZs.bytes(), cudaMemcpyHostToDevice, ctx->stream));
+    int rc = rlc_mix_device(ctx, rho_coeffs, dZs.p, count, m, dmix.p, drot.p);
+    if (rc) return rc;
+    NEO_CK(ctx, cudaMemcpyAsync(Zmix, dmix.p, dmix.bytes(), cudaMemcpyDeviceToHost, ctx->stream));
+    NEO_CK(ctx, cudaStreamSynchronize(ctx->stream));
+    return NEO_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Pi_DEC split (common.rs:75-268; balanced_divrem common.rs:44-58)
+// flags[0] = out-of-range error, flags[1 + i] = plane i nonzero
+// ---------------------------------------------------------------------------
+__global__ void split_b_kernel(const int32_t* __restrict__ Zmix, uint64_t len, uint32_t k, int32_t b,
+                               int8_t* __restrict__ planes, uint32_t* __restrict__ flags) {
+    uint64_t idx = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+    uint32_t nz_mask = 0;
+    if (idx < len) {
+        int64_t v = Zmix[idx];
+        int64_t B = 1;
+        for (uint32_t i = 0; i < k; i++) B *= b;
+        if (v >= B || v <= -B) atomicOr(&flags[0], 1u);
+        int64_t half = b / 2;
+        for (uint32_t i = 0; i < k; i++) {
+            int64_t r = v % b;
+            int64_t q = (v - r) / b;
+            if (r > half) { r -= b; q += 1; }
+            else if (r < -half) { r += b; q -= 1; }
+            planes[(uint64_t)i * len + idx] = (int8_t)r;
+            if (r) nz_mask |= 1u << i;
+            v = q;
+        }
+        if (v != 0) atomicOr(&flags[0], 1u);
+    }
+    // warp-aggregate the nonzero plane mask
+    for (int o = 16; o > 0; o >>= 1) nz_mask |= __shfl_xor_sync(0xffffffffu, nz_mask, o);
+    if ((threadIdx.x & 31) == 0 && nz_mask) atomicOr(&flags[1], nz_mask);
+}
+
+int split_b_device(neo_gpu_ctx* ctx, const int32_t* d_Zmix, uint64_t len, uint32_t k, uint32_t b, int8_t* d_planes,
+                   uint32_t* d_flags) {
+    if (k == 0 || k > 31 || b < 2 || b > 64) return ctx->fail(NEO_ERR_UNSUPPORTED, "split_b: k/b out of range");
+    NEO_CK(ctx, cudaMemsetAsync(d_flags, 0, 2 * sizeof(uint32_t), ctx->stream));
+    split_b_kernel<<<ceil_div(len, 256), 256, 0, ctx->stream>>>(d_Zmix, len, k, (int32_t)b, d_planes, d_flags);
+    NEO_LAUNCHED(ctx);
+    return NEO_OK;
+}
+
+extern "C" int neo_gpu_split_b(neo_gpu_ctx* ctx, const int32_t* Zmix, uint64_t len, uint32_t k, uint32_t b,
+                               int8_t* planes, uint8_t* nonzero) {
+    if (!ctx) return NEO_ERR_ARG;
+    if (!Zmix || !planes || !nonzero || len == 0) return ctx->fail(NEO_ERR_ARG, "split_b: bad args");
+    cudaSetDevice(ctx->device);
+    DevBuf<int32_t> dmix;
+    DevBuf<int8_t> dpl;
+    DevBuf<uint32_t> dfl;
+    NEO_CK(ctx, dmix.alloc(len));
+    NEO_CK(ctx, dpl.alloc((size_t)k * len));
+    NEO_CK(ctx, dfl.alloc(2));
+    NEO_CK(ctx, cudaMemcpyAsync(dmix.p, Zmix, len * 4, cudaMemcpyHostToDevice, ctx->stream));
+    int rc = split_b_device(ctx, dmix.p, len, k, b, dpl.p, dfl.p);
+    if (rc) return rc;
+    uint32_t flags[2];
+    NEO_CK(ctx, cudaMemcpyAsync(flags, dfl.p, 8, cudaMemcpyDeviceToHost, ctx->stream));
+    NEO_CK(ctx, cudaMemcpyAsync(planes, dpl.p, (size_t)k * len, cudaMemcpyDeviceToHost, ctx->stream));
+    NEO_CK(ctx, cudaStreamSynchronize(ctx->stream));
+    if (flags[0]) return ctx->fail(NEO_ERR_INVARIANT, "DEC split: entry out of range for k_rho digits");
+    for (uint32_t i = 0; i < k; i++) nonzero[i] = (flags[1] >> i) & 1;
+    return NEO_OK;
+}
+
+// ---------------------------------------------------------------------------
+// ME evaluations: v_j = M_j^T chi_r (CSC), y[w][j][rho] = sum_c Z_w[rho][c] v_j[c]
+// (crates/neo-reductions/src/common.rs:582-650; oracle.rs:1694-1768)
+// ---------------------------------------------------------------------------
+__global__ void matT_chi_kernel(const uint64_t* __restrict__ csc_ptr, const uint32_t* __restrict__ csc_row,
+                                const uint64_t* __restrict__ csc_val, int is_identity, uint32_t n, uint32_t m,
+                                uint64_t n_sz, const K* __restrict__ chi, K* __restrict__ v) {
+    uint64_t c = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+    if (c >= m) return;
+    uint64_t n_eff = n < n_sz ? n : n_sz;
+    if (is_identity) {
+        v[c] = c < n_eff ? chi[c] : gl::kzero();
+        return;
+    }
+    K acc = gl::kzero();
+    for (uint64_t k = csc_ptr[c]; k < csc_ptr[c + 1]; k++) {
+        uint32_t r = csc_row[k];
+        if (r < n_eff) acc = gl::kadd(acc, gl::kscale(chi[r], csc_val[k]));
+    }
+    v[c] = acc;
+}
+
+// one block per (w, rho); threads stride over columns; t accumulators.
+template <int TMAX>
+__global__ void __launch_bounds__(256) zv_dot_kernel(const int8_t* __restrict__ Z, uint64_t m, uint32_t t,
+                                                     const K* __restrict__ v, K* __restrict__ y) {
+    const uint32_t row = blockIdx.x;  // w*54 + rho
+    const int8_t* zr = Z + (uint64_t)row * m;
+    K acc[TMAX];
+#pragma unroll
+    for (int j = 0; j < TMAX; j++) acc[j] = gl::kzero();
+    for (uint64_t c = threadIdx.x; c < m; c += blockDim.x) {
+        int z = zr[c];
+        if (z == 0) continue;
+#pragma unroll
+        for (int j = 0; j < TMAX; j++) {
+            if (j < (int)t) {
+                K x = v[(uint64_t)j * m + c];
+                acc[j] = z == 1 ? gl::kadd(acc[j], x) : (z == -1 ? gl::ksub(acc[j], x) : gl::kadd(acc[j], gl::kscale_small(x, z)));
+            }
+        }
+    }
+    __shared__ K red[TMAX][8];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int j = 0; j < TMAX; j++) {
+        K a = acc[j];
+        for (int o = 16; o > 0; o >>= 1) {
+            K b;
+            b.re = __shfl_xor_sync(0xffffffffu, a.re, o);
+            b.im = __shfl_xor_sync(0xffffffffu, a.im, o);
+            a = gl::kadd(a, b);
+        }
+        if (lane == 0) red[j][warp] = a;
+    }
+    __syncthreads();
+    if (threadIdx.x < t) {
+        K a = gl::kzero();
+        for (int wv = 0; wv < (int)(blockDim.x >> 5); wv++) a = gl::kadd(a, red[threadIdx.x][wv]);
+        // y layout [w][t][54]
+        uint32_t w = row / NEO_D, rho = row % NEO_D;
+        y[((uint64_t)w * t + threadIdx.x) * NEO_D + rho] = a;
+    }
+}
+
+__global__ void y_scalars_kernel(const K* __restrict__ y, uint32_t count, uint32_t b, K* __restrict__ ysc) {
+    uint32_t q = blockIdx.x * blockDim.x + threadIdx.x;  // (w, j)
+    if (q >= count) return;
+    K acc = gl::kzero();
+    uint64_t pw = 1;
+    for (int rho = 0; rho < NEO_D; rho++) {
+        acc = gl::kadd(acc, gl::kscale(y[(uint64_t)q * NEO_D + rho], pw));
+        pw = gl::mul(pw, b);
+    }
+    ysc[q] = acc;
+}
+
+int launch_me_y(neo_gpu_ctx* ctx, const DevCcs& ccs, const int8_t* d_Z, uint32_t n_w, uint64_t m, const K* d_chi,
+                uint32_t ell_n, uint32_t b, K* d_vj, K* d_y, K* d_ysc) {
+    uint64_t n_sz = 1ULL << ell_n;
+    for (uint32_t j = 0; j < ccs.t; j++) {
+        matT_chi_kernel<<<ceil_div(m, 256), 256, 0, ctx->stream>>>(
+            ccs.csc_ptr.p + (size_t)j * (m + 1), ccs.csc_row.p + ccs.nnz_off[j], ccs.csc_val.p + ccs.nnz_off[j],
+            ccs.is_identity[j], ccs.n, (uint32_t)m, n_sz, d_chi, d_vj + (size_t)j * m);
+        NEO_LAUNCHED(ctx);
+    }
+    if (ccs.t <= 4)
+        zv_dot_kernel<4><<<n_w * NEO_D, 256, 0, ctx->stream>>>(d_Z, m, ccs.t, d_vj, d_y);
+    else
+        zv_dot_kernel<16><<<n_w * NEO_D, 256, 0, ctx->stream>>>(d_Z, m, ccs.t, d_vj, d_y);
+    NEO_LAUNCHED(ctx);
+    if (d_ysc) {
+        y_scalars_kernel<<<ceil_div(n_w * ccs.t, 64), 64, 0, ctx->stream>>>(d_y, n_w * ccs.t, b, d_ysc);
+        NEO_LAUNCHED(ctx);
+    }
+    return NEO_OK;
+}
+
+extern "C" int neo_gpu_me_y(neo_gpu_ctx* ctx, const neo_ccs_desc* desc, const int8_t* Z, uint32_t n_w, uint32_t ell_n,
+                            const uint64_t* r, uint32_t b, uint64_t* y, uint64_t* y_scalars) {
+    if (!ctx) return NEO_ERR_ARG;
+    if (!desc || !Z || !r || !y || !y_scalars || n_w == 0 || ell_n == 0 || ell_n > 30)
+        return ctx->fail(NEO_ERR_ARG, "me_y: bad args");
+    cudaSetDevice(ctx->device);
+    DevCcs ccs;
+    int rc = dev_ccs_upload(ctx, desc, ccs);
+    if (rc) return rc;
+    uint64_t m = desc->m;
+    DevBuf<int8_t> dZ;
+    DevBuf<K> dr, dchi, dvj, dy, dysc;
+    NEO_CK(ctx, dZ.alloc((size_t)n_w * NEO_D * m));
+    NEO_CK(ctx, dr.alloc(ell_n));
+    NEO_CK(ctx, dchi.alloc(1ULL << ell_n));
+    NEO_CK(ctx, dvj.alloc((size_t)ccs.t * m));
+    NEO_CK(ctx, dy.alloc((size_t)n_w * ccs.t * NEO_D));
+    NEO_CK(ctx, dysc.alloc((size_t)n_w * ccs.t));
+    NEO_CK(ctx, cudaMemcpyAsync(dZ.p, Z, dZ.bytes(), cudaMemcpyHostToDevice, ctx->stream));
+    NEO_CK(ctx, cudaMemcpyAsync(dr.p, r, ell_n * 16, cudaMemcpyHostToDevice, ctx->stream));
+    if ((rc = launch_chi_table(ctx, dr.p, ell_n, dchi.p))) return rc;
+    if ((rc = launch_me_y(ctx, ccs, dZ.p, n_w, m, dchi.p, ell_n, b, dvj.p, dy.p, dysc.p))) return rc;
+    NEO_CK(ctx, cudaMemcpyAsync(y, dy.p, dy.bytes(), cudaMemcpyDeviceToHost, ctx->stream));
+    NEO_CK(ctx, cudaMemcpyAsync(y_scalars, dysc.p, dysc.bytes(), cudaMemcpyDeviceToHost, ctx->stream));
+    NEO_CK(ctx, cudaStreamSynchronize(ctx->stream));
+    return NEO_OK;
+}

@@ -1,0 +1,113 @@
+// gl.cuh -- Goldilocks F_q and K = F_q[u]/(u^2 - 7) arithmetic for sm_100a.
+//
+// q = 2^64 - 2^32 + 1 (crates/neo-math/src/field.rs:10-16).  Elements are
+// canonical u64 < q.  Products use mul.lo/mul.hi (64x64 -> 128) and the
+// reduction 2^64 = 2^32 - 1, 2^96 = -1 (mod q).  K elements are (re, im) with
+// u^2 = 7 (crates/neo-math/src/s_action.rs:65).
+#pragma once
+#include <cstdint>
+
+#define GL_Q 0xFFFFFFFF00000001ULL
+#define GL_EPS 0xFFFFFFFFULL
+
+#ifdef __CUDACC__
+#define GL_HD __host__ __device__ __forceinline__
+#else
+#define GL_HD inline
+#endif
+
+namespace gl {
+
+GL_HD uint64_t canon(uint64_t a) { return a >= GL_Q ? a - GL_Q : a; }
+
+GL_HD uint64_t add(uint64_t a, uint64_t b) {
+    uint64_t s = a + b;
+    s += (s < a) ? GL_EPS : 0ULL;
+    return canon(s);
+}
+
+GL_HD uint64_t sub(uint64_t a, uint64_t b) {
+    uint64_t d = a - b;
+    return (a < b) ? d + GL_Q : d;   // a - b + q, exact mod 2^64
+}
+
+GL_HD uint64_t neg(uint64_t a) { return a ? GL_Q - a : 0ULL; }
+
+GL_HD uint64_t reduce128(uint64_t lo, uint64_t hi) {
+    uint64_t hi_hi = hi >> 32;
+    uint64_t hi_lo = hi & GL_EPS;
+    uint64_t t0 = lo - hi_hi;
+    if (lo < hi_hi) t0 -= GL_EPS;
+    uint64_t t1 = (hi_lo << 32) - hi_lo;  // hi_lo * (2^32 - 1)
+    uint64_t s = t0 + t1;
+    if (s < t0) s += GL_EPS;
+    return canon(s);
+}
+
+GL_HD uint64_t mulhi(uint64_t a, uint64_t b) {
+#ifdef __CUDA_ARCH__
+    return __umul64hi(a, b);
+#else
+    return (uint64_t)(((unsigned __int128)a * b) >> 64);
+#endif
+}
+
+GL_HD uint64_t mul(uint64_t a, uint64_t b) { return reduce128(a * b, mulhi(a, b)); }
+
+GL_HD uint64_t from_i64(int64_t v) { return v >= 0 ? (uint64_t)v : GL_Q - (uint64_t)(-v); }
+
+// multiply by a small non-negative integer s < 2^31
+GL_HD uint64_t mul_small(uint64_t a, uint32_t s) { return reduce128(a * (uint64_t)s, mulhi(a, (uint64_t)s)); }
+
+GL_HD uint64_t pow(uint64_t a, uint64_t e) {
+    uint64_t r = 1;
+    while (e) {
+        if (e & 1) r = mul(r, a);
+        a = mul(a, a);
+        e >>= 1;
+    }
+    return r;
+}
+GL_HD uint64_t inv(uint64_t a) { return pow(a, GL_Q - 2); }
+
+struct K {
+    uint64_t re, im;
+};
+
+GL_HD K kmk(uint64_t re, uint64_t im) { K r; r.re = re; r.im = im; return r; }
+GL_HD K kzero() { return kmk(0, 0); }
+GL_HD K kone() { return kmk(1, 0); }
+GL_HD K kfq(uint64_t a) { return kmk(a, 0); }
+GL_HD K kadd(K a, K b) { return kmk(add(a.re, b.re), add(a.im, b.im)); }
+GL_HD K ksub(K a, K b) { return kmk(sub(a.re, b.re), sub(a.im, b.im)); }
+GL_HD K kneg(K a) { return kmk(neg(a.re), neg(a.im)); }
+GL_HD K kdbl(K a) { return kadd(a, a); }
+GL_HD bool kiszero(K a) { return (a.re | a.im) == 0; }
+
+// 7x mod q for x < q
+GL_HD uint64_t mul7(uint64_t x) { return mul_small(x, 7); }
+
+GL_HD K kmul(K a, K b) {
+    uint64_t rr = add(mul(a.re, b.re), mul7(mul(a.im, b.im)));
+    uint64_t ii = add(mul(a.re, b.im), mul(a.im, b.re));
+    return kmk(rr, ii);
+}
+GL_HD K ksqr(K a) {
+    uint64_t x = mul(a.re, a.im);
+    return kmk(add(mul(a.re, a.re), mul7(mul(a.im, a.im))), add(x, x));
+}
+GL_HD K kscale(K a, uint64_t s) { return kmk(mul(a.re, s), mul(a.im, s)); }
+// multiply by a small signed integer |s| < 2^31
+GL_HD K kscale_small(K a, int32_t s) {
+    if (s >= 0) return kmk(mul_small(a.re, (uint32_t)s), mul_small(a.im, (uint32_t)s));
+    return kneg(kmk(mul_small(a.re, (uint32_t)(-s)), mul_small(a.im, (uint32_t)(-s))));
+}
+GL_HD K kinv(K a) {
+    uint64_t n = sub(mul(a.re, a.re), mul7(mul(a.im, a.im)));
+    uint64_t ni = inv(n);
+    return kmk(mul(a.re, ni), mul(neg(a.im), ni));
+}
+// a + (b - a) * r
+GL_HD K klerp(K a, K b, K r) { return kadd(a, kmul(ksub(b, a), r)); }
+
+}  // namespace gl

@@ -1,0 +1,101 @@
+// internal.cuh -- context, status handling and device buffers shared by the
+// CUDA translation units of libneo_gpu.so.
+#pragma once
+#include <cuda_runtime.h>
+#include <cstdint>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+#include "../../include/neo_gpu.h"
+#include "gl.cuh"
+
+#define NEO_D 54
+
+struct neo_gpu_ctx {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    std::string err;
+    uint64_t launches = 0;
+    // Ajtai public parameters
+    uint32_t kappa = 0;
+    uint64_t pp_m = 0;
+    uint64_t* d_pp = nullptr;       // [kappa][m][54] canonical u64
+    uint8_t* d_pp_limbs = nullptr;  // [kappa*8][m*54] byte limbs (tensor-core layout)
+    int fail(int code, const char* what, cudaError_t e = cudaSuccess) {
+        char buf[512];
+        if (e != cudaSuccess)
+            snprintf(buf, sizeof buf, "%s: %s", what, cudaGetErrorString(e));
+        else
+            snprintf(buf, sizeof buf, "%s", what);
+        err = buf;
+        return code;
+    }
+};
+
+#define NEO_CK(ctx, call)                                                         \
+    do {                                                                          \
+        cudaError_t _e = (call);                                                  \
+        if (_e != cudaSuccess) {                                                  \
+            return (ctx)->fail(_e == cudaErrorMemoryAllocation ? NEO_ERR_OOM      \
+                                                               : NEO_ERR_CUDA,    \
+                               #call, _e);                                        \
+        }                                                                         \
+    } while (0)
+
+#define NEO_LAUNCHED(ctx)                                                         \
+    do {                                                                          \
+        (ctx)->launches++;                                                        \
+        cudaError_t _e = cudaGetLastError();                                      \
+        if (_e != cudaSuccess) return (ctx)->fail(NEO_ERR_CUDA, "kernel launch", _e); \
+    } while (0)
+
+// Owning device buffer (freed on scope exit).
+template <typename T>
+struct DevBuf {
+    T* p = nullptr;
+    size_t n = 0;
+    DevBuf() = default;
+    DevBuf(const DevBuf&) = delete;
+    DevBuf& operator=(const DevBuf&) = delete;
+    ~DevBuf() { release(); }
+    cudaError_t alloc(size_t count) {
+        release();
+        n = count;
+        if (count == 0) return cudaSuccess;
+        return cudaMalloc(&p, count * sizeof(T));
+    }
+    void release() {
+        if (p) cudaFree(p);
+        p = nullptr;
+        n = 0;
+    }
+    size_t bytes() const { return n * sizeof(T); }
+};
+
+// Device-side CCS copy in both CSR (row SpMV) and CSC (transposed SpMV) form.
+struct DevCcs {
+    uint32_t n = 0, m = 0, t = 0;
+    std::vector<uint8_t> is_identity;
+    std::vector<uint64_t> f_coeff;
+    std::vector<uint32_t> f_exps;
+    uint32_t n_terms = 0;
+    // per matrix offsets into the packed arrays
+    std::vector<uint64_t> nnz_off;
+    DevBuf<uint64_t> csr_ptr;   // [t][n+1] (relative to nnz_off[j])
+    DevBuf<uint32_t> csr_col;   // [nnz]
+    DevBuf<uint64_t> csr_val;   // [nnz]
+    DevBuf<uint64_t> csc_ptr;   // [t][m+1]
+    DevBuf<uint32_t> csc_row;   // [nnz]
+    DevBuf<uint64_t> csc_val;   // [nnz]
+};
+int dev_ccs_upload(neo_gpu_ctx* ctx, const neo_ccs_desc* desc, DevCcs& out);
+
+// Kernels callable from several translation units.
+int launch_chi_table(neo_gpu_ctx* ctx, const gl::K* d_bits, uint32_t nbits, gl::K* d_out);
+int launch_me_y(neo_gpu_ctx* ctx, const DevCcs& ccs, const int8_t* d_Z, uint32_t n_w, uint64_t m,
+                const gl::K* d_chi, uint32_t ell_n, uint32_t b, gl::K* d_vj_scratch, gl::K* d_y,
+                gl::K* d_ysc);
+int launch_commit(neo_gpu_ctx* ctx, const int8_t* d_digits, uint32_t n_vec, uint64_t m, uint64_t* d_out);
+
+inline unsigned ceil_div(uint64_t a, uint64_t b) { return (unsigned)((a + b - 1) / b); }

@@ -1,0 +1,1032 @@
+/*
+ * neo_oracle.c -- CPU restatement of the Neo fold-step hot path.
+ *
+ * TEST INFRASTRUCTURE ONLY (parity checker and timed CPU baseline); the
+ * product never links this file.  See neo_oracle.h for the parity status.
+ * Citations are path:line within the reference project.
+ */
+#include "neo_oracle.h"
+#include <stdlib.h>
+#include <string.h>
+#include <stdio.h>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+typedef unsigned __int128 u128;
+#define D OR_D
+#define Q OR_Q
+#define EPS 0xFFFFFFFFULL /* 2^64 mod q = 2^32 - 1 */
+
+/* ------------------------------------------------------------------------ */
+/* Fq: Goldilocks.  Reduction of a 128-bit product uses 2^64 = 2^32-1 and    */
+/* 2^96 = -1 (mod q); a standard published identity for this prime.         */
+/* ------------------------------------------------------------------------ */
+static inline uint64_t fq_canon(uint64_t a) { return a >= Q ? a - Q : a; }
+static inline uint64_t fq_add(uint64_t a, uint64_t b) {
+    uint64_t s = a + b;
+    uint64_t c = (s < a);              /* carry => s + 2^64 = s + EPS (mod q) */
+    s += c * EPS;
+    /* s < 2^64 here because a,b < q */
+    return fq_canon(s);
+}
+static inline uint64_t fq_sub(uint64_t a, uint64_t b) {
+    return a >= b ? a - b : a + (Q - b);
+}
+static inline uint64_t fq_neg(uint64_t a) { return a == 0 ? 0 : Q - a; }
+static inline uint64_t fq_reduce128(u128 x) {
+    uint64_t lo = (uint64_t)x, hi = (uint64_t)(x >> 64);
+    uint64_t hi_hi = hi >> 32, hi_lo = hi & EPS;
+    uint64_t t0 = lo - hi_hi;
+    if (lo < hi_hi) t0 -= EPS;         /* borrow: -2^64 = -EPS */
+    uint64_t t1 = hi_lo * EPS;         /* < 2^64 */
+    uint64_t s = t0 + t1;
+    if (s < t0) s += EPS;              /* carry */
+    return fq_canon(s);
+}
+static inline uint64_t fq_mul(uint64_t a, uint64_t b) { return fq_reduce128((u128)a * b); }
+static inline uint64_t fq_from_i64(int64_t v) { return v >= 0 ? (uint64_t)v : Q - (uint64_t)(-v); }
+static uint64_t fq_pow(uint64_t a, uint64_t e) {
+    uint64_t r = 1;
+    while (e) { if (e & 1) r = fq_mul(r, a); a = fq_mul(a, a); e >>= 1; }
+    return r;
+}
+static inline uint64_t fq_inv(uint64_t a) { return fq_pow(a, Q - 2); }
+
+/* ------------------------------------------------------------------------ */
+/* K = Fq[u]/(u^2 - 7)   (neo-math/src/field.rs:13; s_action.rs:65)          */
+/* ------------------------------------------------------------------------ */
+typedef struct { uint64_t re, im; } kq;
+static const kq K0 = {0, 0};
+static const kq K1 = {1, 0};
+static inline kq kk(uint64_t re, uint64_t im) { kq r = {re, im}; return r; }
+static inline kq kload(const uint64_t* p) { return kk(p[0], p[1]); }
+static inline void kstore(uint64_t* p, kq a) { p[0] = a.re; p[1] = a.im; }
+static inline kq kadd(kq a, kq b) { return kk(fq_add(a.re, b.re), fq_add(a.im, b.im)); }
+static inline kq ksub(kq a, kq b) { return kk(fq_sub(a.re, b.re), fq_sub(a.im, b.im)); }
+static inline kq kneg(kq a) { return kk(fq_neg(a.re), fq_neg(a.im)); }
+static inline kq kmul(kq a, kq b) {
+    uint64_t rr = fq_add(fq_mul(a.re, b.re), fq_mul(7, fq_mul(a.im, b.im)));
+    uint64_t ii = fq_add(fq_mul(a.re, b.im), fq_mul(a.im, b.re));
+    return kk(rr, ii);
+}
+static inline kq kscale(kq a, uint64_t s) { return kk(fq_mul(a.re, s), fq_mul(a.im, s)); }
+static inline int keq(kq a, kq b) { return a.re == b.re && a.im == b.im; }
+static inline int kiszero(kq a) { return a.re == 0 && a.im == 0; }
+static inline kq kfq(uint64_t a) { return kk(a, 0); }
+static kq kinv(kq a) {
+    /* (a0 + a1 u)^{-1} = (a0 - a1 u) / (a0^2 - 7 a1^2) */
+    uint64_t n = fq_sub(fq_mul(a.re, a.re), fq_mul(7, fq_mul(a.im, a.im)));
+    uint64_t ni = fq_inv(n);
+    return kk(fq_mul(a.re, ni), fq_mul(fq_neg(a.im), ni));
+}
+
+void or_fq_mul_batch(const uint64_t* a, const uint64_t* b, size_t n, uint64_t* out) {
+    for (size_t i = 0; i < n; i++) out[i] = fq_mul(a[i], b[i]);
+}
+void or_k_mul_batch(const uint64_t* a, const uint64_t* b, size_t n, uint64_t* out) {
+    for (size_t i = 0; i < n; i++) kstore(out + 2 * i, kmul(kload(a + 2 * i), kload(b + 2 * i)));
+}
+void or_k_inv_batch(const uint64_t* a, size_t n, uint64_t* out) {
+    for (size_t i = 0; i < n; i++) kstore(out + 2 * i, kinv(kload(a + 2 * i)));
+}
+
+/* ------------------------------------------------------------------------ */
+/* Rq schoolbook multiply mod Phi_81 = X^54 + X^27 + 1 (ring.rs:54-67,187-204)*/
+/* ------------------------------------------------------------------------ */
+static void reduce_mod_phi81(uint64_t* c /* [2D-1] */) {
+    for (int i = 2 * D - 2; i >= D; i--) {
+        uint64_t t = c[i];
+        c[i] = 0;
+        c[i - D] = fq_sub(c[i - D], t);
+        int i27 = i - 27;
+        if (i27 < D) {
+            c[i27] = fq_sub(c[i27], t);
+        } else {
+            c[i27 - D] = fq_add(c[i27 - D], t);
+            if (i27 - 27 < D) c[i27 - 27] = fq_add(c[i27 - 27], t);
+        }
+    }
+}
+void or_rq_mul(const uint64_t* a, const uint64_t* b, uint64_t* out) {
+    uint64_t tmp[2 * D - 1];
+    memset(tmp, 0, sizeof tmp);
+    for (int i = 0; i < D; i++)
+        for (int j = 0; j < D; j++) tmp[i + j] = fq_add(tmp[i + j], fq_mul(a[i], b[j]));
+    reduce_mod_phi81(tmp);
+    memcpy(out, tmp, D * sizeof(uint64_t));
+}
+
+/* rot_step for Phi_81 (commit.rs:46-54): column t -> t+1 */
+static inline void rot_step(const uint64_t* cur, uint64_t* nxt) {
+    uint64_t last = cur[D - 1];
+    nxt[0] = fq_neg(last);
+    for (int k = 1; k < D; k++) nxt[k] = cur[k - 1];
+    nxt[27] = fq_sub(nxt[27], last);
+}
+
+/* commit_precomp_ct_row_major (commit.rs:679-744): c_i = sum_j rot(a_ij) Z[:,j].
+   Digit masks in {-1,0,1} take the add/sub fast path of acc_mul_add_inplace
+   (commit.rs:73-131); any other digit value multiplies. */
+void or_commit_digits(const uint64_t* pp, int kappa, int64_t m, const int8_t* Z, uint64_t* out, int threads) {
+#ifdef _OPENMP
+    if (threads <= 0) threads = omp_get_max_threads();
+#else
+    (void)threads;
+#endif
+    for (int i = 0; i < kappa; i++) {
+        uint64_t acc[D];
+        memset(acc, 0, sizeof acc);
+#ifdef _OPENMP
+#pragma omp parallel num_threads(threads)
+#endif
+        {
+            uint64_t lacc[D];
+            uint64_t cols[D][D];
+            memset(lacc, 0, sizeof lacc);
+#ifdef _OPENMP
+#pragma omp for schedule(static)
+#endif
+            for (int64_t j = 0; j < m; j++) {
+                const uint64_t* a = pp + ((size_t)i * m + j) * D;
+                memcpy(cols[0], a, sizeof(uint64_t) * D);
+                for (int t = 1; t < D; t++) rot_step(cols[t - 1], cols[t]);
+                for (int t = 0; t < D; t++) {
+                    int8_t z = Z[(size_t)t * m + j];
+                    if (z == 0) continue;
+                    if (z == 1) {
+                        for (int r = 0; r < D; r++) lacc[r] = fq_add(lacc[r], cols[t][r]);
+                    } else if (z == -1) {
+                        for (int r = 0; r < D; r++) lacc[r] = fq_sub(lacc[r], cols[t][r]);
+                    } else {
+                        uint64_t s = fq_from_i64(z);
+                        for (int r = 0; r < D; r++) lacc[r] = fq_add(lacc[r], fq_mul(cols[t][r], s));
+                    }
+                }
+            }
+#ifdef _OPENMP
+#pragma omp critical
+#endif
+            for (int r = 0; r < D; r++) acc[r] = fq_add(acc[r], lacc[r]);
+        }
+        memcpy(out + (size_t)i * D, acc, sizeof acc);
+    }
+}
+
+/* commit_masked_ct semantics over a general Fq matrix (commit.rs:512-553) */
+void or_commit_fq(const uint64_t* pp, int kappa, int64_t m, const uint64_t* Z, uint64_t* out) {
+    for (int i = 0; i < kappa; i++) {
+        uint64_t acc[D], col[D], nxt[D];
+        memset(acc, 0, sizeof acc);
+        for (int64_t j = 0; j < m; j++) {
+            memcpy(col, pp + ((size_t)i * m + j) * D, sizeof col);
+            for (int t = 0; t < D; t++) {
+                uint64_t mask = Z[(size_t)t * m + j];
+                for (int r = 0; r < D; r++) acc[r] = fq_add(acc[r], fq_mul(col[r], mask));
+                rot_step(col, nxt);
+                memcpy(col, nxt, sizeof col);
+            }
+        }
+        memcpy(out + (size_t)i * D, acc, sizeof acc);
+    }
+}
+
+/* to_balanced_i64 (neo-ajtai/src/util.rs:19-29) */
+static inline int64_t to_balanced_i64(uint64_t u) {
+    const uint64_t half = (Q - 1) / 2;
+    return u <= half ? (int64_t)u : -(int64_t)(Q - u);
+}
+
+/* decomp_b_row_major, b=2 Balanced (decomp.rs:118-158) */
+void or_decomp_b2(const uint64_t* z, int64_t m, int8_t* Z) {
+    for (int64_t c = 0; c < m; c++) {
+        int64_t a = to_balanced_i64(z[c]);
+        for (int row = 0; row < D; row++) {
+            int64_t digit = (a & 1) == 0 ? 0 : (a >= 0 ? 1 : -1);
+            Z[(size_t)row * m + c] = (int8_t)digit;
+            a = (a - digit) >> 1;
+        }
+    }
+}
+
+/* recomposed_z_from_Z (paper_exact.rs:52-78), b=2 */
+void or_recompose_b2(const int8_t* Z, int64_t m, uint64_t* z) {
+    uint64_t pw[D];
+    pw[0] = 1;
+    for (int i = 1; i < D; i++) pw[i] = fq_mul(pw[i - 1], 2);
+    for (int64_t c = 0; c < m; c++) {
+        uint64_t acc = 0;
+        for (int rho = 0; rho < D; rho++)
+            acc = fq_add(acc, fq_mul(fq_from_i64(Z[(size_t)rho * m + c]), pw[rho]));
+        z[c] = acc;
+    }
+}
+
+/* ------------------------------------------------------------------------ */
+/* RLC / DEC                                                                 */
+/* ------------------------------------------------------------------------ */
+/* rot_from_coeffs (common.rs:398-430): column j = cf(a X^j) */
+void or_rot_matrix(const int8_t* a, uint64_t* out) {
+    uint64_t col[D], nxt[D];
+    for (int r = 0; r < D; r++) col[r] = fq_from_i64(a[r]);
+    for (int j = 0; j < D; j++) {
+        for (int r = 0; r < D; r++) out[r * D + j] = col[r];
+        rot_step(col, nxt);
+        memcpy(col, nxt, sizeof col);
+    }
+}
+
+/* Z_mix = sum_i rho_i Z_i (rlc_reduction_optimized, optimized_engine/common.rs:1221-1379;
+   left_mul_acc common.rs:656-672).  All values are small integers, so the
+   Fq computation equals integer arithmetic; accumulate in int64. */
+void or_rlc_mix(const int8_t* rho_coeffs, const int8_t* Zs, int count, int64_t m, int32_t* Zmix, int threads) {
+    /* integer rot matrices */
+    int32_t* rot = (int32_t*)malloc(sizeof(int32_t) * count * D * D);
+    for (int i = 0; i < count; i++) {
+        int32_t col[D], nxt[D];
+        for (int r = 0; r < D; r++) col[r] = rho_coeffs[i * D + r];
+        for (int j = 0; j < D; j++) {
+            for (int r = 0; r < D; r++) rot[(size_t)i * D * D + r * D + j] = col[r];
+            int32_t last = col[D - 1];
+            nxt[0] = -last;
+            for (int k = 1; k < D; k++) nxt[k] = col[k - 1];
+            nxt[27] -= last;
+            memcpy(col, nxt, sizeof col);
+        }
+    }
+    if (count == 1) {
+        /* Pi_RLC with one input is the identity (common.rs:560-564) */
+        for (int64_t x = 0; x < (int64_t)D * m; x++) Zmix[x] = Zs[x];
+        free(rot);
+        return;
+    }
+#ifdef _OPENMP
+    if (threads <= 0) threads = omp_get_max_threads();
+#pragma omp parallel for num_threads(threads) schedule(static)
+#else
+    (void)threads;
+#endif
+    for (int64_t c = 0; c < m; c++) {
+        int64_t acc[D];
+        memset(acc, 0, sizeof acc);
+        for (int i = 0; i < count; i++) {
+            const int8_t* Zi = Zs + (size_t)i * D * m;
+            const int32_t* R = rot + (size_t)i * D * D;
+            for (int k = 0; k < D; k++) {
+                int8_t z = Zi[(size_t)k * m + c];
+                if (!z) continue;
+                for (int r = 0; r < D; r++) acc[r] += (int64_t)R[r * D + k] * z;
+            }
+        }
+        for (int r = 0; r < D; r++) Zmix[(size_t)r * m + c] = (int32_t)acc[r];
+    }
+    free(rot);
+}
+
+/* balanced_divrem_i64 (common.rs:44-58) */
+static inline void balanced_divrem(int64_t v, int64_t b, int64_t* r_out, int64_t* q_out) {
+    int64_t r = v % b;
+    int64_t q = (v - r) / b;
+    int64_t half = b / 2;
+    if (r > half) { r -= b; q += 1; }
+    else if (r < -half) { r += b; q -= 1; }
+    *r_out = r; *q_out = q;
+}
+
+/* split_b_matrix_k_with_nonzero_flags (common.rs:75-268) */
+int or_split_b(const int32_t* Zmix, int64_t len, int k, int b, int8_t* planes, uint8_t* nonzero) {
+    int64_t B = 1;
+    for (int i = 0; i < k; i++) B *= b;
+    memset(planes, 0, (size_t)k * len);
+    memset(nonzero, 0, (size_t)k);
+    for (int64_t idx = 0; idx < len; idx++) {
+        int64_t v = Zmix[idx];
+        if (v >= B || v <= -B) return -1;
+        for (int i = 0; i < k; i++) {
+            if (v == 0) break;
+            int64_t r, q;
+            balanced_divrem(v, b, &r, &q);
+            if (r != 0) { planes[(size_t)i * len + idx] = (int8_t)r; nonzero[i] = 1; }
+            v = q;
+        }
+        if (v != 0) return -1;
+    }
+    return 0;
+}
+
+/* ------------------------------------------------------------------------ */
+/* Sum-check helpers (sumcheck.rs:48-118)                                    */
+/* ------------------------------------------------------------------------ */
+static kq poly_eval(const kq* c, int n, kq x) {
+    if (n == 0) return K0;
+    kq r = c[n - 1];
+    for (int i = n - 2; i >= 0; i--) r = kadd(kmul(r, x), c[i]);
+    return r;
+}
+void or_poly_eval_k(const uint64_t* coeffs, int n, const uint64_t* x, uint64_t* out) {
+    kstore(out, poly_eval((const kq*)coeffs, n, kload(x)));
+}
+static void interpolate(const kq* xs, const kq* ys, int n, kq* coeffs) {
+    for (int i = 0; i < n; i++) coeffs[i] = K0;
+    kq numer[32], next[32];
+    for (int i = 0; i < n; i++) {
+        for (int d = 0; d < n; d++) numer[d] = K0;
+        numer[0] = K1;
+        int cur = 0;
+        for (int j = 0; j < n; j++) {
+            if (i == j) continue;
+            kq xj = xs[j];
+            for (int d = 0; d < n; d++) next[d] = K0;
+            for (int d = 0; d <= cur; d++) {
+                next[d + 1] = kadd(next[d + 1], numer[d]);
+                next[d] = kadd(next[d], kmul(kneg(xj), numer[d]));
+            }
+            memcpy(numer, next, sizeof(kq) * n);
+            cur++;
+        }
+        kq den = K1;
+        for (int j = 0; j < n; j++) if (i != j) den = kmul(den, ksub(xs[i], xs[j]));
+        kq sc = kmul(ys[i], kinv(den));
+        for (int d = 0; d <= cur; d++) coeffs[d] = kadd(coeffs[d], kmul(sc, numer[d]));
+    }
+}
+void or_interpolate(const uint64_t* xs, const uint64_t* ys, int n, uint64_t* coeffs) {
+    interpolate((const kq*)xs, (const kq*)ys, n, (kq*)coeffs);
+}
+
+/* chi_tail_weights (oracle.rs:1525-1540): w[mask] = prod_i (bit_i ? b_i : 1-b_i) */
+static kq* chi_table(const kq* bits, int nbits) {
+    size_t len = (size_t)1 << nbits;
+    kq* w = (kq*)calloc(len, sizeof(kq));
+    w[0] = K1;
+    for (int i = 0; i < nbits; i++) {
+        size_t step = (size_t)1 << i;
+        kq om = ksub(K1, bits[i]);
+        for (size_t mask = 0; mask < step; mask++) {
+            kq v = w[mask];
+            w[mask] = kmul(v, om);
+            w[mask + step] = kmul(v, bits[i]);
+        }
+    }
+    return w;
+}
+void or_chi_table(const uint64_t* bits, int nbits, uint64_t* out) {
+    kq* w = chi_table((const kq*)bits, nbits);
+    memcpy(out, w, sizeof(kq) << nbits);
+    free(w);
+}
+static kq eq_points_bool_mask(size_t mask, const kq* pts, int n) {
+    kq p = K1;
+    for (int i = 0; i < n; i++) p = kmul(p, ((mask >> i) & 1) ? pts[i] : ksub(K1, pts[i]));
+    return p;
+}
+static inline kq eq_lin(kq a, kq b) {
+    return kadd(kmul(ksub(K1, a), ksub(K1, b)), kmul(a, b));
+}
+static kq eq_points(const kq* p, const kq* q, int n) {
+    kq acc = K1;
+    for (int i = 0; i < n; i++) acc = kmul(acc, eq_lin(p[i], q[i]));
+    return acc;
+}
+
+/* ------------------------------------------------------------------------ */
+/* CCS helpers                                                               */
+/* ------------------------------------------------------------------------ */
+/* out[r] += coeff * (M_j x)[r] for r < n (CSC scatter, oracle.rs:206-236) */
+static void ccs_matvec_acc(const or_ccs* s, int j, const kq* x, kq coeff, kq* out) {
+    uint32_t n = s->n, m = s->m;
+    if (s->is_identity[j]) {
+        uint32_t cap = n < m ? n : m;
+        for (uint32_t r = 0; r < cap; r++) out[r] = kadd(out[r], kmul(coeff, x[r]));
+        return;
+    }
+    const uint64_t* cp = s->col_ptr + (size_t)j * (m + 1);
+    const uint32_t* ri = s->row_idx + s->nnz_off[j];
+    const uint64_t* vv = s->vals + s->nnz_off[j];
+    for (uint32_t c = 0; c < m; c++) {
+        if (kiszero(x[c])) continue;
+        kq sx = kmul(coeff, x[c]);
+        for (uint64_t k = cp[c]; k < cp[c + 1]; k++) {
+            uint32_t r = ri[k];
+            if (r < n) out[r] = kadd(out[r], kscale(sx, vv[k]));
+        }
+    }
+}
+/* v[c] = (M_j^T chi)[c] (oracle.rs:1694-1728) */
+static void ccs_matTvec(const or_ccs* s, int j, const kq* chi, size_t chi_len, kq* v) {
+    uint32_t n = s->n, m = s->m;
+    size_t n_eff = n < chi_len ? n : chi_len;
+    for (uint32_t c = 0; c < m; c++) v[c] = K0;
+    if (s->is_identity[j]) {
+        size_t cap = m < n_eff ? m : n_eff;
+        for (size_t c = 0; c < cap; c++) v[c] = chi[c];
+        return;
+    }
+    const uint64_t* cp = s->col_ptr + (size_t)j * (m + 1);
+    const uint32_t* ri = s->row_idx + s->nnz_off[j];
+    const uint64_t* vv = s->vals + s->nnz_off[j];
+    for (uint32_t c = 0; c < m; c++) {
+        kq acc = K0;
+        for (uint64_t k = cp[c]; k < cp[c + 1]; k++) {
+            uint32_t r = ri[k];
+            if (r < n_eff) acc = kadd(acc, kscale(chi[r], vv[k]));
+        }
+        v[c] = acc;
+    }
+}
+/* f.eval_in_ext */
+static kq f_eval(const or_ccs* s, const kq* mv) {
+    kq acc = K0;
+    for (uint32_t tt = 0; tt < s->n_terms; tt++) {
+        kq p = kfq(s->f_coeff[tt]);
+        for (uint32_t j = 0; j < s->t; j++) {
+            uint32_t e = s->f_exps[(size_t)tt * s->t + j];
+            for (uint32_t q = 0; q < e; q++) p = kmul(p, mv[j]);
+        }
+        acc = kadd(acc, p);
+    }
+    return acc;
+}
+static inline kq range_product_b2(kq y) { return kmul(y, ksub(kmul(y, y), K1)); }
+
+/* ------------------------------------------------------------------------ */
+/* Pi_CCS optimized oracle (oracle.rs)                                       */
+/* ------------------------------------------------------------------------ */
+struct or_ccs_oracle {
+    const or_ccs* s;   /* caller keeps alive */
+    int k, b, ell_d, ell_n, d_sc;
+    int64_t m;
+    const int8_t* Z;   /* caller keeps alive: [k][54][m] */
+    kq *alpha, *beta_a, *beta_r, gamma, *r_inputs;
+    int has_inputs;
+    /* row stream */
+    size_t cur_len;
+    kq *eq_beta_r, *eq_rin, *z1, **fvar, *nc, *wg, *eval_tbl, gamma_to_k;
+    int n_fvar, *fvar_j;
+    int deg_max;
+    /* rounds */
+    int round_idx;
+    kq *row_chals, *ajtai_chals;
+    /* ajtai precomp */
+    int have_pre;
+    kq *y_nc;   /* [k][D] */
+    kq *y_eval; /* [k][t][D] */
+    kq f_prime, pre_eq_beta_r, pre_eq_rin;
+};
+
+static kq* kdup(const uint64_t* src, int n) {
+    kq* d = (kq*)malloc(sizeof(kq) * (n > 0 ? n : 1));
+    for (int i = 0; i < n; i++) d[i] = kload(src + 2 * i);
+    return d;
+}
+
+or_ccs_oracle* or_ccs_oracle_new(const or_ccs* s, const int8_t* Z, int k, int b,
+                                 const uint64_t* alpha, const uint64_t* beta_a, const uint64_t* beta_r,
+                                 const uint64_t* gamma, const uint64_t* r_inputs,
+                                 int ell_d, int ell_n, int d_sc) {
+    if (b != 2 || k < 1) return NULL;
+    or_ccs_oracle* o = (or_ccs_oracle*)calloc(1, sizeof(*o));
+    o->s = s; o->k = k; o->b = b; o->ell_d = ell_d; o->ell_n = ell_n; o->d_sc = d_sc;
+    o->m = s->m; o->Z = Z;
+    o->alpha = kdup(alpha, ell_d); o->beta_a = kdup(beta_a, ell_d); o->beta_r = kdup(beta_r, ell_n);
+    o->gamma = kload(gamma);
+    o->has_inputs = r_inputs != NULL;
+    o->r_inputs = r_inputs ? kdup(r_inputs, ell_n) : NULL;
+    o->row_chals = (kq*)calloc(ell_n + 1, sizeof(kq));
+    o->ajtai_chals = (kq*)calloc(ell_d + 1, sizeof(kq));
+    size_t n_pad = (size_t)1 << ell_n;
+    size_t n_eff = s->n;
+    size_t m = s->m;
+    o->cur_len = n_pad;
+    o->eq_beta_r = chi_table(o->beta_r, ell_n);
+    o->eq_rin = o->has_inputs ? chi_table(o->r_inputs, ell_n) : NULL;
+
+    /* compile f: used variables (oracle.rs:136-186) */
+    int t = s->t;
+    o->fvar_j = (int*)calloc(t, sizeof(int));
+    int fmaxdeg = 0;
+    for (int j = 0; j < t; j++) {
+        int used = 0;
+        for (uint32_t tt = 0; tt < s->n_terms; tt++) if (s->f_exps[tt * t + j]) used = 1;
+        if (used) o->fvar_j[o->n_fvar++] = j;
+    }
+    for (uint32_t tt = 0; tt < s->n_terms; tt++) {
+        int dg = 0;
+        for (int j = 0; j < t; j++) dg += s->f_exps[tt * t + j];
+        if (dg > fmaxdeg) fmaxdeg = dg;
+    }
+    o->deg_max = fmaxdeg + 1 > 4 ? fmaxdeg + 1 : 4;
+
+    /* w_gamma_nc[i*D+rho] = chi_{beta_a}[rho] * gamma^(i+1)  (oracle.rs:196-213) */
+    o->wg = (kq*)calloc((size_t)k * D, sizeof(kq));
+    {
+        kq g = o->gamma;
+        for (int i = 0; i < k; i++) {
+            for (int rho = 0; rho < D; rho++)
+                o->wg[i * D + rho] = kmul(eq_points_bool_mask(rho, o->beta_a, ell_d), g);
+            g = kmul(g, o->gamma);
+        }
+    }
+    /* z1 (oracle.rs:215-243) */
+    o->z1 = (kq*)calloc(m, sizeof(kq));
+    {
+        uint64_t pw[D]; pw[0] = 1;
+        for (int r = 1; r < D; r++) pw[r] = fq_mul(pw[r - 1], (uint64_t)b);
+        for (int rho = 0; rho < D; rho++)
+            for (size_t c = 0; c < m; c++)
+                o->z1[c] = kadd(o->z1[c], kfq(fq_mul(fq_from_i64(Z[rho * m + c]), pw[rho])));
+    }
+    /* f-var tables (oracle.rs:245-285) */
+    o->fvar = (kq**)calloc(o->n_fvar > 0 ? o->n_fvar : 1, sizeof(kq*));
+    for (int v = 0; v < o->n_fvar; v++) {
+        o->fvar[v] = (kq*)calloc(n_pad, sizeof(kq));
+        ccs_matvec_acc(s, o->fvar_j[v], o->z1, K1, o->fvar[v]);
+    }
+    /* NC tables: nc[(i*n_pad + row)*D + rho] (oracle.rs:287-308) */
+    o->nc = (kq*)calloc((size_t)k * n_pad * D, sizeof(kq));
+    {
+        size_t cap = n_eff < n_pad ? n_eff : n_pad;
+        if (cap > m) cap = m;
+        for (int i = 0; i < k; i++)
+            for (size_t row = 0; row < cap; row++)
+                for (int rho = 0; rho < D; rho++)
+                    o->nc[((size_t)i * n_pad + row) * D + rho] = kfq(fq_from_i64(Z[((size_t)i * D + rho) * m + row]));
+    }
+    /* gamma^k and Eval table (oracle.rs:310-393) */
+    o->gamma_to_k = K1;
+    for (int i = 0; i < k; i++) o->gamma_to_k = kmul(o->gamma_to_k, o->gamma);
+    if (k >= 2 && o->has_inputs) {
+        kq w_alpha[D];
+        for (int rho = 0; rho < D; rho++) w_alpha[rho] = eq_points_bool_mask(rho, o->alpha, ell_d);
+        o->eval_tbl = (kq*)calloc(n_pad, sizeof(kq));
+        kq* s_alpha = (kq*)calloc(m, sizeof(kq));
+        kq gpi = K1;
+        for (int i = 1; i < k; i++) {
+            gpi = kmul(gpi, o->gamma);
+            for (size_t c = 0; c < m; c++) s_alpha[c] = K0;
+            for (int rho = 0; rho < D; rho++) {
+                for (size_t c = 0; c < m; c++) {
+                    int8_t z = Z[((size_t)i * D + rho) * m + c];
+                    if (z) s_alpha[c] = kadd(s_alpha[c], kscale(w_alpha[rho], fq_from_i64(z)));
+                }
+            }
+            kq gkj = K1;
+            for (int j = 0; j < t; j++) {
+                kq coeff = kmul(gpi, gkj);
+                ccs_matvec_acc(s, j, s_alpha, coeff, o->eval_tbl);
+                gkj = kmul(gkj, o->gamma_to_k);
+            }
+        }
+        free(s_alpha);
+    }
+    return o;
+}
+
+void or_ccs_oracle_free(or_ccs_oracle* o) {
+    if (!o) return;
+    free(o->alpha); free(o->beta_a); free(o->beta_r); free(o->r_inputs);
+    free(o->row_chals); free(o->ajtai_chals);
+    free(o->eq_beta_r); free(o->eq_rin); free(o->z1);
+    for (int v = 0; v < o->n_fvar; v++) free(o->fvar[v]);
+    free(o->fvar); free(o->fvar_j); free(o->nc); free(o->wg); free(o->eval_tbl);
+    free(o->y_nc); free(o->y_eval);
+    free(o);
+}
+int or_ccs_oracle_num_rounds(const or_ccs_oracle* o) { return o->ell_n + o->ell_d; }
+
+/* poly_mul_affine_inplace (oracle.rs:1036-1045) */
+static void poly_mul_affine(kq* poly, int len, kq a, kq b) {
+    kq prev = K0;
+    for (int i = 0; i < len; i++) {
+        kq old = poly[i];
+        poly[i] = kadd(kmul(a, old), kmul(b, prev));
+        prev = old;
+    }
+}
+
+/* evals_row_phase_impl, b=2 generic K path (oracle.rs:1047-1178) */
+static void evals_row_phase(or_ccs_oracle* o, const kq* xs, int nx, kq* ys) {
+    const or_ccs* s = o->s;
+    size_t tail = o->cur_len / 2;
+    size_t L = o->cur_len;
+    int dm = o->deg_max;
+    kq coeffs[16], inner[16], tp[16];
+    kq three = kfq(3);
+    for (int i = 0; i <= dm; i++) coeffs[i] = K0;
+    for (size_t t = 0; t < tail; t++) {
+        kq e0 = o->eq_beta_r[2 * t];
+        kq e1 = ksub(o->eq_beta_r[2 * t + 1], e0);
+        for (int i = 0; i <= dm; i++) inner[i] = K0;
+        for (uint32_t tt = 0; tt < s->n_terms; tt++) {
+            for (int i = 0; i <= dm; i++) tp[i] = K0;
+            tp[0] = kfq(s->f_coeff[tt]);
+            for (int v = 0; v < o->n_fvar; v++) {
+                uint32_t e = s->f_exps[tt * s->t + o->fvar_j[v]];
+                if (!e) continue;
+                kq a = o->fvar[v][2 * t];
+                kq bb = ksub(o->fvar[v][2 * t + 1], a);
+                for (uint32_t q = 0; q < e; q++) poly_mul_affine(tp, dm + 1, a, bb);
+            }
+            for (int i = 0; i <= dm; i++) inner[i] = kadd(inner[i], tp[i]);
+        }
+        for (int w = 0; w < o->k; w++) {
+            const kq* lo = o->nc + ((size_t)w * L + 2 * t) * D;
+            const kq* hi = lo + D;
+            for (int rho = 0; rho < D; rho++) {
+                kq wg = o->wg[w * D + rho];
+                kq a = lo[rho];
+                kq bb = ksub(hi[rho], a);
+                kq a2 = kmul(a, a), a3 = kmul(a2, a), b2 = kmul(bb, bb), b3 = kmul(b2, bb);
+                kq t0 = ksub(a3, a);
+                kq t1 = ksub(kmul(kmul(a2, bb), three), bb);
+                kq t2 = kmul(kmul(a, b2), three);
+                kq t3 = b3;
+                inner[0] = kadd(inner[0], kmul(wg, t0));
+                inner[1] = kadd(inner[1], kmul(wg, t1));
+                inner[2] = kadd(inner[2], kmul(wg, t2));
+                inner[3] = kadd(inner[3], kmul(wg, t3));
+            }
+        }
+        coeffs[0] = kadd(coeffs[0], kmul(e0, inner[0]));
+        for (int d = 1; d <= dm; d++)
+            coeffs[d] = kadd(coeffs[d], kadd(kmul(e0, inner[d]), kmul(e1, inner[d - 1])));
+        if (o->eq_rin && o->eval_tbl) {
+            kq r0 = o->eq_rin[2 * t], r1 = ksub(o->eq_rin[2 * t + 1], r0);
+            kq v0 = o->eval_tbl[2 * t], v1 = ksub(o->eval_tbl[2 * t + 1], v0);
+            kq g = o->gamma_to_k;
+            coeffs[0] = kadd(coeffs[0], kmul(g, kmul(r0, v0)));
+            coeffs[1] = kadd(coeffs[1], kmul(g, kadd(kmul(r0, v1), kmul(r1, v0))));
+            coeffs[2] = kadd(coeffs[2], kmul(g, kmul(r1, v1)));
+        }
+    }
+    for (int i = 0; i < nx; i++) ys[i] = poly_eval(coeffs, dm + 1, xs[i]);
+}
+
+static void fold_tbl(kq* T, size_t len, kq r) {
+    size_t half = len / 2;
+    for (size_t i = 0; i < half; i++) T[i] = kadd(T[2 * i], kmul(ksub(T[2 * i + 1], T[2 * i]), r));
+}
+
+/* RowStreamState::fold_inplace (oracle.rs:470-503) */
+static void row_fold(or_ccs_oracle* o, kq r) {
+    size_t L = o->cur_len, half = L / 2;
+    fold_tbl(o->eq_beta_r, L, r);
+    if (o->eq_rin) fold_tbl(o->eq_rin, L, r);
+    for (int v = 0; v < o->n_fvar; v++) fold_tbl(o->fvar[v], L, r);
+    for (int w = 0; w < o->k; w++) {
+        kq* base = o->nc + (size_t)w * L * D;          /* old layout stride L */
+        kq* dst = o->nc + (size_t)w * half * D;        /* compact to stride half */
+        for (size_t i = 0; i < half; i++)
+            for (int rho = 0; rho < D; rho++) {
+                kq lo = base[(2 * i) * D + rho], hi = base[(2 * i + 1) * D + rho];
+                dst[i * D + rho] = kadd(lo, kmul(ksub(hi, lo), r));
+            }
+    }
+    if (o->eval_tbl) fold_tbl(o->eval_tbl, L, r);
+    o->cur_len = half;
+}
+
+/* precompute_for_r (oracle.rs:1659-1783) */
+static void precompute_for_r(or_ccs_oracle* o) {
+    const or_ccs* s = o->s;
+    int t = s->t, k = o->k;
+    size_t m = s->m;
+    kq* chi_r = chi_table(o->row_chals, o->ell_n);
+    size_t n_sz = (size_t)1 << o->ell_n;
+    o->pre_eq_beta_r = eq_points(o->row_chals, o->beta_r, o->ell_n);
+    o->pre_eq_rin = o->has_inputs ? eq_points(o->row_chals, o->r_inputs, o->ell_n) : K0;
+    kq* vj = (kq*)calloc((size_t)t * m, sizeof(kq));
+    for (int j = 0; j < t; j++) ccs_matTvec(s, j, chi_r, n_sz, vj + (size_t)j * m);
+    kq mv[64];
+    for (int j = 0; j < t; j++) {
+        kq acc = K0;
+        for (size_t c = 0; c < m; c++) acc = kadd(acc, kmul(o->z1[c], vj[(size_t)j * m + c]));
+        mv[j] = acc;
+    }
+    o->f_prime = f_eval(s, mv);
+    o->y_nc = (kq*)calloc((size_t)k * D, sizeof(kq));
+    o->y_eval = (kq*)calloc((size_t)k * t * D, sizeof(kq));
+    for (int i = 0; i < k; i++) {
+        for (int j = 0; j < t; j++) {
+            for (int rho = 0; rho < D; rho++) {
+                const int8_t* zr = o->Z + ((size_t)i * D + rho) * m;
+                kq acc = K0;
+                for (size_t c = 0; c < m; c++) {
+                    if (zr[c] == 1) acc = kadd(acc, vj[(size_t)j * m + c]);
+                    else if (zr[c] == -1) acc = ksub(acc, vj[(size_t)j * m + c]);
+                    else if (zr[c]) acc = kadd(acc, kscale(vj[(size_t)j * m + c], fq_from_i64(zr[c])));
+                }
+                o->y_eval[((size_t)i * t + j) * D + rho] = acc;
+            }
+        }
+        /* NC uses v_1 = chi_r restricted (matrix 0 is the identity) */
+        memcpy(o->y_nc + (size_t)i * D, o->y_eval + ((size_t)i * t + 0) * D, sizeof(kq) * D);
+    }
+    free(vj); free(chi_r);
+    o->have_pre = 1;
+}
+
+/* fold_bit_inplace (oracle.rs:1447-1468) */
+static void fold_bit_inplace(kq* dg, int bit, kq a) {
+    int stride = 1 << bit, step = stride << 1;
+    for (int base = 0; base < D; base += step)
+        for (int off = 0; off < stride; off++) {
+            int i0 = base + off;
+            if (i0 >= D) break;
+            int i1 = i0 + stride;
+            kq lo = dg[i0], hi = i1 < D ? dg[i1] : K0;
+            dg[i0] = kadd(lo, kmul(ksub(hi, lo), a));
+        }
+}
+
+/* evals_ajtai_phase (oracle.rs:1812-1951) */
+static void evals_ajtai_phase(or_ccs_oracle* o, const kq* xs, int nx, kq* ys) {
+    const or_ccs* s = o->s;
+    int j = o->round_idx - o->ell_n;
+    int k = o->k, t = s->t;
+    if (!o->have_pre) precompute_for_r(o);
+    int ntail = o->ell_d - j - 1;
+    kq* wb = chi_table(o->beta_a + j + 1, ntail);
+    kq* wa = chi_table(o->alpha + j + 1, ntail);
+    int tail_len = 1 << ntail;
+    int hs = 1 << (j + 1);
+    kq ebp = K1, eap = K1;
+    for (int i = 0; i < j; i++) {
+        ebp = kmul(ebp, eq_lin(o->ajtai_chals[i], o->beta_a[i]));
+        eap = kmul(eap, eq_lin(o->ajtai_chals[i], o->alpha[i]));
+    }
+    kq* gpi = (kq*)malloc(sizeof(kq) * k);
+    gpi[0] = K1;
+    for (int i = 1; i < k; i++) gpi[i] = kmul(gpi[i - 1], o->gamma);
+    kq gk = o->gamma_to_k;
+    kq gkj[64]; gkj[0] = K1;
+    for (int jj = 1; jj < t; jj++) gkj[jj] = kmul(gkj[jj - 1], gk);
+    kq* ync = (kq*)malloc(sizeof(kq) * k * D);
+    memcpy(ync, o->y_nc, sizeof(kq) * k * D);
+    for (int i = 0; i < k; i++) for (int bb = 0; bb < j; bb++) fold_bit_inplace(ync + i * D, bb, o->ajtai_chals[bb]);
+    kq* yev = (kq*)malloc(sizeof(kq) * k * t * D);
+    memcpy(yev, o->y_eval, sizeof(kq) * k * t * D);
+    for (int q = 0; q < k * t; q++) for (int bb = 0; bb < j; bb++) fold_bit_inplace(yev + q * D, bb, o->ajtai_chals[bb]);
+    kq beta_j = o->beta_a[j], alpha_j = o->alpha[j];
+    for (int xi = 0; xi < nx; xi++) {
+        kq x = xs[xi];
+        kq eq_beta = kmul(o->pre_eq_beta_r, kmul(ebp, eq_lin(x, beta_j)));
+        kq eq_ar = o->has_inputs ? kmul(o->pre_eq_rin, kmul(eap, eq_lin(x, alpha_j))) : K0;
+        kq nc_sum = K0, g = o->gamma;
+        kq tmp[D];
+        for (int i = 0; i < k; i++) {
+            memcpy(tmp, ync + i * D, sizeof tmp);
+            fold_bit_inplace(tmp, j, x);
+            kq acc = K0;
+            for (int tt = 0; tt < tail_len; tt++) {
+                int idx = tt * hs;
+                if (idx < D) acc = kadd(acc, kmul(wb[tt], range_product_b2(tmp[idx])));
+            }
+            nc_sum = kadd(nc_sum, kmul(g, acc));
+            g = kmul(g, o->gamma);
+        }
+        kq out = kmul(eq_beta, kadd(o->f_prime, nc_sum));
+        if (k >= 2 && !kiszero(eq_ar)) {
+            kq inner = K0;
+            for (int jm = 0; jm < t; jm++) {
+                kq sum_j = K0;
+                for (int i = 1; i < k; i++) {
+                    memcpy(tmp, yev + (i * t + jm) * D, sizeof tmp);
+                    fold_bit_inplace(tmp, j, x);
+                    kq ydot = K0;
+                    for (int tt = 0; tt < tail_len; tt++) {
+                        int idx = tt * hs;
+                        if (idx < D) ydot = kadd(ydot, kmul(wa[tt], tmp[idx]));
+                    }
+                    sum_j = kadd(sum_j, kmul(kmul(gpi[i], gkj[jm]), ydot));
+                }
+                inner = kadd(inner, sum_j);
+            }
+            out = kadd(out, kmul(eq_ar, kmul(gk, inner)));
+        }
+        ys[xi] = out;
+    }
+    free(wb); free(wa); free(gpi); free(ync); free(yev);
+}
+
+void or_ccs_oracle_evals(or_ccs_oracle* o, const uint64_t* xs, int nx, uint64_t* ys) {
+    if (o->round_idx < o->ell_n) evals_row_phase(o, (const kq*)xs, nx, (kq*)ys);
+    else evals_ajtai_phase(o, (const kq*)xs, nx, (kq*)ys);
+}
+void or_ccs_oracle_fold(or_ccs_oracle* o, const uint64_t* r) {
+    kq rr = kload(r);
+    if (o->round_idx < o->ell_n) {
+        o->row_chals[o->round_idx] = rr;
+        row_fold(o, rr);
+    } else {
+        o->ajtai_chals[o->round_idx - o->ell_n] = rr;
+    }
+    o->round_idx++;
+}
+/* build_me_outputs_from_ajtai_precomp (oracle.rs:1955-2072): y digits + y_scalars */
+void or_ccs_oracle_me_outputs(or_ccs_oracle* o, uint64_t* y_out, uint64_t* y_scalars) {
+    if (!o->have_pre) precompute_for_r(o);
+    int t = o->s->t;
+    uint64_t pw[D]; pw[0] = 1;
+    for (int r = 1; r < D; r++) pw[r] = fq_mul(pw[r - 1], (uint64_t)o->b);
+    for (int i = 0; i < o->k; i++)
+        for (int j = 0; j < t; j++) {
+            const kq* dg = o->y_eval + ((size_t)i * t + j) * D;
+            kq acc = K0;
+            for (int rho = 0; rho < D; rho++) {
+                kstore(y_out + 2 * (((size_t)i * t + j) * D + rho), dg[rho]);
+                acc = kadd(acc, kscale(dg[rho], pw[rho]));
+            }
+            kstore(y_scalars + 2 * ((size_t)i * t + j), acc);
+        }
+}
+
+/* run_sumcheck_prover with externally fixed challenges (sumcheck.rs:124-209) */
+int or_ccs_sumcheck_fixed(or_ccs_oracle* o, const uint64_t* initial_sum, const uint64_t* chals,
+                          uint64_t* evals_out, uint64_t* final_sum) {
+    int rounds = or_ccs_oracle_num_rounds(o);
+    int np = o->d_sc + 1;
+    kq xs[32], ys[32], co[32];
+    for (int i = 0; i < np; i++) xs[i] = kfq((uint64_t)i);
+    kq running = kload(initial_sum);
+    for (int r = 0; r < rounds; r++) {
+        or_ccs_oracle_evals(o, (const uint64_t*)xs, np, (uint64_t*)ys);
+        if (evals_out) memcpy(evals_out + (size_t)r * np * 2, ys, sizeof(kq) * np);
+        if (!keq(kadd(ys[0], ys[1]), running)) return -1 - r;
+        interpolate(xs, ys, np, co);
+        kq c = kload(chals + 2 * r);
+        running = poly_eval(co, np, c);
+        or_ccs_oracle_fold(o, chals + 2 * r);
+    }
+    kstore(final_sum, running);
+    return 0;
+}
+
+/* ------------------------------------------------------------------------ */
+/* Paper-exact Q (paper_exact.rs:136-340, 414-687)                           */
+/* ------------------------------------------------------------------------ */
+static kq csc_get(const or_ccs* s, int j, uint32_t row, uint32_t col) {
+    if (s->is_identity[j]) return (row == col && row < s->n) ? K1 : K0;
+    const uint64_t* cp = s->col_ptr + (size_t)j * (s->m + 1);
+    const uint32_t* ri = s->row_idx + s->nnz_off[j];
+    const uint64_t* vv = s->vals + s->nnz_off[j];
+    uint64_t acc = 0;
+    for (uint64_t k = cp[col]; k < cp[col + 1]; k++) if (ri[k] == row) acc = fq_add(acc, vv[k]);
+    return kfq(acc);
+}
+
+void or_q_sum_hypercube(const or_ccs* s, const int8_t* Z, int k, int b,
+                        const uint64_t* alpha_, const uint64_t* beta_a_, const uint64_t* beta_r_,
+                        const uint64_t* gamma_, const uint64_t* r_inputs_, int ell_d, int ell_n, uint64_t* out) {
+    (void)b;
+    const kq* alpha = (const kq*)alpha_; const kq* beta_a = (const kq*)beta_a_;
+    const kq* beta_r = (const kq*)beta_r_; kq gamma = kload(gamma_);
+    const kq* rin = (const kq*)r_inputs_;
+    size_t m = s->m;
+    int t = s->t;
+    uint64_t* z1 = (uint64_t*)malloc(8 * m);
+    or_recompose_b2(Z, m, z1);
+    kq gk = K1;
+    for (int i = 0; i < k; i++) gk = kmul(gk, gamma);
+    kq total = K0;
+    for (size_t xr = 0; xr < ((size_t)1 << ell_n); xr++) {
+        /* F(xr) */
+        kq mv[64];
+        for (int j = 0; j < t; j++) {
+            kq acc = K0;
+            if (xr < s->n)
+                for (size_t c = 0; c < m; c++) acc = kadd(acc, kmul(csc_get(s, j, xr, c), kfq(z1[c])));
+            mv[j] = acc;
+        }
+        kq Fv = f_eval(s, mv);
+        kq eqr = eq_points_bool_mask(xr, beta_r, ell_n);
+        kq eqrin = rin ? eq_points_bool_mask(xr, rin, ell_n) : K0;
+        for (size_t xa = 0; xa < ((size_t)1 << ell_d); xa++) {
+            kq eq_beta = kmul(eq_points_bool_mask(xa, beta_a, ell_d), eqr);
+            kq nc = K0, g = gamma;
+            for (int i = 0; i < k; i++) {
+                kq y = K0;
+                if (xa < D && xr < m && xr < s->n) y = kfq(fq_from_i64(Z[((size_t)i * D + xa) * m + xr]));
+                nc = kadd(nc, kmul(g, range_product_b2(y)));
+                g = kmul(g, gamma);
+            }
+            kq acc = kmul(eq_beta, kadd(Fv, nc));
+            if (rin && k >= 2) {
+                kq eq_ar = kmul(eq_points_bool_mask(xa, alpha, ell_d), eqrin);
+                kq inner = K0;
+                kq gkj = K1;
+                for (int j = 0; j < t; j++) {
+                    kq w = gkj;
+                    for (int i = 1; i < k; i++) {
+                        w = kmul(w, gamma); /* gamma^i * gk^j */
+                        kq y = K0;
+                        if (xa < D && xr < s->n)
+                            for (size_t c = 0; c < m; c++) {
+                                int8_t z = Z[((size_t)i * D + xa) * m + c];
+                                if (z) y = kadd(y, kscale(csc_get(s, j, xr, c), fq_from_i64(z)));
+                            }
+                        inner = kadd(inner, kmul(w, kmul(eq_ar, y)));
+                    }
+                    gkj = kmul(gkj, gk);
+                }
+                acc = kadd(acc, kmul(gk, inner));
+            }
+            total = kadd(total, acc);
+        }
+    }
+    free(z1);
+    kstore(out, total);
+}
+
+void or_q_eval_ext(const or_ccs* s, const int8_t* Z, int k, int b,
+                   const uint64_t* alpha_, const uint64_t* beta_a_, const uint64_t* beta_r_,
+                   const uint64_t* gamma_, const uint64_t* r_inputs_, int ell_d, int ell_n,
+                   const uint64_t* alpha_p_, const uint64_t* r_p_, uint64_t* out) {
+    (void)b;
+    const kq* alpha = (const kq*)alpha_; const kq* beta_a = (const kq*)beta_a_;
+    const kq* beta_r = (const kq*)beta_r_; kq gamma = kload(gamma_);
+    const kq* rin = (const kq*)r_inputs_;
+    const kq* ap = (const kq*)alpha_p_; const kq* rp = (const kq*)r_p_;
+    size_t m = s->m;
+    int t = s->t;
+    size_t n_sz = (size_t)1 << ell_n;
+    kq* chi_a = chi_table(ap, ell_d);
+    kq* chi_r = chi_table(rp, ell_n);
+    kq eq_beta = kmul(eq_points(ap, beta_a, ell_d), eq_points(rp, beta_r, ell_n));
+    kq eq_ar = rin ? kmul(eq_points(ap, alpha, ell_d), eq_points(rp, rin, ell_n)) : K0;
+    uint64_t* z1 = (uint64_t*)malloc(8 * m);
+    or_recompose_b2(Z, m, z1);
+    kq* zk = (kq*)malloc(sizeof(kq) * m);
+    for (size_t c = 0; c < m; c++) zk[c] = kfq(z1[c]);
+    kq* vj = (kq*)malloc(sizeof(kq) * m);
+    kq mv[64];
+    for (int j = 0; j < t; j++) {
+        ccs_matTvec(s, j, chi_r, n_sz, vj);
+        kq acc = K0;
+        for (size_t c = 0; c < m; c++) acc = kadd(acc, kmul(vj[c], zk[c]));
+        mv[j] = acc;
+    }
+    kq Fp = f_eval(s, mv);
+    kq gk = K1;
+    for (int i = 0; i < k; i++) gk = kmul(gk, gamma);
+    /* NC with v1 = M_0^T chi_r */
+    ccs_matTvec(s, 0, chi_r, n_sz, vj);
+    kq nc = K0, g = gamma;
+    for (int i = 0; i < k; i++) {
+        kq ye = K0;
+        for (int rho = 0; rho < D && rho < (1 << ell_d); rho++) {
+            kq acc = K0;
+            const int8_t* zr = Z + ((size_t)i * D + rho) * m;
+            for (size_t c = 0; c < m; c++) if (zr[c]) acc = kadd(acc, kscale(vj[c], fq_from_i64(zr[c])));
+            ye = kadd(ye, kmul(acc, chi_a[rho]));
+        }
+        nc = kadd(nc, kmul(g, range_product_b2(ye)));
+        g = kmul(g, gamma);
+    }
+    kq ev = K0;
+    if (k >= 2) {
+        for (int j = 0; j < t; j++) {
+            ccs_matTvec(s, j, chi_r, n_sz, vj);
+            for (int i = 1; i < k; i++) {
+                kq ye = K0;
+                for (int rho = 0; rho < D && rho < (1 << ell_d); rho++) {
+                    kq acc = K0;
+                    const int8_t* zr = Z + ((size_t)i * D + rho) * m;
+                    for (size_t c = 0; c < m; c++) if (zr[c]) acc = kadd(acc, kscale(vj[c], fq_from_i64(zr[c])));
+                    ye = kadd(ye, kmul(acc, chi_a[rho]));
+                }
+                kq w = K1;
+                for (int q = 0; q < i; q++) w = kmul(w, gamma);
+                for (int q = 0; q < j; q++) w = kmul(w, gk);
+                ev = kadd(ev, kmul(w, ye));
+            }
+        }
+    }
+    kq lhs = kadd(kmul(eq_beta, kadd(Fp, nc)), kmul(eq_ar, kmul(gk, ev)));
+    kstore(out, lhs);
+    free(chi_a); free(chi_r); free(z1); free(zk); free(vj);
+}
+
+/* compute_y_from_Z_and_r (common.rs:582-650): y_j = Z (M_j^T chi_r) */
+void or_me_y_at_r(const or_ccs* s, const int8_t* Z, int ell_n, const uint64_t* r, int b,
+                  uint64_t* y, uint64_t* y_scalars) {
+    size_t m = s->m;
+    int t = s->t;
+    kq* chi = chi_table((const kq*)r, ell_n);
+    kq* vj = (kq*)malloc(sizeof(kq) * m);
+    uint64_t pw[D]; pw[0] = 1;
+    for (int q = 1; q < D; q++) pw[q] = fq_mul(pw[q - 1], (uint64_t)b);
+    for (int j = 0; j < t; j++) {
+        ccs_matTvec(s, j, chi, (size_t)1 << ell_n, vj);
+        kq sc = K0;
+        for (int rho = 0; rho < D; rho++) {
+            kq acc = K0;
+            const int8_t* zr = Z + (size_t)rho * m;
+            for (size_t c = 0; c < m; c++) if (zr[c]) acc = kadd(acc, kscale(vj[c], fq_from_i64(zr[c])));
+            kstore(y + 2 * ((size_t)j * D + rho), acc);
+            sc = kadd(sc, kscale(acc, pw[rho]));
+        }
+        kstore(y_scalars + 2 * j, sc);
+    }
+    free(chi); free(vj);
+}

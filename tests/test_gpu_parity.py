@@ -1,0 +1,105 @@
+"""GPU (sm_100a) results through the C ABI against the C oracle: bit-exact."""
+import numpy as np
+import pytest
+
+import oracle as O
+from tests.helpers import ccs_case, ELL_D, D_SC, XS
+
+Q = (1 << 64) - (1 << 32) + 1
+pytestmark = pytest.mark.gpu
+
+
+def _pp(kappa, m, seed):
+    return np.random.default_rng(seed).integers(0, Q, size=(kappa, m, 54), dtype=np.uint64)
+
+
+@pytest.mark.parametrize("m,n_vec", [(64, 1), (1024, 3), (4096, 13), (1 << 16, 1)])
+def test_commit_matches_oracle(ctx, m, n_vec):
+    pp = _pp(16, m, m)
+    rng = np.random.default_rng(m + n_vec)
+    Z = rng.integers(-1, 2, size=(n_vec, 54, m)).astype(np.int8)
+    ctx.pp_upload(pp)
+    got = ctx.commit(Z)
+    for v in range(n_vec):
+        assert np.array_equal(got[v], O.commit_digits(pp, Z[v]))
+
+
+def test_commit_edge_digits(ctx):
+    m = 256
+    pp = _pp(16, m, 1)
+    ctx.pp_upload(pp)
+    zeros = np.zeros((54, m), np.int8)
+    assert np.all(ctx.commit(zeros) == 0)
+    ones = np.ones((54, m), np.int8)
+    big = np.full((54, m), -128, np.int8)
+    assert np.array_equal(ctx.commit(ones), O.commit_digits(pp, ones))
+    assert np.array_equal(ctx.commit(big), O.commit_digits(pp, big))
+
+
+def test_decomp_matches_oracle(ctx):
+    rng = np.random.default_rng(3)
+    z = np.concatenate([rng.integers(0, 1 << 32, size=5000, dtype=np.uint64),
+                        (Q - rng.integers(1, 1 << 50, size=5000, dtype=np.uint64)).astype(np.uint64),
+                        np.array([0, 1, Q - 1, 1 << 60], np.uint64)])
+    assert np.array_equal(ctx.decomp_b2(z), O.decomp_b2(z))
+
+
+def test_rlc_mix_and_split_match_oracle(ctx):
+    rng = np.random.default_rng(4)
+    count, m = 13, 4096
+    rho = rng.integers(-2, 3, size=(count, 54)).astype(np.int8)
+    Zs = rng.integers(-1, 2, size=(count, 54, m)).astype(np.int8)
+    mix = ctx.rlc_mix(rho, Zs)
+    assert np.array_equal(mix, O.rlc_mix(rho, Zs))
+    planes, nz = ctx.split_b(mix, 12, 2)
+    p2, nz2 = O.split_b(mix, 12, 2)
+    assert np.array_equal(planes, p2) and np.array_equal(nz, nz2)
+    assert np.array_equal(ctx.rlc_mix(rho[:1], Zs[:1]), Zs[0].astype(np.int32))
+
+
+def test_split_out_of_range_is_an_error(ctx):
+    from nightstream_b200.gpu import NeoGpuError
+    with pytest.raises(NeoGpuError) as e:
+        ctx.split_b(np.array([[4096, 1]], np.int32), 12, 2)
+    assert e.value.code == 3
+
+
+def test_me_y_matches_oracle(ctx):
+    ccs, z, Z, ch, chals = ccs_case(10, 3, True)
+    r = chals[:10]
+    y, ys = ctx.me_y(ccs, Z, r)
+    for i in range(3):
+        y2, ys2 = O.me_y_at_r(ccs, Z[i], 10, r)
+        assert np.array_equal(y[i], y2) and np.array_equal(ys[i], ys2)
+
+
+def _run_both(ctx, ell, k, inputs, seed=7):
+    from nightstream_b200.gpu import GpuCcsOracle
+    ccs, z, Z, ch, chals = ccs_case(ell, k, inputs, seed)
+    args = (ccs, Z, 2, ch["alpha"], ch["beta_a"], ch["beta_r"], ch["gamma"], ch["r_inputs"], ELL_D, ell, D_SC)
+    g = GpuCcsOracle(ctx, *args)
+    o = O.CcsOracle(*args)
+    assert g.num_rounds() == ell + ELL_D and g.degree_bound() == D_SC
+    for r in range(ell + ELL_D):
+        yg = g.evals_at(XS)
+        yo = o.evals_at(XS)
+        assert np.array_equal(yg, yo), f"round {r}"
+        # a second evaluation in the same round (other points) must agree too
+        xs2 = chals[r:r + 2]
+        assert np.array_equal(g.evals_at(xs2), o.evals_at(xs2)), f"round {r} ext points"
+        g.fold(chals[r])
+        o.fold(chals[r])
+    yg, ysg = g.me_outputs()
+    yo, yso = o.me_outputs()
+    assert np.array_equal(yg, yo) and np.array_equal(ysg, yso)
+    g.close()
+
+
+@pytest.mark.parametrize("ell,k,inputs", [(1, 1, False), (3, 2, True), (6, 1, False), (10, 13, True), (12, 3, True)])
+def test_ccs_oracle_all_rounds_match(ctx, ell, k, inputs):
+    _run_both(ctx, ell, k, inputs)
+
+
+def test_ccs_oracle_steady_state_full_size(ctx):
+    # k = 13 (1 MCS + 12 carried children), n = m = 2^16
+    _run_both(ctx, 16, 13, True, seed=11)
