@@ -1,0 +1,212 @@
+// transcript.cpp -- Poseidon2 width-8 permutation, ChaCha8 and the sponge.
+#include "transcript.h"
+#include "gl.cuh"
+
+namespace neo {
+
+// ---------------------------------------------------------------- ChaCha8 --
+static inline uint32_t rotl(uint32_t x, int n) { return (x << n) | (x >> (32 - n)); }
+#define QR(a, b, c, d)          \
+    a += b; d ^= a; d = rotl(d, 16); \
+    c += d; b ^= c; b = rotl(b, 12); \
+    a += b; d ^= a; d = rotl(d, 8);  \
+    c += d; b ^= c; b = rotl(b, 7);
+
+ChaCha8::ChaCha8(const uint8_t seed[32]) {
+    for (int i = 0; i < 8; i++)
+        key[i] = (uint32_t)seed[4 * i] | ((uint32_t)seed[4 * i + 1] << 8) | ((uint32_t)seed[4 * i + 2] << 16) |
+                 ((uint32_t)seed[4 * i + 3] << 24);
+}
+
+void ChaCha8::refill() {
+    uint32_t s[16] = {0x61707865u, 0x3320646eu, 0x79622d32u, 0x6b206574u, key[0], key[1], key[2], key[3],
+                      key[4],      key[5],      key[6],      key[7],      (uint32_t)counter,
+                      (uint32_t)(counter >> 32), 0u, 0u};
+    uint32_t x[16];
+    memcpy(x, s, sizeof x);
+    for (int r = 0; r < 4; r++) {  // 8 rounds = 4 double rounds
+        QR(x[0], x[4], x[8], x[12]);
+        QR(x[1], x[5], x[9], x[13]);
+        QR(x[2], x[6], x[10], x[14]);
+        QR(x[3], x[7], x[11], x[15]);
+        QR(x[0], x[5], x[10], x[15]);
+        QR(x[1], x[6], x[11], x[12]);
+        QR(x[2], x[7], x[8], x[13]);
+        QR(x[3], x[4], x[9], x[14]);
+    }
+    for (int i = 0; i < 16; i++) block[i] = x[i] + s[i];
+    counter++;
+    idx = 0;
+}
+
+uint32_t ChaCha8::next_u32() {
+    if (idx >= 16) refill();
+    return block[idx++];
+}
+uint64_t ChaCha8::next_u64() {
+    uint64_t lo = next_u32();
+    uint64_t hi = next_u32();
+    return lo | (hi << 32);
+}
+void ChaCha8::fill_bytes(uint8_t* out, size_t n) {
+    size_t i = 0;
+    while (i < n) {
+        uint32_t w = next_u32();
+        for (int b = 0; b < 4 && i < n; b++, i++) out[i] = (uint8_t)(w >> (8 * b));
+    }
+}
+
+// --------------------------------------------------------------- Poseidon2 --
+static const uint8_t SEED[32] = {'n', 'e', 'o', '_', 'p', 'o', 's', 'e', 'i', 'd', 'o', 'n', '2', '_', 'g', 'o',
+                                 'l', 'd', 'i', 'l', 'o', 'c', 'k', 's', '_', 's', 'e', 'e', 'd', '_', '_', '_'};
+
+static uint64_t sample_fq(ChaCha8& rng) {
+    for (;;) {
+        uint64_t x = rng.next_u64();
+        if (x < GL_Q) return x;
+    }
+}
+
+Poseidon2W8::Poseidon2W8() {
+    ChaCha8 rng(SEED);
+    for (int r = 0; r < RF; r++)
+        for (int i = 0; i < W; i++) rc_ext[r][i] = sample_fq(rng);
+    for (int r = 0; r < RP; r++) rc_int[r] = sample_fq(rng);
+    for (int i = 0; i < W; i++) mu[i] = sample_fq(rng);
+}
+
+const Poseidon2W8& Poseidon2W8::get() {
+    static const Poseidon2W8 inst;
+    return inst;
+}
+
+static inline uint64_t sbox7(uint64_t x) {
+    uint64_t x2 = gl::mul(x, x);
+    uint64_t x3 = gl::mul(x2, x);
+    uint64_t x6 = gl::mul(x3, x3);
+    return gl::mul(x6, x);
+}
+
+// M4 of the Poseidon2 paper: [[5,7,1,3],[4,6,1,1],[1,3,5,7],[1,1,4,6]]
+static inline void m4(uint64_t* x) {
+    static const uint32_t M[4][4] = {{5, 7, 1, 3}, {4, 6, 1, 1}, {1, 3, 5, 7}, {1, 1, 4, 6}};
+    uint64_t y[4];
+    for (int r = 0; r < 4; r++) {
+        uint64_t acc = 0;
+        for (int c = 0; c < 4; c++) acc = gl::add(acc, gl::mul_small(x[c], M[r][c]));
+        y[r] = acc;
+    }
+    memcpy(x, y, sizeof y);
+}
+
+// external layer circ(2 M4, M4): y_i = M4 x_blk(i) + sum_blk M4 x_blk
+static inline void external_layer(uint64_t* st) {
+    m4(st);
+    m4(st + 4);
+    for (int i = 0; i < 4; i++) {
+        uint64_t s = gl::add(st[i], st[4 + i]);
+        st[i] = gl::add(st[i], s);
+        st[4 + i] = gl::add(st[4 + i], s);
+    }
+}
+
+static inline void internal_layer(uint64_t* st, const uint64_t* mu) {
+    uint64_t sum = 0;
+    for (int i = 0; i < 8; i++) sum = gl::add(sum, st[i]);
+    for (int i = 0; i < 8; i++) st[i] = gl::add(sum, gl::mul(mu[i], st[i]));
+}
+
+void Poseidon2W8::permute(uint64_t st[W]) const {
+    external_layer(st);
+    for (int r = 0; r < RF / 2; r++) {
+        for (int i = 0; i < W; i++) st[i] = sbox7(gl::add(st[i], rc_ext[r][i]));
+        external_layer(st);
+    }
+    for (int r = 0; r < RP; r++) {
+        st[0] = sbox7(gl::add(st[0], rc_int[r]));
+        internal_layer(st, mu);
+    }
+    for (int r = RF / 2; r < RF; r++) {
+        for (int i = 0; i < W; i++) st[i] = sbox7(gl::add(st[i], rc_ext[r][i]));
+        external_layer(st);
+    }
+}
+
+// -------------------------------------------------------------- transcript --
+static const char* APP_DOMAIN = "neo/transcript/v1|poseidon2-goldilocks-w8-r4";
+
+Transcript::Transcript(const std::string& app_label) {
+    memset(st_, 0, sizeof st_);
+    append_message(APP_DOMAIN, reinterpret_cast<const uint8_t*>(app_label.data()), app_label.size());
+}
+
+void Transcript::permute() {
+    Poseidon2W8::get().permute(st_);
+    absorbed_ = 0;
+    perms_++;
+}
+
+void Transcript::absorb_elem(uint64_t x) {
+    if (absorbed_ >= RATE) permute();
+    st_[absorbed_++] = x;
+}
+
+void Transcript::absorb_slice(const uint64_t* xs, size_t len) {
+    size_t src = 0;
+    while (absorbed_ < RATE && src < len) st_[absorbed_++] = xs[src++];
+    if (absorbed_ == RATE) permute();
+    while (len - src >= (size_t)RATE) {
+        for (int i = 0; i < RATE; i++) st_[i] = xs[src + i];
+        permute();
+        src += RATE;
+    }
+    while (src < len) st_[absorbed_++] = xs[src++];
+}
+
+void Transcript::absorb_label(const std::string& label) {
+    for (unsigned char c : label) absorb_elem((uint64_t)c);
+}
+
+void Transcript::append_message(const std::string& label, const uint8_t* msg, size_t len) {
+    absorb_label(label);
+    absorb_elem((uint64_t)len);
+    for (size_t i = 0; i < len; i++) absorb_elem((uint64_t)msg[i]);
+}
+
+void Transcript::append_fields(const std::string& label, const uint64_t* fs, size_t n) {
+    absorb_label(label);
+    absorb_elem((uint64_t)n);
+    absorb_slice(fs, n);
+}
+
+void Transcript::append_u64s(const std::string& label, const uint64_t* us, size_t n) {
+    absorb_label(label);
+    absorb_elem((uint64_t)n);
+    for (size_t i = 0; i < n; i++) absorb_elem(gl::canon(us[i]));
+}
+
+uint64_t Transcript::challenge_field(const std::string& label) {
+    append_message("chal/label", reinterpret_cast<const uint8_t*>(label.data()), label.size());
+    absorb_elem(1);
+    permute();
+    return st_[0];
+}
+
+void Transcript::challenge_fields(const std::string& label, size_t n, uint64_t* out) {
+    append_message("chal/label", reinterpret_cast<const uint8_t*>(label.data()), label.size());
+    size_t got = 0;
+    while (got < n) {
+        absorb_elem(1);
+        permute();
+        for (int i = 0; i < 4 && got < n; i++) out[got++] = st_[i];
+    }
+}
+
+void Transcript::digest32(uint8_t out[32]) {
+    absorb_elem(1);
+    permute();
+    for (int i = 0; i < 4; i++)
+        for (int b = 0; b < 8; b++) out[8 * i + b] = (uint8_t)(st_[i] >> (8 * b));
+}
+
+}  // namespace neo

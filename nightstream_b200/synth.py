@@ -16,6 +16,8 @@ from .params import Q
 
 def _distinct_cols(rng, n, m, k):
     cols = rng.integers(0, m, size=(n, k), dtype=np.int64)
+    if m < 2 * k:
+        return cols  # too few columns for distinct picks: duplicates add up
     while True:
         s = np.sort(cols, axis=1)
         dup = np.any(s[:, 1:] == s[:, :-1], axis=1)

@@ -1030,3 +1030,138 @@ void or_me_y_at_r(const or_ccs* s, const int8_t* Z, int ell_n, const uint64_t* r
     }
     free(chi); free(vj);
 }
+
+/* ------------------------------------------------------------------------ */
+/* Transcript: Poseidon2 width-8 overwrite sponge                            */
+/* (crates/neo-transcript/src/poseidon2.rs:10-310).  Permutation restated     */
+/* from the Poseidon2 paper (eprint 2023/323): t=8, x^7, R_F=8, R_P=22,       */
+/* external circ(2M4, M4), internal 1 + diag(mu); constants from ChaCha8      */
+/* (RFC 7539 block function, 8 rounds) seeded with the reference SEED, by     */
+/* rejection sampling.  Parity unpinned (p3-poseidon2 0.4.1 not vendored).    */
+/* ------------------------------------------------------------------------ */
+typedef struct { uint32_t key[8]; uint64_t ctr; uint32_t blk[16]; int idx; } or_chacha;
+static uint32_t rl(uint32_t x, int n) { return (x << n) | (x >> (32 - n)); }
+static void cc_refill(or_chacha* c) {
+    uint32_t s[16] = {0x61707865u, 0x3320646eu, 0x79622d32u, 0x6b206574u};
+    for (int i = 0; i < 8; i++) s[4 + i] = c->key[i];
+    s[12] = (uint32_t)c->ctr; s[13] = (uint32_t)(c->ctr >> 32); s[14] = 0; s[15] = 0;
+    uint32_t x[16];
+    memcpy(x, s, sizeof x);
+    static const int QI[8][4] = {{0,4,8,12},{1,5,9,13},{2,6,10,14},{3,7,11,15},{0,5,10,15},{1,6,11,12},{2,7,8,13},{3,4,9,14}};
+    for (int r = 0; r < 4; r++)
+        for (int q = 0; q < 8; q++) {
+            uint32_t *a = &x[QI[q][0]], *b = &x[QI[q][1]], *cc = &x[QI[q][2]], *d = &x[QI[q][3]];
+            *a += *b; *d ^= *a; *d = rl(*d, 16);
+            *cc += *d; *b ^= *cc; *b = rl(*b, 12);
+            *a += *b; *d ^= *a; *d = rl(*d, 8);
+            *cc += *d; *b ^= *cc; *b = rl(*b, 7);
+        }
+    for (int i = 0; i < 16; i++) c->blk[i] = x[i] + s[i];
+    c->ctr++;
+    c->idx = 0;
+}
+static uint64_t cc_u64(or_chacha* c) {
+    if (c->idx >= 16) cc_refill(c);
+    uint64_t lo = c->blk[c->idx++];
+    if (c->idx >= 16) cc_refill(c);
+    uint64_t hi = c->blk[c->idx++];
+    return lo | (hi << 32);
+}
+
+static uint64_t P2_RCE[8][8], P2_RCI[22], P2_MU[8];
+static int p2_ready = 0;
+static void p2_init(void) {
+    if (p2_ready) return;
+    const char* seed = "neo_poseidon2_goldilocks_seed___";
+    or_chacha c;
+    for (int i = 0; i < 8; i++)
+        c.key[i] = (uint32_t)(uint8_t)seed[4*i] | ((uint32_t)(uint8_t)seed[4*i+1] << 8) |
+                   ((uint32_t)(uint8_t)seed[4*i+2] << 16) | ((uint32_t)(uint8_t)seed[4*i+3] << 24);
+    c.ctr = 0; c.idx = 16;
+    uint64_t* outs[3] = {&P2_RCE[0][0], P2_RCI, P2_MU};
+    int lens[3] = {64, 22, 8};
+    for (int g = 0; g < 3; g++)
+        for (int i = 0; i < lens[g]; i++) {
+            uint64_t x;
+            do { x = cc_u64(&c); } while (x >= Q);
+            outs[g][i] = x;
+        }
+    p2_ready = 1;
+}
+static uint64_t p2_s7(uint64_t x) { uint64_t x2 = fq_mul(x, x), x3 = fq_mul(x2, x), x6 = fq_mul(x3, x3); return fq_mul(x6, x); }
+static void p2_ext(uint64_t* st) {
+    static const uint64_t M[4][4] = {{5,7,1,3},{4,6,1,1},{1,3,5,7},{1,1,4,6}};
+    uint64_t y[8];
+    for (int b = 0; b < 2; b++)
+        for (int r = 0; r < 4; r++) {
+            uint64_t a = 0;
+            for (int cc = 0; cc < 4; cc++) a = fq_add(a, fq_mul(M[r][cc], st[4*b + cc]));
+            y[4*b + r] = a;
+        }
+    for (int i = 0; i < 4; i++) {
+        uint64_t s = fq_add(y[i], y[4 + i]);
+        st[i] = fq_add(y[i], s);
+        st[4 + i] = fq_add(y[4 + i], s);
+    }
+}
+void or_poseidon2_permute(uint64_t* st) {
+    p2_init();
+    p2_ext(st);
+    for (int r = 0; r < 4; r++) { for (int i = 0; i < 8; i++) st[i] = p2_s7(fq_add(st[i], P2_RCE[r][i])); p2_ext(st); }
+    for (int r = 0; r < 22; r++) {
+        st[0] = p2_s7(fq_add(st[0], P2_RCI[r]));
+        uint64_t s = 0;
+        for (int i = 0; i < 8; i++) s = fq_add(s, st[i]);
+        for (int i = 0; i < 8; i++) st[i] = fq_add(s, fq_mul(P2_MU[i], st[i]));
+    }
+    for (int r = 4; r < 8; r++) { for (int i = 0; i < 8; i++) st[i] = p2_s7(fq_add(st[i], P2_RCE[r][i])); p2_ext(st); }
+}
+
+typedef struct or_transcript { uint64_t st[8]; int absorbed; } or_transcript;
+static void tr_perm(or_transcript* t) { or_poseidon2_permute(t->st); t->absorbed = 0; }
+static void tr_elem(or_transcript* t, uint64_t x) { if (t->absorbed >= 4) tr_perm(t); t->st[t->absorbed++] = x; }
+static void tr_bytes(or_transcript* t, const char* s, size_t n) { for (size_t i = 0; i < n; i++) tr_elem(t, (uint8_t)s[i]); }
+void or_tr_append_message(or_transcript* t, const char* label, const uint8_t* msg, size_t len) {
+    tr_bytes(t, label, strlen(label));
+    tr_elem(t, len);
+    for (size_t i = 0; i < len; i++) tr_elem(t, msg[i]);
+}
+or_transcript* or_tr_new(const char* app_label) {
+    or_transcript* t = (or_transcript*)calloc(1, sizeof(*t));
+    or_tr_append_message(t, "neo/transcript/v1|poseidon2-goldilocks-w8-r4", (const uint8_t*)app_label, strlen(app_label));
+    return t;
+}
+void or_tr_free(or_transcript* t) { free(t); }
+void or_tr_append_fields(or_transcript* t, const char* label, const uint64_t* fs, size_t n) {
+    tr_bytes(t, label, strlen(label));
+    tr_elem(t, n);
+    /* absorb_slice overwrite semantics are element-wise identical to repeated absorb_elem
+       except that a full chunk triggers the permutation eagerly (poseidon2.rs:29-60) */
+    size_t src = 0;
+    while (t->absorbed < 4 && src < n) t->st[t->absorbed++] = fs[src++];
+    if (t->absorbed == 4) tr_perm(t);
+    while (n - src >= 4) { for (int i = 0; i < 4; i++) t->st[i] = fs[src + i]; tr_perm(t); src += 4; }
+    while (src < n) t->st[t->absorbed++] = fs[src++];
+}
+void or_tr_append_u64s(or_transcript* t, const char* label, const uint64_t* us, size_t n) {
+    tr_bytes(t, label, strlen(label));
+    tr_elem(t, n);
+    for (size_t i = 0; i < n; i++) tr_elem(t, fq_canon(us[i]));
+}
+uint64_t or_tr_challenge_field(or_transcript* t, const char* label) {
+    or_tr_append_message(t, "chal/label", (const uint8_t*)label, strlen(label));
+    tr_elem(t, 1);
+    tr_perm(t);
+    return t->st[0];
+}
+void or_tr_challenge_fields(or_transcript* t, const char* label, size_t n, uint64_t* out) {
+    or_tr_append_message(t, "chal/label", (const uint8_t*)label, strlen(label));
+    size_t got = 0;
+    while (got < n) { tr_elem(t, 1); tr_perm(t); for (int i = 0; i < 4 && got < n; i++) out[got++] = t->st[i]; }
+}
+void or_tr_digest32(or_transcript* t, uint8_t* out) {
+    tr_elem(t, 1);
+    tr_perm(t);
+    for (int i = 0; i < 4; i++) for (int b = 0; b < 8; b++) out[8*i + b] = (uint8_t)(t->st[i] >> (8*b));
+}
+void or_tr_state(const or_transcript* t, uint64_t* out) { memcpy(out, t->st, 64); }

@@ -105,6 +105,19 @@ void or_q_eval_ext(const or_ccs* s, const int8_t* Z, int k, int b,
 void or_me_y_at_r(const or_ccs* s, const int8_t* Z, int ell_n, const uint64_t* r, int b,
                   uint64_t* y, uint64_t* y_scalars);
 
+/* ---- transcript (crates/neo-transcript/src/poseidon2.rs; parity unpinned) ---- */
+typedef struct or_transcript or_transcript;
+void or_poseidon2_permute(uint64_t* st);
+or_transcript* or_tr_new(const char* app_label);
+void or_tr_free(or_transcript* t);
+void or_tr_append_message(or_transcript* t, const char* label, const uint8_t* msg, size_t len);
+void or_tr_append_fields(or_transcript* t, const char* label, const uint64_t* fs, size_t n);
+void or_tr_append_u64s(or_transcript* t, const char* label, const uint64_t* us, size_t n);
+uint64_t or_tr_challenge_field(or_transcript* t, const char* label);
+void or_tr_challenge_fields(or_transcript* t, const char* label, size_t n, uint64_t* out);
+void or_tr_digest32(or_transcript* t, uint8_t* out);
+void or_tr_state(const or_transcript* t, uint64_t* out);
+
 #ifdef __cplusplus
 }
 #endif
