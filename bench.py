@@ -1,0 +1,306 @@
+#!/usr/bin/env python
+"""Shard fold-steps/sec of the Neo fold step on B200.
+
+One "step" is one steady-state fold step of a shard (k = 13: the step's MCS
+instance plus 12 carried DEC children): witness decomposition + MCS Ajtai
+commitment, Pi_CCS sum-check (ell_n batched-time rounds + 6 Ajtai rounds), ME
+outputs, Pi_RLC and Pi_DEC (12 child commitments and child ME claims), with the
+Poseidon2 Fiat-Shamir transcript in between, over a seeded synthetic R1CS of
+n = m = 2^16 constraints (3 nonzeros per row, uniform F_q coefficients).
+
+Usage: python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+Multi-GPU runs (torchrun) place one independent shard per rank (replicas):
+value = steps of all ranks / max-over-ranks device time.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+Q = (1 << 64) - (1 << 32) + 1
+METRIC = "shard fold-steps/sec"
+UNIT = "fold-steps/s"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--ell", type=int, default=16, help="log2 of the CCS size n = m")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def workload(ell, rank):
+    from nightstream_b200 import synth
+    ccs, z = synth.make_r1cs(ell, 1234 + rank)
+    pp = np.random.default_rng(99 + rank).integers(0, Q, size=(16, 1 << ell, 54), dtype=np.uint64)
+    return ccs, z, pp
+
+
+def config(ell):
+    return {
+        "workload": f"steady-state fold step, main lane (Pi_CCS + Pi_RLC + Pi_DEC), "
+                    f"R1CS n=m=2^{ell}, k=13, no Twist/Shout",
+        "n": 1 << ell, "m": 1 << ell, "k": 13, "kappa": 16, "d": 54, "b": 2, "k_rho": 12,
+        "sumcheck_rounds": ell + 6, "commits_per_step": 13,
+        "l2": "inputs larger than L2 (PP limbs 453 MB at 2^16, read by every commit)",
+        "witness": "seeded synthetic R1CS witness, values in [0, 2^32), same witness each step",
+    }
+
+
+class Clocks:
+    """nvidia-smi sampling during the timed region."""
+
+    def __init__(self, index):
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", f"--id={index}", f"--query-gpu={q}", "--format=csv,noheader,nounits",
+                                       "-lms", "200"], stdout=self.f, stderr=subprocess.DEVNULL)
+        except OSError:
+            self.p = None
+
+    def stop(self):
+        if not self.p:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.p.terminate()
+        self.p.wait()
+        self.f.seek(0)
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.f.read().splitlines():
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx.append(float(parts[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        os.unlink(self.f.name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def measured_peaks():
+    try:
+        return json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except (OSError, ValueError):
+        return {}
+
+
+def int8_peak_tops():
+    """Dense int8 GEMM throughput via torch._int_mm (cuBLASLt), 8192^3."""
+    import torch
+    try:
+        a = torch.randint(-64, 64, (8192, 8192), dtype=torch.int8, device="cuda")
+        b = torch.randint(-64, 64, (8192, 8192), dtype=torch.int8, device="cuda")
+        for _ in range(3):
+            torch._int_mm(a, b)
+        torch.cuda.synchronize()
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        best = 1e9
+        for _ in range(5):
+            s.record()
+            for _ in range(5):
+                torch._int_mm(a, b)
+            e.record()
+            e.synchronize()
+            best = min(best, s.elapsed_time(e) / 5)
+        return 2 * 8192 ** 3 / (best * 1e-3) / 1e12, "measured torch._int_mm 8192^3 (cuBLASLt int8)"
+    except Exception as ex:  # pragma: no cover - depends on the box
+        pk = measured_peaks().get("bf16_tflops", 1590.0)
+        return 2 * pk, f"2x measured bf16 (int8 GEMM unavailable: {type(ex).__name__})"
+
+
+def cpu_baseline(ell, ccs, z, pp):
+    """One oracle fold step (C restatement, OpenMP on all host cores) after step 0."""
+    from oracle.fold import OracleShard
+    sh = OracleShard(ccs, pp, m_in=1, k_rho=12, app_label=b"neo/bench")
+    sh.fold_step(z)  # step 0 (k = 1)
+    t0 = time.perf_counter()
+    sh.fold_step(z)
+    dt = time.perf_counter() - t0
+    return {"value": 1.0 / dt, "unit": UNIT, "cores": os.cpu_count(), "kind": "port",
+            "sample": f"one steady-state fold step (k=13) at n=m=2^{ell} on the C oracle "
+                      f"(OpenMP, {os.cpu_count()} threads): {dt:.2f} s"}
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return
+    from oracle.fold import OracleShard
+    ccs, z, pp = workload(args.ell, 0)
+    sh = OracleShard(ccs, pp, m_in=1, k_rho=12, app_label=b"neo/bench")
+    sh.fold_step(z)
+    t0 = time.perf_counter()
+    sh.fold_step(z)
+    est = time.perf_counter() - t0
+    budget = 150.0
+    warm = min(args.warmup, max(0, int(budget / 3 / est) - 1))
+    steps = max(1, min(args.steps, int(budget / est)))
+    for _ in range(warm):
+        sh.fold_step(z)
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        sh.fold_step(z)
+    dt = time.perf_counter() - t0
+    value = steps / dt
+    out = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": steps,
+           "warmup": warm, "ms_per_step": dt / steps * 1e3, "higher_is_better": True, "scaling": "weak",
+           "vs_baseline": None, "dtype": "u64 (F_q, K = F_q^2), int8 digits", "data": "synthetic",
+           "config": config(args.ell), "impl": "reference",
+           "cpu_baseline": {"value": value, "unit": UNIT, "cores": os.cpu_count(), "kind": "port",
+                            "sample": f"{steps} steady-state fold steps at n=m=2^{args.ell} on the C restatement "
+                                      f"(Rust reference not buildable here: no cargo/rustc)"},
+           "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(out), flush=True)
+
+
+def run_ours(args, rank, world, local_rank):
+    import torch
+    from nightstream_b200 import gpu
+    torch.cuda.set_device(local_rank)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+    ccs, z, pp = workload(args.ell, rank)
+    m = 1 << args.ell
+    ctx = gpu.Context(local_rank)
+    ctx.pp_upload(pp)
+    shard = gpu.Shard(ctx, ccs, m_in=1, k_rho=12, app_label=b"neo/bench")
+    stream = torch.cuda.ExternalStream(ctx.stream)
+    zt = torch.from_numpy(z.view(np.int64).copy()).cuda()
+    d_z = zt.data_ptr()
+    torch.cuda.synchronize()
+    shard.fold_step_device(d_z)  # step 0: k = 1 -> steady state afterwards
+    for _ in range(args.warmup):
+        shard.fold_step_device(d_z)
+    ctx.synchronize()
+
+    def barrier():
+        if dist:
+            dist.barrier()
+
+    barrier()
+    clocks = Clocks(local_rank)
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    l0 = ctx.kernel_launches
+    ctx.synchronize()
+    torch.cuda.synchronize()
+    ev0.record(stream)
+    for _ in range(args.steps):
+        shard.fold_step_device(d_z)
+    ev1.record(stream)
+    ev1.synchronize()
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    ms = ev0.elapsed_time(ev1)
+    launches = ctx.kernel_launches - l0
+    barrier()
+    stats = shard.step_stats()
+    if dist:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    value = world * args.steps / (ms * 1e-3)
+
+    # end-to-end through the C ABI with host buffers: pinned z in, proof words out
+    e2e = None
+    if not args.no_e2e:
+        zp = torch.from_numpy(z.view(np.int64).copy()).pin_memory()
+        zh = zp.numpy().view(np.uint64)
+        proof = shard.fold_step(zh)  # sizes the proof buffer
+        barrier()
+        ctx.synchronize()
+        ev0.record(stream)
+        for _ in range(args.steps):
+            proof = shard.fold_step(zh)
+        ev1.record(stream)
+        ev1.synchronize()
+        ems = ev0.elapsed_time(ev1)
+        if dist:
+            t = torch.tensor([ems], device="cuda")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ems = float(t.item())
+        e2e = {"value": world * args.steps / (ems * 1e-3), "unit": UNIT, "h2d_bytes_per_step": int(zh.nbytes),
+               "d2h_bytes_per_step": int(proof.nbytes)}
+
+    # dominant kernel roofline: the DEC batch commitment (12 digit planes, one launch pair)
+    n_vec = 12
+    digits = torch.randint(-1, 2, (n_vec, 54, m), dtype=torch.int8, device="cuda")
+    outc = torch.empty((n_vec, 16, 54), dtype=torch.int64, device="cuda")
+    torch.cuda.synchronize()
+    for _ in range(2):
+        ctx.commit_device(digits.data_ptr(), n_vec, m, outc.data_ptr())
+    ctx.synchronize()
+    reps = 5
+    ev0.record(stream)
+    for _ in range(reps):
+        ctx.commit_device(digits.data_ptr(), n_vec, m, outc.data_ptr())
+    ev1.record(stream)
+    ev1.synchronize()
+    commit_ms = ev0.elapsed_time(ev1) / reps
+    ops = 746496 * m * n_vec  # 2 * 8 limbs * kappa * d^2 * m per commitment
+    peak, peak_src = int8_peak_tops()
+    achieved = ops / (commit_ms * 1e-3) / 1e12
+    roofline = {"kernel": "Ajtai commit, 12 DEC planes per launch (commit_partial_kernel + commit_reduce_kernel)",
+                "bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TOPS", "frac": achieved / peak,
+                "traffic": None, "launch_ms": commit_ms, "peak_source": peak_src,
+                "algorithmic_ops_per_launch": ops}
+
+    if rank == 0:
+        out = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+               "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+               "vs_baseline": None, "dtype": "u64 (F_q, K = F_q^2), int8 digits", "data": "synthetic",
+               "config": config(args.ell), "e2e": e2e, "gpu_launches": int(launches), "clocks": clk,
+               "roofline": roofline, "step_breakdown_ms": stats}
+        if world == 1 and not args.no_cpu_baseline:
+            out["cpu_baseline"] = cpu_baseline(args.ell, ccs, z, pp)
+        print(json.dumps(out), flush=True)
+    shard.close()
+    ctx.close()
+
+
+def main():
+    args = parse()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    try:
+        if args.impl == "reference":
+            run_reference(args, rank, world)
+        else:
+            run_ours(args, rank, world, local_rank)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -57,6 +57,9 @@ int neo_gpu_ctx_destroy(neo_gpu_ctx* ctx);
 const char* neo_gpu_last_error(const neo_gpu_ctx* ctx);
 /* Number of kernels this context has launched so far (instrumentation). */
 uint64_t neo_gpu_kernel_launches(const neo_gpu_ctx* ctx);
+/* The context's CUDA stream (a cudaStream_t), for event timing by callers. */
+int neo_gpu_ctx_stream(const neo_gpu_ctx* ctx, void** stream);
+int neo_gpu_synchronize(neo_gpu_ctx* ctx);
 
 /* ---- Ajtai commitment (crates/neo-ajtai) ---------------------------- */
 /* Upload public parameters M in R_q^{kappa x m}: coeffs[(i*m + j)*54 + s] is
@@ -71,6 +74,10 @@ int neo_gpu_pp_upload(neo_gpu_ctx* ctx, uint32_t kappa, uint64_t m, const uint64
  * (crates/neo-ccs/src/traits.rs:8-14; crates/neo-ajtai/src/s_module.rs:335-377)
  * and commit_row_major (crates/neo-ajtai/src/commit.rs:376-402, 679-744). */
 int neo_gpu_commit(neo_gpu_ctx* ctx, const int8_t* digits, uint32_t n_vec, uint64_t m, uint64_t* out);
+
+/* neo_gpu_commit with DEVICE pointers (digits and out already in HBM); the
+ * call is asynchronous on the context stream. */
+int neo_gpu_commit_device(neo_gpu_ctx* ctx, const int8_t* d_digits, uint32_t n_vec, uint64_t m, uint64_t* d_out);
 
 /* Balanced base-2 decomposition z in F_q^m -> Z in {-1,0,1}^{54 x m}
  * row-major (crates/neo-ajtai/src/decomp.rs:118-158, DecompStyle::Balanced). */
@@ -118,6 +125,51 @@ uint32_t neo_gpu_ccs_oracle_degree_bound(const neo_gpu_ccs_oracle* o);
  * ell_n row rounds: y [k][t][54] K digits and y_scalars [k][t] K. */
 int neo_gpu_ccs_oracle_me_outputs(neo_gpu_ccs_oracle* o, uint64_t* y, uint64_t* y_scalars);
 int neo_gpu_ccs_oracle_destroy(neo_gpu_ccs_oracle* o);
+
+/* ---- shard prove loop (crates/neo-fold/src/shard.rs:1725-2283) ------- */
+typedef struct neo_gpu_shard neo_gpu_shard;
+/* A shard prover over one CCS (n == m == 2^ell_n, identity-first, t <= 4,
+ * b = 2) with its own Poseidon2 transcript (new(app_label)), a device-resident
+ * accumulator and k_rho DEC children per step.  PP for this m must already be
+ * uploaded on ctx.  Computes the CCS matrix digest
+ * (crates/neo-reductions/src/engines/utils.rs:214-321) once. */
+int neo_gpu_shard_create(neo_gpu_ctx* ctx, const neo_ccs_desc* ccs, uint32_t m_in, uint32_t k_rho,
+                         const char* app_label, neo_gpu_shard** out);
+/* One fold step on the main lane (no Twist/Shout): witness build
+ * (decomp + MCS commit, crates/neo-fold/src/session.rs:977-978), Pi_CCS
+ * (batched time rounds + Ajtai rounds), ME outputs, Pi_RLC, Pi_DEC
+ * (shard.rs:1803-2180, 1170-1331).  z: the step witness (m values, host).
+ * proof: canonical dump of the step proof (see DESIGN.md for the word order);
+ * pass NULL to query *proof_len. */
+int neo_gpu_shard_fold_step(neo_gpu_shard* sh, const uint64_t* z, uint64_t* proof, uint64_t proof_cap,
+                            uint64_t* proof_len);
+/* Same step with the witness already resident in device memory (d_z). */
+int neo_gpu_shard_fold_step_device(neo_gpu_shard* sh, const uint64_t* d_z, uint64_t* proof_len);
+/* Transcript sponge state (8 words) and CCS matrix digest (4 words). */
+int neo_gpu_shard_transcript_state(const neo_gpu_shard* sh, uint64_t* st8);
+int neo_gpu_shard_ccs_digest(const neo_gpu_shard* sh, uint64_t* d4);
+/* Host milliseconds of the last step: [0] total, [1] witness decomp+commit,
+ * [2] header/ME binding + challenges, [3] Pi_CCS table build, [4] batched
+ * time rounds, [5] Ajtai rounds, [6] ME outputs, [7] Pi_RLC, [8] Pi_DEC;
+ * [9] transcript permutations of the step. */
+int neo_gpu_shard_step_stats(const neo_gpu_shard* sh, double* out, uint32_t n);
+int neo_gpu_shard_destroy(neo_gpu_shard* sh);
+
+/* ---- Fiat-Shamir transcript (host only, no GPU needed) --------------- */
+/* Poseidon2Transcript (crates/neo-transcript/src/poseidon2.rs:10-310):
+ * width-8 overwrite sponge, rate 4, one field element per label byte. */
+typedef struct neo_transcript neo_transcript;
+int neo_transcript_new(const char* app_label, neo_transcript** out);
+int neo_transcript_append_message(neo_transcript* t, const char* label, const uint8_t* msg, size_t len);
+int neo_transcript_append_fields(neo_transcript* t, const char* label, const uint64_t* fs, size_t n);
+int neo_transcript_append_u64s(neo_transcript* t, const char* label, const uint64_t* us, size_t n);
+int neo_transcript_challenge_field(neo_transcript* t, const char* label, uint64_t* out);
+int neo_transcript_challenge_fields(neo_transcript* t, const char* label, size_t n, uint64_t* out);
+int neo_transcript_digest32(neo_transcript* t, uint8_t* out32);
+int neo_transcript_state(const neo_transcript* t, uint64_t* st8);
+int neo_transcript_destroy(neo_transcript* t);
+/* digest_ccs_matrices (crates/neo-reductions/src/engines/utils.rs:214-321). */
+int neo_ccs_digest(const neo_ccs_desc* ccs, uint64_t* out4);
 
 #ifdef __cplusplus
 }

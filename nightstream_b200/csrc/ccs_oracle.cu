@@ -571,8 +571,10 @@ struct neo_gpu_ccs_oracle {
     neo_gpu_ctx* ctx = nullptr;
     uint32_t k = 0, b = 2, ell_d = 0, ell_n = 0, d_sc = 0, t = 0;
     uint64_t n_pad = 0, m = 0;
-    DevCcs ccs;
-    DevBuf<int8_t> Z;
+    DevCcs own_ccs;          // used when the oracle owns its CCS copy
+    const DevCcs* ccs = nullptr;
+    DevBuf<int8_t> own_Z;    // used when the oracle owns its witness copy
+    const int8_t* Z = nullptr;
     FTerms f{};
     int n_fvar = 0;
     int fvar_j[MAX_FVAR] = {0};
@@ -607,6 +609,10 @@ static K host_chi_mask(size_t mask, const std::vector<K>& pts) {
     return p;
 }
 
+static int oracle_init(neo_gpu_ctx* ctx, neo_gpu_ccs_oracle* o, const int8_t* d_Z, uint32_t k, uint32_t b,
+                       const K* alpha, const K* beta_a, const K* beta_r, K gamma, const K* r_inputs,
+                       uint32_t ell_d, uint32_t ell_n, uint32_t d_sc);
+
 extern "C" int neo_gpu_ccs_oracle_create(neo_gpu_ctx* ctx, const neo_ccs_desc* desc, const int8_t* Z, uint32_t k,
                                          uint32_t b, const uint64_t* alpha, const uint64_t* beta_a,
                                          const uint64_t* beta_r, const uint64_t* gamma, const uint64_t* r_inputs,
@@ -614,30 +620,66 @@ extern "C" int neo_gpu_ccs_oracle_create(neo_gpu_ctx* ctx, const neo_ccs_desc* d
     if (!ctx) return NEO_ERR_ARG;
     if (!out || !desc || !Z || !alpha || !beta_a || !beta_r || !gamma) return ctx->fail(NEO_ERR_ARG, "ccs_oracle: null argument");
     *out = nullptr;
+    if (ell_d == 0 || ell_d > 8 || ell_n < 1 || ell_n > 30) return ctx->fail(NEO_ERR_ARG, "ccs_oracle: ell_d/ell_n out of range");
+    cudaSetDevice(ctx->device);
+    auto* o = new neo_gpu_ccs_oracle();
+    std::unique_ptr<neo_gpu_ccs_oracle> guard(o);
+    int rc = dev_ccs_upload(ctx, desc, o->own_ccs);
+    if (rc) return rc;
+    o->ccs = &o->own_ccs;
+    if (k == 0 || k > 18) return ctx->fail(NEO_ERR_ARG, "ccs_oracle: k must be in 1..18");
+    NEO_CK(ctx, o->own_Z.alloc((size_t)k * NEO_D * desc->m));
+    NEO_CK(ctx, cudaMemcpyAsync(o->own_Z.p, Z, o->own_Z.bytes(), cudaMemcpyHostToDevice, ctx->stream));
+    std::vector<K> al = load_k(alpha, ell_d), ba = load_k(beta_a, ell_d), br = load_k(beta_r, ell_n);
+    std::vector<K> ri;
+    if (r_inputs) ri = load_k(r_inputs, ell_n);
+    rc = oracle_init(ctx, o, o->own_Z.p, k, b, al.data(), ba.data(), br.data(), load_k(gamma, 1)[0],
+                     r_inputs ? ri.data() : nullptr, ell_d, ell_n, d_sc);
+    if (rc) return rc;
+    *out = guard.release();
+    return NEO_OK;
+}
+
+int ccs_oracle_create_dev(neo_gpu_ctx* ctx, const DevCcs* ccs, const int8_t* d_Z, uint32_t k, uint32_t b,
+                          const K* alpha, const K* beta_a, const K* beta_r, K gamma, const K* r_inputs,
+                          uint32_t ell_d, uint32_t ell_n, uint32_t d_sc, neo_gpu_ccs_oracle** out) {
+    auto* o = new neo_gpu_ccs_oracle();
+    std::unique_ptr<neo_gpu_ccs_oracle> guard(o);
+    o->ccs = ccs;
+    int rc = oracle_init(ctx, o, d_Z, k, b, alpha, beta_a, beta_r, gamma, r_inputs, ell_d, ell_n, d_sc);
+    if (rc) return rc;
+    *out = guard.release();
+    return NEO_OK;
+}
+
+static int oracle_init(neo_gpu_ctx* ctx, neo_gpu_ccs_oracle* o, const int8_t* d_Z, uint32_t k, uint32_t b,
+                       const K* alpha, const K* beta_a, const K* beta_r, K gamma, const K* r_inputs,
+                       uint32_t ell_d, uint32_t ell_n, uint32_t d_sc) {
+    const DevCcs& cc = *o->ccs;
     if (b != 2) return ctx->fail(NEO_ERR_UNSUPPORTED, "ccs_oracle: only b = 2 is implemented");
     if (k == 0 || k > 18) return ctx->fail(NEO_ERR_ARG, "ccs_oracle: k must be in 1..18");
     if (ell_d == 0 || ell_d > 8 || (1u << ell_d) < NEO_D) return ctx->fail(NEO_ERR_ARG, "ccs_oracle: ell_d");
     if (ell_n < 1 || ell_n > 30) return ctx->fail(NEO_ERR_ARG, "ccs_oracle: ell_n");
-    if (desc->n != desc->m || desc->n != (1u << ell_n))
+    if (cc.n != cc.m || cc.n != (1u << ell_n))
         return ctx->fail(NEO_ERR_UNSUPPORTED, "ccs_oracle: requires n == m == 2^ell_n");
-    if (!desc->is_identity[0]) return ctx->fail(NEO_ERR_ARG, "ccs_oracle: CCS must be identity-first");
-    cudaSetDevice(ctx->device);
-    auto* o = new neo_gpu_ccs_oracle();
-    std::unique_ptr<neo_gpu_ccs_oracle> guard(o);
+    if (!cc.is_identity[0]) return ctx->fail(NEO_ERR_ARG, "ccs_oracle: CCS must be identity-first");
     o->ctx = ctx;
+    o->Z = d_Z;
     o->k = k; o->b = b; o->ell_d = ell_d; o->ell_n = ell_n; o->d_sc = d_sc;
-    int rc = dev_ccs_upload(ctx, desc, o->ccs);
-    if (rc) return rc;
-    o->t = desc->t;
-    o->m = desc->m;
+    int rc = 0;
+    o->t = cc.t;
+    o->m = cc.m;
     o->n_pad = 1ULL << ell_n;
-    o->alpha = load_k(alpha, ell_d);
-    o->beta_a = load_k(beta_a, ell_d);
-    o->beta_r = load_k(beta_r, ell_n);
-    o->gamma = load_k(gamma, 1)[0];
+    o->alpha.assign(alpha, alpha + ell_d);
+    o->beta_a.assign(beta_a, beta_a + ell_d);
+    o->beta_r.assign(beta_r, beta_r + ell_n);
+    o->gamma = gamma;
     o->has_inputs = r_inputs != nullptr;
-    if (o->has_inputs) o->r_in = load_k(r_inputs, ell_n);
+    if (o->has_inputs) o->r_in.assign(r_inputs, r_inputs + ell_n);
     o->has_eval = o->has_inputs && k >= 2;
+    struct { uint32_t n, m, n_terms; const uint32_t* f_exps; const uint64_t* f_coeff; } dd{
+        cc.n, cc.m, cc.n_terms, cc.f_exps.data(), cc.f_coeff.data()};
+    const auto* desc = &dd;
 
     // compile f (oracle.rs:136-186)
     const uint32_t t = o->t;
@@ -674,8 +716,6 @@ extern "C" int neo_gpu_ccs_oracle_create(neo_gpu_ctx* ctx, const neo_ccs_desc* d
 
     const uint64_t n_pad = o->n_pad, m = o->m;
     const uint32_t nq = k * NEO_D;
-    NEO_CK(ctx, o->Z.alloc((size_t)nq * m));
-    NEO_CK(ctx, cudaMemcpyAsync(o->Z.p, Z, o->Z.bytes(), cudaMemcpyHostToDevice, ctx->stream));
 
     // small tables: [0] eq_beta_r, [1..n_fvar] f vars, then eq_rin, eval
     o->n_small = 1 + o->n_fvar;
@@ -692,13 +732,13 @@ extern "C" int neo_gpu_ccs_oracle_create(neo_gpu_ctx* ctx, const neo_ccs_desc* d
     if ((rc = launch_chi_table(ctx, dbits.p, ell_n, S))) return rc;
     DevBuf<uint64_t> z1;
     NEO_CK(ctx, z1.alloc(m));
-    z1_kernel<<<ceil_div(m, 256), 256, 0, ctx->stream>>>(o->Z.p, m, b, z1.p);
+    z1_kernel<<<ceil_div(m, 256), 256, 0, ctx->stream>>>(o->Z, m, b, z1.p);
     NEO_LAUNCHED(ctx);
     for (int v = 0; v < o->n_fvar; v++) {
         int j = o->fvar_j[v];
         spmv_fq_kernel<<<ceil_div(n_pad, 256), 256, 0, ctx->stream>>>(
-            o->ccs.csr_ptr.p + (size_t)j * (desc->n + 1), o->ccs.csr_col.p + o->ccs.nnz_off[j],
-            o->ccs.csr_val.p + o->ccs.nnz_off[j], o->ccs.is_identity[j], desc->n, desc->m, z1.p, n_pad,
+            o->ccs->csr_ptr.p + (size_t)j * (desc->n + 1), o->ccs->csr_col.p + o->ccs->nnz_off[j],
+            o->ccs->csr_val.p + o->ccs->nnz_off[j], o->ccs->is_identity[j], desc->n, desc->m, z1.p, n_pad,
             S + (size_t)(1 + v) * n_pad);
         NEO_LAUNCHED(ctx);
     }
@@ -733,16 +773,16 @@ extern "C" int neo_gpu_ccs_oracle_create(neo_gpu_ctx* ctx, const neo_ccs_desc* d
         NEO_CK(ctx, du.alloc(m));
         NEO_CK(ctx, cudaMemcpyAsync(dw.p, w.data(), nq * 16, cudaMemcpyHostToDevice, ctx->stream));
         NEO_CK(ctx, cudaMemcpyAsync(dcoef.p, coef.data(), t * 16, cudaMemcpyHostToDevice, ctx->stream));
-        eval_u_kernel<<<ceil_div(m, 256), 256, 0, ctx->stream>>>(o->Z.p, m, k, dw.p, du.p);
+        eval_u_kernel<<<ceil_div(m, 256), 256, 0, ctx->stream>>>(o->Z, m, k, dw.p, du.p);
         NEO_LAUNCHED(ctx);
         DevBuf<uint8_t> isid;
         NEO_CK(ctx, isid.alloc(t));
-        NEO_CK(ctx, cudaMemcpyAsync(isid.p, o->ccs.is_identity.data(), t, cudaMemcpyHostToDevice, ctx->stream));
+        NEO_CK(ctx, cudaMemcpyAsync(isid.p, o->ccs->is_identity.data(), t, cudaMemcpyHostToDevice, ctx->stream));
         DevBuf<uint64_t> nnzoff;
         NEO_CK(ctx, nnzoff.alloc(t + 1));
-        NEO_CK(ctx, cudaMemcpyAsync(nnzoff.p, o->ccs.nnz_off.data(), (t + 1) * 8, cudaMemcpyHostToDevice, ctx->stream));
+        NEO_CK(ctx, cudaMemcpyAsync(nnzoff.p, o->ccs->nnz_off.data(), (t + 1) * 8, cudaMemcpyHostToDevice, ctx->stream));
         eval_tbl_kernel<<<ceil_div(n_pad, 256), 256, 0, ctx->stream>>>(
-            o->ccs.csr_ptr.p, o->ccs.csr_col.p, o->ccs.csr_val.p, nnzoff.p, isid.p, t, desc->n, desc->m, du.p,
+            o->ccs->csr_ptr.p, o->ccs->csr_col.p, o->ccs->csr_val.p, nnzoff.p, isid.p, t, desc->n, desc->m, du.p,
             dcoef.p, n_pad, S + (size_t)o->idx_eval * n_pad);
         NEO_LAUNCHED(ctx);
         NEO_CK(ctx, cudaStreamSynchronize(ctx->stream));
@@ -760,7 +800,6 @@ extern "C" int neo_gpu_ccs_oracle_create(neo_gpu_ctx* ctx, const neo_ccs_desc* d
     NEO_CK(ctx, o->coeffs.alloc(MAX_DEG + 1));
     NEO_CK(ctx, o->ys.alloc(16));
     NEO_CK(ctx, cudaStreamSynchronize(ctx->stream));
-    *out = guard.release();
     return NEO_OK;
 }
 
@@ -779,7 +818,7 @@ static int row_round(neo_gpu_ccs_oracle* o) {
     a.deg_max = o->deg_max;
     a.wg = o->wg.p;
     a.nq = (int)nq;
-    a.Z = o->Z.p;
+    a.Z = o->Z;
     a.m = o->m;
     const bool last = j + 1 == o->ell_n;
     // small tables
@@ -869,7 +908,7 @@ static int ajtai_precompute(neo_gpu_ccs_oracle* o) {
     NEO_CK(ctx, cudaMemcpyAsync(dbits.p, o->row_chals.data(), o->ell_n * 16, cudaMemcpyHostToDevice, ctx->stream));
     int rc = launch_chi_table(ctx, dbits.p, o->ell_n, o->chi_r.p);
     if (rc) return rc;
-    rc = launch_me_y(ctx, o->ccs, o->Z.p, o->k, o->m, o->chi_r.p, o->ell_n, o->b, o->vj.p, o->y_eval.p, o->y_sc.p);
+    rc = launch_me_y(ctx, *o->ccs, o->Z, o->k, o->m, o->chi_r.p, o->ell_n, o->b, o->vj.p, o->y_eval.p, o->y_sc.p);
     if (rc) return rc;
     NEO_CK(ctx, cudaStreamSynchronize(ctx->stream));
     o->have_pre = true;
@@ -976,5 +1015,16 @@ extern "C" int neo_gpu_ccs_oracle_destroy(neo_gpu_ccs_oracle* o) {
     cudaSetDevice(o->ctx->device);
     cudaStreamSynchronize(o->ctx->stream);
     delete o;
+    return NEO_OK;
+}
+
+// device view of v_j = M_j^T chi_r' for the fold step (child ME claims reuse it)
+int ccs_oracle_dev_vj(neo_gpu_ccs_oracle* o, const K** vj) {
+    if (o->row_chals.size() != o->ell_n) return o->ctx->fail(NEO_ERR_ARG, "dev_vj: row phase not finished");
+    if (!o->have_pre) {
+        int rc = ajtai_precompute(o);
+        if (rc) return rc;
+    }
+    *vj = o->vj.p;
     return NEO_OK;
 }

@@ -93,16 +93,14 @@ int launch_commit(neo_gpu_ctx* ctx, const int8_t* d_digits, uint32_t n_vec, uint
     uint64_t cols_per_block = (m + n_chunks - 1) / n_chunks;
     if (cols_per_block < CHUNK_COLS) cols_per_block = CHUNK_COLS;
     n_chunks = (uint32_t)((m + cols_per_block - 1) / cols_per_block);
-    DevBuf<uint64_t> partial;
-    NEO_CK(ctx, partial.alloc((size_t)n_vec * n_chunks * kappa * 81));
+    uint64_t* partial = nullptr;
+    NEO_CK(ctx, ctx_scratch(ctx, (size_t)n_vec * n_chunks * kappa * 81 * 8, (void**)&partial));
     dim3 grid(n_chunks, kappa, n_vec);
     commit_partial_kernel<<<grid, COMMIT_THREADS, 0, ctx->stream>>>(ctx->d_pp, kappa, m, d_digits,
-                                                                     (uint32_t)cols_per_block, partial.p);
+                                                                     (uint32_t)cols_per_block, partial);
     NEO_LAUNCHED(ctx);
-    commit_reduce_kernel<<<n_vec * kappa, 96, 0, ctx->stream>>>(partial.p, n_chunks, kappa, n_vec, d_out);
+    commit_reduce_kernel<<<n_vec * kappa, 96, 0, ctx->stream>>>(partial, n_chunks, kappa, n_vec, d_out);
     NEO_LAUNCHED(ctx);
-    // partial is freed at scope exit: make sure the kernels are done with it
-    NEO_CK(ctx, cudaStreamSynchronize(ctx->stream));
     return NEO_OK;
 }
 
@@ -133,4 +131,12 @@ extern "C" int neo_gpu_commit(neo_gpu_ctx* ctx, const int8_t* digits, uint32_t n
     NEO_CK(ctx, cudaMemcpyAsync(out, dout.p, dout.bytes(), cudaMemcpyDeviceToHost, ctx->stream));
     NEO_CK(ctx, cudaStreamSynchronize(ctx->stream));
     return NEO_OK;
+}
+
+extern "C" int neo_gpu_commit_device(neo_gpu_ctx* ctx, const int8_t* d_digits, uint32_t n_vec, uint64_t m,
+                                     uint64_t* d_out) {
+    if (!ctx) return NEO_ERR_ARG;
+    if (!d_digits || !d_out || n_vec == 0 || m == 0) return ctx->fail(NEO_ERR_ARG, "commit_device: bad args");
+    cudaSetDevice(ctx->device);
+    return launch_commit(ctx, d_digits, n_vec, m, d_out);
 }

@@ -28,6 +28,7 @@ extern "C" int neo_gpu_ctx_destroy(neo_gpu_ctx* ctx) {
     cudaStreamSynchronize(ctx->stream);
     if (ctx->d_pp) cudaFree(ctx->d_pp);
     if (ctx->d_pp_limbs) cudaFree(ctx->d_pp_limbs);
+    if (ctx->scratch) cudaFree(ctx->scratch);
     cudaStreamDestroy(ctx->stream);
     delete ctx;
     return NEO_OK;
@@ -35,6 +36,17 @@ extern "C" int neo_gpu_ctx_destroy(neo_gpu_ctx* ctx) {
 
 extern "C" const char* neo_gpu_last_error(const neo_gpu_ctx* ctx) { return ctx ? ctx->err.c_str() : "null context"; }
 extern "C" uint64_t neo_gpu_kernel_launches(const neo_gpu_ctx* ctx) { return ctx ? ctx->launches : 0; }
+extern "C" int neo_gpu_ctx_stream(const neo_gpu_ctx* ctx, void** stream) {
+    if (!ctx || !stream) return NEO_ERR_ARG;
+    *stream = (void*)ctx->stream;
+    return NEO_OK;
+}
+extern "C" int neo_gpu_synchronize(neo_gpu_ctx* ctx) {
+    if (!ctx) return NEO_ERR_ARG;
+    cudaSetDevice(ctx->device);
+    NEO_CK(ctx, cudaStreamSynchronize(ctx->stream));
+    return NEO_OK;
+}
 
 // ---------------------------------------------------------------------------
 // CCS upload: CSC as given, plus a CSR copy built on the host.

@@ -22,6 +22,8 @@ struct neo_gpu_ctx {
     uint64_t pp_m = 0;
     uint64_t* d_pp = nullptr;       // [kappa][m][54] canonical u64
     uint8_t* d_pp_limbs = nullptr;  // [kappa*8][m*54] byte limbs (tensor-core layout)
+    void* scratch = nullptr;         // growable per-context scratch (stream-ordered use)
+    size_t scratch_bytes = 0;
     int fail(int code, const char* what, cudaError_t e = cudaSuccess) {
         char buf[512];
         if (e != cudaSuccess)
@@ -89,6 +91,22 @@ struct DevCcs {
     DevBuf<uint32_t> csc_row;   // [nnz]
     DevBuf<uint64_t> csc_val;   // [nnz]
 };
+// Grow-only scratch owned by the context; valid until the next call that grows it.
+inline cudaError_t ctx_scratch(neo_gpu_ctx* ctx, size_t bytes, void** p) {
+    if (bytes > ctx->scratch_bytes) {
+        if (ctx->scratch) {
+            cudaStreamSynchronize(ctx->stream);
+            cudaFree(ctx->scratch);
+            ctx->scratch = nullptr;
+            ctx->scratch_bytes = 0;
+        }
+        cudaError_t e = cudaMalloc(&ctx->scratch, bytes);
+        if (e != cudaSuccess) return e;
+        ctx->scratch_bytes = bytes;
+    }
+    *p = ctx->scratch;
+    return cudaSuccess;
+}
 int dev_ccs_upload(neo_gpu_ctx* ctx, const neo_ccs_desc* desc, DevCcs& out);
 
 // Kernels callable from several translation units.

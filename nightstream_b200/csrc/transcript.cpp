@@ -67,16 +67,37 @@ static uint64_t sample_fq(ChaCha8& rng) {
     }
 }
 
-Poseidon2W8::Poseidon2W8() {
-    ChaCha8 rng(SEED);
+void seed_from_u64(uint64_t state, uint8_t seed[32]) {
+    const uint64_t MUL = 6364136223846793005ULL, INC = 11634580027462260723ULL;
+    for (int c = 0; c < 8; c++) {
+        state = state * MUL + INC;
+        uint32_t xorshifted = (uint32_t)(((state >> 18) ^ state) >> 27);
+        uint32_t rot = (uint32_t)(state >> 59);
+        uint32_t x = (xorshifted >> rot) | (xorshifted << ((32 - rot) & 31));
+        for (int b = 0; b < 4; b++) seed[4 * c + b] = (uint8_t)(x >> (8 * b));
+    }
+}
+
+template <int W>
+Poseidon2<W>::Poseidon2(const uint8_t seed[32]) {
+    ChaCha8 rng(seed);
     for (int r = 0; r < RF; r++)
         for (int i = 0; i < W; i++) rc_ext[r][i] = sample_fq(rng);
     for (int r = 0; r < RP; r++) rc_int[r] = sample_fq(rng);
     for (int i = 0; i < W; i++) mu[i] = sample_fq(rng);
 }
 
-const Poseidon2W8& Poseidon2W8::get() {
-    static const Poseidon2W8 inst;
+const Poseidon2W8& transcript_perm() {
+    static const Poseidon2W8 inst(SEED);
+    return inst;
+}
+
+const Poseidon2W16& digest_perm() {
+    static const Poseidon2W16 inst([] {
+        static uint8_t s[32];
+        seed_from_u64(0x434353445F4D4154ULL, s);
+        return (const uint8_t*)s;
+    }());
     return inst;
 }
 
@@ -99,38 +120,43 @@ static inline void m4(uint64_t* x) {
     memcpy(x, y, sizeof y);
 }
 
-// external layer circ(2 M4, M4): y_i = M4 x_blk(i) + sum_blk M4 x_blk
+// external layer circ(2 M4, M4, ..., M4): y_blk = M4 x_blk + sum_blk' M4 x_blk'
+template <int W>
 static inline void external_layer(uint64_t* st) {
-    m4(st);
-    m4(st + 4);
+    for (int b = 0; b < W / 4; b++) m4(st + 4 * b);
     for (int i = 0; i < 4; i++) {
-        uint64_t s = gl::add(st[i], st[4 + i]);
-        st[i] = gl::add(st[i], s);
-        st[4 + i] = gl::add(st[4 + i], s);
+        uint64_t s = 0;
+        for (int b = 0; b < W / 4; b++) s = gl::add(s, st[4 * b + i]);
+        for (int b = 0; b < W / 4; b++) st[4 * b + i] = gl::add(st[4 * b + i], s);
     }
 }
 
+template <int W>
 static inline void internal_layer(uint64_t* st, const uint64_t* mu) {
     uint64_t sum = 0;
-    for (int i = 0; i < 8; i++) sum = gl::add(sum, st[i]);
-    for (int i = 0; i < 8; i++) st[i] = gl::add(sum, gl::mul(mu[i], st[i]));
+    for (int i = 0; i < W; i++) sum = gl::add(sum, st[i]);
+    for (int i = 0; i < W; i++) st[i] = gl::add(sum, gl::mul(mu[i], st[i]));
 }
 
-void Poseidon2W8::permute(uint64_t st[W]) const {
-    external_layer(st);
+template <int W>
+void Poseidon2<W>::permute(uint64_t* st) const {
+    external_layer<W>(st);
     for (int r = 0; r < RF / 2; r++) {
         for (int i = 0; i < W; i++) st[i] = sbox7(gl::add(st[i], rc_ext[r][i]));
-        external_layer(st);
+        external_layer<W>(st);
     }
     for (int r = 0; r < RP; r++) {
         st[0] = sbox7(gl::add(st[0], rc_int[r]));
-        internal_layer(st, mu);
+        internal_layer<W>(st, mu);
     }
     for (int r = RF / 2; r < RF; r++) {
         for (int i = 0; i < W; i++) st[i] = sbox7(gl::add(st[i], rc_ext[r][i]));
-        external_layer(st);
+        external_layer<W>(st);
     }
 }
+
+template struct Poseidon2<8>;
+template struct Poseidon2<16>;
 
 // -------------------------------------------------------------- transcript --
 static const char* APP_DOMAIN = "neo/transcript/v1|poseidon2-goldilocks-w8-r4";
@@ -141,7 +167,7 @@ Transcript::Transcript(const std::string& app_label) {
 }
 
 void Transcript::permute() {
-    Poseidon2W8::get().permute(st_);
+    transcript_perm().permute(st_);
     absorbed_ = 0;
     perms_++;
 }

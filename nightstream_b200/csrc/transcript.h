@@ -37,15 +37,26 @@ struct ChaCha8 {
     void refill();
 };
 
-struct Poseidon2W8 {
-    static constexpr int W = 8, RF = 8, RP = 22;
+// rand_core's documented seed_from_u64 expansion: a PCG32 (XSH-RR) stream
+// fills the 32-byte seed 4 bytes at a time.
+void seed_from_u64(uint64_t state, uint8_t seed[32]);
+
+// Poseidon2 over Goldilocks with width W in {8, 16}.
+template <int W>
+struct Poseidon2 {
+    static constexpr int RF = 8, RP = 22;
     uint64_t rc_ext[RF][W];
     uint64_t rc_int[RP];
     uint64_t mu[W];  // internal diagonal: M_I x = sum(x) + mu_i * x_i
-    Poseidon2W8();
-    void permute(uint64_t st[W]) const;
-    static const Poseidon2W8& get();
+    explicit Poseidon2(const uint8_t seed[32]);
+    void permute(uint64_t* st) const;
 };
+using Poseidon2W8 = Poseidon2<8>;
+using Poseidon2W16 = Poseidon2<16>;
+// the transcript permutation (seeded with the reference SEED)
+const Poseidon2W8& transcript_perm();
+// the CCS-digest permutation (ChaCha8Rng::seed_from_u64(0x434353445F4D4154))
+const Poseidon2W16& digest_perm();
 
 class Transcript {
    public:

@@ -41,6 +41,26 @@ SIGNATURES = {
     "neo_gpu_ccs_oracle_degree_bound": [P],
     "neo_gpu_ccs_oracle_me_outputs": [P, P, P],
     "neo_gpu_ccs_oracle_destroy": [P],
+    "neo_gpu_ctx_stream": [P, P],
+    "neo_gpu_synchronize": [P],
+    "neo_gpu_commit_device": [P, ctypes.c_void_p, U32, U64, ctypes.c_void_p],
+    "neo_gpu_shard_step_stats": [P, P, U32],
+    "neo_gpu_shard_create": [P, P, U32, U32, ctypes.c_char_p, P],
+    "neo_gpu_shard_fold_step": [P, P, P, U64, P],
+    "neo_gpu_shard_fold_step_device": [P, ctypes.c_void_p, P],
+    "neo_gpu_shard_transcript_state": [P, P],
+    "neo_gpu_shard_ccs_digest": [P, P],
+    "neo_gpu_shard_destroy": [P],
+    "neo_transcript_new": [ctypes.c_char_p, P],
+    "neo_transcript_append_message": [P, ctypes.c_char_p, P, ctypes.c_size_t],
+    "neo_transcript_append_fields": [P, ctypes.c_char_p, P, ctypes.c_size_t],
+    "neo_transcript_append_u64s": [P, ctypes.c_char_p, P, ctypes.c_size_t],
+    "neo_transcript_challenge_field": [P, ctypes.c_char_p, P],
+    "neo_transcript_challenge_fields": [P, ctypes.c_char_p, ctypes.c_size_t, P],
+    "neo_transcript_digest32": [P, P],
+    "neo_transcript_state": [P, P],
+    "neo_transcript_destroy": [P],
+    "neo_ccs_digest": [P, P],
 }
 _RESTYPES = {
     "neo_gpu_last_error": ctypes.c_char_p,
@@ -103,6 +123,18 @@ class Context:
     @property
     def kernel_launches(self) -> int:
         return int(self.lib.neo_gpu_kernel_launches(self.h))
+
+    @property
+    def stream(self) -> int:
+        s = ctypes.c_void_p()
+        self.check(self.lib.neo_gpu_ctx_stream(self.h, ctypes.byref(s)))
+        return s.value or 0
+
+    def synchronize(self):
+        self.check(self.lib.neo_gpu_synchronize(self.h))
+
+    def commit_device(self, d_digits: int, n_vec: int, m: int, d_out: int):
+        self.check(self.lib.neo_gpu_commit_device(self.h, ctypes.c_void_p(d_digits), n_vec, m, ctypes.c_void_p(d_out)))
 
     def close(self):
         if getattr(self, "h", None):
@@ -213,3 +245,115 @@ class GpuCcsOracle:
 
     def __del__(self):
         self.close()
+
+
+class Shard:
+    """Shard prover with a device-resident accumulator (neo_gpu_shard)."""
+
+    def __init__(self, ctx: Context, ccs, m_in: int = 1, k_rho: int = 12, app_label: bytes = b"neo/shard"):
+        self.ctx = ctx
+        self._desc = ccs.desc()
+        h = ctypes.c_void_p()
+        ctx.check(ctx.lib.neo_gpu_shard_create(ctx.h, ctypes.byref(self._desc), m_in, k_rho, app_label,
+                                               ctypes.byref(h)))
+        self.h = h
+        self._cap = 0
+
+    def fold_step(self, z: np.ndarray) -> np.ndarray:
+        """One fold step; returns the canonical step-proof words."""
+        z = _u64(z)
+        n = ctypes.c_uint64()
+        if self._cap == 0:
+            self._cap = 1 << 20
+        out = np.empty(self._cap, np.uint64)
+        self.ctx.check(self.ctx.lib.neo_gpu_shard_fold_step(self.h, _p(z), _p(out), self._cap, ctypes.byref(n)))
+        return out[: n.value].copy()
+
+    def fold_step_device(self, d_z_ptr: int) -> int:
+        n = ctypes.c_uint64()
+        self.ctx.check(self.ctx.lib.neo_gpu_shard_fold_step_device(self.h, ctypes.c_void_p(d_z_ptr), ctypes.byref(n)))
+        return n.value
+
+    STAT_NAMES = ["total", "witness", "bind", "ccs_build", "time_rounds", "ajtai_rounds", "me_outputs", "rlc",
+                  "dec", "transcript_perms"]
+
+    def step_stats(self) -> dict:
+        out = np.zeros(12, np.float64)
+        self.ctx.check(self.ctx.lib.neo_gpu_shard_step_stats(self.h, _p(out), 12))
+        return {k: float(v) for k, v in zip(self.STAT_NAMES, out)}
+
+    def transcript_state(self) -> np.ndarray:
+        st = np.empty(8, np.uint64)
+        self.ctx.check(self.ctx.lib.neo_gpu_shard_transcript_state(self.h, _p(st)))
+        return st
+
+    def ccs_digest(self) -> np.ndarray:
+        d = np.empty(4, np.uint64)
+        self.ctx.check(self.ctx.lib.neo_gpu_shard_ccs_digest(self.h, _p(d)))
+        return d
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.ctx.lib.neo_gpu_shard_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
+
+
+class HostTranscript:
+    """The library's host transcript (neo_transcript_*), usable without a GPU."""
+
+    def __init__(self, app_label: bytes):
+        self.lib = load()
+        h = ctypes.c_void_p()
+        rc = self.lib.neo_transcript_new(app_label, ctypes.byref(h))
+        if rc:
+            raise NeoGpuError(rc, "transcript")
+        self.h = h
+
+    def append_message(self, label: bytes, msg: bytes = b""):
+        buf = ctypes.create_string_buffer(msg, len(msg)) if msg else None
+        self.lib.neo_transcript_append_message(self.h, label, buf, len(msg))
+
+    def append_fields(self, label: bytes, fs):
+        fs = _u64(np.asarray(fs, dtype=np.uint64).reshape(-1))
+        self.lib.neo_transcript_append_fields(self.h, label, _p(fs) if fs.size else None, fs.size)
+
+    def append_u64s(self, label: bytes, us):
+        us = _u64(us)
+        self.lib.neo_transcript_append_u64s(self.h, label, _p(us), us.size)
+
+    def challenge_field(self, label: bytes) -> int:
+        out = ctypes.c_uint64()
+        self.lib.neo_transcript_challenge_field(self.h, label, ctypes.byref(out))
+        return out.value
+
+    def challenge_fields(self, label: bytes, n: int):
+        out = np.empty(n, np.uint64)
+        self.lib.neo_transcript_challenge_fields(self.h, label, n, _p(out))
+        return out
+
+    def digest32(self) -> bytes:
+        out = np.empty(32, np.uint8)
+        self.lib.neo_transcript_digest32(self.h, _p(out))
+        return out.tobytes()
+
+    def state(self):
+        st = np.empty(8, np.uint64)
+        self.lib.neo_transcript_state(self.h, _p(st))
+        return st
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            self.lib.neo_transcript_destroy(self.h)
+            self.h = None
+
+
+def ccs_digest(ccs) -> np.ndarray:
+    d = np.empty(4, np.uint64)
+    desc = ccs.desc()
+    rc = load().neo_ccs_digest(ctypes.byref(desc), _p(d))
+    if rc:
+        raise NeoGpuError(rc, "ccs digest")
+    return d

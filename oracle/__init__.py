@@ -55,12 +55,26 @@ def lib():
             "or_q_sum_hypercube": [P, P, I, I, P, P, P, P, P, I, I, P],
             "or_q_eval_ext": [P, P, I, I, P, P, P, P, P, I, I, P, P, P],
             "or_me_y_at_r": [P, P, I, P, I, P, P],
+            "or_poseidon2_permute": [P],
+            "or_poseidon2_w16_permute": [P],
+            "or_ccs_digest": [P, P],
+            "or_tr_new": [ctypes.c_char_p],
+            "or_tr_free": [P],
+            "or_tr_append_message": [P, ctypes.c_char_p, P, SZ],
+            "or_tr_append_fields": [P, ctypes.c_char_p, P, SZ],
+            "or_tr_append_u64s": [P, ctypes.c_char_p, P, SZ],
+            "or_tr_challenge_field": [P, ctypes.c_char_p],
+            "or_tr_challenge_fields": [P, ctypes.c_char_p, SZ, P],
+            "or_tr_digest32": [P, P],
+            "or_tr_state": [P, P],
         }
         for name, args in sigs.items():
             fn = getattr(L, name)
             fn.argtypes = args
             fn.restype = I if name in ("or_split_b", "or_ccs_oracle_num_rounds", "or_ccs_sumcheck_fixed") else None
         L.or_ccs_oracle_new.restype = P
+        L.or_tr_new.restype = P
+        L.or_tr_challenge_field.restype = ctypes.c_uint64
         _lib = L
     return _lib
 
@@ -250,3 +264,52 @@ def me_y_at_r(ccs, Z, ell_n, r, b=2):
     ys = np.empty((ccs.t, 2), np.uint64)
     lib().or_me_y_at_r(ctypes.byref(desc), ptr(Z), ell_n, ptr(u64(r)), b, ptr(y), ptr(ys))
     return y, ys
+
+
+class Transcript:
+    """Poseidon2 sponge transcript restatement (neo-transcript/src/poseidon2.rs)."""
+
+    def __init__(self, app_label: bytes):
+        self.h = lib().or_tr_new(app_label)
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            lib().or_tr_free(self.h)
+            self.h = None
+
+    def append_message(self, label: bytes, msg: bytes = b""):
+        buf = np.frombuffer(msg, dtype=np.uint8) if msg else np.zeros(1, np.uint8)
+        lib().or_tr_append_message(self.h, label, buf.ctypes.data, len(msg))
+
+    def append_fields(self, label: bytes, fs):
+        fs = np.ascontiguousarray(np.asarray(fs, dtype=np.uint64).reshape(-1))
+        lib().or_tr_append_fields(self.h, label, fs.ctypes.data if fs.size else None, fs.size)
+
+    def append_u64s(self, label: bytes, us):
+        us = u64(us)
+        lib().or_tr_append_u64s(self.h, label, us.ctypes.data, us.size)
+
+    def challenge_field(self, label: bytes) -> int:
+        return int(lib().or_tr_challenge_field(self.h, label))
+
+    def challenge_fields(self, label: bytes, n: int):
+        out = np.empty(n, np.uint64)
+        lib().or_tr_challenge_fields(self.h, label, n, out.ctypes.data)
+        return out
+
+    def digest32(self) -> bytes:
+        out = np.empty(32, np.uint8)
+        lib().or_tr_digest32(self.h, out.ctypes.data)
+        return out.tobytes()
+
+    def state(self):
+        out = np.empty(8, np.uint64)
+        lib().or_tr_state(self.h, out.ctypes.data)
+        return out
+
+
+def ccs_digest(ccs):
+    desc = ccs.desc()
+    out = np.empty(4, np.uint64)
+    lib().or_ccs_digest(ctypes.byref(desc), out.ctypes.data)
+    return out

@@ -604,60 +604,80 @@ static void poly_mul_affine(kq* poly, int len, kq a, kq b) {
     }
 }
 
-/* evals_row_phase_impl, b=2 generic K path (oracle.rs:1047-1178) */
-static void evals_row_phase(or_ccs_oracle* o, const kq* xs, int nx, kq* ys) {
+/* evals_row_phase_impl, b=2 generic K path (oracle.rs:1047-1178); the pair
+   loop is split across threads like the reference's rayon fold/reduce
+   (oracle.rs:542-658), exact arithmetic makes the split invisible. */
+static void row_pair_accum(or_ccs_oracle* o, size_t t, kq* coeffs) {
     const or_ccs* s = o->s;
-    size_t tail = o->cur_len / 2;
     size_t L = o->cur_len;
     int dm = o->deg_max;
-    kq coeffs[16], inner[16], tp[16];
+    kq inner[16], tp[16];
     kq three = kfq(3);
+    kq e0 = o->eq_beta_r[2 * t];
+    kq e1 = ksub(o->eq_beta_r[2 * t + 1], e0);
+    for (int i = 0; i <= dm; i++) inner[i] = K0;
+    for (uint32_t tt = 0; tt < s->n_terms; tt++) {
+        for (int i = 0; i <= dm; i++) tp[i] = K0;
+        tp[0] = kfq(s->f_coeff[tt]);
+        for (int v = 0; v < o->n_fvar; v++) {
+            uint32_t e = s->f_exps[tt * s->t + o->fvar_j[v]];
+            if (!e) continue;
+            kq a = o->fvar[v][2 * t];
+            kq bb = ksub(o->fvar[v][2 * t + 1], a);
+            for (uint32_t q = 0; q < e; q++) poly_mul_affine(tp, dm + 1, a, bb);
+        }
+        for (int i = 0; i <= dm; i++) inner[i] = kadd(inner[i], tp[i]);
+    }
+    for (int w = 0; w < o->k; w++) {
+        const kq* lo = o->nc + ((size_t)w * L + 2 * t) * D;
+        const kq* hi = lo + D;
+        for (int rho = 0; rho < D; rho++) {
+            kq wg = o->wg[w * D + rho];
+            kq a = lo[rho];
+            kq bb = ksub(hi[rho], a);
+            kq a2 = kmul(a, a), a3 = kmul(a2, a), b2 = kmul(bb, bb), b3 = kmul(b2, bb);
+            kq t0 = ksub(a3, a);
+            kq t1 = ksub(kmul(kmul(a2, bb), three), bb);
+            kq t2 = kmul(kmul(a, b2), three);
+            kq t3 = b3;
+            inner[0] = kadd(inner[0], kmul(wg, t0));
+            inner[1] = kadd(inner[1], kmul(wg, t1));
+            inner[2] = kadd(inner[2], kmul(wg, t2));
+            inner[3] = kadd(inner[3], kmul(wg, t3));
+        }
+    }
+    coeffs[0] = kadd(coeffs[0], kmul(e0, inner[0]));
+    for (int d = 1; d <= dm; d++)
+        coeffs[d] = kadd(coeffs[d], kadd(kmul(e0, inner[d]), kmul(e1, inner[d - 1])));
+    if (o->eq_rin && o->eval_tbl) {
+        kq r0 = o->eq_rin[2 * t], r1 = ksub(o->eq_rin[2 * t + 1], r0);
+        kq v0 = o->eval_tbl[2 * t], v1 = ksub(o->eval_tbl[2 * t + 1], v0);
+        kq g = o->gamma_to_k;
+        coeffs[0] = kadd(coeffs[0], kmul(g, kmul(r0, v0)));
+        coeffs[1] = kadd(coeffs[1], kmul(g, kadd(kmul(r0, v1), kmul(r1, v0))));
+        coeffs[2] = kadd(coeffs[2], kmul(g, kmul(r1, v1)));
+    }
+}
+
+static void evals_row_phase(or_ccs_oracle* o, const kq* xs, int nx, kq* ys) {
+    size_t tail = o->cur_len / 2;
+    int dm = o->deg_max;
+    kq coeffs[16];
     for (int i = 0; i <= dm; i++) coeffs[i] = K0;
-    for (size_t t = 0; t < tail; t++) {
-        kq e0 = o->eq_beta_r[2 * t];
-        kq e1 = ksub(o->eq_beta_r[2 * t + 1], e0);
-        for (int i = 0; i <= dm; i++) inner[i] = K0;
-        for (uint32_t tt = 0; tt < s->n_terms; tt++) {
-            for (int i = 0; i <= dm; i++) tp[i] = K0;
-            tp[0] = kfq(s->f_coeff[tt]);
-            for (int v = 0; v < o->n_fvar; v++) {
-                uint32_t e = s->f_exps[tt * s->t + o->fvar_j[v]];
-                if (!e) continue;
-                kq a = o->fvar[v][2 * t];
-                kq bb = ksub(o->fvar[v][2 * t + 1], a);
-                for (uint32_t q = 0; q < e; q++) poly_mul_affine(tp, dm + 1, a, bb);
-            }
-            for (int i = 0; i <= dm; i++) inner[i] = kadd(inner[i], tp[i]);
-        }
-        for (int w = 0; w < o->k; w++) {
-            const kq* lo = o->nc + ((size_t)w * L + 2 * t) * D;
-            const kq* hi = lo + D;
-            for (int rho = 0; rho < D; rho++) {
-                kq wg = o->wg[w * D + rho];
-                kq a = lo[rho];
-                kq bb = ksub(hi[rho], a);
-                kq a2 = kmul(a, a), a3 = kmul(a2, a), b2 = kmul(bb, bb), b3 = kmul(b2, bb);
-                kq t0 = ksub(a3, a);
-                kq t1 = ksub(kmul(kmul(a2, bb), three), bb);
-                kq t2 = kmul(kmul(a, b2), three);
-                kq t3 = b3;
-                inner[0] = kadd(inner[0], kmul(wg, t0));
-                inner[1] = kadd(inner[1], kmul(wg, t1));
-                inner[2] = kadd(inner[2], kmul(wg, t2));
-                inner[3] = kadd(inner[3], kmul(wg, t3));
-            }
-        }
-        coeffs[0] = kadd(coeffs[0], kmul(e0, inner[0]));
-        for (int d = 1; d <= dm; d++)
-            coeffs[d] = kadd(coeffs[d], kadd(kmul(e0, inner[d]), kmul(e1, inner[d - 1])));
-        if (o->eq_rin && o->eval_tbl) {
-            kq r0 = o->eq_rin[2 * t], r1 = ksub(o->eq_rin[2 * t + 1], r0);
-            kq v0 = o->eval_tbl[2 * t], v1 = ksub(o->eval_tbl[2 * t + 1], v0);
-            kq g = o->gamma_to_k;
-            coeffs[0] = kadd(coeffs[0], kmul(g, kmul(r0, v0)));
-            coeffs[1] = kadd(coeffs[1], kmul(g, kadd(kmul(r0, v1), kmul(r1, v0))));
-            coeffs[2] = kadd(coeffs[2], kmul(g, kmul(r1, v1)));
-        }
+#ifdef _OPENMP
+#pragma omp parallel if (tail >= 1024)
+#endif
+    {
+        kq local[16];
+        for (int i = 0; i <= dm; i++) local[i] = K0;
+#ifdef _OPENMP
+#pragma omp for schedule(static)
+#endif
+        for (size_t t = 0; t < tail; t++) row_pair_accum(o, t, local);
+#ifdef _OPENMP
+#pragma omp critical
+#endif
+        for (int i = 0; i <= dm; i++) coeffs[i] = kadd(coeffs[i], local[i]);
     }
     for (int i = 0; i < nx; i++) ys[i] = poly_eval(coeffs, dm + 1, xs[i]);
 }
@@ -676,6 +696,11 @@ static void row_fold(or_ccs_oracle* o, kq r) {
     for (int w = 0; w < o->k; w++) {
         kq* base = o->nc + (size_t)w * L * D;          /* old layout stride L */
         kq* dst = o->nc + (size_t)w * half * D;        /* compact to stride half */
+        /* w == 0 folds in place front to back: element i reads 2i, 2i+1 >= i,
+           so only a serial loop is safe there; w >= 1 writes below its source */
+#ifdef _OPENMP
+#pragma omp parallel for schedule(static) if (w > 0 && half >= 4096)
+#endif
         for (size_t i = 0; i < half; i++)
             for (int rho = 0; rho < D; rho++) {
                 kq lo = base[(2 * i) * D + rho], hi = base[(2 * i + 1) * D + rho];
@@ -706,6 +731,9 @@ static void precompute_for_r(or_ccs_oracle* o) {
     o->f_prime = f_eval(s, mv);
     o->y_nc = (kq*)calloc((size_t)k * D, sizeof(kq));
     o->y_eval = (kq*)calloc((size_t)k * t * D, sizeof(kq));
+#ifdef _OPENMP
+#pragma omp parallel for collapse(3) schedule(dynamic)
+#endif
     for (int i = 0; i < k; i++) {
         for (int j = 0; j < t; j++) {
             for (int rho = 0; rho < D; rho++) {
@@ -719,9 +747,9 @@ static void precompute_for_r(or_ccs_oracle* o) {
                 o->y_eval[((size_t)i * t + j) * D + rho] = acc;
             }
         }
-        /* NC uses v_1 = chi_r restricted (matrix 0 is the identity) */
-        memcpy(o->y_nc + (size_t)i * D, o->y_eval + ((size_t)i * t + 0) * D, sizeof(kq) * D);
     }
+    /* NC uses v_1 = chi_r restricted (matrix 0 is the identity) */
+    for (int i = 0; i < k; i++) memcpy(o->y_nc + (size_t)i * D, o->y_eval + ((size_t)i * t + 0) * D, sizeof(kq) * D);
     free(vj); free(chi_r);
     o->have_pre = 1;
 }
@@ -1018,14 +1046,17 @@ void or_me_y_at_r(const or_ccs* s, const int8_t* Z, int ell_n, const uint64_t* r
     for (int q = 1; q < D; q++) pw[q] = fq_mul(pw[q - 1], (uint64_t)b);
     for (int j = 0; j < t; j++) {
         ccs_matTvec(s, j, chi, (size_t)1 << ell_n, vj);
-        kq sc = K0;
+#ifdef _OPENMP
+#pragma omp parallel for schedule(static) if (m >= 4096)
+#endif
         for (int rho = 0; rho < D; rho++) {
             kq acc = K0;
             const int8_t* zr = Z + (size_t)rho * m;
             for (size_t c = 0; c < m; c++) if (zr[c]) acc = kadd(acc, kscale(vj[c], fq_from_i64(zr[c])));
             kstore(y + 2 * ((size_t)j * D + rho), acc);
-            sc = kadd(sc, kscale(acc, pw[rho]));
         }
+        kq sc = K0;
+        for (int rho = 0; rho < D; rho++) sc = kadd(sc, kscale(kload(y + 2 * ((size_t)j * D + rho)), pw[rho]));
         kstore(y_scalars + 2 * j, sc);
     }
     free(chi); free(vj);
@@ -1165,3 +1196,113 @@ void or_tr_digest32(or_transcript* t, uint8_t* out) {
     for (int i = 0; i < 4; i++) for (int b = 0; b < 8; b++) out[8*i + b] = (uint8_t)(t->st[i] >> (8*b));
 }
 void or_tr_state(const or_transcript* t, uint64_t* out) { memcpy(out, t->st, 64); }
+
+/* Width-16 Poseidon2 for the CCS matrix digest (engines/utils.rs:214-321):
+   constants from ChaCha8 seeded by rand_core's seed_from_u64 (PCG32 XSH-RR
+   expansion) of 0x434353445F4D4154.  Parity unpinned. */
+static uint64_t P16_RCE[8][16], P16_RCI[22], P16_MU[16];
+static int p16_ready = 0;
+static void p16_init(void) {
+    if (p16_ready) return;
+    uint8_t seed[32];
+    uint64_t state = 0x434353445F4D4154ULL;
+    for (int c = 0; c < 8; c++) {
+        state = state * 6364136223846793005ULL + 11634580027462260723ULL;
+        uint32_t xs = (uint32_t)(((state >> 18) ^ state) >> 27);
+        uint32_t rot = (uint32_t)(state >> 59);
+        uint32_t x = (xs >> rot) | (xs << ((32 - rot) & 31));
+        for (int b = 0; b < 4; b++) seed[4 * c + b] = (uint8_t)(x >> (8 * b));
+    }
+    or_chacha c;
+    for (int i = 0; i < 8; i++)
+        c.key[i] = (uint32_t)seed[4*i] | ((uint32_t)seed[4*i+1] << 8) | ((uint32_t)seed[4*i+2] << 16) | ((uint32_t)seed[4*i+3] << 24);
+    c.ctr = 0; c.idx = 16;
+    uint64_t* outs[3] = {&P16_RCE[0][0], P16_RCI, P16_MU};
+    int lens[3] = {128, 22, 16};
+    for (int g = 0; g < 3; g++)
+        for (int i = 0; i < lens[g]; i++) {
+            uint64_t x;
+            do { x = cc_u64(&c); } while (x >= Q);
+            outs[g][i] = x;
+        }
+    p16_ready = 1;
+}
+static void p16_ext(uint64_t* st) {
+    static const uint64_t M[4][4] = {{5,7,1,3},{4,6,1,1},{1,3,5,7},{1,1,4,6}};
+    uint64_t y[16];
+    for (int b = 0; b < 4; b++)
+        for (int r = 0; r < 4; r++) {
+            uint64_t a = 0;
+            for (int cc = 0; cc < 4; cc++) a = fq_add(a, fq_mul(M[r][cc], st[4*b + cc]));
+            y[4*b + r] = a;
+        }
+    for (int i = 0; i < 4; i++) {
+        uint64_t s = 0;
+        for (int b = 0; b < 4; b++) s = fq_add(s, y[4*b + i]);
+        for (int b = 0; b < 4; b++) st[4*b + i] = fq_add(y[4*b + i], s);
+    }
+}
+void or_poseidon2_w16_permute(uint64_t* st) {
+    p16_init();
+    p16_ext(st);
+    for (int r = 0; r < 4; r++) { for (int i = 0; i < 16; i++) st[i] = p2_s7(fq_add(st[i], P16_RCE[r][i])); p16_ext(st); }
+    for (int r = 0; r < 22; r++) {
+        st[0] = p2_s7(fq_add(st[0], P16_RCI[r]));
+        uint64_t s = 0;
+        for (int i = 0; i < 16; i++) s = fq_add(s, st[i]);
+        for (int i = 0; i < 16; i++) st[i] = fq_add(s, fq_mul(P16_MU[i], st[i]));
+    }
+    for (int r = 4; r < 8; r++) { for (int i = 0; i < 16; i++) st[i] = p2_s7(fq_add(st[i], P16_RCE[r][i])); p16_ext(st); }
+}
+
+/* digest_ccs_matrices (engines/utils.rs:214-321): dense row-major scan of
+   nonzeros, emitted as (row, col, val) triples into a width-16 state. */
+void or_ccs_digest(const or_ccs* s, uint64_t* out4) {
+    uint64_t st[16] = {0};
+    int ab = 0;
+    const char* dom = "neo/ccs/matrices/v1";
+    for (const char* p = dom; *p; p++) { if (ab >= 15) { or_poseidon2_w16_permute(st); ab = 0; } st[ab++] = (uint8_t)*p; }
+    if (ab + 3 >= 16) { or_poseidon2_w16_permute(st); ab = 0; }
+    st[ab] = s->n; st[ab + 1] = s->m; st[ab + 2] = s->t;
+    or_poseidon2_w16_permute(st);
+    for (uint32_t j = 0; j < s->t; j++) {
+        ab = 0;
+        st[ab++] = j;
+        for (uint32_t row = 0; row < s->n; row++) {
+            if (s->is_identity[j]) {
+                if (ab + 3 > 15) { or_poseidon2_w16_permute(st); ab = 0; }
+                st[ab] = row; st[ab + 1] = row; st[ab + 2] = 1; ab += 3;
+                continue;
+            }
+            /* columns ascending within the row: scan the row's entries */
+            const uint64_t* cp = s->col_ptr + (size_t)j * (s->m + 1);
+            const uint32_t* ri = s->row_idx + s->nnz_off[j];
+            const uint64_t* vv = s->vals + s->nnz_off[j];
+            (void)cp; (void)ri; (void)vv;
+        }
+        if (!s->is_identity[j]) {
+            /* build row lists (O(nnz)) */
+            const uint64_t* cp = s->col_ptr + (size_t)j * (s->m + 1);
+            const uint32_t* ri = s->row_idx + s->nnz_off[j];
+            const uint64_t* vv = s->vals + s->nnz_off[j];
+            uint64_t nnz = s->nnz_off[j + 1] - s->nnz_off[j];
+            uint64_t* cnt = (uint64_t*)calloc(s->n + 1, 8);
+            for (uint64_t k = 0; k < nnz; k++) cnt[ri[k] + 1]++;
+            for (uint32_t r = 0; r < s->n; r++) cnt[r + 1] += cnt[r];
+            uint64_t* pos = (uint64_t*)malloc(8 * (s->n + 1));
+            memcpy(pos, cnt, 8 * (s->n + 1));
+            uint64_t* ec = (uint64_t*)malloc(8 * (nnz ? nnz : 1));
+            uint64_t* ev = (uint64_t*)malloc(8 * (nnz ? nnz : 1));
+            for (uint32_t c = 0; c < s->m; c++)
+                for (uint64_t k = cp[c]; k < cp[c + 1]; k++) { uint64_t p = pos[ri[k]]++; ec[p] = c; ev[p] = vv[k]; }
+            for (uint32_t r = 0; r < s->n; r++)
+                for (uint64_t e = cnt[r]; e < cnt[r + 1]; e++) {
+                    if (ab + 3 > 15) { or_poseidon2_w16_permute(st); ab = 0; }
+                    st[ab] = r; st[ab + 1] = ec[e]; st[ab + 2] = fq_canon(ev[e]); ab += 3;
+                }
+            free(cnt); free(pos); free(ec); free(ev);
+        }
+        or_poseidon2_w16_permute(st);
+    }
+    memcpy(out4, st, 32);
+}

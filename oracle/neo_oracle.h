@@ -117,6 +117,8 @@ uint64_t or_tr_challenge_field(or_transcript* t, const char* label);
 void or_tr_challenge_fields(or_transcript* t, const char* label, size_t n, uint64_t* out);
 void or_tr_digest32(or_transcript* t, uint8_t* out);
 void or_tr_state(const or_transcript* t, uint64_t* out);
+void or_poseidon2_w16_permute(uint64_t* st);
+void or_ccs_digest(const or_ccs* s, uint64_t* out4);
 
 #ifdef __cplusplus
 }

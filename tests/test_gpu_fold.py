@@ -1,0 +1,41 @@
+"""Whole fold steps through the C ABI (neo_gpu_shard_fold_step) against the
+oracle's fold-step restatement: every proof word and the transcript state must
+be identical, for the first step (k = 1) and steady-state steps (k = 13)."""
+import numpy as np
+import pytest
+
+from oracle.fold import OracleShard
+from nightstream_b200 import gpu, synth
+
+Q = (1 << 64) - (1 << 32) + 1
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize("ell,steps", [(6, 3), (10, 3)])
+def test_fold_steps_match_oracle(ctx, ell, steps):
+    ccs, z = synth.make_r1cs(ell, 21)
+    pp = np.random.default_rng(ell).integers(0, Q, size=(16, 1 << ell, 54), dtype=np.uint64)
+    ctx.pp_upload(pp)
+    g = gpu.Shard(ctx, ccs, m_in=1, k_rho=12, app_label=b"neo/test-shard")
+    o = OracleShard(ccs, pp, m_in=1, k_rho=12, app_label=b"neo/test-shard")
+    assert np.array_equal(g.ccs_digest(), o.digest)
+    for s in range(steps):
+        pg = g.fold_step(z)
+        po = o.fold_step(z)
+        assert pg.shape == po.shape, f"step {s}: proof length"
+        assert np.array_equal(pg, po), f"step {s}: first mismatch at word {int(np.argmax(pg != po))}"
+        assert np.array_equal(g.transcript_state(), o.tr.state()), f"step {s}: transcript state"
+    g.close()
+
+
+def test_fold_step_rejects_unsatisfied_witness(ctx):
+    ccs, z = synth.make_r1cs(6, 22)
+    pp = np.random.default_rng(1).integers(0, Q, size=(16, 64, 54), dtype=np.uint64)
+    ctx.pp_upload(pp)
+    g = gpu.Shard(ctx, ccs)
+    bad = z.copy()
+    bad[3] = (int(bad[3]) + 1) % Q
+    with pytest.raises(gpu.NeoGpuError) as e:
+        g.fold_step(bad)
+    assert e.value.code == 3  # NEO_ERR_INVARIANT: sum-check p(0)+p(1) check
+    g.close()
