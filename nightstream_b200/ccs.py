@@ -7,7 +7,7 @@ sentinel or CSC (crates/neo-ccs/src/sparse.rs:19, 151-191), and
 identity-first, matrices [I, A, B, C] and f = X1*X2 - X3.
 """
 import ctypes
-from dataclasses import dataclass, field
+from dataclasses import dataclass
 from typing import List, Optional, Tuple
 
 import numpy as np
@@ -73,7 +73,6 @@ class CcsStructure:
     m: int
     matrices: List[Optional[CscMatrix]]          # None = identity sentinel
     f_terms: List[Tuple[int, List[int]]]         # (coeff mod q, exps[t])
-    _keep: list = field(default_factory=list, repr=False)
 
     @property
     def t(self) -> int:
@@ -103,8 +102,8 @@ class CcsStructure:
         f_coeff = np.array([c % Q for c, _ in self.f_terms], dtype=np.uint64)
         f_exps = np.array([e for _, e in self.f_terms], dtype=np.uint32).reshape(-1)
         keep = [is_id, col_ptr, nnz_off, row_idx, vv, f_coeff, f_exps]
-        self._keep = keep
         d = CcsDesc()
+        d._keep = keep  # the struct owns the arrays it points to
         d.n, d.m, d.t = self.n, self.m, t
         d.is_identity = is_id.ctypes.data
         d.col_ptr = col_ptr.ctypes.data

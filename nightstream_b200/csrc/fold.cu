@@ -144,11 +144,17 @@ static void header_params(neo_gpu_shard* sh) {
         while (x) { b++; x >>= 1; }
         return b;
     };
+    const unsigned __int128 ld = (unsigned __int128)ell * sh->d_sc;
+    const unsigned __int128 U128_MAX = ~(unsigned __int128)0;
     for (uint32_t lam = 127; lam >= 96; lam--) {
-        unsigned __int128 rhs = ((unsigned __int128)1 << lam) * (unsigned __int128)(ell * sh->d_sc);
+        // rhs = 2^lam * ell * d_sc; an overflow means s = 2 is unsupported (checked_shl/checked_mul)
+        unsigned __int128 p2 = (unsigned __int128)1 << lam;
+        if (ld != 0 && p2 > U128_MAX / ld) continue;
+        unsigned __int128 rhs = p2 * ld;
         if (q2 < rhs) continue;
         int slack = bitlen(q2) - bitlen(rhs);
-        if (q2 < (rhs << slack)) slack -= 1;
+        // rhs.checked_shl(slack): shift only when the result stays below 2^128
+        if (slack < 128 && bitlen(rhs) + slack <= 128 && q2 < (rhs << slack)) slack -= 1;
         if (slack >= 2) {
             sh->lambda = lam;
             sh->slack_bits = slack;

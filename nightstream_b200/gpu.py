@@ -240,7 +240,8 @@ class GpuCcsOracle:
 
     def close(self):
         if getattr(self, "h", None):
-            self.ctx.lib.neo_gpu_ccs_oracle_destroy(self.h)
+            if self.ctx.h is not None:  # a closed context already released the device
+                self.ctx.lib.neo_gpu_ccs_oracle_destroy(self.h)
             self.h = None
 
     def __del__(self):
@@ -294,7 +295,8 @@ class Shard:
 
     def close(self):
         if getattr(self, "h", None):
-            self.ctx.lib.neo_gpu_shard_destroy(self.h)
+            if self.ctx.h is not None:
+                self.ctx.lib.neo_gpu_shard_destroy(self.h)
             self.h = None
 
     def __del__(self):
