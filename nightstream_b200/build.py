@@ -10,7 +10,7 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libneo_gpu.so")
-SOURCES = ["core.cu", "commit.cu", "ccs_oracle.cu", "fold.cu", "transcript.cpp", "transcript_capi.cpp"]
+SOURCES = ["core.cu", "commit.cu", "commit_tc.cu", "ccs_oracle.cu", "fold.cu", "transcript.cpp", "transcript_capi.cpp"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
@@ -37,7 +37,7 @@ def needs_build() -> bool:
 def build(force: bool = False, verbose: bool = False) -> str:
     if not force and not needs_build():
         return LIB
-    cmd = [NVCC] + FLAGS + ["-o", LIB] + sources() + ["-lcuda"]
+    cmd = [NVCC] + FLAGS + ["-o", LIB] + sources()
     if verbose:
         print(" ".join(cmd), file=sys.stderr)
     subprocess.run(cmd, check=True)

@@ -85,6 +85,14 @@ __global__ void commit_reduce_kernel(const uint64_t* __restrict__ partial, uint3
 
 int launch_commit(neo_gpu_ctx* ctx, const int8_t* d_digits, uint32_t n_vec, uint64_t m, uint64_t* d_out) {
     if (!ctx->d_pp || ctx->pp_m != m) return ctx->fail(NEO_ERR_ARG, "commit: PP not loaded for this m");
+    if (ctx->d_pp_limbs) {
+        // tensor-core path (commit_tc.cu)
+        uint32_t g, k, kb;
+        size_t need = tc_scratch_bytes(n_vec, m, &g, &k, &kb);
+        void* scratch = nullptr;
+        NEO_CK(ctx, ctx_scratch(ctx, need, &scratch));
+        return launch_commit_tc(ctx, d_digits, n_vec, m, d_out, (uint8_t*)scratch, ctx->d_err);
+    }
     const uint32_t kappa = ctx->kappa;
     // pick a chunking that fills the GPU: ~4 blocks per SM in total
     uint32_t target_blocks = 148 * 8;
@@ -114,6 +122,9 @@ extern "C" int neo_gpu_pp_upload(neo_gpu_ctx* ctx, uint32_t kappa, uint64_t m, c
     NEO_CK(ctx, cudaMemcpy(ctx->d_pp, coeffs, n * 8, cudaMemcpyHostToDevice));
     ctx->kappa = kappa;
     ctx->pp_m = m;
+    if (ctx->d_pp_limbs) { cudaFree(ctx->d_pp_limbs); ctx->d_pp_limbs = nullptr; }
+    // tensor-core layout of the PP (byte limbs, pre-swizzled tiles) when the shape allows it
+    if (kappa <= 16 && m % 2 == 0) return tc_pp_prepare(ctx);
     return NEO_OK;
 }
 
@@ -128,6 +139,7 @@ extern "C" int neo_gpu_commit(neo_gpu_ctx* ctx, const int8_t* digits, uint32_t n
     NEO_CK(ctx, cudaMemcpyAsync(dZ.p, digits, dZ.bytes(), cudaMemcpyHostToDevice, ctx->stream));
     int rc = launch_commit(ctx, dZ.p, n_vec, m, dout.p);
     if (rc) return rc;
+    if ((rc = check_device_error(ctx))) return rc;
     NEO_CK(ctx, cudaMemcpyAsync(out, dout.p, dout.bytes(), cudaMemcpyDeviceToHost, ctx->stream));
     NEO_CK(ctx, cudaStreamSynchronize(ctx->stream));
     return NEO_OK;

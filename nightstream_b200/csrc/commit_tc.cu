@@ -1,0 +1,423 @@
+// commit_tc.cu -- Ajtai commitment as an exact int8 tensor-core GEMM (tcgen05).
+//
+// c_i(X) = sum_j M[i][j](X) z_j(X) mod Phi_81 (crates/neo-ajtai/src/commit.rs:679-744).
+// Phi_81 divides X^81 - 1, so the product is taken mod X^81 - 1 (a length-81
+// cyclic convolution whose matrix entries are the raw PP coefficients) and
+// folded back with X^54 = -X^27 - 1.  As a GEMM:
+//
+//   D[(i,l)][(v,r)] = sum_{j, s<64} A[(i,l)][(j,s)] * B[(v,r)][(j,s)]
+//   A[(i,l)][(j,s)] = byte l of M[i][j][s]  (u8; 0 for s >= 54)
+//   B[(v,r)][(j,s)] = z_{v,j}[(r - s) mod 81] (s8; z[x] = 0 for x >= 54)
+//   c'_{v,i}[r] = sum_l 2^(8l) D[(i,l)][(v,r)]  (mod q), r < 81
+//
+// M = 128 = kappa * 8 rows, K = 64 m (s padded to 64 so one 128-byte K block
+// holds exactly two columns j), N = 81 per vector.  Accumulation is int32 in
+// TMEM; a CTA covers at most 512 K blocks, so |D| <= 255*128*65536 < 2^31 for
+// any int8 digit: no overflow.  CTAs split K and groups of NV vectors; a second
+// kernel sums the int32 partials, recombines limbs mod q and folds 81 -> 54.
+//
+// A tiles are stored in HBM already in the 128B-swizzled K-major UMMA layout
+// (16 KB per K block, contiguous) and fetched with one cp.async.bulk each.
+// B tiles are built in shared memory by 4 warps: row (v,r) of K block kb is
+// F_{v,j}[80 - r + s] for s in [0,64), a contiguous window of the 144-byte
+// sequence F_{v,j}[w] = z_{v,j}[(80 - w) mod 81] precomputed per column.
+#include "internal.cuh"
+
+namespace {
+
+constexpr int TC_NV = 4;                    // vectors per CTA
+constexpr int TC_NROWS = TC_NV * 81;        // 324 B rows used
+constexpr int TC_NPAD = 336;                // MMA N total (multiple of 16, atoms of 8)
+constexpr int TC_N0 = 256, TC_N1 = TC_NPAD - 256;  // two MMAs per K step
+constexpr int TC_STAGES = 3;
+constexpr int TC_A_BYTES = 128 * 128;       // 16 KB
+constexpr int TC_B_BYTES = TC_NPAD * 128;   // 42 KB
+constexpr int TC_STAGE_BYTES = TC_A_BYTES + TC_B_BYTES;
+constexpr int TC_THREADS = 192;             // warp0 producer, warp1 MMA, warps2-5 B build + epilogue
+constexpr int TC_MAX_KB = 512;              // K blocks per CTA (int32 overflow bound)
+constexpr int TC_FBYTES = 144;              // F sequence length (9 x 16 B)
+constexpr uint32_t TC_SPIN_LIMIT = 1u << 22;  // ~0.3 s with the back-off below
+
+static_assert(TC_B_BYTES % 1024 == 0 && TC_A_BYTES % 1024 == 0, "stage buffers stay 1024-byte aligned");
+static_assert(TC_NPAD % 16 == 0 && TC_N1 % 16 == 0 && TC_N1 >= 16, "MMA N constraints (M=128)");
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count));
+}
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+    asm volatile("{\n\t.reg .b64 st;\n\tmbarrier.arrive.shared::cta.b64 st, [%0];\n\t}" ::"r"(smem_u32(bar)) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+    asm volatile("{\n\t.reg .b64 st;\n\tmbarrier.arrive.expect_tx.shared::cta.b64 st, [%0], %1;\n\t}" ::"r"(smem_u32(bar)),
+                 "r"(bytes)
+                 : "memory");
+}
+// bounded wait on phase parity (non-blocking test + back-off); false on timeout
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
+    uint32_t addr = smem_u32(bar);
+    for (uint32_t it = 0; it < TC_SPIN_LIMIT; it++) {
+        uint32_t done;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\tmbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n\t}"
+            : "=r"(done)
+            : "r"(addr), "r"(parity)
+            : "memory");
+        if (done) return true;
+        if (it > 256) __nanosleep(64);
+    }
+    return false;
+}
+
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     smem_u32(dst)),
+                 "l"(src), "r"(bytes), "r"(smem_u32(bar))
+                 : "memory");
+}
+
+// UMMA shared-memory descriptor: K-major, 128B swizzle, 8-row atoms 1024 B apart.
+__device__ __forceinline__ uint64_t sw128_desc(uint32_t saddr) {
+    uint64_t d = 0;
+    d |= (uint64_t)((saddr >> 4) & 0x3FFF);          // start address
+    d |= (uint64_t)1 << 16;                           // leading byte offset (unused for SW128 K-major)
+    d |= (uint64_t)(1024 >> 4) << 32;                 // stride byte offset: 8 rows x 128 B
+    d |= (uint64_t)1 << 46;                           // descriptor version (sm_100)
+    d |= (uint64_t)2 << 61;                           // layout: SWIZZLE_128B
+    return d;
+}
+
+// instruction descriptor: kind::i8, D = s32, A = u8 (K-major), B = s8 (K-major), M = 128
+__host__ __device__ constexpr uint32_t idesc_i8(int n) {
+    return (2u << 4)            // c_format = S32
+           | (0u << 7)          // a_format = unsigned 8-bit
+           | (1u << 10)         // b_format = signed 8-bit
+           | ((uint32_t)(n >> 3) << 17) | ((uint32_t)(128 >> 4) << 24);
+}
+
+__device__ __forceinline__ void mma_i8(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
+                                       uint32_t accumulate) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem_d),
+        "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate));
+}
+
+__device__ __forceinline__ void mma_commit(uint64_t* bar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
+                 : "memory");
+}
+
+// ---------------------------------------------------------------------------
+// prep: PP -> pre-swizzled u8 limb tiles  PPL[kb][row][128 B]
+// ---------------------------------------------------------------------------
+__global__ void pp_limbs_kernel(const uint64_t* __restrict__ pp, uint32_t kappa, uint64_t m, uint8_t* __restrict__ ppl) {
+    // one thread per (kb, row, 16-byte chunk)
+    const uint64_t n_kb = m / 2;
+    const uint64_t tid = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+    if (tid >= n_kb * 128 * 8) return;
+    const uint32_t c = tid & 7, row = (tid >> 3) & 127;
+    const uint64_t kb = tid >> 10;
+    const uint32_t i = row >> 3, l = row & 7;
+    uint8_t out[16];
+#pragma unroll
+    for (int b = 0; b < 16; b++) {
+        uint32_t k = c * 16 + b;
+        uint64_t j = kb * 2 + (k >> 6);
+        uint32_t s = k & 63;
+        uint8_t v = 0;
+        if (i < kappa && s < NEO_D) v = (uint8_t)(pp[((uint64_t)i * m + j) * NEO_D + s] >> (8 * l));
+        out[b] = v;
+    }
+    uint32_t p = c ^ (row & 7);
+    uint4* dst = reinterpret_cast<uint4*>(ppl + kb * TC_A_BYTES + row * 128 + p * 16);
+    *dst = *reinterpret_cast<uint4*>(out);
+}
+
+// prep: F[v][j][w] = z_{v,j}[(80 - w) mod 81] (0 for indices >= 54), w < 144
+__global__ void f_seq_kernel(const int8_t* __restrict__ digits, uint32_t n_vec, uint64_t m, uint8_t* __restrict__ F) {
+    const uint64_t tid = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+    if (tid >= (uint64_t)n_vec * m) return;
+    const uint64_t v = tid / m, j = tid % m;
+    int8_t z[NEO_D];
+    const int8_t* zv = digits + v * NEO_D * m + j;
+#pragma unroll
+    for (int x = 0; x < NEO_D; x++) z[x] = zv[(uint64_t)x * m];
+    uint32_t w32[TC_FBYTES / 4];
+#pragma unroll
+    for (int q = 0; q < TC_FBYTES / 4; q++) {
+        uint32_t word = 0;
+#pragma unroll
+        for (int b = 0; b < 4; b++) {
+            int w = q * 4 + b;
+            int x = w <= 80 ? 80 - w : 161 - w;
+            uint8_t byte = (x >= 0 && x < NEO_D) ? (uint8_t)z[x] : 0;
+            word |= (uint32_t)byte << (8 * b);
+        }
+        w32[q] = word;
+    }
+    uint4* dst = reinterpret_cast<uint4*>(F + tid * TC_FBYTES);
+#pragma unroll
+    for (int q = 0; q < TC_FBYTES / 16; q++) dst[q] = make_uint4(w32[4 * q], w32[4 * q + 1], w32[4 * q + 2], w32[4 * q + 3]);
+}
+
+// ---------------------------------------------------------------------------
+// main GEMM kernel
+// ---------------------------------------------------------------------------
+struct TcArgs {
+    const uint8_t* ppl;     // pre-swizzled limb tiles
+    const uint8_t* F;       // [n_vec][m][144]
+    int32_t* partial;       // [n_cta][128][TC_NPAD]
+    uint32_t* err;          // error flag (timeouts)
+    uint64_t m;
+    uint32_t n_vec, n_groups, n_ksplit, kb_per_cta, n_kb;
+};
+
+__global__ void __launch_bounds__(TC_THREADS, 1) commit_tc_kernel(const TcArgs a) {
+    extern __shared__ __align__(1024) uint8_t smem_raw[];
+    // 1024-align the stage buffers (dynamic smem base alignment is not guaranteed)
+    uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+    uint8_t* sA = smem;                                   // [STAGES][16 KB]
+    uint8_t* sB = smem + TC_STAGES * TC_A_BYTES;          // [STAGES][42 KB]
+    uint64_t* bars = reinterpret_cast<uint64_t*>(sB + TC_STAGES * TC_B_BYTES);
+    uint64_t* full_a = bars;                  // [STAGES]
+    uint64_t* full_b = bars + TC_STAGES;      // [STAGES]
+    uint64_t* empty = bars + 2 * TC_STAGES;   // [STAGES]
+    uint64_t* done = bars + 3 * TC_STAGES;    // [1]
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 3 * TC_STAGES + 1);
+    __shared__ int s_abort;
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const uint32_t cta = blockIdx.x;
+    const uint32_t group = cta % a.n_groups, ks = cta / a.n_groups;
+    const uint32_t kb0 = ks * a.kb_per_cta;
+    const uint32_t kb1 = min(a.n_kb, kb0 + a.kb_per_cta);
+    const uint32_t nkb = kb1 > kb0 ? kb1 - kb0 : 0;
+
+    if (threadIdx.x == 0) {
+        s_abort = 0;
+        for (int s = 0; s < TC_STAGES; s++) {
+            mbar_init(&full_a[s], 1);
+            mbar_init(&full_b[s], 4);
+            mbar_init(&empty[s], 1);
+        }
+        mbar_init(done, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    // zero the padding rows of every B stage once (never rewritten)
+    for (int s = 0; s < TC_STAGES; s++)
+        for (int x = threadIdx.x; x < (TC_NPAD - TC_NROWS) * 8; x += blockDim.x) {
+            int row = TC_NROWS + x / 8, c = x % 8;
+            *reinterpret_cast<uint4*>(sB + s * TC_B_BYTES + (row >> 3) * 1024 + (row & 7) * 128 + c * 16) = make_uint4(0, 0, 0, 0);
+        }
+    if (warp == 1) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], 512;" ::"r"(smem_u32(tmem_slot)));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;");
+    const uint32_t tmem = *tmem_slot;
+
+    if (warp == 0) {
+        // ---- producer: A tiles ----
+        if (lane == 0) {
+            for (uint32_t it = 0; it < nkb; it++) {
+                const int s = it % TC_STAGES;
+                const uint32_t ph = (it / TC_STAGES) & 1;
+                if (it >= TC_STAGES && !mbar_wait(&empty[s], ph ^ 1)) { atomicOr(a.err, 1u); s_abort = 1; break; }
+                if (s_abort) break;
+                mbar_expect_tx(&full_a[s], TC_A_BYTES);
+                bulk_g2s(sA + s * TC_A_BYTES, a.ppl + (uint64_t)(kb0 + it) * TC_A_BYTES, TC_A_BYTES, &full_a[s]);
+            }
+        }
+    } else if (warp == 1) {
+        // ---- MMA issuer ----
+        if (lane == 0) {
+            const uint32_t id0 = idesc_i8(TC_N0), id1 = idesc_i8(TC_N1);
+            for (uint32_t it = 0; it < nkb; it++) {
+                const int s = it % TC_STAGES;
+                const uint32_t ph = (it / TC_STAGES) & 1;
+                if (!mbar_wait(&full_a[s], ph) || !mbar_wait(&full_b[s], ph)) { atomicOr(a.err, 2u); s_abort = 1; break; }
+                asm volatile("tcgen05.fence::after_thread_sync;");
+                const uint32_t a0 = smem_u32(sA + s * TC_A_BYTES), b0 = smem_u32(sB + s * TC_B_BYTES);
+#pragma unroll
+                for (int k = 0; k < 4; k++) {  // 4 x 32-byte K steps inside the 128-byte swizzle atom
+                    const uint64_t ad = sw128_desc(a0 + 32 * k);
+                    const uint32_t acc = (it > 0 || k > 0) ? 1u : 0u;
+                    mma_i8(tmem, ad, sw128_desc(b0 + 32 * k), id0, acc);
+                    mma_i8(tmem + TC_N0, ad, sw128_desc(b0 + (TC_N0 / 8) * 1024 + 32 * k), id1, acc);
+                }
+                mma_commit(&empty[s]);  // stage free once these MMAs complete
+            }
+            mma_commit(done);
+        }
+    } else {
+        // ---- B builders (warps 2..5, 128 threads) ----
+        const int bt = threadIdx.x - 64;
+        for (uint32_t it = 0; it < nkb; it++) {
+            const int s = it % TC_STAGES;
+            const uint32_t ph = (it / TC_STAGES) & 1;
+            if (it >= TC_STAGES && !mbar_wait(&empty[s], ph ^ 1)) { atomicOr(a.err, 4u); s_abort = 1; break; }
+            if (s_abort) break;
+            const uint64_t kb = kb0 + it;
+            uint8_t* dstB = sB + s * TC_B_BYTES;
+            for (int task = bt; task < TC_NROWS * 2; task += 128) {
+                const int half = task & 1, row = task >> 1;
+                const int vl = row / 81, r = row - vl * 81;
+                const uint32_t vg = group * TC_NV + vl;
+                uint32_t out[16];
+                if (vg < a.n_vec) {
+                    const uint64_t j = kb * 2 + half;
+                    const int o = 80 - r;  // window start in F
+                    const uint32_t* src =
+                        reinterpret_cast<const uint32_t*>(a.F + ((uint64_t)vg * a.m + j) * TC_FBYTES + (o & ~3));
+                    uint32_t w[17];
+#pragma unroll
+                    for (int q = 0; q < 17; q++) w[q] = __ldg(src + q);
+                    const uint32_t sh = 8 * (o & 3);
+#pragma unroll
+                    for (int q = 0; q < 16; q++) out[q] = __funnelshift_r(w[q], w[q + 1], sh);
+                } else {
+#pragma unroll
+                    for (int q = 0; q < 16; q++) out[q] = 0;
+                }
+                uint8_t* rowp = dstB + (row >> 3) * 1024 + (row & 7) * 128;
+#pragma unroll
+                for (int c = 0; c < 4; c++) {
+                    const int chunk = half * 4 + c;
+                    *reinterpret_cast<uint4*>(rowp + ((chunk ^ (row & 7)) * 16)) =
+                        make_uint4(out[4 * c], out[4 * c + 1], out[4 * c + 2], out[4 * c + 3]);
+                }
+            }
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&full_b[s]);
+        }
+        // ---- epilogue: TMEM -> int32 partials ----
+        bool ok = nkb > 0 && !s_abort && mbar_wait(done, 0);
+        if (nkb > 0 && !ok) atomicOr(a.err, 8u);
+        asm volatile("tcgen05.fence::after_thread_sync;");
+        const int lg = warp & 3;  // TMEM lane group this warp may access
+        const int row = lg * 32 + lane;
+        int32_t* dst = a.partial + ((uint64_t)cta * 128 + row) * TC_NPAD;
+        for (int c0 = 0; c0 < TC_NPAD; c0 += 16) {
+            uint32_t v[16];
+            const uint32_t taddr = tmem + ((uint32_t)(lg * 32) << 16) + (uint32_t)c0;
+            asm volatile(
+                "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+                : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
+                  "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
+                : "r"(taddr));
+            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+            if (ok) {
+#pragma unroll
+                for (int q = 0; q < 16; q += 4)
+                    *reinterpret_cast<int4*>(dst + c0 + q) = make_int4((int)v[q], (int)v[q + 1], (int)v[q + 2], (int)v[q + 3]);
+            } else {
+#pragma unroll
+                for (int q = 0; q < 16; q += 4) *reinterpret_cast<int4*>(dst + c0 + q) = make_int4(0, 0, 0, 0);
+            }
+        }
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;");
+    __syncthreads();
+    if (warp == 1) {
+        asm volatile("tcgen05.fence::after_thread_sync;");
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 512;" ::"r"(tmem));
+    }
+}
+
+// c'_{v,i}[r] = sum_{ks} sum_l 2^(8l) D[ks][(i,l)][(v,r)] mod q, then fold 81 -> 54
+__global__ void commit_tc_reduce_kernel(const int32_t* __restrict__ partial, uint32_t n_groups, uint32_t n_ksplit,
+                                        uint32_t kappa, uint32_t n_vec, uint64_t* __restrict__ out) {
+    const uint32_t vi = blockIdx.x;  // v * kappa + i
+    const uint32_t v = vi / kappa, i = vi % kappa;
+    const uint32_t group = v / TC_NV, vl = v % TC_NV;
+    __shared__ uint64_t s_c[81];
+    const int r = threadIdx.x;
+    if (r < 81) {
+        int64_t acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+        for (uint32_t ks = 0; ks < n_ksplit; ks++) {
+            const uint32_t cta = ks * n_groups + group;
+            const int32_t* p = partial + ((uint64_t)cta * 128 + i * 8) * TC_NPAD + vl * 81 + r;
+#pragma unroll
+            for (int l = 0; l < 8; l++) acc[l] += p[(uint64_t)l * TC_NPAD];
+        }
+        uint64_t c = 0;
+#pragma unroll
+        for (int l = 0; l < 8; l++) c = gl::add(c, gl::mul(gl::from_i64(acc[l]), 1ULL << (8 * l)));
+        s_c[r] = c;
+    }
+    __syncthreads();
+    if (r < NEO_D) out[((uint64_t)v * kappa + i) * NEO_D + r] = gl::sub(s_c[r], r >= 27 ? s_c[r + 27] : s_c[r + 54]);
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+int tc_pp_prepare(neo_gpu_ctx* ctx) {
+    if (ctx->kappa * 8 > 128) return ctx->fail(NEO_ERR_UNSUPPORTED, "tensor-core commit: kappa <= 16");
+    if (ctx->pp_m % 2) return ctx->fail(NEO_ERR_UNSUPPORTED, "tensor-core commit: m must be even");
+    if (ctx->d_pp_limbs) { cudaFree(ctx->d_pp_limbs); ctx->d_pp_limbs = nullptr; }
+    const uint64_t n_kb = ctx->pp_m / 2;
+    NEO_CK(ctx, cudaMalloc(&ctx->d_pp_limbs, n_kb * TC_A_BYTES));
+    const uint64_t threads = n_kb * 128 * 8;
+    pp_limbs_kernel<<<ceil_div(threads, 256), 256, 0, ctx->stream>>>(ctx->d_pp, ctx->kappa, ctx->pp_m, ctx->d_pp_limbs);
+    NEO_LAUNCHED(ctx);
+    NEO_CK(ctx, cudaStreamSynchronize(ctx->stream));
+    return NEO_OK;
+}
+
+size_t tc_scratch_bytes(uint32_t n_vec, uint64_t m, uint32_t* n_groups_out, uint32_t* n_ksplit_out,
+                        uint32_t* kb_per_cta_out) {
+    const uint32_t n_groups = (n_vec + TC_NV - 1) / TC_NV;
+    const uint32_t n_kb = (uint32_t)(m / 2);
+    // fill whole waves of 148 SMs (1 CTA per SM), at most TC_MAX_KB K blocks per CTA
+    uint32_t waves = 1, n_ksplit;
+    for (;; waves++) {
+        n_ksplit = (148 * waves + n_groups - 1) / n_groups;
+        if (n_ksplit > n_kb) n_ksplit = n_kb;
+        if ((n_kb + n_ksplit - 1) / n_ksplit <= TC_MAX_KB) break;
+    }
+    const uint32_t kb_per_cta = (n_kb + n_ksplit - 1) / n_ksplit;
+    n_ksplit = (n_kb + kb_per_cta - 1) / kb_per_cta;
+    *n_groups_out = n_groups;
+    *n_ksplit_out = n_ksplit;
+    *kb_per_cta_out = kb_per_cta;
+    size_t f_bytes = (size_t)n_vec * m * TC_FBYTES + 64;  // window reads may run 4 bytes past the last F
+    size_t p_bytes = (size_t)n_groups * n_ksplit * 128 * TC_NPAD * 4;
+    return ((f_bytes + 255) & ~size_t(255)) + p_bytes + 256;
+}
+
+int launch_commit_tc(neo_gpu_ctx* ctx, const int8_t* d_digits, uint32_t n_vec, uint64_t m, uint64_t* d_out,
+                     uint8_t* scratch, uint32_t* d_err) {
+    uint32_t n_groups, n_ksplit, kb_per_cta;
+    tc_scratch_bytes(n_vec, m, &n_groups, &n_ksplit, &kb_per_cta);
+    uint8_t* F = scratch;
+    int32_t* partial = reinterpret_cast<int32_t*>(scratch + (((size_t)n_vec * m * TC_FBYTES + 64 + 255) & ~size_t(255)));
+    f_seq_kernel<<<ceil_div((uint64_t)n_vec * m, 128), 128, 0, ctx->stream>>>(d_digits, n_vec, m, F);
+    NEO_LAUNCHED(ctx);
+    TcArgs a;
+    a.ppl = ctx->d_pp_limbs;
+    a.F = F;
+    a.partial = partial;
+    a.err = d_err;
+    a.m = m;
+    a.n_vec = n_vec;
+    a.n_groups = n_groups;
+    a.n_ksplit = n_ksplit;
+    a.kb_per_cta = kb_per_cta;
+    a.n_kb = (uint32_t)(m / 2);
+    const size_t smem = TC_STAGES * TC_STAGE_BYTES + 1024 /*align*/ + 256 /*barriers*/;
+    NEO_CK(ctx, cudaFuncSetAttribute(commit_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    commit_tc_kernel<<<n_groups * n_ksplit, TC_THREADS, smem, ctx->stream>>>(a);
+    NEO_LAUNCHED(ctx);
+    commit_tc_reduce_kernel<<<n_vec * ctx->kappa, 96, 0, ctx->stream>>>(partial, n_groups, n_ksplit, ctx->kappa, n_vec,
+                                                                        d_out);
+    NEO_LAUNCHED(ctx);
+    return NEO_OK;
+}

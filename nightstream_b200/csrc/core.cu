@@ -18,6 +18,11 @@ extern "C" int neo_gpu_ctx_create(int device, neo_gpu_ctx** out) {
         delete c;
         return NEO_ERR_CUDA;
     }
+    if (cudaMalloc(&c->d_err, sizeof(uint32_t)) != cudaSuccess || cudaMemset(c->d_err, 0, sizeof(uint32_t)) != cudaSuccess) {
+        cudaStreamDestroy(c->stream);
+        delete c;
+        return NEO_ERR_CUDA;
+    }
     *out = c;
     return NEO_OK;
 }
@@ -29,6 +34,7 @@ extern "C" int neo_gpu_ctx_destroy(neo_gpu_ctx* ctx) {
     if (ctx->d_pp) cudaFree(ctx->d_pp);
     if (ctx->d_pp_limbs) cudaFree(ctx->d_pp_limbs);
     if (ctx->scratch) cudaFree(ctx->scratch);
+    if (ctx->d_err) cudaFree(ctx->d_err);
     cudaStreamDestroy(ctx->stream);
     delete ctx;
     return NEO_OK;
@@ -36,6 +42,19 @@ extern "C" int neo_gpu_ctx_destroy(neo_gpu_ctx* ctx) {
 
 extern "C" const char* neo_gpu_last_error(const neo_gpu_ctx* ctx) { return ctx ? ctx->err.c_str() : "null context"; }
 extern "C" uint64_t neo_gpu_kernel_launches(const neo_gpu_ctx* ctx) { return ctx ? ctx->launches : 0; }
+int check_device_error(neo_gpu_ctx* ctx) {
+    uint32_t e = 0;
+    NEO_CK(ctx, cudaMemcpyAsync(&e, ctx->d_err, 4, cudaMemcpyDeviceToHost, ctx->stream));
+    NEO_CK(ctx, cudaStreamSynchronize(ctx->stream));
+    if (e) {
+        NEO_CK(ctx, cudaMemsetAsync(ctx->d_err, 0, 4, ctx->stream));
+        char buf[96];
+        snprintf(buf, sizeof buf, "device wait timed out (error bits 0x%x)", e);
+        return ctx->fail(NEO_ERR_CUDA, buf);
+    }
+    return NEO_OK;
+}
+
 extern "C" int neo_gpu_ctx_stream(const neo_gpu_ctx* ctx, void** stream) {
     if (!ctx || !stream) return NEO_ERR_ARG;
     *stream = (void*)ctx->stream;

@@ -357,6 +357,7 @@ static int fold_step_impl(neo_gpu_shard* sh, const uint64_t* z_host, const uint6
     NEO_CK(ctx, cudaMemcpyAsync(x.data(), d_z, sh->m_in * 8, cudaMemcpyDeviceToHost, ctx->stream));
     NEO_CK(ctx, cudaMemcpy2DAsync(Xd.data(), sh->m_in, sh->Zall.p, m, sh->m_in, NEO_D, cudaMemcpyDeviceToHost, ctx->stream));
     NEO_CK(ctx, cudaStreamSynchronize(ctx->stream));
+    if ((rc = check_device_error(ctx))) return rc;
     for (auto& v : x) v = gl::canon(v);
     mcs.m_in = sh->m_in;
     mcs.X.resize(Xd.size());
@@ -648,6 +649,7 @@ static int fold_step_impl(neo_gpu_shard* sh, const uint64_t* z_host, const uint6
     NEO_CK(ctx, cudaMemcpy2DAsync(Xc.data(), sh->m_in, planes, m, sh->m_in, (size_t)sh->k_rho * NEO_D,
                                   cudaMemcpyDeviceToHost, ctx->stream));
     NEO_CK(ctx, cudaStreamSynchronize(ctx->stream));
+    if ((rc = check_device_error(ctx))) return rc;
     if (flags[0]) return ctx->fail(NEO_ERR_INVARIANT, "DEC split: Z_mix entry out of range for k_rho digits");
     // DEC public checks (dec_children_with_commit_cached): c and y recompose in base b
     {

@@ -22,6 +22,7 @@ struct neo_gpu_ctx {
     uint64_t pp_m = 0;
     uint64_t* d_pp = nullptr;       // [kappa][m][54] canonical u64
     uint8_t* d_pp_limbs = nullptr;  // [kappa*8][m*54] byte limbs (tensor-core layout)
+    uint32_t* d_err = nullptr;       // device error word (bounded-wait timeouts); 0 = ok
     void* scratch = nullptr;         // growable per-context scratch (stream-ordered use)
     size_t scratch_bytes = 0;
     int fail(int code, const char* what, cudaError_t e = cudaSuccess) {
@@ -115,5 +116,11 @@ int launch_me_y(neo_gpu_ctx* ctx, const DevCcs& ccs, const int8_t* d_Z, uint32_t
                 const gl::K* d_chi, uint32_t ell_n, uint32_t b, gl::K* d_vj_scratch, gl::K* d_y,
                 gl::K* d_ysc);
 int launch_commit(neo_gpu_ctx* ctx, const int8_t* d_digits, uint32_t n_vec, uint64_t m, uint64_t* d_out);
+int tc_pp_prepare(neo_gpu_ctx* ctx);
+size_t tc_scratch_bytes(uint32_t n_vec, uint64_t m, uint32_t* n_groups, uint32_t* n_ksplit, uint32_t* kb_per_cta);
+int launch_commit_tc(neo_gpu_ctx* ctx, const int8_t* d_digits, uint32_t n_vec, uint64_t m, uint64_t* d_out,
+                     uint8_t* scratch, uint32_t* d_err);
+// reads and clears the device error word (synchronizes the stream)
+int check_device_error(neo_gpu_ctx* ctx);
 
 inline unsigned ceil_div(uint64_t a, uint64_t b) { return (unsigned)((a + b - 1) / b); }

@@ -13,7 +13,7 @@ def _pp(kappa, m, seed):
     return np.random.default_rng(seed).integers(0, Q, size=(kappa, m, 54), dtype=np.uint64)
 
 
-@pytest.mark.parametrize("m,n_vec", [(64, 1), (1024, 3), (4096, 13), (1 << 16, 1)])
+@pytest.mark.parametrize("m,n_vec", [(2, 1), (64, 1), (1024, 3), (1024, 5), (4096, 13), (1 << 16, 1), (1 << 16, 12)])
 def test_commit_matches_oracle(ctx, m, n_vec):
     pp = _pp(16, m, m)
     rng = np.random.default_rng(m + n_vec)
@@ -32,8 +32,21 @@ def test_commit_edge_digits(ctx):
     assert np.all(ctx.commit(zeros) == 0)
     ones = np.ones((54, m), np.int8)
     big = np.full((54, m), -128, np.int8)
-    assert np.array_equal(ctx.commit(ones), O.commit_digits(pp, ones))
-    assert np.array_equal(ctx.commit(big), O.commit_digits(pp, big))
+    top = np.full((54, m), 127, np.int8)
+    for Z in (ones, big, top):
+        assert np.array_equal(ctx.commit(Z), O.commit_digits(pp, Z))
+
+
+def test_commit_int32_bound_extreme_pp(ctx):
+    # all PP limbs 0xFF and all digits -128: the per-CTA int32 partials sit at the
+    # overflow bound of the K split (512 K blocks of 128 bytes)
+    m = 1 << 12
+    pp = np.full((16, m, 54), (1 << 64) - (1 << 32), dtype=np.uint64)  # q - 1: every byte limb is 0xFF or 0x00
+    pp[:, :, ::2] = np.uint64(0xFEFFFFFFFFFFFFFF)
+    ctx.pp_upload(pp)
+    Z = np.full((2, 54, m), -128, np.int8)
+    got = ctx.commit(Z)
+    assert np.array_equal(got[0], O.commit_digits(pp, Z[0]))
 
 
 def test_decomp_matches_oracle(ctx):
