@@ -18,17 +18,20 @@
 
 namespace gl {
 
-GL_HD uint64_t canon(uint64_t a) { return a >= GL_Q ? a - GL_Q : a; }
+// Branch-free forms: field elements are data-dependent, so conditional
+// corrections are written as masks (no mispredicted branches on the host,
+// predicated selects on the device).
+GL_HD uint64_t canon(uint64_t a) { return a - ((uint64_t)(a >= GL_Q) * GL_Q); }
 
 GL_HD uint64_t add(uint64_t a, uint64_t b) {
     uint64_t s = a + b;
-    s += (s < a) ? GL_EPS : 0ULL;
+    s += (uint64_t)(s < a) * GL_EPS;  // carry: 2^64 = 2^32 - 1 (mod q)
     return canon(s);
 }
 
 GL_HD uint64_t sub(uint64_t a, uint64_t b) {
     uint64_t d = a - b;
-    return (a < b) ? d + GL_Q : d;   // a - b + q, exact mod 2^64
+    return d + (uint64_t)(a < b) * GL_Q;  // a - b + q, exact mod 2^64
 }
 
 GL_HD uint64_t neg(uint64_t a) { return a ? GL_Q - a : 0ULL; }
@@ -37,10 +40,10 @@ GL_HD uint64_t reduce128(uint64_t lo, uint64_t hi) {
     uint64_t hi_hi = hi >> 32;
     uint64_t hi_lo = hi & GL_EPS;
     uint64_t t0 = lo - hi_hi;
-    if (lo < hi_hi) t0 -= GL_EPS;
-    uint64_t t1 = (hi_lo << 32) - hi_lo;  // hi_lo * (2^32 - 1)
+    t0 -= (uint64_t)(lo < hi_hi) * GL_EPS;  // borrow: -2^64 = -(2^32 - 1)
+    uint64_t t1 = (hi_lo << 32) - hi_lo;     // hi_lo * (2^32 - 1)
     uint64_t s = t0 + t1;
-    if (s < t0) s += GL_EPS;
+    s += (uint64_t)(s < t0) * GL_EPS;       // carry
     return canon(s);
 }
 

@@ -101,41 +101,55 @@ const Poseidon2W16& digest_perm() {
     return inst;
 }
 
+typedef unsigned __int128 u128;
+
+// reduce x < 2^128 mod q (2^64 = 2^32 - 1, 2^96 = -1); canonical result
+static inline uint64_t red128(u128 x) { return gl::reduce128((uint64_t)x, (uint64_t)(x >> 64)); }
+
+static inline uint64_t mulq(uint64_t a, uint64_t b) { return red128((u128)a * b); }
+
 static inline uint64_t sbox7(uint64_t x) {
-    uint64_t x2 = gl::mul(x, x);
-    uint64_t x3 = gl::mul(x2, x);
-    uint64_t x6 = gl::mul(x3, x3);
-    return gl::mul(x6, x);
+    uint64_t x2 = mulq(x, x);
+    uint64_t x3 = mulq(x2, x);
+    uint64_t x6 = mulq(x3, x3);
+    return mulq(x6, x);
 }
 
-// M4 of the Poseidon2 paper: [[5,7,1,3],[4,6,1,1],[1,3,5,7],[1,1,4,6]]
-static inline void m4(uint64_t* x) {
-    static const uint32_t M[4][4] = {{5, 7, 1, 3}, {4, 6, 1, 1}, {1, 3, 5, 7}, {1, 1, 4, 6}};
-    uint64_t y[4];
-    for (int r = 0; r < 4; r++) {
-        uint64_t acc = 0;
-        for (int c = 0; c < 4; c++) acc = gl::add(acc, gl::mul_small(x[c], M[r][c]));
-        y[r] = acc;
-    }
-    memcpy(x, y, sizeof y);
+// M4 = [[5,7,1,3],[4,6,1,1],[1,3,5,7],[1,1,4,6]] by the Poseidon2 paper's
+// addition chain (8 additions, 4 doublings); inputs < 2^64, outputs < 2^69.
+static inline void m4_lazy(const uint64_t* x, u128* y) {
+    u128 t0 = (u128)x[0] + x[1];
+    u128 t1 = (u128)x[2] + x[3];
+    u128 t2 = ((u128)x[1] << 1) + t1;
+    u128 t3 = ((u128)x[3] << 1) + t0;
+    u128 t4 = (t1 << 2) + t3;
+    u128 t5 = (t0 << 2) + t2;
+    u128 t6 = t3 + t5;
+    u128 t7 = t2 + t4;
+    y[0] = t6;
+    y[1] = t5;
+    y[2] = t7;
+    y[3] = t4;
 }
 
 // external layer circ(2 M4, M4, ..., M4): y_blk = M4 x_blk + sum_blk' M4 x_blk'
 template <int W>
 static inline void external_layer(uint64_t* st) {
-    for (int b = 0; b < W / 4; b++) m4(st + 4 * b);
+    u128 y[W];
+    for (int b = 0; b < W / 4; b++) m4_lazy(st + 4 * b, y + 4 * b);
     for (int i = 0; i < 4; i++) {
-        uint64_t s = 0;
-        for (int b = 0; b < W / 4; b++) s = gl::add(s, st[4 * b + i]);
-        for (int b = 0; b < W / 4; b++) st[4 * b + i] = gl::add(st[4 * b + i], s);
+        u128 s = 0;
+        for (int b = 0; b < W / 4; b++) s += y[4 * b + i];
+        for (int b = 0; b < W / 4; b++) st[4 * b + i] = red128(y[4 * b + i] + s);
     }
 }
 
 template <int W>
 static inline void internal_layer(uint64_t* st, const uint64_t* mu) {
-    uint64_t sum = 0;
-    for (int i = 0; i < W; i++) sum = gl::add(sum, st[i]);
-    for (int i = 0; i < W; i++) st[i] = gl::add(sum, gl::mul(mu[i], st[i]));
+    u128 acc = 0;
+    for (int i = 0; i < W; i++) acc += st[i];
+    const uint64_t sum = red128(acc);
+    for (int i = 0; i < W; i++) st[i] = red128((u128)mu[i] * st[i] + sum);
 }
 
 template <int W>
