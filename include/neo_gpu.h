@@ -79,6 +79,21 @@ int neo_gpu_commit(neo_gpu_ctx* ctx, const int8_t* digits, uint32_t n_vec, uint6
  * call is asynchronous on the context stream. */
 int neo_gpu_commit_device(neo_gpu_ctx* ctx, const int8_t* d_digits, uint32_t n_vec, uint64_t m, uint64_t* d_out);
 
+/* Allocation-free commitment (no counterpart in the reference).  Same result
+ * as neo_gpu_commit_device, for callers that cannot allocate device memory
+ * when they commit: code running under CUDA stream capture, hosts whose
+ * framework owns all device memory through its own pool, and latency-critical
+ * provers that cannot afford the implicit synchronization of cudaMalloc /
+ * cudaFree.  Inputs and outputs are DEVICE pointers owned by the caller; the
+ * split-K scratch is a fixed 4 MiB device array inside the library (held by
+ * every GPU that loads the library until exit).  n_vec * kappa * 81 must not
+ * exceed 524288 (n_vec <= 404 for kappa = 16), else NEO_ERR_ARG.  The first
+ * call on a device resolves the array's device address (cudaGetSymbolAddress):
+ * make that first call before any stream capture.  All calls share the array,
+ * so calls that overlap on the GPU (other streams or contexts) race.  The call
+ * is asynchronous on the context stream and allocates nothing. */
+int neo_gpu_commit_noalloc(neo_gpu_ctx* ctx, const int8_t* d_digits, uint32_t n_vec, uint64_t m, uint64_t* d_out);
+
 /* Balanced base-2 decomposition z in F_q^m -> Z in {-1,0,1}^{54 x m}
  * row-major (crates/neo-ajtai/src/decomp.rs:118-158, DecompStyle::Balanced). */
 int neo_gpu_decomp_b2(neo_gpu_ctx* ctx, const uint64_t* z, uint64_t m, int8_t* Z);

@@ -152,3 +152,73 @@ extern "C" int neo_gpu_commit_device(neo_gpu_ctx* ctx, const int8_t* d_digits, u
     cudaSetDevice(ctx->device);
     return launch_commit(ctx, d_digits, n_vec, m, d_out);
 }
+
+// ---------------------------------------------------------------------------
+// Allocation-free commitment.
+//
+// Some callers cannot allocate device memory at the moment they commit: code
+// running while a CUDA stream is being captured into a graph (cudaMalloc and
+// cudaFree are not stream-ordered and break or serialize the capture), hosts
+// whose framework owns every device byte through its own pool and forbids
+// untracked allocations, and latency-critical provers for which the implicit
+// device synchronization of cudaMalloc/cudaFree would stall other streams.
+// For them, neo_gpu_commit_noalloc runs the CUDA-core commitment kernels above
+// with their split-K partial sums in the fixed device array below instead of
+// context scratch.  The array is part of the library image, so every GPU that
+// loads the library holds its 4 MiB until the process exits.
+// ---------------------------------------------------------------------------
+#include <mutex>
+
+namespace {
+constexpr uint64_t NOALLOC_SCRATCH_WORDS = 1ull << 19;  // 524288 uint64 = 4 MiB of partial sums
+static __device__ __align__(256) uint64_t g_commit_noalloc_scratch[NOALLOC_SCRATCH_WORDS];
+constexpr int NOALLOC_MAX_DEVICES = 64;
+std::mutex g_noalloc_mu;
+uint64_t* g_noalloc_ptr[NOALLOC_MAX_DEVICES] = {nullptr};
+}  // namespace
+
+extern "C" int neo_gpu_commit_noalloc(neo_gpu_ctx* ctx, const int8_t* d_digits, uint32_t n_vec, uint64_t m,
+                                      uint64_t* d_out) {
+    if (!ctx) return NEO_ERR_ARG;
+    if (!d_digits || !d_out || n_vec == 0 || m == 0) return ctx->fail(NEO_ERR_ARG, "commit_noalloc: bad args");
+    if (!ctx->d_pp || ctx->pp_m != m) return ctx->fail(NEO_ERR_ARG, "commit_noalloc: PP not loaded for this m");
+    if (ctx->device < 0 || ctx->device >= NOALLOC_MAX_DEVICES) return ctx->fail(NEO_ERR_UNSUPPORTED, "commit_noalloc: device index");
+    const uint32_t kappa = ctx->kappa;
+    const uint64_t per_chunk = (uint64_t)n_vec * kappa * 81;  // partial words needed per column chunk
+    if (per_chunk > NOALLOC_SCRATCH_WORDS)
+        return ctx->fail(NEO_ERR_ARG,
+                         "commit_noalloc: n_vec * kappa * 81 exceeds the fixed 524288-word scratch "
+                         "(at most 404 vectors for kappa = 16); use neo_gpu_commit_device");
+    NEO_CK(ctx, cudaSetDevice(ctx->device));
+    // one-time set-up on this device: the array's device address (the host-side
+    // symbol is only a stand-in and must never be handed to a kernel)
+    uint64_t* scratch = nullptr;
+    {
+        std::lock_guard<std::mutex> lk(g_noalloc_mu);
+        if (!g_noalloc_ptr[ctx->device]) {
+            void* p = nullptr;
+            cudaError_t e = cudaGetSymbolAddress(&p, g_commit_noalloc_scratch);
+            if (e != cudaSuccess || !p) return ctx->fail(NEO_ERR_CUDA, "commit_noalloc: cudaGetSymbolAddress", e);
+            g_noalloc_ptr[ctx->device] = static_cast<uint64_t*>(p);
+        }
+        scratch = g_noalloc_ptr[ctx->device];
+    }
+    // same chunking rule as launch_commit, capped by the scratch capacity
+    uint32_t target_blocks = 148 * 8;
+    uint32_t per = (uint32_t)((uint64_t)kappa * n_vec);
+    uint64_t n_chunks = (target_blocks + per - 1) / per;
+    const uint64_t cap_chunks = NOALLOC_SCRATCH_WORDS / per_chunk;
+    if (n_chunks > cap_chunks) n_chunks = cap_chunks;
+    uint64_t cols_per_block = (m + n_chunks - 1) / n_chunks;
+    if (cols_per_block < CHUNK_COLS) cols_per_block = CHUNK_COLS;
+    n_chunks = (m + cols_per_block - 1) / cols_per_block;  // never grows past cap_chunks
+    dim3 grid((uint32_t)n_chunks, kappa, n_vec);
+    // every partial word a reduce reads is written by commit_partial_kernel first,
+    // so the array needs no clearing between calls
+    commit_partial_kernel<<<grid, COMMIT_THREADS, 0, ctx->stream>>>(ctx->d_pp, kappa, m, d_digits,
+                                                                     (uint32_t)cols_per_block, scratch);
+    NEO_LAUNCHED(ctx);
+    commit_reduce_kernel<<<n_vec * kappa, 96, 0, ctx->stream>>>(scratch, (uint32_t)n_chunks, kappa, n_vec, d_out);
+    NEO_LAUNCHED(ctx);
+    return NEO_OK;
+}

@@ -44,6 +44,7 @@ SIGNATURES = {
     "neo_gpu_ctx_stream": [P, P],
     "neo_gpu_synchronize": [P],
     "neo_gpu_commit_device": [P, ctypes.c_void_p, U32, U64, ctypes.c_void_p],
+    "neo_gpu_commit_noalloc": [P, ctypes.c_void_p, U32, U64, ctypes.c_void_p],
     "neo_gpu_shard_step_stats": [P, P, U32],
     "neo_gpu_shard_create": [P, P, U32, U32, ctypes.c_char_p, P],
     "neo_gpu_shard_fold_step": [P, P, P, U64, P],
@@ -135,6 +136,10 @@ class Context:
 
     def commit_device(self, d_digits: int, n_vec: int, m: int, d_out: int):
         self.check(self.lib.neo_gpu_commit_device(self.h, ctypes.c_void_p(d_digits), n_vec, m, ctypes.c_void_p(d_out)))
+
+    def commit_noalloc(self, d_digits: int, n_vec: int, m: int, d_out: int):
+        """Commitment with the library's fixed device scratch (no allocation)."""
+        self.check(self.lib.neo_gpu_commit_noalloc(self.h, ctypes.c_void_p(d_digits), n_vec, m, ctypes.c_void_p(d_out)))
 
     def close(self):
         if getattr(self, "h", None):
