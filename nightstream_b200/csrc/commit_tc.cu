@@ -32,13 +32,16 @@ constexpr int TC_N0 = 256, TC_N1 = TC_NPAD - 256;  // two MMAs per K step
 constexpr int TC_STAGES = 3;
 constexpr int TC_A_BYTES = 128 * 128;       // 16 KB
 constexpr int TC_B_BYTES = TC_NPAD * 128;   // 42 KB
-constexpr int TC_STAGE_BYTES = TC_A_BYTES + TC_B_BYTES;
-constexpr int TC_THREADS = 192;             // warp0 producer, warp1 MMA, warps2-5 B build + epilogue
-constexpr int TC_MAX_KB = 512;              // K blocks per CTA (int32 overflow bound)
 constexpr int TC_FBYTES = 144;              // F sequence length (9 x 16 B)
+constexpr int TC_F_STAGE = 1280;            // NV x 2 columns x 144 B, padded (window reads overrun by 4 B)
+constexpr int TC_STAGE_BYTES = TC_A_BYTES + TC_B_BYTES + TC_F_STAGE;
+constexpr int TC_BUILDERS = 256;            // 8 builder warps
+constexpr int TC_THREADS = 64 + TC_BUILDERS;  // warp0 producer, warp1 MMA, warps2-9 B build (2-5 epilogue)
+constexpr int TC_MAX_KB = 512;              // K blocks per CTA (int32 overflow bound)
 constexpr uint32_t TC_SPIN_LIMIT = 1u << 22;  // ~0.3 s with the back-off below
 
 static_assert(TC_B_BYTES % 1024 == 0 && TC_A_BYTES % 1024 == 0, "stage buffers stay 1024-byte aligned");
+static_assert(TC_NV * 2 * TC_FBYTES + 16 <= TC_F_STAGE, "F staging holds the window overrun");
 static_assert(TC_NPAD % 16 == 0 && TC_N1 % 16 == 0 && TC_N1 >= 16, "MMA N constraints (M=128)");
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
@@ -182,7 +185,8 @@ __global__ void __launch_bounds__(TC_THREADS, 1) commit_tc_kernel(const TcArgs a
     uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
     uint8_t* sA = smem;                                   // [STAGES][16 KB]
     uint8_t* sB = smem + TC_STAGES * TC_A_BYTES;          // [STAGES][42 KB]
-    uint64_t* bars = reinterpret_cast<uint64_t*>(sB + TC_STAGES * TC_B_BYTES);
+    uint8_t* sF = sB + TC_STAGES * TC_B_BYTES;            // [STAGES][1280 B] F sequences of the stage
+    uint64_t* bars = reinterpret_cast<uint64_t*>(sF + TC_STAGES * TC_F_STAGE);
     uint64_t* full_a = bars;                  // [STAGES]
     uint64_t* full_b = bars + TC_STAGES;      // [STAGES]
     uint64_t* empty = bars + 2 * TC_STAGES;   // [STAGES]
@@ -196,12 +200,13 @@ __global__ void __launch_bounds__(TC_THREADS, 1) commit_tc_kernel(const TcArgs a
     const uint32_t kb0 = ks * a.kb_per_cta;
     const uint32_t kb1 = min(a.n_kb, kb0 + a.kb_per_cta);
     const uint32_t nkb = kb1 > kb0 ? kb1 - kb0 : 0;
+    const uint32_t nvalid = min((uint32_t)TC_NV, a.n_vec - group * TC_NV);  // vectors of this group
 
     if (threadIdx.x == 0) {
         s_abort = 0;
         for (int s = 0; s < TC_STAGES; s++) {
             mbar_init(&full_a[s], 1);
-            mbar_init(&full_b[s], 4);
+            mbar_init(&full_b[s], TC_BUILDERS / 32);
             mbar_init(&empty[s], 1);
         }
         mbar_init(done, 1);
@@ -230,8 +235,13 @@ __global__ void __launch_bounds__(TC_THREADS, 1) commit_tc_kernel(const TcArgs a
                 const uint32_t ph = (it / TC_STAGES) & 1;
                 if (it >= TC_STAGES && !mbar_wait(&empty[s], ph ^ 1)) { atomicOr(a.err, 1u); s_abort = 1; break; }
                 if (s_abort) break;
-                mbar_expect_tx(&full_a[s], TC_A_BYTES);
-                bulk_g2s(sA + s * TC_A_BYTES, a.ppl + (uint64_t)(kb0 + it) * TC_A_BYTES, TC_A_BYTES, &full_a[s]);
+                const uint64_t kb = kb0 + it;
+                mbar_expect_tx(&full_a[s], TC_A_BYTES + nvalid * 2 * TC_FBYTES);
+                bulk_g2s(sA + s * TC_A_BYTES, a.ppl + kb * TC_A_BYTES, TC_A_BYTES, &full_a[s]);
+                // F sequences of columns 2kb, 2kb+1 for each vector of the group (288 contiguous bytes)
+                for (uint32_t vl = 0; vl < nvalid; vl++)
+                    bulk_g2s(sF + s * TC_F_STAGE + vl * 2 * TC_FBYTES,
+                             a.F + ((uint64_t)(group * TC_NV + vl) * a.m + kb * 2) * TC_FBYTES, 2 * TC_FBYTES, &full_a[s]);
             }
         }
     } else if (warp == 1) {
@@ -256,28 +266,27 @@ __global__ void __launch_bounds__(TC_THREADS, 1) commit_tc_kernel(const TcArgs a
             mma_commit(done);
         }
     } else {
-        // ---- B builders (warps 2..5, 128 threads) ----
+        // ---- B builders (warps 2..9) ----
         const int bt = threadIdx.x - 64;
         for (uint32_t it = 0; it < nkb; it++) {
             const int s = it % TC_STAGES;
             const uint32_t ph = (it / TC_STAGES) & 1;
-            if (it >= TC_STAGES && !mbar_wait(&empty[s], ph ^ 1)) { atomicOr(a.err, 4u); s_abort = 1; break; }
+            // the stage's A tile and F sequences have landed (which also means the stage is free)
+            if (!mbar_wait(&full_a[s], ph)) { atomicOr(a.err, 4u); s_abort = 1; break; }
             if (s_abort) break;
-            const uint64_t kb = kb0 + it;
             uint8_t* dstB = sB + s * TC_B_BYTES;
-            for (int task = bt; task < TC_NROWS * 2; task += 128) {
+            const uint8_t* srcF = sF + s * TC_F_STAGE;
+            for (int task = bt; task < TC_NROWS * 2; task += TC_BUILDERS) {
                 const int half = task & 1, row = task >> 1;
                 const int vl = row / 81, r = row - vl * 81;
-                const uint32_t vg = group * TC_NV + vl;
                 uint32_t out[16];
-                if (vg < a.n_vec) {
-                    const uint64_t j = kb * 2 + half;
+                if ((uint32_t)vl < nvalid) {
                     const int o = 80 - r;  // window start in F
                     const uint32_t* src =
-                        reinterpret_cast<const uint32_t*>(a.F + ((uint64_t)vg * a.m + j) * TC_FBYTES + (o & ~3));
+                        reinterpret_cast<const uint32_t*>(srcF + (vl * 2 + half) * TC_FBYTES + (o & ~3));
                     uint32_t w[17];
 #pragma unroll
-                    for (int q = 0; q < 17; q++) w[q] = __ldg(src + q);
+                    for (int q = 0; q < 17; q++) w[q] = src[q];
                     const uint32_t sh = 8 * (o & 3);
 #pragma unroll
                     for (int q = 0; q < 16; q++) out[q] = __funnelshift_r(w[q], w[q + 1], sh);
@@ -297,14 +306,14 @@ __global__ void __launch_bounds__(TC_THREADS, 1) commit_tc_kernel(const TcArgs a
             __syncwarp();
             if (lane == 0) mbar_arrive(&full_b[s]);
         }
-        // ---- epilogue: TMEM -> int32 partials ----
+        // ---- epilogue (warps 2..5 cover TMEM lane groups 2, 3, 0, 1): TMEM -> int32 partials ----
         bool ok = nkb > 0 && !s_abort && mbar_wait(done, 0);
-        if (nkb > 0 && !ok) atomicOr(a.err, 8u);
+        if (nkb > 0 && !ok && warp < 6) atomicOr(a.err, 8u);
         asm volatile("tcgen05.fence::after_thread_sync;");
         const int lg = warp & 3;  // TMEM lane group this warp may access
         const int row = lg * 32 + lane;
         int32_t* dst = a.partial + ((uint64_t)cta * 128 + row) * TC_NPAD;
-        for (int c0 = 0; c0 < TC_NPAD; c0 += 16) {
+        for (int c0 = 0; c0 < (warp < 6 ? TC_NPAD : 0); c0 += 16) {
             uint32_t v[16];
             const uint32_t taddr = tmem + ((uint32_t)(lg * 32) << 16) + (uint32_t)c0;
             asm volatile(
@@ -413,6 +422,7 @@ int launch_commit_tc(neo_gpu_ctx* ctx, const int8_t* d_digits, uint32_t n_vec, u
     a.kb_per_cta = kb_per_cta;
     a.n_kb = (uint32_t)(m / 2);
     const size_t smem = TC_STAGES * TC_STAGE_BYTES + 1024 /*align*/ + 256 /*barriers*/;
+    static_assert(TC_STAGES * TC_STAGE_BYTES + 1024 + 256 <= 232448, "shared memory budget");
     NEO_CK(ctx, cudaFuncSetAttribute(commit_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     commit_tc_kernel<<<n_groups * n_ksplit, TC_THREADS, smem, ctx->stream>>>(a);
     NEO_LAUNCHED(ctx);
