@@ -595,6 +595,10 @@ struct neo_gpu_ccs_oracle {
     // Ajtai-phase state
     bool have_pre = false;
     DevBuf<K> chi_r, vj, y_eval, y_sc;
+    // build temporaries, kept across re-initialisations
+    DevBuf<K> ws_bits, ws_w, ws_coef, ws_u;
+    DevBuf<uint64_t> ws_z1, ws_nnzoff;
+    DevBuf<uint8_t> ws_isid;
 };
 
 static std::vector<K> load_k(const uint64_t* p, size_t n) {
@@ -640,15 +644,21 @@ extern "C" int neo_gpu_ccs_oracle_create(neo_gpu_ctx* ctx, const neo_ccs_desc* d
     return NEO_OK;
 }
 
+// Builds the oracle in *inout; an existing oracle is re-initialised in place so
+// its device workspaces are reused across fold steps.
 int ccs_oracle_create_dev(neo_gpu_ctx* ctx, const DevCcs* ccs, const int8_t* d_Z, uint32_t k, uint32_t b,
                           const K* alpha, const K* beta_a, const K* beta_r, K gamma, const K* r_inputs,
-                          uint32_t ell_d, uint32_t ell_n, uint32_t d_sc, neo_gpu_ccs_oracle** out) {
-    auto* o = new neo_gpu_ccs_oracle();
-    std::unique_ptr<neo_gpu_ccs_oracle> guard(o);
+                          uint32_t ell_d, uint32_t ell_n, uint32_t d_sc, neo_gpu_ccs_oracle** inout) {
+    std::unique_ptr<neo_gpu_ccs_oracle> guard;
+    neo_gpu_ccs_oracle* o = *inout;
+    if (!o) {
+        o = new neo_gpu_ccs_oracle();
+        guard.reset(o);
+    }
     o->ccs = ccs;
     int rc = oracle_init(ctx, o, d_Z, k, b, alpha, beta_a, beta_r, gamma, r_inputs, ell_d, ell_n, d_sc);
     if (rc) return rc;
-    *out = guard.release();
+    if (guard) *inout = guard.release();
     return NEO_OK;
 }
 
@@ -666,6 +676,13 @@ static int oracle_init(neo_gpu_ctx* ctx, neo_gpu_ccs_oracle* o, const int8_t* d_
     o->ctx = ctx;
     o->Z = d_Z;
     o->k = k; o->b = b; o->ell_d = ell_d; o->ell_n = ell_n; o->d_sc = d_sc;
+    // (re)initialisation: protocol state starts over, device buffers are reused
+    o->f = FTerms{};
+    o->n_fvar = 0;
+    o->n_small = 0; o->idx_eqrin = -1; o->idx_eval = -1;
+    o->small_cur = 0; o->nc_cur = 0;
+    o->row_chals.clear(); o->ajtai_chals.clear(); o->r_in.clear();
+    o->round_idx = 0; o->coeffs_valid = false; o->have_pre = false;
     int rc = 0;
     o->t = cc.t;
     o->m = cc.m;
@@ -723,15 +740,15 @@ static int oracle_init(neo_gpu_ctx* ctx, neo_gpu_ccs_oracle* o, const int8_t* d_
         o->idx_eqrin = o->n_small++;
         o->idx_eval = o->n_small++;
     }
-    NEO_CK(ctx, o->small[0].alloc((size_t)o->n_small * n_pad));
-    NEO_CK(ctx, o->small[1].alloc((size_t)o->n_small * n_pad / 2 + 1));
+    NEO_CK(ctx, o->small[0].ensure((size_t)o->n_small * n_pad));
+    NEO_CK(ctx, o->small[1].ensure((size_t)o->n_small * n_pad / 2 + 1));
     K* S = o->small[0].p;
-    DevBuf<K> dbits;
-    NEO_CK(ctx, dbits.alloc(ell_n));
+    DevBuf<K>& dbits = o->ws_bits;
+    NEO_CK(ctx, dbits.ensure(2 * ell_n));
     NEO_CK(ctx, cudaMemcpyAsync(dbits.p, o->beta_r.data(), ell_n * 16, cudaMemcpyHostToDevice, ctx->stream));
     if ((rc = launch_chi_table(ctx, dbits.p, ell_n, S))) return rc;
-    DevBuf<uint64_t> z1;
-    NEO_CK(ctx, z1.alloc(m));
+    DevBuf<uint64_t>& z1 = o->ws_z1;
+    NEO_CK(ctx, z1.ensure(m));
     z1_kernel<<<ceil_div(m, 256), 256, 0, ctx->stream>>>(o->Z, m, b, z1.p);
     NEO_LAUNCHED(ctx);
     for (int v = 0; v < o->n_fvar; v++) {
@@ -753,11 +770,11 @@ static int oracle_init(neo_gpu_ctx* ctx, neo_gpu_ccs_oracle* o, const int8_t* d_
             g = gl::kmul(g, o->gamma);
         }
     }
-    NEO_CK(ctx, o->wg.alloc(nq));
+    NEO_CK(ctx, o->wg.ensure(nq));
     NEO_CK(ctx, cudaMemcpyAsync(o->wg.p, wg.data(), nq * 16, cudaMemcpyHostToDevice, ctx->stream));
     if (o->has_eval) {
-        NEO_CK(ctx, cudaMemcpyAsync(dbits.p, o->r_in.data(), ell_n * 16, cudaMemcpyHostToDevice, ctx->stream));
-        if ((rc = launch_chi_table(ctx, dbits.p, ell_n, S + (size_t)o->idx_eqrin * n_pad))) return rc;
+        NEO_CK(ctx, cudaMemcpyAsync(dbits.p + ell_n, o->r_in.data(), ell_n * 16, cudaMemcpyHostToDevice, ctx->stream));
+        if ((rc = launch_chi_table(ctx, dbits.p + ell_n, ell_n, S + (size_t)o->idx_eqrin * n_pad))) return rc;
         // w[i*54+rho] = gamma^i chi_alpha[rho]
         std::vector<K> w((size_t)nq), coef(t);
         K gi = gl::kone();
@@ -767,19 +784,21 @@ static int oracle_init(neo_gpu_ctx* ctx, neo_gpu_ccs_oracle* o, const int8_t* d_
         }
         K gkj = gl::kone();
         for (uint32_t j = 0; j < t; j++) { coef[j] = gkj; gkj = gl::kmul(gkj, o->gamma_to_k); }
-        DevBuf<K> dw, dcoef, du;
-        NEO_CK(ctx, dw.alloc(nq));
-        NEO_CK(ctx, dcoef.alloc(t));
-        NEO_CK(ctx, du.alloc(m));
+        DevBuf<K>& dw = o->ws_w;
+        DevBuf<K>& dcoef = o->ws_coef;
+        DevBuf<K>& du = o->ws_u;
+        NEO_CK(ctx, dw.ensure(nq));
+        NEO_CK(ctx, dcoef.ensure(t));
+        NEO_CK(ctx, du.ensure(m));
         NEO_CK(ctx, cudaMemcpyAsync(dw.p, w.data(), nq * 16, cudaMemcpyHostToDevice, ctx->stream));
         NEO_CK(ctx, cudaMemcpyAsync(dcoef.p, coef.data(), t * 16, cudaMemcpyHostToDevice, ctx->stream));
         eval_u_kernel<<<ceil_div(m, 256), 256, 0, ctx->stream>>>(o->Z, m, k, dw.p, du.p);
         NEO_LAUNCHED(ctx);
-        DevBuf<uint8_t> isid;
-        NEO_CK(ctx, isid.alloc(t));
+        DevBuf<uint8_t>& isid = o->ws_isid;
+        NEO_CK(ctx, isid.ensure(t));
         NEO_CK(ctx, cudaMemcpyAsync(isid.p, o->ccs->is_identity.data(), t, cudaMemcpyHostToDevice, ctx->stream));
-        DevBuf<uint64_t> nnzoff;
-        NEO_CK(ctx, nnzoff.alloc(t + 1));
+        DevBuf<uint64_t>& nnzoff = o->ws_nnzoff;
+        NEO_CK(ctx, nnzoff.ensure(t + 1));
         NEO_CK(ctx, cudaMemcpyAsync(nnzoff.p, o->ccs->nnz_off.data(), (t + 1) * 8, cudaMemcpyHostToDevice, ctx->stream));
         eval_tbl_kernel<<<ceil_div(n_pad, 256), 256, 0, ctx->stream>>>(
             o->ccs->csr_ptr.p, o->ccs->csr_col.p, o->ccs->csr_val.p, nnzoff.p, isid.p, t, desc->n, desc->m, du.p,
@@ -791,14 +810,14 @@ static int oracle_init(neo_gpu_ctx* ctx, neo_gpu_ccs_oracle* o, const int8_t* d_
     o->J = (int)std::min<uint32_t>(JMAX, ell_n - 1);
     if ((uint32_t)o->J < ell_n - 1) {
         uint64_t LJ = n_pad >> o->J;
-        NEO_CK(ctx, o->nc[0].alloc((size_t)nq * LJ));
-        NEO_CK(ctx, o->nc[1].alloc((size_t)nq * LJ / 2 + 1));
+        NEO_CK(ctx, o->nc[0].ensure((size_t)nq * LJ));
+        NEO_CK(ctx, o->nc[1].ensure((size_t)nq * LJ / 2 + 1));
     }
-    NEO_CK(ctx, o->eqw.alloc(1 << JMAX));
+    NEO_CK(ctx, o->eqw.ensure(1 << JMAX));
     uint64_t max_blocks = (uint64_t)ceil_div(n_pad / 2, RT) * nq + 16;
-    NEO_CK(ctx, o->partials.alloc(max_blocks * (o->deg_max + 1)));
-    NEO_CK(ctx, o->coeffs.alloc(MAX_DEG + 1));
-    NEO_CK(ctx, o->ys.alloc(16));
+    NEO_CK(ctx, o->partials.ensure(max_blocks * (o->deg_max + 1)));
+    NEO_CK(ctx, o->coeffs.ensure(MAX_DEG + 1));
+    NEO_CK(ctx, o->ys.ensure(16));
     NEO_CK(ctx, cudaStreamSynchronize(ctx->stream));
     return NEO_OK;
 }
@@ -899,12 +918,12 @@ static int row_round(neo_gpu_ccs_oracle* o) {
 
 static int ajtai_precompute(neo_gpu_ccs_oracle* o) {
     neo_gpu_ctx* ctx = o->ctx;
-    NEO_CK(ctx, o->chi_r.alloc(o->n_pad));
-    NEO_CK(ctx, o->vj.alloc((size_t)o->t * o->m));
-    NEO_CK(ctx, o->y_eval.alloc((size_t)o->k * o->t * NEO_D));
-    NEO_CK(ctx, o->y_sc.alloc((size_t)o->k * o->t));
-    DevBuf<K> dbits;
-    NEO_CK(ctx, dbits.alloc(o->ell_n));
+    NEO_CK(ctx, o->chi_r.ensure(o->n_pad));
+    NEO_CK(ctx, o->vj.ensure((size_t)o->t * o->m));
+    NEO_CK(ctx, o->y_eval.ensure((size_t)o->k * o->t * NEO_D));
+    NEO_CK(ctx, o->y_sc.ensure((size_t)o->k * o->t));
+    DevBuf<K>& dbits = o->ws_bits;
+    NEO_CK(ctx, dbits.ensure(2 * o->ell_n));
     NEO_CK(ctx, cudaMemcpyAsync(dbits.p, o->row_chals.data(), o->ell_n * 16, cudaMemcpyHostToDevice, ctx->stream));
     int rc = launch_chi_table(ctx, dbits.p, o->ell_n, o->chi_r.p);
     if (rc) return rc;

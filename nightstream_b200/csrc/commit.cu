@@ -83,17 +83,30 @@ __global__ void commit_reduce_kernel(const uint64_t* __restrict__ partial, uint3
 
 }  // namespace
 
+// PP registry: one entry per (device, m), shared by all contexts
+#include <map>
+#include <mutex>
+static std::mutex g_pp_mu;
+static std::map<std::pair<int, uint64_t>, PPEntry*> g_pp;
+
+PPEntry* pp_lookup(int device, uint64_t m) {
+    std::lock_guard<std::mutex> lk(g_pp_mu);
+    auto it = g_pp.find({device, m});
+    return it == g_pp.end() ? nullptr : it->second;
+}
+
 int launch_commit(neo_gpu_ctx* ctx, const int8_t* d_digits, uint32_t n_vec, uint64_t m, uint64_t* d_out) {
-    if (!ctx->d_pp || ctx->pp_m != m) return ctx->fail(NEO_ERR_ARG, "commit: PP not loaded for this m");
-    if (ctx->d_pp_limbs) {
+    PPEntry* pp = pp_lookup(ctx->device, m);
+    if (!pp) return ctx->fail(NEO_ERR_ARG, "commit: PP not loaded for this m");
+    if (pp->d_pp_limbs) {
         // tensor-core path (commit_tc.cu)
         uint32_t g, k, kb;
         size_t need = tc_scratch_bytes(n_vec, m, &g, &k, &kb);
         void* scratch = nullptr;
         NEO_CK(ctx, ctx_scratch(ctx, need, &scratch));
-        return launch_commit_tc(ctx, d_digits, n_vec, m, d_out, (uint8_t*)scratch, ctx->d_err);
+        return launch_commit_tc(ctx, pp, d_digits, n_vec, d_out, (uint8_t*)scratch, ctx->d_err);
     }
-    const uint32_t kappa = ctx->kappa;
+    const uint32_t kappa = pp->kappa;
     // pick a chunking that fills the GPU: ~4 blocks per SM in total
     uint32_t target_blocks = 148 * 8;
     uint32_t per = (uint32_t)((uint64_t)kappa * n_vec);
@@ -104,7 +117,7 @@ int launch_commit(neo_gpu_ctx* ctx, const int8_t* d_digits, uint32_t n_vec, uint
     uint64_t* partial = nullptr;
     NEO_CK(ctx, ctx_scratch(ctx, (size_t)n_vec * n_chunks * kappa * 81 * 8, (void**)&partial));
     dim3 grid(n_chunks, kappa, n_vec);
-    commit_partial_kernel<<<grid, COMMIT_THREADS, 0, ctx->stream>>>(ctx->d_pp, kappa, m, d_digits,
+    commit_partial_kernel<<<grid, COMMIT_THREADS, 0, ctx->stream>>>(pp->d_pp, kappa, m, d_digits,
                                                                      (uint32_t)cols_per_block, partial);
     NEO_LAUNCHED(ctx);
     commit_reduce_kernel<<<n_vec * kappa, 96, 0, ctx->stream>>>(partial, n_chunks, kappa, n_vec, d_out);
@@ -116,15 +129,23 @@ extern "C" int neo_gpu_pp_upload(neo_gpu_ctx* ctx, uint32_t kappa, uint64_t m, c
     if (!ctx) return NEO_ERR_ARG;
     if (!coeffs || kappa == 0 || m == 0 || kappa > 64) return ctx->fail(NEO_ERR_ARG, "pp_upload: bad args");
     cudaSetDevice(ctx->device);
-    if (ctx->d_pp) { cudaFree(ctx->d_pp); ctx->d_pp = nullptr; }
-    size_t n = (size_t)kappa * m * NEO_D;
-    NEO_CK(ctx, cudaMalloc(&ctx->d_pp, n * 8));
-    NEO_CK(ctx, cudaMemcpy(ctx->d_pp, coeffs, n * 8, cudaMemcpyHostToDevice));
-    ctx->kappa = kappa;
-    ctx->pp_m = m;
-    if (ctx->d_pp_limbs) { cudaFree(ctx->d_pp_limbs); ctx->d_pp_limbs = nullptr; }
+    NEO_CK(ctx, cudaStreamSynchronize(ctx->stream));
+    std::lock_guard<std::mutex> lk(g_pp_mu);  // uploads are serialized; replacing a PP in use races (documented)
+    PPEntry*& slot = g_pp[{ctx->device, m}];
+    if (!slot) {
+        slot = new PPEntry();
+        slot->device = ctx->device;
+        slot->m = m;
+    }
+    PPEntry* pp = slot;
+    const size_t n = (size_t)kappa * m * NEO_D;
+    if (pp->d_pp && pp->kappa != kappa) { cudaFree(pp->d_pp); pp->d_pp = nullptr; }
+    if (!pp->d_pp) NEO_CK(ctx, cudaMalloc(&pp->d_pp, n * 8));
+    NEO_CK(ctx, cudaMemcpy(pp->d_pp, coeffs, n * 8, cudaMemcpyHostToDevice));
+    pp->kappa = kappa;
+    if (pp->d_pp_limbs) { cudaFree(pp->d_pp_limbs); pp->d_pp_limbs = nullptr; }
     // tensor-core layout of the PP (byte limbs, pre-swizzled tiles) when the shape allows it
-    if (kappa <= 16 && m % 2 == 0) return tc_pp_prepare(ctx);
+    if (kappa <= 16 && m % 2 == 0) return tc_pp_prepare(ctx, pp);
     return NEO_OK;
 }
 
@@ -132,10 +153,12 @@ extern "C" int neo_gpu_commit(neo_gpu_ctx* ctx, const int8_t* digits, uint32_t n
     if (!ctx) return NEO_ERR_ARG;
     if (!digits || !out || n_vec == 0 || m == 0) return ctx->fail(NEO_ERR_ARG, "commit: bad args");
     cudaSetDevice(ctx->device);
+    PPEntry* pp = pp_lookup(ctx->device, m);
+    if (!pp) return ctx->fail(NEO_ERR_ARG, "commit: PP not loaded for this m");
     DevBuf<int8_t> dZ;
     DevBuf<uint64_t> dout;
     NEO_CK(ctx, dZ.alloc((size_t)n_vec * NEO_D * m));
-    NEO_CK(ctx, dout.alloc((size_t)n_vec * ctx->kappa * NEO_D));
+    NEO_CK(ctx, dout.alloc((size_t)n_vec * pp->kappa * NEO_D));
     NEO_CK(ctx, cudaMemcpyAsync(dZ.p, digits, dZ.bytes(), cudaMemcpyHostToDevice, ctx->stream));
     int rc = launch_commit(ctx, dZ.p, n_vec, m, dout.p);
     if (rc) return rc;
@@ -181,9 +204,10 @@ extern "C" int neo_gpu_commit_noalloc(neo_gpu_ctx* ctx, const int8_t* d_digits, 
                                       uint64_t* d_out) {
     if (!ctx) return NEO_ERR_ARG;
     if (!d_digits || !d_out || n_vec == 0 || m == 0) return ctx->fail(NEO_ERR_ARG, "commit_noalloc: bad args");
-    if (!ctx->d_pp || ctx->pp_m != m) return ctx->fail(NEO_ERR_ARG, "commit_noalloc: PP not loaded for this m");
+    PPEntry* pp = pp_lookup(ctx->device, m);
+    if (!pp) return ctx->fail(NEO_ERR_ARG, "commit_noalloc: PP not loaded for this m");
     if (ctx->device < 0 || ctx->device >= NOALLOC_MAX_DEVICES) return ctx->fail(NEO_ERR_UNSUPPORTED, "commit_noalloc: device index");
-    const uint32_t kappa = ctx->kappa;
+    const uint32_t kappa = pp->kappa;
     const uint64_t per_chunk = (uint64_t)n_vec * kappa * 81;  // partial words needed per column chunk
     if (per_chunk > NOALLOC_SCRATCH_WORDS)
         return ctx->fail(NEO_ERR_ARG,
@@ -215,7 +239,7 @@ extern "C" int neo_gpu_commit_noalloc(neo_gpu_ctx* ctx, const int8_t* d_digits, 
     dim3 grid((uint32_t)n_chunks, kappa, n_vec);
     // every partial word a reduce reads is written by commit_partial_kernel first,
     // so the array needs no clearing between calls
-    commit_partial_kernel<<<grid, COMMIT_THREADS, 0, ctx->stream>>>(ctx->d_pp, kappa, m, d_digits,
+    commit_partial_kernel<<<grid, COMMIT_THREADS, 0, ctx->stream>>>(pp->d_pp, kappa, m, d_digits,
                                                                      (uint32_t)cols_per_block, scratch);
     NEO_LAUNCHED(ctx);
     commit_reduce_kernel<<<n_vec * kappa, 96, 0, ctx->stream>>>(scratch, (uint32_t)n_chunks, kappa, n_vec, d_out);

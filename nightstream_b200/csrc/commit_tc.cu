@@ -29,18 +29,20 @@ constexpr int TC_NV = 4;                    // vectors per CTA
 constexpr int TC_NROWS = TC_NV * 81;        // 324 B rows used
 constexpr int TC_NPAD = 336;                // MMA N total (multiple of 16, atoms of 8)
 constexpr int TC_N0 = 256, TC_N1 = TC_NPAD - 256;  // two MMAs per K step
-constexpr int TC_STAGES = 3;
+constexpr int TC_ASTAGES = 6;               // A tiles + F sequences ring (bulk copies run ahead)
+constexpr int TC_BSTAGES = 2;               // B tiles ring (built by threads, overlaps MMA)
 constexpr int TC_A_BYTES = 128 * 128;       // 16 KB
 constexpr int TC_B_BYTES = TC_NPAD * 128;   // 42 KB
 constexpr int TC_FBYTES = 144;              // F sequence length (9 x 16 B)
 constexpr int TC_F_STAGE = 1280;            // NV x 2 columns x 144 B, padded (window reads overrun by 4 B)
-constexpr int TC_STAGE_BYTES = TC_A_BYTES + TC_B_BYTES + TC_F_STAGE;
+constexpr int TC_SMEM_BYTES = TC_ASTAGES * (TC_A_BYTES + TC_F_STAGE) + TC_BSTAGES * TC_B_BYTES;
 constexpr int TC_BUILDERS = 256;            // 8 builder warps
 constexpr int TC_THREADS = 64 + TC_BUILDERS;  // warp0 producer, warp1 MMA, warps2-9 B build (2-5 epilogue)
 constexpr int TC_MAX_KB = 512;              // K blocks per CTA (int32 overflow bound)
 constexpr uint32_t TC_SPIN_LIMIT = 1u << 22;  // ~0.3 s with the back-off below
 
 static_assert(TC_B_BYTES % 1024 == 0 && TC_A_BYTES % 1024 == 0, "stage buffers stay 1024-byte aligned");
+static_assert(TC_SMEM_BYTES + 1024 + 256 <= 232448, "shared memory budget");
 static_assert(TC_NV * 2 * TC_FBYTES + 16 <= TC_F_STAGE, "F staging holds the window overrun");
 static_assert(TC_NPAD % 16 == 0 && TC_N1 % 16 == 0 && TC_N1 >= 16, "MMA N constraints (M=128)");
 
@@ -181,17 +183,18 @@ struct TcArgs {
 
 __global__ void __launch_bounds__(TC_THREADS, 1) commit_tc_kernel(const TcArgs a) {
     extern __shared__ __align__(1024) uint8_t smem_raw[];
-    // 1024-align the stage buffers (dynamic smem base alignment is not guaranteed)
+    // 1024-align the tile buffers (dynamic smem base alignment is not guaranteed)
     uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
-    uint8_t* sA = smem;                                   // [STAGES][16 KB]
-    uint8_t* sB = smem + TC_STAGES * TC_A_BYTES;          // [STAGES][42 KB]
-    uint8_t* sF = sB + TC_STAGES * TC_B_BYTES;            // [STAGES][1280 B] F sequences of the stage
-    uint64_t* bars = reinterpret_cast<uint64_t*>(sF + TC_STAGES * TC_F_STAGE);
-    uint64_t* full_a = bars;                  // [STAGES]
-    uint64_t* full_b = bars + TC_STAGES;      // [STAGES]
-    uint64_t* empty = bars + 2 * TC_STAGES;   // [STAGES]
-    uint64_t* done = bars + 3 * TC_STAGES;    // [1]
-    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 3 * TC_STAGES + 1);
+    uint8_t* sA = smem;                                        // [ASTAGES][16 KB]
+    uint8_t* sB = sA + TC_ASTAGES * TC_A_BYTES;                // [BSTAGES][42 KB]
+    uint8_t* sF = sB + TC_BSTAGES * TC_B_BYTES;                // [ASTAGES][1280 B]
+    uint64_t* bars = reinterpret_cast<uint64_t*>(sF + TC_ASTAGES * TC_F_STAGE);
+    uint64_t* full_a = bars;                                   // [ASTAGES] A tile + F landed
+    uint64_t* empty_a = bars + TC_ASTAGES;                     // [ASTAGES] MMAs done reading the A tile
+    uint64_t* full_b = bars + 2 * TC_ASTAGES;                  // [BSTAGES] B tile built
+    uint64_t* empty_b = full_b + TC_BSTAGES;                   // [BSTAGES] MMAs done reading the B tile
+    uint64_t* done = empty_b + TC_BSTAGES;                     // [1]
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(done + 1);
     __shared__ int s_abort;
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -204,16 +207,19 @@ __global__ void __launch_bounds__(TC_THREADS, 1) commit_tc_kernel(const TcArgs a
 
     if (threadIdx.x == 0) {
         s_abort = 0;
-        for (int s = 0; s < TC_STAGES; s++) {
+        for (int s = 0; s < TC_ASTAGES; s++) {
             mbar_init(&full_a[s], 1);
+            mbar_init(&empty_a[s], 1);
+        }
+        for (int s = 0; s < TC_BSTAGES; s++) {
             mbar_init(&full_b[s], TC_BUILDERS / 32);
-            mbar_init(&empty[s], 1);
+            mbar_init(&empty_b[s], 1);
         }
         mbar_init(done, 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     // zero the padding rows of every B stage once (never rewritten)
-    for (int s = 0; s < TC_STAGES; s++)
+    for (int s = 0; s < TC_BSTAGES; s++)
         for (int x = threadIdx.x; x < (TC_NPAD - TC_NROWS) * 8; x += blockDim.x) {
             int row = TC_NROWS + x / 8, c = x % 8;
             *reinterpret_cast<uint4*>(sB + s * TC_B_BYTES + (row >> 3) * 1024 + (row & 7) * 128 + c * 16) = make_uint4(0, 0, 0, 0);
@@ -228,12 +234,12 @@ __global__ void __launch_bounds__(TC_THREADS, 1) commit_tc_kernel(const TcArgs a
     const uint32_t tmem = *tmem_slot;
 
     if (warp == 0) {
-        // ---- producer: A tiles ----
+        // ---- producer: A tiles and F sequences ----
         if (lane == 0) {
             for (uint32_t it = 0; it < nkb; it++) {
-                const int s = it % TC_STAGES;
-                const uint32_t ph = (it / TC_STAGES) & 1;
-                if (it >= TC_STAGES && !mbar_wait(&empty[s], ph ^ 1)) { atomicOr(a.err, 1u); s_abort = 1; break; }
+                const int s = it % TC_ASTAGES;
+                const uint32_t ph = (it / TC_ASTAGES) & 1;
+                if (it >= TC_ASTAGES && !mbar_wait(&empty_a[s], ph ^ 1)) { atomicOr(a.err, 1u); s_abort = 1; break; }
                 if (s_abort) break;
                 const uint64_t kb = kb0 + it;
                 mbar_expect_tx(&full_a[s], TC_A_BYTES + nvalid * 2 * TC_FBYTES);
@@ -249,11 +255,14 @@ __global__ void __launch_bounds__(TC_THREADS, 1) commit_tc_kernel(const TcArgs a
         if (lane == 0) {
             const uint32_t id0 = idesc_i8(TC_N0), id1 = idesc_i8(TC_N1);
             for (uint32_t it = 0; it < nkb; it++) {
-                const int s = it % TC_STAGES;
-                const uint32_t ph = (it / TC_STAGES) & 1;
-                if (!mbar_wait(&full_a[s], ph) || !mbar_wait(&full_b[s], ph)) { atomicOr(a.err, 2u); s_abort = 1; break; }
+                const int sa = it % TC_ASTAGES, sb = it % TC_BSTAGES;
+                if (!mbar_wait(&full_a[sa], (it / TC_ASTAGES) & 1) || !mbar_wait(&full_b[sb], (it / TC_BSTAGES) & 1)) {
+                    atomicOr(a.err, 2u);
+                    s_abort = 1;
+                    break;
+                }
                 asm volatile("tcgen05.fence::after_thread_sync;");
-                const uint32_t a0 = smem_u32(sA + s * TC_A_BYTES), b0 = smem_u32(sB + s * TC_B_BYTES);
+                const uint32_t a0 = smem_u32(sA + sa * TC_A_BYTES), b0 = smem_u32(sB + sb * TC_B_BYTES);
 #pragma unroll
                 for (int k = 0; k < 4; k++) {  // 4 x 32-byte K steps inside the 128-byte swizzle atom
                     const uint64_t ad = sw128_desc(a0 + 32 * k);
@@ -261,7 +270,8 @@ __global__ void __launch_bounds__(TC_THREADS, 1) commit_tc_kernel(const TcArgs a
                     mma_i8(tmem, ad, sw128_desc(b0 + 32 * k), id0, acc);
                     mma_i8(tmem + TC_N0, ad, sw128_desc(b0 + (TC_N0 / 8) * 1024 + 32 * k), id1, acc);
                 }
-                mma_commit(&empty[s]);  // stage free once these MMAs complete
+                mma_commit(&empty_a[sa]);  // tiles free once these MMAs complete
+                mma_commit(&empty_b[sb]);
             }
             mma_commit(done);
         }
@@ -269,13 +279,17 @@ __global__ void __launch_bounds__(TC_THREADS, 1) commit_tc_kernel(const TcArgs a
         // ---- B builders (warps 2..9) ----
         const int bt = threadIdx.x - 64;
         for (uint32_t it = 0; it < nkb; it++) {
-            const int s = it % TC_STAGES;
-            const uint32_t ph = (it / TC_STAGES) & 1;
-            // the stage's A tile and F sequences have landed (which also means the stage is free)
-            if (!mbar_wait(&full_a[s], ph)) { atomicOr(a.err, 4u); s_abort = 1; break; }
+            const int sa = it % TC_ASTAGES, sb = it % TC_BSTAGES;
+            // F of this K block has landed, and the MMAs of K block it-2 released the B buffer
+            if (!mbar_wait(&full_a[sa], (it / TC_ASTAGES) & 1) ||
+                (it >= TC_BSTAGES && !mbar_wait(&empty_b[sb], ((it / TC_BSTAGES) & 1) ^ 1))) {
+                atomicOr(a.err, 4u);
+                s_abort = 1;
+                break;
+            }
             if (s_abort) break;
-            uint8_t* dstB = sB + s * TC_B_BYTES;
-            const uint8_t* srcF = sF + s * TC_F_STAGE;
+            uint8_t* dstB = sB + sb * TC_B_BYTES;
+            const uint8_t* srcF = sF + sa * TC_F_STAGE;
             for (int task = bt; task < TC_NROWS * 2; task += TC_BUILDERS) {
                 const int half = task & 1, row = task >> 1;
                 const int vl = row / 81, r = row - vl * 81;
@@ -304,7 +318,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1) commit_tc_kernel(const TcArgs a
             }
             asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
             __syncwarp();
-            if (lane == 0) mbar_arrive(&full_b[s]);
+            if (lane == 0) mbar_arrive(&full_b[sb]);
         }
         // ---- epilogue (warps 2..5 cover TMEM lane groups 2, 3, 0, 1): TMEM -> int32 partials ----
         bool ok = nkb > 0 && !s_abort && mbar_wait(done, 0);
@@ -368,14 +382,14 @@ __global__ void commit_tc_reduce_kernel(const int32_t* __restrict__ partial, uin
 }  // namespace
 
 // ---------------------------------------------------------------------------
-int tc_pp_prepare(neo_gpu_ctx* ctx) {
-    if (ctx->kappa * 8 > 128) return ctx->fail(NEO_ERR_UNSUPPORTED, "tensor-core commit: kappa <= 16");
-    if (ctx->pp_m % 2) return ctx->fail(NEO_ERR_UNSUPPORTED, "tensor-core commit: m must be even");
-    if (ctx->d_pp_limbs) { cudaFree(ctx->d_pp_limbs); ctx->d_pp_limbs = nullptr; }
-    const uint64_t n_kb = ctx->pp_m / 2;
-    NEO_CK(ctx, cudaMalloc(&ctx->d_pp_limbs, n_kb * TC_A_BYTES));
+int tc_pp_prepare(neo_gpu_ctx* ctx, PPEntry* pp) {
+    if (pp->kappa * 8 > 128) return ctx->fail(NEO_ERR_UNSUPPORTED, "tensor-core commit: kappa <= 16");
+    if (pp->m % 2) return ctx->fail(NEO_ERR_UNSUPPORTED, "tensor-core commit: m must be even");
+    if (pp->d_pp_limbs) { cudaFree(pp->d_pp_limbs); pp->d_pp_limbs = nullptr; }
+    const uint64_t n_kb = pp->m / 2;
+    NEO_CK(ctx, cudaMalloc(&pp->d_pp_limbs, n_kb * TC_A_BYTES));
     const uint64_t threads = n_kb * 128 * 8;
-    pp_limbs_kernel<<<ceil_div(threads, 256), 256, 0, ctx->stream>>>(ctx->d_pp, ctx->kappa, ctx->pp_m, ctx->d_pp_limbs);
+    pp_limbs_kernel<<<ceil_div(threads, 256), 256, 0, ctx->stream>>>(pp->d_pp, pp->kappa, pp->m, pp->d_pp_limbs);
     NEO_LAUNCHED(ctx);
     NEO_CK(ctx, cudaStreamSynchronize(ctx->stream));
     return NEO_OK;
@@ -388,7 +402,8 @@ size_t tc_scratch_bytes(uint32_t n_vec, uint64_t m, uint32_t* n_groups_out, uint
     // fill whole waves of 148 SMs (1 CTA per SM), at most TC_MAX_KB K blocks per CTA
     uint32_t waves = 1, n_ksplit;
     for (;; waves++) {
-        n_ksplit = (148 * waves + n_groups - 1) / n_groups;
+        n_ksplit = (148 * waves) / n_groups;  // n_groups * n_ksplit <= whole waves of 148 CTAs
+        if (n_ksplit == 0) n_ksplit = 1;
         if (n_ksplit > n_kb) n_ksplit = n_kb;
         if ((n_kb + n_ksplit - 1) / n_ksplit <= TC_MAX_KB) break;
     }
@@ -402,8 +417,9 @@ size_t tc_scratch_bytes(uint32_t n_vec, uint64_t m, uint32_t* n_groups_out, uint
     return ((f_bytes + 255) & ~size_t(255)) + p_bytes + 256;
 }
 
-int launch_commit_tc(neo_gpu_ctx* ctx, const int8_t* d_digits, uint32_t n_vec, uint64_t m, uint64_t* d_out,
+int launch_commit_tc(neo_gpu_ctx* ctx, const PPEntry* pp, const int8_t* d_digits, uint32_t n_vec, uint64_t* d_out,
                      uint8_t* scratch, uint32_t* d_err) {
+    const uint64_t m = pp->m;
     uint32_t n_groups, n_ksplit, kb_per_cta;
     tc_scratch_bytes(n_vec, m, &n_groups, &n_ksplit, &kb_per_cta);
     uint8_t* F = scratch;
@@ -411,7 +427,7 @@ int launch_commit_tc(neo_gpu_ctx* ctx, const int8_t* d_digits, uint32_t n_vec, u
     f_seq_kernel<<<ceil_div((uint64_t)n_vec * m, 128), 128, 0, ctx->stream>>>(d_digits, n_vec, m, F);
     NEO_LAUNCHED(ctx);
     TcArgs a;
-    a.ppl = ctx->d_pp_limbs;
+    a.ppl = pp->d_pp_limbs;
     a.F = F;
     a.partial = partial;
     a.err = d_err;
@@ -421,12 +437,11 @@ int launch_commit_tc(neo_gpu_ctx* ctx, const int8_t* d_digits, uint32_t n_vec, u
     a.n_ksplit = n_ksplit;
     a.kb_per_cta = kb_per_cta;
     a.n_kb = (uint32_t)(m / 2);
-    const size_t smem = TC_STAGES * TC_STAGE_BYTES + 1024 /*align*/ + 256 /*barriers*/;
-    static_assert(TC_STAGES * TC_STAGE_BYTES + 1024 + 256 <= 232448, "shared memory budget");
+    const size_t smem = TC_SMEM_BYTES + 1024 /*align*/ + 256 /*barriers*/;
     NEO_CK(ctx, cudaFuncSetAttribute(commit_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     commit_tc_kernel<<<n_groups * n_ksplit, TC_THREADS, smem, ctx->stream>>>(a);
     NEO_LAUNCHED(ctx);
-    commit_tc_reduce_kernel<<<n_vec * ctx->kappa, 96, 0, ctx->stream>>>(partial, n_groups, n_ksplit, ctx->kappa, n_vec,
+    commit_tc_reduce_kernel<<<n_vec * pp->kappa, 96, 0, ctx->stream>>>(partial, n_groups, n_ksplit, pp->kappa, n_vec,
                                                                         d_out);
     NEO_LAUNCHED(ctx);
     return NEO_OK;

@@ -31,8 +31,6 @@ extern "C" int neo_gpu_ctx_destroy(neo_gpu_ctx* ctx) {
     if (!ctx) return NEO_ERR_ARG;
     cudaSetDevice(ctx->device);
     cudaStreamSynchronize(ctx->stream);
-    if (ctx->d_pp) cudaFree(ctx->d_pp);
-    if (ctx->d_pp_limbs) cudaFree(ctx->d_pp_limbs);
     if (ctx->scratch) cudaFree(ctx->scratch);
     if (ctx->d_err) cudaFree(ctx->d_err);
     cudaStreamDestroy(ctx->stream);

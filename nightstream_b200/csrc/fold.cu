@@ -110,6 +110,7 @@ __global__ void __launch_bounds__(256) child_y_kernel(const int8_t* __restrict__
 struct neo_gpu_shard {
     neo_gpu_ctx* ctx = nullptr;
     DevCcs ccs;
+    uint32_t kappa = 16;
     uint32_t n = 0, m32 = 0, t = 0, ell_n = 0, ell_d = 6, d_sc = 6, k_rho = 12, b = 2, m_in = 1, lambda = 127;
     uint64_t m = 0;
     int64_t slack_bits = 0;
@@ -123,6 +124,7 @@ struct neo_gpu_shard {
     DevBuf<int8_t> d_rot;
     DevBuf<uint32_t> d_flags;
     DevBuf<K> d_ychild;
+    neo_gpu_ccs_oracle* orc = nullptr;  // Pi_CCS oracle workspace reused across steps
     std::vector<uint64_t> proof;  // canonical dump of the last step
     double stats[12] = {0};       // host ms per phase of the last step, see neo_gpu_shard_step_stats
 };
@@ -218,7 +220,8 @@ extern "C" int neo_gpu_shard_create(neo_gpu_ctx* ctx, const neo_ccs_desc* desc, 
     *out = nullptr;
     if (desc->n != desc->m || desc->n < 2 || (desc->n & (desc->n - 1)))
         return ctx->fail(NEO_ERR_UNSUPPORTED, "shard_create: requires n == m == power of two");
-    if (!ctx->d_pp || ctx->pp_m != desc->m) return ctx->fail(NEO_ERR_ARG, "shard_create: upload PP for this m first");
+    PPEntry* pp = pp_lookup(ctx->device, desc->m);
+    if (!pp) return ctx->fail(NEO_ERR_ARG, "shard_create: upload PP for this m first");
     if (k_rho == 0 || k_rho > 17 || m_in == 0 || m_in > desc->m) return ctx->fail(NEO_ERR_ARG, "shard_create: k_rho/m_in");
     cudaSetDevice(ctx->device);
     auto* sh = new neo_gpu_shard();
@@ -227,6 +230,7 @@ extern "C" int neo_gpu_shard_create(neo_gpu_ctx* ctx, const neo_ccs_desc* desc, 
     int rc = dev_ccs_upload(ctx, desc, sh->ccs);
     if (rc) return rc;
     sh->n = desc->n; sh->m = desc->m; sh->m32 = desc->m; sh->t = desc->t; sh->m_in = m_in; sh->k_rho = k_rho;
+    sh->kappa = pp->kappa;
     if (sh->t > 4) return ctx->fail(NEO_ERR_UNSUPPORTED, "shard_create: t <= 4 supported by the fold step");
     while ((1u << sh->ell_n) < sh->n) sh->ell_n++;
     int fdeg = 0;
@@ -244,10 +248,10 @@ extern "C" int neo_gpu_shard_create(neo_gpu_ctx* ctx, const neo_ccs_desc* desc, 
     NEO_CK(ctx, sh->d_z.alloc(m));
     NEO_CK(ctx, sh->d_mix.alloc((size_t)NEO_D * m));
     NEO_CK(ctx, sh->d_rot.alloc((size_t)(1 + k_rho) * NEO_D * NEO_D));
-    NEO_CK(ctx, sh->d_commits.alloc((size_t)(1 + k_rho) * ctx->kappa * NEO_D));
+    NEO_CK(ctx, sh->d_commits.alloc((size_t)(1 + k_rho) * sh->kappa * NEO_D));
     NEO_CK(ctx, sh->d_flags.alloc(2));
     NEO_CK(ctx, sh->d_ychild.alloc((size_t)k_rho * sh->t * NEO_D));
-    size_t mixv = (size_t)(1 + k_rho) * std::max<uint32_t>(ctx->kappa, 2 * sh->t + m_in) * NEO_D * 2;
+    size_t mixv = (size_t)(1 + k_rho) * std::max<uint32_t>(sh->kappa, 2 * sh->t + m_in) * NEO_D * 2;
     NEO_CK(ctx, sh->d_mixv.alloc(mixv));
     NEO_CK(ctx, sh->d_mixo.alloc(mixv));
     *out = guard.release();
@@ -258,6 +262,7 @@ extern "C" int neo_gpu_shard_destroy(neo_gpu_shard* sh) {
     if (!sh) return NEO_ERR_ARG;
     cudaSetDevice(sh->ctx->device);
     cudaStreamSynchronize(sh->ctx->stream);
+    if (sh->orc) neo_gpu_ccs_oracle_destroy(sh->orc);
     delete sh;
     return NEO_OK;
 }
@@ -327,7 +332,7 @@ static int fold_step_impl(neo_gpu_shard* sh, const uint64_t* z_host, const uint6
     neo_gpu_ctx* ctx = sh->ctx;
     neo::Transcript& tr = *sh->tr;
     const uint64_t m = sh->m;
-    const uint32_t kappa = ctx->kappa, t = sh->t, ell_n = sh->ell_n, ell_d = sh->ell_d, d_sc = sh->d_sc;
+    const uint32_t kappa = sh->kappa, t = sh->t, ell_n = sh->ell_n, ell_d = sh->ell_d, d_sc = sh->d_sc;
     const uint32_t idx = sh->step_idx;
     const uint32_t n_acc = (uint32_t)sh->acc.size();
     const uint32_t k = 1 + n_acc;
@@ -464,13 +469,12 @@ static int fold_step_impl(neo_gpu_shard* sh, const uint64_t* z_host, const uint6
 
     sh->stats[2] = ms_since(t_ph);
     t_ph = hclock::now();
-    // ---- Pi_CCS oracle over Zall slots 0..n_acc ----
-    neo_gpu_ccs_oracle* orc = nullptr;
+    // ---- Pi_CCS oracle over Zall slots 0..n_acc (workspace reused across steps) ----
     const K* rin = n_acc ? sh->acc[0].r.data() : nullptr;
     if ((rc = ccs_oracle_create_dev(ctx, &sh->ccs, sh->Zall.p, k, sh->b, alpha.data(), beta_a.data(), beta_r.data(),
-                                    gamma, rin, ell_d, ell_n, d_sc, &orc)))
+                                    gamma, rin, ell_d, ell_n, d_sc, &sh->orc)))
         return rc;
-    std::unique_ptr<neo_gpu_ccs_oracle, int (*)(neo_gpu_ccs_oracle*)> oguard(orc, neo_gpu_ccs_oracle_destroy);
+    neo_gpu_ccs_oracle* orc = sh->orc;
 
     sh->stats[3] = ms_since(t_ph);
     t_ph = hclock::now();

@@ -17,11 +17,6 @@ struct neo_gpu_ctx {
     cudaStream_t stream = nullptr;
     std::string err;
     uint64_t launches = 0;
-    // Ajtai public parameters
-    uint32_t kappa = 0;
-    uint64_t pp_m = 0;
-    uint64_t* d_pp = nullptr;       // [kappa][m][54] canonical u64
-    uint8_t* d_pp_limbs = nullptr;  // [kappa*8][m*54] byte limbs (tensor-core layout)
     uint32_t* d_err = nullptr;       // device error word (bounded-wait timeouts); 0 = ok
     void* scratch = nullptr;         // growable per-context scratch (stream-ordered use)
     size_t scratch_bytes = 0;
@@ -53,6 +48,18 @@ struct neo_gpu_ctx {
         if (_e != cudaSuccess) return (ctx)->fail(NEO_ERR_CUDA, "kernel launch", _e); \
     } while (0)
 
+// Ajtai public parameters of one m on one device, shared by every context on
+// that device (the reference keeps one PP per (d, m) in a global registry,
+// crates/neo-ajtai/src/s_module.rs:23-222).
+struct PPEntry {
+    int device = 0;
+    uint64_t m = 0;
+    uint32_t kappa = 0;
+    uint64_t* d_pp = nullptr;       // [kappa][m][54] canonical u64
+    uint8_t* d_pp_limbs = nullptr;  // tensor-core tiles: [m/2][128 rows][128 B], pre-swizzled
+};
+PPEntry* pp_lookup(int device, uint64_t m);
+
 // Owning device buffer (freed on scope exit).
 template <typename T>
 struct DevBuf {
@@ -62,16 +69,27 @@ struct DevBuf {
     DevBuf(const DevBuf&) = delete;
     DevBuf& operator=(const DevBuf&) = delete;
     ~DevBuf() { release(); }
+    size_t cap = 0;
     cudaError_t alloc(size_t count) {
         release();
         n = count;
+        cap = count;
         if (count == 0) return cudaSuccess;
         return cudaMalloc(&p, count * sizeof(T));
+    }
+    // keep the allocation when it is large enough (reused workspaces)
+    cudaError_t ensure(size_t count) {
+        if (p && count <= cap) {
+            n = count;
+            return cudaSuccess;
+        }
+        return alloc(count);
     }
     void release() {
         if (p) cudaFree(p);
         p = nullptr;
         n = 0;
+        cap = 0;
     }
     size_t bytes() const { return n * sizeof(T); }
 };
@@ -116,9 +134,9 @@ int launch_me_y(neo_gpu_ctx* ctx, const DevCcs& ccs, const int8_t* d_Z, uint32_t
                 const gl::K* d_chi, uint32_t ell_n, uint32_t b, gl::K* d_vj_scratch, gl::K* d_y,
                 gl::K* d_ysc);
 int launch_commit(neo_gpu_ctx* ctx, const int8_t* d_digits, uint32_t n_vec, uint64_t m, uint64_t* d_out);
-int tc_pp_prepare(neo_gpu_ctx* ctx);
+int tc_pp_prepare(neo_gpu_ctx* ctx, PPEntry* pp);
 size_t tc_scratch_bytes(uint32_t n_vec, uint64_t m, uint32_t* n_groups, uint32_t* n_ksplit, uint32_t* kb_per_cta);
-int launch_commit_tc(neo_gpu_ctx* ctx, const int8_t* d_digits, uint32_t n_vec, uint64_t m, uint64_t* d_out,
+int launch_commit_tc(neo_gpu_ctx* ctx, const PPEntry* pp, const int8_t* d_digits, uint32_t n_vec, uint64_t* d_out,
                      uint8_t* scratch, uint32_t* d_err);
 // reads and clears the device error word (synchronizes the stream)
 int check_device_error(neo_gpu_ctx* ctx);
