@@ -40,6 +40,13 @@ def parse():
     ap.add_argument("--ell", type=int, default=16, help="log2 of the CCS size n = m")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--mode", default="plain", choices=["plain", "batched", "served"],
+                    help="plain: one shard; batched: 64 uneven shards batched vs one at a time; "
+                         "served: Poisson arrivals, p50/p99 latency")
+    ap.add_argument("--shards", type=int, default=64)
+    ap.add_argument("--shard-steps", type=int, default=3)
+    ap.add_argument("--workers", type=int, default=0, help="batch workers (0: min(16, host cores))")
+    ap.add_argument("--batch-in-plain", action="store_true", help="also run the batched mix in plain mode")
     return ap.parse_args()
 
 
@@ -142,6 +149,109 @@ def cpu_baseline(ell, ccs, z, pp):
     return {"value": 1.0 / dt, "unit": UNIT, "cores": os.cpu_count(), "kind": "port",
             "sample": f"one steady-state fold step (k=13) at n=m=2^{ell} on the C oracle "
                       f"(OpenMP, {os.cpu_count()} threads): {dt:.2f} s"}
+
+
+def shard_mix(n_shards, lo, hi, seed):
+    """n_shards synthetic R1CS shards with log2(n) uniform in [lo, hi]."""
+    from nightstream_b200 import synth
+    rng = np.random.default_rng(seed)
+    ells = rng.integers(lo, hi + 1, size=n_shards)
+    return [(int(ell),) + synth.make_r1cs(int(ell), seed * 1000 + i) for i, ell in enumerate(ells)]
+
+
+def upload_pps(ctx, ells):
+    for ell in sorted(set(ells)):
+        pp = np.random.default_rng(7000 + ell).integers(0, Q, size=(16, 1 << ell, 54), dtype=np.uint64)
+        ctx.pp_upload(pp)
+
+
+def run_mix(mix, shards, steps, workers):
+    """Prove every shard of the mix for `steps` fold steps on a Batch with `workers` workers."""
+    from nightstream_b200 import gpu
+    b = gpu.Batch(0, n_workers=workers)
+    t0 = time.perf_counter()
+    ids = [b.submit(ccs, z, steps, app_label=b"neo/mix-%d" % i) for i, (ell, ccs, z) in enumerate(shards)]
+    b.wait_all(3600)
+    dt = time.perf_counter() - t0
+    infos = [b.job_info(j) for j in ids]
+    launches = b.kernel_launches
+    b.close()
+    assert all(i["status"] == 1 for i in infos), [i["status"] for i in infos]
+    return dt, infos, launches
+
+
+def batched_result(args):
+    from nightstream_b200 import gpu
+    workers = args.workers or min(16, os.cpu_count() or 8)
+    shards = shard_mix(args.shards, 10, 16, 77)
+    ctx = gpu.Context(0)
+    upload_pps(ctx, [s[0] for s in shards])
+    steps = args.shard_steps
+    total_steps = steps * len(shards)
+    dt_plain, infos_plain, _ = run_mix(None, shards, steps, 1)
+    dt_b, infos_b, launches = run_mix(None, shards, steps, workers)
+    same = all(np.array_equal(a["transcript_state"], b["transcript_state"]) for a, b in zip(infos_plain, infos_b))
+    lat = sorted(i["latency_ms"] for i in infos_b)
+    ctx.close()
+    return {"value": total_steps / dt_b, "plain_value": total_steps / dt_plain, "speedup": dt_plain / dt_b,
+            "workers": workers, "shards": len(shards), "steps_per_shard": steps,
+            "sizes_log2": [s[0] for s in shards], "bit_identical_to_plain": bool(same),
+            "p50_ms": lat[len(lat) // 2], "p99_ms": lat[min(len(lat) - 1, int(0.99 * len(lat)))],
+            "gpu_launches": int(launches), "seconds": dt_b, "plain_seconds": dt_plain}
+
+
+def run_batched(args):
+    r = batched_result(args)
+    out = {"metric": METRIC, "value": r["value"], "unit": UNIT, "n_gpus": 1, "steps": r["shards"] * r["steps_per_shard"],
+           "warmup": 0, "ms_per_step": 1e3 / r["value"], "higher_is_better": True, "scaling": "weak",
+           "vs_baseline": None, "dtype": "u64 (F_q, K = F_q^2), int8 digits", "data": "synthetic",
+           "config": {"workload": f"batched: {r['shards']} shards, n=m=2^U with U uniform in [10,16], "
+                                  f"{r['steps_per_shard']} fold steps each (main lane, no Twist/Shout), "
+                                  f"{r['workers']} workers vs one worker",
+                      "l2": "PP of all sizes (>1 GB) exceeds L2"},
+           "batched": r, "gpu_launches": r["gpu_launches"],
+           "e2e": {"value": r["value"], "unit": UNIT, "h2d_bytes_per_step": None, "d2h_bytes_per_step": None}}
+    print(json.dumps(out), flush=True)
+
+
+def run_served(args):
+    """Poisson arrivals of shard-prove requests (n log-uniform 2^10..2^18) at swept rates."""
+    from nightstream_b200 import gpu
+    workers = args.workers or min(16, os.cpu_count() or 8)
+    n_req = args.shards
+    shards = shard_mix(n_req, 10, 18, 91)
+    ctx = gpu.Context(0)
+    upload_pps(ctx, [s[0] for s in shards])
+    rates = [2.0, 5.0, 10.0]
+    res = []
+    for lam in rates:
+        rng = np.random.default_rng(int(lam * 100))
+        gaps = rng.exponential(1.0 / lam, size=n_req)
+        b = gpu.Batch(0, n_workers=workers)
+        t0 = time.perf_counter()
+        ids = []
+        t_next = t0
+        for i, (ell, ccs, z) in enumerate(shards):
+            t_next += gaps[i]
+            while time.perf_counter() < t_next:
+                time.sleep(min(0.005, max(0.0, t_next - time.perf_counter())))
+            ids.append(b.submit(ccs, z, args.shard_steps, app_label=b"neo/req-%d" % i))
+        b.wait_all(3600)
+        dt = time.perf_counter() - t0
+        infos = [b.job_info(j) for j in ids]
+        b.close()
+        lat = sorted(i["latency_ms"] for i in infos)
+        res.append({"rate_per_s": lam, "p50_ms": lat[len(lat) // 2], "p99_ms": lat[min(len(lat) - 1, int(0.99 * len(lat)))],
+                    "fold_steps_per_s": n_req * args.shard_steps / dt, "max_queue_ms": max(i["queue_ms"] for i in infos)})
+    ctx.close()
+    best = max(r["fold_steps_per_s"] for r in res)
+    out = {"metric": METRIC, "value": best, "unit": UNIT, "n_gpus": 1, "steps": n_req * args.shard_steps,
+           "warmup": 0, "ms_per_step": 1e3 / best, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+           "dtype": "u64 (F_q, K = F_q^2), int8 digits", "data": "synthetic",
+           "config": {"workload": f"served: {n_req} shard-prove requests, n=m=2^U, U uniform in [10,18], "
+                                  f"{args.shard_steps} fold steps each, Poisson arrivals, {workers} workers"},
+           "served": res}
+    print(json.dumps(out), flush=True)
 
 
 def run_reference(args, rank, world):
@@ -275,6 +385,8 @@ def run_ours(args, rank, world, local_rank):
                "roofline": roofline, "step_breakdown_ms": stats}
         if world == 1 and not args.no_cpu_baseline:
             out["cpu_baseline"] = cpu_baseline(args.ell, ccs, z, pp)
+        if world == 1 and args.batch_in_plain:
+            out["batched"] = batched_result(args)
         print(json.dumps(out), flush=True)
     shard.close()
     ctx.close()
@@ -294,6 +406,12 @@ def main():
     try:
         if args.impl == "reference":
             run_reference(args, rank, world)
+        elif args.mode == "batched":
+            if rank == 0:
+                run_batched(args)
+        elif args.mode == "served":
+            if rank == 0:
+                run_served(args)
         else:
             run_ours(args, rank, world, local_rank)
     finally:

@@ -170,6 +170,29 @@ int neo_gpu_shard_ccs_digest(const neo_gpu_shard* sh, uint64_t* d4);
 int neo_gpu_shard_step_stats(const neo_gpu_shard* sh, double* out, uint32_t n);
 int neo_gpu_shard_destroy(neo_gpu_shard* sh);
 
+/* ---- batched / served proving of many shards --------------------------- */
+/* No single reference function: the reference proves shards one at a time
+ * (crates/neo-fold/src/shard.rs:2285 fold_shard_prove).  A batch owns
+ * n_workers host threads, each with its own context (CUDA stream) on `device`.
+ * Submitted shard-prove requests (CCS + witness + number of fold steps) are
+ * admitted against free device memory, assigned to the least-loaded worker and
+ * advanced one fold step at a time, round-robin, alongside earlier requests.
+ * PP for every m used must be uploaded first (any context on the device). */
+typedef struct neo_gpu_batch neo_gpu_batch;
+int neo_gpu_batch_create(int device, uint32_t n_workers, neo_gpu_batch** out);
+/* Device bytes kept free when admitting requests (default 2 GiB). */
+int neo_gpu_batch_set_reserve(neo_gpu_batch* b, uint64_t bytes);
+/* Inputs are copied; z has ccs->m words.  *job_id identifies the request. */
+int neo_gpu_batch_submit(neo_gpu_batch* b, const neo_ccs_desc* ccs, const uint64_t* z, uint32_t n_steps,
+                         uint32_t m_in, uint32_t k_rho, const char* app_label, uint64_t* job_id);
+/* Waits until every submitted request has finished (NEO_ERR_CUDA on timeout). */
+int neo_gpu_batch_wait_all(neo_gpu_batch* b, double timeout_ms);
+/* times3 = {submit->done ms, submit->admit ms, submit time since creation ms};
+ * tr_state8 = final transcript state; status 1 = done, 0 = running, < 0 = -error. */
+int neo_gpu_batch_job_info(neo_gpu_batch* b, uint64_t job_id, double* times3, uint64_t* tr_state8, int* status);
+uint64_t neo_gpu_batch_kernel_launches(const neo_gpu_batch* b);
+int neo_gpu_batch_destroy(neo_gpu_batch* b);
+
 /* ---- Fiat-Shamir transcript (host only, no GPU needed) --------------- */
 /* Poseidon2Transcript (crates/neo-transcript/src/poseidon2.rs:10-310):
  * width-8 overwrite sponge, rate 4, one field element per label byte. */

@@ -1,0 +1,282 @@
+// batch.cu -- many shards proven concurrently on one GPU (batched and served modes).
+//
+// A zkVM run yields many shards of uneven size; each shard is an independent
+// fold-step chain (own transcript, own accumulator: crates/neo-fold/src/shard.rs:1725-2283).
+// The engine runs W worker threads, each with its own context (CUDA stream).
+// Requests are admitted against free HBM (cudaMemGetInfo minus what admitted
+// requests have reserved), assigned to the least-loaded worker, and every
+// worker advances its active shards one fold step at a time, round-robin.
+// Host-side Fiat-Shamir work of different shards thus runs in parallel and
+// their kernels overlap on the device; requests that arrive while others are
+// running join the rotation between steps (continuous batching).
+#include "internal.cuh"
+#include <atomic>
+#include <chrono>
+#include <condition_variable>
+#include <deque>
+#include <memory>
+#include <mutex>
+#include <thread>
+
+typedef struct neo_gpu_shard neo_gpu_shard;
+extern "C" int neo_gpu_shard_create(neo_gpu_ctx* ctx, const neo_ccs_desc* ccs, uint32_t m_in, uint32_t k_rho,
+                                    const char* app_label, neo_gpu_shard** out);
+extern "C" int neo_gpu_shard_fold_step(neo_gpu_shard* sh, const uint64_t* z, uint64_t* proof, uint64_t proof_cap,
+                                       uint64_t* proof_len);
+extern "C" int neo_gpu_shard_transcript_state(const neo_gpu_shard* sh, uint64_t* st8);
+extern "C" int neo_gpu_shard_destroy(neo_gpu_shard* sh);
+
+namespace {
+
+using bclock = std::chrono::steady_clock;
+
+// Owned copy of a CCS description (the caller's arrays may go away).
+struct CcsCopy {
+    neo_ccs_desc d{};
+    std::vector<uint8_t> is_identity;
+    std::vector<uint64_t> col_ptr, nnz_off, vals, f_coeff;
+    std::vector<uint32_t> row_idx, f_exps;
+    explicit CcsCopy(const neo_ccs_desc* s) {
+        is_identity.assign(s->is_identity, s->is_identity + s->t);
+        col_ptr.assign(s->col_ptr, s->col_ptr + (size_t)s->t * (s->m + 1));
+        nnz_off.assign(s->nnz_off, s->nnz_off + s->t + 1);
+        const uint64_t nnz = nnz_off.back();
+        row_idx.assign(s->row_idx, s->row_idx + nnz);
+        vals.assign(s->vals, s->vals + nnz);
+        f_coeff.assign(s->f_coeff, s->f_coeff + s->n_terms);
+        f_exps.assign(s->f_exps, s->f_exps + (size_t)s->n_terms * s->t);
+        d = *s;
+        d.is_identity = is_identity.data();
+        d.col_ptr = col_ptr.data();
+        d.nnz_off = nnz_off.data();
+        d.row_idx = row_idx.data();
+        d.vals = vals.data();
+        d.f_coeff = f_coeff.data();
+        d.f_exps = f_exps.data();
+    }
+};
+
+struct Job {
+    uint64_t id = 0;
+    std::unique_ptr<CcsCopy> ccs;
+    std::vector<uint64_t> z;
+    uint32_t n_steps = 0, m_in = 1, k_rho = 12;
+    std::string label;
+    uint64_t footprint = 0;
+    neo_gpu_shard* shard = nullptr;
+    uint32_t steps_done = 0;
+    int status = 0;  // 0 pending/running, 1 done, <0 -(error code)
+    std::string error;
+    bclock::time_point t_submit, t_admit, t_done;
+    uint64_t tr_state[8] = {0};
+    std::vector<uint64_t> last_proof;
+};
+
+struct Worker {
+    neo_gpu_ctx* ctx = nullptr;
+    std::vector<Job*> active;
+    std::deque<Job*> inbox;
+    uint64_t load = 0;  // outstanding work estimate (steps x m)
+};
+
+}  // namespace
+
+struct neo_gpu_batch {
+    int device = 0;
+    std::vector<Worker> workers;
+    std::vector<std::thread> threads;
+    std::mutex mu;
+    std::condition_variable cv_work, cv_done;
+    std::deque<Job*> pending;                 // not yet admitted (HBM)
+    std::vector<std::unique_ptr<Job>> jobs;   // all jobs, by id
+    uint64_t reserved = 0;                    // bytes reserved by admitted, unfinished jobs
+    uint64_t reserve_margin = 2ull << 30;     // headroom kept free on the device
+    uint64_t unfinished = 0;
+    bool stop = false;
+    bclock::time_point t0 = bclock::now();
+};
+
+// device bytes a shard of size m holds while it is being proven: digit planes,
+// Pi_CCS tables (K), commitment scratch, fold buffers.
+static uint64_t shard_footprint(uint64_t m, uint32_t k_rho) {
+    const uint64_t k = 1 + k_rho;
+    uint64_t zall = k * 54 * m;
+    uint64_t small = 6 * m * 16 * 3 / 2;
+    uint64_t nc = k * 54 * (m / 16) * 16 * 3 / 2;
+    uint64_t commit_scratch = (uint64_t)k_rho * m * 144 + 64ull * 1024 * 1024;
+    uint64_t fold = 54 * m * 4 + 54 * m * 8 + k * 4 * m * 16;
+    return zall + small + nc + commit_scratch + fold;
+}
+
+// caller holds b->mu
+static void admit_locked(neo_gpu_batch* b) {
+    while (!b->pending.empty()) {
+        Job* j = b->pending.front();
+        size_t free_b = 0, total_b = 0;
+        if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) free_b = 0;
+        const uint64_t avail = free_b > b->reserved + b->reserve_margin ? free_b - b->reserved - b->reserve_margin : 0;
+        // always admit when nothing is running, so a large request cannot starve
+        if (j->footprint > avail && b->reserved > 0) break;
+        b->pending.pop_front();
+        b->reserved += j->footprint;
+        j->t_admit = bclock::now();
+        Worker* best = &b->workers[0];
+        for (auto& w : b->workers)
+            if (w.load < best->load) best = &w;
+        best->load += (uint64_t)j->n_steps * j->z.size();
+        best->inbox.push_back(j);
+    }
+}
+
+static void finish_job(neo_gpu_batch* b, Worker& w, Job* j, int status, const char* err) {
+    if (j->shard) {
+        neo_gpu_shard_transcript_state(j->shard, j->tr_state);
+        neo_gpu_shard_destroy(j->shard);
+        j->shard = nullptr;
+    }
+    std::lock_guard<std::mutex> lk(b->mu);
+    j->status = status;
+    if (err) j->error = err;
+    j->t_done = bclock::now();
+    b->reserved -= std::min(b->reserved, j->footprint);
+    const uint64_t work = (uint64_t)j->n_steps * j->z.size();
+    w.load -= std::min(w.load, work);
+    b->unfinished--;
+    admit_locked(b);
+    b->cv_work.notify_all();
+    b->cv_done.notify_all();
+}
+
+static void worker_main(neo_gpu_batch* b, size_t wi) {
+    Worker& w = b->workers[wi];
+    cudaSetDevice(b->device);
+    size_t rr = 0;
+    for (;;) {
+        {
+            std::unique_lock<std::mutex> lk(b->mu);
+            b->cv_work.wait(lk, [&] { return b->stop || !w.inbox.empty() || !w.active.empty(); });
+            if (b->stop && w.inbox.empty() && w.active.empty()) return;
+            while (!w.inbox.empty()) {
+                w.active.push_back(w.inbox.front());
+                w.inbox.pop_front();
+            }
+        }
+        if (w.active.empty()) continue;
+        rr %= w.active.size();
+        Job* j = w.active[rr];
+        int rc = NEO_OK;
+        if (!j->shard) rc = neo_gpu_shard_create(w.ctx, &j->ccs->d, j->m_in, j->k_rho, j->label.c_str(), &j->shard);
+        if (rc == NEO_OK) {
+            uint64_t len = 0;
+            rc = neo_gpu_shard_fold_step(j->shard, j->z.data(), nullptr, 0, &len);
+            if (rc == NEO_OK) j->steps_done++;
+        }
+        if (rc != NEO_OK || j->steps_done == j->n_steps) {
+            std::string err = rc != NEO_OK ? std::string(neo_gpu_last_error(w.ctx)) : std::string();
+            w.active.erase(w.active.begin() + rr);
+            finish_job(b, w, j, rc == NEO_OK ? 1 : -rc, rc != NEO_OK ? err.c_str() : nullptr);
+        } else {
+            rr++;
+        }
+    }
+}
+
+extern "C" int neo_gpu_batch_create(int device, uint32_t n_workers, neo_gpu_batch** out) {
+    if (!out || n_workers == 0 || n_workers > 256) return NEO_ERR_ARG;
+    *out = nullptr;
+    auto* b = new neo_gpu_batch();
+    b->device = device;
+    b->workers.resize(n_workers);
+    for (auto& w : b->workers) {
+        int rc = neo_gpu_ctx_create(device, &w.ctx);
+        if (rc != NEO_OK) {
+            for (auto& w2 : b->workers)
+                if (w2.ctx) neo_gpu_ctx_destroy(w2.ctx);
+            delete b;
+            return rc;
+        }
+    }
+    for (size_t i = 0; i < b->workers.size(); i++) b->threads.emplace_back(worker_main, b, i);
+    *out = b;
+    return NEO_OK;
+}
+
+extern "C" int neo_gpu_batch_set_reserve(neo_gpu_batch* b, uint64_t bytes) {
+    if (!b) return NEO_ERR_ARG;
+    std::lock_guard<std::mutex> lk(b->mu);
+    b->reserve_margin = bytes;
+    return NEO_OK;
+}
+
+extern "C" int neo_gpu_batch_submit(neo_gpu_batch* b, const neo_ccs_desc* ccs, const uint64_t* z, uint32_t n_steps,
+                                    uint32_t m_in, uint32_t k_rho, const char* app_label, uint64_t* job_id) {
+    if (!b || !ccs || !z || !app_label || !job_id || n_steps == 0 || ccs->m == 0) return NEO_ERR_ARG;
+    auto j = std::make_unique<Job>();
+    j->ccs = std::make_unique<CcsCopy>(ccs);
+    j->z.assign(z, z + ccs->m);
+    j->n_steps = n_steps;
+    j->m_in = m_in;
+    j->k_rho = k_rho;
+    j->label = app_label;
+    j->footprint = shard_footprint(ccs->m, k_rho);
+    j->t_submit = bclock::now();
+    std::lock_guard<std::mutex> lk(b->mu);
+    j->id = b->jobs.size();
+    *job_id = j->id;
+    b->pending.push_back(j.get());
+    b->jobs.push_back(std::move(j));
+    b->unfinished++;
+    admit_locked(b);
+    b->cv_work.notify_all();
+    return NEO_OK;
+}
+
+extern "C" int neo_gpu_batch_wait_all(neo_gpu_batch* b, double timeout_ms) {
+    if (!b) return NEO_ERR_ARG;
+    std::unique_lock<std::mutex> lk(b->mu);
+    bool ok = b->cv_done.wait_for(lk, std::chrono::duration<double, std::milli>(timeout_ms),
+                                  [&] { return b->unfinished == 0; });
+    return ok ? NEO_OK : NEO_ERR_CUDA;
+}
+
+/* times3: [submit -> done ms, submit -> admit ms, submit time since batch creation ms] */
+extern "C" int neo_gpu_batch_job_info(neo_gpu_batch* b, uint64_t job_id, double* times3, uint64_t* tr_state8,
+                                      int* status) {
+    if (!b) return NEO_ERR_ARG;
+    std::lock_guard<std::mutex> lk(b->mu);
+    if (job_id >= b->jobs.size()) return NEO_ERR_ARG;
+    Job* j = b->jobs[job_id].get();
+    if (status) *status = j->status;
+    if (times3) {
+        using ms = std::chrono::duration<double, std::milli>;
+        times3[0] = j->status ? ms(j->t_done - j->t_submit).count() : -1.0;
+        times3[1] = ms(j->t_admit - j->t_submit).count();
+        times3[2] = ms(j->t_submit - b->t0).count();
+    }
+    if (tr_state8) memcpy(tr_state8, j->tr_state, 64);
+    return NEO_OK;
+}
+
+extern "C" int neo_gpu_batch_destroy(neo_gpu_batch* b) {
+    if (!b) return NEO_ERR_ARG;
+    {
+        std::lock_guard<std::mutex> lk(b->mu);
+        b->stop = true;
+        b->cv_work.notify_all();
+    }
+    for (auto& t : b->threads) t.join();
+    for (auto& w : b->workers) {
+        for (Job* j : w.active)
+            if (j->shard) neo_gpu_shard_destroy(j->shard);
+        neo_gpu_ctx_destroy(w.ctx);
+    }
+    delete b;
+    return NEO_OK;
+}
+
+extern "C" uint64_t neo_gpu_batch_kernel_launches(const neo_gpu_batch* b) {
+    if (!b) return 0;
+    uint64_t n = 0;
+    for (auto& w : b->workers) n += neo_gpu_kernel_launches(w.ctx);
+    return n;
+}

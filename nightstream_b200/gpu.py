@@ -52,6 +52,13 @@ SIGNATURES = {
     "neo_gpu_shard_transcript_state": [P, P],
     "neo_gpu_shard_ccs_digest": [P, P],
     "neo_gpu_shard_destroy": [P],
+    "neo_gpu_batch_create": [I, U32, P],
+    "neo_gpu_batch_set_reserve": [P, U64],
+    "neo_gpu_batch_submit": [P, P, P, U32, U32, U32, ctypes.c_char_p, P],
+    "neo_gpu_batch_wait_all": [P, ctypes.c_double],
+    "neo_gpu_batch_job_info": [P, U64, P, P, P],
+    "neo_gpu_batch_kernel_launches": [P],
+    "neo_gpu_batch_destroy": [P],
     "neo_transcript_new": [ctypes.c_char_p, P],
     "neo_transcript_append_message": [P, ctypes.c_char_p, P, ctypes.c_size_t],
     "neo_transcript_append_fields": [P, ctypes.c_char_p, P, ctypes.c_size_t],
@@ -68,6 +75,7 @@ _RESTYPES = {
     "neo_gpu_kernel_launches": U64,
     "neo_gpu_ccs_oracle_num_rounds": U32,
     "neo_gpu_ccs_oracle_degree_bound": U32,
+    "neo_gpu_batch_kernel_launches": U64,
 }
 
 _lib = None
@@ -364,3 +372,55 @@ def ccs_digest(ccs) -> np.ndarray:
     if rc:
         raise NeoGpuError(rc, "ccs digest")
     return d
+
+
+class Batch:
+    """Many shard-prove requests on one GPU (neo_gpu_batch): n_workers host
+    threads, one CUDA stream each, HBM-based admission, round-robin fold steps."""
+
+    def __init__(self, device: int = 0, n_workers: int = 8, reserve_bytes: int = None):
+        self.lib = load()
+        h = ctypes.c_void_p()
+        rc = self.lib.neo_gpu_batch_create(device, n_workers, ctypes.byref(h))
+        if rc:
+            raise NeoGpuError(rc, "batch creation failed")
+        self.h = h
+        if reserve_bytes is not None:
+            self.lib.neo_gpu_batch_set_reserve(self.h, reserve_bytes)
+        self._descs = []
+
+    def submit(self, ccs, z: np.ndarray, n_steps: int, m_in: int = 1, k_rho: int = 12,
+               app_label: bytes = b"neo/shard") -> int:
+        desc = ccs.desc()
+        z = _u64(z)
+        jid = ctypes.c_uint64()
+        rc = self.lib.neo_gpu_batch_submit(self.h, ctypes.byref(desc), _p(z), n_steps, m_in, k_rho, app_label,
+                                           ctypes.byref(jid))
+        if rc:
+            raise NeoGpuError(rc, "batch submit")
+        return jid.value
+
+    def wait_all(self, timeout_s: float = 3600.0):
+        rc = self.lib.neo_gpu_batch_wait_all(self.h, timeout_s * 1e3)
+        if rc:
+            raise NeoGpuError(rc, "batch wait timed out")
+
+    def job_info(self, jid: int) -> dict:
+        t = np.zeros(3, np.float64)
+        st = np.zeros(8, np.uint64)
+        status = ctypes.c_int()
+        self.lib.neo_gpu_batch_job_info(self.h, jid, _p(t), _p(st), ctypes.byref(status))
+        return {"latency_ms": float(t[0]), "queue_ms": float(t[1]), "submit_ms": float(t[2]),
+                "transcript_state": st, "status": status.value}
+
+    @property
+    def kernel_launches(self) -> int:
+        return int(self.lib.neo_gpu_batch_kernel_launches(self.h))
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.neo_gpu_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
