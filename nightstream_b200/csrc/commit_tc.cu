@@ -305,25 +305,35 @@ __global__ void __launch_bounds__(TC_THREADS, 1) commit_tc_kernel(const TcArgs a
 #pragma unroll
                     for (int q = 0; q < 18; q++) L[q] = src[q];
                 }
+                // all four rows first (static offsets), then store them in an order rotated by
+                // (g >> 1) & 3 so the 8 threads of a store phase hit 8 distinct rows mod 8
+                uint32_t out[4][16];
 #pragma unroll
-                for (int j = 0; j < 4; j++) {
-                    const int r = 4 * g + j;
-                    if (r > 80) break;
-                    const int row = vl * 81 + r;
-                    uint32_t out[16];
+                for (int j = 0; j < 4; j++)
 #pragma unroll
                     for (int q = 0; q < 16; q++) {
-                        if (!valid) out[q] = 0;
-                        else if (j == 0) out[q] = L[q + 1];
-                        else out[q] = __funnelshift_r(L[q], L[q + 1], 8 * (4 - j));
+                        if (!valid) out[j][q] = 0;
+                        else if (j == 0) out[j][q] = L[q + 1];
+                        else out[j][q] = __funnelshift_r(L[q], L[q + 1], 8 * (4 - j));
                     }
+                const int rot = (g >> 1) & 3;
+                auto store_row = [&](int j, const uint32_t* o) {
+                    const int r = 4 * g + j;
+                    if (r > 80) return;
+                    const int row = vl * 81 + r;
                     uint8_t* rowp = dstB + (row >> 3) * 1024 + (row & 7) * 128;
 #pragma unroll
                     for (int c = 0; c < 4; c++) {
                         const int chunk = half * 4 + c;
                         *reinterpret_cast<uint4*>(rowp + ((chunk ^ (row & 7)) * 16)) =
-                            make_uint4(out[4 * c], out[4 * c + 1], out[4 * c + 2], out[4 * c + 3]);
+                            make_uint4(o[4 * c], o[4 * c + 1], o[4 * c + 2], o[4 * c + 3]);
                     }
+                };
+                switch (rot) {  // static register indices in every branch
+                    case 0: store_row(0, out[0]); store_row(1, out[1]); store_row(2, out[2]); store_row(3, out[3]); break;
+                    case 1: store_row(1, out[1]); store_row(2, out[2]); store_row(3, out[3]); store_row(0, out[0]); break;
+                    case 2: store_row(2, out[2]); store_row(3, out[3]); store_row(0, out[0]); store_row(1, out[1]); break;
+                    default: store_row(3, out[3]); store_row(0, out[0]); store_row(1, out[1]); store_row(2, out[2]); break;
                 }
             }
             asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
