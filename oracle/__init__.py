@@ -67,12 +67,21 @@ def lib():
             "or_tr_challenge_fields": [P, ctypes.c_char_p, SZ, P],
             "or_tr_digest32": [P, P],
             "or_tr_state": [P, P],
+            "or_mem_oracle_new": [I, I, P, I, P, P, I, P, P, P],
+            "or_mem_oracle_free": [P],
+            "or_mem_oracle_num_rounds": [P],
+            "or_mem_oracle_degree_bound": [P],
+            "or_mem_oracle_evals": [P, P, I, P],
+            "or_mem_oracle_fold": [P, P],
+            "or_addr_lookup_weights": [I, P, I, P, P, P, SZ, P, P],
         }
         for name, args in sigs.items():
             fn = getattr(L, name)
             fn.argtypes = args
-            fn.restype = I if name in ("or_split_b", "or_ccs_oracle_num_rounds", "or_ccs_sumcheck_fixed") else None
+            fn.restype = I if name in ("or_split_b", "or_ccs_oracle_num_rounds", "or_ccs_sumcheck_fixed",
+                                        "or_mem_oracle_num_rounds", "or_mem_oracle_degree_bound") else None
         L.or_ccs_oracle_new.restype = P
+        L.or_mem_oracle_new.restype = P
         L.or_tr_new.restype = P
         L.or_tr_challenge_field.restype = ctypes.c_uint64
         _lib = L
@@ -313,3 +322,57 @@ def ccs_digest(ccs):
     out = np.empty(4, np.uint64)
     lib().or_ccs_digest(ctypes.byref(desc), out.ctypes.data)
     return out
+
+
+MEM_SHOUT_VALUE, MEM_SHOUT_ADAPTER, MEM_BITNESS, MEM_TWIST_READ, MEM_TWIST_WRITE, MEM_VAL_EVAL, MEM_TOTAL_INC, \
+    MEM_PRODUCT = range(8)
+
+
+class MemOracle:
+    """Twist / Shout time-lane oracle restatement (literal sparse algorithm of
+    crates/neo-memory/src/twist_oracle.rs). cols: uint64 [n_cols, 2^ell, 2]."""
+
+    def __init__(self, kind, cols, r_point=None, r_addr=None, init=None, weights=None):
+        self.cols = u64(cols)
+        n_cols, L = self.cols.shape[0], self.cols.shape[1]
+        ell = L.bit_length() - 1
+        ell_addr = 0 if r_addr is None else len(r_addr)
+        self._keep = [None if r_point is None else u64(r_point), None if r_addr is None else u64(r_addr),
+                      None if init is None else u64(init), None if weights is None else u64(weights)]
+        self.claim = np.zeros(2, np.uint64)
+        self.h = lib().or_mem_oracle_new(kind, ell, ptr(self._keep[0]), ell_addr, ptr(self._keep[1]),
+                                         ptr(self._keep[2]), n_cols, ptr(self.cols), ptr(self._keep[3]),
+                                         ptr(self.claim))
+        if not self.h:
+            raise ValueError("memory oracle construction failed")
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            lib().or_mem_oracle_free(self.h)
+            self.h = None
+
+    def num_rounds(self):
+        return lib().or_mem_oracle_num_rounds(self.h)
+
+    def degree_bound(self):
+        return lib().or_mem_oracle_degree_bound(self.h)
+
+    def evals_at(self, xs):
+        xs = u64(xs)
+        ys = np.empty_like(xs)
+        lib().or_mem_oracle_evals(self.h, ptr(xs), xs.shape[0], ptr(ys))
+        return ys
+
+    def fold(self, r):
+        lib().or_mem_oracle_fold(self.h, ptr(u64(r)))
+
+
+def addr_lookup_weights(r_cycle, has_lookup, addr_bits, table):
+    """AddressLookupOracle weight table and claimed sum (twist_oracle.rs:1671-1724)."""
+    r_cycle, has_lookup, addr_bits, table = u64(r_cycle), u64(has_lookup), u64(addr_bits), u64(table)
+    ell, ell_addr = r_cycle.shape[0], addr_bits.shape[0]
+    w = np.empty((1 << ell_addr, 2), np.uint64)
+    claim = np.empty(2, np.uint64)
+    lib().or_addr_lookup_weights(ell, ptr(r_cycle), ell_addr, ptr(has_lookup), ptr(addr_bits), ptr(table),
+                                 table.shape[0], ptr(w), ptr(claim))
+    return w, claim

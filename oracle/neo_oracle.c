@@ -1306,3 +1306,415 @@ void or_ccs_digest(const or_ccs* s, uint64_t* out4) {
     }
     memcpy(out4, st, 32);
 }
+
+/* ------------------------------------------------------------------------ */
+/* Twist / Shout time-lane oracles (crates/neo-memory/src/twist_oracle.rs).  */
+/* This is the literal sparse algorithm: SparseIdxVec columns folded on the  */
+/* least-significant bit (sparse_time.rs:69-117), pairs gathered from the    */
+/* gate column's entries (twist_oracle.rs:187-199), χ_{r_cycle} children per */
+/* pair (twist_oracle.rs:163-185), and Val_pre recomputed at every child     */
+/* time point from the increment terms through LT (twist_oracle.rs:311-379). */
+/* ------------------------------------------------------------------------ */
+typedef struct { size_t len, n; size_t* idx; kq* val; } spv;
+
+static spv spv_from_dense(const kq* d, size_t len) {
+    spv v; v.len = len; v.n = 0;
+    v.idx = (size_t*)malloc(sizeof(size_t) * (len ? len : 1));
+    v.val = (kq*)malloc(sizeof(kq) * (len ? len : 1));
+    for (size_t i = 0; i < len; i++) if (!kiszero(d[i])) { v.idx[v.n] = i; v.val[v.n] = d[i]; v.n++; }
+    return v;
+}
+static void spv_free(spv* v) { free(v->idx); free(v->val); }
+/* SparseIdxVec::get: binary search, zero when absent (sparse_time.rs:58-64) */
+static kq spv_get(const spv* v, size_t i) {
+    size_t lo = 0, hi = v->n;
+    while (lo < hi) { size_t mid = (lo + hi) / 2; if (v->idx[mid] < i) lo = mid + 1; else hi = mid; }
+    return (lo < v->n && v->idx[lo] == i) ? v->val[lo] : K0;
+}
+static kq spv_single(const spv* v) { return v->n ? v->val[0] : K0; }
+/* SparseIdxVec::fold_round_in_place (sparse_time.rs:69-117) */
+static void spv_fold(spv* v, kq r) {
+    kq omr = ksub(K1, r);
+    size_t o = 0, i = 0;
+    size_t* nidx = (size_t*)malloc(sizeof(size_t) * (v->n ? v->n : 1));
+    kq* nval = (kq*)malloc(sizeof(kq) * (v->n ? v->n : 1));
+    while (i < v->n) {
+        size_t idx = v->idx[i], parent = idx >> 1;
+        kq acc = K0;
+        if ((idx & 1) == 0) {
+            acc = kadd(acc, kmul(v->val[i], omr)); i++;
+            if (i < v->n && v->idx[i] == idx + 1) { acc = kadd(acc, kmul(v->val[i], r)); i++; }
+        } else { acc = kadd(acc, kmul(v->val[i], r)); i++; }
+        if (!kiszero(acc)) {
+            if (o > 0 && nidx[o - 1] == parent) nval[o - 1] = kadd(nval[o - 1], acc);
+            else { nidx[o] = parent; nval[o] = acc; o++; }
+        }
+    }
+    free(v->idx); free(v->val);
+    v->idx = nidx; v->val = nval; v->n = o; v->len >>= 1;
+}
+
+/* eq(bit, u) = bit·(2u − 1) + (1 − u)  (neo-memory/src/bit_ops.rs:5-9) */
+static inline kq eq_bit_affine_k(kq bit, kq u) { return kadd(kmul(bit, ksub(kadd(u, u), K1)), ksub(K1, u)); }
+static inline kq interp_k(kq f0, kq f1, kq x) { return kadd(f0, kmul(ksub(f1, f0), x)); }
+
+/* twist_oracle.rs:163-185 */
+static void chi_cycle_children(const kq* r_cycle, int ell, int bit_idx, kq prefix_eq, size_t pair, kq* c0, kq* c1) {
+    kq suffix = K1;
+    int shift = 0;
+    for (int b = bit_idx + 1; b < ell; b++) {
+        suffix = kmul(suffix, ((pair >> shift) & 1) ? r_cycle[b] : ksub(K1, r_cycle[b]));
+        shift++;
+    }
+    kq r = r_cycle[bit_idx];
+    *c0 = kmul(kmul(prefix_eq, ksub(K1, r)), suffix);
+    *c1 = kmul(kmul(prefix_eq, r), suffix);
+}
+/* twist_oracle.rs:305-318 */
+static void fill_time_point(kq* out, int ell, const kq* prefix, int bit_idx, kq bit_value, size_t pair) {
+    for (int b = 0; b < bit_idx; b++) out[b] = prefix[b];
+    out[bit_idx] = bit_value;
+    int shift = 0;
+    for (int b = bit_idx + 1; b < ell; b++) { out[b] = ((pair >> shift) & 1) ? K1 : K0; shift++; }
+}
+/* LT(idx, point) with idx Boolean (twist_oracle.rs:320-334) */
+static kq lt_eval_at_bool_index(size_t idx, const kq* point, int ell) {
+    kq suffix = K1, acc = K0;
+    for (int i = ell - 1; i >= 0; i--) {
+        if (((idx >> i) & 1) == 0) { acc = kadd(acc, kmul(point[i], suffix)); suffix = kmul(suffix, ksub(K1, point[i])); }
+        else suffix = kmul(suffix, point[i]);
+    }
+    return acc;
+}
+/* LT(j', j) (neo-memory/src/mle.rs:7-24) */
+static kq lt_eval_k(const kq* jp, const kq* j, int ell) {
+    kq* suf = (kq*)malloc(sizeof(kq) * (ell + 1));
+    suf[ell] = K1;
+    for (int i = ell - 1; i >= 0; i--) suf[i] = kmul(suf[i + 1], eq_lin(jp[i], j[i]));
+    kq acc = K0;
+    for (int i = 0; i < ell; i++) acc = kadd(acc, kmul(kmul(ksub(K1, jp[i]), j[i]), suf[i + 1]));
+    free(suf);
+    return acc;
+}
+
+struct or_mem_oracle {
+    int kind, ell, ell_addr, bit_idx, degree, n_cols, n_fold;
+    kq *rpt, *r_addr, *w, *chal, init, prefix_eq, claim;
+    spv* cols;
+    size_t n_inc; size_t* inc_t; kq* inc_v;
+    kq *t0, *t1;
+};
+
+/* build_inc_terms_at_r_addr (twist_oracle.rs:351-378) */
+static void build_inc_terms(or_mem_oracle* o, const spv* has_w, const spv* inc, const spv* wa) {
+    o->inc_t = (size_t*)malloc(sizeof(size_t) * (has_w->n + 1));
+    o->inc_v = (kq*)malloc(sizeof(kq) * (has_w->n + 1));
+    o->n_inc = 0;
+    for (size_t e = 0; e < has_w->n; e++) {
+        size_t t = has_w->idx[e];
+        kq hw = has_w->val[e], it = spv_get(inc, t);
+        if (kiszero(hw) || kiszero(it)) continue;
+        kq eq = K1;
+        for (int b = 0; b < o->ell_addr; b++) eq = kmul(eq, eq_bit_affine_k(spv_get(&wa[b], t), o->r_addr[b]));
+        kq v = kmul(kmul(hw, it), eq);
+        if (!kiszero(v)) { o->inc_t[o->n_inc] = t; o->inc_v[o->n_inc] = v; o->n_inc++; }
+    }
+}
+/* val_pre_from_inc_terms (twist_oracle.rs:336-342) */
+static kq val_pre(const or_mem_oracle* o, const kq* tp) {
+    kq acc = o->init;
+    for (size_t i = 0; i < o->n_inc; i++) acc = kadd(acc, kmul(o->inc_v[i], lt_eval_at_bool_index(o->inc_t[i], tp, o->ell)));
+    return acc;
+}
+static kq eq_addr_at(const or_mem_oracle* o, const spv* bits, size_t t, int single) {
+    kq eq = K1;
+    for (int b = 0; b < o->ell_addr; b++)
+        eq = kmul(eq, eq_bit_affine_k(single ? spv_single(&bits[b]) : spv_get(&bits[b], t), o->r_addr[b]));
+    return eq;
+}
+
+static int sz_cmp(const void* a, const void* b) {
+    size_t x = *(const size_t*)a, y = *(const size_t*)b;
+    return x < y ? -1 : x > y;
+}
+
+/* Round evaluations at xs (each kind's evals_at). */
+static void mem_evals(or_mem_oracle* o, const kq* xs, int nx, kq* ys) {
+    int A = o->ell_addr, k = o->kind;
+    for (int i = 0; i < nx; i++) ys[i] = K0;
+    if (k == OR_MEM_BITNESS && o->n_cols == 0) return;
+    if (o->cols[0].len == 1) {
+        kq v = K0;
+        switch (k) {
+            case OR_MEM_SHOUT_VALUE: v = kmul(kmul(o->prefix_eq, spv_single(&o->cols[0])), spv_single(&o->cols[1])); break;
+            case OR_MEM_SHOUT_ADAPTER: v = kmul(kmul(o->prefix_eq, spv_single(&o->cols[0])), eq_addr_at(o, &o->cols[1], 0, 1)); break;
+            case OR_MEM_BITNESS: {
+                kq acc = K0;
+                for (int c = 0; c < o->n_cols; c++) { kq b = spv_single(&o->cols[c]); acc = kadd(acc, kmul(kmul(o->w[c], b), ksub(b, K1))); }
+                v = kmul(o->prefix_eq, acc);
+            } break;
+            case OR_MEM_TWIST_READ: {
+                kq diff = ksub(val_pre(o, o->chal), spv_single(&o->cols[1]));
+                v = kmul(kmul(kmul(o->prefix_eq, spv_single(&o->cols[0])), diff), eq_addr_at(o, &o->cols[2], 0, 1));
+            } break;
+            case OR_MEM_TWIST_WRITE: {
+                kq delta = ksub(ksub(spv_single(&o->cols[1]), val_pre(o, o->chal)), spv_single(&o->cols[2]));
+                v = kmul(kmul(kmul(o->prefix_eq, spv_single(&o->cols[0])), delta), eq_addr_at(o, &o->cols[3], 0, 1));
+            } break;
+            case OR_MEM_VAL_EVAL:
+                v = kmul(kmul(kmul(spv_single(&o->cols[0]), spv_single(&o->cols[1])), eq_addr_at(o, &o->cols[2], 0, 1)),
+                         lt_eval_k(o->chal, o->rpt, o->ell));
+                break;
+            case OR_MEM_TOTAL_INC:
+                v = kmul(kmul(spv_single(&o->cols[0]), spv_single(&o->cols[1])), eq_addr_at(o, &o->cols[2], 0, 1));
+                break;
+            case OR_MEM_PRODUCT: {
+                v = K1;
+                for (int c = 0; c < o->n_cols; c++) v = kmul(v, spv_single(&o->cols[c]));
+            } break;
+        }
+        for (int i = 0; i < nx; i++) ys[i] = v;
+        return;
+    }
+    /* pairs: from the gate column (gather_pairs_from_sparse), the union of all
+       columns for bitness (twist_oracle.rs:560-568), every pair for products */
+    size_t np = 0, half = o->cols[0].len / 2;
+    size_t* pairs;
+    if (k == OR_MEM_PRODUCT) {
+        pairs = (size_t*)malloc(sizeof(size_t) * half);
+        for (size_t p = 0; p < half; p++) pairs[np++] = p;
+    } else if (k == OR_MEM_BITNESS) {
+        size_t tot = 0;
+        for (int c = 0; c < o->n_cols; c++) tot += o->cols[c].n;
+        pairs = (size_t*)malloc(sizeof(size_t) * (tot + 1));
+        for (int c = 0; c < o->n_cols; c++) for (size_t e = 0; e < o->cols[c].n; e++) pairs[np++] = o->cols[c].idx[e] >> 1;
+        qsort(pairs, np, sizeof(size_t), sz_cmp);
+        size_t u = 0;
+        for (size_t i = 0; i < np; i++) if (u == 0 || pairs[u - 1] != pairs[i]) pairs[u++] = pairs[i];
+        np = u;
+    } else {
+        pairs = (size_t*)malloc(sizeof(size_t) * (o->cols[0].n + 1));
+        for (size_t e = 0; e < o->cols[0].n; e++) {
+            size_t p = o->cols[0].idx[e] >> 1;
+            if (np == 0 || pairs[np - 1] != p) pairs[np++] = p;
+        }
+    }
+    int maxf = 4 + A + o->n_cols;
+    kq* f0 = (kq*)malloc(sizeof(kq) * maxf);
+    kq* f1 = (kq*)malloc(sizeof(kq) * maxf);
+    for (size_t pi = 0; pi < np; pi++) {
+        size_t pair = pairs[pi], c0 = 2 * pair, c1 = c0 + 1;
+        int nf = 0;
+        if (k == OR_MEM_BITNESS) {
+            kq ch0, ch1;
+            chi_cycle_children(o->rpt, o->ell, o->bit_idx, o->prefix_eq, pair, &ch0, &ch1);
+            for (int i = 0; i < nx; i++) {
+                kq chi_x = interp_k(ch0, ch1, xs[i]);
+                if (kiszero(chi_x)) continue;
+                kq bs = K0;
+                for (int c = 0; c < o->n_cols; c++) {
+                    kq b0 = spv_get(&o->cols[c], c0), b1 = spv_get(&o->cols[c], c1);
+                    if (kiszero(b0) && kiszero(b1)) continue;
+                    kq bx = interp_k(b0, b1, xs[i]);
+                    bs = kadd(bs, kmul(kmul(o->w[c], bx), ksub(bx, K1)));
+                }
+                ys[i] = kadd(ys[i], kmul(chi_x, bs));
+            }
+            continue;
+        }
+        if (k != OR_MEM_PRODUCT) {
+            kq g0 = spv_get(&o->cols[0], c0), g1 = spv_get(&o->cols[0], c1);
+            if (kiszero(g0) && kiszero(g1)) continue;
+            f0[nf] = g0; f1[nf] = g1; nf++;
+        }
+        if (k == OR_MEM_SHOUT_VALUE || k == OR_MEM_SHOUT_ADAPTER || k == OR_MEM_TWIST_READ || k == OR_MEM_TWIST_WRITE) {
+            chi_cycle_children(o->rpt, o->ell, o->bit_idx, o->prefix_eq, pair, &f0[nf], &f1[nf]); nf++;
+        }
+        const spv* bits = NULL;
+        switch (k) {
+            case OR_MEM_SHOUT_VALUE:
+                f0[nf] = spv_get(&o->cols[1], c0); f1[nf] = spv_get(&o->cols[1], c1); nf++;
+                break;
+            case OR_MEM_SHOUT_ADAPTER: bits = &o->cols[1]; break;
+            case OR_MEM_TWIST_READ: {
+                fill_time_point(o->t0, o->ell, o->chal, o->bit_idx, K0, pair);
+                fill_time_point(o->t1, o->ell, o->chal, o->bit_idx, K1, pair);
+                f0[nf] = ksub(val_pre(o, o->t0), spv_get(&o->cols[1], c0));
+                f1[nf] = ksub(val_pre(o, o->t1), spv_get(&o->cols[1], c1)); nf++;
+                bits = &o->cols[2];
+            } break;
+            case OR_MEM_TWIST_WRITE: {
+                fill_time_point(o->t0, o->ell, o->chal, o->bit_idx, K0, pair);
+                fill_time_point(o->t1, o->ell, o->chal, o->bit_idx, K1, pair);
+                f0[nf] = ksub(ksub(spv_get(&o->cols[1], c0), val_pre(o, o->t0)), spv_get(&o->cols[2], c0));
+                f1[nf] = ksub(ksub(spv_get(&o->cols[1], c1), val_pre(o, o->t1)), spv_get(&o->cols[2], c1)); nf++;
+                bits = &o->cols[3];
+            } break;
+            case OR_MEM_VAL_EVAL: {
+                f0[nf] = spv_get(&o->cols[1], c0); f1[nf] = spv_get(&o->cols[1], c1); nf++;
+                fill_time_point(o->t0, o->ell, o->chal, o->bit_idx, K0, pair);
+                fill_time_point(o->t1, o->ell, o->chal, o->bit_idx, K1, pair);
+                f0[nf] = lt_eval_k(o->t0, o->rpt, o->ell); f1[nf] = lt_eval_k(o->t1, o->rpt, o->ell); nf++;
+                bits = &o->cols[2];
+            } break;
+            case OR_MEM_TOTAL_INC:
+                f0[nf] = spv_get(&o->cols[1], c0); f1[nf] = spv_get(&o->cols[1], c1); nf++;
+                bits = &o->cols[2];
+                break;
+            case OR_MEM_PRODUCT:
+                for (int c = 0; c < o->n_cols; c++) { f0[nf] = spv_get(&o->cols[c], c0); f1[nf] = spv_get(&o->cols[c], c1); nf++; }
+                break;
+        }
+        if (bits)
+            for (int b = 0; b < A; b++) {
+                f0[nf] = eq_bit_affine_k(spv_get(&bits[b], c0), o->r_addr[b]);
+                f1[nf] = eq_bit_affine_k(spv_get(&bits[b], c1), o->r_addr[b]);
+                nf++;
+            }
+        for (int i = 0; i < nx; i++) {
+            kq prod = K1;
+            for (int f = 0; f < nf; f++) prod = kmul(prod, interp_k(f0[f], f1[f], xs[i]));
+            ys[i] = kadd(ys[i], prod);
+        }
+    }
+    free(f0); free(f1); free(pairs);
+}
+
+or_mem_oracle* or_mem_oracle_new(int kind, int ell, const uint64_t* r_point, int ell_addr, const uint64_t* r_addr,
+                                 const uint64_t* init, int n_cols, const uint64_t* cols, const uint64_t* weights,
+                                 uint64_t* claim_out) {
+    int A = ell_addr;
+    int need = -1;
+    switch (kind) {
+        case OR_MEM_SHOUT_VALUE: need = 2; break;
+        case OR_MEM_SHOUT_ADAPTER: need = 1 + A; break;
+        case OR_MEM_BITNESS: need = n_cols; break;
+        case OR_MEM_TWIST_READ: need = 4 + 2 * A; break;
+        case OR_MEM_TWIST_WRITE: need = 3 + A; break;
+        case OR_MEM_VAL_EVAL: case OR_MEM_TOTAL_INC: need = 2 + A; break;
+        case OR_MEM_PRODUCT: need = n_cols; break;
+        default: return NULL;
+    }
+    if (n_cols != need || ell < 0) return NULL;
+    or_mem_oracle* o = (or_mem_oracle*)calloc(1, sizeof(*o));
+    size_t L = (size_t)1 << ell;
+    o->kind = kind; o->ell = ell; o->ell_addr = A; o->n_cols = n_cols;
+    o->rpt = kdup(r_point, r_point ? ell : 0);
+    o->r_addr = kdup(r_addr, r_addr ? A : 0);
+    o->init = init ? kload(init) : K0;
+    o->prefix_eq = K1;
+    o->chal = (kq*)calloc(ell + 1, sizeof(kq));
+    o->t0 = (kq*)calloc(ell + 1, sizeof(kq));
+    o->t1 = (kq*)calloc(ell + 1, sizeof(kq));
+    o->cols = (spv*)calloc(n_cols + 1, sizeof(spv));
+    for (int c = 0; c < n_cols; c++) o->cols[c] = spv_from_dense((const kq*)cols + (size_t)c * L, L);
+    if (kind == OR_MEM_BITNESS) o->w = kdup(weights, n_cols);
+    o->n_fold = n_cols;
+    switch (kind) {
+        case OR_MEM_SHOUT_VALUE: case OR_MEM_BITNESS: o->degree = 3; break;
+        case OR_MEM_SHOUT_ADAPTER: o->degree = 2 + A; break;
+        case OR_MEM_TWIST_READ:
+            o->degree = 3 + A; o->n_fold = 2 + A;  /* the write stream enters only through Val_pre */
+            build_inc_terms(o, &o->cols[2 + A], &o->cols[3 + A], &o->cols[4 + A]);
+            break;
+        case OR_MEM_TWIST_WRITE:
+            o->degree = 3 + A;
+            build_inc_terms(o, &o->cols[0], &o->cols[2], &o->cols[3]);
+            break;
+        case OR_MEM_VAL_EVAL: o->degree = 3 + A; break;
+        case OR_MEM_TOTAL_INC: o->degree = 2 + A; break;
+        case OR_MEM_PRODUCT: o->degree = n_cols; break;
+    }
+    /* claims: the constructors' direct sums where the reference computes one
+       (twist_oracle.rs:214-241, 396-437, 928-974, 1064-1102, 89-101); the
+       hypercube sum p(0) + p(1) of round 0 for bitness / read / write checks,
+       whose claimed sums the caller supplies (zero for an honest witness) */
+    kq claim = K0;
+    if (kind == OR_MEM_SHOUT_VALUE) {
+        for (size_t e = 0; e < o->cols[0].n; e++) {
+            size_t t = o->cols[0].idx[e];
+            kq v = spv_get(&o->cols[1], t);
+            if (kiszero(v)) continue;
+            claim = kadd(claim, kmul(kmul(eq_points_bool_mask(t, o->rpt, ell), o->cols[0].val[e]), v));
+        }
+    } else if (kind == OR_MEM_SHOUT_ADAPTER) {
+        for (size_t e = 0; e < o->cols[0].n; e++) {
+            size_t t = o->cols[0].idx[e];
+            claim = kadd(claim, kmul(kmul(eq_points_bool_mask(t, o->rpt, ell), o->cols[0].val[e]), eq_addr_at(o, &o->cols[1], t, 0)));
+        }
+    } else if (kind == OR_MEM_VAL_EVAL || kind == OR_MEM_TOTAL_INC) {
+        for (size_t e = 0; e < o->cols[0].n; e++) {
+            size_t t = o->cols[0].idx[e];
+            kq it = spv_get(&o->cols[1], t);
+            if (kiszero(it)) continue;
+            kq term = kmul(kmul(o->cols[0].val[e], it), eq_addr_at(o, &o->cols[2], t, 0));
+            if (kind == OR_MEM_VAL_EVAL) term = kmul(term, lt_eval_at_bool_index(t, o->rpt, ell));
+            claim = kadd(claim, term);
+        }
+    } else if (kind == OR_MEM_PRODUCT) {
+        for (size_t t = 0; t < L; t++) {
+            kq p = K1;
+            for (int c = 0; c < n_cols; c++) p = kmul(p, ((const kq*)cols)[(size_t)c * L + t]);
+            claim = kadd(claim, p);
+        }
+    } else if (ell > 0) {
+        kq xs[2] = {K0, K1}, ys[2];
+        mem_evals(o, xs, 2, ys);
+        claim = kadd(ys[0], ys[1]);
+    } else {
+        kq xs[1] = {K0}, ys[1];
+        mem_evals(o, xs, 1, ys);
+        claim = ys[0];
+    }
+    o->claim = claim;
+    if (claim_out) kstore(claim_out, claim);
+    return o;
+}
+
+void or_mem_oracle_free(or_mem_oracle* o) {
+    if (!o) return;
+    for (int c = 0; c < o->n_cols; c++) spv_free(&o->cols[c]);
+    free(o->cols); free(o->rpt); free(o->r_addr); free(o->w); free(o->chal); free(o->t0); free(o->t1);
+    free(o->inc_t); free(o->inc_v); free(o);
+}
+int or_mem_oracle_num_rounds(const or_mem_oracle* o) { return o->ell - o->bit_idx; }
+int or_mem_oracle_degree_bound(const or_mem_oracle* o) { return o->degree; }
+void or_mem_oracle_evals(or_mem_oracle* o, const uint64_t* xs, int nx, uint64_t* ys) {
+    mem_evals(o, (const kq*)xs, nx, (kq*)ys);
+}
+void or_mem_oracle_fold(or_mem_oracle* o, const uint64_t* rp) {
+    if (o->bit_idx >= o->ell) return;
+    kq r = kload(rp);
+    int k = o->kind;
+    if (k == OR_MEM_SHOUT_VALUE || k == OR_MEM_SHOUT_ADAPTER || k == OR_MEM_BITNESS || k == OR_MEM_TWIST_READ ||
+        k == OR_MEM_TWIST_WRITE)
+        o->prefix_eq = kmul(o->prefix_eq, eq_lin(r, o->rpt[o->bit_idx]));
+    for (int c = 0; c < o->n_fold; c++) spv_fold(&o->cols[c], r);
+    o->chal[o->bit_idx++] = r;
+}
+
+/* Weight table of AddressLookupOracle::new (twist_oracle.rs:1671-1724):
+   w[addr(t)] += χ_{r_cycle}(t)·has_lookup(t), addr(t) from bit columns equal
+   to one; claim = Σ_a table[a]·w[a]. */
+void or_addr_lookup_weights(int ell, const uint64_t* r_cycle, int ell_addr, const uint64_t* has_lookup,
+                            const uint64_t* addr_bits, const uint64_t* table, size_t table_len,
+                            uint64_t* weights_out, uint64_t* claim_out) {
+    size_t L = (size_t)1 << ell, P = (size_t)1 << ell_addr;
+    kq* r = kdup(r_cycle, ell);
+    kq* w = (kq*)weights_out;
+    for (size_t a = 0; a < P; a++) w[a] = K0;
+    const kq* hl = (const kq*)has_lookup;
+    const kq* ab = (const kq*)addr_bits;
+    for (size_t t = 0; t < L; t++) {
+        if (kiszero(hl[t])) continue;
+        kq wt = kmul(eq_points_bool_mask(t, r, ell), hl[t]);
+        if (kiszero(wt)) continue;
+        size_t a = 0;
+        for (int b = 0; b < ell_addr; b++) if (keq(ab[(size_t)b * L + t], K1)) a |= (size_t)1 << b;
+        w[a] = kadd(w[a], wt);
+    }
+    kq claim = K0;
+    for (size_t a = 0; a < P && a < table_len; a++) claim = kadd(claim, kmul(((const kq*)table)[a], w[a]));
+    kstore(claim_out, claim);
+    free(r);
+}

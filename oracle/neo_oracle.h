@@ -120,6 +120,29 @@ void or_tr_state(const or_transcript* t, uint64_t* out);
 void or_poseidon2_w16_permute(uint64_t* st);
 void or_ccs_digest(const or_ccs* s, uint64_t* out4);
 
+
+/* Twist / Shout time-lane oracles (crates/neo-memory/src/twist_oracle.rs).
+   cols: n_cols dense K columns of 2^ell entries; layouts per kind:
+   SHOUT_VALUE [has_lookup, val]; SHOUT_ADAPTER [has_lookup, addr_bits...];
+   BITNESS [cols...] with weights; TWIST_READ [has_read, rv, ra_bits...,
+   has_write, inc_at_write_addr, wa_bits...]; TWIST_WRITE [has_write, wv,
+   inc_at_write_addr, wa_bits...]; VAL_EVAL / TOTAL_INC [has_write,
+   inc_at_write_addr, wa_bits...]; PRODUCT [factors...]. */
+enum { OR_MEM_SHOUT_VALUE = 0, OR_MEM_SHOUT_ADAPTER = 1, OR_MEM_BITNESS = 2, OR_MEM_TWIST_READ = 3,
+       OR_MEM_TWIST_WRITE = 4, OR_MEM_VAL_EVAL = 5, OR_MEM_TOTAL_INC = 6, OR_MEM_PRODUCT = 7 };
+typedef struct or_mem_oracle or_mem_oracle;
+or_mem_oracle* or_mem_oracle_new(int kind, int ell, const uint64_t* r_point, int ell_addr, const uint64_t* r_addr,
+                                 const uint64_t* init, int n_cols, const uint64_t* cols, const uint64_t* weights,
+                                 uint64_t* claim_out);
+void or_mem_oracle_free(or_mem_oracle* o);
+int or_mem_oracle_num_rounds(const or_mem_oracle* o);
+int or_mem_oracle_degree_bound(const or_mem_oracle* o);
+void or_mem_oracle_evals(or_mem_oracle* o, const uint64_t* xs, int nx, uint64_t* ys);
+void or_mem_oracle_fold(or_mem_oracle* o, const uint64_t* r);
+void or_addr_lookup_weights(int ell, const uint64_t* r_cycle, int ell_addr, const uint64_t* has_lookup,
+                            const uint64_t* addr_bits, const uint64_t* table, size_t table_len,
+                            uint64_t* weights_out, uint64_t* claim_out);
+
 #ifdef __cplusplus
 }
 #endif

@@ -44,3 +44,138 @@ def commit(pp, Z):
             acc = [(x + y) % Q for x, y in zip(acc, p)]
         out.append(acc)
     return out
+
+
+# --- Twist / Shout time-lane sums, dense restatement --------------------------
+# Each oracle is a sum over the time hypercube of a product of multilinear
+# tables; here every factor is materialised as a dense table (χ_r, eq-bit
+# factors, the exclusive prefix sum Val_pre, LT(·, r_time)) and folded on the
+# least-significant variable. Independent of the sparse C restatement.
+
+def kadd(a, b):
+    return ((a[0] + b[0]) % Q, (a[1] + b[1]) % Q)
+
+
+def ksub(a, b):
+    return ((a[0] - b[0]) % Q, (a[1] - b[1]) % Q)
+
+
+K0, K1 = (0, 0), (1, 0)
+
+
+def chi_dense(r):
+    t = [K1]
+    for ri in r:  # variable i is bit i of the index (little-endian)
+        t = [kmul(v, ksub(K1, ri)) for v in t] + [kmul(v, ri) for v in t]
+    return t
+
+
+def eq_bit(bit, u):
+    return kadd(kmul(bit, ksub(kadd(u, u), K1)), ksub(K1, u))
+
+
+def lt_table(r_time):
+    ell = len(r_time)
+    out = []
+    for j in range(1 << ell):
+        # LT(j, r) = Σ_i [j_i = 0]·r_i·Π_{k>i} eq(j_k, r_k)
+        acc = K0
+        for i in range(ell):
+            if (j >> i) & 1:
+                continue
+            term = r_time[i]
+            for k in range(i + 1, ell):
+                term = kmul(term, r_time[k] if (j >> k) & 1 else ksub(K1, r_time[k]))
+            acc = kadd(acc, term)
+        out.append(acc)
+    return out
+
+
+def prefix_excl(init, inc_terms):
+    out, acc = [], init
+    for v in inc_terms:
+        out.append(acc)
+        acc = kadd(acc, v)
+    return out
+
+
+class DenseMemSum:
+    """kind names follow the C ABI: 0 shout value, 1 adapter, 2 bitness,
+    3 twist read, 4 twist write, 5 val eval, 6 total inc, 7 product."""
+
+    def __init__(self, kind, cols, r_point=None, r_addr=None, init=K0, weights=None):
+        L = len(cols[0])
+        A = 0 if r_addr is None else len(r_addr)
+        self.kind, self.w = kind, weights
+        eqb = lambda col, b: [eq_bit(v, r_addr[b]) for v in col]
+        E = chi_dense(r_point) if r_point is not None and kind not in (5,) else None
+        if kind == 0:
+            F = [E, cols[0], cols[1]]
+        elif kind == 1:
+            F = [E, cols[0]] + [eqb(cols[1 + b], b) for b in range(A)]
+        elif kind == 2:
+            F = [E] + list(cols)
+        elif kind in (3, 4):
+            if kind == 3:
+                hw, inc, wa = cols[2 + A], cols[3 + A], cols[4 + A:4 + 2 * A]
+            else:
+                hw, inc, wa = cols[0], cols[2], cols[3:3 + A]
+            terms = []
+            for t in range(L):
+                v = kmul(hw[t], inc[t])
+                for b in range(A):
+                    v = kmul(v, eq_bit(wa[b][t], r_addr[b]))
+                terms.append(v)
+            VP = prefix_excl(init, terms)
+            if kind == 3:
+                F = [E, cols[0], [ksub(VP[t], cols[1][t]) for t in range(L)]] + [eqb(cols[2 + b], b) for b in range(A)]
+            else:
+                F = [E, cols[0], [ksub(ksub(cols[1][t], VP[t]), cols[2][t]) for t in range(L)]] + \
+                    [eqb(cols[3 + b], b) for b in range(A)]
+        elif kind == 5:
+            F = [cols[0], cols[1], lt_table(r_point)] + [eqb(cols[2 + b], b) for b in range(A)]
+        elif kind == 6:
+            F = [cols[0], cols[1]] + [eqb(cols[2 + b], b) for b in range(A)]
+        else:
+            F = list(cols)
+        self.F = [list(f) for f in F]
+
+    def _term(self, vals):
+        if self.kind == 2:
+            acc = K0
+            for w, b in zip(self.w, vals[1:]):
+                acc = kadd(acc, kmul(kmul(w, b), ksub(b, K1)))
+            return kmul(vals[0], acc)
+        p = K1
+        for v in vals:
+            p = kmul(p, v)
+        return p
+
+    def total(self):
+        return _ksum(self._term([f[t] for f in self.F]) for t in range(len(self.F[0])))
+
+    def evals(self, xs):
+        L = len(self.F[0])
+        if L == 1:
+            v = self._term([f[0] for f in self.F])
+            return [v for _ in xs]
+        ys = []
+        for x in xs:
+            acc = K0
+            for p in range(L // 2):
+                vals = [kadd(f[2 * p], kmul(ksub(f[2 * p + 1], f[2 * p]), x)) for f in self.F]
+                acc = kadd(acc, self._term(vals))
+            ys.append(acc)
+        return ys
+
+    def fold(self, r):
+        if len(self.F[0]) == 1:
+            return
+        self.F = [[kadd(f[2 * p], kmul(ksub(f[2 * p + 1], f[2 * p]), r)) for p in range(len(f) // 2)] for f in self.F]
+
+
+def _ksum(it):
+    acc = K0
+    for v in it:
+        acc = kadd(acc, v)
+    return acc
