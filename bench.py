@@ -372,7 +372,7 @@ def run_ours(args, rank, world, local_rank):
     ops = 746496 * m * n_vec  # 2 * 8 limbs * kappa * d^2 * m per commitment
     peak, peak_src = int8_peak_tops()
     achieved = ops / (commit_ms * 1e-3) / 1e12
-    roofline = {"kernel": "Ajtai commit, 12 DEC planes per launch (commit_partial_kernel + commit_reduce_kernel)",
+    roofline = {"kernel": "Ajtai commit, 12 DEC planes per launch (commit_tc_kernel: tcgen05 kind::i8, + commit_tc_reduce_kernel)",
                 "bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TOPS", "frac": achieved / peak,
                 "traffic": None, "launch_ms": commit_ms, "peak_source": peak_src,
                 "algorithmic_ops_per_launch": ops}

@@ -141,6 +141,55 @@ uint32_t neo_gpu_ccs_oracle_degree_bound(const neo_gpu_ccs_oracle* o);
 int neo_gpu_ccs_oracle_me_outputs(neo_gpu_ccs_oracle* o, uint64_t* y, uint64_t* y_scalars);
 int neo_gpu_ccs_oracle_destroy(neo_gpu_ccs_oracle* o);
 
+/* ---- Twist / Shout time-lane oracles (RoundOracle) ------------------- */
+/* The sparse-in-time oracles of crates/neo-memory/src/twist_oracle.rs, on
+ * dense tables.  cols: n_cols K columns of 2^ell entries each (column-major,
+ * K = two u64), in this order per kind:
+ *   SHOUT_VALUE    [has_lookup, val]                    ShoutValueOracleSparse::new (twist_oracle.rs:203-241)
+ *   SHOUT_ADAPTER  [has_lookup, addr_bits x ell_addr]   IndexAdapterOracleSparseTime::new_with_gate (:384-437)
+ *   BITNESS        [cols...], weights[n_cols]           LazyWeightedBitnessOracleSparseTime::new_with_cycle (:515-542)
+ *   TWIST_READ     [has_read, rv, ra_bits x ell_addr, has_write, inc_at_write_addr, wa_bits x ell_addr]
+ *                                                       TwistReadCheckOracleSparseTime::new (:622-682)
+ *   TWIST_WRITE    [has_write, wv, inc_at_write_addr, wa_bits x ell_addr]
+ *                                                       TwistWriteCheckOracleSparseTime::new (:767-824)
+ *   VAL_EVAL       [has_write, inc_at_write_addr, wa_bits x ell_addr]  (r_point = r_time)
+ *                                                       TwistValEvalOracleSparseTime::new (:911-974)
+ *   TOTAL_INC      [has_write, inc_at_write_addr, wa_bits x ell_addr]  (no r_point)
+ *                                                       TwistTotalIncOracleSparseTime::new (:1054-1102)
+ *   PRODUCT        [factors...]  (degree bound = n_cols) ProductRoundOracle::new (:50-71)
+ * r_point: r_cycle (ell K) for the χ-weighted kinds, r_time for VAL_EVAL.
+ * init_at_r_addr: 1 K (Twist read / write).  *claim: the sum over the time
+ * hypercube (the constructors' claimed sums; for bitness / read / write the
+ * value the caller's claimed sum must equal).  Status 1 on a column count
+ * that does not match the kind, 5 for a degree bound above 31. */
+enum { NEO_MEM_SHOUT_VALUE = 0, NEO_MEM_SHOUT_ADAPTER = 1, NEO_MEM_BITNESS = 2, NEO_MEM_TWIST_READ = 3,
+       NEO_MEM_TWIST_WRITE = 4, NEO_MEM_VAL_EVAL = 5, NEO_MEM_TOTAL_INC = 6, NEO_MEM_PRODUCT = 7 };
+typedef struct neo_gpu_mem_oracle neo_gpu_mem_oracle;
+int neo_gpu_mem_oracle_create(neo_gpu_ctx* ctx, int kind, uint32_t ell, const uint64_t* r_point,
+                              uint32_t ell_addr, const uint64_t* r_addr, const uint64_t* init_at_r_addr,
+                              uint32_t n_cols, const uint64_t* cols, const uint64_t* weights, uint64_t* claim,
+                              neo_gpu_mem_oracle** out);
+/* Same with the columns in device memory (d_cols); points stay host. */
+int neo_gpu_mem_oracle_create_device(neo_gpu_ctx* ctx, int kind, uint32_t ell, const uint64_t* r_point,
+                                     uint32_t ell_addr, const uint64_t* r_addr, const uint64_t* init_at_r_addr,
+                                     uint32_t n_cols, const uint64_t* d_cols, const uint64_t* weights,
+                                     uint64_t* claim, neo_gpu_mem_oracle** out);
+/* RoundOracle::evals_at: ys[i] = p_round(xs[i]); after the last round every
+ * point gets the final product (the reference's len == 1 branch). */
+int neo_gpu_mem_oracle_evals(neo_gpu_mem_oracle* o, const uint64_t* xs, uint32_t nx, uint64_t* ys);
+/* RoundOracle::fold; ignored once no rounds remain. */
+int neo_gpu_mem_oracle_fold(neo_gpu_mem_oracle* o, const uint64_t* r);
+uint32_t neo_gpu_mem_oracle_num_rounds(const neo_gpu_mem_oracle* o);
+uint32_t neo_gpu_mem_oracle_degree_bound(const neo_gpu_mem_oracle* o);
+int neo_gpu_mem_oracle_destroy(neo_gpu_mem_oracle* o);
+/* AddressLookupOracle::new (twist_oracle.rs:1671-1724): weights[2^ell_addr]
+ * with w[addr(t)] += χ_{r_cycle}(t)·has_lookup(t) (addr from bit columns
+ * equal to one) and claim = Σ_a table[a]·w[a]; the address rounds are then a
+ * PRODUCT oracle over [table, weights].  addr_bits: ell_addr columns of 2^ell. */
+int neo_gpu_addr_lookup_weights(neo_gpu_ctx* ctx, uint32_t ell, const uint64_t* r_cycle, uint32_t ell_addr,
+                                const uint64_t* has_lookup, const uint64_t* addr_bits, const uint64_t* table,
+                                uint64_t table_len, uint64_t* weights, uint64_t* claim);
+
 /* ---- shard prove loop (crates/neo-fold/src/shard.rs:1725-2283) ------- */
 typedef struct neo_gpu_shard neo_gpu_shard;
 /* A shard prover over one CCS (n == m == 2^ell_n, identity-first, t <= 4,

@@ -290,50 +290,30 @@ __global__ void __launch_bounds__(TC_THREADS, 1) commit_tc_kernel(const TcArgs a
             if (s_abort) break;
             uint8_t* dstB = sB + sb * TC_B_BYTES;
             const uint8_t* srcF = sF + sa * TC_F_STAGE;
-            // task = (vector vl, column half, row group g): rows r = 4g .. 4g+3 (r <= 80).
-            // With o = 80 - r the window start, row 4g+j reads word (20-g) at byte 0 (j = 0)
-            // or word (19-g) at byte 4-j (j >= 1): all offsets are static given L[0] = word 19-g.
-            for (int task = bt; task < TC_NV * 2 * 21; task += TC_BUILDERS) {
-                const int g = task % 21, vh = task / 21;
-                const int vl = vh >> 1, half = vh & 1;
-                uint32_t L[18];
-                const bool valid = (uint32_t)vl < nvalid;
-                if (valid) {
-                    // for g = 20 word -1 is read (4 bytes before this F, still inside shared memory);
-                    // it only feeds rows r >= 81, which are not stored
-                    const uint32_t* src = reinterpret_cast<const uint32_t*>(srcF + (vl * 2 + half) * TC_FBYTES) + (19 - g);
+            for (int task = bt; task < TC_NROWS * 2; task += TC_BUILDERS) {
+                const int half = task & 1, row = task >> 1;
+                const int vl = row / 81, r = row - vl * 81;
+                uint32_t out[16];
+                if ((uint32_t)vl < nvalid) {
+                    const int o = 80 - r;  // window start in F
+                    const uint32_t* src =
+                        reinterpret_cast<const uint32_t*>(srcF + (vl * 2 + half) * TC_FBYTES + (o & ~3));
+                    uint32_t w[17];
 #pragma unroll
-                    for (int q = 0; q < 18; q++) L[q] = src[q];
+                    for (int q = 0; q < 17; q++) w[q] = src[q];
+                    const uint32_t sh = 8 * (o & 3);
+#pragma unroll
+                    for (int q = 0; q < 16; q++) out[q] = __funnelshift_r(w[q], w[q + 1], sh);
+                } else {
+#pragma unroll
+                    for (int q = 0; q < 16; q++) out[q] = 0;
                 }
-                // all four rows first (static offsets), then store them in an order rotated by
-                // (g >> 1) & 3 so the 8 threads of a store phase hit 8 distinct rows mod 8
-                uint32_t out[4][16];
+                uint8_t* rowp = dstB + (row >> 3) * 1024 + (row & 7) * 128;
 #pragma unroll
-                for (int j = 0; j < 4; j++)
-#pragma unroll
-                    for (int q = 0; q < 16; q++) {
-                        if (!valid) out[j][q] = 0;
-                        else if (j == 0) out[j][q] = L[q + 1];
-                        else out[j][q] = __funnelshift_r(L[q], L[q + 1], 8 * (4 - j));
-                    }
-                const int rot = (g >> 1) & 3;
-                auto store_row = [&](int j, const uint32_t* o) {
-                    const int r = 4 * g + j;
-                    if (r > 80) return;
-                    const int row = vl * 81 + r;
-                    uint8_t* rowp = dstB + (row >> 3) * 1024 + (row & 7) * 128;
-#pragma unroll
-                    for (int c = 0; c < 4; c++) {
-                        const int chunk = half * 4 + c;
-                        *reinterpret_cast<uint4*>(rowp + ((chunk ^ (row & 7)) * 16)) =
-                            make_uint4(o[4 * c], o[4 * c + 1], o[4 * c + 2], o[4 * c + 3]);
-                    }
-                };
-                switch (rot) {  // static register indices in every branch
-                    case 0: store_row(0, out[0]); store_row(1, out[1]); store_row(2, out[2]); store_row(3, out[3]); break;
-                    case 1: store_row(1, out[1]); store_row(2, out[2]); store_row(3, out[3]); store_row(0, out[0]); break;
-                    case 2: store_row(2, out[2]); store_row(3, out[3]); store_row(0, out[0]); store_row(1, out[1]); break;
-                    default: store_row(3, out[3]); store_row(0, out[0]); store_row(1, out[1]); store_row(2, out[2]); break;
+                for (int c = 0; c < 4; c++) {
+                    const int chunk = half * 4 + c;
+                    *reinterpret_cast<uint4*>(rowp + ((chunk ^ (row & 7)) * 16)) =
+                        make_uint4(out[4 * c], out[4 * c + 1], out[4 * c + 2], out[4 * c + 3]);
                 }
             }
             asm volatile("fence.proxy.async.shared::cta;" ::: "memory");

@@ -1,0 +1,687 @@
+// mem_oracle.cu -- Twist / Shout time-lane sum-check oracles on dense tables.
+//
+// Every time-lane oracle of crates/neo-memory/src/twist_oracle.rs is a sum over
+// the time hypercube of a product of multilinear factors (bitness: χ times a
+// weighted sum of b(b-1)).  The reference walks sparse columns pair by pair and
+// recomputes χ_{r_cycle} children, eq-bit factors and, for Twist, Val_pre by a
+// quadratic sum over all increments at every pair of every round
+// (twist_oracle.rs:163-185, 311-379, 684-749).  Here each factor is a dense
+// K table in HBM, built once:
+//   * χ_{r_cycle} as a table, folded like any factor: folding variable 0 at c
+//     multiplies by eq(c, r_0), which is the reference's prefix_eq update;
+//   * eq_bit_affine(bit(t), r_b) per address bit: affine in the column, so
+//     folding the factor equals the factor of the folded column;
+//   * Val_pre(t) = init + Σ_{u<t} inc_terms(u): LT(u, ·) is the multilinear
+//     extension of [u < t], so the reference's Σ inc_u·LT(u, point) is the
+//     folded exclusive prefix sum (one scan here);
+//   * LT(t, r_time) for the val-evaluation oracle.
+// A round evaluates Σ_pairs Π_f (f0 + x (f1 - f0)) at x = 0..deg (one thread
+// per (pair, x)), sums per block and then over blocks, and interpolates the
+// requested points on the host. fold(r) is one pass over every factor.
+// All arithmetic is exact in F_q / K, so values equal the reference's.
+#include "internal.cuh"
+
+using gl::K;
+
+namespace {
+
+constexpr int MEM_MAX_DEG = 31;
+constexpr int MT = 256;
+
+__device__ __forceinline__ K shfl_xor_km(K a, int o) {
+    K r;
+    r.re = __shfl_xor_sync(0xffffffffu, a.re, o);
+    r.im = __shfl_xor_sync(0xffffffffu, a.im, o);
+    return r;
+}
+
+// eq(bit, u) = bit·(2u − 1) + (1 − u)   (neo-memory/src/bit_ops.rs:5-9)
+__device__ __forceinline__ K eq_bit_affine(K bit, K u) {
+    return gl::kadd(gl::kmul(bit, gl::ksub(gl::kdbl(u), gl::kone())), gl::ksub(gl::kone(), u));
+}
+
+__global__ void eqbit_kernel(K* __restrict__ col, uint64_t len, K u) {
+    uint64_t t = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+    if (t < len) col[t] = eq_bit_affine(col[t], u);
+}
+
+// inc_terms(t) = has_write(t)·inc(t)·Π_b eq_bit_affine(wa_b(t), r_addr_b)
+// (build_inc_terms_at_r_addr, twist_oracle.rs:351-378)
+__global__ void inc_terms_kernel(const K* __restrict__ has_w, const K* __restrict__ inc, const K* __restrict__ wa,
+                                 uint32_t A, const K* __restrict__ r_addr, uint64_t len, K* __restrict__ out) {
+    uint64_t t = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+    if (t >= len) return;
+    K v = gl::kmul(has_w[t], inc[t]);
+    for (uint32_t b = 0; b < A; b++) v = gl::kmul(v, eq_bit_affine(wa[(uint64_t)b * len + t], r_addr[b]));
+    out[t] = v;
+}
+
+// exclusive prefix sum over K in three passes: per-block sums, a scan of the
+// block sums (one block), and the per-element scan with the block offset.
+constexpr int SCAN_T = 256, SCAN_E = 4, SCAN_BLK = SCAN_T * SCAN_E;
+
+__device__ K block_excl_scan(K v, K* s_warp, K* total) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    K inc = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        K n;
+        n.re = __shfl_up_sync(0xffffffffu, inc.re, o);
+        n.im = __shfl_up_sync(0xffffffffu, inc.im, o);
+        if (lane >= o) inc = gl::kadd(inc, n);
+    }
+    if (lane == 31) s_warp[warp] = inc;
+    __syncthreads();
+    if (warp == 0) {
+        const int nw = blockDim.x >> 5;
+        K w = lane < nw ? s_warp[lane] : gl::kzero();
+        K wi = w;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            K n;
+            n.re = __shfl_up_sync(0xffffffffu, wi.re, o);
+            n.im = __shfl_up_sync(0xffffffffu, wi.im, o);
+            if (lane >= o) wi = gl::kadd(wi, n);
+        }
+        if (lane < nw) s_warp[lane] = gl::ksub(wi, w);  // exclusive warp offsets
+        if (lane == nw - 1) *total = wi;
+    }
+    __syncthreads();
+    K r = gl::kadd(s_warp[warp], gl::ksub(inc, v));
+    __syncthreads();
+    return r;
+}
+
+__global__ void __launch_bounds__(SCAN_T) scan_sums_kernel(const K* __restrict__ in, uint64_t len, K* __restrict__ sums) {
+    __shared__ K s_warp[32];
+    __shared__ K s_tot;
+    uint64_t base = blockIdx.x * (uint64_t)SCAN_BLK + threadIdx.x * SCAN_E;
+    K v = gl::kzero();
+#pragma unroll
+    for (int e = 0; e < SCAN_E; e++)
+        if (base + e < len) v = gl::kadd(v, in[base + e]);
+    block_excl_scan(v, s_warp, &s_tot);
+    if (threadIdx.x == 0) sums[blockIdx.x] = s_tot;
+}
+
+// one block scans up to SCAN_T * chunk block sums, in place, exclusive, plus init
+__global__ void __launch_bounds__(SCAN_T) scan_top_kernel(K* __restrict__ sums, uint32_t n, K init) {
+    __shared__ K s_warp[32];
+    __shared__ K s_tot;
+    K carry = init;
+    for (uint32_t base = 0; base < n; base += SCAN_T) {
+        uint32_t i = base + threadIdx.x;
+        K v = i < n ? sums[i] : gl::kzero();
+        K ex = block_excl_scan(v, s_warp, &s_tot);
+        if (i < n) sums[i] = gl::kadd(carry, ex);
+        carry = gl::kadd(carry, s_tot);
+        __syncthreads();
+    }
+}
+
+// out = prefix(in) combined per kind:
+//   combine 0: out = VP                      (plain exclusive prefix + init)
+//   combine 1: out = VP − a                  (read check:  Val_pre − rv)
+//   combine 2: out = a − VP − b              (write check: wv − Val_pre − inc)
+__global__ void __launch_bounds__(SCAN_T) scan_final_kernel(const K* __restrict__ in, uint64_t len,
+                                                            const K* __restrict__ offs, int combine,
+                                                            const K* __restrict__ a, const K* __restrict__ b,
+                                                            K* __restrict__ out) {
+    __shared__ K s_warp[32];
+    __shared__ K s_tot;
+    uint64_t base = blockIdx.x * (uint64_t)SCAN_BLK + threadIdx.x * SCAN_E;
+    K v[SCAN_E];
+    K s = gl::kzero();
+#pragma unroll
+    for (int e = 0; e < SCAN_E; e++) {
+        v[e] = base + e < len ? in[base + e] : gl::kzero();
+        s = gl::kadd(s, v[e]);
+    }
+    K run = gl::kadd(offs[blockIdx.x], block_excl_scan(s, s_warp, &s_tot));
+#pragma unroll
+    for (int e = 0; e < SCAN_E; e++) {
+        uint64_t t = base + e;
+        if (t < len) {
+            K o = run;
+            if (combine == 1) o = gl::ksub(run, a[t]);
+            else if (combine == 2) o = gl::ksub(gl::ksub(a[t], run), b[t]);
+            out[t] = o;
+        }
+        run = gl::kadd(run, v[e]);
+    }
+}
+
+// LT(t, r) for Boolean t (twist_oracle.rs:320-334)
+__global__ void lt_table_kernel(const K* __restrict__ r, uint32_t ell, K* __restrict__ out) {
+    uint64_t t = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+    if (t >= (1ULL << ell)) return;
+    K suffix = gl::kone(), acc = gl::kzero();
+    for (int i = (int)ell - 1; i >= 0; i--) {
+        K ri = r[i];
+        if (((t >> i) & 1) == 0) {
+            acc = gl::kadd(acc, gl::kmul(ri, suffix));
+            suffix = gl::kmul(suffix, gl::ksub(gl::kone(), ri));
+        } else {
+            suffix = gl::kmul(suffix, ri);
+        }
+    }
+    out[t] = acc;
+}
+
+// fold every factor on variable 0: dst[f][p] = src[f][2p] + r (src[f][2p+1] − src[f][2p])
+__global__ void mem_fold_kernel(const K* __restrict__ src, uint64_t src_len, K* __restrict__ dst, uint32_t nf, K r) {
+    const uint64_t half = src_len >> 1;
+    uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+    if (i >= half * nf) return;
+    uint64_t f = i / half, p = i - f * half;
+    const K* s = src + f * src_len + 2 * p;
+    dst[f * half + p] = gl::klerp(s[0], s[1], r);
+}
+
+struct MemEvalArgs {
+    const K* tab;       // [nf][len]
+    uint64_t len;       // current table length (>= 2)
+    uint32_t nf;
+    int bitness;        // 1: factor 0 is χ, the rest columns weighted by w
+    const K* w;         // bitness weights [nf - 1]
+    K* partials;        // [npts][gridDim.x]
+};
+
+// one thread per (pair, x); x = blockIdx.y
+__global__ void __launch_bounds__(MT) mem_eval_kernel(const MemEvalArgs a) {
+    __shared__ K s_red[MT / 32];
+    const uint64_t pairs = a.len >> 1;
+    const uint64_t p = blockIdx.x * (uint64_t)MT + threadIdx.x;
+    const uint32_t x = blockIdx.y;
+    K acc = gl::kzero();
+    if (p < pairs) {
+        if (!a.bitness) {
+            K prod = gl::kone();
+            for (uint32_t f = 0; f < a.nf; f++) {
+                const K* s = a.tab + (uint64_t)f * a.len + 2 * p;
+                K f0 = s[0], f1 = s[1];
+                K v = gl::kadd(f0, gl::kscale_small(gl::ksub(f1, f0), (int32_t)x));
+                prod = gl::kmul(prod, v);
+            }
+            acc = prod;
+        } else {
+            const K* s = a.tab + 2 * p;
+            K chi = gl::kadd(s[0], gl::kscale_small(gl::ksub(s[1], s[0]), (int32_t)x));
+            K sum = gl::kzero();
+            for (uint32_t f = 1; f < a.nf; f++) {
+                const K* c = a.tab + (uint64_t)f * a.len + 2 * p;
+                K bx = gl::kadd(c[0], gl::kscale_small(gl::ksub(c[1], c[0]), (int32_t)x));
+                sum = gl::kadd(sum, gl::kmul(gl::kmul(a.w[f - 1], bx), gl::ksub(bx, gl::kone())));
+            }
+            acc = gl::kmul(chi, sum);
+        }
+    }
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) acc = gl::kadd(acc, shfl_xor_km(acc, o));
+    if (lane == 0) s_red[warp] = acc;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        K s = gl::kzero();
+#pragma unroll
+        for (int w = 0; w < MT / 32; w++) s = gl::kadd(s, s_red[w]);
+        a.partials[(uint64_t)x * gridDim.x + blockIdx.x] = s;
+    }
+}
+
+// vals[x] = Σ_b partials[x][b]; one block per x
+__global__ void __launch_bounds__(256) mem_reduce_kernel(const K* __restrict__ partials, uint32_t nblocks,
+                                                         K* __restrict__ vals) {
+    __shared__ K s_red[8];
+    const uint32_t x = blockIdx.x;
+    K v = gl::kzero();
+    for (uint32_t b = threadIdx.x; b < nblocks; b += blockDim.x) v = gl::kadd(v, partials[(uint64_t)x * nblocks + b]);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = gl::kadd(v, shfl_xor_km(v, o));
+    if (lane == 0) s_red[warp] = v;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        K s = gl::kzero();
+        for (int w = 0; w < 8; w++) s = gl::kadd(s, s_red[w]);
+        vals[x] = s;
+    }
+}
+
+// AddressLookupOracle weight table (twist_oracle.rs:1671-1724):
+// w[addr(t)] += χ_{r_cycle}(t)·has_lookup(t), addr from bit columns equal to 1.
+// Exact order-free accumulation: each u64 component is summed with a 64-bit
+// atomic and its carries are counted separately (sum = lo + 2^64·carries).
+__global__ void addr_weights_kernel(const K* __restrict__ chi, const K* __restrict__ has, const K* __restrict__ bits,
+                                    uint32_t A, uint64_t len, unsigned long long* __restrict__ lo,
+                                    unsigned long long* __restrict__ carry) {
+    uint64_t t = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+    if (t >= len) return;
+    K g = has[t];
+    if (gl::kiszero(g)) return;
+    K wt = gl::kmul(chi[t], g);
+    if (gl::kiszero(wt)) return;
+    uint64_t addr = 0;
+    for (uint32_t b = 0; b < A; b++) {
+        K v = bits[(uint64_t)b * len + t];
+        if (v.re == 1 && v.im == 0) addr |= 1ULL << b;
+    }
+    unsigned long long o = atomicAdd(&lo[2 * addr], (unsigned long long)wt.re);
+    if (o + wt.re < o) atomicAdd(&carry[2 * addr], 1ULL);
+    o = atomicAdd(&lo[2 * addr + 1], (unsigned long long)wt.im);
+    if (o + wt.im < o) atomicAdd(&carry[2 * addr + 1], 1ULL);
+}
+
+__global__ void addr_weights_finish_kernel(const unsigned long long* __restrict__ lo,
+                                           const unsigned long long* __restrict__ carry, uint64_t n, K* __restrict__ w) {
+    uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    // lo + carry·2^64 with 2^64 = 2^32 − 1 (mod q)
+    uint64_t re = gl::add(gl::canon(lo[2 * i]), gl::mul(gl::canon(carry[2 * i]), GL_EPS));
+    uint64_t im = gl::add(gl::canon(lo[2 * i + 1]), gl::mul(gl::canon(carry[2 * i + 1]), GL_EPS));
+    w[i] = gl::kmk(re, im);
+}
+
+// claim = Σ_a table[a]·w[a] (block partials, reduced by mem_reduce_kernel)
+__global__ void __launch_bounds__(256) dot_kernel(const K* __restrict__ a, const K* __restrict__ b, uint64_t n,
+                                                  K* __restrict__ partials) {
+    __shared__ K s_red[8];
+    K v = gl::kzero();
+    for (uint64_t i = blockIdx.x * 256ULL + threadIdx.x; i < n; i += 256ULL * gridDim.x)
+        v = gl::kadd(v, gl::kmul(a[i], b[i]));
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = gl::kadd(v, shfl_xor_km(v, o));
+    if (lane == 0) s_red[warp] = v;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        K s = gl::kzero();
+        for (int w = 0; w < 8; w++) s = gl::kadd(s, s_red[w]);
+        partials[blockIdx.x] = s;
+    }
+}
+
+inline K kload_h(const uint64_t* p) { return gl::kmk(p[0], p[1]); }
+
+}  // namespace
+
+struct neo_gpu_mem_oracle {
+    neo_gpu_ctx* ctx = nullptr;
+    int kind = 0;
+    uint32_t ell = 0, A = 0, deg = 0, nf = 0, bit_idx = 0;
+    int bitness = 0;
+    uint64_t len = 0;     // current table length
+    DevBuf<K> tab[2];     // ping-pong factor tables [nf][len]
+    int cur = 0;
+    bool pending = false; // a fold challenge not yet applied
+    K pending_r{};
+    DevBuf<K> w;          // bitness weights
+    std::vector<K> hw;    // host copy of the weights
+    DevBuf<K> partials, vals;
+    std::vector<K> hvals;
+    K claim{};
+};
+
+namespace {
+
+uint32_t factor_count(int kind, uint32_t A, uint32_t n_cols) {
+    switch (kind) {
+        case NEO_MEM_SHOUT_VALUE: return 3;
+        case NEO_MEM_SHOUT_ADAPTER: return 2 + A;
+        case NEO_MEM_BITNESS: return 1 + n_cols;
+        case NEO_MEM_TWIST_READ: return 3 + A;
+        case NEO_MEM_TWIST_WRITE: return 3 + A;
+        case NEO_MEM_VAL_EVAL: return 3 + A;
+        case NEO_MEM_TOTAL_INC: return 2 + A;
+        case NEO_MEM_PRODUCT: return n_cols;
+    }
+    return 0;
+}
+
+int expected_cols(int kind, uint32_t A, uint32_t n_cols) {
+    switch (kind) {
+        case NEO_MEM_SHOUT_VALUE: return 2;
+        case NEO_MEM_SHOUT_ADAPTER: return 1 + A;
+        case NEO_MEM_BITNESS: return n_cols;
+        case NEO_MEM_TWIST_READ: return 4 + 2 * A;
+        case NEO_MEM_TWIST_WRITE: return 3 + A;
+        case NEO_MEM_VAL_EVAL: case NEO_MEM_TOTAL_INC: return 2 + A;
+        case NEO_MEM_PRODUCT: return n_cols;
+    }
+    return -1;
+}
+
+uint32_t degree_of(int kind, uint32_t A, uint32_t n_cols) {
+    switch (kind) {
+        case NEO_MEM_SHOUT_VALUE: case NEO_MEM_BITNESS: return 3;
+        case NEO_MEM_SHOUT_ADAPTER: case NEO_MEM_TOTAL_INC: return 2 + A;
+        case NEO_MEM_TWIST_READ: case NEO_MEM_TWIST_WRITE: case NEO_MEM_VAL_EVAL: return 3 + A;
+        case NEO_MEM_PRODUCT: return n_cols;
+    }
+    return 0;
+}
+
+// round values at x = 0..deg into o->hvals (applies a pending fold first)
+int mem_round_values(neo_gpu_mem_oracle* o) {
+    neo_gpu_ctx* ctx = o->ctx;
+    if (o->pending) {
+        K* src = o->tab[o->cur].p;
+        K* dst = o->tab[o->cur ^ 1].p;
+        uint64_t tot = (o->len >> 1) * o->nf;
+        mem_fold_kernel<<<ceil_div(tot, 256), 256, 0, ctx->stream>>>(src, o->len, dst, o->nf, o->pending_r);
+        NEO_LAUNCHED(ctx);
+        o->cur ^= 1;
+        o->len >>= 1;
+        o->pending = false;
+    }
+    const uint32_t npts = o->deg + 1;
+    o->hvals.assign(npts, gl::kzero());
+    if (o->len == 1) {
+        std::vector<K> v(o->nf);
+        NEO_CK(ctx, cudaMemcpyAsync(v.data(), o->tab[o->cur].p, o->nf * sizeof(K), cudaMemcpyDeviceToHost, ctx->stream));
+        NEO_CK(ctx, cudaStreamSynchronize(ctx->stream));
+        K val;
+        if (o->bitness) {
+            K s = gl::kzero();
+            for (uint32_t f = 1; f < o->nf; f++)
+                s = gl::kadd(s, gl::kmul(gl::kmul(o->hw[f - 1], v[f]), gl::ksub(v[f], gl::kone())));
+            val = gl::kmul(v[0], s);
+        } else {
+            val = gl::kone();
+            for (uint32_t f = 0; f < o->nf; f++) val = gl::kmul(val, v[f]);
+        }
+        for (auto& h : o->hvals) h = val;
+        return NEO_OK;
+    }
+    const uint64_t pairs = o->len >> 1;
+    const uint32_t nb = (uint32_t)ceil_div(pairs, MT);
+    NEO_CK(ctx, o->partials.ensure((size_t)nb * npts));
+    MemEvalArgs a;
+    a.tab = o->tab[o->cur].p;
+    a.len = o->len;
+    a.nf = o->nf;
+    a.bitness = o->bitness;
+    a.w = o->w.p;
+    a.partials = o->partials.p;
+    mem_eval_kernel<<<dim3(nb, npts), MT, 0, ctx->stream>>>(a);
+    NEO_LAUNCHED(ctx);
+    mem_reduce_kernel<<<npts, 256, 0, ctx->stream>>>(o->partials.p, nb, o->vals.p);
+    NEO_LAUNCHED(ctx);
+    NEO_CK(ctx, cudaMemcpyAsync(o->hvals.data(), o->vals.p, npts * sizeof(K), cudaMemcpyDeviceToHost, ctx->stream));
+    NEO_CK(ctx, cudaStreamSynchronize(ctx->stream));
+    return NEO_OK;
+}
+
+// p(x) from p(0..n-1) (Lagrange on the integer nodes)
+K lagrange_at(const std::vector<K>& v, K x) {
+    const int n = (int)v.size();
+    if (x.im == 0 && x.re < (uint64_t)n) return v[x.re];
+    K acc = gl::kzero();
+    for (int i = 0; i < n; i++) {
+        K num = gl::kone();
+        uint64_t den = 1;
+        for (int j = 0; j < n; j++) {
+            if (j == i) continue;
+            num = gl::kmul(num, gl::ksub(x, gl::kfq((uint64_t)j)));
+            den = gl::mul(den, i > j ? (uint64_t)(i - j) : gl::neg((uint64_t)(j - i)));
+        }
+        acc = gl::kadd(acc, gl::kmul(v[i], gl::kscale(num, gl::inv(den))));
+    }
+    return acc;
+}
+
+int mem_create(neo_gpu_ctx* ctx, int kind, uint32_t ell, const uint64_t* r_point, uint32_t A, const uint64_t* r_addr,
+               const uint64_t* init, uint32_t n_cols, const uint64_t* cols, bool cols_on_device,
+               const uint64_t* weights, uint64_t* claim_out, neo_gpu_mem_oracle** out) {
+    if (!ctx || !out) return NEO_ERR_ARG;
+    *out = nullptr;
+    if (kind < NEO_MEM_SHOUT_VALUE || kind > NEO_MEM_PRODUCT) return ctx->fail(NEO_ERR_ARG, "mem_oracle: unknown kind");
+    if (ell > 30) return ctx->fail(NEO_ERR_ARG, "mem_oracle: ell > 30");
+    if (expected_cols(kind, A, n_cols) != (int)n_cols || (n_cols == 0 && kind != NEO_MEM_BITNESS))
+        return ctx->fail(NEO_ERR_ARG, "mem_oracle: column count does not match the kind");
+    const bool chi = kind <= NEO_MEM_TWIST_WRITE;
+    if ((chi || kind == NEO_MEM_VAL_EVAL) && !r_point) return ctx->fail(NEO_ERR_ARG, "mem_oracle: missing r_cycle / r_time");
+    if (A && !r_addr && kind != NEO_MEM_BITNESS && kind != NEO_MEM_PRODUCT && kind != NEO_MEM_SHOUT_VALUE)
+        return ctx->fail(NEO_ERR_ARG, "mem_oracle: missing r_addr");
+    if (kind == NEO_MEM_BITNESS && !weights && n_cols) return ctx->fail(NEO_ERR_ARG, "mem_oracle: missing weights");
+    if (!cols && n_cols) return ctx->fail(NEO_ERR_ARG, "mem_oracle: null columns");
+    const uint32_t deg = degree_of(kind, A, n_cols);
+    if (deg > MEM_MAX_DEG) return ctx->fail(NEO_ERR_UNSUPPORTED, "mem_oracle: degree bound above 31");
+    cudaSetDevice(ctx->device);
+
+    auto* o = new neo_gpu_mem_oracle();
+    o->ctx = ctx;
+    o->kind = kind;
+    o->ell = ell;
+    o->A = A;
+    o->deg = deg;
+    o->nf = factor_count(kind, A, n_cols);
+    o->bitness = kind == NEO_MEM_BITNESS;
+    o->len = 1ULL << ell;
+    const uint64_t L = o->len;
+    auto fail = [&](int rc) { delete o; return rc; };
+    if (o->tab[0].alloc((size_t)o->nf * L) || o->tab[1].alloc((size_t)o->nf * (L > 1 ? L / 2 : 1)) ||
+        o->vals.alloc(deg + 1))
+        return fail(ctx->fail(NEO_ERR_OOM, "mem_oracle: table allocation"));
+    K* T = o->tab[0].p;
+    cudaStream_t S = ctx->stream;
+    const cudaMemcpyKind cpk = cols_on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+    const size_t colb = L * sizeof(K);
+    auto col = [&](uint32_t c) { return reinterpret_cast<const K*>(cols) + (size_t)c * L; };
+    auto put = [&](uint32_t f, uint32_t c) { return cudaMemcpyAsync(T + (size_t)f * L, col(c), colb, cpk, S); };
+    DevBuf<K> dpt, dra, tmp;
+    if (r_point && dpt.alloc(ell ? ell : 1)) return fail(ctx->fail(NEO_ERR_OOM, "mem_oracle: point"));
+    if (r_point && ell && cudaMemcpyAsync(dpt.p, r_point, ell * sizeof(K), cudaMemcpyHostToDevice, S))
+        return fail(ctx->fail(NEO_ERR_CUDA, "mem_oracle: point upload"));
+    if (A && r_addr) {
+        if (dra.alloc(A) || cudaMemcpyAsync(dra.p, r_addr, A * sizeof(K), cudaMemcpyHostToDevice, S))
+            return fail(ctx->fail(NEO_ERR_OOM, "mem_oracle: r_addr"));
+    }
+    auto eqbits = [&](uint32_t f0, uint32_t c0) -> int {
+        for (uint32_t b = 0; b < A; b++) {
+            if (put(f0 + b, c0 + b)) return ctx->fail(NEO_ERR_CUDA, "mem_oracle: column upload");
+            eqbit_kernel<<<ceil_div(L, 256), 256, 0, S>>>(T + (size_t)(f0 + b) * L, L, kload_h(r_addr + 2 * b));
+            NEO_LAUNCHED(ctx);
+        }
+        return NEO_OK;
+    };
+    int rc = NEO_OK;
+    if (chi) {
+        rc = launch_chi_table(ctx, dpt.p, ell, T);  // factor 0 = χ_{r_cycle}
+        if (rc) return fail(rc);
+    }
+    cudaError_t ce = cudaSuccess;
+    switch (kind) {
+        case NEO_MEM_SHOUT_VALUE:
+            ce = put(1, 0);
+            if (!ce) ce = put(2, 1);
+            break;
+        case NEO_MEM_SHOUT_ADAPTER:
+            ce = put(1, 0);
+            if (!ce) rc = eqbits(2, 1);
+            break;
+        case NEO_MEM_BITNESS:
+            for (uint32_t c = 0; c < n_cols && !ce; c++) ce = put(1 + c, c);
+            for (uint32_t c = 0; c < n_cols; c++) o->hw.push_back(kload_h(weights + 2 * c));
+            if (!ce && n_cols && (o->w.alloc(n_cols) ||
+                        cudaMemcpyAsync(o->w.p, weights, n_cols * sizeof(K), cudaMemcpyHostToDevice, S)))
+                ce = cudaErrorMemoryAllocation;
+            break;
+        case NEO_MEM_TWIST_READ:
+        case NEO_MEM_TWIST_WRITE: {
+            const bool rd = kind == NEO_MEM_TWIST_READ;
+            // write stream columns: has_write, inc, wa bits
+            const uint32_t c_hw = rd ? 2 + A : 0, c_inc = rd ? 3 + A : 2, c_wa = rd ? 4 + A : 3;
+            const uint32_t c_a = rd ? 1 : 1;  // rv (read) or wv (write)
+            if (tmp.alloc((size_t)(4 + A) * L)) { ce = cudaErrorMemoryAllocation; break; }
+            K* hw = tmp.p;
+            K* inc = tmp.p + L;
+            K* aa = tmp.p + 2 * L;
+            K* terms = tmp.p + 3 * L;
+            K* wa = tmp.p + 4 * L;
+            ce = cudaMemcpyAsync(hw, col(c_hw), colb, cpk, S);
+            if (!ce) ce = cudaMemcpyAsync(inc, col(c_inc), colb, cpk, S);
+            if (!ce) ce = cudaMemcpyAsync(aa, col(c_a), colb, cpk, S);
+            if (!ce && A) ce = cudaMemcpyAsync(wa, col(c_wa), colb * A, cpk, S);
+            if (ce) break;
+            inc_terms_kernel<<<ceil_div(L, 256), 256, 0, S>>>(hw, inc, wa, A, dra.p, L, terms);
+            NEO_LAUNCHED(ctx);
+            const uint32_t nblk = (uint32_t)ceil_div(L, SCAN_BLK);
+            DevBuf<K> sums;
+            if (sums.alloc(nblk)) { ce = cudaErrorMemoryAllocation; break; }
+            scan_sums_kernel<<<nblk, SCAN_T, 0, S>>>(terms, L, sums.p);
+            NEO_LAUNCHED(ctx);
+            K init_k = init ? kload_h(init) : gl::kzero();
+            scan_top_kernel<<<1, SCAN_T, 0, S>>>(sums.p, nblk, init_k);
+            NEO_LAUNCHED(ctx);
+            // factor 2 = Val_pre − rv  |  wv − Val_pre − inc
+            scan_final_kernel<<<nblk, SCAN_T, 0, S>>>(terms, L, sums.p, rd ? 1 : 2, aa, inc, T + 2 * L);
+            NEO_LAUNCHED(ctx);
+            ce = put(1, 0);  // gate: has_read | has_write
+            if (!ce) rc = eqbits(3, rd ? 2 : 3);
+            if (!ce) ce = cudaStreamSynchronize(S);  // sums / tmp are released at scope exit
+        } break;
+        case NEO_MEM_VAL_EVAL:
+            ce = put(0, 0);
+            if (!ce) ce = put(1, 1);
+            if (ce) break;
+            lt_table_kernel<<<ceil_div(L, 256), 256, 0, S>>>(dpt.p, ell, T + 2 * L);
+            NEO_LAUNCHED(ctx);
+            rc = eqbits(3, 2);
+            break;
+        case NEO_MEM_TOTAL_INC:
+            ce = put(0, 0);
+            if (!ce) ce = put(1, 1);
+            if (!ce) rc = eqbits(2, 2);
+            break;
+        case NEO_MEM_PRODUCT:
+            for (uint32_t c = 0; c < n_cols && !ce; c++) ce = put(c, c);
+            break;
+    }
+    if (ce) return fail(ctx->fail(ce == cudaErrorMemoryAllocation ? NEO_ERR_OOM : NEO_ERR_CUDA, "mem_oracle: build", ce));
+    if (rc) return fail(rc);
+    // claim = Σ over the hypercube = p_0(0) + p_0(1)  (the constructors' sums)
+    rc = mem_round_values(o);
+    if (rc) return fail(rc);
+    o->claim = ell ? gl::kadd(o->hvals[0], o->hvals[1]) : o->hvals[0];
+    if (claim_out) {
+        claim_out[0] = o->claim.re;
+        claim_out[1] = o->claim.im;
+    }
+    NEO_CK(ctx, cudaStreamSynchronize(S));
+    *out = o;
+    return NEO_OK;
+}
+
+}  // namespace
+
+extern "C" int neo_gpu_mem_oracle_create(neo_gpu_ctx* ctx, int kind, uint32_t ell, const uint64_t* r_point,
+                                         uint32_t ell_addr, const uint64_t* r_addr, const uint64_t* init_at_r_addr,
+                                         uint32_t n_cols, const uint64_t* cols, const uint64_t* weights,
+                                         uint64_t* claim, neo_gpu_mem_oracle** out) {
+    return mem_create(ctx, kind, ell, r_point, ell_addr, r_addr, init_at_r_addr, n_cols, cols, false, weights, claim,
+                      out);
+}
+
+extern "C" int neo_gpu_mem_oracle_create_device(neo_gpu_ctx* ctx, int kind, uint32_t ell, const uint64_t* r_point,
+                                                uint32_t ell_addr, const uint64_t* r_addr,
+                                                const uint64_t* init_at_r_addr, uint32_t n_cols,
+                                                const uint64_t* d_cols, const uint64_t* weights, uint64_t* claim,
+                                                neo_gpu_mem_oracle** out) {
+    return mem_create(ctx, kind, ell, r_point, ell_addr, r_addr, init_at_r_addr, n_cols, d_cols, true, weights, claim,
+                      out);
+}
+
+extern "C" int neo_gpu_mem_oracle_evals(neo_gpu_mem_oracle* o, const uint64_t* xs, uint32_t nx, uint64_t* ys) {
+    if (!o) return NEO_ERR_ARG;
+    if ((!xs || !ys) && nx) return o->ctx->fail(NEO_ERR_ARG, "mem_oracle_evals: null buffer");
+    cudaSetDevice(o->ctx->device);
+    int rc = mem_round_values(o);
+    if (rc) return rc;
+    for (uint32_t i = 0; i < nx; i++) {
+        K y = lagrange_at(o->hvals, kload_h(xs + 2 * i));
+        ys[2 * i] = y.re;
+        ys[2 * i + 1] = y.im;
+    }
+    return NEO_OK;
+}
+
+extern "C" int neo_gpu_mem_oracle_fold(neo_gpu_mem_oracle* o, const uint64_t* r) {
+    if (!o) return NEO_ERR_ARG;
+    if (!r) return o->ctx->fail(NEO_ERR_ARG, "mem_oracle_fold: null challenge");
+    if (o->bit_idx >= o->ell) return NEO_OK;  // no rounds left: ignored, as in the reference
+    if (o->pending) {
+        // two folds without an evaluation in between: apply the first now
+        neo_gpu_ctx* ctx = o->ctx;
+        cudaSetDevice(ctx->device);
+        uint64_t tot = (o->len >> 1) * o->nf;
+        mem_fold_kernel<<<ceil_div(tot, 256), 256, 0, ctx->stream>>>(o->tab[o->cur].p, o->len, o->tab[o->cur ^ 1].p,
+                                                                     o->nf, o->pending_r);
+        NEO_LAUNCHED(ctx);
+        o->cur ^= 1;
+        o->len >>= 1;
+    }
+    o->pending = true;
+    o->pending_r = kload_h(r);
+    o->bit_idx++;
+    return NEO_OK;
+}
+
+extern "C" uint32_t neo_gpu_mem_oracle_num_rounds(const neo_gpu_mem_oracle* o) { return o ? o->ell - o->bit_idx : 0; }
+extern "C" uint32_t neo_gpu_mem_oracle_degree_bound(const neo_gpu_mem_oracle* o) { return o ? o->deg : 0; }
+
+extern "C" int neo_gpu_mem_oracle_destroy(neo_gpu_mem_oracle* o) {
+    if (!o) return NEO_OK;
+    cudaSetDevice(o->ctx->device);
+    cudaStreamSynchronize(o->ctx->stream);
+    delete o;
+    return NEO_OK;
+}
+
+extern "C" int neo_gpu_addr_lookup_weights(neo_gpu_ctx* ctx, uint32_t ell, const uint64_t* r_cycle, uint32_t ell_addr,
+                                           const uint64_t* has_lookup, const uint64_t* addr_bits,
+                                           const uint64_t* table, uint64_t table_len, uint64_t* weights,
+                                           uint64_t* claim) {
+    if (!ctx) return NEO_ERR_ARG;
+    if (!r_cycle || !has_lookup || (!addr_bits && ell_addr) || !weights || !claim || (!table && table_len))
+        return ctx->fail(NEO_ERR_ARG, "addr_lookup_weights: null buffer");
+    if (ell > 30 || ell_addr > 30) return ctx->fail(NEO_ERR_ARG, "addr_lookup_weights: size");
+    cudaSetDevice(ctx->device);
+    cudaStream_t S = ctx->stream;
+    const uint64_t L = 1ULL << ell, P = 1ULL << ell_addr;
+    DevBuf<K> dr, chi, has, bits, w, tab, part;
+    DevBuf<unsigned long long> acc;
+    NEO_CK(ctx, dr.alloc(ell ? ell : 1));
+    NEO_CK(ctx, chi.alloc(L));
+    NEO_CK(ctx, has.alloc(L));
+    NEO_CK(ctx, bits.alloc((size_t)L * (ell_addr ? ell_addr : 1)));
+    NEO_CK(ctx, acc.alloc(4 * P));
+    NEO_CK(ctx, w.alloc(P));
+    if (ell) NEO_CK(ctx, cudaMemcpyAsync(dr.p, r_cycle, ell * sizeof(K), cudaMemcpyHostToDevice, S));
+    NEO_CK(ctx, cudaMemcpyAsync(has.p, has_lookup, L * sizeof(K), cudaMemcpyHostToDevice, S));
+    if (ell_addr) NEO_CK(ctx, cudaMemcpyAsync(bits.p, addr_bits, (size_t)L * ell_addr * sizeof(K), cudaMemcpyHostToDevice, S));
+    NEO_CK(ctx, cudaMemsetAsync(acc.p, 0, 4 * P * sizeof(unsigned long long), S));
+    int rc = launch_chi_table(ctx, dr.p, ell, chi.p);
+    if (rc) return rc;
+    addr_weights_kernel<<<ceil_div(L, 256), 256, 0, S>>>(chi.p, has.p, bits.p, ell_addr, L, acc.p, acc.p + 2 * P);
+    NEO_LAUNCHED(ctx);
+    addr_weights_finish_kernel<<<ceil_div(P, 256), 256, 0, S>>>(acc.p, acc.p + 2 * P, P, w.p);
+    NEO_LAUNCHED(ctx);
+    const uint64_t n = table_len < P ? table_len : P;
+    const uint32_t nb = 148;
+    NEO_CK(ctx, part.alloc(nb));
+    DevBuf<K> out1;
+    NEO_CK(ctx, out1.alloc(1));
+    if (n) {
+        NEO_CK(ctx, tab.alloc(n));
+        NEO_CK(ctx, cudaMemcpyAsync(tab.p, table, n * sizeof(K), cudaMemcpyHostToDevice, S));
+    }
+    dot_kernel<<<nb, 256, 0, S>>>(tab.p, w.p, n, part.p);
+    NEO_LAUNCHED(ctx);
+    mem_reduce_kernel<<<1, 256, 0, S>>>(part.p, nb, out1.p);
+    NEO_LAUNCHED(ctx);
+    NEO_CK(ctx, cudaMemcpyAsync(weights, w.p, P * sizeof(K), cudaMemcpyDeviceToHost, S));
+    NEO_CK(ctx, cudaMemcpyAsync(claim, out1.p, sizeof(K), cudaMemcpyDeviceToHost, S));
+    NEO_CK(ctx, cudaStreamSynchronize(S));
+    return NEO_OK;
+}

@@ -69,6 +69,14 @@ SIGNATURES = {
     "neo_transcript_state": [P, P],
     "neo_transcript_destroy": [P],
     "neo_ccs_digest": [P, P],
+    "neo_gpu_mem_oracle_create": [P, I, U32, P, U32, P, P, U32, P, P, P, P],
+    "neo_gpu_mem_oracle_create_device": [P, I, U32, P, U32, P, P, U32, ctypes.c_void_p, P, P, P],
+    "neo_gpu_mem_oracle_evals": [P, P, U32, P],
+    "neo_gpu_mem_oracle_fold": [P, P],
+    "neo_gpu_mem_oracle_num_rounds": [P],
+    "neo_gpu_mem_oracle_degree_bound": [P],
+    "neo_gpu_mem_oracle_destroy": [P],
+    "neo_gpu_addr_lookup_weights": [P, U32, P, U32, P, P, P, U64, P, P],
 }
 _RESTYPES = {
     "neo_gpu_last_error": ctypes.c_char_p,
@@ -76,6 +84,8 @@ _RESTYPES = {
     "neo_gpu_ccs_oracle_num_rounds": U32,
     "neo_gpu_ccs_oracle_degree_bound": U32,
     "neo_gpu_batch_kernel_launches": U64,
+    "neo_gpu_mem_oracle_num_rounds": U32,
+    "neo_gpu_mem_oracle_degree_bound": U32,
 }
 
 _lib = None
@@ -259,6 +269,68 @@ class GpuCcsOracle:
 
     def __del__(self):
         self.close()
+
+
+MEM_SHOUT_VALUE, MEM_SHOUT_ADAPTER, MEM_BITNESS, MEM_TWIST_READ, MEM_TWIST_WRITE, MEM_VAL_EVAL, MEM_TOTAL_INC, \
+    MEM_PRODUCT = range(8)
+
+
+class GpuMemOracle:
+    """Twist / Shout time-lane RoundOracle on the GPU (crates/neo-memory/src/
+    twist_oracle.rs).  cols: uint64 [n_cols, 2^ell, 2] in the C ABI's column
+    order for `kind`; claim: the hypercube sum."""
+
+    def __init__(self, ctx: Context, kind: int, cols, r_point=None, r_addr=None, init=None, weights=None):
+        self.ctx = ctx
+        cols = _u64(cols)
+        n_cols, L = cols.shape[0], cols.shape[1]
+        ell = L.bit_length() - 1
+        if L != 1 << ell:
+            raise ValueError("column length must be a power of two")
+        self._keep = [None if r_point is None else _u64(r_point), None if r_addr is None else _u64(r_addr),
+                      None if init is None else _u64(init), None if weights is None else _u64(weights)]
+        ell_addr = 0 if r_addr is None else self._keep[1].shape[0]
+        self.claim = np.zeros(2, np.uint64)
+        h = ctypes.c_void_p()
+        ctx.check(ctx.lib.neo_gpu_mem_oracle_create(ctx.h, kind, ell, _p(self._keep[0]), ell_addr, _p(self._keep[1]),
+                                                    _p(self._keep[2]), n_cols, _p(cols), _p(self._keep[3]),
+                                                    _p(self.claim), ctypes.byref(h)))
+        self.h = h
+
+    def num_rounds(self) -> int:
+        return int(self.ctx.lib.neo_gpu_mem_oracle_num_rounds(self.h))
+
+    def degree_bound(self) -> int:
+        return int(self.ctx.lib.neo_gpu_mem_oracle_degree_bound(self.h))
+
+    def evals_at(self, xs: np.ndarray) -> np.ndarray:
+        xs = _u64(xs)
+        ys = np.empty_like(xs)
+        self.ctx.check(self.ctx.lib.neo_gpu_mem_oracle_evals(self.h, _p(xs), xs.shape[0], _p(ys)))
+        return ys
+
+    def fold(self, r: np.ndarray):
+        self.ctx.check(self.ctx.lib.neo_gpu_mem_oracle_fold(self.h, _p(_u64(r))))
+
+    def close(self):
+        if getattr(self, "h", None):
+            if self.ctx.h is not None:
+                self.ctx.lib.neo_gpu_mem_oracle_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
+
+
+def addr_lookup_weights(ctx: Context, r_cycle, has_lookup, addr_bits, table):
+    """AddressLookupOracle weight table and claimed sum on the GPU (twist_oracle.rs:1671-1724)."""
+    r_cycle, has_lookup, addr_bits, table = _u64(r_cycle), _u64(has_lookup), _u64(addr_bits), _u64(table)
+    ell, ell_addr = r_cycle.shape[0], addr_bits.shape[0]
+    w = np.empty((1 << ell_addr, 2), np.uint64)
+    claim = np.empty(2, np.uint64)
+    ctx.check(ctx.lib.neo_gpu_addr_lookup_weights(ctx.h, ell, _p(r_cycle), ell_addr, _p(has_lookup), _p(addr_bits),
+                                                  _p(table), table.shape[0], _p(w), _p(claim)))
+    return w, claim
 
 
 class Shard:

@@ -98,3 +98,56 @@ def kind_cols(kind, c, s=None):
     if kind in (5, 6):
         return np.concatenate([c["has_write"][None], c["inc"][None], c["wa_bits"]])
     raise ValueError(kind)
+
+
+# --- vectorised K helpers for size-independent checks --------------------------
+def _canon(x):
+    q = np.uint64(Q)
+    return np.where(x >= q, x - q, x)
+
+
+def kadd_np(a, b):
+    a, b = np.asarray(a, np.uint64), np.asarray(b, np.uint64)
+    s = a + b
+    s = s + (s < a).astype(np.uint64) * np.uint64(0xFFFFFFFF)
+    return _canon(s)
+
+
+def ksub_np(a, b):
+    a, b = np.asarray(a, np.uint64), np.asarray(b, np.uint64)
+    d = a - b
+    return d + (a < b).astype(np.uint64) * np.uint64(Q)
+
+
+def ksum_np(a):
+    """Σ over axis 0 of a (n, 2) K array, exactly (32-bit halves)."""
+    a = np.asarray(a, np.uint64)
+    lo = (a & np.uint64(0xFFFFFFFF)).sum(axis=0, dtype=np.uint64)
+    hi = (a >> np.uint64(32)).sum(axis=0, dtype=np.uint64)
+    return np.array([(int(lo[i]) + (int(hi[i]) << 32)) % Q for i in range(2)], np.uint64)
+
+
+def mle_eval(oracle_mod, col, point):
+    """Multilinear extension of a K column at a K point (little-endian variables)."""
+    chi = oracle_mod.chi_table(point)
+    return ksum_np(oracle_mod.k_mul(chi, col).reshape(-1, 2))
+
+
+def eq_bit_np(oracle_mod, col, u):
+    """eq_bit_affine(col, u) = col·(2u−1) + (1−u), elementwise."""
+    u = np.asarray(u, np.uint64)
+    two_u_m1 = ksub_np(kadd_np(u, u), np.array([1, 0], np.uint64))
+    one_m_u = ksub_np(np.array([1, 0], np.uint64), u)
+    prod = oracle_mod.k_mul(np.asarray(col, np.uint64).reshape(-1, 2),
+                            np.broadcast_to(two_u_m1, (col.shape[0], 2)).copy())
+    return kadd_np(prod, one_m_u)
+
+
+def excl_prefix_np(init, terms):
+    re, im = int(init[0]), int(init[1])
+    out = np.empty_like(terms)
+    for t in range(terms.shape[0]):
+        out[t, 0], out[t, 1] = re, im
+        re = (re + int(terms[t, 0])) % Q
+        im = (im + int(terms[t, 1])) % Q
+    return out
