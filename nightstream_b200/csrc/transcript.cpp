@@ -103,32 +103,50 @@ const Poseidon2W16& digest_perm() {
 
 typedef unsigned __int128 u128;
 
-// reduce x < 2^128 mod q (2^64 = 2^32 - 1, 2^96 = -1); canonical result
-static inline uint64_t red128(u128 x) { return gl::reduce128((uint64_t)x, (uint64_t)(x >> 64)); }
-
+// Permutation arithmetic keeps lanes in [0, 2^64) (not necessarily < q) and
+// canonicalises once at the end. Corrections are masks, not branches: the
+// carries are data dependent, and a mispredicted branch per reduction costs
+// more than the whole multiply. State loops are fully unrolled so the eight
+// independent S-box chains of a full round overlap.
+static inline uint64_t red_nc(uint64_t lo, uint64_t hi) {
+    // lo + 2^64 hi with 2^64 = 2^32 - 1 and 2^96 = -1 (mod q)
+    const uint64_t hh = hi >> 32, hl = hi & GL_EPS;
+    uint64_t t0;
+    const uint64_t br = __builtin_sub_overflow(lo, hh, &t0);
+    t0 -= GL_EPS & (0 - br);
+    const uint64_t t1 = (hl << 32) - hl;
+    uint64_t s;
+    const uint64_t c = __builtin_add_overflow(t0, t1, &s);
+    return s + (GL_EPS & (0 - c));
+}
+static inline uint64_t red128(u128 x) { return red_nc((uint64_t)x, (uint64_t)(x >> 64)); }
 static inline uint64_t mulq(uint64_t a, uint64_t b) { return red128((u128)a * b); }
+static inline uint64_t addq(uint64_t a, uint64_t b) {
+    uint64_t s;
+    const uint64_t c = __builtin_add_overflow(a, b, &s);
+    return s + (GL_EPS & (0 - c));
+}
+static inline uint64_t canonq(uint64_t a) { return a >= GL_Q ? a - GL_Q : a; }
 
 static inline uint64_t sbox7(uint64_t x) {
-    uint64_t x2 = mulq(x, x);
-    uint64_t x3 = mulq(x2, x);
-    uint64_t x6 = mulq(x3, x3);
-    return mulq(x6, x);
+    const uint64_t x2 = mulq(x, x);
+    const uint64_t x3 = mulq(x2, x);
+    const uint64_t x4 = mulq(x2, x2);
+    return mulq(x3, x4);
 }
 
 // M4 = [[5,7,1,3],[4,6,1,1],[1,3,5,7],[1,1,4,6]] by the Poseidon2 paper's
 // addition chain (8 additions, 4 doublings); inputs < 2^64, outputs < 2^69.
 static inline void m4_lazy(const uint64_t* x, u128* y) {
-    u128 t0 = (u128)x[0] + x[1];
-    u128 t1 = (u128)x[2] + x[3];
-    u128 t2 = ((u128)x[1] << 1) + t1;
-    u128 t3 = ((u128)x[3] << 1) + t0;
-    u128 t4 = (t1 << 2) + t3;
-    u128 t5 = (t0 << 2) + t2;
-    u128 t6 = t3 + t5;
-    u128 t7 = t2 + t4;
-    y[0] = t6;
+    const u128 t0 = (u128)x[0] + x[1];
+    const u128 t1 = (u128)x[2] + x[3];
+    const u128 t2 = ((u128)x[1] << 1) + t1;
+    const u128 t3 = ((u128)x[3] << 1) + t0;
+    const u128 t4 = (t1 << 2) + t3;
+    const u128 t5 = (t0 << 2) + t2;
+    y[0] = t3 + t5;
     y[1] = t5;
-    y[2] = t7;
+    y[2] = t2 + t4;
     y[3] = t4;
 }
 
@@ -136,37 +154,49 @@ static inline void m4_lazy(const uint64_t* x, u128* y) {
 template <int W>
 static inline void external_layer(uint64_t* st) {
     u128 y[W];
+#pragma GCC unroll 4
     for (int b = 0; b < W / 4; b++) m4_lazy(st + 4 * b, y + 4 * b);
+#pragma GCC unroll 4
     for (int i = 0; i < 4; i++) {
         u128 s = 0;
+#pragma GCC unroll 4
         for (int b = 0; b < W / 4; b++) s += y[4 * b + i];
+#pragma GCC unroll 4
         for (int b = 0; b < W / 4; b++) st[4 * b + i] = red128(y[4 * b + i] + s);
     }
 }
 
 template <int W>
-static inline void internal_layer(uint64_t* st, const uint64_t* mu) {
-    u128 acc = 0;
-    for (int i = 0; i < W; i++) acc += st[i];
-    const uint64_t sum = red128(acc);
-    for (int i = 0; i < W; i++) st[i] = red128((u128)mu[i] * st[i] + sum);
+static inline void full_round(uint64_t* st, const uint64_t* rc) {
+#pragma GCC unroll 16
+    for (int i = 0; i < W; i++) st[i] = sbox7(addq(st[i], rc[i]));
+    external_layer<W>(st);
 }
 
 template <int W>
-void Poseidon2<W>::permute(uint64_t* st) const {
+void Poseidon2<W>::permute(uint64_t* st_io) const {
+    uint64_t st[W];
+    uint64_t m[W];
+#pragma GCC unroll 16
+    for (int i = 0; i < W; i++) {
+        st[i] = st_io[i];
+        m[i] = mu[i];
+    }
     external_layer<W>(st);
-    for (int r = 0; r < RF / 2; r++) {
-        for (int i = 0; i < W; i++) st[i] = sbox7(gl::add(st[i], rc_ext[r][i]));
-        external_layer<W>(st);
-    }
+    for (int r = 0; r < RF / 2; r++) full_round<W>(st, rc_ext[r]);
     for (int r = 0; r < RP; r++) {
-        st[0] = sbox7(gl::add(st[0], rc_int[r]));
-        internal_layer<W>(st, mu);
+        st[0] = sbox7(addq(st[0], rc_int[r]));
+        // internal layer: M_I x = sum(x) + mu_i * x_i
+        u128 acc = 0;
+#pragma GCC unroll 16
+        for (int i = 0; i < W; i++) acc += st[i];
+        const uint64_t sum = red128(acc);
+#pragma GCC unroll 16
+        for (int i = 0; i < W; i++) st[i] = red128((u128)m[i] * st[i] + sum);
     }
-    for (int r = RF / 2; r < RF; r++) {
-        for (int i = 0; i < W; i++) st[i] = sbox7(gl::add(st[i], rc_ext[r][i]));
-        external_layer<W>(st);
-    }
+    for (int r = RF / 2; r < RF; r++) full_round<W>(st, rc_ext[r]);
+#pragma GCC unroll 16
+    for (int i = 0; i < W; i++) st_io[i] = canonq(st[i]);
 }
 
 template struct Poseidon2<8>;
