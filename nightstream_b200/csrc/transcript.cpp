@@ -108,7 +108,7 @@ typedef unsigned __int128 u128;
 // carries are data dependent, and a mispredicted branch per reduction costs
 // more than the whole multiply. State loops are fully unrolled so the eight
 // independent S-box chains of a full round overlap.
-static inline uint64_t red_nc(uint64_t lo, uint64_t hi) {
+static inline __attribute__((always_inline)) uint64_t red_nc(uint64_t lo, uint64_t hi) {
     // lo + 2^64 hi with 2^64 = 2^32 - 1 and 2^96 = -1 (mod q)
     const uint64_t hh = hi >> 32, hl = hi & GL_EPS;
     uint64_t t0;
@@ -119,16 +119,16 @@ static inline uint64_t red_nc(uint64_t lo, uint64_t hi) {
     const uint64_t c = __builtin_add_overflow(t0, t1, &s);
     return s + (GL_EPS & (0 - c));
 }
-static inline uint64_t red128(u128 x) { return red_nc((uint64_t)x, (uint64_t)(x >> 64)); }
-static inline uint64_t mulq(uint64_t a, uint64_t b) { return red128((u128)a * b); }
-static inline uint64_t addq(uint64_t a, uint64_t b) {
+static inline __attribute__((always_inline)) uint64_t red128(u128 x) { return red_nc((uint64_t)x, (uint64_t)(x >> 64)); }
+static inline __attribute__((always_inline)) uint64_t mulq(uint64_t a, uint64_t b) { return red128((u128)a * b); }
+static inline __attribute__((always_inline)) uint64_t addq(uint64_t a, uint64_t b) {
     uint64_t s;
     const uint64_t c = __builtin_add_overflow(a, b, &s);
     return s + (GL_EPS & (0 - c));
 }
-static inline uint64_t canonq(uint64_t a) { return a >= GL_Q ? a - GL_Q : a; }
+static inline __attribute__((always_inline)) uint64_t canonq(uint64_t a) { return a >= GL_Q ? a - GL_Q : a; }
 
-static inline uint64_t sbox7(uint64_t x) {
+static inline __attribute__((always_inline)) uint64_t sbox7(uint64_t x) {
     const uint64_t x2 = mulq(x, x);
     const uint64_t x3 = mulq(x2, x);
     const uint64_t x4 = mulq(x2, x2);
@@ -137,7 +137,7 @@ static inline uint64_t sbox7(uint64_t x) {
 
 // M4 = [[5,7,1,3],[4,6,1,1],[1,3,5,7],[1,1,4,6]] by the Poseidon2 paper's
 // addition chain (8 additions, 4 doublings); inputs < 2^64, outputs < 2^69.
-static inline void m4_lazy(const uint64_t* x, u128* y) {
+static inline __attribute__((always_inline)) void m4_lazy(const uint64_t* x, u128* y) {
     const u128 t0 = (u128)x[0] + x[1];
     const u128 t1 = (u128)x[2] + x[3];
     const u128 t2 = ((u128)x[1] << 1) + t1;
@@ -152,7 +152,7 @@ static inline void m4_lazy(const uint64_t* x, u128* y) {
 
 // external layer circ(2 M4, M4, ..., M4): y_blk = M4 x_blk + sum_blk' M4 x_blk'
 template <int W>
-static inline void external_layer(uint64_t* st) {
+static inline __attribute__((always_inline)) void external_layer(uint64_t* st) {
     u128 y[W];
 #pragma GCC unroll 4
     for (int b = 0; b < W / 4; b++) m4_lazy(st + 4 * b, y + 4 * b);
@@ -166,37 +166,50 @@ static inline void external_layer(uint64_t* st) {
     }
 }
 
+// the S-box steps of all lanes are issued stage by stage (x^2, x^3, x^4, x^7)
+// so the independent multiply chains interleave
 template <int W>
-static inline void full_round(uint64_t* st, const uint64_t* rc) {
+static inline __attribute__((always_inline)) void full_round(uint64_t* st, const uint64_t* rc) {
+    uint64_t x[W], x2[W], x3[W], x4[W];
 #pragma GCC unroll 16
-    for (int i = 0; i < W; i++) st[i] = sbox7(addq(st[i], rc[i]));
+    for (int i = 0; i < W; i++) x[i] = addq(st[i], rc[i]);
+#pragma GCC unroll 16
+    for (int i = 0; i < W; i++) x2[i] = mulq(x[i], x[i]);
+#pragma GCC unroll 16
+    for (int i = 0; i < W; i++) x3[i] = mulq(x2[i], x[i]);
+#pragma GCC unroll 16
+    for (int i = 0; i < W; i++) x4[i] = mulq(x2[i], x2[i]);
+#pragma GCC unroll 16
+    for (int i = 0; i < W; i++) st[i] = mulq(x3[i], x4[i]);
     external_layer<W>(st);
 }
 
 template <int W>
-void Poseidon2<W>::permute(uint64_t* st_io) const {
+__attribute__((noinline)) static void permute_impl(const Poseidon2<W>& P, uint64_t* st_io) {
+    constexpr int RF = Poseidon2<W>::RF, RP = Poseidon2<W>::RP;
     uint64_t st[W];
-    uint64_t m[W];
 #pragma GCC unroll 16
-    for (int i = 0; i < W; i++) {
-        st[i] = st_io[i];
-        m[i] = mu[i];
-    }
+    for (int i = 0; i < W; i++) st[i] = st_io[i];
     external_layer<W>(st);
-    for (int r = 0; r < RF / 2; r++) full_round<W>(st, rc_ext[r]);
+    for (int r = 0; r < RF / 2; r++) full_round<W>(st, P.rc_ext[r]);
     for (int r = 0; r < RP; r++) {
-        st[0] = sbox7(addq(st[0], rc_int[r]));
+        st[0] = sbox7(addq(st[0], P.rc_int[r]));
         // internal layer: M_I x = sum(x) + mu_i * x_i
         u128 acc = 0;
 #pragma GCC unroll 16
         for (int i = 0; i < W; i++) acc += st[i];
         const uint64_t sum = red128(acc);
 #pragma GCC unroll 16
-        for (int i = 0; i < W; i++) st[i] = red128((u128)m[i] * st[i] + sum);
+        for (int i = 0; i < W; i++) st[i] = red128((u128)P.mu[i] * st[i] + sum);
     }
-    for (int r = RF / 2; r < RF; r++) full_round<W>(st, rc_ext[r]);
+    for (int r = RF / 2; r < RF; r++) full_round<W>(st, P.rc_ext[r]);
 #pragma GCC unroll 16
     for (int i = 0; i < W; i++) st_io[i] = canonq(st[i]);
+}
+
+template <int W>
+void Poseidon2<W>::permute(uint64_t* st_io) const {
+    permute_impl<W>(*this, st_io);
 }
 
 template struct Poseidon2<8>;
