@@ -107,11 +107,82 @@ class Clocks:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
+# DRAM bytes (read + write) of one 12-plane commit_tc launch per witness column,
+# from an ncu capture at m = 2^14 (166.56 MB / 16384); the tiles scale with m.
+COMMIT_TRAFFIC_PER_M = 166.56e6 / 16384
+
+
+# DRAM bytes (read + write) of the 16 row-round launches of one k = 13 step,
+# per row, from an ncu capture at 2^16 rows (347.2 MB / 65536).
+ROUNDS_TRAFFIC_PER_ROW = 347.22e6 / 65536
+
+
 def measured_peaks():
     try:
         return json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
     except (OSError, ValueError):
         return {}
+
+
+def flush_l2():
+    """Write 512 MB (4x the 126 MB L2) so the next launch starts cold."""
+    import torch
+    buf = torch.empty(512 << 20, dtype=torch.uint8, device="cuda")
+    buf.fill_(1)
+    del buf
+
+
+def rounds_roofline(ctx, ccs, z, ell, stream, reps=3):
+    """The Pi_CCS time rounds of a steady-state step (k = 13: the MCS witness
+    and 12 carried DEC children), all ell row rounds launched back to back
+    through neo_gpu_ccs_oracle_row_rounds_device and timed with CUDA events on
+    the library stream. L2 is flushed before each timed sequence.
+    Algorithmic bytes B_ccs = 2^ell [(54k + 48) + 32 (54k + 6)]: round 0 reads
+    the witness at compact width, every later round reads and writes the
+    K-width tables."""
+    import torch
+    from nightstream_b200 import gpu, synth
+    m = 1 << ell
+    rng = np.random.default_rng(1234)
+    Z0 = ctx.decomp_b2(z)
+    Z = np.stack([Z0] + [rng.integers(-1, 2, size=(54, m)).astype(np.int8) for _ in range(12)])
+    k = Z.shape[0]
+    d = torch.empty((ell, 7, 2), dtype=torch.int64, device="cuda")
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    times = []
+    launches = 0
+    for rep in range(reps + 1):
+        uk = lambda n: synth.uniform_k(rng, n)
+        o = gpu.GpuCcsOracle(ctx, ccs, Z, 2, uk(6), uk(6), uk(ell), uk(1)[0], uk(ell), 6, ell, 6)
+        ctx.synchronize()
+        flush_l2()
+        torch.cuda.synchronize()
+        l0 = ctx.kernel_launches
+        ev0.record(stream)
+        o.row_rounds_device(uk(ell), d.data_ptr())
+        ev1.record(stream)
+        ev1.synchronize()
+        if rep:
+            times.append(ev0.elapsed_time(ev1))
+            launches = ctx.kernel_launches - l0
+        o.close()
+    ms = statistics.median(times)
+    B = m * ((54 * k + 48) + 32 * (54 * k + 6))
+    peak = measured_peaks().get("hbm_gbs")
+    src = "measured HBM copy bandwidth (MEASURED_PEAKS.json hbm_gbs)"
+    if not peak:
+        peak, src = 6650.0, "fallback 6.65 TB/s"
+    achieved = B / (ms * 1e-3) / 1e9
+    return {"kernel": f"Pi_CCS time rounds: ccs_round_kernel<0..5> + reduce_eval_kernel, {ell} rounds, k = {k}, "
+                      f"{launches} launches per sequence",
+            "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+            "traffic": ROUNDS_TRAFFIC_PER_ROW * m,
+            "traffic_source": "ncu dram__bytes_read+write of the 16 row-round launches of one k = 13 step at "
+                              "2^16 rows, per row (profiles/ccs_round_kernel_ell16_k13.md)",
+            "launch_ms": ms / ell, "sequence_ms": ms, "peak_source": src,
+            "algorithmic_bytes_per_sequence": B,
+            "note": "integer-ALU bound: the rounds stream int8 digit planes in rounds 0..4 and move far fewer "
+                    "bytes than B_ccs; see profiles/ccs_round_kernel_ell16_k13.md"}
 
 
 def int8_peak_tops():
@@ -372,17 +443,21 @@ def run_ours(args, rank, world, local_rank):
     ops = 746496 * m * n_vec  # 2 * 8 limbs * kappa * d^2 * m per commitment
     peak, peak_src = int8_peak_tops()
     achieved = ops / (commit_ms * 1e-3) / 1e12
-    roofline = {"kernel": "Ajtai commit, 12 DEC planes per launch (commit_tc_kernel: tcgen05 kind::i8, + commit_tc_reduce_kernel)",
-                "bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TOPS", "frac": achieved / peak,
-                "traffic": None, "launch_ms": commit_ms, "peak_source": peak_src,
-                "algorithmic_ops_per_launch": ops}
+    roofline_commit = {"kernel": "Ajtai commit, 12 DEC planes per launch (commit_tc_kernel: tcgen05 kind::i8, "
+                                 "+ commit_tc_reduce_kernel)",
+                       "bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TOPS", "frac": achieved / peak,
+                       "traffic": COMMIT_TRAFFIC_PER_M * m if m >= 1 << 14 else None,
+                       "traffic_source": "ncu dram__bytes_read+write of one 12-plane launch at m = 2^14, scaled by m "
+                                         "(profiles/commit_tc_kernel_m16384_12planes.md)",
+                       "launch_ms": commit_ms, "peak_source": peak_src, "algorithmic_ops_per_launch": ops}
+    roofline = rounds_roofline(ctx, ccs, z, args.ell, stream)
 
     if rank == 0:
         out = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
                "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
                "vs_baseline": None, "dtype": "u64 (F_q, K = F_q^2), int8 digits", "data": "synthetic",
                "config": config(args.ell), "e2e": e2e, "gpu_launches": int(launches), "clocks": clk,
-               "roofline": roofline, "step_breakdown_ms": stats}
+               "roofline": roofline, "roofline_commit": roofline_commit, "step_breakdown_ms": stats}
         if world == 1 and not args.no_cpu_baseline:
             out["cpu_baseline"] = cpu_baseline(args.ell, ccs, z, pp)
         if world == 1 and args.batch_in_plain:

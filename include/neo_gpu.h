@@ -134,6 +134,14 @@ int neo_gpu_ccs_oracle_create(neo_gpu_ctx* ctx, const neo_ccs_desc* ccs, const i
 int neo_gpu_ccs_oracle_evals(neo_gpu_ccs_oracle* o, const uint64_t* xs, uint32_t nx, uint64_t* ys);
 /* RoundOracle::fold (oracle.rs:2095-2103). */
 int neo_gpu_ccs_oracle_fold(neo_gpu_ccs_oracle* o, const uint64_t* r);
+/* No counterpart in the reference (its rounds are driven one at a time by the
+ * transcript): runs the next n row rounds back to back with caller-chosen
+ * challenges chals[n] (host K), writing each round polynomial's d_sc + 1
+ * coefficients (lowest first) to d_coeffs[n][d_sc + 1] (device K), with no
+ * host synchronisation in between.  For fixed-challenge replays, benchmarks
+ * and graph capture; the oracle is left after those n folds. */
+int neo_gpu_ccs_oracle_row_rounds_device(neo_gpu_ccs_oracle* o, const uint64_t* chals, uint32_t n,
+                                         uint64_t* d_coeffs);
 uint32_t neo_gpu_ccs_oracle_num_rounds(const neo_gpu_ccs_oracle* o);
 uint32_t neo_gpu_ccs_oracle_degree_bound(const neo_gpu_ccs_oracle* o);
 /* build_me_outputs_from_ajtai_precomp (oracle.rs:1955-2072), after the

@@ -586,6 +586,7 @@ struct neo_gpu_ccs_oracle {
     int nc_cur = 0;
     int J = 0;
     DevBuf<K> wg, eqw, partials, coeffs, ys, scratch_k;
+    DevBuf<K> d_chals;  // row challenges on the device (prefix χ tables of the streaming rounds)
     K gamma{}, gamma_to_k{};
     std::vector<K> alpha, beta_a, beta_r, r_in, row_chals, ajtai_chals;
     bool has_inputs = false, has_eval = false;
@@ -814,6 +815,7 @@ static int oracle_init(neo_gpu_ctx* ctx, neo_gpu_ccs_oracle* o, const int8_t* d_
         NEO_CK(ctx, o->nc[1].ensure((size_t)nq * LJ / 2 + 1));
     }
     NEO_CK(ctx, o->eqw.ensure(1 << JMAX));
+    NEO_CK(ctx, o->d_chals.ensure(o->ell_n ? o->ell_n : 1));
     uint64_t max_blocks = (uint64_t)ceil_div(n_pad / 2, RT) * nq + 16;
     NEO_CK(ctx, o->partials.ensure(max_blocks * (o->deg_max + 1)));
     NEO_CK(ctx, o->coeffs.ensure(MAX_DEG + 1));
@@ -822,7 +824,10 @@ static int oracle_init(neo_gpu_ctx* ctx, neo_gpu_ccs_oracle* o, const int8_t* d_
     return NEO_OK;
 }
 
-static int row_round(neo_gpu_ccs_oracle* o) {
+// Launches row round j = round_idx (folding the previous challenge in) and
+// leaves its deg_max + 1 coefficients in coeffs_dst (device); no host sync.
+// d_chals must hold the row challenges of the rounds already bound.
+static int row_round_launch(neo_gpu_ccs_oracle* o, K* coeffs_dst) {
     neo_gpu_ctx* ctx = o->ctx;
     const uint32_t j = o->round_idx;
     const uint32_t nq = o->k * NEO_D;
@@ -858,10 +863,9 @@ static int row_round(neo_gpu_ccs_oracle* o) {
     const int J = o->J;
     if ((int)j <= J) {
         if (j > 0) {
-            std::vector<K> w(1u << j);
-            std::vector<K> pre(o->row_chals.begin(), o->row_chals.begin() + j);
-            for (uint32_t bsel = 0; bsel < (1u << j); bsel++) w[bsel] = host_chi_mask(bsel, pre);
-            NEO_CK(ctx, cudaMemcpyAsync(o->eqw.p, w.data(), w.size() * 16, cudaMemcpyHostToDevice, ctx->stream));
+            // χ of the bound prefix r_0..r_{j-1}
+            int rc = launch_chi_table(ctx, o->d_chals.p, j, o->eqw.p);
+            if (rc) return rc;
         }
         a.eqw = o->eqw.p;
         if ((int)j == J && !last) {
@@ -905,10 +909,21 @@ static int row_round(neo_gpu_ccs_oracle* o) {
     e.nblocks = gx * gy;
     e.ncoef = o->deg_max + 1;
     e.nx = 0;
-    e.coeffs_out = o->coeffs.p;
+    e.coeffs_out = coeffs_dst;
     e.ys_out = o->ys.p;
     reduce_eval_kernel<<<1, 256, 0, ctx->stream>>>(e);
     NEO_LAUNCHED(ctx);
+    return NEO_OK;
+}
+
+static int row_round(neo_gpu_ccs_oracle* o) {
+    neo_gpu_ctx* ctx = o->ctx;
+    const uint32_t j = o->round_idx;
+    if (j > 0 && (int)j <= o->J)
+        NEO_CK(ctx, cudaMemcpyAsync(o->d_chals.p, o->row_chals.data(), j * sizeof(K), cudaMemcpyHostToDevice,
+                                    ctx->stream));
+    int rc = row_round_launch(o, o->coeffs.p);
+    if (rc) return rc;
     o->h_coeffs.resize(o->deg_max + 1);
     NEO_CK(ctx, cudaMemcpyAsync(o->h_coeffs.data(), o->coeffs.p, (o->deg_max + 1) * 16, cudaMemcpyDeviceToHost, ctx->stream));
     NEO_CK(ctx, cudaStreamSynchronize(ctx->stream));
@@ -1007,6 +1022,31 @@ extern "C" int neo_gpu_ccs_oracle_fold(neo_gpu_ccs_oracle* o, const uint64_t* r)
         return o->ctx->fail(NEO_ERR_ARG, "fold: all rounds done");
     }
     o->round_idx++;
+    return NEO_OK;
+}
+
+extern "C" int neo_gpu_ccs_oracle_row_rounds_device(neo_gpu_ccs_oracle* o, const uint64_t* chals, uint32_t n,
+                                                    uint64_t* d_coeffs) {
+    if (!o) return NEO_ERR_ARG;
+    neo_gpu_ctx* ctx = o->ctx;
+    if (!chals || !d_coeffs || n == 0) return ctx->fail(NEO_ERR_ARG, "row_rounds_device: bad args");
+    if (o->round_idx + n > o->ell_n) return ctx->fail(NEO_ERR_ARG, "row_rounds_device: beyond the row rounds");
+    cudaSetDevice(ctx->device);
+    const uint32_t j0 = o->round_idx;
+    for (uint32_t i = 0; i < n; i++) o->row_chals.push_back(gl::kmk(gl::canon(chals[2 * i]), gl::canon(chals[2 * i + 1])));
+    // every challenge of the sequence goes up once; round j reads only the first j
+    NEO_CK(ctx, cudaMemcpyAsync(o->d_chals.p, o->row_chals.data(), (j0 + n) * sizeof(K), cudaMemcpyHostToDevice,
+                                ctx->stream));
+    // rounds are written at stride d_sc + 1; coefficients above deg_max are zero
+    const uint32_t ncoef = o->d_sc + 1;
+    if ((uint32_t)o->deg_max > o->d_sc) return ctx->fail(NEO_ERR_INVARIANT, "row_rounds_device: degree above d_sc");
+    NEO_CK(ctx, cudaMemsetAsync(d_coeffs, 0, (size_t)n * ncoef * sizeof(K), ctx->stream));
+    for (uint32_t i = 0; i < n; i++) {
+        int rc = row_round_launch(o, reinterpret_cast<K*>(d_coeffs) + (size_t)i * ncoef);
+        if (rc) return rc;
+        o->round_idx++;
+    }
+    o->coeffs_valid = false;
     return NEO_OK;
 }
 

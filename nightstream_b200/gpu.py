@@ -38,6 +38,7 @@ SIGNATURES = {
     "neo_gpu_ccs_oracle_evals": [P, P, U32, P],
     "neo_gpu_ccs_oracle_fold": [P, P],
     "neo_gpu_ccs_oracle_num_rounds": [P],
+    "neo_gpu_ccs_oracle_row_rounds_device": [P, P, U32, ctypes.c_void_p],
     "neo_gpu_ccs_oracle_degree_bound": [P],
     "neo_gpu_ccs_oracle_me_outputs": [P, P, P],
     "neo_gpu_ccs_oracle_destroy": [P],
@@ -254,6 +255,12 @@ class GpuCcsOracle:
         self.ctx.check(self.ctx.lib.neo_gpu_ccs_oracle_fold(self.h, _p(r)))
 
     bind = fold
+
+    def row_rounds_device(self, chals: np.ndarray, d_coeffs: int):
+        """Next len(chals) row rounds back to back; coefficients to device memory."""
+        chals = _u64(chals)
+        self.ctx.check(self.ctx.lib.neo_gpu_ccs_oracle_row_rounds_device(self.h, _p(chals), chals.shape[0],
+                                                                         d_coeffs))
 
     def me_outputs(self):
         y = np.empty((self.k, self.t, 54, 2), np.uint64)

@@ -116,3 +116,34 @@ def test_ccs_oracle_all_rounds_match(ctx, ell, k, inputs):
 def test_ccs_oracle_steady_state_full_size(ctx):
     # k = 13 (1 MCS + 12 carried children), n = m = 2^16
     _run_both(ctx, 16, 13, True, seed=11)
+
+
+def test_row_rounds_device_matches_oracle(ctx):
+    """The back-to-back device round sequence gives the same round polynomials
+    as the transcript-driven rounds, and the Ajtai rounds continue from it."""
+    import torch
+    from nightstream_b200.gpu import GpuCcsOracle
+    ell, k = 10, 3
+    ccs, z, Z, ch, chals = ccs_case(ell, k, True)
+    args = (ccs, Z, 2, ch["alpha"], ch["beta_a"], ch["beta_r"], ch["gamma"], ch["r_inputs"], ELL_D, ell, D_SC)
+    g = GpuCcsOracle(ctx, *args)
+    o = O.CcsOracle(*args)
+    d = torch.zeros((ell, D_SC + 1, 2), dtype=torch.int64, device="cuda")
+    torch.cuda.synchronize()
+    g.row_rounds_device(chals[:4], d.data_ptr())
+    g.row_rounds_device(chals[4:ell], d[4:].data_ptr())
+    ctx.synchronize()
+    coeffs = d.cpu().numpy().view(np.uint64)
+    for r in range(ell):
+        yo = o.evals_at(XS)
+        yg = np.stack([O.poly_eval_k(coeffs[r], x) for x in XS])
+        assert np.array_equal(yg, yo), f"round {r}"
+        o.fold(chals[r])
+    for r in range(ell, ell + ELL_D):
+        assert np.array_equal(g.evals_at(XS), o.evals_at(XS)), f"round {r}"
+        g.fold(chals[r])
+        o.fold(chals[r])
+    yg, ysg = g.me_outputs()
+    yo, yso = o.me_outputs()
+    assert np.array_equal(yg, yo) and np.array_equal(ysg, yso)
+    g.close()
