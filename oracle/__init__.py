@@ -74,14 +74,22 @@ def lib():
             "or_mem_oracle_evals": [P, P, I, P],
             "or_mem_oracle_fold": [P, P],
             "or_addr_lookup_weights": [I, P, I, P, P, P, SZ, P, P],
+            "or_twist_addr_new": [I, I, P, I, SZ, P, P, P],
+            "or_twist_addr_free": [P],
+            "or_twist_addr_num_rounds": [P],
+            "or_twist_addr_evals": [P, P, I, P],
+            "or_twist_addr_fold": [P, P],
+            "or_bus_openings": [P, I64, I64, I64, I, I64, P, I, P, P],
         }
         for name, args in sigs.items():
             fn = getattr(L, name)
             fn.argtypes = args
             fn.restype = I if name in ("or_split_b", "or_ccs_oracle_num_rounds", "or_ccs_sumcheck_fixed",
-                                        "or_mem_oracle_num_rounds", "or_mem_oracle_degree_bound") else None
+                                        "or_mem_oracle_num_rounds", "or_mem_oracle_degree_bound",
+                                        "or_twist_addr_num_rounds") else None
         L.or_ccs_oracle_new.restype = P
         L.or_mem_oracle_new.restype = P
+        L.or_twist_addr_new.restype = P
         L.or_tr_new.restype = P
         L.or_tr_challenge_field.restype = ctypes.c_uint64
         _lib = L
@@ -376,3 +384,49 @@ def addr_lookup_weights(r_cycle, has_lookup, addr_bits, table):
     lib().or_addr_lookup_weights(ell, ptr(r_cycle), ell_addr, ptr(has_lookup), ptr(addr_bits), ptr(table),
                                  table.shape[0], ptr(w), ptr(claim))
     return w, claim
+
+
+class TwistAddrOracle:
+    """Twist address-lane read (kind 0) / write (kind 1) check oracle
+    (twist_oracle.rs:1259-1642); degree bound 2, ell_addr rounds."""
+
+    def __init__(self, kind, cols, r_cycle, ell_addr, init_pairs=()):
+        self.cols = u64(cols)
+        L = self.cols.shape[1]
+        ell = L.bit_length() - 1
+        self._r = u64(r_cycle)
+        ia = np.array([a for a, _ in init_pairs], np.uint64) if init_pairs else np.zeros(1, np.uint64)
+        iv = u64(np.array([v for _, v in init_pairs], np.uint64).reshape(-1, 2)) if init_pairs else np.zeros((1, 2), np.uint64)
+        self._init = (ia, iv)
+        self.h = lib().or_twist_addr_new(kind, ell, ptr(self._r), ell_addr, len(init_pairs), ptr(ia), ptr(iv),
+                                         ptr(self.cols))
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            lib().or_twist_addr_free(self.h)
+            self.h = None
+
+    def num_rounds(self):
+        return lib().or_twist_addr_num_rounds(self.h)
+
+    def degree_bound(self):
+        return 2
+
+    def evals_at(self, xs):
+        xs = u64(xs)
+        ys = np.empty_like(xs)
+        lib().or_twist_addr_evals(self.h, ptr(xs), xs.shape[0], ptr(ys))
+        return ys
+
+    def fold(self, r):
+        lib().or_twist_addr_fold(self.h, ptr(u64(r)))
+
+
+def bus_openings(Z, bus_base, chunk, n_cols, m_in, r):
+    """Bus-column openings of a digit witness at r (cpu_bus.rs:195-320)."""
+    Z = np.ascontiguousarray(Z, np.int8)
+    r = u64(r)
+    y = np.empty((n_cols, 54, 2), np.uint64)
+    ysc = np.empty((n_cols, 2), np.uint64)
+    lib().or_bus_openings(ptr(Z), Z.shape[1], bus_base, chunk, n_cols, m_in, ptr(r), r.shape[0], ptr(y), ptr(ysc))
+    return y, ysc

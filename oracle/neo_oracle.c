@@ -1718,3 +1718,169 @@ void or_addr_lookup_weights(int ell, const uint64_t* r_cycle, int ell_addr, cons
     kstore(claim_out, claim);
     free(r);
 }
+
+/* ------------------------------------------------------------------------ */
+/* Twist address-lane oracles: TwistReadCheckAddrOracleSparseTime and        */
+/* TwistWriteCheckAddrOracleSparseTime (twist_oracle.rs:1259-1642). Events   */
+/* are the merged nonzero times of has_read / has_write (read) or of         */
+/* has_write (write); a memory keyed by addr >> bit_idx is replayed in time  */
+/* order every round (reads see it before the same event's write).          */
+/* ------------------------------------------------------------------------ */
+struct or_twist_addr {
+    int kind, ell_addr, bit_idx;
+    size_t n_ev, n_init;
+    kq *eq, *hr, *rv, *hw, *inc, *wv, *rpw, *wpw, *ival, *ipw;
+    size_t *ra, *wa, *iaddr;
+    kq* mem;
+};
+typedef struct or_twist_addr or_twist_addr;
+
+/* addr_from_sparse_bits_at_time (twist_oracle.rs:1207-1215): bit b set iff column b equals one */
+static size_t addr_at(const kq* bits, size_t L, int A, size_t t) {
+    size_t a = 0;
+    for (int b = 0; b < A; b++) if (keq(bits[(size_t)b * L + t], K1)) a |= (size_t)1 << b;
+    return a;
+}
+
+/* kind 0: cols [has_read, rv, ra_bits x A, has_write, inc, wa_bits x A];
+   kind 1: cols [has_write, wv, inc, wa_bits x A]. init: n_init (addr, K value). */
+or_twist_addr* or_twist_addr_new(int kind, int ell, const uint64_t* r_cycle, int A, size_t n_init,
+                                 const uint64_t* init_addr, const uint64_t* init_val, const uint64_t* cols) {
+    size_t L = (size_t)1 << ell;
+    const kq* C = (const kq*)cols;
+    const kq *hr = NULL, *rv = NULL, *ra = NULL, *hw, *inc, *wa, *wv = NULL;
+    if (kind == 0) { hr = C; rv = C + L; ra = C + 2 * L; hw = C + (2 + A) * L; inc = C + (3 + A) * L; wa = C + (4 + A) * L; }
+    else { hw = C; wv = C + L; inc = C + 2 * L; wa = C + 3 * L; }
+    kq* r = kdup(r_cycle, ell);
+    or_twist_addr* o = (or_twist_addr*)calloc(1, sizeof(*o));
+    o->kind = kind; o->ell_addr = A;
+    size_t cap = L ? L : 1;
+#define ALLOC_K(f) o->f = (kq*)calloc(cap, sizeof(kq))
+    ALLOC_K(eq); ALLOC_K(hr); ALLOC_K(rv); ALLOC_K(hw); ALLOC_K(inc); ALLOC_K(wv); ALLOC_K(rpw); ALLOC_K(wpw);
+#undef ALLOC_K
+    o->ra = (size_t*)calloc(cap, sizeof(size_t));
+    o->wa = (size_t*)calloc(cap, sizeof(size_t));
+    size_t n = 0;
+    for (size_t t = 0; t < L; t++) {
+        int has_r = kind == 0 && !kiszero(hr[t]);
+        int has_w = !kiszero(hw[t]);
+        if (!has_r && !has_w) continue;
+        o->eq[n] = eq_points_bool_mask(t, r, ell);
+        o->hw[n] = hw[t];
+        o->inc[n] = inc[t];
+        if (kind == 0) {
+            o->hr[n] = hr[t];
+            o->rv[n] = rv[t];
+            o->ra[n] = has_r ? addr_at(ra, L, A, t) : 0;
+            o->wa[n] = has_w ? addr_at(wa, L, A, t) : 0;
+        } else {
+            o->wv[n] = wv[t];
+            o->wa[n] = addr_at(wa, L, A, t);
+        }
+        o->rpw[n] = K1;
+        o->wpw[n] = K1;
+        n++;
+    }
+    o->n_ev = n;
+    o->n_init = n_init;
+    o->iaddr = (size_t*)calloc(n_init + 1, sizeof(size_t));
+    o->ival = (kq*)calloc(n_init + 1, sizeof(kq));
+    o->ipw = (kq*)calloc(n_init + 1, sizeof(kq));
+    for (size_t i = 0; i < n_init; i++) { o->iaddr[i] = init_addr[i]; o->ival[i] = kload(init_val + 2 * i); o->ipw[i] = K1; }
+    o->mem = (kq*)calloc(((size_t)1 << A) + 1, sizeof(kq));
+    free(r);
+    return o;
+}
+
+void or_twist_addr_free(or_twist_addr* o) {
+    if (!o) return;
+    free(o->eq); free(o->hr); free(o->rv); free(o->hw); free(o->inc); free(o->wv); free(o->rpw); free(o->wpw);
+    free(o->ra); free(o->wa); free(o->iaddr); free(o->ival); free(o->ipw); free(o->mem); free(o);
+}
+int or_twist_addr_num_rounds(const or_twist_addr* o) { return o->ell_addr - o->bit_idx; }
+
+void or_twist_addr_evals(or_twist_addr* o, const uint64_t* xs_u, int nx, uint64_t* ys_u) {
+    const kq* xs = (const kq*)xs_u;
+    kq* ys = (kq*)ys_u;
+    for (int i = 0; i < nx; i++) ys[i] = K0;
+    if (o->bit_idx >= o->ell_addr) {
+        kq mem = K0, sum = K0;
+        for (size_t i = 0; i < o->n_init; i++) mem = kadd(mem, kmul(o->ival[i], o->ipw[i]));
+        for (size_t i = 0; i < o->n_ev; i++) {
+            if (o->kind == 0) {
+                if (!kiszero(o->hr[i]))
+                    sum = kadd(sum, kmul(kmul(kmul(o->eq[i], o->hr[i]), o->rpw[i]), ksub(mem, o->rv[i])));
+            } else {
+                kq delta = ksub(ksub(o->wv[i], mem), o->inc[i]);
+                sum = kadd(sum, kmul(kmul(kmul(o->eq[i], o->hw[i]), o->wpw[i]), delta));
+            }
+            if (!kiszero(o->hw[i])) mem = kadd(mem, kmul(kmul(o->inc[i], o->hw[i]), o->wpw[i]));
+        }
+        for (int i = 0; i < nx; i++) ys[i] = sum;
+        return;
+    }
+    const int bit = o->bit_idx;
+    const size_t P = (size_t)1 << (o->ell_addr - bit);
+    kq* mem = o->mem;
+    for (size_t a = 0; a < P; a++) mem[a] = K0;
+    for (size_t i = 0; i < o->n_init; i++) mem[o->iaddr[i] >> bit] = kadd(mem[o->iaddr[i] >> bit], kmul(o->ival[i], o->ipw[i]));
+    for (size_t i = 0; i < o->n_ev; i++) {
+        const int q_read = o->kind == 0 && !kiszero(o->hr[i]);
+        const int q_write = o->kind == 1 && !kiszero(o->hw[i]);
+        if (q_read || q_write) {
+            const size_t a = q_read ? o->ra[i] : o->wa[i];
+            const size_t base = (a >> (bit + 1)) * 2;
+            const kq v0 = mem[base], v1 = mem[base + 1], dv = ksub(v1, v0);
+            const int b = (a >> bit) & 1;
+            const kq w = q_read ? kmul(kmul(o->eq[i], o->hr[i]), o->rpw[i]) : kmul(kmul(o->eq[i], o->hw[i]), o->wpw[i]);
+            for (int j = 0; j < nx; j++) {
+                kq vx = kadd(v0, kmul(dv, xs[j]));
+                kq af = b ? xs[j] : ksub(K1, xs[j]);
+                kq term = q_read ? ksub(vx, o->rv[i]) : ksub(ksub(o->wv[i], vx), o->inc[i]);
+                ys[j] = kadd(ys[j], kmul(kmul(w, af), term));
+            }
+        }
+        if (!kiszero(o->hw[i])) {
+            size_t idx = o->wa[i] >> bit;
+            mem[idx] = kadd(mem[idx], kmul(kmul(o->inc[i], o->hw[i]), o->wpw[i]));
+        }
+    }
+}
+
+/* update_prefix_weights_in_place (twist_oracle.rs:1196-1205) */
+void or_twist_addr_fold(or_twist_addr* o, const uint64_t* rp) {
+    if (o->bit_idx >= o->ell_addr) return;
+    kq r = kload(rp), omr = ksub(K1, r);
+    int bit = o->bit_idx;
+    for (size_t i = 0; i < o->n_init; i++) o->ipw[i] = kmul(o->ipw[i], ((o->iaddr[i] >> bit) & 1) ? r : omr);
+    for (size_t i = 0; i < o->n_ev; i++) {
+        if (o->kind == 0) o->rpw[i] = kmul(o->rpw[i], ((o->ra[i] >> bit) & 1) ? r : omr);
+        o->wpw[i] = kmul(o->wpw[i], ((o->wa[i] >> bit) & 1) ? r : omr);
+    }
+    o->bit_idx++;
+}
+
+/* append_bus_openings_to_me_instance (crates/neo-fold/src/memory_sidecar/cpu_bus.rs:195-320):
+   y[c][rho] = Σ_j χ_r(m_in + j)·Z[rho][bus_base + col_c·chunk + j], y_scalar[c] = Σ_rho b^rho y[c][rho]. */
+void or_bus_openings(const int8_t* Z, int64_t m, int64_t bus_base, int64_t chunk, int n_cols, int64_t m_in,
+                     const uint64_t* r, int ell, uint64_t* y_out /* [n_cols][54] K */, uint64_t* ysc_out) {
+    kq* rr = kdup(r, ell);
+    kq* w = (kq*)malloc(sizeof(kq) * (chunk ? chunk : 1));
+    for (int64_t j = 0; j < chunk; j++) w[j] = eq_points_bool_mask((size_t)(m_in + j), rr, ell);
+    kq* y = (kq*)y_out;
+    for (int c = 0; c < n_cols; c++) {
+        kq sc = K0, pw = K1;
+        for (int rho = 0; rho < D; rho++) {
+            kq acc = K0;
+            for (int64_t j = 0; j < chunk; j++) {
+                int8_t z = Z[(size_t)rho * m + bus_base + (int64_t)c * chunk + j];
+                if (z) acc = kadd(acc, kmul(w[j], kfq(fq_from_i64(z))));
+            }
+            y[(size_t)c * D + rho] = acc;
+            sc = kadd(sc, kmul(acc, pw));
+            pw = kscale(pw, 2);
+        }
+        kstore(ysc_out + 2 * c, sc);
+    }
+    free(rr); free(w);
+}

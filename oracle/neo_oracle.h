@@ -143,6 +143,18 @@ void or_addr_lookup_weights(int ell, const uint64_t* r_cycle, int ell_addr, cons
                             const uint64_t* addr_bits, const uint64_t* table, size_t table_len,
                             uint64_t* weights_out, uint64_t* claim_out);
 
+
+/* Twist address-lane oracles (twist_oracle.rs:1259-1642); kind 0 read, 1 write. */
+typedef struct or_twist_addr or_twist_addr;
+or_twist_addr* or_twist_addr_new(int kind, int ell, const uint64_t* r_cycle, int ell_addr, size_t n_init,
+                                 const uint64_t* init_addr, const uint64_t* init_val, const uint64_t* cols);
+void or_twist_addr_free(or_twist_addr* o);
+int or_twist_addr_num_rounds(const or_twist_addr* o);
+void or_twist_addr_evals(or_twist_addr* o, const uint64_t* xs, int nx, uint64_t* ys);
+void or_twist_addr_fold(or_twist_addr* o, const uint64_t* r);
+void or_bus_openings(const int8_t* Z, int64_t m, int64_t bus_base, int64_t chunk, int n_cols, int64_t m_in,
+                     const uint64_t* r, int ell, uint64_t* y_out, uint64_t* ysc_out);
+
 #ifdef __cplusplus
 }
 #endif

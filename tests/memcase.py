@@ -33,6 +33,7 @@ def trace(ell, ell_addr, active, seed, general=False):
     rng = np.random.default_rng(seed)
     L, P = 1 << ell, 1 << ell_addr
     mem = [int(x) for x in rng.integers(0, 1 << 32, size=P)]
+    init = [(a, mem[a]) for a in range(P) if mem[a]]
     has_r, has_w, ra, wa, rv, wv, inc = (np.zeros(L, np.uint64) for _ in range(7))
     pos = 0
     for t in range(active):
@@ -55,7 +56,7 @@ def trace(ell, ell_addr, active, seed, general=False):
         else:
             wa[t] = 0
     c = dict(has_read=to_k(has_r), has_write=to_k(has_w), rv=to_k(rv), wv=to_k(wv), inc=to_k(inc),
-             ra_bits=bit_cols(ra * has_r, ell_addr), wa_bits=bit_cols(wa, ell_addr))
+             ra_bits=bit_cols(ra * has_r, ell_addr), wa_bits=bit_cols(wa, ell_addr), init=init)
     if general:
         for key in ("has_read", "has_write"):
             g = c[key]

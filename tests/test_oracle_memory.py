@@ -113,3 +113,64 @@ def test_mem_oracle_empty_and_single():
     o = oracle.MemOracle(3, kind_cols(3, c), rand_k(rng, ell), rand_k(rng, A), rand_k(rng, 1)[0])
     assert tk(o.claim) == K0
     assert all(tk(y) == K0 for y in o.evals_at(np.array([[x, 0] for x in range(6)], np.uint64)))
+
+
+def _init_at(init, r_addr):
+    """eval_init_at_r_addr (neo-memory/src/mem_init.rs:133-163)."""
+    acc = K0
+    for a, v in init:
+        chi = (1, 0)
+        for b, rb in enumerate(r_addr):
+            rb = tk(rb)
+            chi = kmul(chi, rb if (a >> b) & 1 else ((1 - rb[0]) % Q, (-rb[1]) % Q))
+        acc = kadd(acc, kmul((v % Q, 0), chi))
+    return acc
+
+
+Q = (1 << 64) - (1 << 32) + 1
+
+
+@pytest.mark.parametrize("kind", [0, 1])
+def test_twist_addr_lane_hands_over_to_time_lane(kind):
+    """An honest trace: the address-lane sum is zero, and after ell_addr rounds
+    its running claim equals the time-lane check's hypercube sum at r_addr."""
+    ell, A = 6, 3
+    c, rng = trace(ell, A, active=48, seed=21 + kind)
+    r_cycle = rand_k(rng, ell)
+    cols = kind_cols(3 if kind == 0 else 4, c)
+    o = oracle.TwistAddrOracle(kind, cols, r_cycle, A, [(a, (v, 0)) for a, v in c["init"]])
+    xs = np.array([[0, 0], [1, 0], [2, 0]], np.uint64)
+    claim = K0
+    chals = []
+    for rnd in range(A):
+        ys = o.evals_at(xs)
+        assert kadd(tk(ys[0]), tk(ys[1])) == claim, f"round {rnd}"
+        r = rand_k(rng, 1)[0]
+        claim = tk(oracle.poly_eval_k(oracle.interpolate(xs, ys), r))
+        o.fold(r)
+        chals.append(r)
+    assert o.num_rounds() == 0
+    assert tk(o.evals_at(xs[:1])[0]) == claim
+    init_r = _init_at(c["init"], chals)
+    t = oracle.MemOracle(3 if kind == 0 else 4, cols, r_cycle, np.array(chals), np.array(init_r, np.uint64))
+    assert tk(t.claim) == claim
+
+
+def test_bus_openings_match_definition():
+    rng = np.random.default_rng(4)
+    m, chunk, ncols, m_in, ell = 256, 8, 5, 2, 8
+    Z = rng.integers(-1, 2, size=(54, m)).astype(np.int8)
+    r = rand_k(rng, ell)
+    base = m - ncols * chunk
+    y, ysc = oracle.bus_openings(Z, base, chunk, ncols, m_in, r)
+    chi = oracle.chi_table(r)
+    for cidx in range(ncols):
+        sc = K0
+        for rho in range(54):
+            acc = K0
+            for j in range(chunk):
+                z = int(Z[rho, base + cidx * chunk + j]) % Q
+                acc = kadd(acc, kmul(tk(chi[m_in + j]), (z, 0)))
+            assert tk(y[cidx, rho]) == acc
+            sc = kadd(sc, kmul(acc, (pow(2, rho, Q), 0)))
+        assert tk(ysc[cidx]) == sc
