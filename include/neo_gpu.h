@@ -198,6 +198,29 @@ int neo_gpu_addr_lookup_weights(neo_gpu_ctx* ctx, uint32_t ell, const uint64_t* 
                                 const uint64_t* has_lookup, const uint64_t* addr_bits, const uint64_t* table,
                                 uint64_t table_len, uint64_t* weights, uint64_t* claim);
 
+/* ---- Twist address-lane oracles (RoundOracle, degree 2) ---------------- */
+/* TwistReadCheckAddrOracleSparseTime::new (kind 0, twist_oracle.rs:1259-1367)
+ * and TwistWriteCheckAddrOracleSparseTime::new (kind 1, :1468-1548).
+ * cols (2^ell K rows each) as for NEO_MEM_TWIST_READ / NEO_MEM_TWIST_WRITE;
+ * init: n_init (address, K value) pairs of the initial memory
+ * (MemInit::Sparse; addresses < 2^ell_addr).  Claimed sum: zero.  The
+ * rounds bind the ell_addr address bits, low bit first; after the last
+ * round every point evaluates to the final sum (the value the time-lane
+ * check at r_addr must start from). */
+typedef struct neo_gpu_twist_addr neo_gpu_twist_addr;
+int neo_gpu_twist_addr_create(neo_gpu_ctx* ctx, int kind, uint32_t ell, const uint64_t* r_cycle, uint32_t ell_addr,
+                              uint64_t n_init, const uint64_t* init_addr, const uint64_t* init_val,
+                              const uint64_t* cols, neo_gpu_twist_addr** out);
+/* Same with the columns in device memory. */
+int neo_gpu_twist_addr_create_device(neo_gpu_ctx* ctx, int kind, uint32_t ell, const uint64_t* r_cycle,
+                                     uint32_t ell_addr, uint64_t n_init, const uint64_t* init_addr,
+                                     const uint64_t* init_val, const uint64_t* d_cols, neo_gpu_twist_addr** out);
+int neo_gpu_twist_addr_evals(neo_gpu_twist_addr* o, const uint64_t* xs, uint32_t nx, uint64_t* ys);
+int neo_gpu_twist_addr_fold(neo_gpu_twist_addr* o, const uint64_t* r);
+uint32_t neo_gpu_twist_addr_num_rounds(const neo_gpu_twist_addr* o);
+uint32_t neo_gpu_twist_addr_degree_bound(const neo_gpu_twist_addr* o);
+int neo_gpu_twist_addr_destroy(neo_gpu_twist_addr* o);
+
 /* ---- shard prove loop (crates/neo-fold/src/shard.rs:1725-2283) ------- */
 typedef struct neo_gpu_shard neo_gpu_shard;
 /* A shard prover over one CCS (n == m == 2^ell_n, identity-first, t <= 4,

@@ -685,3 +685,413 @@ extern "C" int neo_gpu_addr_lookup_weights(neo_gpu_ctx* ctx, uint32_t ell, const
     NEO_CK(ctx, cudaStreamSynchronize(S));
     return NEO_OK;
 }
+
+// ===========================================================================
+// Twist address-lane oracles (TwistReadCheckAddrOracleSparseTime /
+// TwistWriteCheckAddrOracleSparseTime, twist_oracle.rs:1259-1642).
+//
+// The reference replays a HashMap memory over the time-ordered events every
+// round.  Here the events are compacted once into arrays; the memory value a
+// query event i sees at address block idx is
+//     init_tab[idx] + Σ_{j < i, wa_j >> bit = idx} inc_j·hw_j·wpw_j,
+// where init_tab is the initial memory folded on its low address bits (the
+// reference's init prefix weights are exactly that fold).  One thread per
+// query event sums the earlier writes from shared-memory tiles.  Degree 2:
+// values at x = 0, 1, 2 are reduced and interpolated on the host.
+// ===========================================================================
+namespace {
+
+constexpr int TA_T = 256;
+
+__device__ __forceinline__ uint32_t addr_bits_at(const K* bits, uint64_t L, uint32_t A, uint64_t t) {
+    uint32_t a = 0;
+    for (uint32_t b = 0; b < A; b++) {
+        K v = bits[(uint64_t)b * L + t];
+        if (v.re == 1 && v.im == 0) a |= 1u << b;
+    }
+    return a;
+}
+
+// event flags: read kind: has_read | has_write nonzero; write kind: has_write nonzero
+__global__ void ta_count_kernel(const K* __restrict__ hr, const K* __restrict__ hw, uint64_t L, uint32_t* __restrict__ counts) {
+    __shared__ uint32_t s_cnt;
+    if (threadIdx.x == 0) s_cnt = 0;
+    __syncthreads();
+    const uint64_t t = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+    bool f = false;
+    if (t < L) f = !gl::kiszero(hw[t]) || (hr && !gl::kiszero(hr[t]));
+    unsigned bal = __ballot_sync(0xffffffffu, f);
+    if ((threadIdx.x & 31) == 0 && bal) atomicAdd(&s_cnt, (uint32_t)__popc(bal));
+    __syncthreads();
+    if (threadIdx.x == 0) counts[blockIdx.x] = s_cnt;
+}
+
+struct TaBuild {
+    const K *hr, *rv, *ra, *hw, *inc, *wa, *wv;
+    const K* r_cycle;
+    uint32_t ell, A;
+    uint64_t L;
+    const uint32_t* offs;   // exclusive prefix of the per-block counts
+    // outputs [E]
+    K *eq, *ehr, *erv, *ehw, *einc, *ewv;
+    uint32_t *era, *ewa;
+};
+
+__global__ void ta_build_kernel(const TaBuild a) {
+    __shared__ uint32_t s_warp[TA_T / 32];
+    const uint64_t t = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+    bool f = false;
+    if (t < a.L) f = !gl::kiszero(a.hw[t]) || (a.hr && !gl::kiszero(a.hr[t]));
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    unsigned bal = __ballot_sync(0xffffffffu, f);
+    if (lane == 0) s_warp[warp] = __popc(bal);
+    __syncthreads();
+    uint32_t before = 0;
+    for (int w = 0; w < warp; w++) before += s_warp[w];
+    before += __popc(bal & ((1u << lane) - 1));
+    if (!f) return;
+    const uint32_t e = a.offs[blockIdx.x] + before;
+    // χ_{r_cycle}(t)
+    K chi = gl::kone();
+    for (uint32_t i = 0; i < a.ell; i++) {
+        K ri = a.r_cycle[i];
+        chi = gl::kmul(chi, ((t >> i) & 1) ? ri : gl::ksub(gl::kone(), ri));
+    }
+    a.eq[e] = chi;
+    K hw = a.hw[t];
+    a.ehw[e] = hw;
+    a.einc[e] = a.inc[t];
+    const bool has_w = !gl::kiszero(hw);
+    if (a.hr) {
+        K hr = a.hr[t];
+        a.ehr[e] = hr;
+        a.erv[e] = a.rv[t];
+        a.era[e] = gl::kiszero(hr) ? 0u : addr_bits_at(a.ra, a.L, a.A, t);
+        a.ewa[e] = has_w ? addr_bits_at(a.wa, a.L, a.A, t) : 0u;
+    } else {
+        a.ewv[e] = a.wv[t];
+        a.ewa[e] = addr_bits_at(a.wa, a.L, a.A, t);
+    }
+}
+
+// per round: write keys and deltas
+__global__ void ta_prep_kernel(const K* __restrict__ hw, const K* __restrict__ inc, const uint32_t* __restrict__ wa,
+                               const K* __restrict__ wpw, uint32_t E, uint32_t bit, uint32_t* __restrict__ wkey,
+                               K* __restrict__ wdelta) {
+    uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= E) return;
+    K h = hw[j];
+    if (gl::kiszero(h)) {
+        wkey[j] = 0xFFFFFFFFu;
+        wdelta[j] = gl::kzero();
+        return;
+    }
+    wkey[j] = bit >= 32 ? 0u : (wa[j] >> bit);
+    wdelta[j] = gl::kmul(gl::kmul(inc[j], h), wpw[j]);
+}
+
+struct TaEval {
+    int kind;  // 0 read, 1 write
+    uint32_t E, bit;
+    const K *eq, *hr, *rv, *hw, *inc, *wv, *rpw, *wpw;
+    const uint32_t *ra, *wa;
+    const uint32_t* wkey;
+    const K* wdelta;
+    const K* init_tab;  // folded initial memory, >= 2 entries
+    K* partials;        // [3][gridDim.x]
+};
+
+__global__ void __launch_bounds__(TA_T) ta_eval_kernel(const TaEval a) {
+    __shared__ uint32_t s_key[TA_T];
+    __shared__ K s_d[TA_T];
+    __shared__ K s_red[3][TA_T / 32];
+    const uint32_t i = blockIdx.x * TA_T + threadIdx.x;
+    const uint32_t i_end = min(a.E, blockIdx.x * TA_T + TA_T);
+    bool q = false;
+    uint32_t addr = 0;
+    if (i < a.E) {
+        if (a.kind == 0) { q = !gl::kiszero(a.hr[i]); addr = a.ra[i]; }
+        else { q = !gl::kiszero(a.hw[i]); addr = a.wa[i]; }
+    }
+    const uint32_t base = a.bit >= 31 ? 0u : ((addr >> (a.bit + 1)) << 1);
+    K v0 = gl::kzero(), v1 = gl::kzero();
+    if (q) {
+        v0 = a.init_tab[base];
+        v1 = a.init_tab[base + 1];
+    }
+    // earlier writes, tile by tile (j < i)
+    for (uint32_t j0 = 0; j0 < i_end; j0 += TA_T) {
+        const uint32_t j = j0 + threadIdx.x;
+        __syncthreads();
+        if (j < a.E) {
+            s_key[threadIdx.x] = a.wkey[j];
+            s_d[threadIdx.x] = a.wdelta[j];
+        }
+        __syncthreads();
+        if (q) {
+            const uint32_t jn = min((uint32_t)TA_T, i - j0 < TA_T ? i - j0 : TA_T);
+            if (i > j0)
+                for (uint32_t u = 0; u < jn; u++) {
+                    const uint32_t k = s_key[u];
+                    if (k == base) v0 = gl::kadd(v0, s_d[u]);
+                    else if (k == base + 1) v1 = gl::kadd(v1, s_d[u]);
+                }
+        }
+    }
+    K c[3] = {gl::kzero(), gl::kzero(), gl::kzero()};
+    if (q) {
+        const bool b = a.bit < 32 && ((addr >> a.bit) & 1);
+        K w = a.kind == 0 ? gl::kmul(gl::kmul(a.eq[i], a.hr[i]), a.rpw[i]) : gl::kmul(gl::kmul(a.eq[i], a.hw[i]), a.wpw[i]);
+        K dv = gl::ksub(v1, v0);
+        K vx = v0;
+#pragma unroll
+        for (int x = 0; x < 3; x++) {
+            K af = b ? gl::kfq((uint64_t)x) : gl::kfq(gl::sub(1, (uint64_t)x));
+            K term = a.kind == 0 ? gl::ksub(vx, a.rv[i]) : gl::ksub(gl::ksub(a.wv[i], vx), a.inc[i]);
+            c[x] = gl::kmul(gl::kmul(w, af), term);
+            vx = gl::kadd(vx, dv);
+        }
+    }
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int x = 0; x < 3; x++) {
+        K v = c[x];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v = gl::kadd(v, shfl_xor_km(v, o));
+        if (lane == 0) s_red[x][warp] = v;
+    }
+    __syncthreads();
+    if (threadIdx.x < 3) {
+        K s = gl::kzero();
+        for (int w = 0; w < TA_T / 32; w++) s = gl::kadd(s, s_red[threadIdx.x][w]);
+        a.partials[(uint64_t)threadIdx.x * gridDim.x + blockIdx.x] = s;
+    }
+}
+
+__global__ void ta_fold_kernel(const uint32_t* __restrict__ ra, const uint32_t* __restrict__ wa, K* __restrict__ rpw,
+                               K* __restrict__ wpw, uint32_t E, uint32_t bit, K r, int kind) {
+    uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= E) return;
+    const K omr = gl::ksub(gl::kone(), r);
+    if (kind == 0) rpw[j] = gl::kmul(rpw[j], ((ra[j] >> bit) & 1) ? r : omr);
+    wpw[j] = gl::kmul(wpw[j], ((wa[j] >> bit) & 1) ? r : omr);
+}
+
+__global__ void scatter_init_kernel(const uint64_t* __restrict__ addr, const K* __restrict__ val, uint64_t n,
+                                    K* __restrict__ tab) {
+    uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+    if (i < n) tab[addr[i]] = val[i];
+}
+
+}  // namespace
+
+struct neo_gpu_twist_addr {
+    neo_gpu_ctx* ctx = nullptr;
+    int kind = 0;
+    uint32_t A = 0, bit = 0, E = 0;
+    DevBuf<K> eq, hr, rv, hw, inc, wv, rpw, wpw, wdelta, tab[2], partials, vals;
+    DevBuf<uint32_t> ra, wa, wkey;
+    uint64_t tab_len = 0;
+    int cur = 0;
+    bool pending = false;
+    K pending_r{};
+    std::vector<K> hvals;
+};
+
+namespace {
+
+int ta_apply_fold(neo_gpu_twist_addr* o) {
+    neo_gpu_ctx* ctx = o->ctx;
+    cudaStream_t S = ctx->stream;
+    if (o->E) {
+        ta_fold_kernel<<<ceil_div(o->E, 256), 256, 0, S>>>(o->ra.p, o->wa.p, o->rpw.p, o->wpw.p, o->E, o->bit,
+                                                         o->pending_r, o->kind);
+        NEO_LAUNCHED(ctx);
+    }
+    // fold the initial-memory table on its low address bit
+    const uint64_t half = o->tab_len >> 1;
+    mem_fold_kernel<<<ceil_div(half ? half : 1, 256), 256, 0, S>>>(o->tab[o->cur].p, o->tab_len, o->tab[o->cur ^ 1].p, 1,
+                                                                   o->pending_r);
+    NEO_LAUNCHED(ctx);
+    o->cur ^= 1;
+    o->tab_len = half;
+    o->bit++;
+    o->pending = false;
+    return NEO_OK;
+}
+
+int ta_values(neo_gpu_twist_addr* o) {
+    neo_gpu_ctx* ctx = o->ctx;
+    cudaStream_t S = ctx->stream;
+    if (o->pending) {
+        int rc = ta_apply_fold(o);
+        if (rc) return rc;
+    }
+    o->hvals.assign(3, gl::kzero());
+    if (o->E == 0) return NEO_OK;
+    ta_prep_kernel<<<ceil_div(o->E, 256), 256, 0, S>>>(o->hw.p, o->inc.p, o->wa.p, o->wpw.p, o->E, o->bit, o->wkey.p,
+                                                     o->wdelta.p);
+    NEO_LAUNCHED(ctx);
+    const uint32_t nb = ceil_div(o->E, TA_T);
+    NEO_CK(ctx, o->partials.ensure((size_t)3 * nb));
+    TaEval a;
+    a.kind = o->kind;
+    a.E = o->E;
+    a.bit = o->bit;
+    a.eq = o->eq.p; a.hr = o->hr.p; a.rv = o->rv.p; a.hw = o->hw.p; a.inc = o->inc.p; a.wv = o->wv.p;
+    a.rpw = o->rpw.p; a.wpw = o->wpw.p; a.ra = o->ra.p; a.wa = o->wa.p;
+    a.wkey = o->wkey.p; a.wdelta = o->wdelta.p;
+    a.init_tab = o->tab[o->cur].p;
+    a.partials = o->partials.p;
+    ta_eval_kernel<<<nb, TA_T, 0, S>>>(a);
+    NEO_LAUNCHED(ctx);
+    mem_reduce_kernel<<<3, 256, 0, S>>>(o->partials.p, nb, o->vals.p);
+    NEO_LAUNCHED(ctx);
+    NEO_CK(ctx, cudaMemcpyAsync(o->hvals.data(), o->vals.p, 3 * sizeof(K), cudaMemcpyDeviceToHost, S));
+    NEO_CK(ctx, cudaStreamSynchronize(S));
+    return NEO_OK;
+}
+
+int ta_create(neo_gpu_ctx* ctx, int kind, uint32_t ell, const uint64_t* r_cycle, uint32_t A, uint64_t n_init,
+              const uint64_t* init_addr, const uint64_t* init_val, const uint64_t* cols, bool dev,
+              neo_gpu_twist_addr** out) {
+    if (!ctx || !out) return NEO_ERR_ARG;
+    *out = nullptr;
+    if (kind != 0 && kind != 1) return ctx->fail(NEO_ERR_ARG, "twist_addr: kind must be 0 (read) or 1 (write)");
+    if (ell > 30 || A > 30 || A == 0) return ctx->fail(NEO_ERR_ARG, "twist_addr: ell / ell_addr out of range");
+    if (!cols || (ell && !r_cycle) || (n_init && (!init_addr || !init_val)))
+        return ctx->fail(NEO_ERR_ARG, "twist_addr: null buffer");
+    for (uint64_t i = 0; i < n_init; i++)
+        if (init_addr[i] >> A) return ctx->fail(NEO_ERR_ARG, "twist_addr: init address out of range");
+    cudaSetDevice(ctx->device);
+    cudaStream_t S = ctx->stream;
+    const uint64_t L = 1ULL << ell, P = 1ULL << A;
+    const uint32_t n_cols = kind == 0 ? 4 + 2 * A : 3 + A;
+    auto* o = new neo_gpu_twist_addr();
+    o->ctx = ctx;
+    o->kind = kind;
+    o->A = A;
+    auto fail = [&](int rc) { delete o; return rc; };
+    DevBuf<K> dcols, dr;
+    const K* C = reinterpret_cast<const K*>(cols);
+    if (!dev) {
+        if (dcols.alloc((size_t)n_cols * L)) return fail(ctx->fail(NEO_ERR_OOM, "twist_addr: columns"));
+        if (cudaMemcpyAsync(dcols.p, cols, (size_t)n_cols * L * sizeof(K), cudaMemcpyHostToDevice, S))
+            return fail(ctx->fail(NEO_ERR_CUDA, "twist_addr: column upload"));
+        C = dcols.p;
+    }
+    if (dr.alloc(ell ? ell : 1)) return fail(ctx->fail(NEO_ERR_OOM, "twist_addr: r"));
+    if (ell && cudaMemcpyAsync(dr.p, r_cycle, ell * sizeof(K), cudaMemcpyHostToDevice, S))
+        return fail(ctx->fail(NEO_ERR_CUDA, "twist_addr: r upload"));
+    TaBuild b{};
+    if (kind == 0) {
+        b.hr = C; b.rv = C + L; b.ra = C + 2 * L; b.hw = C + (2 + A) * L; b.inc = C + (3 + A) * L; b.wa = C + (4 + A) * L;
+    } else {
+        b.hw = C; b.wv = C + L; b.inc = C + 2 * L; b.wa = C + 3 * L;
+    }
+    const uint32_t nblk = ceil_div(L, TA_T);
+    DevBuf<uint32_t> counts;
+    if (counts.alloc(nblk)) return fail(ctx->fail(NEO_ERR_OOM, "twist_addr: counts"));
+    ta_count_kernel<<<nblk, TA_T, 0, S>>>(b.hr, b.hw, L, counts.p);
+    NEO_LAUNCHED(ctx);
+    std::vector<uint32_t> hc(nblk);
+    NEO_CK(ctx, cudaMemcpyAsync(hc.data(), counts.p, nblk * 4, cudaMemcpyDeviceToHost, S));
+    NEO_CK(ctx, cudaStreamSynchronize(S));
+    uint64_t E = 0;
+    for (auto& c : hc) { uint32_t v = c; c = (uint32_t)E; E += v; }
+    o->E = (uint32_t)E;
+    const size_t ecap = E ? E : 1;
+    if (o->eq.alloc(ecap) || o->hr.alloc(ecap) || o->rv.alloc(ecap) || o->hw.alloc(ecap) || o->inc.alloc(ecap) ||
+        o->wv.alloc(ecap) || o->rpw.alloc(ecap) || o->wpw.alloc(ecap) || o->wdelta.alloc(ecap) || o->ra.alloc(ecap) ||
+        o->wa.alloc(ecap) || o->wkey.alloc(ecap) || o->vals.alloc(3) || o->tab[0].alloc(P + 1) ||
+        o->tab[1].alloc(P / 2 + 1))
+        return fail(ctx->fail(NEO_ERR_OOM, "twist_addr: event arrays"));
+    NEO_CK(ctx, cudaMemcpyAsync(counts.p, hc.data(), nblk * 4, cudaMemcpyHostToDevice, S));
+    b.r_cycle = dr.p; b.ell = ell; b.A = A; b.L = L; b.offs = counts.p;
+    b.eq = o->eq.p; b.ehr = o->hr.p; b.erv = o->rv.p; b.ehw = o->hw.p; b.einc = o->inc.p; b.ewv = o->wv.p;
+    b.era = o->ra.p; b.ewa = o->wa.p;
+    NEO_CK(ctx, cudaMemsetAsync(o->ra.p, 0, ecap * 4, S));
+    NEO_CK(ctx, cudaMemsetAsync(o->hr.p, 0, ecap * sizeof(K), S));
+    NEO_CK(ctx, cudaMemsetAsync(o->wv.p, 0, ecap * sizeof(K), S));
+    ta_build_kernel<<<nblk, TA_T, 0, S>>>(b);
+    NEO_LAUNCHED(ctx);
+    // prefix weights start at one
+    std::vector<K> ones(ecap, gl::kone());
+    NEO_CK(ctx, cudaMemcpyAsync(o->rpw.p, ones.data(), ecap * sizeof(K), cudaMemcpyHostToDevice, S));
+    NEO_CK(ctx, cudaMemcpyAsync(o->wpw.p, ones.data(), ecap * sizeof(K), cudaMemcpyHostToDevice, S));
+    // initial memory as a dense table over the 2^A addresses (plus one zero pad)
+    NEO_CK(ctx, cudaMemsetAsync(o->tab[0].p, 0, (P + 1) * sizeof(K), S));
+    NEO_CK(ctx, cudaMemsetAsync(o->tab[1].p, 0, (P / 2 + 1) * sizeof(K), S));
+    if (n_init) {
+        DevBuf<uint64_t> da;
+        DevBuf<K> dv;
+        if (da.alloc(n_init) || dv.alloc(n_init)) return fail(ctx->fail(NEO_ERR_OOM, "twist_addr: init"));
+        NEO_CK(ctx, cudaMemcpyAsync(da.p, init_addr, n_init * 8, cudaMemcpyHostToDevice, S));
+        NEO_CK(ctx, cudaMemcpyAsync(dv.p, init_val, n_init * sizeof(K), cudaMemcpyHostToDevice, S));
+        scatter_init_kernel<<<ceil_div(n_init, 256), 256, 0, S>>>(da.p, dv.p, n_init, o->tab[0].p);
+        NEO_LAUNCHED(ctx);
+        NEO_CK(ctx, cudaStreamSynchronize(S));
+    }
+    o->tab_len = P;
+    NEO_CK(ctx, cudaStreamSynchronize(S));
+    *out = o;
+    return NEO_OK;
+}
+
+}  // namespace
+
+extern "C" int neo_gpu_twist_addr_create(neo_gpu_ctx* ctx, int kind, uint32_t ell, const uint64_t* r_cycle,
+                                         uint32_t ell_addr, uint64_t n_init, const uint64_t* init_addr,
+                                         const uint64_t* init_val, const uint64_t* cols, neo_gpu_twist_addr** out) {
+    return ta_create(ctx, kind, ell, r_cycle, ell_addr, n_init, init_addr, init_val, cols, false, out);
+}
+
+extern "C" int neo_gpu_twist_addr_create_device(neo_gpu_ctx* ctx, int kind, uint32_t ell, const uint64_t* r_cycle,
+                                                uint32_t ell_addr, uint64_t n_init, const uint64_t* init_addr,
+                                                const uint64_t* init_val, const uint64_t* d_cols,
+                                                neo_gpu_twist_addr** out) {
+    return ta_create(ctx, kind, ell, r_cycle, ell_addr, n_init, init_addr, init_val, d_cols, true, out);
+}
+
+extern "C" int neo_gpu_twist_addr_evals(neo_gpu_twist_addr* o, const uint64_t* xs, uint32_t nx, uint64_t* ys) {
+    if (!o) return NEO_ERR_ARG;
+    if ((!xs || !ys) && nx) return o->ctx->fail(NEO_ERR_ARG, "twist_addr_evals: null buffer");
+    cudaSetDevice(o->ctx->device);
+    int rc = ta_values(o);
+    if (rc) return rc;
+    for (uint32_t i = 0; i < nx; i++) {
+        // after the last round the value does not depend on x (the reference's constant branch)
+        K y = o->bit >= o->A ? o->hvals[0] : lagrange_at(o->hvals, kload_h(xs + 2 * i));
+        ys[2 * i] = y.re;
+        ys[2 * i + 1] = y.im;
+    }
+    return NEO_OK;
+}
+
+extern "C" int neo_gpu_twist_addr_fold(neo_gpu_twist_addr* o, const uint64_t* r) {
+    if (!o) return NEO_ERR_ARG;
+    if (!r) return o->ctx->fail(NEO_ERR_ARG, "twist_addr_fold: null challenge");
+    const uint32_t done = o->bit + (o->pending ? 1 : 0);
+    if (done >= o->A) return NEO_OK;
+    cudaSetDevice(o->ctx->device);
+    if (o->pending) {
+        int rc = ta_apply_fold(o);
+        if (rc) return rc;
+    }
+    o->pending = true;
+    o->pending_r = kload_h(r);
+    return NEO_OK;
+}
+
+extern "C" uint32_t neo_gpu_twist_addr_num_rounds(const neo_gpu_twist_addr* o) {
+    return o ? o->A - o->bit - (o->pending ? 1 : 0) : 0;
+}
+extern "C" uint32_t neo_gpu_twist_addr_degree_bound(const neo_gpu_twist_addr* o) { return o ? 2 : 0; }
+
+extern "C" int neo_gpu_twist_addr_destroy(neo_gpu_twist_addr* o) {
+    if (!o) return NEO_OK;
+    cudaSetDevice(o->ctx->device);
+    cudaStreamSynchronize(o->ctx->stream);
+    delete o;
+    return NEO_OK;
+}

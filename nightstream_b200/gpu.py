@@ -78,6 +78,13 @@ SIGNATURES = {
     "neo_gpu_mem_oracle_degree_bound": [P],
     "neo_gpu_mem_oracle_destroy": [P],
     "neo_gpu_addr_lookup_weights": [P, U32, P, U32, P, P, P, U64, P, P],
+    "neo_gpu_twist_addr_create": [P, I, U32, P, U32, U64, P, P, P, P],
+    "neo_gpu_twist_addr_create_device": [P, I, U32, P, U32, U64, P, P, ctypes.c_void_p, P],
+    "neo_gpu_twist_addr_evals": [P, P, U32, P],
+    "neo_gpu_twist_addr_fold": [P, P],
+    "neo_gpu_twist_addr_num_rounds": [P],
+    "neo_gpu_twist_addr_degree_bound": [P],
+    "neo_gpu_twist_addr_destroy": [P],
 }
 _RESTYPES = {
     "neo_gpu_last_error": ctypes.c_char_p,
@@ -87,6 +94,8 @@ _RESTYPES = {
     "neo_gpu_batch_kernel_launches": U64,
     "neo_gpu_mem_oracle_num_rounds": U32,
     "neo_gpu_mem_oracle_degree_bound": U32,
+    "neo_gpu_twist_addr_num_rounds": U32,
+    "neo_gpu_twist_addr_degree_bound": U32,
 }
 
 _lib = None
@@ -323,6 +332,48 @@ class GpuMemOracle:
         if getattr(self, "h", None):
             if self.ctx.h is not None:
                 self.ctx.lib.neo_gpu_mem_oracle_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
+
+
+class GpuTwistAddrOracle:
+    """Twist address-lane read (0) / write (1) check oracle on the GPU
+    (twist_oracle.rs:1259-1642)."""
+
+    def __init__(self, ctx: Context, kind: int, cols, r_cycle, ell_addr: int, init_pairs=()):
+        self.ctx = ctx
+        cols = _u64(cols)
+        ell = cols.shape[1].bit_length() - 1
+        self._r = _u64(r_cycle)
+        ia = np.array([a for a, _ in init_pairs], np.uint64) if init_pairs else np.zeros(1, np.uint64)
+        iv = _u64(np.array([v for _, v in init_pairs], np.uint64).reshape(-1, 2)) if init_pairs else \
+            np.zeros((1, 2), np.uint64)
+        h = ctypes.c_void_p()
+        ctx.check(ctx.lib.neo_gpu_twist_addr_create(ctx.h, kind, ell, _p(self._r), ell_addr, len(init_pairs), _p(ia),
+                                                    _p(iv), _p(cols), ctypes.byref(h)))
+        self.h = h
+
+    def num_rounds(self) -> int:
+        return int(self.ctx.lib.neo_gpu_twist_addr_num_rounds(self.h))
+
+    def degree_bound(self) -> int:
+        return int(self.ctx.lib.neo_gpu_twist_addr_degree_bound(self.h))
+
+    def evals_at(self, xs: np.ndarray) -> np.ndarray:
+        xs = _u64(xs)
+        ys = np.empty_like(xs)
+        self.ctx.check(self.ctx.lib.neo_gpu_twist_addr_evals(self.h, _p(xs), xs.shape[0], _p(ys)))
+        return ys
+
+    def fold(self, r: np.ndarray):
+        self.ctx.check(self.ctx.lib.neo_gpu_twist_addr_fold(self.h, _p(_u64(r))))
+
+    def close(self):
+        if getattr(self, "h", None):
+            if self.ctx.h is not None:
+                self.ctx.lib.neo_gpu_twist_addr_destroy(self.h)
             self.h = None
 
     def __del__(self):

@@ -157,3 +157,56 @@ def test_bitness_without_columns(ctx):
     assert np.array_equal(g.claim, np.zeros(2, np.uint64))
     assert not g.evals_at(np.array([[0, 0], [3, 0]], np.uint64)).any()
     g.close()
+
+
+@pytest.mark.parametrize("kind", [0, 1])
+@pytest.mark.parametrize("general", [False, True])
+def test_twist_addr_gpu_matches_oracle(ctx, kind, general):
+    ell, A = 10, 6
+    c, rng = trace(ell, A, active=700, seed=50 + kind, general=general)
+    r_cycle = rand_k(rng, ell)
+    cols = kind_cols(3 if kind == 0 else 4, c)
+    init = [(a, (v, 0)) for a, v in c["init"][:40]]
+    ref = oracle.TwistAddrOracle(kind, cols, r_cycle, A, init)
+    g = gpu.GpuTwistAddrOracle(ctx, kind, cols, r_cycle, A, init)
+    xs = np.array([[0, 0], [1, 0], [2, 0], [77, 5]], np.uint64)
+    for rnd in range(A + 1):
+        assert np.array_equal(g.evals_at(xs), ref.evals_at(xs)), f"round {rnd}"
+        if rnd < A:
+            r = rand_k(rng, 1)[0]
+            g.fold(r)
+            ref.fold(r)
+    assert g.num_rounds() == 0
+    g.close()
+
+
+def test_twist_addr_gpu_full_size(ctx):
+    """Twist 2^12 cells, 2^14 events in a 2^16 time domain: the address lane
+    sums to zero for an honest trace and hands over to the time-lane claim."""
+    ell, A = 16, 12
+    c, rng = trace(ell, A, active=1 << 14, seed=77)
+    r_cycle = rand_k(rng, ell)
+    init = [(a, (v, 0)) for a, v in c["init"]]
+    for kind in (0, 1):
+        cols = kind_cols(3 if kind == 0 else 4, c)
+        g = gpu.GpuTwistAddrOracle(ctx, kind, cols, r_cycle, A, init)
+        xs = np.array([[0, 0], [1, 0], [2, 0]], np.uint64)
+        claim = np.zeros(2, np.uint64)
+        chals = []
+        for rnd in range(A):
+            ys = g.evals_at(xs)
+            assert np.array_equal(kadd_np(ys[0], ys[1]), claim), f"kind {kind} round {rnd}"
+            r = rand_k(rng, 1)[0]
+            claim = oracle.poly_eval_k(oracle.interpolate(xs, ys), r)
+            g.fold(r)
+            chals.append(r)
+        assert np.array_equal(g.evals_at(xs[:1])[0], claim)
+        # time-lane check at r_addr starts from the address lane's final value
+        init_r = np.zeros(2, np.uint64)
+        chi_addr = oracle.chi_table(np.array(chals))
+        for a, (v, _) in init:
+            init_r = kadd_np(init_r, oracle.k_mul(np.array([[v, 0]], np.uint64), chi_addr[a:a + 1])[0])
+        t = gpu.GpuMemOracle(ctx, 3 if kind == 0 else 4, cols, r_cycle, np.array(chals), init_r)
+        assert np.array_equal(t.claim, claim)
+        t.close()
+        g.close()
