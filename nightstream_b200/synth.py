@@ -36,12 +36,17 @@ def _uniform_fq(rng, shape):
         return v
 
 
-def make_r1cs(ell: int, seed: int, z_bits: int = 32):
-    """Return (ccs, z) for a satisfied random R1CS with n = m = 2^ell."""
+def make_r1cs(ell: int, seed: int, z_bits: int = 32, z: np.ndarray = None):
+    """Return (ccs, z) for a satisfied random R1CS with n = m = 2^ell
+    (z drawn here, or the given witness with z[0] = 1)."""
     n = m = 1 << ell
     rng = np.random.default_rng(seed)
-    z = rng.integers(0, 1 << z_bits, size=m, dtype=np.uint64)
-    z[0] = 1
+    if z is None:
+        z = rng.integers(0, 1 << z_bits, size=m, dtype=np.uint64)
+        z[0] = 1
+    else:
+        z = np.asarray(z, dtype=np.uint64).copy()
+        rng.integers(0, 1 << z_bits, size=m, dtype=np.uint64)  # keep the stream aligned
     a_cols = _distinct_cols(rng, n, m, 3)
     b_cols = _distinct_cols(rng, n, m, 3)
     c_cols = _distinct_cols(rng, n, m, 3)
@@ -89,3 +94,75 @@ def check_r1cs(ccs: CcsStructure, z: np.ndarray) -> bool:
 def uniform_k(rng, count: int) -> np.ndarray:
     """count uniform K = F_q[u]/(u^2-7) elements as [count, 2] uint64."""
     return _uniform_fq(rng, (count, 2))
+
+
+def memory_trace(steps: int, shout_ell: int, twist_ell: int, seed: int, table_len: int = None, init_cells: int = 64):
+    """One fold step's worth of a RISC-V-style trace: per step one Shout lookup
+    (uniform index into a table of uniform 32-bit entries) and one Twist read +
+    one write (addresses 70 % stride-4 sequential / 30 % uniform over 2^twist_ell
+    cells, 32-bit values).  Returns the bus columns (values per step, Shout
+    first then Twist, in the shared-bus column order) and the instance data."""
+    rng = np.random.default_rng(seed)
+    table_len = table_len or (1 << shout_ell)
+    table = rng.integers(0, 1 << 32, size=table_len, dtype=np.uint64)
+    P = 1 << twist_ell
+    init = [(int(a), int(v)) for a, v in
+            zip(range(min(init_cells, P)), rng.integers(1, 1 << 32, size=min(init_cells, P)))]
+    mem = np.zeros(P, dtype=object)
+    for a, v in init:
+        mem[a] = v
+    idx = rng.integers(0, table_len, size=steps)
+    cols = []
+    for b in range(shout_ell):
+        cols.append((idx >> b) & 1)
+    cols.append(np.ones(steps, dtype=np.int64))       # has_lookup
+    cols.append(table[idx])                            # val
+    ra = np.zeros(steps, np.int64)
+    wa = np.zeros(steps, np.int64)
+    rv = np.zeros(steps, dtype=object)
+    wv = rng.integers(0, 1 << 32, size=steps)
+    inc = np.zeros(steps, dtype=object)
+    pos = 0
+    for j in range(steps):
+        if rng.random() < 0.7:
+            pos = (pos + 4) % P
+            ra[j] = pos
+        else:
+            ra[j] = int(rng.integers(0, P))
+        wa[j] = ra[j] if rng.random() < 0.5 else int(rng.integers(0, P))
+        rv[j] = mem[ra[j]]
+        inc[j] = (int(wv[j]) - int(mem[wa[j]])) % Q
+        mem[wa[j]] = int(wv[j])
+    for b in range(twist_ell):
+        cols.append((ra >> b) & 1)
+    for b in range(twist_ell):
+        cols.append((wa >> b) & 1)
+    cols.append(np.ones(steps, dtype=np.int64))        # has_read
+    cols.append(np.ones(steps, dtype=np.int64))        # has_write
+    cols.append(wv)
+    cols.append(rv)
+    cols.append(inc)
+    bus = np.array([[int(v) % Q for v in c] for c in cols], dtype=np.uint64)
+    mem_desc = dict(steps=steps,
+                    shout=[dict(ell_addr=shout_ell, k=1 << shout_ell, d=1, n_side=1 << shout_ell, ell=shout_ell,
+                                table=table)],
+                    twist=[dict(ell_addr=twist_ell, k=P, d=1, n_side=P, ell=twist_ell, init=init)])
+    return bus, mem_desc
+
+
+def make_memory_workload(ell: int, seed: int, steps: int, shout_ell: int, twist_ell: int, m_in: int = 1,
+                         table_len: int = None):
+    """Single shard with memory: a satisfied R1CS of n = m = 2^ell whose witness
+    carries the shared CPU bus (the Twist / Shout columns of `steps` trace steps)
+    in its tail, bus cell (col, j) at m - bus_cols*steps + col*steps + j."""
+    m = 1 << ell
+    bus, mem = memory_trace(steps, shout_ell, twist_ell, seed + 1, table_len)
+    rng = np.random.default_rng(seed + 2)
+    z = rng.integers(0, 1 << 32, size=m, dtype=np.uint64)
+    z[0] = 1
+    base = m - bus.shape[0] * steps
+    if base < m_in or m_in + steps > m:
+        raise ValueError("bus does not fit the witness")
+    z[base:] = bus.reshape(-1)
+    ccs, z = make_r1cs(ell, seed, z=z)
+    return ccs, z, mem

@@ -60,6 +60,7 @@ def lib():
             "or_ccs_digest": [P, P],
             "or_tr_new": [ctypes.c_char_p],
             "or_tr_free": [P],
+            "or_tr_clone": [P],
             "or_tr_append_message": [P, ctypes.c_char_p, P, SZ],
             "or_tr_append_fields": [P, ctypes.c_char_p, P, SZ],
             "or_tr_append_u64s": [P, ctypes.c_char_p, P, SZ],
@@ -91,6 +92,7 @@ def lib():
         L.or_mem_oracle_new.restype = P
         L.or_twist_addr_new.restype = P
         L.or_tr_new.restype = P
+        L.or_tr_clone.restype = P
         L.or_tr_challenge_field.restype = ctypes.c_uint64
         _lib = L
     return _lib
@@ -293,6 +295,12 @@ class Transcript:
         if getattr(self, "h", None):
             lib().or_tr_free(self.h)
             self.h = None
+
+    def clone_state(self):
+        """A copy of the sponge (the reference's Clone, used by fork())."""
+        c = Transcript.__new__(Transcript)
+        c.h = lib().or_tr_clone(self.h)
+        return c
 
     def append_message(self, label: bytes, msg: bytes = b""):
         buf = np.frombuffer(msg, dtype=np.uint8) if msg else np.zeros(1, np.uint8)

@@ -1163,6 +1163,12 @@ or_transcript* or_tr_new(const char* app_label) {
     return t;
 }
 void or_tr_free(or_transcript* t) { free(t); }
+/* Poseidon2Transcript is Clone: fork() clones the sponge (neo-transcript/src/poseidon2.rs:160-164) */
+or_transcript* or_tr_clone(const or_transcript* t) {
+    or_transcript* c = (or_transcript*)malloc(sizeof(*c));
+    memcpy(c, t, sizeof(*c));
+    return c;
+}
 void or_tr_append_fields(or_transcript* t, const char* label, const uint64_t* fs, size_t n) {
     tr_bytes(t, label, strlen(label));
     tr_elem(t, n);

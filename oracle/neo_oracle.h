@@ -110,6 +110,7 @@ typedef struct or_transcript or_transcript;
 void or_poseidon2_permute(uint64_t* st);
 or_transcript* or_tr_new(const char* app_label);
 void or_tr_free(or_transcript* t);
+or_transcript* or_tr_clone(const or_transcript* t);
 void or_tr_append_message(or_transcript* t, const char* label, const uint8_t* msg, size_t len);
 void or_tr_append_fields(or_transcript* t, const char* label, const uint64_t* fs, size_t n);
 void or_tr_append_u64s(or_transcript* t, const char* label, const uint64_t* us, size_t n);
