@@ -230,6 +230,43 @@ typedef struct neo_gpu_shard neo_gpu_shard;
  * (crates/neo-reductions/src/engines/utils.rs:214-321) once. */
 int neo_gpu_shard_create(neo_gpu_ctx* ctx, const neo_ccs_desc* ccs, uint32_t m_in, uint32_t k_rho,
                          const char* app_label, neo_gpu_shard** out);
+/* One Twist memory or Shout lookup instance on the shared CPU bus
+ * (neo-memory MemInstance / LutInstance, bit addressing: ell_addr = d * ell;
+ * k, d, n_side, ell are bound into the transcript as given). */
+typedef struct {
+    uint32_t ell_addr;
+    uint64_t k, d, n_side, ell;
+    const uint64_t* table;        /* Shout: table_len F_q entries (NULL for Twist) */
+    uint64_t table_len;
+    uint64_t n_init;              /* Twist: MemInit::Sparse (address, value) pairs; 0 = MemInit::Zero */
+    const uint64_t* init_addr;
+    const uint64_t* init_val;
+} neo_mem_instance;
+/* The instances of every fold step of a shard.  `steps` trace steps per fold
+ * step occupy the tail of z: bus cell (col, j) at z[m - bus_cols*steps +
+ * col*steps + j], time row m_in + j, columns ordered as in
+ * build_bus_layout_for_instances (neo-memory/src/cpu/bus_layout.rs:91-190):
+ * every Shout [addr_bits.., has_lookup, val], then every Twist [ra_bits..,
+ * wa_bits.., has_read, has_write, wv, rv, inc]. */
+typedef struct {
+    uint64_t steps;
+    uint32_t n_shout;
+    const neo_mem_instance* shout;
+    uint32_t n_twist;
+    const neo_mem_instance* twist;
+} neo_mem_desc;
+/* A shard prover whose fold steps also prove the Route-A memory sidecar
+ * (fold_shard_prove_impl with a shared CPU bus, crates/neo-fold/src/
+ * shard.rs:1803-2283; memory_sidecar/memory.rs:86-1670): Shout / Twist
+ * address pre-time sum-checks, the Route-A time claims batched with the CCS
+ * rounds, bus openings on every ME claim, the Twist val-eval batch and the
+ * val lane (RLC + DEC of the CPU ME claims at r_val).  Shout instances share
+ * one ell_addr; ell_addr <= 24. */
+int neo_gpu_shard_create_mem(neo_gpu_ctx* ctx, const neo_ccs_desc* ccs, uint32_t m_in, uint32_t k_rho,
+                             const char* app_label, const neo_mem_desc* mem, neo_gpu_shard** out);
+/* Number of val-lane DEC children emitted so far (the reference's
+ * val_lane_obligations, shard.rs:2548-2991). */
+int neo_gpu_shard_val_obligations(const neo_gpu_shard* sh, uint64_t* count);
 /* One fold step on the main lane (no Twist/Shout): witness build
  * (decomp + MCS commit, crates/neo-fold/src/session.rs:977-978), Pi_CCS
  * (batched time rounds + Ajtai rounds), ME outputs, Pi_RLC, Pi_DEC
@@ -244,9 +281,10 @@ int neo_gpu_shard_fold_step_device(neo_gpu_shard* sh, const uint64_t* d_z, uint6
 int neo_gpu_shard_transcript_state(const neo_gpu_shard* sh, uint64_t* st8);
 int neo_gpu_shard_ccs_digest(const neo_gpu_shard* sh, uint64_t* d4);
 /* Host milliseconds of the last step: [0] total, [1] witness decomp+commit,
- * [2] header/ME binding + challenges, [3] Pi_CCS table build, [4] batched
- * time rounds, [5] Ajtai rounds, [6] ME outputs, [7] Pi_RLC, [8] Pi_DEC;
- * [9] transcript permutations of the step. */
+ * [2] header/ME binding + challenges, [3] Pi_CCS table build, [4] memory
+ * address pre-time + batched time rounds, [5] Ajtai rounds, [6] ME outputs,
+ * [7] val-eval batch + main-lane Pi_RLC/Pi_DEC, [8] val lane; [9] transcript
+ * permutations of the step; [10] memory-sidecar share of [4] and [7]. */
 int neo_gpu_shard_step_stats(const neo_gpu_shard* sh, double* out, uint32_t n);
 int neo_gpu_shard_destroy(neo_gpu_shard* sh);
 

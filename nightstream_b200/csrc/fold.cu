@@ -1,22 +1,31 @@
-// fold.cu -- device-resident Neo fold step for one shard (main lane, no
-// Twist/Shout): MCS commit -> Pi_CCS (batched time rounds + Ajtai rounds) ->
-// ME outputs -> Pi_RLC -> Pi_DEC (12 child commitments + child ME claims).
+// fold.cu -- device-resident Neo fold step for one shard, with the optional
+// shared-CPU-bus memory sidecar (Twist read/write memories, Shout lookups):
+// MCS commit -> [Shout / Twist address pre-time sum-checks] -> Pi_CCS
+// (batched time rounds over the CCS and Route-A memory claims + Ajtai rounds)
+// -> ME outputs (+ bus openings) -> [Twist val-eval batch, val-lane CPU ME
+// claims] -> Pi_RLC -> Pi_DEC (main lane, 12 child commitments) -> [val lane
+// RLC / DEC].
 //
 // Reference: fold_shard_prove_impl (crates/neo-fold/src/shard.rs:1725-2283),
 // prove_rlc_dec_lane (shard.rs:1170-1331), prove_route_a_batched_time
-// (crates/neo-fold/src/memory_sidecar/route_a_time.rs:28-152), the sum-check
-// drivers (crates/neo-reductions/src/sumcheck.rs:124-456) and their domain
-// separation (memory_sidecar/sumcheck_ds.rs:11-77).  The transcript calls are
-// issued in the reference's order with the reference's labels.
+// (crates/neo-fold/src/memory_sidecar/route_a_time.rs:28-152), the memory
+// sidecar (memory_sidecar/memory.rs:86-1670, cpu_bus.rs:195-320, 969-1016,
+// transcript.rs:4-63, utils.rs:43-71), the sum-check drivers
+// (crates/neo-reductions/src/sumcheck.rs:124-456) and their domain separation
+// (memory_sidecar/sumcheck_ds.rs:11-77).  The transcript calls are issued in
+// the reference's order with the reference's labels.
 //
 // All witness digit planes live in one device buffer Zall[1 + k_rho][54][m]:
 // slot 0 holds the step's MCS witness, slots 1..k_rho the carried children.
-// Pi_DEC writes the new children straight into slots 1..k_rho.
+// Pi_DEC writes the new children straight into slots 1..k_rho.  Bus columns
+// (the tail of z: cell (col, j) at bus_base + col * steps + j, time row
+// m_in + j) are decoded into dense K time columns d_cols[bus_cols][2^ell_n].
 #include "internal.cuh"
 #include "transcript.h"
 #include <algorithm>
 #include <chrono>
 #include <memory>
+#include <string>
 
 using gl::K;
 
@@ -32,10 +41,27 @@ struct MeInst {
     std::vector<uint64_t> c;      // kappa*54 (Commitment.data, column-major)
     std::vector<uint64_t> X;      // 54*m_in row-major
     std::vector<K> r;             // ell_n
-    std::vector<K> y;             // t * 2^ell_d (padded)
-    std::vector<K> ysc;           // t
+    std::vector<K> y;             // (t + bus_cols) * 2^ell_d (padded)
+    std::vector<K> ysc;           // t + bus_cols
     uint32_t m_in = 0;
     uint8_t digest[32] = {0};
+};
+
+struct ShoutInst {
+    uint32_t ea = 0;                      // ell_addr = d * ell
+    uint64_t k = 0, d = 0, n_side = 0, ell = 0;
+    std::vector<uint64_t> table;          // F_q entries
+    uint8_t digest[32] = {0};
+    DevBuf<K> d_table;                    // min(len, 2^ea) entries as K, zero padded to 2^ea
+    uint32_t col0 = 0;                    // addr bits col0.., has_lookup col0+ea, val col0+ea+1
+};
+
+struct TwistInst {
+    uint32_t ea = 0;
+    uint64_t k = 0, d = 0, n_side = 0, ell = 0;
+    std::vector<uint64_t> init_addr, init_val;  // MemInit::Sparse (empty: MemInit::Zero)
+    uint8_t digest[32] = {0};
+    uint32_t col0 = 0;  // ra col0.., wa col0+ea.., has_read +2ea, has_write +2ea+1, wv +2, rv +3, inc +4
 };
 
 static std::vector<uint8_t> le64(uint64_t v) {
@@ -104,6 +130,60 @@ __global__ void __launch_bounds__(256) child_y_kernel(const int8_t* __restrict__
     }
 }
 
+// build_time_sparse_from_bus_col (memory_sidecar/cpu_bus.rs:976-1016), dense:
+// out[c][t] = z[bus_base + c*steps + (t - m_in)] for m_in <= t < m_in + steps, else 0
+__global__ void bus_decode_kernel(const uint64_t* __restrict__ z, uint32_t m_in, uint64_t bus_base, uint64_t steps,
+                                  uint32_t ncols, uint64_t L, K* __restrict__ out) {
+    const uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+    if (i >= (uint64_t)ncols * L) return;
+    const uint64_t c = i / L, t = i - c * L;
+    K v = gl::kzero();
+    if (t >= m_in && t - m_in < steps) v = gl::kfq(gl::canon(z[bus_base + c * steps + (t - m_in)]));
+    out[i] = v;
+}
+
+// χ_r(m_in + j) for the bus time rows (cpu_bus.rs:180-192, 279-283)
+__global__ void bus_weights_kernel(const K* __restrict__ r, uint32_t ell, uint32_t m_in, uint64_t steps,
+                                   K* __restrict__ w) {
+    const uint64_t j = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+    if (j >= steps) return;
+    const uint64_t row = m_in + j;
+    K acc = gl::kone();
+    for (uint32_t b = 0; b < ell; b++) acc = gl::kmul(acc, ((row >> b) & 1) ? r[b] : gl::ksub(gl::kone(), r[b]));
+    w[j] = acc;
+}
+
+// bus openings y[w][c][rho] = Σ_j χ_r(m_in + j) Z_w[rho][bus_base + c*steps + j]
+// (append_bus_openings_to_me_instance, cpu_bus.rs:195-320); block per (c, rho), grid.y witnesses
+__global__ void __launch_bounds__(256) bus_open_kernel(const int8_t* __restrict__ Z, uint64_t m, uint64_t bus_base,
+                                                       uint64_t steps, uint32_t ncols, const K* __restrict__ w,
+                                                       K* __restrict__ y) {
+    const uint32_t c = blockIdx.x / NEO_D, rho = blockIdx.x % NEO_D, wi = blockIdx.y;
+    const int8_t* zr = Z + ((uint64_t)wi * NEO_D + rho) * m + bus_base + (uint64_t)c * steps;
+    K acc = gl::kzero();
+    for (uint64_t j = threadIdx.x; j < steps; j += blockDim.x) {
+        int z = zr[j];
+        if (z == 1) acc = gl::kadd(acc, w[j]);
+        else if (z == -1) acc = gl::ksub(acc, w[j]);
+        else if (z != 0) acc = gl::kadd(acc, gl::kscale_small(w[j], z));
+    }
+    __shared__ K red[8];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int o = 16; o > 0; o >>= 1) {
+        K b;
+        b.re = __shfl_xor_sync(0xffffffffu, acc.re, o);
+        b.im = __shfl_xor_sync(0xffffffffu, acc.im, o);
+        acc = gl::kadd(acc, b);
+    }
+    if (lane == 0) red[warp] = acc;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        K s = gl::kzero();
+        for (int u = 0; u < 8; u++) s = gl::kadd(s, red[u]);
+        y[((uint64_t)wi * ncols + c) * NEO_D + rho] = s;
+    }
+}
+
 }  // namespace
 
 // ---------------------------------------------------------------------------
@@ -127,6 +207,17 @@ struct neo_gpu_shard {
     neo_gpu_ccs_oracle* orc = nullptr;  // Pi_CCS oracle workspace reused across steps
     std::vector<uint64_t> proof;  // canonical dump of the last step
     double stats[12] = {0};       // host ms per phase of the last step, see neo_gpu_shard_step_stats
+    // ---- shared CPU bus (memory sidecar) ----
+    uint64_t steps = 0, bus_base = 0;
+    uint32_t bus_cols = 0;
+    std::vector<std::unique_ptr<ShoutInst>> shout;
+    std::vector<std::unique_ptr<TwistInst>> twist;
+    DevBuf<K> d_cols, d_prev_cols, d_asm, d_busw, d_busy, d_r, d_chi, d_vj, d_yv, d_yvsc, d_w;
+    DevBuf<int8_t> valwit;     // [2][54][m]: this step's and the previous step's MCS digits
+    DevBuf<int8_t> valplanes;  // [k_rho][54][m]: val-lane DEC children
+    bool has_prev = false;
+    std::vector<uint64_t> prev_c, prev_X;
+    uint64_t val_obligations = 0;
 };
 
 using hclock = std::chrono::steady_clock;
@@ -207,14 +298,26 @@ static void ccs_digest_words(const neo_ccs_desc* d, uint64_t* out4) {
     for (int i = 0; i < 4; i++) out4[i] = st[i];
 }
 
+// digest_fields (crates/neo-fold/src/memory_sidecar/transcript.rs:4-10)
+static void digest_fields(const char* label, const std::vector<uint64_t>& fs, uint8_t out[32]) {
+    neo::Transcript h("memory/public_digest");
+    h.append_message("digest/label", label);
+    auto n = le64(fs.size());
+    h.append_message("digest/len", n.data(), 8);
+    std::vector<uint64_t> c(fs.size());
+    for (size_t i = 0; i < fs.size(); i++) c[i] = gl::canon(fs[i]);
+    h.append_fields("digest/fields", c.data(), c.size());
+    h.digest32(out);
+}
+
 extern "C" int neo_ccs_digest(const neo_ccs_desc* d, uint64_t* out4) {
     if (!d || !out4 || d->t == 0 || d->n == 0 || d->m == 0) return NEO_ERR_ARG;
     ccs_digest_words(d, out4);
     return NEO_OK;
 }
 
-extern "C" int neo_gpu_shard_create(neo_gpu_ctx* ctx, const neo_ccs_desc* desc, uint32_t m_in, uint32_t k_rho,
-                                    const char* app_label, neo_gpu_shard** out) {
+static int shard_create_impl(neo_gpu_ctx* ctx, const neo_ccs_desc* desc, uint32_t m_in, uint32_t k_rho,
+                             const char* app_label, const neo_mem_desc* mem, neo_gpu_shard** out) {
     if (!ctx) return NEO_ERR_ARG;
     if (!desc || !out || !app_label) return ctx->fail(NEO_ERR_ARG, "shard_create: null argument");
     *out = nullptr;
@@ -244,6 +347,80 @@ extern "C" int neo_gpu_shard_create(neo_gpu_ctx* ctx, const neo_ccs_desc* desc, 
     ccs_digest_words(desc, sh->mat_digest);
     sh->tr.reset(new neo::Transcript(app_label));
     const uint64_t m = sh->m;
+    const uint64_t L = 1ULL << sh->ell_n;
+    // ---- memory instances and the bus layout (neo-memory/src/cpu/bus_layout.rs:91-190) ----
+    if (mem && (mem->n_shout || mem->n_twist)) {
+        if ((mem->n_shout && !mem->shout) || (mem->n_twist && !mem->twist))
+            return ctx->fail(NEO_ERR_ARG, "shard_create: null memory instance array");
+        if (mem->steps == 0) return ctx->fail(NEO_ERR_ARG, "shard_create: memory steps must be >= 1");
+        uint32_t col = 0;
+        for (uint32_t i = 0; i < mem->n_shout; i++) {
+            const neo_mem_instance& s = mem->shout[i];
+            if (s.ell_addr == 0 || s.ell_addr > 24) return ctx->fail(NEO_ERR_UNSUPPORTED, "shard_create: Shout ell_addr in 1..24");
+            if (i && s.ell_addr != mem->shout[0].ell_addr)
+                return ctx->fail(NEO_ERR_ARG, "shard_create: Shout instances need one ell_addr (batched addr-pre)");
+            if (s.table_len && !s.table) return ctx->fail(NEO_ERR_ARG, "shard_create: Shout table is null");
+            auto si = std::make_unique<ShoutInst>();
+            si->ea = s.ell_addr; si->k = s.k; si->d = s.d; si->n_side = s.n_side; si->ell = s.ell;
+            si->table.assign(s.table, s.table + s.table_len);
+            digest_fields("shout/table", si->table, si->digest);
+            const uint64_t P = 1ULL << s.ell_addr;
+            std::vector<K> tk(P, gl::kzero());
+            for (uint64_t a = 0; a < P && a < s.table_len; a++) tk[a] = gl::kfq(gl::canon(s.table[a]));
+            NEO_CK(ctx, si->d_table.alloc(P));
+            NEO_CK(ctx, cudaMemcpy(si->d_table.p, tk.data(), P * sizeof(K), cudaMemcpyHostToDevice));
+            si->col0 = col;
+            col += s.ell_addr + 2;
+            sh->shout.push_back(std::move(si));
+        }
+        for (uint32_t i = 0; i < mem->n_twist; i++) {
+            const neo_mem_instance& w = mem->twist[i];
+            if (w.ell_addr == 0 || w.ell_addr > 24) return ctx->fail(NEO_ERR_UNSUPPORTED, "shard_create: Twist ell_addr in 1..24");
+            if (w.n_init && (!w.init_addr || !w.init_val)) return ctx->fail(NEO_ERR_ARG, "shard_create: Twist init is null");
+            auto ti = std::make_unique<TwistInst>();
+            ti->ea = w.ell_addr; ti->k = w.k; ti->d = w.d; ti->n_side = w.n_side; ti->ell = w.ell;
+            std::vector<uint64_t> fs;
+            for (uint64_t e = 0; e < w.n_init; e++) {
+                if (w.init_addr[e] >> w.ell_addr) return ctx->fail(NEO_ERR_ARG, "shard_create: Twist init address out of range");
+                ti->init_addr.push_back(w.init_addr[e]);
+                ti->init_val.push_back(gl::canon(w.init_val[e]));
+                fs.push_back(w.init_addr[e]);
+                fs.push_back(w.init_val[e]);
+            }
+            if (w.n_init) digest_fields("twist/init/sparse", fs, ti->digest);
+            else digest_fields("twist/init/zero", fs, ti->digest);
+            ti->col0 = col;
+            col += 2 * w.ell_addr + 5;
+            sh->twist.push_back(std::move(ti));
+        }
+        sh->steps = mem->steps;
+        sh->bus_cols = col;
+        const uint64_t region = (uint64_t)col * mem->steps;
+        if (region > m || m - region < m_in) return ctx->fail(NEO_ERR_ARG, "shard_create: bus region overlaps the public inputs");
+        if (m_in + mem->steps > sh->n) return ctx->fail(NEO_ERR_ARG, "shard_create: bus time rows out of range");
+        sh->bus_base = m - region;
+        uint32_t max_asm = 2;
+        for (auto& s : sh->shout) max_asm = std::max(max_asm, s->ea + 1);
+        for (auto& w : sh->twist) max_asm = std::max(max_asm, 2 * w->ea + 4);
+        NEO_CK(ctx, sh->d_cols.alloc((size_t)col * L));
+        NEO_CK(ctx, sh->d_prev_cols.alloc((size_t)col * L));
+        size_t asm_len = (size_t)max_asm * L;
+        for (auto& s : sh->shout) asm_len = std::max<size_t>(asm_len, 2ULL << s->ea);
+        NEO_CK(ctx, sh->d_asm.alloc(asm_len));
+        NEO_CK(ctx, sh->d_busw.alloc(mem->steps));
+        NEO_CK(ctx, sh->d_busy.alloc((size_t)std::max<uint32_t>(1 + k_rho, 2) * col * NEO_D));
+        NEO_CK(ctx, sh->d_r.alloc(std::max<uint32_t>(sh->ell_n, 32)));
+        NEO_CK(ctx, sh->d_chi.alloc(L));
+        NEO_CK(ctx, sh->d_vj.alloc((size_t)sh->t * m));
+        NEO_CK(ctx, sh->d_yv.alloc((size_t)std::max<uint32_t>(k_rho, 2) * sh->t * NEO_D));
+        NEO_CK(ctx, sh->d_yvsc.alloc((size_t)std::max<uint32_t>(k_rho, 2) * sh->t));
+        NEO_CK(ctx, sh->valwit.alloc((size_t)2 * NEO_D * m));
+        NEO_CK(ctx, sh->valplanes.alloc((size_t)k_rho * NEO_D * m));
+        for (auto& s : sh->shout) (void)s;
+        size_t wmax = 1;
+        for (auto& s : sh->shout) wmax = std::max<size_t>(wmax, 1ULL << s->ea);
+        NEO_CK(ctx, sh->d_w.alloc(wmax));
+    }
     NEO_CK(ctx, sh->Zall.alloc((size_t)(1 + k_rho) * NEO_D * m));
     NEO_CK(ctx, sh->d_z.alloc(m));
     NEO_CK(ctx, sh->d_mix.alloc((size_t)NEO_D * m));
@@ -258,6 +435,16 @@ extern "C" int neo_gpu_shard_create(neo_gpu_ctx* ctx, const neo_ccs_desc* desc, 
     return NEO_OK;
 }
 
+extern "C" int neo_gpu_shard_create(neo_gpu_ctx* ctx, const neo_ccs_desc* desc, uint32_t m_in, uint32_t k_rho,
+                                    const char* app_label, neo_gpu_shard** out) {
+    return shard_create_impl(ctx, desc, m_in, k_rho, app_label, nullptr, out);
+}
+
+extern "C" int neo_gpu_shard_create_mem(neo_gpu_ctx* ctx, const neo_ccs_desc* desc, uint32_t m_in, uint32_t k_rho,
+                                        const char* app_label, const neo_mem_desc* mem, neo_gpu_shard** out) {
+    return shard_create_impl(ctx, desc, m_in, k_rho, app_label, mem, out);
+}
+
 extern "C" int neo_gpu_shard_destroy(neo_gpu_shard* sh) {
     if (!sh) return NEO_ERR_ARG;
     cudaSetDevice(sh->ctx->device);
@@ -270,12 +457,12 @@ extern "C" int neo_gpu_shard_destroy(neo_gpu_shard* sh) {
 // ---------------------------------------------------------------------------
 // one fold step
 // ---------------------------------------------------------------------------
-namespace {
+int ccs_oracle_create_dev(neo_gpu_ctx* ctx, const DevCcs* ccs, const int8_t* d_Z, uint32_t k, uint32_t b,
+                          const K* alpha, const K* beta_a, const K* beta_r, K gamma, const K* r_inputs,
+                          uint32_t ell_d, uint32_t ell_n, uint32_t d_sc, neo_gpu_ccs_oracle** out);
+int ccs_oracle_dev_vj(neo_gpu_ccs_oracle* o, const K** vj);
 
-struct Rounds {
-    std::vector<K> coeffs;  // rounds x (d_sc+1)
-    std::vector<K> chals;
-};
+namespace {
 
 static void interpolate(const std::vector<K>& xs, const std::vector<K>& ys, std::vector<K>& co) {
     // sumcheck.rs:74-118
@@ -321,12 +508,347 @@ static std::vector<uint64_t> k_flat(const std::vector<K>& v) {
     return f;
 }
 
-}  // namespace
+static inline bool keq(K a, K b) { return a.re == b.re && a.im == b.im; }
+static inline void push_k(std::vector<uint64_t>& P, K v) { P.push_back(v.re); P.push_back(v.im); }
 
-int ccs_oracle_create_dev(neo_gpu_ctx* ctx, const DevCcs* ccs, const int8_t* d_Z, uint32_t k, uint32_t b,
-                          const K* alpha, const K* beta_a, const K* beta_r, K gamma, const K* r_inputs,
-                          uint32_t ell_d, uint32_t ell_n, uint32_t d_sc, neo_gpu_ccs_oracle** out);
-int ccs_oracle_dev_vj(neo_gpu_ccs_oracle* o, const K** vj);
+// One claim of a batched sum-check: a GPU round oracle of one of three families.
+struct Claim {
+    std::string label;
+    uint32_t deg = 0;
+    bool dyn = true;
+    K sum{};
+    neo_gpu_ccs_oracle* ccs = nullptr;
+    neo_gpu_mem_oracle* mem = nullptr;
+    neo_gpu_twist_addr* ta = nullptr;
+    int evals(const K* xs, uint32_t nx, K* ys) const {
+        if (ccs) return neo_gpu_ccs_oracle_evals(ccs, (const uint64_t*)xs, nx, (uint64_t*)ys);
+        if (mem) return neo_gpu_mem_oracle_evals(mem, (const uint64_t*)xs, nx, (uint64_t*)ys);
+        return neo_gpu_twist_addr_evals(ta, (const uint64_t*)xs, nx, (uint64_t*)ys);
+    }
+    int fold(K r) const {
+        if (ccs) return neo_gpu_ccs_oracle_fold(ccs, (const uint64_t*)&r);
+        if (mem) return neo_gpu_mem_oracle_fold(mem, (const uint64_t*)&r);
+        return neo_gpu_twist_addr_fold(ta, (const uint64_t*)&r);
+    }
+};
+
+// Owns the memory oracles of one step.
+struct OracleSet {
+    std::vector<neo_gpu_mem_oracle*> mem;
+    std::vector<neo_gpu_twist_addr*> ta;
+    ~OracleSet() {
+        for (auto* o : mem) neo_gpu_mem_oracle_destroy(o);
+        for (auto* o : ta) neo_gpu_twist_addr_destroy(o);
+    }
+};
+
+// run_batched_sumcheck_prover (sumcheck.rs:350-456) inside sc_start / sc_end
+// (sumcheck_ds.rs:11-19); round polynomials appended to P in claim order
+static int run_batched_ds(neo_gpu_shard* sh, const char* domain, uint64_t inst_idx, std::vector<Claim>& cl,
+                          uint32_t rounds, std::vector<K>& chals, std::vector<K>& finals, std::vector<uint64_t>& P) {
+    neo_gpu_ctx* ctx = sh->ctx;
+    neo::Transcript& tr = *sh->tr;
+    auto bi = le64(inst_idx);
+    tr.append_message("sc/domain", domain);
+    tr.append_message("sc/inst_idx", bi.data(), 8);
+    std::vector<K> running(cl.size());
+    for (size_t i = 0; i < cl.size(); i++) running[i] = cl[i].sum;
+    std::vector<std::vector<K>> polys(cl.size());
+    chals.clear();
+    for (uint32_t rd = 0; rd < rounds; rd++) {
+        auto br = le64(rd);
+        tr.append_message("batched/round_idx", br.data(), 8);
+        for (size_t i = 0; i < cl.size(); i++) {
+            const uint32_t np = cl[i].deg + 1;
+            std::vector<K> xs(np), ys(np);
+            for (uint32_t x = 0; x < np; x++) xs[x] = gl::kfq(x);
+            int rc = cl[i].evals(xs.data(), np, ys.data());
+            if (rc) return rc;
+            if (!keq(gl::kadd(ys[0], ys[1]), running[i]))
+                return ctx->fail(NEO_ERR_INVARIANT, ("batched sum-check " + cl[i].label + ": p(0)+p(1) != running sum").c_str());
+            interpolate(xs, ys, polys[i]);
+        }
+        for (size_t i = 0; i < cl.size(); i++) {
+            tr.append_message("batched/claim_label", cl[i].label);
+            auto bc = le64(i);
+            tr.append_message("batched/claim_idx", bc.data(), 8);
+            for (auto& c : polys[i]) absorb_k(tr, "batched/round/coeff", c);
+        }
+        uint64_t c0 = tr.challenge_field("batched/challenge/0");
+        uint64_t c1 = tr.challenge_field("batched/challenge/1");
+        K r = gl::kmk(c0, c1);
+        chals.push_back(r);
+        for (size_t i = 0; i < cl.size(); i++) {
+            running[i] = poly_eval(polys[i], r);
+            int rc = cl[i].fold(r);
+            if (rc) return rc;
+            for (auto& c : polys[i]) push_k(P, c);
+        }
+    }
+    tr.append_message("sc/domain_end", domain);
+    tr.append_message("sc/inst_idx_end", bi.data(), 8);
+    finals = running;
+    return NEO_OK;
+}
+
+// bind_batched_claim_sums (memory_sidecar/transcript.rs:12-26)
+static void bind_claim_sums(neo::Transcript& tr, const char* prefix, const std::vector<K>& sums,
+                            const std::vector<std::string>& labels) {
+    auto n = le64(sums.size());
+    tr.append_message(prefix, n.data(), 8);
+    for (size_t i = 0; i < sums.size(); i++) {
+        tr.append_message("addr_batch/label", labels[i]);
+        auto bi = le64(i);
+        tr.append_message("addr_batch/idx", bi.data(), 8);
+        absorb_k(tr, "addr_batch/claimed_sum", sums[i]);
+    }
+}
+
+// sample_ext_point (neo-memory/src/ts_common.rs:22-37)
+static std::vector<K> sample_ext_point(neo::Transcript& tr, const char* label, const char* l0, const char* l1,
+                                       uint32_t n) {
+    std::vector<K> out;
+    for (uint32_t i = 0; i < n; i++) {
+        auto b8 = le64(i);
+        tr.append_message(label, b8.data(), 8);
+        uint64_t c0 = tr.challenge_field(l0);
+        uint64_t c1 = tr.challenge_field(l1);
+        out.push_back(gl::kmk(c0, c1));
+    }
+    return out;
+}
+
+// bitness_weights (memory_sidecar/utils.rs:43-71)
+static std::vector<K> bitness_weights(K r0, uint32_t n, uint64_t sep) {
+    K base = gl::kadd(r0, gl::kfq(gl::canon(sep)));
+    if (keq(base, gl::kzero()) || keq(base, gl::kone()) || keq(base, gl::kneg(gl::kone())))
+        base = gl::kadd(base, gl::kone());
+    if (keq(base, gl::kzero())) base = gl::kone();
+    std::vector<K> w;
+    K cur = gl::kone();
+    for (uint32_t i = 0; i < n; i++) {
+        w.push_back(cur);
+        cur = gl::kmul(cur, base);
+    }
+    return w;
+}
+
+// bus openings of n_w consecutive digit witnesses (stride 54*m) at the point
+// already in sh->d_r: y rows appended to the host vectors (bus_cols x 54 K per
+// witness) and their base-b scalars.
+static int bus_openings(neo_gpu_shard* sh, const int8_t* d_Z, uint32_t n_w, std::vector<K>& y, std::vector<K>& ysc) {
+    neo_gpu_ctx* ctx = sh->ctx;
+    const uint32_t nb = sh->bus_cols;
+    bus_weights_kernel<<<ceil_div(sh->steps, 256), 256, 0, ctx->stream>>>(sh->d_r.p, sh->ell_n, sh->m_in, sh->steps,
+                                                                          sh->d_busw.p);
+    NEO_LAUNCHED(ctx);
+    bus_open_kernel<<<dim3(nb * NEO_D, n_w), 256, 0, ctx->stream>>>(d_Z, sh->m, sh->bus_base, sh->steps, nb,
+                                                                    sh->d_busw.p, sh->d_busy.p);
+    NEO_LAUNCHED(ctx);
+    y.resize((size_t)n_w * nb * NEO_D);
+    NEO_CK(ctx, cudaMemcpyAsync(y.data(), sh->d_busy.p, y.size() * sizeof(K), cudaMemcpyDeviceToHost, ctx->stream));
+    NEO_CK(ctx, cudaStreamSynchronize(ctx->stream));
+    ysc.assign((size_t)n_w * nb, gl::kzero());
+    for (size_t q = 0; q < (size_t)n_w * nb; q++) {
+        K s = gl::kzero();
+        uint64_t pw = 1;
+        for (int rho = 0; rho < NEO_D; rho++) {
+            s = gl::kadd(s, gl::kscale(y[q * NEO_D + rho], pw));
+            pw = gl::mul(pw, sh->b);
+        }
+        ysc[q] = s;
+    }
+    return NEO_OK;
+}
+
+static int upload_point(neo_gpu_shard* sh, const std::vector<K>& r) {
+    NEO_CK(sh->ctx, cudaMemcpyAsync(sh->d_r.p, r.data(), r.size() * sizeof(K), cudaMemcpyHostToDevice, sh->ctx->stream));
+    return NEO_OK;
+}
+
+// gather bus columns (ids) of `src` into d_asm, in the given order
+static int assemble(neo_gpu_shard* sh, const K* src, const std::vector<uint32_t>& ids) {
+    const uint64_t L = 1ULL << sh->ell_n;
+    for (size_t i = 0; i < ids.size(); i++)
+        NEO_CK(sh->ctx, cudaMemcpyAsync(sh->d_asm.p + i * L, src + (size_t)ids[i] * L, L * sizeof(K),
+                                        cudaMemcpyDeviceToDevice, sh->ctx->stream));
+    return NEO_OK;
+}
+
+static std::vector<uint32_t> twist_read_ids(const TwistInst& w) {
+    std::vector<uint32_t> v = {w.col0 + 2 * w.ea, w.col0 + 2 * w.ea + 3};  // has_read, rv
+    for (uint32_t b = 0; b < w.ea; b++) v.push_back(w.col0 + b);            // ra bits
+    v.push_back(w.col0 + 2 * w.ea + 1);                                     // has_write
+    v.push_back(w.col0 + 2 * w.ea + 4);                                     // inc
+    for (uint32_t b = 0; b < w.ea; b++) v.push_back(w.col0 + w.ea + b);     // wa bits
+    return v;
+}
+static std::vector<uint32_t> twist_write_ids(const TwistInst& w) {
+    std::vector<uint32_t> v = {w.col0 + 2 * w.ea + 1, w.col0 + 2 * w.ea + 2, w.col0 + 2 * w.ea + 4};  // hw, wv, inc
+    for (uint32_t b = 0; b < w.ea; b++) v.push_back(w.col0 + w.ea + b);
+    return v;
+}
+static std::vector<uint32_t> twist_val_ids(const TwistInst& w) {
+    std::vector<uint32_t> v = {w.col0 + 2 * w.ea + 1, w.col0 + 2 * w.ea + 4};  // hw, inc
+    for (uint32_t b = 0; b < w.ea; b++) v.push_back(w.col0 + w.ea + b);
+    return v;
+}
+
+// prove_rlc_dec_lane (shard.rs:1170-1331): bind inputs, sample rhos, mix,
+// split into k_rho planes (d_planes), commit, child ME claims at r (core rows
+// from vj, bus rows from the planes), DEC public checks.
+static int rlc_dec_lane(neo_gpu_shard* sh, const char* lane, uint32_t idx, const std::vector<MeInst>& ins,
+                        const int8_t* d_wits, int8_t* d_planes, const std::vector<K>& r, const K* d_vj,
+                        const uint8_t* digest, std::vector<MeInst>& children, std::vector<uint64_t>& P) {
+    neo_gpu_ctx* ctx = sh->ctx;
+    neo::Transcript& tr = *sh->tr;
+    const uint32_t k = (uint32_t)ins.size(), t = sh->t, kappa = sh->kappa, nb = sh->bus_cols;
+    const uint32_t d_pad = 1u << sh->ell_d;
+    const uint64_t m = sh->m;
+    int rc;
+    tr.append_message("fold/rlc_inputs/v1", lane);
+    uint64_t si = idx, mc = k;
+    tr.append_u64s("step_idx", &si, 1);
+    tr.append_u64s("me_count", &mc, 1);
+    for (auto& me : ins) {
+        tr.append_fields("c_data", me.c.data(), me.c.size());
+        uint64_t mi = me.m_in;
+        tr.append_u64s("m_in", &mi, 1);
+        tr.append_message("me_fold_digest", me.digest, 32);
+        for (auto& rl : me.r) absorb_k(tr, "r_limb", rl);
+        tr.append_fields("X", me.X.data(), me.X.size());
+        for (auto& ye : me.y) absorb_k(tr, "y_elem", ye);
+        for (auto& ys_ : me.ysc) absorb_k(tr, "y_scalar", ys_);
+        uint64_t zero = 0;
+        tr.append_u64s("c_step_coords_len", &zero, 1);
+        tr.append_fields("c_step_coords", nullptr, 0);
+        tr.append_u64s("u_offset", &zero, 1);
+        tr.append_u64s("u_len", &zero, 1);
+    }
+    // sample_rot_rhos_n (common.rs:467-573) with draw_alphabet_vector (common.rs:432-465)
+    std::vector<int8_t> rhos((size_t)k * NEO_D);
+    static const int8_t A5[5] = {-2, -1, 0, 1, 2};
+    for (uint32_t i = 0; i < k; i++) {
+        auto bi = le64(i);
+        tr.append_message("rlc/rot/index", bi.data(), 8);
+        const uint32_t bucket = (1u << 16) / 5 * 5;
+        uint64_t ctr = i;
+        size_t got = 0;
+        while (got < NEO_D) {
+            auto bc = le64(ctr);
+            tr.append_message("rlc/rot/chunk", bc.data(), 8);
+            uint8_t dig[32];
+            tr.digest32(dig);
+            for (int w = 0; w < 16 && got < NEO_D; w++) {
+                uint32_t xv = (uint32_t)dig[2 * w] | ((uint32_t)dig[2 * w + 1] << 8);
+                if (xv < bucket) rhos[(size_t)i * NEO_D + got++] = A5[xv % 5];
+            }
+            ctr++;
+        }
+    }
+    for (auto v : rhos) P.push_back(gl::from_i64(v));
+    // Z_mix = sum rho_i Z_i (count == 1: identity)
+    if ((rc = rlc_mix_device(ctx, rhos.data(), d_wits, k, m, sh->d_mix.p, sh->d_rot.p))) return rc;
+    // parent commitment and core y: rot mixes of the k commitments / y vectors
+    std::vector<uint64_t> c_parent((size_t)kappa * NEO_D);
+    std::vector<K> y_parent((size_t)t * NEO_D);
+    {
+        std::vector<uint64_t> cv((size_t)k * kappa * NEO_D);
+        for (uint32_t i = 0; i < k; i++) memcpy(&cv[(size_t)i * kappa * NEO_D], ins[i].c.data(), kappa * NEO_D * 8);
+        NEO_CK(ctx, cudaMemcpyAsync(sh->d_mixv.p, cv.data(), cv.size() * 8, cudaMemcpyHostToDevice, ctx->stream));
+        rot_mix_kernel<<<kappa, 64, 0, ctx->stream>>>(sh->d_rot.p, k, sh->d_mixv.p, kappa, 1, sh->d_mixo.p);
+        NEO_LAUNCHED(ctx);
+        NEO_CK(ctx, cudaMemcpyAsync(c_parent.data(), sh->d_mixo.p, c_parent.size() * 8, cudaMemcpyDeviceToHost, ctx->stream));
+        NEO_CK(ctx, cudaStreamSynchronize(ctx->stream));
+        std::vector<K> yv((size_t)k * t * NEO_D);
+        for (uint32_t i = 0; i < k; i++)
+            for (uint32_t j = 0; j < t; j++)
+                for (int rho = 0; rho < NEO_D; rho++) yv[((size_t)i * t + j) * NEO_D + rho] = ins[i].y[(size_t)j * d_pad + rho];
+        // y vectors as [k][t][54] K = stride-2 F_q
+        NEO_CK(ctx, cudaMemcpyAsync(sh->d_mixv.p, yv.data(), yv.size() * 16, cudaMemcpyHostToDevice, ctx->stream));
+        rot_mix_kernel<<<t * 2, 64, 0, ctx->stream>>>(sh->d_rot.p, k, sh->d_mixv.p, t, 2, sh->d_mixo.p);
+        NEO_LAUNCHED(ctx);
+        NEO_CK(ctx, cudaMemcpyAsync(y_parent.data(), sh->d_mixo.p, y_parent.size() * 16, cudaMemcpyDeviceToHost, ctx->stream));
+        NEO_CK(ctx, cudaStreamSynchronize(ctx->stream));
+    }
+    P.insert(P.end(), c_parent.begin(), c_parent.end());
+    // Pi_DEC: split into k_rho planes, commit, child claims
+    if ((rc = split_b_device(ctx, sh->d_mix.p, (uint64_t)NEO_D * m, sh->k_rho, sh->b, d_planes, sh->d_flags.p))) return rc;
+    if ((rc = launch_commit(ctx, d_planes, sh->k_rho, m, sh->d_commits.p))) return rc;
+    child_y_kernel<<<sh->k_rho * NEO_D, 256, 0, ctx->stream>>>(d_planes, m, t, d_vj, sh->d_ychild.p);
+    NEO_LAUNCHED(ctx);
+    uint32_t flags[2];
+    std::vector<uint64_t> cc((size_t)sh->k_rho * kappa * NEO_D);
+    std::vector<K> yc((size_t)sh->k_rho * t * NEO_D);
+    std::vector<int8_t> Xc((size_t)sh->k_rho * NEO_D * sh->m_in);
+    NEO_CK(ctx, cudaMemcpyAsync(flags, sh->d_flags.p, 8, cudaMemcpyDeviceToHost, ctx->stream));
+    NEO_CK(ctx, cudaMemcpyAsync(cc.data(), sh->d_commits.p, cc.size() * 8, cudaMemcpyDeviceToHost, ctx->stream));
+    NEO_CK(ctx, cudaMemcpyAsync(yc.data(), sh->d_ychild.p, yc.size() * 16, cudaMemcpyDeviceToHost, ctx->stream));
+    NEO_CK(ctx, cudaMemcpy2DAsync(Xc.data(), sh->m_in, d_planes, m, sh->m_in, (size_t)sh->k_rho * NEO_D,
+                                  cudaMemcpyDeviceToHost, ctx->stream));
+    NEO_CK(ctx, cudaStreamSynchronize(ctx->stream));
+    if ((rc = check_device_error(ctx))) return rc;
+    if (flags[0]) return ctx->fail(NEO_ERR_INVARIANT, "DEC split: Z_mix entry out of range for k_rho digits");
+    std::vector<K> by, bsc;
+    if (nb) {
+        if ((rc = upload_point(sh, r))) return rc;
+        if ((rc = bus_openings(sh, d_planes, sh->k_rho, by, bsc))) return rc;
+    }
+    // DEC public checks (dec_children_with_commit_cached): c and core y recompose in base b
+    {
+        std::vector<uint64_t> cs(c_parent.size(), 0);
+        uint64_t pw = 1;
+        for (uint32_t i = 0; i < sh->k_rho; i++) {
+            for (size_t q = 0; q < cs.size(); q++) cs[q] = gl::add(cs[q], gl::mul(cc[(size_t)i * kappa * NEO_D + q], pw));
+            pw = gl::mul(pw, sh->b);
+        }
+        if (cs != c_parent) return ctx->fail(NEO_ERR_INVARIANT, "DEC public check failed (c)");
+        std::vector<K> ysum(y_parent.size(), gl::kzero());
+        pw = 1;
+        for (uint32_t i = 0; i < sh->k_rho; i++) {
+            for (size_t q = 0; q < ysum.size(); q++) ysum[q] = gl::kadd(ysum[q], gl::kscale(yc[(size_t)i * t * NEO_D + q], pw));
+            pw = gl::mul(pw, sh->b);
+        }
+        for (size_t q = 0; q < ysum.size(); q++)
+            if (!keq(ysum[q], y_parent[q])) return ctx->fail(NEO_ERR_INVARIANT, "DEC public check failed (y)");
+    }
+    children.assign(sh->k_rho, MeInst());
+    uint64_t pwb[NEO_D];
+    pwb[0] = 1;
+    for (int q = 1; q < NEO_D; q++) pwb[q] = gl::mul(pwb[q - 1], sh->b);
+    for (uint32_t i = 0; i < sh->k_rho; i++) {
+        MeInst& ch = children[i];
+        ch.c.assign(cc.begin() + (size_t)i * kappa * NEO_D, cc.begin() + (size_t)(i + 1) * kappa * NEO_D);
+        ch.X.resize((size_t)NEO_D * sh->m_in);
+        for (size_t q = 0; q < ch.X.size(); q++) ch.X[q] = gl::from_i64(Xc[(size_t)i * NEO_D * sh->m_in + q]);
+        ch.r = r;
+        ch.m_in = sh->m_in;
+        ch.y.assign((size_t)(t + nb) * d_pad, gl::kzero());
+        ch.ysc.resize(t + nb);
+        for (uint32_t j = 0; j < t; j++) {
+            K s = gl::kzero();
+            for (int rho = 0; rho < NEO_D; rho++) {
+                K v = yc[((size_t)i * t + j) * NEO_D + rho];
+                ch.y[j * d_pad + rho] = v;
+                s = gl::kadd(s, gl::kscale(v, pwb[rho]));
+            }
+            ch.ysc[j] = s;
+        }
+        for (uint32_t c = 0; c < nb; c++) {
+            for (int rho = 0; rho < NEO_D; rho++) ch.y[(size_t)(t + c) * d_pad + rho] = by[((size_t)i * nb + c) * NEO_D + rho];
+            ch.ysc[t + c] = bsc[(size_t)i * nb + c];
+        }
+        memcpy(ch.digest, digest, 32);
+        P.insert(P.end(), ch.c.begin(), ch.c.end());
+        for (uint32_t j = 0; j < t; j++)
+            for (int rho = 0; rho < NEO_D; rho++) push_k(P, ch.y[j * d_pad + rho]);
+        for (uint32_t c = 0; c < nb; c++)
+            for (int rho = 0; rho < NEO_D; rho++) push_k(P, ch.y[(size_t)(t + c) * d_pad + rho]);
+    }
+    return NEO_OK;
+}
+
+}  // namespace
 
 static int fold_step_impl(neo_gpu_shard* sh, const uint64_t* z_host, const uint64_t* d_z_in) {
     neo_gpu_ctx* ctx = sh->ctx;
@@ -337,6 +859,9 @@ static int fold_step_impl(neo_gpu_shard* sh, const uint64_t* z_host, const uint6
     const uint32_t n_acc = (uint32_t)sh->acc.size();
     const uint32_t k = 1 + n_acc;
     const uint32_t d_pad = 1u << ell_d;
+    const uint32_t nb = sh->bus_cols;
+    const uint64_t L = 1ULL << ell_n;
+    const bool has_mem = nb > 0;
     std::vector<uint64_t>& P = sh->proof;
     P.clear();
     int rc;
@@ -344,6 +869,7 @@ static int fold_step_impl(neo_gpu_shard* sh, const uint64_t* z_host, const uint6
     const uint64_t perms0 = tr.permutations();
     for (double& v : sh->stats) v = 0;
     auto t_ph = hclock::now();
+    double mem_ms = 0;
 
     // ---- witness build: z -> Z (decomp) -> c = commit(Z)  (session.rs:977-978) ----
     const uint64_t* d_z = d_z_in;
@@ -354,6 +880,11 @@ static int fold_step_impl(neo_gpu_shard* sh, const uint64_t* z_host, const uint6
     decomp_b2_kernel<<<ceil_div(m, 256), 256, 0, ctx->stream>>>(d_z, m, sh->Zall.p);
     NEO_LAUNCHED(ctx);
     if ((rc = launch_commit(ctx, sh->Zall.p, 1, m, sh->d_commits.p))) return rc;
+    if (has_mem) {
+        bus_decode_kernel<<<ceil_div((uint64_t)nb * L, 256), 256, 0, ctx->stream>>>(d_z, sh->m_in, sh->bus_base, sh->steps,
+                                                                                    nb, L, sh->d_cols.p);
+        NEO_LAUNCHED(ctx);
+    }
     MeInst mcs;
     mcs.c.resize((size_t)kappa * NEO_D);
     std::vector<uint64_t> x(sh->m_in);
@@ -371,6 +902,37 @@ static int fold_step_impl(neo_gpu_shard* sh, const uint64_t* z_host, const uint6
     sh->stats[1] = ms_since(t_ph);
     t_ph = hclock::now();
 
+    // ---- absorb_step_memory_witness (memory_sidecar/memory.rs:86-124) ----
+    {
+        auto u = [&](const char* label, uint64_t v) {
+            auto b8 = le64(v);
+            tr.append_message(label, b8.data(), 8);
+        };
+        tr.append_message("step/absorb_memory_start", nullptr, 0);
+        u("step/lut_count", sh->shout.size());
+        for (size_t i = 0; i < sh->shout.size(); i++) {
+            const ShoutInst& s = *sh->shout[i];
+            u("step/lut_idx", i);
+            u("shout/k", s.k);
+            u("shout/d", s.d);
+            u("shout/n_side", s.n_side);
+            u("shout/steps", sh->steps);
+            u("shout/ell", s.ell);
+            tr.append_message("shout/table_digest", s.digest, 32);
+        }
+        u("step/mem_count", sh->twist.size());
+        for (size_t i = 0; i < sh->twist.size(); i++) {
+            const TwistInst& w = *sh->twist[i];
+            u("step/mem_idx", i);
+            u("twist/k", w.k);
+            u("twist/d", w.d);
+            u("twist/n_side", w.n_side);
+            u("twist/steps", sh->steps);
+            u("twist/ell", w.ell);
+            tr.append_message("twist/init_digest", w.digest, 32);
+        }
+        tr.append_message("step/absorb_memory_done", nullptr, 0);
+    }
     // ---- bind_header_and_instances_with_digest (engines/utils.rs:83-136) ----
     tr.append_message("phase/pi-ccs", nullptr, 0);
     tr.append_message("neo/ccs/header/v1", nullptr, 0);
@@ -431,7 +993,7 @@ static int fold_step_impl(neo_gpu_shard* sh, const uint64_t* z_host, const uint6
     for (auto& bb : beta) bb = chal_k();
     K gamma = chal_k();
     std::vector<K> beta_a(beta.begin(), beta.begin() + ell_d), beta_r(beta.begin() + ell_d, beta.end());
-    // ---- claimed_initial_sum_from_inputs (optimized_engine/common.rs:839-947) ----
+    // ---- claimed_initial_sum_from_inputs (optimized_engine/common.rs:839-947), core rows ----
     K T = gl::kzero();
     if (k >= 2) {
         std::vector<K> chi_a(d_pad);
@@ -457,15 +1019,9 @@ static int fold_step_impl(neo_gpu_shard* sh, const uint64_t* z_host, const uint6
         T = gl::kmul(gk, inner);
     }
     absorb_k(tr, "sumcheck/initial_sum", T);
-    P.push_back(T.re);
-    P.push_back(T.im);
+    push_k(P, T);
     // ---- r_cycle = sample_ext_point (neo-memory/src/ts_common.rs:22-37) ----
-    for (uint32_t i = 0; i < ell_n; i++) {
-        auto b8 = le64(i);
-        tr.append_message("route_a/r_cycle", b8.data(), 8);
-        tr.challenge_field("route_a/cycle/0");
-        tr.challenge_field("route_a/cycle/1");
-    }
+    std::vector<K> r_cycle = sample_ext_point(tr, "route_a/r_cycle", "route_a/cycle/0", "route_a/cycle/1", ell_n);
 
     sh->stats[2] = ms_since(t_ph);
     t_ph = hclock::now();
@@ -475,59 +1031,221 @@ static int fold_step_impl(neo_gpu_shard* sh, const uint64_t* z_host, const uint6
                                     gamma, rin, ell_d, ell_n, d_sc, &sh->orc)))
         return rc;
     neo_gpu_ccs_oracle* orc = sh->orc;
-
     sh->stats[3] = ms_since(t_ph);
     t_ph = hclock::now();
-    std::vector<K> xs(d_sc + 1), ys(d_sc + 1), co;
-    for (uint32_t i = 0; i <= d_sc; i++) xs[i] = gl::kfq(i);
-    // ---- batched time sum-check, one claim "ccs/time" (route_a_time.rs:28-152) ----
+
+    OracleSet os;
+    std::vector<Claim> claims;
     {
-        auto b1 = le64(1), b0 = le64(0), bd = le64(d_sc);
-        tr.append_message("batched/dynamic_bind/len", b1.data(), 8);
-        tr.append_message("batched/dynamic_bind/claim_label", "ccs/time");
-        tr.append_message("batched/dynamic_bind/claim_idx", b0.data(), 8);
-        tr.append_message("batched/dynamic_bind/degree_bound", bd.data(), 8);
-        uint8_t one = 1;
-        tr.append_message("batched/dynamic_bind/is_dynamic", &one, 1);
-        absorb_k(tr, "batched/dynamic_bind/claimed_sum", T);
+        Claim c;
+        c.label = "ccs/time";
+        c.deg = d_sc;
+        c.dyn = true;
+        c.sum = T;
+        c.ccs = orc;
+        claims.push_back(c);
     }
-    auto bidx = le64(idx);
-    tr.append_message("sc/domain", "shard/batched_time");
-    tr.append_message("sc/inst_idx", bidx.data(), 8);
-    K running = T;
-    std::vector<K> r_time;
-    for (uint32_t rd = 0; rd < ell_n; rd++) {
-        auto br = le64(rd);
-        tr.append_message("batched/round_idx", br.data(), 8);
-        if ((rc = neo_gpu_ccs_oracle_evals(orc, (const uint64_t*)xs.data(), d_sc + 1, (uint64_t*)ys.data()))) return rc;
-        K s01 = gl::kadd(ys[0], ys[1]);
-        if (s01.re != running.re || s01.im != running.im)
-            return ctx->fail(NEO_ERR_INVARIANT, "batched sum-check: p(0)+p(1) != running sum");
-        interpolate(xs, ys, co);
-        tr.append_message("batched/claim_label", "ccs/time");
-        auto b0 = le64(0);
-        tr.append_message("batched/claim_idx", b0.data(), 8);
-        for (auto& c : co) absorb_k(tr, "batched/round/coeff", c);
-        uint64_t c0 = tr.challenge_field("batched/challenge/0");
-        uint64_t c1 = tr.challenge_field("batched/challenge/1");
-        K r = gl::kmk(c0, c1);
-        r_time.push_back(r);
-        running = poly_eval(co, r);
-        if ((rc = neo_gpu_ccs_oracle_fold(orc, (const uint64_t*)&r))) return rc;
-        for (auto& c : co) { P.push_back(c.re); P.push_back(c.im); }
+    std::vector<K> r_addr_s;
+    std::vector<std::vector<K>> r_addr_t(sh->twist.size());
+    std::vector<K> twist_read(sh->twist.size()), twist_write(sh->twist.size());
+    if (has_mem) {
+        auto t_mem = hclock::now();
+        if ((rc = upload_point(sh, r_cycle))) return rc;
+        const K* C = sh->d_cols.p;
+        // ---- Shout address pre-time (memory.rs:430-621) ----
+        if (!sh->shout.empty()) {
+            const uint32_t ea = sh->shout[0]->ea;
+            std::vector<K> sums;
+            uint64_t active = 0;
+            std::vector<Claim> ac;
+            for (size_t i = 0; i < sh->shout.size(); i++) {
+                const ShoutInst& s = *sh->shout[i];
+                const K* has = C + (size_t)(s.col0 + s.ea) * L;
+                // has_any_lookup: any nonzero gate in this step's bus column
+                std::vector<K> hg(sh->steps);
+                NEO_CK(ctx, cudaMemcpy(hg.data(), has + sh->m_in, sh->steps * sizeof(K), cudaMemcpyDeviceToHost));
+                bool any = false;
+                for (auto& g : hg) any |= !gl::kiszero(g);
+                if (!any) {
+                    sums.push_back(gl::kzero());
+                    continue;
+                }
+                const uint64_t Pn = 1ULL << s.ea;
+                K cl;
+                if ((rc = addr_weights_device(ctx, ell_n, sh->d_r.p, s.ea, has, C + (size_t)s.col0 * L, s.d_table.p,
+                                              std::min<uint64_t>(s.table.size(), Pn), sh->d_w.p, &cl)))
+                    return rc;
+                // ProductRoundOracle over [table, weights] (twist_oracle.rs:1719-1722), degree 2
+                NEO_CK(ctx, cudaMemcpyAsync(sh->d_asm.p, s.d_table.p, Pn * sizeof(K), cudaMemcpyDeviceToDevice, ctx->stream));
+                NEO_CK(ctx, cudaMemcpyAsync(sh->d_asm.p + Pn, sh->d_w.p, Pn * sizeof(K), cudaMemcpyDeviceToDevice, ctx->stream));
+                neo_gpu_mem_oracle* po = nullptr;
+                if ((rc = neo_gpu_mem_oracle_create_device(ctx, NEO_MEM_PRODUCT, s.ea, nullptr, 0, nullptr, nullptr, 2,
+                                                           (const uint64_t*)sh->d_asm.p, nullptr, nullptr, &po)))
+                    return rc;
+                os.mem.push_back(po);
+                Claim c;
+                c.label = "shout/addr_pre";
+                c.deg = 2;
+                c.sum = cl;
+                c.mem = po;
+                ac.push_back(c);
+                sums.push_back(cl);
+                active |= 1ULL << i;
+            }
+            auto bi = le64(idx);
+            tr.append_message("shout/addr_pre_time/step_idx", bi.data(), 8);
+            bind_claim_sums(tr, "shout/addr_pre_time/claimed_sums", sums,
+                            std::vector<std::string>(sums.size(), "shout/addr_pre"));
+            for (auto& s : sums) push_k(P, s);
+            P.push_back(active);
+            if (active == 0) {
+                tr.append_message("shout/addr_pre_time/no_sumcheck", bi.data(), 8);
+                r_addr_s = sample_ext_point(tr, "shout/addr_pre_time/no_sumcheck/r_addr",
+                                            "shout/addr_pre_time/no_sumcheck/r_addr/0",
+                                            "shout/addr_pre_time/no_sumcheck/r_addr/1", ea);
+            } else {
+                std::vector<K> fin;
+                if ((rc = run_batched_ds(sh, "shout/addr_pre_time", idx, ac, ea, r_addr_s, fin, P))) return rc;
+            }
+            for (auto& r : r_addr_s) push_k(P, r);
+        }
+        // ---- Twist address pre-time (memory.rs:232-428) ----
+        for (size_t i = 0; i < sh->twist.size(); i++) {
+            const TwistInst& w = *sh->twist[i];
+            std::vector<uint64_t> iv(2 * w.init_val.size());
+            for (size_t e = 0; e < w.init_val.size(); e++) { iv[2 * e] = w.init_val[e]; iv[2 * e + 1] = 0; }
+            neo_gpu_twist_addr *ro = nullptr, *wo = nullptr;
+            if ((rc = assemble(sh, C, twist_read_ids(w)))) return rc;
+            if ((rc = neo_gpu_twist_addr_create_device(ctx, 0, ell_n, (const uint64_t*)r_cycle.data(), w.ea,
+                                                       w.init_addr.size(), w.init_addr.data(), iv.data(),
+                                                       (const uint64_t*)sh->d_asm.p, &ro)))
+                return rc;
+            os.ta.push_back(ro);
+            if ((rc = assemble(sh, C, twist_write_ids(w)))) return rc;
+            if ((rc = neo_gpu_twist_addr_create_device(ctx, 1, ell_n, (const uint64_t*)r_cycle.data(), w.ea,
+                                                       w.init_addr.size(), w.init_addr.data(), iv.data(),
+                                                       (const uint64_t*)sh->d_asm.p, &wo)))
+                return rc;
+            os.ta.push_back(wo);
+            auto bi = le64(i);
+            tr.append_message("twist/addr_pre_time/claim_idx", bi.data(), 8);
+            std::vector<std::string> labels = {"twist/read_addr_pre", "twist/write_addr_pre"};
+            bind_claim_sums(tr, "twist/addr_pre_time/claimed_sums", {gl::kzero(), gl::kzero()}, labels);
+            std::vector<Claim> tc(2);
+            tc[0].label = labels[0]; tc[0].deg = 2; tc[0].sum = gl::kzero(); tc[0].ta = ro;
+            tc[1].label = labels[1]; tc[1].deg = 2; tc[1].sum = gl::kzero(); tc[1].ta = wo;
+            std::vector<K> fin;
+            if ((rc = run_batched_ds(sh, "twist/addr_pre_time", i, tc, w.ea, r_addr_t[i], fin, P))) return rc;
+            for (auto& r : r_addr_t[i]) push_k(P, r);
+            twist_read[i] = fin[0];
+            twist_write[i] = fin[1];
+            push_k(P, fin[0]);
+            push_k(P, fin[1]);
+        }
+        // ---- Route-A time oracles (memory.rs:905-1033) ----
+        for (size_t i = 0; i < sh->shout.size(); i++) {
+            const ShoutInst& s = *sh->shout[i];
+            neo_gpu_mem_oracle *vo = nullptr, *ao = nullptr, *bo = nullptr;
+            K vc, ac_, bc;
+            // value: [has_lookup, val] are adjacent bus columns
+            if ((rc = neo_gpu_mem_oracle_create_device(ctx, NEO_MEM_SHOUT_VALUE, ell_n, (const uint64_t*)r_cycle.data(),
+                                                       0, nullptr, nullptr, 2, (const uint64_t*)(C + (size_t)(s.col0 + s.ea) * L),
+                                                       nullptr, (uint64_t*)&vc, &vo)))
+                return rc;
+            os.mem.push_back(vo);
+            std::vector<uint32_t> ids = {s.col0 + s.ea};
+            for (uint32_t b = 0; b < s.ea; b++) ids.push_back(s.col0 + b);
+            if ((rc = assemble(sh, C, ids))) return rc;
+            if ((rc = neo_gpu_mem_oracle_create_device(ctx, NEO_MEM_SHOUT_ADAPTER, ell_n, (const uint64_t*)r_cycle.data(),
+                                                       s.ea, (const uint64_t*)r_addr_s.data(), nullptr, 1 + s.ea,
+                                                       (const uint64_t*)sh->d_asm.p, nullptr, (uint64_t*)&ac_, &ao)))
+                return rc;
+            os.mem.push_back(ao);
+            // bitness over [addr_bits..., has_lookup] (adjacent columns)
+            auto bw = bitness_weights(r_cycle[0], s.ea + 1, 0x53484F5554ULL + i);
+            if ((rc = neo_gpu_mem_oracle_create_device(ctx, NEO_MEM_BITNESS, ell_n, (const uint64_t*)r_cycle.data(), 0,
+                                                       nullptr, nullptr, s.ea + 1, (const uint64_t*)(C + (size_t)s.col0 * L),
+                                                       (const uint64_t*)bw.data(), (uint64_t*)&bc, &bo)))
+                return rc;
+            os.mem.push_back(bo);
+            Claim cv, ca, cb;
+            cv.label = "shout/value"; cv.deg = 3; cv.sum = vc; cv.mem = vo;
+            ca.label = "shout/adapter"; ca.deg = 2 + s.ea; ca.sum = ac_; ca.mem = ao;
+            cb.label = "shout/bitness"; cb.deg = 3; cb.dyn = false; cb.sum = gl::kzero(); cb.mem = bo;
+            claims.push_back(cv);
+            claims.push_back(ca);
+            claims.push_back(cb);
+        }
+        for (size_t i = 0; i < sh->twist.size(); i++) {
+            const TwistInst& w = *sh->twist[i];
+            // eval_init_at_r_addr (neo-memory/src/mem_init.rs:133-163)
+            K init_r = gl::kzero();
+            for (size_t e = 0; e < w.init_addr.size(); e++) {
+                K chi = gl::kone();
+                for (uint32_t b = 0; b < w.ea; b++)
+                    chi = gl::kmul(chi, ((w.init_addr[e] >> b) & 1) ? r_addr_t[i][b] : gl::ksub(gl::kone(), r_addr_t[i][b]));
+                init_r = gl::kadd(init_r, gl::kscale(chi, w.init_val[e]));
+            }
+            neo_gpu_mem_oracle *ro = nullptr, *wo = nullptr, *bo = nullptr;
+            if ((rc = assemble(sh, C, twist_read_ids(w)))) return rc;
+            if ((rc = neo_gpu_mem_oracle_create_device(ctx, NEO_MEM_TWIST_READ, ell_n, (const uint64_t*)r_cycle.data(),
+                                                       w.ea, (const uint64_t*)r_addr_t[i].data(), (const uint64_t*)&init_r,
+                                                       4 + 2 * w.ea, (const uint64_t*)sh->d_asm.p, nullptr, nullptr, &ro)))
+                return rc;
+            os.mem.push_back(ro);
+            if ((rc = assemble(sh, C, twist_write_ids(w)))) return rc;
+            if ((rc = neo_gpu_mem_oracle_create_device(ctx, NEO_MEM_TWIST_WRITE, ell_n, (const uint64_t*)r_cycle.data(),
+                                                       w.ea, (const uint64_t*)r_addr_t[i].data(), (const uint64_t*)&init_r,
+                                                       3 + w.ea, (const uint64_t*)sh->d_asm.p, nullptr, nullptr, &wo)))
+                return rc;
+            os.mem.push_back(wo);
+            // bitness over [ra bits, wa bits, has_read, has_write] (adjacent columns)
+            auto bw = bitness_weights(r_cycle[0], 2 * w.ea + 2, 0x5457495354ULL + i);
+            if ((rc = neo_gpu_mem_oracle_create_device(ctx, NEO_MEM_BITNESS, ell_n, (const uint64_t*)r_cycle.data(), 0,
+                                                       nullptr, nullptr, 2 * w.ea + 2, (const uint64_t*)(C + (size_t)w.col0 * L),
+                                                       (const uint64_t*)bw.data(), nullptr, &bo)))
+                return rc;
+            os.mem.push_back(bo);
+            Claim cr, cw, cb;
+            cr.label = "twist/read_check"; cr.deg = 3 + w.ea; cr.sum = twist_read[i]; cr.mem = ro;
+            cw.label = "twist/write_check"; cw.deg = 3 + w.ea; cw.sum = twist_write[i]; cw.mem = wo;
+            cb.label = "twist/bitness"; cb.deg = 3; cb.dyn = false; cb.sum = gl::kzero(); cb.mem = bo;
+            claims.push_back(cr);
+            claims.push_back(cw);
+            claims.push_back(cb);
+        }
+        mem_ms += ms_since(t_mem);
     }
-    tr.append_message("sc/domain_end", "shard/batched_time");
-    tr.append_message("sc/inst_idx_end", bidx.data(), 8);
+    // ---- bind_batched_dynamic_claims (memory_sidecar/transcript.rs:37-63) ----
+    {
+        auto bl = le64(claims.size());
+        tr.append_message("batched/dynamic_bind/len", bl.data(), 8);
+        for (size_t i = 0; i < claims.size(); i++) {
+            auto bi = le64(i), bd = le64(claims[i].deg);
+            tr.append_message("batched/dynamic_bind/claim_label", claims[i].label);
+            tr.append_message("batched/dynamic_bind/claim_idx", bi.data(), 8);
+            tr.append_message("batched/dynamic_bind/degree_bound", bd.data(), 8);
+            uint8_t dy = claims[i].dyn ? 1 : 0;
+            tr.append_message("batched/dynamic_bind/is_dynamic", &dy, 1);
+            if (claims[i].dyn) absorb_k(tr, "batched/dynamic_bind/claimed_sum", claims[i].sum);
+        }
+    }
+    // ---- batched time sum-check (route_a_time.rs:28-152) ----
+    std::vector<K> r_time, finals;
+    if ((rc = run_batched_ds(sh, "shard/batched_time", idx, claims, ell_n, r_time, finals, P))) return rc;
+    K running = finals[0];
     sh->stats[4] = ms_since(t_ph);
     t_ph = hclock::now();
     // ---- Ajtai rounds: run_sumcheck_prover_ds("ccs/ajtai") ----
+    auto bidx = le64(idx);
+    std::vector<K> xs(d_sc + 1), ys(d_sc + 1), co;
+    for (uint32_t i = 0; i <= d_sc; i++) xs[i] = gl::kfq(i);
     tr.append_message("sc/domain", "ccs/ajtai");
     tr.append_message("sc/inst_idx", bidx.data(), 8);
     absorb_k(tr, "sc/claimed_sum", running);
     for (uint32_t rd = 0; rd < ell_d; rd++) {
         if ((rc = neo_gpu_ccs_oracle_evals(orc, (const uint64_t*)xs.data(), d_sc + 1, (uint64_t*)ys.data()))) return rc;
-        K s01 = gl::kadd(ys[0], ys[1]);
-        if (s01.re != running.re || s01.im != running.im)
+        if (!keq(gl::kadd(ys[0], ys[1]), running))
             return ctx->fail(NEO_ERR_INVARIANT, "Ajtai sum-check: p(0)+p(1) != running sum");
         interpolate(xs, ys, co);
         for (auto& c : co) absorb_k(tr, "sumcheck/round/coeff", c);
@@ -536,20 +1254,24 @@ static int fold_step_impl(neo_gpu_shard* sh, const uint64_t* z_host, const uint6
         K r = gl::kmk(c0, c1);
         running = poly_eval(co, r);
         if ((rc = neo_gpu_ccs_oracle_fold(orc, (const uint64_t*)&r))) return rc;
-        for (auto& c : co) { P.push_back(c.re); P.push_back(c.im); }
+        for (auto& c : co) push_k(P, c);
     }
     tr.append_message("sc/domain_end", "ccs/ajtai");
     tr.append_message("sc/inst_idx_end", bidx.data(), 8);
-    P.push_back(running.re);
-    P.push_back(running.im);
+    push_k(P, running);
     uint8_t fold_digest[32];
     tr.digest32(fold_digest);
 
     sh->stats[5] = ms_since(t_ph);
     t_ph = hclock::now();
-    // ---- ME outputs (oracle.rs:1955-2072) ----
+    // ---- ME outputs (oracle.rs:1955-2072) + bus openings at r_time (cpu_bus.rs:195-320) ----
     std::vector<K> y_eval((size_t)k * t * NEO_D), y_sc((size_t)k * t);
     if ((rc = neo_gpu_ccs_oracle_me_outputs(orc, (uint64_t*)y_eval.data(), (uint64_t*)y_sc.data()))) return rc;
+    std::vector<K> by, bsc;
+    if (has_mem) {
+        if ((rc = upload_point(sh, r_time))) return rc;
+        if ((rc = bus_openings(sh, sh->Zall.p, k, by, bsc))) return rc;
+    }
     std::vector<MeInst> outs(k);
     for (uint32_t i = 0; i < k; i++) {
         MeInst& o = outs[i];
@@ -558,153 +1280,166 @@ static int fold_step_impl(neo_gpu_shard* sh, const uint64_t* z_host, const uint6
         o.X = src.X;
         o.m_in = src.m_in;
         o.r = r_time;
-        o.y.assign((size_t)t * d_pad, gl::kzero());
-        for (uint32_t j = 0; j < t; j++)
+        o.y.assign((size_t)(t + nb) * d_pad, gl::kzero());
+        o.ysc.assign(t + nb, gl::kzero());
+        for (uint32_t j = 0; j < t; j++) {
             for (int rho = 0; rho < NEO_D; rho++) o.y[j * d_pad + rho] = y_eval[((size_t)i * t + j) * NEO_D + rho];
-        o.ysc.assign(y_sc.begin() + (size_t)i * t, y_sc.begin() + (size_t)(i + 1) * t);
+            o.ysc[j] = y_sc[(size_t)i * t + j];
+        }
+        for (uint32_t c = 0; c < nb; c++) {
+            for (int rho = 0; rho < NEO_D; rho++) o.y[(size_t)(t + c) * d_pad + rho] = by[((size_t)i * nb + c) * NEO_D + rho];
+            o.ysc[t + c] = bsc[(size_t)i * nb + c];
+        }
         memcpy(o.digest, fold_digest, 32);
     }
-    for (auto& v : y_eval) { P.push_back(v.re); P.push_back(v.im); }
-    for (auto& v : y_sc) { P.push_back(v.re); P.push_back(v.im); }
-
+    for (auto& v : y_eval) push_k(P, v);
+    for (auto& v : y_sc) push_k(P, v);
+    for (uint32_t i = 0; i < k && nb; i++) {
+        for (uint32_t c = 0; c < nb; c++)
+            for (int rho = 0; rho < NEO_D; rho++) push_k(P, outs[i].y[(size_t)(t + c) * d_pad + rho]);
+        for (uint32_t c = 0; c < nb; c++) push_k(P, outs[i].ysc[t + c]);
+    }
     sh->stats[6] = ms_since(t_ph);
     t_ph = hclock::now();
-    // ---- Pi_RLC: bind_rlc_inputs (shard.rs:1125-1168) + sample_rot_rhos_n (common.rs:467-573) ----
-    tr.append_message("fold/rlc_inputs/v1", "main");
-    uint64_t si = idx, mc = k;
-    tr.append_u64s("step_idx", &si, 1);
-    tr.append_u64s("me_count", &mc, 1);
-    for (auto& me : outs) {
-        tr.append_fields("c_data", me.c.data(), me.c.size());
-        uint64_t mi = me.m_in;
-        tr.append_u64s("m_in", &mi, 1);
-        tr.append_message("me_fold_digest", me.digest, 32);
-        for (auto& rl : me.r) absorb_k(tr, "r_limb", rl);
-        tr.append_fields("X", me.X.data(), me.X.size());
-        for (auto& ye : me.y) absorb_k(tr, "y_elem", ye);
-        for (auto& ys_ : me.ysc) absorb_k(tr, "y_scalar", ys_);
-        uint64_t zero = 0;
-        tr.append_u64s("c_step_coords_len", &zero, 1);
-        tr.append_fields("c_step_coords", nullptr, 0);
-        tr.append_u64s("u_offset", &zero, 1);
-        tr.append_u64s("u_len", &zero, 1);
-    }
-    std::vector<int8_t> rhos((size_t)k * NEO_D);
-    static const int8_t A5[5] = {-2, -1, 0, 1, 2};
-    for (uint32_t i = 0; i < k; i++) {
-        auto bi = le64(i);
-        tr.append_message("rlc/rot/index", bi.data(), 8);
-        // draw_alphabet_vector (common.rs:432-465): 16-bit chunks of digest32, rejection >= 65535
-        const uint32_t bucket = (1u << 16) / 5 * 5;
-        uint64_t ctr = i;
-        size_t got = 0;
-        while (got < NEO_D) {
-            auto bc = le64(ctr);
-            tr.append_message("rlc/rot/chunk", bc.data(), 8);
-            uint8_t dig[32];
-            tr.digest32(dig);
-            for (int w = 0; w < 16 && got < NEO_D; w++) {
-                uint32_t xv = (uint32_t)dig[2 * w] | ((uint32_t)dig[2 * w + 1] << 8);
-                if (xv < bucket) rhos[(size_t)i * NEO_D + got++] = A5[xv % 5];
-            }
-            ctr++;
-        }
-    }
-    for (auto v : rhos) P.push_back(gl::from_i64(v));
-    // Z_mix = sum rho_i Z_i (count == 1: identity)
-    if ((rc = rlc_mix_device(ctx, rhos.data(), sh->Zall.p, k, m, sh->d_mix.p, sh->d_rot.p))) return rc;
-    // parent commitment and y: rot mixes of the k commitments / y vectors
-    {
-        std::vector<uint64_t> cv((size_t)k * kappa * NEO_D);
-        for (uint32_t i = 0; i < k; i++) memcpy(&cv[(size_t)i * kappa * NEO_D], outs[i].c.data(), kappa * NEO_D * 8);
-        NEO_CK(ctx, cudaMemcpyAsync(sh->d_mixv.p, cv.data(), cv.size() * 8, cudaMemcpyHostToDevice, ctx->stream));
-        rot_mix_kernel<<<kappa, 64, 0, ctx->stream>>>(sh->d_rot.p, k, sh->d_mixv.p, kappa, 1, sh->d_mixo.p);
-        NEO_LAUNCHED(ctx);
-    }
-    std::vector<uint64_t> c_parent((size_t)kappa * NEO_D);
-    NEO_CK(ctx, cudaMemcpyAsync(c_parent.data(), sh->d_mixo.p, c_parent.size() * 8, cudaMemcpyDeviceToHost, ctx->stream));
-    std::vector<K> y_parent((size_t)t * NEO_D);
-    {
-        // y vectors as [k][t][54] K = stride-2 F_q
-        NEO_CK(ctx, cudaMemcpyAsync(sh->d_mixv.p, y_eval.data(), y_eval.size() * 16, cudaMemcpyHostToDevice, ctx->stream));
-        rot_mix_kernel<<<t * 2, 64, 0, ctx->stream>>>(sh->d_rot.p, k, sh->d_mixv.p, t, 2, sh->d_mixo.p);
-        NEO_LAUNCHED(ctx);
-        NEO_CK(ctx, cudaMemcpyAsync(y_parent.data(), sh->d_mixo.p, y_parent.size() * 16, cudaMemcpyDeviceToHost, ctx->stream));
-    }
-    P.insert(P.end(), c_parent.begin(), c_parent.end());
 
-    sh->stats[7] = ms_since(t_ph);
-    t_ph = hclock::now();
-    // ---- Pi_DEC: split into k_rho planes (slots 1..k_rho), commit, child claims ----
-    int8_t* planes = sh->Zall.p + (size_t)NEO_D * m;
-    if ((rc = split_b_device(ctx, sh->d_mix.p, (uint64_t)NEO_D * m, sh->k_rho, sh->b, planes, sh->d_flags.p))) return rc;
-    if ((rc = launch_commit(ctx, planes, sh->k_rho, m, sh->d_commits.p))) return rc;
+    // ---- finalize_route_a_memory_prover (memory.rs:1284-1670): Twist val-eval batch + CPU ME claims at r_val ----
+    std::vector<MeInst> val_claims;
+    std::vector<K> r_val;
+    uint8_t vdigest[32] = {0};
+    if (!sh->twist.empty()) {
+        auto t_mem = hclock::now();
+        const K* C = sh->d_cols.p;
+        std::vector<Claim> vcl;
+        std::vector<uint8_t> tags;
+        for (size_t i = 0; i < sh->twist.size(); i++) {
+            const TwistInst& w = *sh->twist[i];
+            neo_gpu_mem_oracle *lo = nullptr, *to = nullptr, *po = nullptr;
+            K lc, tc_, pc;
+            if ((rc = assemble(sh, C, twist_val_ids(w)))) return rc;
+            if ((rc = neo_gpu_mem_oracle_create_device(ctx, NEO_MEM_VAL_EVAL, ell_n, (const uint64_t*)r_time.data(), w.ea,
+                                                       (const uint64_t*)r_addr_t[i].data(), nullptr, 2 + w.ea,
+                                                       (const uint64_t*)sh->d_asm.p, nullptr, (uint64_t*)&lc, &lo)))
+                return rc;
+            os.mem.push_back(lo);
+            if ((rc = neo_gpu_mem_oracle_create_device(ctx, NEO_MEM_TOTAL_INC, ell_n, nullptr, w.ea,
+                                                       (const uint64_t*)r_addr_t[i].data(), nullptr, 2 + w.ea,
+                                                       (const uint64_t*)sh->d_asm.p, nullptr, (uint64_t*)&tc_, &to)))
+                return rc;
+            os.mem.push_back(to);
+            Claim c1, c2;
+            c1.label = "twist/val_eval_lt"; c1.deg = w.ea + 3; c1.sum = lc; c1.mem = lo;
+            c2.label = "twist/val_eval_total"; c2.deg = w.ea + 2; c2.sum = tc_; c2.mem = to;
+            vcl.push_back(c1); tags.push_back(0);
+            vcl.push_back(c2); tags.push_back(1);
+            if (sh->has_prev) {
+                if ((rc = assemble(sh, sh->d_prev_cols.p, twist_val_ids(w)))) return rc;
+                if ((rc = neo_gpu_mem_oracle_create_device(ctx, NEO_MEM_TOTAL_INC, ell_n, nullptr, w.ea,
+                                                           (const uint64_t*)r_addr_t[i].data(), nullptr, 2 + w.ea,
+                                                           (const uint64_t*)sh->d_asm.p, nullptr, (uint64_t*)&pc, &po)))
+                    return rc;
+                os.mem.push_back(po);
+                Claim c3;
+                c3.label = "twist/rollover_prev_total"; c3.deg = w.ea + 2; c3.sum = pc; c3.mem = po;
+                vcl.push_back(c3); tags.push_back(2);
+            }
+        }
+        auto bn = le64(sh->twist.size());
+        tr.append_message("twist/val_eval/batch_start", bn.data(), 8);
+        tr.append_message("twist/val_eval/step_idx", bidx.data(), 8);
+        // bind_twist_val_eval_claim_sums (memory_sidecar/transcript.rs:28-35)
+        auto bl = le64(vcl.size());
+        tr.append_message("twist/val_eval/claimed_sums_len", bl.data(), 8);
+        for (size_t i = 0; i < vcl.size(); i++) {
+            auto bi = le64(i);
+            tr.append_message("twist/val_eval/claim_idx", bi.data(), 8);
+            tr.append_message("twist/val_eval/claim_kind", &tags[i], 1);
+            absorb_k(tr, "twist/val_eval/claimed_sum", vcl[i].sum);
+            push_k(P, vcl[i].sum);
+        }
+        std::vector<K> fin;
+        if ((rc = run_batched_ds(sh, "twist/val_eval_batch", idx, vcl, ell_n, r_val, fin, P))) return rc;
+        tr.append_message("twist/val_eval/batch_done", nullptr, 0);
+        for (auto& r : r_val) push_k(P, r);
+        // emit_me_claims_for_mats (neo-memory/src/ts_common.rs:100-258): fold digest of the fork
+        {
+            neo::Transcript fork = tr;
+            fork.append_message("fork", "cpu_bus/me_digest_val");
+            fork.digest32(vdigest);
+        }
+        // witnesses: this step's MCS digits (and the previous step's) in valwit slots 0 (and 1)
+        NEO_CK(ctx, cudaMemcpyAsync(sh->valwit.p, sh->Zall.p, (size_t)NEO_D * m, cudaMemcpyDeviceToDevice, ctx->stream));
+        const uint32_t nv = sh->has_prev ? 2 : 1;
+        if ((rc = upload_point(sh, r_val))) return rc;
+        if ((rc = launch_chi_table(ctx, sh->d_r.p, ell_n, sh->d_chi.p))) return rc;
+        if ((rc = launch_me_y(ctx, sh->ccs, sh->valwit.p, nv, m, sh->d_chi.p, ell_n, sh->b, sh->d_vj.p, sh->d_yv.p,
+                              sh->d_yvsc.p)))
+            return rc;
+        std::vector<K> yv((size_t)nv * t * NEO_D), yvsc((size_t)nv * t);
+        NEO_CK(ctx, cudaMemcpyAsync(yv.data(), sh->d_yv.p, yv.size() * sizeof(K), cudaMemcpyDeviceToHost, ctx->stream));
+        NEO_CK(ctx, cudaMemcpyAsync(yvsc.data(), sh->d_yvsc.p, yvsc.size() * sizeof(K), cudaMemcpyDeviceToHost, ctx->stream));
+        NEO_CK(ctx, cudaStreamSynchronize(ctx->stream));
+        std::vector<K> vby, vbsc;
+        if ((rc = bus_openings(sh, sh->valwit.p, nv, vby, vbsc))) return rc;
+        for (uint32_t v = 0; v < nv; v++) {
+            MeInst me;
+            me.c = v == 0 ? mcs.c : sh->prev_c;
+            me.X = v == 0 ? mcs.X : sh->prev_X;
+            me.m_in = sh->m_in;
+            me.r = r_val;
+            me.y.assign((size_t)(t + nb) * d_pad, gl::kzero());
+            me.ysc.assign(t + nb, gl::kzero());
+            for (uint32_t j = 0; j < t; j++) {
+                for (int rho = 0; rho < NEO_D; rho++) me.y[j * d_pad + rho] = yv[((size_t)v * t + j) * NEO_D + rho];
+                me.ysc[j] = yvsc[(size_t)v * t + j];
+            }
+            for (uint32_t c = 0; c < nb; c++) {
+                for (int rho = 0; rho < NEO_D; rho++) me.y[(size_t)(t + c) * d_pad + rho] = vby[((size_t)v * nb + c) * NEO_D + rho];
+                me.ysc[t + c] = vbsc[(size_t)v * nb + c];
+            }
+            memcpy(me.digest, vdigest, 32);
+            for (uint32_t j = 0; j < t + nb; j++)
+                for (int rho = 0; rho < NEO_D; rho++) push_k(P, me.y[(size_t)j * d_pad + rho]);
+            for (auto& s : me.ysc) push_k(P, s);
+            val_claims.push_back(std::move(me));
+        }
+        mem_ms += ms_since(t_mem);
+    }
+
+    // ---- Pi_RLC + Pi_DEC, main lane (children into Zall slots 1..k_rho) ----
     const K* vj = nullptr;
     if ((rc = ccs_oracle_dev_vj(orc, &vj))) return rc;
-    child_y_kernel<<<sh->k_rho * NEO_D, 256, 0, ctx->stream>>>(planes, m, t, vj, sh->d_ychild.p);
-    NEO_LAUNCHED(ctx);
-    uint32_t flags[2];
-    std::vector<uint64_t> cc((size_t)sh->k_rho * kappa * NEO_D);
-    std::vector<K> yc((size_t)sh->k_rho * t * NEO_D);
-    std::vector<int8_t> Xc((size_t)sh->k_rho * NEO_D * sh->m_in);
-    NEO_CK(ctx, cudaMemcpyAsync(flags, sh->d_flags.p, 8, cudaMemcpyDeviceToHost, ctx->stream));
-    NEO_CK(ctx, cudaMemcpyAsync(cc.data(), sh->d_commits.p, cc.size() * 8, cudaMemcpyDeviceToHost, ctx->stream));
-    NEO_CK(ctx, cudaMemcpyAsync(yc.data(), sh->d_ychild.p, yc.size() * 16, cudaMemcpyDeviceToHost, ctx->stream));
-    NEO_CK(ctx, cudaMemcpy2DAsync(Xc.data(), sh->m_in, planes, m, sh->m_in, (size_t)sh->k_rho * NEO_D,
-                                  cudaMemcpyDeviceToHost, ctx->stream));
-    NEO_CK(ctx, cudaStreamSynchronize(ctx->stream));
-    if ((rc = check_device_error(ctx))) return rc;
-    if (flags[0]) return ctx->fail(NEO_ERR_INVARIANT, "DEC split: Z_mix entry out of range for k_rho digits");
-    // DEC public checks (dec_children_with_commit_cached): c and y recompose in base b
-    {
-        std::vector<uint64_t> cs(c_parent.size(), 0);
-        uint64_t pw = 1;
-        for (uint32_t i = 0; i < sh->k_rho; i++) {
-            for (size_t q = 0; q < cs.size(); q++) cs[q] = gl::add(cs[q], gl::mul(cc[(size_t)i * kappa * NEO_D + q], pw));
-            pw = gl::mul(pw, sh->b);
-        }
-        if (cs != c_parent) return ctx->fail(NEO_ERR_INVARIANT, "DEC public check failed (c)");
-        std::vector<K> ysum(y_parent.size(), gl::kzero());
-        pw = 1;
-        for (uint32_t i = 0; i < sh->k_rho; i++) {
-            for (size_t q = 0; q < ysum.size(); q++) ysum[q] = gl::kadd(ysum[q], gl::kscale(yc[(size_t)i * t * NEO_D + q], pw));
-            pw = gl::mul(pw, sh->b);
-        }
-        for (size_t q = 0; q < ysum.size(); q++)
-            if (ysum[q].re != y_parent[q].re || ysum[q].im != y_parent[q].im)
-                return ctx->fail(NEO_ERR_INVARIANT, "DEC public check failed (y)");
+    std::vector<MeInst> children;
+    if ((rc = rlc_dec_lane(sh, "main", idx, outs, sh->Zall.p, sh->Zall.p + (size_t)NEO_D * m, r_time, vj, fold_digest,
+                           children, P)))
+        return rc;
+    sh->stats[7] = ms_since(t_ph);
+    t_ph = hclock::now();
+    // ---- val lane (shard.rs:2195-2252) ----
+    if (!val_claims.empty()) {
+        tr.append_message("fold/val_lane_start", bidx.data(), 8);
+        // v_j = M_j^T chi(r_val) is still in d_vj from the CPU ME claims
+        std::vector<MeInst> vch;
+        if ((rc = rlc_dec_lane(sh, "val", idx, val_claims, sh->valwit.p, sh->valplanes.p, r_val, sh->d_vj.p, vdigest, vch,
+                               P)))
+            return rc;
+        sh->val_obligations += vch.size();
     }
-    // new accumulator = children
-    std::vector<MeInst> children(sh->k_rho);
-    uint64_t pwb[NEO_D];
-    pwb[0] = 1;
-    for (int q = 1; q < NEO_D; q++) pwb[q] = gl::mul(pwb[q - 1], sh->b);
-    for (uint32_t i = 0; i < sh->k_rho; i++) {
-        MeInst& ch = children[i];
-        ch.c.assign(cc.begin() + (size_t)i * kappa * NEO_D, cc.begin() + (size_t)(i + 1) * kappa * NEO_D);
-        ch.X.resize((size_t)NEO_D * sh->m_in);
-        for (size_t q = 0; q < ch.X.size(); q++) ch.X[q] = gl::from_i64(Xc[(size_t)i * NEO_D * sh->m_in + q]);
-        ch.r = r_time;
-        ch.m_in = sh->m_in;
-        ch.y.assign((size_t)t * d_pad, gl::kzero());
-        ch.ysc.resize(t);
-        for (uint32_t j = 0; j < t; j++) {
-            K s = gl::kzero();
-            for (int rho = 0; rho < NEO_D; rho++) {
-                K v = yc[((size_t)i * t + j) * NEO_D + rho];
-                ch.y[j * d_pad + rho] = v;
-                s = gl::kadd(s, gl::kscale(v, pwb[rho]));
-            }
-            ch.ysc[j] = s;
-        }
-        memcpy(ch.digest, fold_digest, 32);
-        P.insert(P.end(), ch.c.begin(), ch.c.end());
-        for (uint32_t j = 0; j < t; j++)
-            for (int rho = 0; rho < NEO_D; rho++) { P.push_back(ch.y[j * d_pad + rho].re); P.push_back(ch.y[j * d_pad + rho].im); }
-    }
+    tr.append_message("fold/step_done", bidx.data(), 8);
     sh->acc.swap(children);
+    if (!sh->twist.empty()) {
+        // this step becomes the rollover source of the next one
+        NEO_CK(ctx, cudaMemcpyAsync(sh->valwit.p + (size_t)NEO_D * m, sh->valwit.p, (size_t)NEO_D * m,
+                                    cudaMemcpyDeviceToDevice, ctx->stream));
+        NEO_CK(ctx, cudaMemcpyAsync(sh->d_prev_cols.p, sh->d_cols.p, (size_t)nb * L * sizeof(K), cudaMemcpyDeviceToDevice,
+                                    ctx->stream));
+        NEO_CK(ctx, cudaStreamSynchronize(ctx->stream));
+        sh->prev_c = mcs.c;
+        sh->prev_X = mcs.X;
+        sh->has_prev = true;
+    }
     sh->step_idx++;
     sh->stats[8] = ms_since(t_ph);
+    sh->stats[10] = mem_ms;
     sh->stats[0] = ms_since(t_step);
     sh->stats[9] = (double)(tr.permutations() - perms0);
     return NEO_OK;
@@ -751,5 +1486,11 @@ extern "C" int neo_gpu_shard_ccs_digest(const neo_gpu_shard* sh, uint64_t* d4) {
 extern "C" int neo_gpu_shard_step_stats(const neo_gpu_shard* sh, double* out, uint32_t n) {
     if (!sh || !out) return NEO_ERR_ARG;
     for (uint32_t i = 0; i < n && i < 12; i++) out[i] = sh->stats[i];
+    return NEO_OK;
+}
+
+extern "C" int neo_gpu_shard_val_obligations(const neo_gpu_shard* sh, uint64_t* count) {
+    if (!sh || !count) return NEO_ERR_ARG;
+    *count = sh->val_obligations;
     return NEO_OK;
 }

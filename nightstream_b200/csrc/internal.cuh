@@ -141,4 +141,8 @@ int launch_commit_tc(neo_gpu_ctx* ctx, const PPEntry* pp, const int8_t* d_digits
 // reads and clears the device error word (synchronizes the stream)
 int check_device_error(neo_gpu_ctx* ctx);
 
+// AddressLookupOracle weight table and claimed sum from device columns (mem_oracle.cu)
+int addr_weights_device(neo_gpu_ctx* ctx, uint32_t ell, const gl::K* d_rcycle, uint32_t A, const gl::K* d_has,
+                        const gl::K* d_bits, const gl::K* d_table, uint64_t table_len, gl::K* d_w, gl::K* claim);
+
 inline unsigned ceil_div(uint64_t a, uint64_t b) { return (unsigned)((a + b - 1) / b); }

@@ -638,6 +638,37 @@ extern "C" int neo_gpu_mem_oracle_destroy(neo_gpu_mem_oracle* o) {
     return NEO_OK;
 }
 
+// AddressLookupOracle weights from device columns: d_rcycle (ell K), d_has
+// (2^ell K), d_bits (A columns of 2^ell K), d_table (table_len K).  Writes
+// d_w (2^A K) and the claimed sum to *claim (host); synchronizes the stream.
+int addr_weights_device(neo_gpu_ctx* ctx, uint32_t ell, const K* d_rcycle, uint32_t A, const K* d_has,
+                        const K* d_bits, const K* d_table, uint64_t table_len, K* d_w, K* claim) {
+    cudaStream_t S = ctx->stream;
+    const uint64_t L = 1ULL << ell, P = 1ULL << A;
+    DevBuf<K> chi, part, out1;
+    DevBuf<unsigned long long> acc;
+    NEO_CK(ctx, chi.alloc(L));
+    NEO_CK(ctx, acc.alloc(4 * P));
+    NEO_CK(ctx, cudaMemsetAsync(acc.p, 0, 4 * P * sizeof(unsigned long long), S));
+    int rc = launch_chi_table(ctx, d_rcycle, ell, chi.p);
+    if (rc) return rc;
+    addr_weights_kernel<<<ceil_div(L, 256), 256, 0, S>>>(chi.p, d_has, d_bits, A, L, acc.p, acc.p + 2 * P);
+    NEO_LAUNCHED(ctx);
+    addr_weights_finish_kernel<<<ceil_div(P, 256), 256, 0, S>>>(acc.p, acc.p + 2 * P, P, d_w);
+    NEO_LAUNCHED(ctx);
+    const uint64_t n = table_len < P ? table_len : P;
+    const uint32_t nb = 148;
+    NEO_CK(ctx, part.alloc(nb));
+    NEO_CK(ctx, out1.alloc(1));
+    dot_kernel<<<nb, 256, 0, S>>>(d_table, d_w, n, part.p);
+    NEO_LAUNCHED(ctx);
+    mem_reduce_kernel<<<1, 256, 0, S>>>(part.p, nb, out1.p);
+    NEO_LAUNCHED(ctx);
+    NEO_CK(ctx, cudaMemcpyAsync(claim, out1.p, sizeof(K), cudaMemcpyDeviceToHost, S));
+    NEO_CK(ctx, cudaStreamSynchronize(S));
+    return NEO_OK;
+}
+
 extern "C" int neo_gpu_addr_lookup_weights(neo_gpu_ctx* ctx, uint32_t ell, const uint64_t* r_cycle, uint32_t ell_addr,
                                            const uint64_t* has_lookup, const uint64_t* addr_bits,
                                            const uint64_t* table, uint64_t table_len, uint64_t* weights,
@@ -649,40 +680,22 @@ extern "C" int neo_gpu_addr_lookup_weights(neo_gpu_ctx* ctx, uint32_t ell, const
     cudaSetDevice(ctx->device);
     cudaStream_t S = ctx->stream;
     const uint64_t L = 1ULL << ell, P = 1ULL << ell_addr;
-    DevBuf<K> dr, chi, has, bits, w, tab, part;
-    DevBuf<unsigned long long> acc;
+    DevBuf<K> dr, has, bits, w, tab;
     NEO_CK(ctx, dr.alloc(ell ? ell : 1));
-    NEO_CK(ctx, chi.alloc(L));
     NEO_CK(ctx, has.alloc(L));
     NEO_CK(ctx, bits.alloc((size_t)L * (ell_addr ? ell_addr : 1)));
-    NEO_CK(ctx, acc.alloc(4 * P));
     NEO_CK(ctx, w.alloc(P));
+    NEO_CK(ctx, tab.alloc(table_len ? table_len : 1));
     if (ell) NEO_CK(ctx, cudaMemcpyAsync(dr.p, r_cycle, ell * sizeof(K), cudaMemcpyHostToDevice, S));
     NEO_CK(ctx, cudaMemcpyAsync(has.p, has_lookup, L * sizeof(K), cudaMemcpyHostToDevice, S));
     if (ell_addr) NEO_CK(ctx, cudaMemcpyAsync(bits.p, addr_bits, (size_t)L * ell_addr * sizeof(K), cudaMemcpyHostToDevice, S));
-    NEO_CK(ctx, cudaMemsetAsync(acc.p, 0, 4 * P * sizeof(unsigned long long), S));
-    int rc = launch_chi_table(ctx, dr.p, ell, chi.p);
+    if (table_len) NEO_CK(ctx, cudaMemcpyAsync(tab.p, table, table_len * sizeof(K), cudaMemcpyHostToDevice, S));
+    K cl;
+    int rc = addr_weights_device(ctx, ell, dr.p, ell_addr, has.p, bits.p, tab.p, table_len, w.p, &cl);
     if (rc) return rc;
-    addr_weights_kernel<<<ceil_div(L, 256), 256, 0, S>>>(chi.p, has.p, bits.p, ell_addr, L, acc.p, acc.p + 2 * P);
-    NEO_LAUNCHED(ctx);
-    addr_weights_finish_kernel<<<ceil_div(P, 256), 256, 0, S>>>(acc.p, acc.p + 2 * P, P, w.p);
-    NEO_LAUNCHED(ctx);
-    const uint64_t n = table_len < P ? table_len : P;
-    const uint32_t nb = 148;
-    NEO_CK(ctx, part.alloc(nb));
-    DevBuf<K> out1;
-    NEO_CK(ctx, out1.alloc(1));
-    if (n) {
-        NEO_CK(ctx, tab.alloc(n));
-        NEO_CK(ctx, cudaMemcpyAsync(tab.p, table, n * sizeof(K), cudaMemcpyHostToDevice, S));
-    }
-    dot_kernel<<<nb, 256, 0, S>>>(tab.p, w.p, n, part.p);
-    NEO_LAUNCHED(ctx);
-    mem_reduce_kernel<<<1, 256, 0, S>>>(part.p, nb, out1.p);
-    NEO_LAUNCHED(ctx);
-    NEO_CK(ctx, cudaMemcpyAsync(weights, w.p, P * sizeof(K), cudaMemcpyDeviceToHost, S));
-    NEO_CK(ctx, cudaMemcpyAsync(claim, out1.p, sizeof(K), cudaMemcpyDeviceToHost, S));
-    NEO_CK(ctx, cudaStreamSynchronize(S));
+    NEO_CK(ctx, cudaMemcpy(weights, w.p, P * sizeof(K), cudaMemcpyDeviceToHost));
+    claim[0] = cl.re;
+    claim[1] = cl.im;
     return NEO_OK;
 }
 

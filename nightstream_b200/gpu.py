@@ -48,6 +48,8 @@ SIGNATURES = {
     "neo_gpu_commit_noalloc": [P, ctypes.c_void_p, U32, U64, ctypes.c_void_p],
     "neo_gpu_shard_step_stats": [P, P, U32],
     "neo_gpu_shard_create": [P, P, U32, U32, ctypes.c_char_p, P],
+    "neo_gpu_shard_create_mem": [P, P, U32, U32, ctypes.c_char_p, P, P],
+    "neo_gpu_shard_val_obligations": [P, P],
     "neo_gpu_shard_fold_step": [P, P, P, U64, P],
     "neo_gpu_shard_fold_step_device": [P, ctypes.c_void_p, P],
     "neo_gpu_shard_transcript_state": [P, P],
@@ -391,15 +393,61 @@ def addr_lookup_weights(ctx: Context, r_cycle, has_lookup, addr_bits, table):
     return w, claim
 
 
+class MemInstance(ctypes.Structure):
+    _fields_ = [("ell_addr", U32), ("k", U64), ("d", U64), ("n_side", U64), ("ell", U64), ("table", P),
+                ("table_len", U64), ("n_init", U64), ("init_addr", P), ("init_val", P)]
+
+
+class MemDesc(ctypes.Structure):
+    _fields_ = [("steps", U64), ("n_shout", U32), ("shout", P), ("n_twist", U32), ("twist", P)]
+
+
+def _mem_desc(mem: dict) -> MemDesc:
+    keep = []
+
+    def inst(d, table=None, init=()):
+        mi = MemInstance()
+        mi.ell_addr, mi.k, mi.d, mi.n_side, mi.ell = d["ell_addr"], d["k"], d["d"], d["n_side"], d["ell"]
+        if table is not None:
+            t = _u64(table)
+            keep.append(t)
+            mi.table, mi.table_len = _p(t), t.shape[0]
+        if init:
+            a = np.array([x for x, _ in init], np.uint64)
+            v = np.array([y for _, y in init], np.uint64)
+            keep.extend([a, v])
+            mi.n_init, mi.init_addr, mi.init_val = len(init), _p(a), _p(v)
+        return mi
+
+    sh = mem.get("shout", [])
+    tw = mem.get("twist", [])
+    sa = (MemInstance * max(1, len(sh)))(*[inst(d, table=d["table"]) for d in sh])
+    ta = (MemInstance * max(1, len(tw)))(*[inst(d, init=d.get("init", ())) for d in tw])
+    md = MemDesc()
+    md.steps = mem["steps"]
+    md.n_shout, md.shout = len(sh), ctypes.cast(sa, ctypes.c_void_p).value
+    md.n_twist, md.twist = len(tw), ctypes.cast(ta, ctypes.c_void_p).value
+    md._keep = (keep, sa, ta)
+    return md
+
+
 class Shard:
     """Shard prover with a device-resident accumulator (neo_gpu_shard)."""
 
-    def __init__(self, ctx: Context, ccs, m_in: int = 1, k_rho: int = 12, app_label: bytes = b"neo/shard"):
+    def __init__(self, ctx: Context, ccs, m_in: int = 1, k_rho: int = 12, app_label: bytes = b"neo/shard",
+                 mem: dict = None):
+        """mem: None, or dict(steps, shout=[dict(ell_addr, k, d, n_side, ell, table)],
+        twist=[dict(ell_addr, k, d, n_side, ell, init=[(addr, value)])])."""
         self.ctx = ctx
         self._desc = ccs.desc()
         h = ctypes.c_void_p()
-        ctx.check(ctx.lib.neo_gpu_shard_create(ctx.h, ctypes.byref(self._desc), m_in, k_rho, app_label,
-                                               ctypes.byref(h)))
+        if mem and (mem.get("shout") or mem.get("twist")):
+            self._mem = _mem_desc(mem)
+            ctx.check(ctx.lib.neo_gpu_shard_create_mem(ctx.h, ctypes.byref(self._desc), m_in, k_rho, app_label,
+                                                       ctypes.byref(self._mem), ctypes.byref(h)))
+        else:
+            ctx.check(ctx.lib.neo_gpu_shard_create(ctx.h, ctypes.byref(self._desc), m_in, k_rho, app_label,
+                                                   ctypes.byref(h)))
         self.h = h
         self._cap = 0
 
@@ -418,13 +466,18 @@ class Shard:
         self.ctx.check(self.ctx.lib.neo_gpu_shard_fold_step_device(self.h, ctypes.c_void_p(d_z_ptr), ctypes.byref(n)))
         return n.value
 
-    STAT_NAMES = ["total", "witness", "bind", "ccs_build", "time_rounds", "ajtai_rounds", "me_outputs", "rlc",
-                  "dec", "transcript_perms"]
+    STAT_NAMES = ("total", "witness", "bind", "ccs_build", "time_rounds", "ajtai_rounds", "me_outputs",
+                  "rlc_dec", "val_lane", "transcript_perms", "memory_sidecar", "unused")
 
     def step_stats(self) -> dict:
         out = np.zeros(12, np.float64)
         self.ctx.check(self.ctx.lib.neo_gpu_shard_step_stats(self.h, _p(out), 12))
         return {k: float(v) for k, v in zip(self.STAT_NAMES, out)}
+
+    def val_obligations(self) -> int:
+        c = ctypes.c_uint64()
+        self.ctx.check(self.ctx.lib.neo_gpu_shard_val_obligations(self.h, ctypes.byref(c)))
+        return int(c.value)
 
     def transcript_state(self) -> np.ndarray:
         st = np.empty(8, np.uint64)

@@ -39,3 +39,42 @@ def test_fold_step_rejects_unsatisfied_witness(ctx):
         g.fold_step(bad)
     assert e.value.code == 3  # NEO_ERR_INVARIANT: sum-check p(0)+p(1) check
     g.close()
+
+
+@pytest.mark.parametrize("ell,steps,chunk,shout_ell,twist_ell", [(10, 3, 16, 6, 5), (12, 2, 64, 8, 6)])
+def test_memory_fold_steps_match_oracle(ctx, ell, steps, chunk, shout_ell, twist_ell):
+    """Fold steps with the shared-CPU-bus memory sidecar (one Shout table, one
+    Twist memory): every proof word (address pre-time rounds, the seven Route-A
+    time claims, bus openings, val-eval batch, both RLC/DEC lanes) and the
+    transcript state match the oracle, for the first step and with rollover."""
+    ccs, z, mem = synth.make_memory_workload(ell, 5, chunk, shout_ell, twist_ell)
+    pp = np.random.default_rng(ell + 1).integers(0, Q, size=(16, 1 << ell, 54), dtype=np.uint64)
+    ctx.pp_upload(pp)
+    g = gpu.Shard(ctx, ccs, m_in=1, k_rho=12, app_label=b"neo/test-mem", mem=mem)
+    o = OracleShard(ccs, pp, m_in=1, k_rho=12, app_label=b"neo/test-mem", mem=mem)
+    for s in range(steps):
+        pg = g.fold_step(z)
+        po = o.fold_step(z)
+        assert pg.shape == po.shape, f"step {s}: proof length {pg.shape} vs {po.shape}"
+        assert np.array_equal(pg, po), f"step {s}: first mismatch at word {int(np.argmax(pg != po))}"
+        assert np.array_equal(g.transcript_state(), o.tr.state()), f"step {s}: transcript state"
+    assert g.val_obligations() == 12 * steps
+    g.close()
+
+
+def test_memory_fold_rejects_bad_read(ctx):
+    """A read value that disagrees with memory breaks the Twist checks: the
+    prover stops with the invariant status instead of emitting a proof."""
+    ccs, z, mem = synth.make_memory_workload(10, 6, 16, 6, 5)
+    pp = np.random.default_rng(3).integers(0, Q, size=(16, 1 << 10, 54), dtype=np.uint64)
+    ctx.pp_upload(pp)
+    g = gpu.Shard(ctx, ccs, mem=mem)
+    bus_cols = (6 + 2) + (2 * 5 + 5)
+    base = (1 << 10) - bus_cols * 16
+    rv_col = 8 + 2 * 5 + 3
+    bad = z.copy()
+    bad[base + rv_col * 16 + 3] = (int(bad[base + rv_col * 16 + 3]) + 1) % Q
+    with pytest.raises(gpu.NeoGpuError) as e:
+        g.fold_step(bad)
+    assert e.value.code == 3
+    g.close()
