@@ -2,11 +2,18 @@
 """Shard fold-steps/sec of the Neo fold step on B200.
 
 One "step" is one steady-state fold step of a shard (k = 13: the step's MCS
-instance plus 12 carried DEC children): witness decomposition + MCS Ajtai
-commitment, Pi_CCS sum-check (ell_n batched-time rounds + 6 Ajtai rounds), ME
-outputs, Pi_RLC and Pi_DEC (12 child commitments and child ME claims), with the
-Poseidon2 Fiat-Shamir transcript in between, over a seeded synthetic R1CS of
-n = m = 2^16 constraints (3 nonzeros per row, uniform F_q coefficients).
+instance plus 12 carried DEC children).  Default workload (single shard with
+memory): a seeded synthetic R1CS of n = m = 2^16 constraints whose witness
+carries the shared CPU bus of 1024 trace steps (a 2^14-step trace folds in 16
+such steps) with one Twist memory of 2^12 cells (one read and one write per
+step, addresses 70 % stride-4 sequential / 30 % uniform, 32-bit values) and
+one Shout table of 2^16 uniform 32-bit entries (uniform lookups).  A step is
+witness decomposition + MCS Ajtai commitment, the Shout and Twist address
+pre-time sum-checks, the Pi_CCS sum-check (16 batched-time rounds over the CCS
+claim and the six Route-A memory claims + 6 Ajtai rounds), ME outputs with bus
+openings, the Twist val-eval batch and val-lane CPU ME claims, and Pi_RLC /
+Pi_DEC on both lanes (24 child commitments), with the Poseidon2 Fiat-Shamir
+transcript in between.  --workload main drops the memory sidecar.
 
 Usage: python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 Multi-GPU runs (torchrun) place one independent shard per rank (replicas):
@@ -38,6 +45,9 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--ell", type=int, default=16, help="log2 of the CCS size n = m")
+    ap.add_argument("--workload", default="memory", choices=["memory", "main"],
+                    help="memory: single shard with Twist + Shout on the shared CPU bus; main: no memory")
+    ap.add_argument("--chunk", type=int, default=1024, help="trace steps per fold step (memory workload)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--mode", default="plain", choices=["plain", "batched", "served"],
@@ -50,14 +60,41 @@ def parse():
     return ap.parse_args()
 
 
-def workload(ell, rank):
+MEM_TWIST_ELL, MEM_SHOUT_ELL = 12, 16
+
+
+def workload(args, rank):
+    """(ccs, z, pp, mem) of the benchmarked shard."""
     from nightstream_b200 import synth
-    ccs, z = synth.make_r1cs(ell, 1234 + rank)
+    ell = args.ell
     pp = np.random.default_rng(99 + rank).integers(0, Q, size=(16, 1 << ell, 54), dtype=np.uint64)
-    return ccs, z, pp
+    if args.workload == "memory":
+        ccs, z, mem = synth.make_memory_workload(ell, 1234 + rank, args.chunk, MEM_SHOUT_ELL, MEM_TWIST_ELL)
+        return ccs, z, pp, mem
+    ccs, z = synth.make_r1cs(ell, 1234 + rank)
+    return ccs, z, pp, None
 
 
-def config(ell):
+def config(args):
+    ell = args.ell
+    if args.workload == "memory":
+        bus_cols = (MEM_SHOUT_ELL + 2) + (2 * MEM_TWIST_ELL + 5)
+        return {
+            "workload": f"single shard with memory: steady-state fold step of an R1CS n=m=2^{ell} (k=13) carrying "
+                        f"the shared CPU bus of {args.chunk} trace steps per fold step; one Twist memory of "
+                        f"2^{MEM_TWIST_ELL} cells (1 read + 1 write per step, 70% stride-4 / 30% uniform "
+                        f"addresses, 32-bit values), one Shout table of 2^{MEM_SHOUT_ELL} uniform 32-bit entries "
+                        f"(uniform lookups); Route-A batched time claims + Twist val-eval + val lane",
+            "n": 1 << ell, "m": 1 << ell, "k": 13, "kappa": 16, "d": 54, "b": 2, "k_rho": 12,
+            "trace_steps_per_fold_step": args.chunk, "bus_cols": bus_cols,
+            "twist_cells": 1 << MEM_TWIST_ELL, "shout_table": 1 << MEM_SHOUT_ELL,
+            "sumcheck_rounds": f"{ell} time (7 claims) + 6 Ajtai + {MEM_SHOUT_ELL} Shout addr + "
+                               f"{MEM_TWIST_ELL} Twist addr + {ell} val-eval",
+            "commits_per_step": 25,
+            "l2": "inputs larger than L2 (PP limbs 453 MB at 2^16, read by every commit)",
+            "witness": "seeded synthetic R1CS witness with the bus tail; values in [0, 2^32) except Twist "
+                       "increments (field differences); the same witness each step",
+        }
     return {
         "workload": f"steady-state fold step, main lane (Pi_CCS + Pi_RLC + Pi_DEC), "
                     f"R1CS n=m=2^{ell}, k=13, no Twist/Shout",
@@ -209,17 +246,17 @@ def int8_peak_tops():
         return 2 * pk, f"2x measured bf16 (int8 GEMM unavailable: {type(ex).__name__})"
 
 
-def cpu_baseline(ell, ccs, z, pp):
+def cpu_baseline(args, ccs, z, pp, mem):
     """One oracle fold step (C restatement, OpenMP on all host cores) after step 0."""
     from oracle.fold import OracleShard
-    sh = OracleShard(ccs, pp, m_in=1, k_rho=12, app_label=b"neo/bench")
+    sh = OracleShard(ccs, pp, m_in=1, k_rho=12, app_label=b"neo/bench", mem=mem)
     sh.fold_step(z)  # step 0 (k = 1)
     t0 = time.perf_counter()
     sh.fold_step(z)
     dt = time.perf_counter() - t0
     return {"value": 1.0 / dt, "unit": UNIT, "cores": os.cpu_count(), "kind": "port",
-            "sample": f"one steady-state fold step (k=13) at n=m=2^{ell} on the C oracle "
-                      f"(OpenMP, {os.cpu_count()} threads): {dt:.2f} s"}
+            "sample": f"one steady-state fold step (k=13, {args.workload} workload) at n=m=2^{args.ell} on the C "
+                      f"oracle (OpenMP, {os.cpu_count()} threads): {dt:.2f} s"}
 
 
 def shard_mix(n_shards, lo, hi, seed):
@@ -329,8 +366,8 @@ def run_reference(args, rank, world):
     if rank != 0:
         return
     from oracle.fold import OracleShard
-    ccs, z, pp = workload(args.ell, 0)
-    sh = OracleShard(ccs, pp, m_in=1, k_rho=12, app_label=b"neo/bench")
+    ccs, z, pp, mem = workload(args, 0)
+    sh = OracleShard(ccs, pp, m_in=1, k_rho=12, app_label=b"neo/bench", mem=mem)
     sh.fold_step(z)
     t0 = time.perf_counter()
     sh.fold_step(z)
@@ -348,9 +385,10 @@ def run_reference(args, rank, world):
     out = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": steps,
            "warmup": warm, "ms_per_step": dt / steps * 1e3, "higher_is_better": True, "scaling": "weak",
            "vs_baseline": None, "dtype": "u64 (F_q, K = F_q^2), int8 digits", "data": "synthetic",
-           "config": config(args.ell), "impl": "reference",
+           "config": config(args), "impl": "reference",
            "cpu_baseline": {"value": value, "unit": UNIT, "cores": os.cpu_count(), "kind": "port",
-                            "sample": f"{steps} steady-state fold steps at n=m=2^{args.ell} on the C restatement "
+                            "sample": f"{steps} steady-state fold steps ({args.workload} workload) at n=m=2^{args.ell} "
+                                      f"on the C restatement "
                                       f"(Rust reference not buildable here: no cargo/rustc)"},
            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(out), flush=True)
@@ -363,11 +401,11 @@ def run_ours(args, rank, world, local_rank):
     dist = None
     if world > 1:
         import torch.distributed as dist
-    ccs, z, pp = workload(args.ell, rank)
+    ccs, z, pp, mem = workload(args, rank)
     m = 1 << args.ell
     ctx = gpu.Context(local_rank)
     ctx.pp_upload(pp)
-    shard = gpu.Shard(ctx, ccs, m_in=1, k_rho=12, app_label=b"neo/bench")
+    shard = gpu.Shard(ctx, ccs, m_in=1, k_rho=12, app_label=b"neo/bench", mem=mem)
     stream = torch.cuda.ExternalStream(ctx.stream)
     zt = torch.from_numpy(z.view(np.int64).copy()).cuda()
     d_z = zt.data_ptr()
@@ -456,10 +494,10 @@ def run_ours(args, rank, world, local_rank):
         out = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
                "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
                "vs_baseline": None, "dtype": "u64 (F_q, K = F_q^2), int8 digits", "data": "synthetic",
-               "config": config(args.ell), "e2e": e2e, "gpu_launches": int(launches), "clocks": clk,
+               "config": config(args), "e2e": e2e, "gpu_launches": int(launches), "clocks": clk,
                "roofline": roofline, "roofline_commit": roofline_commit, "step_breakdown_ms": stats}
         if world == 1 and not args.no_cpu_baseline:
-            out["cpu_baseline"] = cpu_baseline(args.ell, ccs, z, pp)
+            out["cpu_baseline"] = cpu_baseline(args, ccs, z, pp, mem)
         if world == 1 and args.batch_in_plain:
             out["batched"] = batched_result(args)
         print(json.dumps(out), flush=True)
