@@ -259,12 +259,26 @@ def cpu_baseline(args, ccs, z, pp, mem):
                       f"oracle (OpenMP, {os.cpu_count()} threads): {dt:.2f} s"}
 
 
-def shard_mix(n_shards, lo, hi, seed):
-    """n_shards synthetic R1CS shards with log2(n) uniform in [lo, hi]."""
+BATCH_TWIST_ELL, BATCH_SHOUT_ELL = 10, 12
+
+
+def shard_mix(n_shards, lo, hi, seed, memory=True):
+    """n_shards synthetic shards with log2(n) uniform in [lo, hi]; with memory,
+    each carries a Twist memory of 2^10 cells and a 2^12-entry Shout table on
+    its shared CPU bus, min(1024, n/64) trace steps per fold step."""
     from nightstream_b200 import synth
     rng = np.random.default_rng(seed)
     ells = rng.integers(lo, hi + 1, size=n_shards)
-    return [(int(ell),) + synth.make_r1cs(int(ell), seed * 1000 + i) for i, ell in enumerate(ells)]
+    out = []
+    for i, ell in enumerate(ells):
+        ell = int(ell)
+        if memory:
+            chunk = min(1024, (1 << ell) // 64)
+            ccs, z, mem = synth.make_memory_workload(ell, seed * 1000 + i, chunk, BATCH_SHOUT_ELL, BATCH_TWIST_ELL)
+        else:
+            (ccs, z), mem = synth.make_r1cs(ell, seed * 1000 + i), None
+        out.append((ell, ccs, z, mem))
+    return out
 
 
 def upload_pps(ctx, ells):
@@ -278,7 +292,7 @@ def run_mix(mix, shards, steps, workers):
     from nightstream_b200 import gpu
     b = gpu.Batch(0, n_workers=workers)
     t0 = time.perf_counter()
-    ids = [b.submit(ccs, z, steps, app_label=b"neo/mix-%d" % i) for i, (ell, ccs, z) in enumerate(shards)]
+    ids = [b.submit(ccs, z, steps, app_label=b"neo/mix-%d" % i, mem=mem) for i, (ell, ccs, z, mem) in enumerate(shards)]
     b.wait_all(3600)
     dt = time.perf_counter() - t0
     infos = [b.job_info(j) for j in ids]
@@ -314,7 +328,8 @@ def run_batched(args):
            "warmup": 0, "ms_per_step": 1e3 / r["value"], "higher_is_better": True, "scaling": "weak",
            "vs_baseline": None, "dtype": "u64 (F_q, K = F_q^2), int8 digits", "data": "synthetic",
            "config": {"workload": f"batched: {r['shards']} shards, n=m=2^U with U uniform in [10,16], "
-                                  f"{r['steps_per_shard']} fold steps each (main lane, no Twist/Shout), "
+                                  f"{r['steps_per_shard']} fold steps each, each shard with a Twist memory of 2^10 cells and a "
+                                  f"2^12-entry Shout table (min(1024, n/64) trace steps per fold step), "
                                   f"{r['workers']} workers vs one worker",
                       "l2": "PP of all sizes (>1 GB) exceeds L2"},
            "batched": r, "gpu_launches": r["gpu_launches"],
@@ -339,11 +354,11 @@ def run_served(args):
         t0 = time.perf_counter()
         ids = []
         t_next = t0
-        for i, (ell, ccs, z) in enumerate(shards):
+        for i, (ell, ccs, z, mem) in enumerate(shards):
             t_next += gaps[i]
             while time.perf_counter() < t_next:
                 time.sleep(min(0.005, max(0.0, t_next - time.perf_counter())))
-            ids.append(b.submit(ccs, z, args.shard_steps, app_label=b"neo/req-%d" % i))
+            ids.append(b.submit(ccs, z, args.shard_steps, app_label=b"neo/req-%d" % i, mem=mem))
         b.wait_all(3600)
         dt = time.perf_counter() - t0
         infos = [b.job_info(j) for j in ids]
@@ -357,7 +372,8 @@ def run_served(args):
            "warmup": 0, "ms_per_step": 1e3 / best, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
            "dtype": "u64 (F_q, K = F_q^2), int8 digits", "data": "synthetic",
            "config": {"workload": f"served: {n_req} shard-prove requests, n=m=2^U, U uniform in [10,18], "
-                                  f"{args.shard_steps} fold steps each, Poisson arrivals, {workers} workers"},
+                                  f"{args.shard_steps} fold steps each, Twist 2^10 cells + Shout 2^12 table per shard, "
+                                  f"Poisson arrivals, {workers} workers"},
            "served": res}
     print(json.dumps(out), flush=True)
 

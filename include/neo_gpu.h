@@ -303,6 +303,11 @@ int neo_gpu_batch_set_reserve(neo_gpu_batch* b, uint64_t bytes);
 /* Inputs are copied; z has ccs->m words.  *job_id identifies the request. */
 int neo_gpu_batch_submit(neo_gpu_batch* b, const neo_ccs_desc* ccs, const uint64_t* z, uint32_t n_steps,
                          uint32_t m_in, uint32_t k_rho, const char* app_label, uint64_t* job_id);
+/* A request whose shard also proves the shared-CPU-bus memory sidecar
+ * (mem as for neo_gpu_shard_create_mem; copied). */
+int neo_gpu_batch_submit_mem(neo_gpu_batch* b, const neo_ccs_desc* ccs, const neo_mem_desc* mem, const uint64_t* z,
+                             uint32_t n_steps, uint32_t m_in, uint32_t k_rho, const char* app_label,
+                             uint64_t* job_id);
 /* Waits until every submitted request has finished (NEO_ERR_CUDA on timeout). */
 int neo_gpu_batch_wait_all(neo_gpu_batch* b, double timeout_ms);
 /* times3 = {submit->done ms, submit->admit ms, submit time since creation ms};

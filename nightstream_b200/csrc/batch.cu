@@ -21,6 +21,8 @@
 typedef struct neo_gpu_shard neo_gpu_shard;
 extern "C" int neo_gpu_shard_create(neo_gpu_ctx* ctx, const neo_ccs_desc* ccs, uint32_t m_in, uint32_t k_rho,
                                     const char* app_label, neo_gpu_shard** out);
+extern "C" int neo_gpu_shard_create_mem(neo_gpu_ctx* ctx, const neo_ccs_desc* ccs, uint32_t m_in, uint32_t k_rho,
+                                        const char* app_label, const neo_mem_desc* mem, neo_gpu_shard** out);
 extern "C" int neo_gpu_shard_fold_step(neo_gpu_shard* sh, const uint64_t* z, uint64_t* proof, uint64_t proof_cap,
                                        uint64_t* proof_len);
 extern "C" int neo_gpu_shard_transcript_state(const neo_gpu_shard* sh, uint64_t* st8);
@@ -56,9 +58,39 @@ struct CcsCopy {
     }
 };
 
+// Owned copy of a memory description (tables and initial memories).
+struct MemCopy {
+    neo_mem_desc d{};
+    std::vector<neo_mem_instance> shout, twist;
+    std::vector<std::vector<uint64_t>> bufs;
+    explicit MemCopy(const neo_mem_desc* s) {
+        d = *s;
+        auto own = [&](const uint64_t* p, uint64_t n) -> const uint64_t* {
+            if (!p || !n) return nullptr;
+            bufs.emplace_back(p, p + n);
+            return bufs.back().data();
+        };
+        bufs.reserve(3 * (s->n_shout + s->n_twist) + 1);
+        for (uint32_t i = 0; i < s->n_shout; i++) {
+            neo_mem_instance m = s->shout[i];
+            m.table = own(m.table, m.table_len);
+            shout.push_back(m);
+        }
+        for (uint32_t i = 0; i < s->n_twist; i++) {
+            neo_mem_instance m = s->twist[i];
+            m.init_addr = own(m.init_addr, m.n_init);
+            m.init_val = own(m.init_val, m.n_init);
+            twist.push_back(m);
+        }
+        d.shout = shout.data();
+        d.twist = twist.data();
+    }
+};
+
 struct Job {
     uint64_t id = 0;
     std::unique_ptr<CcsCopy> ccs;
+    std::unique_ptr<MemCopy> mem;
     std::vector<uint64_t> z;
     uint32_t n_steps = 0, m_in = 1, k_rho = 12;
     std::string label;
@@ -165,7 +197,10 @@ static void worker_main(neo_gpu_batch* b, size_t wi) {
         rr %= w.active.size();
         Job* j = w.active[rr];
         int rc = NEO_OK;
-        if (!j->shard) rc = neo_gpu_shard_create(w.ctx, &j->ccs->d, j->m_in, j->k_rho, j->label.c_str(), &j->shard);
+        if (!j->shard)
+            rc = j->mem ? neo_gpu_shard_create_mem(w.ctx, &j->ccs->d, j->m_in, j->k_rho, j->label.c_str(), &j->mem->d,
+                                                   &j->shard)
+                        : neo_gpu_shard_create(w.ctx, &j->ccs->d, j->m_in, j->k_rho, j->label.c_str(), &j->shard);
         if (rc == NEO_OK) {
             uint64_t len = 0;
             rc = neo_gpu_shard_fold_step(j->shard, j->z.data(), nullptr, 0, &len);
@@ -208,17 +243,25 @@ extern "C" int neo_gpu_batch_set_reserve(neo_gpu_batch* b, uint64_t bytes) {
     return NEO_OK;
 }
 
-extern "C" int neo_gpu_batch_submit(neo_gpu_batch* b, const neo_ccs_desc* ccs, const uint64_t* z, uint32_t n_steps,
-                                    uint32_t m_in, uint32_t k_rho, const char* app_label, uint64_t* job_id) {
+static int submit_impl(neo_gpu_batch* b, const neo_ccs_desc* ccs, const neo_mem_desc* mem, const uint64_t* z,
+                       uint32_t n_steps, uint32_t m_in, uint32_t k_rho, const char* app_label, uint64_t* job_id) {
     if (!b || !ccs || !z || !app_label || !job_id || n_steps == 0 || ccs->m == 0) return NEO_ERR_ARG;
     auto j = std::make_unique<Job>();
     j->ccs = std::make_unique<CcsCopy>(ccs);
+    if (mem && (mem->n_shout || mem->n_twist)) j->mem = std::make_unique<MemCopy>(mem);
     j->z.assign(z, z + ccs->m);
     j->n_steps = n_steps;
     j->m_in = m_in;
     j->k_rho = k_rho;
     j->label = app_label;
     j->footprint = shard_footprint(ccs->m, k_rho);
+    if (j->mem) {
+        // decoded bus columns (this and the previous step), oracle tables, val-lane planes
+        uint64_t cols = 0;
+        for (auto& s : j->mem->shout) cols += s.ell_addr + 2;
+        for (auto& t : j->mem->twist) cols += 2 * t.ell_addr + 5;
+        j->footprint += 8 * cols * ccs->n * 16 + (uint64_t)(k_rho + 2) * 54 * ccs->m + (64ull << 20);
+    }
     j->t_submit = bclock::now();
     std::lock_guard<std::mutex> lk(b->mu);
     j->id = b->jobs.size();
@@ -229,6 +272,17 @@ extern "C" int neo_gpu_batch_submit(neo_gpu_batch* b, const neo_ccs_desc* ccs, c
     admit_locked(b);
     b->cv_work.notify_all();
     return NEO_OK;
+}
+
+extern "C" int neo_gpu_batch_submit(neo_gpu_batch* b, const neo_ccs_desc* ccs, const uint64_t* z, uint32_t n_steps,
+                                    uint32_t m_in, uint32_t k_rho, const char* app_label, uint64_t* job_id) {
+    return submit_impl(b, ccs, nullptr, z, n_steps, m_in, k_rho, app_label, job_id);
+}
+
+extern "C" int neo_gpu_batch_submit_mem(neo_gpu_batch* b, const neo_ccs_desc* ccs, const neo_mem_desc* mem,
+                                        const uint64_t* z, uint32_t n_steps, uint32_t m_in, uint32_t k_rho,
+                                        const char* app_label, uint64_t* job_id) {
+    return submit_impl(b, ccs, mem, z, n_steps, m_in, k_rho, app_label, job_id);
 }
 
 extern "C" int neo_gpu_batch_wait_all(neo_gpu_batch* b, double timeout_ms) {

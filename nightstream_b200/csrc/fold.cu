@@ -218,6 +218,9 @@ struct neo_gpu_shard {
     bool has_prev = false;
     std::vector<uint64_t> prev_c, prev_X;
     uint64_t val_obligations = 0;
+    std::vector<neo_gpu_mem_oracle*> mem_slots;  // memory oracles, rebuilt in place every step
+    std::vector<neo_gpu_twist_addr*> ta_slots;
+    AddrWs addr_ws;
 };
 
 using hclock = std::chrono::steady_clock;
@@ -450,6 +453,8 @@ extern "C" int neo_gpu_shard_destroy(neo_gpu_shard* sh) {
     cudaSetDevice(sh->ctx->device);
     cudaStreamSynchronize(sh->ctx->stream);
     if (sh->orc) neo_gpu_ccs_oracle_destroy(sh->orc);
+    for (auto* o : sh->mem_slots) neo_gpu_mem_oracle_destroy(o);
+    for (auto* o : sh->ta_slots) neo_gpu_twist_addr_destroy(o);
     delete sh;
     return NEO_OK;
 }
@@ -529,16 +534,6 @@ struct Claim {
         if (ccs) return neo_gpu_ccs_oracle_fold(ccs, (const uint64_t*)&r);
         if (mem) return neo_gpu_mem_oracle_fold(mem, (const uint64_t*)&r);
         return neo_gpu_twist_addr_fold(ta, (const uint64_t*)&r);
-    }
-};
-
-// Owns the memory oracles of one step.
-struct OracleSet {
-    std::vector<neo_gpu_mem_oracle*> mem;
-    std::vector<neo_gpu_twist_addr*> ta;
-    ~OracleSet() {
-        for (auto* o : mem) neo_gpu_mem_oracle_destroy(o);
-        for (auto* o : ta) neo_gpu_twist_addr_destroy(o);
     }
 };
 
@@ -1034,7 +1029,24 @@ static int fold_step_impl(neo_gpu_shard* sh, const uint64_t* z_host, const uint6
     sh->stats[3] = ms_since(t_ph);
     t_ph = hclock::now();
 
-    OracleSet os;
+    // memory oracles are rebuilt every step into the shard's slots (device buffers kept)
+    size_t mem_cur = 0, ta_cur = 0;
+    auto mb = [&](neo_gpu_mem_oracle** dst, int kind, uint32_t ell, const uint64_t* rp, uint32_t A, const uint64_t* ra,
+                  const uint64_t* init, uint32_t nc, const uint64_t* cols, const uint64_t* w, uint64_t* claim) -> int {
+        if (mem_cur == sh->mem_slots.size()) sh->mem_slots.push_back(nullptr);
+        neo_gpu_mem_oracle** sl = &sh->mem_slots[mem_cur++];
+        int r = mem_oracle_build_device(ctx, kind, ell, rp, A, ra, init, nc, cols, w, claim, sl);
+        *dst = *sl;
+        return r;
+    };
+    auto tb = [&](neo_gpu_twist_addr** dst, int kind, uint32_t ell, const uint64_t* rc_, uint32_t A, uint64_t n_init,
+                  const uint64_t* ia, const uint64_t* iv, const uint64_t* cols) -> int {
+        if (ta_cur == sh->ta_slots.size()) sh->ta_slots.push_back(nullptr);
+        neo_gpu_twist_addr** sl = &sh->ta_slots[ta_cur++];
+        int r = twist_addr_build_device(ctx, kind, ell, rc_, A, n_init, ia, iv, cols, sl);
+        *dst = *sl;
+        return r;
+    };
     std::vector<Claim> claims;
     {
         Claim c;
@@ -1063,7 +1075,9 @@ static int fold_step_impl(neo_gpu_shard* sh, const uint64_t* z_host, const uint6
                 const K* has = C + (size_t)(s.col0 + s.ea) * L;
                 // has_any_lookup: any nonzero gate in this step's bus column
                 std::vector<K> hg(sh->steps);
-                NEO_CK(ctx, cudaMemcpy(hg.data(), has + sh->m_in, sh->steps * sizeof(K), cudaMemcpyDeviceToHost));
+                NEO_CK(ctx, cudaMemcpyAsync(hg.data(), has + sh->m_in, sh->steps * sizeof(K), cudaMemcpyDeviceToHost,
+                                            ctx->stream));
+                NEO_CK(ctx, cudaStreamSynchronize(ctx->stream));
                 bool any = false;
                 for (auto& g : hg) any |= !gl::kiszero(g);
                 if (!any) {
@@ -1073,16 +1087,15 @@ static int fold_step_impl(neo_gpu_shard* sh, const uint64_t* z_host, const uint6
                 const uint64_t Pn = 1ULL << s.ea;
                 K cl;
                 if ((rc = addr_weights_device(ctx, ell_n, sh->d_r.p, s.ea, has, C + (size_t)s.col0 * L, s.d_table.p,
-                                              std::min<uint64_t>(s.table.size(), Pn), sh->d_w.p, &cl)))
+                                              std::min<uint64_t>(s.table.size(), Pn), sh->d_w.p, &cl, &sh->addr_ws)))
                     return rc;
                 // ProductRoundOracle over [table, weights] (twist_oracle.rs:1719-1722), degree 2
                 NEO_CK(ctx, cudaMemcpyAsync(sh->d_asm.p, s.d_table.p, Pn * sizeof(K), cudaMemcpyDeviceToDevice, ctx->stream));
                 NEO_CK(ctx, cudaMemcpyAsync(sh->d_asm.p + Pn, sh->d_w.p, Pn * sizeof(K), cudaMemcpyDeviceToDevice, ctx->stream));
                 neo_gpu_mem_oracle* po = nullptr;
-                if ((rc = neo_gpu_mem_oracle_create_device(ctx, NEO_MEM_PRODUCT, s.ea, nullptr, 0, nullptr, nullptr, 2,
-                                                           (const uint64_t*)sh->d_asm.p, nullptr, nullptr, &po)))
+                if ((rc = mb(&po, NEO_MEM_PRODUCT, s.ea, nullptr, 0, nullptr, nullptr, 2,
+                                                           (const uint64_t*)sh->d_asm.p, nullptr, nullptr)))
                     return rc;
-                os.mem.push_back(po);
                 Claim c;
                 c.label = "shout/addr_pre";
                 c.deg = 2;
@@ -1116,17 +1129,15 @@ static int fold_step_impl(neo_gpu_shard* sh, const uint64_t* z_host, const uint6
             for (size_t e = 0; e < w.init_val.size(); e++) { iv[2 * e] = w.init_val[e]; iv[2 * e + 1] = 0; }
             neo_gpu_twist_addr *ro = nullptr, *wo = nullptr;
             if ((rc = assemble(sh, C, twist_read_ids(w)))) return rc;
-            if ((rc = neo_gpu_twist_addr_create_device(ctx, 0, ell_n, (const uint64_t*)r_cycle.data(), w.ea,
+            if ((rc = tb(&ro, 0, ell_n, (const uint64_t*)r_cycle.data(), w.ea,
                                                        w.init_addr.size(), w.init_addr.data(), iv.data(),
-                                                       (const uint64_t*)sh->d_asm.p, &ro)))
+                                                       (const uint64_t*)sh->d_asm.p)))
                 return rc;
-            os.ta.push_back(ro);
             if ((rc = assemble(sh, C, twist_write_ids(w)))) return rc;
-            if ((rc = neo_gpu_twist_addr_create_device(ctx, 1, ell_n, (const uint64_t*)r_cycle.data(), w.ea,
+            if ((rc = tb(&wo, 1, ell_n, (const uint64_t*)r_cycle.data(), w.ea,
                                                        w.init_addr.size(), w.init_addr.data(), iv.data(),
-                                                       (const uint64_t*)sh->d_asm.p, &wo)))
+                                                       (const uint64_t*)sh->d_asm.p)))
                 return rc;
-            os.ta.push_back(wo);
             auto bi = le64(i);
             tr.append_message("twist/addr_pre_time/claim_idx", bi.data(), 8);
             std::vector<std::string> labels = {"twist/read_addr_pre", "twist/write_addr_pre"};
@@ -1148,26 +1159,23 @@ static int fold_step_impl(neo_gpu_shard* sh, const uint64_t* z_host, const uint6
             neo_gpu_mem_oracle *vo = nullptr, *ao = nullptr, *bo = nullptr;
             K vc, ac_, bc;
             // value: [has_lookup, val] are adjacent bus columns
-            if ((rc = neo_gpu_mem_oracle_create_device(ctx, NEO_MEM_SHOUT_VALUE, ell_n, (const uint64_t*)r_cycle.data(),
+            if ((rc = mb(&vo, NEO_MEM_SHOUT_VALUE, ell_n, (const uint64_t*)r_cycle.data(),
                                                        0, nullptr, nullptr, 2, (const uint64_t*)(C + (size_t)(s.col0 + s.ea) * L),
-                                                       nullptr, (uint64_t*)&vc, &vo)))
+                                                       nullptr, (uint64_t*)&vc)))
                 return rc;
-            os.mem.push_back(vo);
             std::vector<uint32_t> ids = {s.col0 + s.ea};
             for (uint32_t b = 0; b < s.ea; b++) ids.push_back(s.col0 + b);
             if ((rc = assemble(sh, C, ids))) return rc;
-            if ((rc = neo_gpu_mem_oracle_create_device(ctx, NEO_MEM_SHOUT_ADAPTER, ell_n, (const uint64_t*)r_cycle.data(),
+            if ((rc = mb(&ao, NEO_MEM_SHOUT_ADAPTER, ell_n, (const uint64_t*)r_cycle.data(),
                                                        s.ea, (const uint64_t*)r_addr_s.data(), nullptr, 1 + s.ea,
-                                                       (const uint64_t*)sh->d_asm.p, nullptr, (uint64_t*)&ac_, &ao)))
+                                                       (const uint64_t*)sh->d_asm.p, nullptr, (uint64_t*)&ac_)))
                 return rc;
-            os.mem.push_back(ao);
             // bitness over [addr_bits..., has_lookup] (adjacent columns)
             auto bw = bitness_weights(r_cycle[0], s.ea + 1, 0x53484F5554ULL + i);
-            if ((rc = neo_gpu_mem_oracle_create_device(ctx, NEO_MEM_BITNESS, ell_n, (const uint64_t*)r_cycle.data(), 0,
+            if ((rc = mb(&bo, NEO_MEM_BITNESS, ell_n, (const uint64_t*)r_cycle.data(), 0,
                                                        nullptr, nullptr, s.ea + 1, (const uint64_t*)(C + (size_t)s.col0 * L),
-                                                       (const uint64_t*)bw.data(), (uint64_t*)&bc, &bo)))
+                                                       (const uint64_t*)bw.data(), (uint64_t*)&bc)))
                 return rc;
-            os.mem.push_back(bo);
             Claim cv, ca, cb;
             cv.label = "shout/value"; cv.deg = 3; cv.sum = vc; cv.mem = vo;
             ca.label = "shout/adapter"; ca.deg = 2 + s.ea; ca.sum = ac_; ca.mem = ao;
@@ -1188,24 +1196,21 @@ static int fold_step_impl(neo_gpu_shard* sh, const uint64_t* z_host, const uint6
             }
             neo_gpu_mem_oracle *ro = nullptr, *wo = nullptr, *bo = nullptr;
             if ((rc = assemble(sh, C, twist_read_ids(w)))) return rc;
-            if ((rc = neo_gpu_mem_oracle_create_device(ctx, NEO_MEM_TWIST_READ, ell_n, (const uint64_t*)r_cycle.data(),
+            if ((rc = mb(&ro, NEO_MEM_TWIST_READ, ell_n, (const uint64_t*)r_cycle.data(),
                                                        w.ea, (const uint64_t*)r_addr_t[i].data(), (const uint64_t*)&init_r,
-                                                       4 + 2 * w.ea, (const uint64_t*)sh->d_asm.p, nullptr, nullptr, &ro)))
+                                                       4 + 2 * w.ea, (const uint64_t*)sh->d_asm.p, nullptr, nullptr)))
                 return rc;
-            os.mem.push_back(ro);
             if ((rc = assemble(sh, C, twist_write_ids(w)))) return rc;
-            if ((rc = neo_gpu_mem_oracle_create_device(ctx, NEO_MEM_TWIST_WRITE, ell_n, (const uint64_t*)r_cycle.data(),
+            if ((rc = mb(&wo, NEO_MEM_TWIST_WRITE, ell_n, (const uint64_t*)r_cycle.data(),
                                                        w.ea, (const uint64_t*)r_addr_t[i].data(), (const uint64_t*)&init_r,
-                                                       3 + w.ea, (const uint64_t*)sh->d_asm.p, nullptr, nullptr, &wo)))
+                                                       3 + w.ea, (const uint64_t*)sh->d_asm.p, nullptr, nullptr)))
                 return rc;
-            os.mem.push_back(wo);
             // bitness over [ra bits, wa bits, has_read, has_write] (adjacent columns)
             auto bw = bitness_weights(r_cycle[0], 2 * w.ea + 2, 0x5457495354ULL + i);
-            if ((rc = neo_gpu_mem_oracle_create_device(ctx, NEO_MEM_BITNESS, ell_n, (const uint64_t*)r_cycle.data(), 0,
+            if ((rc = mb(&bo, NEO_MEM_BITNESS, ell_n, (const uint64_t*)r_cycle.data(), 0,
                                                        nullptr, nullptr, 2 * w.ea + 2, (const uint64_t*)(C + (size_t)w.col0 * L),
-                                                       (const uint64_t*)bw.data(), nullptr, &bo)))
+                                                       (const uint64_t*)bw.data(), nullptr)))
                 return rc;
-            os.mem.push_back(bo);
             Claim cr, cw, cb;
             cr.label = "twist/read_check"; cr.deg = 3 + w.ea; cr.sum = twist_read[i]; cr.mem = ro;
             cw.label = "twist/write_check"; cw.deg = 3 + w.ea; cw.sum = twist_write[i]; cw.mem = wo;
@@ -1316,16 +1321,14 @@ static int fold_step_impl(neo_gpu_shard* sh, const uint64_t* z_host, const uint6
             neo_gpu_mem_oracle *lo = nullptr, *to = nullptr, *po = nullptr;
             K lc, tc_, pc;
             if ((rc = assemble(sh, C, twist_val_ids(w)))) return rc;
-            if ((rc = neo_gpu_mem_oracle_create_device(ctx, NEO_MEM_VAL_EVAL, ell_n, (const uint64_t*)r_time.data(), w.ea,
+            if ((rc = mb(&lo, NEO_MEM_VAL_EVAL, ell_n, (const uint64_t*)r_time.data(), w.ea,
                                                        (const uint64_t*)r_addr_t[i].data(), nullptr, 2 + w.ea,
-                                                       (const uint64_t*)sh->d_asm.p, nullptr, (uint64_t*)&lc, &lo)))
+                                                       (const uint64_t*)sh->d_asm.p, nullptr, (uint64_t*)&lc)))
                 return rc;
-            os.mem.push_back(lo);
-            if ((rc = neo_gpu_mem_oracle_create_device(ctx, NEO_MEM_TOTAL_INC, ell_n, nullptr, w.ea,
+            if ((rc = mb(&to, NEO_MEM_TOTAL_INC, ell_n, nullptr, w.ea,
                                                        (const uint64_t*)r_addr_t[i].data(), nullptr, 2 + w.ea,
-                                                       (const uint64_t*)sh->d_asm.p, nullptr, (uint64_t*)&tc_, &to)))
+                                                       (const uint64_t*)sh->d_asm.p, nullptr, (uint64_t*)&tc_)))
                 return rc;
-            os.mem.push_back(to);
             Claim c1, c2;
             c1.label = "twist/val_eval_lt"; c1.deg = w.ea + 3; c1.sum = lc; c1.mem = lo;
             c2.label = "twist/val_eval_total"; c2.deg = w.ea + 2; c2.sum = tc_; c2.mem = to;
@@ -1333,11 +1336,10 @@ static int fold_step_impl(neo_gpu_shard* sh, const uint64_t* z_host, const uint6
             vcl.push_back(c2); tags.push_back(1);
             if (sh->has_prev) {
                 if ((rc = assemble(sh, sh->d_prev_cols.p, twist_val_ids(w)))) return rc;
-                if ((rc = neo_gpu_mem_oracle_create_device(ctx, NEO_MEM_TOTAL_INC, ell_n, nullptr, w.ea,
+                if ((rc = mb(&po, NEO_MEM_TOTAL_INC, ell_n, nullptr, w.ea,
                                                            (const uint64_t*)r_addr_t[i].data(), nullptr, 2 + w.ea,
-                                                           (const uint64_t*)sh->d_asm.p, nullptr, (uint64_t*)&pc, &po)))
+                                                           (const uint64_t*)sh->d_asm.p, nullptr, (uint64_t*)&pc)))
                     return rc;
-                os.mem.push_back(po);
                 Claim c3;
                 c3.label = "twist/rollover_prev_total"; c3.deg = w.ea + 2; c3.sum = pc; c3.mem = po;
                 vcl.push_back(c3); tags.push_back(2);

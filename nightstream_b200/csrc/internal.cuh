@@ -141,8 +141,22 @@ int launch_commit_tc(neo_gpu_ctx* ctx, const PPEntry* pp, const int8_t* d_digits
 // reads and clears the device error word (synchronizes the stream)
 int check_device_error(neo_gpu_ctx* ctx);
 
-// AddressLookupOracle weight table and claimed sum from device columns (mem_oracle.cu)
+// AddressLookupOracle weight table and claimed sum from device columns (mem_oracle.cu);
+// ws (may be null) keeps the temporaries across calls
+struct AddrWs {
+    DevBuf<gl::K> chi, part, out1;
+    DevBuf<unsigned long long> acc;
+};
 int addr_weights_device(neo_gpu_ctx* ctx, uint32_t ell, const gl::K* d_rcycle, uint32_t A, const gl::K* d_has,
-                        const gl::K* d_bits, const gl::K* d_table, uint64_t table_len, gl::K* d_w, gl::K* claim);
+                        const gl::K* d_bits, const gl::K* d_table, uint64_t table_len, gl::K* d_w, gl::K* claim,
+                        AddrWs* ws);
+// Memory-oracle builds that reuse the object in *slot (mem_oracle.cu)
+int mem_oracle_build_device(neo_gpu_ctx* ctx, int kind, uint32_t ell, const uint64_t* r_point, uint32_t ell_addr,
+                            const uint64_t* r_addr, const uint64_t* init_at_r_addr, uint32_t n_cols,
+                            const uint64_t* d_cols, const uint64_t* weights, uint64_t* claim,
+                            neo_gpu_mem_oracle** slot);
+int twist_addr_build_device(neo_gpu_ctx* ctx, int kind, uint32_t ell, const uint64_t* r_cycle, uint32_t ell_addr,
+                            uint64_t n_init, const uint64_t* init_addr, const uint64_t* init_val,
+                            const uint64_t* d_cols, neo_gpu_twist_addr** slot);
 
 inline unsigned ceil_div(uint64_t a, uint64_t b) { return (unsigned)((a + b - 1) / b); }

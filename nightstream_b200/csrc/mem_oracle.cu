@@ -318,6 +318,7 @@ struct neo_gpu_mem_oracle {
     DevBuf<K> w;          // bitness weights
     std::vector<K> hw;    // host copy of the weights
     DevBuf<K> partials, vals;
+    DevBuf<K> dpt, dra, tmp, sums;  // build workspace, kept for reuse
     std::vector<K> hvals;
     K claim{};
 };
@@ -432,9 +433,9 @@ K lagrange_at(const std::vector<K>& v, K x) {
 
 int mem_create(neo_gpu_ctx* ctx, int kind, uint32_t ell, const uint64_t* r_point, uint32_t A, const uint64_t* r_addr,
                const uint64_t* init, uint32_t n_cols, const uint64_t* cols, bool cols_on_device,
-               const uint64_t* weights, uint64_t* claim_out, neo_gpu_mem_oracle** out) {
+               const uint64_t* weights, uint64_t* claim_out, neo_gpu_mem_oracle** out, bool reuse = false) {
     if (!ctx || !out) return NEO_ERR_ARG;
-    *out = nullptr;
+    if (!reuse) *out = nullptr;
     if (kind < NEO_MEM_SHOUT_VALUE || kind > NEO_MEM_PRODUCT) return ctx->fail(NEO_ERR_ARG, "mem_oracle: unknown kind");
     if (ell > 30) return ctx->fail(NEO_ERR_ARG, "mem_oracle: ell > 30");
     if (expected_cols(kind, A, n_cols) != (int)n_cols || (n_cols == 0 && kind != NEO_MEM_BITNESS))
@@ -449,8 +450,15 @@ int mem_create(neo_gpu_ctx* ctx, int kind, uint32_t ell, const uint64_t* r_point
     if (deg > MEM_MAX_DEG) return ctx->fail(NEO_ERR_UNSUPPORTED, "mem_oracle: degree bound above 31");
     cudaSetDevice(ctx->device);
 
-    auto* o = new neo_gpu_mem_oracle();
+    // reuse: rebuild into the caller's object, keeping its device buffers
+    neo_gpu_mem_oracle* o = reuse ? *out : nullptr;
+    const bool fresh = !o;
+    if (fresh) o = new neo_gpu_mem_oracle();
     o->ctx = ctx;
+    o->bit_idx = 0;
+    o->cur = 0;
+    o->pending = false;
+    o->hw.clear();
     o->kind = kind;
     o->ell = ell;
     o->A = A;
@@ -459,9 +467,12 @@ int mem_create(neo_gpu_ctx* ctx, int kind, uint32_t ell, const uint64_t* r_point
     o->bitness = kind == NEO_MEM_BITNESS;
     o->len = 1ULL << ell;
     const uint64_t L = o->len;
-    auto fail = [&](int rc) { delete o; return rc; };
-    if (o->tab[0].alloc((size_t)o->nf * L) || o->tab[1].alloc((size_t)o->nf * (L > 1 ? L / 2 : 1)) ||
-        o->vals.alloc(deg + 1))
+    auto fail = [&](int rc) {
+        if (fresh) delete o;
+        return rc;
+    };
+    if (o->tab[0].ensure((size_t)o->nf * L) || o->tab[1].ensure((size_t)o->nf * (L > 1 ? L / 2 : 1)) ||
+        o->vals.ensure(deg + 1))
         return fail(ctx->fail(NEO_ERR_OOM, "mem_oracle: table allocation"));
     K* T = o->tab[0].p;
     cudaStream_t S = ctx->stream;
@@ -469,12 +480,14 @@ int mem_create(neo_gpu_ctx* ctx, int kind, uint32_t ell, const uint64_t* r_point
     const size_t colb = L * sizeof(K);
     auto col = [&](uint32_t c) { return reinterpret_cast<const K*>(cols) + (size_t)c * L; };
     auto put = [&](uint32_t f, uint32_t c) { return cudaMemcpyAsync(T + (size_t)f * L, col(c), colb, cpk, S); };
-    DevBuf<K> dpt, dra, tmp;
-    if (r_point && dpt.alloc(ell ? ell : 1)) return fail(ctx->fail(NEO_ERR_OOM, "mem_oracle: point"));
+    DevBuf<K>& dpt = o->dpt;
+    DevBuf<K>& dra = o->dra;
+    DevBuf<K>& tmp = o->tmp;
+    if (r_point && dpt.ensure(ell ? ell : 1)) return fail(ctx->fail(NEO_ERR_OOM, "mem_oracle: point"));
     if (r_point && ell && cudaMemcpyAsync(dpt.p, r_point, ell * sizeof(K), cudaMemcpyHostToDevice, S))
         return fail(ctx->fail(NEO_ERR_CUDA, "mem_oracle: point upload"));
     if (A && r_addr) {
-        if (dra.alloc(A) || cudaMemcpyAsync(dra.p, r_addr, A * sizeof(K), cudaMemcpyHostToDevice, S))
+        if (dra.ensure(A) || cudaMemcpyAsync(dra.p, r_addr, A * sizeof(K), cudaMemcpyHostToDevice, S))
             return fail(ctx->fail(NEO_ERR_OOM, "mem_oracle: r_addr"));
     }
     auto eqbits = [&](uint32_t f0, uint32_t c0) -> int {
@@ -503,7 +516,7 @@ int mem_create(neo_gpu_ctx* ctx, int kind, uint32_t ell, const uint64_t* r_point
         case NEO_MEM_BITNESS:
             for (uint32_t c = 0; c < n_cols && !ce; c++) ce = put(1 + c, c);
             for (uint32_t c = 0; c < n_cols; c++) o->hw.push_back(kload_h(weights + 2 * c));
-            if (!ce && n_cols && (o->w.alloc(n_cols) ||
+            if (!ce && n_cols && (o->w.ensure(n_cols) ||
                         cudaMemcpyAsync(o->w.p, weights, n_cols * sizeof(K), cudaMemcpyHostToDevice, S)))
                 ce = cudaErrorMemoryAllocation;
             break;
@@ -513,7 +526,7 @@ int mem_create(neo_gpu_ctx* ctx, int kind, uint32_t ell, const uint64_t* r_point
             // write stream columns: has_write, inc, wa bits
             const uint32_t c_hw = rd ? 2 + A : 0, c_inc = rd ? 3 + A : 2, c_wa = rd ? 4 + A : 3;
             const uint32_t c_a = rd ? 1 : 1;  // rv (read) or wv (write)
-            if (tmp.alloc((size_t)(4 + A) * L)) { ce = cudaErrorMemoryAllocation; break; }
+            if (tmp.ensure((size_t)(4 + A) * L)) { ce = cudaErrorMemoryAllocation; break; }
             K* hw = tmp.p;
             K* inc = tmp.p + L;
             K* aa = tmp.p + 2 * L;
@@ -527,8 +540,8 @@ int mem_create(neo_gpu_ctx* ctx, int kind, uint32_t ell, const uint64_t* r_point
             inc_terms_kernel<<<ceil_div(L, 256), 256, 0, S>>>(hw, inc, wa, A, dra.p, L, terms);
             NEO_LAUNCHED(ctx);
             const uint32_t nblk = (uint32_t)ceil_div(L, SCAN_BLK);
-            DevBuf<K> sums;
-            if (sums.alloc(nblk)) { ce = cudaErrorMemoryAllocation; break; }
+            DevBuf<K>& sums = o->sums;
+            if (sums.ensure(nblk)) { ce = cudaErrorMemoryAllocation; break; }
             scan_sums_kernel<<<nblk, SCAN_T, 0, S>>>(terms, L, sums.p);
             NEO_LAUNCHED(ctx);
             K init_k = init ? kload_h(init) : gl::kzero();
@@ -539,7 +552,6 @@ int mem_create(neo_gpu_ctx* ctx, int kind, uint32_t ell, const uint64_t* r_point
             NEO_LAUNCHED(ctx);
             ce = put(1, 0);  // gate: has_read | has_write
             if (!ce) rc = eqbits(3, rd ? 2 : 3);
-            if (!ce) ce = cudaStreamSynchronize(S);  // sums / tmp are released at scope exit
         } break;
         case NEO_MEM_VAL_EVAL:
             ce = put(0, 0);
@@ -581,6 +593,18 @@ extern "C" int neo_gpu_mem_oracle_create(neo_gpu_ctx* ctx, int kind, uint32_t el
                                          uint64_t* claim, neo_gpu_mem_oracle** out) {
     return mem_create(ctx, kind, ell, r_point, ell_addr, r_addr, init_at_r_addr, n_cols, cols, false, weights, claim,
                       out);
+}
+
+// Rebuild into *slot when it holds an oracle (its device buffers are kept),
+// create one otherwise; columns in device memory.  Fold steps call this every
+// step so that no device allocation (a device-wide synchronization for
+// cudaFree) happens once the buffers have grown.
+int mem_oracle_build_device(neo_gpu_ctx* ctx, int kind, uint32_t ell, const uint64_t* r_point, uint32_t ell_addr,
+                            const uint64_t* r_addr, const uint64_t* init_at_r_addr, uint32_t n_cols,
+                            const uint64_t* d_cols, const uint64_t* weights, uint64_t* claim,
+                            neo_gpu_mem_oracle** slot) {
+    return mem_create(ctx, kind, ell, r_point, ell_addr, r_addr, init_at_r_addr, n_cols, d_cols, true, weights, claim,
+                      slot, true);
 }
 
 extern "C" int neo_gpu_mem_oracle_create_device(neo_gpu_ctx* ctx, int kind, uint32_t ell, const uint64_t* r_point,
@@ -642,13 +666,17 @@ extern "C" int neo_gpu_mem_oracle_destroy(neo_gpu_mem_oracle* o) {
 // (2^ell K), d_bits (A columns of 2^ell K), d_table (table_len K).  Writes
 // d_w (2^A K) and the claimed sum to *claim (host); synchronizes the stream.
 int addr_weights_device(neo_gpu_ctx* ctx, uint32_t ell, const K* d_rcycle, uint32_t A, const K* d_has,
-                        const K* d_bits, const K* d_table, uint64_t table_len, K* d_w, K* claim) {
+                        const K* d_bits, const K* d_table, uint64_t table_len, K* d_w, K* claim, AddrWs* ws) {
     cudaStream_t S = ctx->stream;
     const uint64_t L = 1ULL << ell, P = 1ULL << A;
-    DevBuf<K> chi, part, out1;
-    DevBuf<unsigned long long> acc;
-    NEO_CK(ctx, chi.alloc(L));
-    NEO_CK(ctx, acc.alloc(4 * P));
+    AddrWs local;
+    AddrWs& W = ws ? *ws : local;
+    DevBuf<K>& chi = W.chi;
+    DevBuf<K>& part = W.part;
+    DevBuf<K>& out1 = W.out1;
+    DevBuf<unsigned long long>& acc = W.acc;
+    NEO_CK(ctx, chi.ensure(L));
+    NEO_CK(ctx, acc.ensure(4 * P));
     NEO_CK(ctx, cudaMemsetAsync(acc.p, 0, 4 * P * sizeof(unsigned long long), S));
     int rc = launch_chi_table(ctx, d_rcycle, ell, chi.p);
     if (rc) return rc;
@@ -658,8 +686,8 @@ int addr_weights_device(neo_gpu_ctx* ctx, uint32_t ell, const K* d_rcycle, uint3
     NEO_LAUNCHED(ctx);
     const uint64_t n = table_len < P ? table_len : P;
     const uint32_t nb = 148;
-    NEO_CK(ctx, part.alloc(nb));
-    NEO_CK(ctx, out1.alloc(1));
+    NEO_CK(ctx, part.ensure(nb));
+    NEO_CK(ctx, out1.ensure(1));
     dot_kernel<<<nb, 256, 0, S>>>(d_table, d_w, n, part.p);
     NEO_LAUNCHED(ctx);
     mem_reduce_kernel<<<1, 256, 0, S>>>(part.p, nb, out1.p);
@@ -691,7 +719,7 @@ extern "C" int neo_gpu_addr_lookup_weights(neo_gpu_ctx* ctx, uint32_t ell, const
     if (ell_addr) NEO_CK(ctx, cudaMemcpyAsync(bits.p, addr_bits, (size_t)L * ell_addr * sizeof(K), cudaMemcpyHostToDevice, S));
     if (table_len) NEO_CK(ctx, cudaMemcpyAsync(tab.p, table, table_len * sizeof(K), cudaMemcpyHostToDevice, S));
     K cl;
-    int rc = addr_weights_device(ctx, ell, dr.p, ell_addr, has.p, bits.p, tab.p, table_len, w.p, &cl);
+    int rc = addr_weights_device(ctx, ell, dr.p, ell_addr, has.p, bits.p, tab.p, table_len, w.p, &cl, nullptr);
     if (rc) return rc;
     NEO_CK(ctx, cudaMemcpy(weights, w.p, P * sizeof(K), cudaMemcpyDeviceToHost));
     claim[0] = cl.re;
@@ -904,6 +932,9 @@ struct neo_gpu_twist_addr {
     uint32_t A = 0, bit = 0, E = 0;
     DevBuf<K> eq, hr, rv, hw, inc, wv, rpw, wpw, wdelta, tab[2], partials, vals;
     DevBuf<uint32_t> ra, wa, wkey;
+    DevBuf<K> dcols, dr, dv;         // build workspace, kept for reuse
+    DevBuf<uint32_t> counts;
+    DevBuf<uint64_t> da;
     uint64_t tab_len = 0;
     int cur = 0;
     bool pending = false;
@@ -967,9 +998,9 @@ int ta_values(neo_gpu_twist_addr* o) {
 
 int ta_create(neo_gpu_ctx* ctx, int kind, uint32_t ell, const uint64_t* r_cycle, uint32_t A, uint64_t n_init,
               const uint64_t* init_addr, const uint64_t* init_val, const uint64_t* cols, bool dev,
-              neo_gpu_twist_addr** out) {
+              neo_gpu_twist_addr** out, bool reuse = false) {
     if (!ctx || !out) return NEO_ERR_ARG;
-    *out = nullptr;
+    if (!reuse) *out = nullptr;
     if (kind != 0 && kind != 1) return ctx->fail(NEO_ERR_ARG, "twist_addr: kind must be 0 (read) or 1 (write)");
     if (ell > 30 || A > 30 || A == 0) return ctx->fail(NEO_ERR_ARG, "twist_addr: ell / ell_addr out of range");
     if (!cols || (ell && !r_cycle) || (n_init && (!init_addr || !init_val)))
@@ -980,20 +1011,29 @@ int ta_create(neo_gpu_ctx* ctx, int kind, uint32_t ell, const uint64_t* r_cycle,
     cudaStream_t S = ctx->stream;
     const uint64_t L = 1ULL << ell, P = 1ULL << A;
     const uint32_t n_cols = kind == 0 ? 4 + 2 * A : 3 + A;
-    auto* o = new neo_gpu_twist_addr();
+    neo_gpu_twist_addr* o = reuse ? *out : nullptr;
+    const bool fresh = !o;
+    if (fresh) o = new neo_gpu_twist_addr();
     o->ctx = ctx;
     o->kind = kind;
     o->A = A;
-    auto fail = [&](int rc) { delete o; return rc; };
-    DevBuf<K> dcols, dr;
+    o->bit = 0;
+    o->cur = 0;
+    o->pending = false;
+    auto fail = [&](int rc) {
+        if (fresh) delete o;
+        return rc;
+    };
+    DevBuf<K>& dcols = o->dcols;
+    DevBuf<K>& dr = o->dr;
     const K* C = reinterpret_cast<const K*>(cols);
     if (!dev) {
-        if (dcols.alloc((size_t)n_cols * L)) return fail(ctx->fail(NEO_ERR_OOM, "twist_addr: columns"));
+        if (dcols.ensure((size_t)n_cols * L)) return fail(ctx->fail(NEO_ERR_OOM, "twist_addr: columns"));
         if (cudaMemcpyAsync(dcols.p, cols, (size_t)n_cols * L * sizeof(K), cudaMemcpyHostToDevice, S))
             return fail(ctx->fail(NEO_ERR_CUDA, "twist_addr: column upload"));
         C = dcols.p;
     }
-    if (dr.alloc(ell ? ell : 1)) return fail(ctx->fail(NEO_ERR_OOM, "twist_addr: r"));
+    if (dr.ensure(ell ? ell : 1)) return fail(ctx->fail(NEO_ERR_OOM, "twist_addr: r"));
     if (ell && cudaMemcpyAsync(dr.p, r_cycle, ell * sizeof(K), cudaMemcpyHostToDevice, S))
         return fail(ctx->fail(NEO_ERR_CUDA, "twist_addr: r upload"));
     TaBuild b{};
@@ -1003,8 +1043,8 @@ int ta_create(neo_gpu_ctx* ctx, int kind, uint32_t ell, const uint64_t* r_cycle,
         b.hw = C; b.wv = C + L; b.inc = C + 2 * L; b.wa = C + 3 * L;
     }
     const uint32_t nblk = ceil_div(L, TA_T);
-    DevBuf<uint32_t> counts;
-    if (counts.alloc(nblk)) return fail(ctx->fail(NEO_ERR_OOM, "twist_addr: counts"));
+    DevBuf<uint32_t>& counts = o->counts;
+    if (counts.ensure(nblk)) return fail(ctx->fail(NEO_ERR_OOM, "twist_addr: counts"));
     ta_count_kernel<<<nblk, TA_T, 0, S>>>(b.hr, b.hw, L, counts.p);
     NEO_LAUNCHED(ctx);
     std::vector<uint32_t> hc(nblk);
@@ -1014,10 +1054,10 @@ int ta_create(neo_gpu_ctx* ctx, int kind, uint32_t ell, const uint64_t* r_cycle,
     for (auto& c : hc) { uint32_t v = c; c = (uint32_t)E; E += v; }
     o->E = (uint32_t)E;
     const size_t ecap = E ? E : 1;
-    if (o->eq.alloc(ecap) || o->hr.alloc(ecap) || o->rv.alloc(ecap) || o->hw.alloc(ecap) || o->inc.alloc(ecap) ||
-        o->wv.alloc(ecap) || o->rpw.alloc(ecap) || o->wpw.alloc(ecap) || o->wdelta.alloc(ecap) || o->ra.alloc(ecap) ||
-        o->wa.alloc(ecap) || o->wkey.alloc(ecap) || o->vals.alloc(3) || o->tab[0].alloc(P + 1) ||
-        o->tab[1].alloc(P / 2 + 1))
+    if (o->eq.ensure(ecap) || o->hr.ensure(ecap) || o->rv.ensure(ecap) || o->hw.ensure(ecap) || o->inc.ensure(ecap) ||
+        o->wv.ensure(ecap) || o->rpw.ensure(ecap) || o->wpw.ensure(ecap) || o->wdelta.ensure(ecap) ||
+        o->ra.ensure(ecap) || o->wa.ensure(ecap) || o->wkey.ensure(ecap) || o->vals.ensure(3) ||
+        o->tab[0].ensure(P + 1) || o->tab[1].ensure(P / 2 + 1))
         return fail(ctx->fail(NEO_ERR_OOM, "twist_addr: event arrays"));
     NEO_CK(ctx, cudaMemcpyAsync(counts.p, hc.data(), nblk * 4, cudaMemcpyHostToDevice, S));
     b.r_cycle = dr.p; b.ell = ell; b.A = A; b.L = L; b.offs = counts.p;
@@ -1036,14 +1076,13 @@ int ta_create(neo_gpu_ctx* ctx, int kind, uint32_t ell, const uint64_t* r_cycle,
     NEO_CK(ctx, cudaMemsetAsync(o->tab[0].p, 0, (P + 1) * sizeof(K), S));
     NEO_CK(ctx, cudaMemsetAsync(o->tab[1].p, 0, (P / 2 + 1) * sizeof(K), S));
     if (n_init) {
-        DevBuf<uint64_t> da;
-        DevBuf<K> dv;
-        if (da.alloc(n_init) || dv.alloc(n_init)) return fail(ctx->fail(NEO_ERR_OOM, "twist_addr: init"));
+        DevBuf<uint64_t>& da = o->da;
+        DevBuf<K>& dv = o->dv;
+        if (da.ensure(n_init) || dv.ensure(n_init)) return fail(ctx->fail(NEO_ERR_OOM, "twist_addr: init"));
         NEO_CK(ctx, cudaMemcpyAsync(da.p, init_addr, n_init * 8, cudaMemcpyHostToDevice, S));
         NEO_CK(ctx, cudaMemcpyAsync(dv.p, init_val, n_init * sizeof(K), cudaMemcpyHostToDevice, S));
         scatter_init_kernel<<<ceil_div(n_init, 256), 256, 0, S>>>(da.p, dv.p, n_init, o->tab[0].p);
         NEO_LAUNCHED(ctx);
-        NEO_CK(ctx, cudaStreamSynchronize(S));
     }
     o->tab_len = P;
     NEO_CK(ctx, cudaStreamSynchronize(S));
@@ -1052,6 +1091,14 @@ int ta_create(neo_gpu_ctx* ctx, int kind, uint32_t ell, const uint64_t* r_cycle,
 }
 
 }  // namespace
+
+// Rebuild into *slot when it holds an oracle (buffers kept), else create;
+// columns in device memory (the fold step's per-step path).
+int twist_addr_build_device(neo_gpu_ctx* ctx, int kind, uint32_t ell, const uint64_t* r_cycle, uint32_t ell_addr,
+                            uint64_t n_init, const uint64_t* init_addr, const uint64_t* init_val,
+                            const uint64_t* d_cols, neo_gpu_twist_addr** slot) {
+    return ta_create(ctx, kind, ell, r_cycle, ell_addr, n_init, init_addr, init_val, d_cols, true, slot, true);
+}
 
 extern "C" int neo_gpu_twist_addr_create(neo_gpu_ctx* ctx, int kind, uint32_t ell, const uint64_t* r_cycle,
                                          uint32_t ell_addr, uint64_t n_init, const uint64_t* init_addr,

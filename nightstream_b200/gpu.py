@@ -59,6 +59,7 @@ SIGNATURES = {
     "neo_gpu_batch_set_reserve": [P, U64],
     "neo_gpu_batch_submit": [P, P, P, U32, U32, U32, ctypes.c_char_p, P],
     "neo_gpu_batch_wait_all": [P, ctypes.c_double],
+    "neo_gpu_batch_submit_mem": [P, P, P, P, U32, U32, U32, ctypes.c_char_p, P],
     "neo_gpu_batch_job_info": [P, U64, P, P, P],
     "neo_gpu_batch_kernel_launches": [P],
     "neo_gpu_batch_destroy": [P],
@@ -573,12 +574,17 @@ class Batch:
         self._descs = []
 
     def submit(self, ccs, z: np.ndarray, n_steps: int, m_in: int = 1, k_rho: int = 12,
-               app_label: bytes = b"neo/shard") -> int:
+               app_label: bytes = b"neo/shard", mem: dict = None) -> int:
         desc = ccs.desc()
         z = _u64(z)
         jid = ctypes.c_uint64()
-        rc = self.lib.neo_gpu_batch_submit(self.h, ctypes.byref(desc), _p(z), n_steps, m_in, k_rho, app_label,
-                                           ctypes.byref(jid))
+        if mem and (mem.get("shout") or mem.get("twist")):
+            md = _mem_desc(mem)
+            rc = self.lib.neo_gpu_batch_submit_mem(self.h, ctypes.byref(desc), ctypes.byref(md), _p(z), n_steps, m_in,
+                                                   k_rho, app_label, ctypes.byref(jid))
+        else:
+            rc = self.lib.neo_gpu_batch_submit(self.h, ctypes.byref(desc), _p(z), n_steps, m_in, k_rho, app_label,
+                                               ctypes.byref(jid))
         if rc:
             raise NeoGpuError(rc, "batch submit")
         return jid.value
