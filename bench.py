@@ -56,7 +56,8 @@ def parse():
     ap.add_argument("--shards", type=int, default=64)
     ap.add_argument("--shard-steps", type=int, default=3)
     ap.add_argument("--workers", type=int, default=0, help="batch workers (0: min(16, host cores))")
-    ap.add_argument("--batch-in-plain", action="store_true", help="also run the batched mix in plain mode")
+    ap.add_argument("--no-batch", action="store_true",
+                    help="plain mode without the batched 64-shard memory mix (batched vs one-at-a-time) sub-result")
     return ap.parse_args()
 
 
@@ -514,7 +515,7 @@ def run_ours(args, rank, world, local_rank):
                "roofline": roofline, "roofline_commit": roofline_commit, "step_breakdown_ms": stats}
         if world == 1 and not args.no_cpu_baseline:
             out["cpu_baseline"] = cpu_baseline(args, ccs, z, pp, mem)
-        if world == 1 and args.batch_in_plain:
+        if world == 1 and not args.no_batch:
             out["batched"] = batched_result(args)
         print(json.dumps(out), flush=True)
     shard.close()

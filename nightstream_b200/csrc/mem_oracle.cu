@@ -195,25 +195,36 @@ __global__ void __launch_bounds__(MT) mem_eval_kernel(const MemEvalArgs a) {
     const uint32_t x = blockIdx.y;
     K acc = gl::kzero();
     if (p < pairs) {
+        // A factor that is zero on both children makes the whole product zero
+        // at every x: gate columns (has_lookup, has_read, has_write, the
+        // address weights) are zero outside the active trace rows, so most
+        // pairs stop after loading the gate (factors are ordered gate-first).
         if (!a.bitness) {
             K prod = gl::kone();
             for (uint32_t f = 0; f < a.nf; f++) {
                 const K* s = a.tab + (uint64_t)f * a.len + 2 * p;
                 K f0 = s[0], f1 = s[1];
+                if (gl::kiszero(f0) && gl::kiszero(f1)) {
+                    prod = gl::kzero();
+                    break;
+                }
                 K v = gl::kadd(f0, gl::kscale_small(gl::ksub(f1, f0), (int32_t)x));
                 prod = gl::kmul(prod, v);
             }
             acc = prod;
         } else {
             const K* s = a.tab + 2 * p;
-            K chi = gl::kadd(s[0], gl::kscale_small(gl::ksub(s[1], s[0]), (int32_t)x));
             K sum = gl::kzero();
             for (uint32_t f = 1; f < a.nf; f++) {
                 const K* c = a.tab + (uint64_t)f * a.len + 2 * p;
+                if (gl::kiszero(c[0]) && gl::kiszero(c[1])) continue;  // b(b - 1) = 0 at every x
                 K bx = gl::kadd(c[0], gl::kscale_small(gl::ksub(c[1], c[0]), (int32_t)x));
                 sum = gl::kadd(sum, gl::kmul(gl::kmul(a.w[f - 1], bx), gl::ksub(bx, gl::kone())));
             }
-            acc = gl::kmul(chi, sum);
+            if (!gl::kiszero(sum)) {
+                K chi = gl::kadd(s[0], gl::kscale_small(gl::ksub(s[1], s[0]), (int32_t)x));
+                acc = gl::kmul(chi, sum);
+            }
         }
     }
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -742,7 +753,7 @@ extern "C" int neo_gpu_addr_lookup_weights(neo_gpu_ctx* ctx, uint32_t ell, const
 // ===========================================================================
 namespace {
 
-constexpr int TA_T = 256;
+constexpr int TA_T = 64;
 
 __device__ __forceinline__ uint32_t addr_bits_at(const K* bits, uint64_t L, uint32_t A, uint64_t t) {
     uint32_t a = 0;
@@ -842,12 +853,17 @@ struct TaEval {
     K* partials;        // [3][gridDim.x]
 };
 
+// grid.x: query events i in tiles of TA_T; grid.y: earlier-event chunks j of
+// TA_T.  The contribution is linear in the memory value, so each chunk adds
+// w·af(x)·(±its partial memory value) and chunk 0 adds the initial memory and
+// the constant terms; the reduction sums all blocks.
 __global__ void __launch_bounds__(TA_T) ta_eval_kernel(const TaEval a) {
     __shared__ uint32_t s_key[TA_T];
     __shared__ K s_d[TA_T];
     __shared__ K s_red[3][TA_T / 32];
     const uint32_t i = blockIdx.x * TA_T + threadIdx.x;
     const uint32_t i_end = min(a.E, blockIdx.x * TA_T + TA_T);
+    const uint32_t j0 = blockIdx.y * TA_T;
     bool q = false;
     uint32_t addr = 0;
     if (i < a.E) {
@@ -856,31 +872,30 @@ __global__ void __launch_bounds__(TA_T) ta_eval_kernel(const TaEval a) {
     }
     const uint32_t base = a.bit >= 31 ? 0u : ((addr >> (a.bit + 1)) << 1);
     K v0 = gl::kzero(), v1 = gl::kzero();
-    if (q) {
+    if (q && blockIdx.y == 0) {
         v0 = a.init_tab[base];
         v1 = a.init_tab[base + 1];
     }
-    // earlier writes, tile by tile (j < i)
-    for (uint32_t j0 = 0; j0 < i_end; j0 += TA_T) {
+    bool any = blockIdx.y == 0;
+    if (j0 < i_end) {  // block-uniform: some query of this block has earlier events in the chunk
         const uint32_t j = j0 + threadIdx.x;
-        __syncthreads();
         if (j < a.E) {
             s_key[threadIdx.x] = a.wkey[j];
             s_d[threadIdx.x] = a.wdelta[j];
         }
         __syncthreads();
-        if (q) {
-            const uint32_t jn = min((uint32_t)TA_T, i - j0 < TA_T ? i - j0 : TA_T);
-            if (i > j0)
-                for (uint32_t u = 0; u < jn; u++) {
-                    const uint32_t k = s_key[u];
-                    if (k == base) v0 = gl::kadd(v0, s_d[u]);
-                    else if (k == base + 1) v1 = gl::kadd(v1, s_d[u]);
-                }
+        if (q && i > j0) {
+            const uint32_t jn = i - j0 < TA_T ? i - j0 : TA_T;
+            any = true;
+            for (uint32_t u = 0; u < jn; u++) {
+                const uint32_t k = s_key[u];
+                if (k == base) v0 = gl::kadd(v0, s_d[u]);
+                else if (k == base + 1) v1 = gl::kadd(v1, s_d[u]);
+            }
         }
     }
     K c[3] = {gl::kzero(), gl::kzero(), gl::kzero()};
-    if (q) {
+    if (q && any) {
         const bool b = a.bit < 32 && ((addr >> a.bit) & 1);
         K w = a.kind == 0 ? gl::kmul(gl::kmul(a.eq[i], a.hr[i]), a.rpw[i]) : gl::kmul(gl::kmul(a.eq[i], a.hw[i]), a.wpw[i]);
         K dv = gl::ksub(v1, v0);
@@ -888,7 +903,9 @@ __global__ void __launch_bounds__(TA_T) ta_eval_kernel(const TaEval a) {
 #pragma unroll
         for (int x = 0; x < 3; x++) {
             K af = b ? gl::kfq((uint64_t)x) : gl::kfq(gl::sub(1, (uint64_t)x));
-            K term = a.kind == 0 ? gl::ksub(vx, a.rv[i]) : gl::ksub(gl::ksub(a.wv[i], vx), a.inc[i]);
+            K term;
+            if (blockIdx.y == 0) term = a.kind == 0 ? gl::ksub(vx, a.rv[i]) : gl::ksub(gl::ksub(a.wv[i], vx), a.inc[i]);
+            else term = a.kind == 0 ? vx : gl::kneg(vx);
             c[x] = gl::kmul(gl::kmul(w, af), term);
             vx = gl::kadd(vx, dv);
         }
@@ -905,7 +922,8 @@ __global__ void __launch_bounds__(TA_T) ta_eval_kernel(const TaEval a) {
     if (threadIdx.x < 3) {
         K s = gl::kzero();
         for (int w = 0; w < TA_T / 32; w++) s = gl::kadd(s, s_red[threadIdx.x][w]);
-        a.partials[(uint64_t)threadIdx.x * gridDim.x + blockIdx.x] = s;
+        const uint64_t nb = (uint64_t)gridDim.x * gridDim.y;
+        a.partials[(uint64_t)threadIdx.x * nb + (uint64_t)blockIdx.y * gridDim.x + blockIdx.x] = s;
     }
 }
 
@@ -976,7 +994,8 @@ int ta_values(neo_gpu_twist_addr* o) {
     ta_prep_kernel<<<ceil_div(o->E, 256), 256, 0, S>>>(o->hw.p, o->inc.p, o->wa.p, o->wpw.p, o->E, o->bit, o->wkey.p,
                                                      o->wdelta.p);
     NEO_LAUNCHED(ctx);
-    const uint32_t nb = ceil_div(o->E, TA_T);
+    const uint32_t nbx = ceil_div(o->E, TA_T);
+    const uint32_t nb = nbx * nbx;
     NEO_CK(ctx, o->partials.ensure((size_t)3 * nb));
     TaEval a;
     a.kind = o->kind;
@@ -987,7 +1006,7 @@ int ta_values(neo_gpu_twist_addr* o) {
     a.wkey = o->wkey.p; a.wdelta = o->wdelta.p;
     a.init_tab = o->tab[o->cur].p;
     a.partials = o->partials.p;
-    ta_eval_kernel<<<nb, TA_T, 0, S>>>(a);
+    ta_eval_kernel<<<dim3(nbx, nbx), TA_T, 0, S>>>(a);
     NEO_LAUNCHED(ctx);
     mem_reduce_kernel<<<3, 256, 0, S>>>(o->partials.p, nb, o->vals.p);
     NEO_LAUNCHED(ctx);

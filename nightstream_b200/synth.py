@@ -96,67 +96,77 @@ def uniform_k(rng, count: int) -> np.ndarray:
     return _uniform_fq(rng, (count, 2))
 
 
-def memory_trace(steps: int, shout_ell: int, twist_ell: int, seed: int, table_len: int = None, init_cells: int = 64):
-    """One fold step's worth of a RISC-V-style trace: per step one Shout lookup
-    (uniform index into a table of uniform 32-bit entries) and one Twist read +
-    one write (addresses 70 % stride-4 sequential / 30 % uniform over 2^twist_ell
-    cells, 32-bit values).  Returns the bus columns (values per step, Shout
-    first then Twist, in the shared-bus column order) and the instance data."""
+def memory_trace(steps: int, shout_ell, twist_ell, seed: int, table_len: int = None, init_cells: int = 64,
+                 lookup_rate: float = 1.0, rw_rate: float = 1.0):
+    """One fold step's worth of a RISC-V-style trace: per step a Shout lookup
+    (probability lookup_rate; uniform index into a table of uniform 32-bit
+    entries) and a Twist read + write (probability rw_rate each; addresses 70 %
+    stride-4 sequential / 30 % uniform over 2^twist_ell cells, 32-bit values;
+    the first init_cells cells start nonzero, 0 = MemInit::Zero).  shout_ell /
+    twist_ell: one int per instance (or a single int).  Returns the bus columns
+    (values per step, Shout instances first then Twist, in the shared-bus
+    column order) and the instance data."""
     rng = np.random.default_rng(seed)
-    table_len = table_len or (1 << shout_ell)
-    table = rng.integers(0, 1 << 32, size=table_len, dtype=np.uint64)
-    P = 1 << twist_ell
-    init = [(int(a), int(v)) for a, v in
-            zip(range(min(init_cells, P)), rng.integers(1, 1 << 32, size=min(init_cells, P)))]
-    mem = np.zeros(P, dtype=object)
-    for a, v in init:
-        mem[a] = v
-    idx = rng.integers(0, table_len, size=steps)
-    cols = []
-    for b in range(shout_ell):
-        cols.append((idx >> b) & 1)
-    cols.append(np.ones(steps, dtype=np.int64))       # has_lookup
-    cols.append(table[idx])                            # val
-    ra = np.zeros(steps, np.int64)
-    wa = np.zeros(steps, np.int64)
-    rv = np.zeros(steps, dtype=object)
-    wv = rng.integers(0, 1 << 32, size=steps)
-    inc = np.zeros(steps, dtype=object)
-    pos = 0
-    for j in range(steps):
-        if rng.random() < 0.7:
-            pos = (pos + 4) % P
-            ra[j] = pos
-        else:
-            ra[j] = int(rng.integers(0, P))
-        wa[j] = ra[j] if rng.random() < 0.5 else int(rng.integers(0, P))
-        rv[j] = mem[ra[j]]
-        inc[j] = (int(wv[j]) - int(mem[wa[j]])) % Q
-        mem[wa[j]] = int(wv[j])
-    for b in range(twist_ell):
-        cols.append((ra >> b) & 1)
-    for b in range(twist_ell):
-        cols.append((wa >> b) & 1)
-    cols.append(np.ones(steps, dtype=np.int64))        # has_read
-    cols.append(np.ones(steps, dtype=np.int64))        # has_write
-    cols.append(wv)
-    cols.append(rv)
-    cols.append(inc)
+    shout_ells = [shout_ell] if isinstance(shout_ell, int) else list(shout_ell)
+    twist_ells = [twist_ell] if isinstance(twist_ell, int) else list(twist_ell)
+    cols, shout, twist = [], [], []
+    for se in shout_ells:
+        tl = table_len or (1 << se)
+        table = rng.integers(0, 1 << 32, size=tl, dtype=np.uint64)
+        idx = rng.integers(0, tl, size=steps)
+        has = (rng.random(steps) < lookup_rate).astype(np.int64)
+        idx = idx * has
+        for b in range(se):
+            cols.append((idx >> b) & 1)
+        cols.append(has)                               # has_lookup
+        cols.append(table[idx] * has.astype(np.uint64))  # val
+        shout.append(dict(ell_addr=se, k=1 << se, d=1, n_side=1 << se, ell=se, table=table))
+    for te in twist_ells:
+        P = 1 << te
+        n0 = min(init_cells, P)
+        init = [(int(a), int(v)) for a, v in zip(range(n0), rng.integers(1, 1 << 32, size=n0))]
+        mem = np.zeros(P, dtype=object)
+        for a, v in init:
+            mem[a] = v
+        ra = np.zeros(steps, np.int64)
+        wa = np.zeros(steps, np.int64)
+        hr = (rng.random(steps) < rw_rate).astype(np.int64)
+        hw = (rng.random(steps) < rw_rate).astype(np.int64)
+        rv = np.zeros(steps, dtype=object)
+        wv = rng.integers(0, 1 << 32, size=steps) * hw
+        inc = np.zeros(steps, dtype=object)
+        pos = 0
+        for j in range(steps):
+            if rng.random() < 0.7:
+                pos = (pos + 4) % P
+                a_r = pos
+            else:
+                a_r = int(rng.integers(0, P))
+            a_w = a_r if rng.random() < 0.5 else int(rng.integers(0, P))
+            if hr[j]:
+                ra[j] = a_r
+                rv[j] = mem[a_r]
+            if hw[j]:
+                wa[j] = a_w
+                inc[j] = (int(wv[j]) - int(mem[a_w])) % Q
+                mem[a_w] = int(wv[j])
+        for b in range(te):
+            cols.append((ra >> b) & 1)
+        for b in range(te):
+            cols.append((wa >> b) & 1)
+        cols += [hr, hw, wv, rv, inc]
+        twist.append(dict(ell_addr=te, k=P, d=1, n_side=P, ell=te, init=init))
     bus = np.array([[int(v) % Q for v in c] for c in cols], dtype=np.uint64)
-    mem_desc = dict(steps=steps,
-                    shout=[dict(ell_addr=shout_ell, k=1 << shout_ell, d=1, n_side=1 << shout_ell, ell=shout_ell,
-                                table=table)],
-                    twist=[dict(ell_addr=twist_ell, k=P, d=1, n_side=P, ell=twist_ell, init=init)])
-    return bus, mem_desc
+    return bus, dict(steps=steps, shout=shout, twist=twist)
 
 
-def make_memory_workload(ell: int, seed: int, steps: int, shout_ell: int, twist_ell: int, m_in: int = 1,
-                         table_len: int = None):
+def make_memory_workload(ell: int, seed: int, steps: int, shout_ell, twist_ell, m_in: int = 1,
+                         table_len: int = None, **trace_kw):
     """Single shard with memory: a satisfied R1CS of n = m = 2^ell whose witness
     carries the shared CPU bus (the Twist / Shout columns of `steps` trace steps)
     in its tail, bus cell (col, j) at m - bus_cols*steps + col*steps + j."""
     m = 1 << ell
-    bus, mem = memory_trace(steps, shout_ell, twist_ell, seed + 1, table_len)
+    bus, mem = memory_trace(steps, shout_ell, twist_ell, seed + 1, table_len, **trace_kw)
     rng = np.random.default_rng(seed + 2)
     z = rng.integers(0, 1 << 32, size=m, dtype=np.uint64)
     z[0] = 1

@@ -78,3 +78,23 @@ def test_memory_fold_rejects_bad_read(ctx):
         g.fold_step(bad)
     assert e.value.code == 3
     g.close()
+
+
+@pytest.mark.parametrize("case", [
+    dict(shout_ell=[6], twist_ell=[5, 4], init_cells=0),           # two Twist memories, MemInit::Zero
+    dict(shout_ell=[6, 6], twist_ell=[5], lookup_rate=0.0),        # no lookups: sampled r_addr, no sum-check
+    dict(shout_ell=[6, 6], twist_ell=[], lookup_rate=0.5),         # Shout only, half the steps look up
+    dict(shout_ell=[], twist_ell=[5], rw_rate=0.6),                # Twist only, sparse reads / writes
+])
+def test_memory_fold_instance_mixes(ctx, case):
+    ell = 10
+    ccs, z, mem = synth.make_memory_workload(ell, 9, 8, **case)
+    pp = np.random.default_rng(ell + 7).integers(0, Q, size=(16, 1 << ell, 54), dtype=np.uint64)
+    ctx.pp_upload(pp)
+    g = gpu.Shard(ctx, ccs, mem=mem, app_label=b"neo/test-mix")
+    o = OracleShard(ccs, pp, mem=mem, app_label=b"neo/test-mix")
+    for s in range(2):
+        pg, po = g.fold_step(z), o.fold_step(z)
+        assert pg.shape == po.shape and np.array_equal(pg, po), f"step {s}"
+        assert np.array_equal(g.transcript_state(), o.tr.state())
+    g.close()
