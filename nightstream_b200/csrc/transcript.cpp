@@ -192,15 +192,26 @@ __attribute__((noinline)) static void permute_impl(const Poseidon2<W>& P, uint64
     for (int i = 0; i < W; i++) st[i] = st_io[i];
     external_layer<W>(st);
     for (int r = 0; r < RF / 2; r++) full_round<W>(st, P.rc_ext[r]);
+    // Partial rounds: internal layer M_I x = sum(x) + mu_i * x_i.  Only lane 0
+    // goes through the S-box, so with rest = Σ_{i>=1} x_i the new lane 0 is
+    // (mu_0 + 1)·s + rest (one multiply-add after the S-box), while lanes
+    // 1..W-1 and the next rest are computed beside the next S-box chain.
+    u128 racc = 0;
+#pragma GCC unroll 16
+    for (int i = 1; i < W; i++) racc += st[i];
+    uint64_t rest = red128(racc);
+    const uint64_t mu0p1 = P.mu[0] + 1;  // mu_0 < q, so no wrap
     for (int r = 0; r < RP; r++) {
-        st[0] = sbox7(addq(st[0], P.rc_int[r]));
-        // internal layer: M_I x = sum(x) + mu_i * x_i
-        u128 acc = 0;
+        const uint64_t x = sbox7(addq(st[0], P.rc_int[r]));
+        const uint64_t sum = addq(x, rest);
+        st[0] = red128((u128)mu0p1 * x + rest);
+        u128 nacc = 0;
 #pragma GCC unroll 16
-        for (int i = 0; i < W; i++) acc += st[i];
-        const uint64_t sum = red128(acc);
-#pragma GCC unroll 16
-        for (int i = 0; i < W; i++) st[i] = red128((u128)P.mu[i] * st[i] + sum);
+        for (int i = 1; i < W; i++) {
+            st[i] = red128((u128)P.mu[i] * st[i] + sum);
+            nacc += st[i];
+        }
+        rest = red128(nacc);
     }
     for (int r = RF / 2; r < RF; r++) full_round<W>(st, P.rc_ext[r]);
 #pragma GCC unroll 16
