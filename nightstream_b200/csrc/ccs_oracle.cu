@@ -805,7 +805,7 @@ static int oracle_init(neo_gpu_ctx* ctx, neo_gpu_ccs_oracle* o, const int8_t* d_
             o->ccs->csr_ptr.p, o->ccs->csr_col.p, o->ccs->csr_val.p, nnzoff.p, isid.p, t, desc->n, desc->m, du.p,
             dcoef.p, n_pad, S + (size_t)o->idx_eval * n_pad);
         NEO_LAUNCHED(ctx);
-        NEO_CK(ctx, cudaStreamSynchronize(ctx->stream));
+        NEO_CK(ctx, ctx_sync(ctx));
     }
     // streamed rounds and the materialised NC table
     o->J = (int)std::min<uint32_t>(JMAX, ell_n - 1);
@@ -820,7 +820,7 @@ static int oracle_init(neo_gpu_ctx* ctx, neo_gpu_ccs_oracle* o, const int8_t* d_
     NEO_CK(ctx, o->partials.ensure(max_blocks * (o->deg_max + 1)));
     NEO_CK(ctx, o->coeffs.ensure(MAX_DEG + 1));
     NEO_CK(ctx, o->ys.ensure(16));
-    NEO_CK(ctx, cudaStreamSynchronize(ctx->stream));
+    NEO_CK(ctx, ctx_sync(ctx));
     return NEO_OK;
 }
 
@@ -925,8 +925,8 @@ static int row_round(neo_gpu_ccs_oracle* o) {
     int rc = row_round_launch(o, o->coeffs.p);
     if (rc) return rc;
     o->h_coeffs.resize(o->deg_max + 1);
-    NEO_CK(ctx, cudaMemcpyAsync(o->h_coeffs.data(), o->coeffs.p, (o->deg_max + 1) * 16, cudaMemcpyDeviceToHost, ctx->stream));
-    NEO_CK(ctx, cudaStreamSynchronize(ctx->stream));
+    NEO_CK(ctx, ctx_d2h(ctx, o->h_coeffs.data(), o->coeffs.p, (o->deg_max + 1) * 16));
+    NEO_CK(ctx, ctx_sync(ctx));
     o->coeffs_valid = true;
     return NEO_OK;
 }
@@ -944,7 +944,7 @@ static int ajtai_precompute(neo_gpu_ccs_oracle* o) {
     if (rc) return rc;
     rc = launch_me_y(ctx, *o->ccs, o->Z, o->k, o->m, o->chi_r.p, o->ell_n, o->b, o->vj.p, o->y_eval.p, o->y_sc.p);
     if (rc) return rc;
-    NEO_CK(ctx, cudaStreamSynchronize(ctx->stream));
+    NEO_CK(ctx, ctx_sync(ctx));
     o->have_pre = true;
     return NEO_OK;
 }
@@ -980,8 +980,8 @@ static int ajtai_round(neo_gpu_ccs_oracle* o, const uint64_t* xs, uint32_t nx, u
     NEO_CK(ctx, cudaFuncSetAttribute(ajtai_round_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     ajtai_round_kernel<<<1, 512, smem, ctx->stream>>>(a);
     NEO_LAUNCHED(ctx);
-    NEO_CK(ctx, cudaMemcpyAsync(ys, o->ys.p, nx * 16, cudaMemcpyDeviceToHost, ctx->stream));
-    NEO_CK(ctx, cudaStreamSynchronize(ctx->stream));
+    NEO_CK(ctx, ctx_d2h(ctx, ys, o->ys.p, nx * 16));
+    NEO_CK(ctx, ctx_sync(ctx));
     return NEO_OK;
 }
 
@@ -1063,9 +1063,9 @@ extern "C" int neo_gpu_ccs_oracle_me_outputs(neo_gpu_ccs_oracle* o, uint64_t* y,
         int rc = ajtai_precompute(o);
         if (rc) return rc;
     }
-    NEO_CK(ctx, cudaMemcpyAsync(y, o->y_eval.p, o->y_eval.bytes(), cudaMemcpyDeviceToHost, ctx->stream));
-    NEO_CK(ctx, cudaMemcpyAsync(y_scalars, o->y_sc.p, o->y_sc.bytes(), cudaMemcpyDeviceToHost, ctx->stream));
-    NEO_CK(ctx, cudaStreamSynchronize(ctx->stream));
+    NEO_CK(ctx, ctx_d2h(ctx, y, o->y_eval.p, o->y_eval.bytes()));
+    NEO_CK(ctx, ctx_d2h(ctx, y_scalars, o->y_sc.p, o->y_sc.bytes()));
+    NEO_CK(ctx, ctx_sync(ctx));
     return NEO_OK;
 }
 

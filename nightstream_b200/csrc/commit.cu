@@ -129,7 +129,7 @@ extern "C" int neo_gpu_pp_upload(neo_gpu_ctx* ctx, uint32_t kappa, uint64_t m, c
     if (!ctx) return NEO_ERR_ARG;
     if (!coeffs || kappa == 0 || m == 0 || kappa > 64) return ctx->fail(NEO_ERR_ARG, "pp_upload: bad args");
     cudaSetDevice(ctx->device);
-    NEO_CK(ctx, cudaStreamSynchronize(ctx->stream));
+    NEO_CK(ctx, ctx_sync(ctx));
     std::lock_guard<std::mutex> lk(g_pp_mu);  // uploads are serialized; replacing a PP in use races (documented)
     PPEntry*& slot = g_pp[{ctx->device, m}];
     if (!slot) {
@@ -163,8 +163,8 @@ extern "C" int neo_gpu_commit(neo_gpu_ctx* ctx, const int8_t* digits, uint32_t n
     int rc = launch_commit(ctx, dZ.p, n_vec, m, dout.p);
     if (rc) return rc;
     if ((rc = check_device_error(ctx))) return rc;
-    NEO_CK(ctx, cudaMemcpyAsync(out, dout.p, dout.bytes(), cudaMemcpyDeviceToHost, ctx->stream));
-    NEO_CK(ctx, cudaStreamSynchronize(ctx->stream));
+    NEO_CK(ctx, ctx_d2h(ctx, out, dout.p, dout.bytes()));
+    NEO_CK(ctx, ctx_sync(ctx));
     return NEO_OK;
 }
 

@@ -391,7 +391,7 @@ int tc_pp_prepare(neo_gpu_ctx* ctx, PPEntry* pp) {
     const uint64_t threads = n_kb * 128 * 8;
     pp_limbs_kernel<<<ceil_div(threads, 256), 256, 0, ctx->stream>>>(pp->d_pp, pp->kappa, pp->m, pp->d_pp_limbs);
     NEO_LAUNCHED(ctx);
-    NEO_CK(ctx, cudaStreamSynchronize(ctx->stream));
+    NEO_CK(ctx, ctx_sync(ctx));
     return NEO_OK;
 }
 

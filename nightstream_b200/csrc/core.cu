@@ -33,6 +33,7 @@ extern "C" int neo_gpu_ctx_destroy(neo_gpu_ctx* ctx) {
     cudaStreamSynchronize(ctx->stream);
     if (ctx->scratch) cudaFree(ctx->scratch);
     if (ctx->d_err) cudaFree(ctx->d_err);
+    if (ctx->sync_ev) cudaEventDestroy(ctx->sync_ev);
     cudaStreamDestroy(ctx->stream);
     delete ctx;
     return NEO_OK;
@@ -42,8 +43,8 @@ extern "C" const char* neo_gpu_last_error(const neo_gpu_ctx* ctx) { return ctx ?
 extern "C" uint64_t neo_gpu_kernel_launches(const neo_gpu_ctx* ctx) { return ctx ? ctx->launches : 0; }
 int check_device_error(neo_gpu_ctx* ctx) {
     uint32_t e = 0;
-    NEO_CK(ctx, cudaMemcpyAsync(&e, ctx->d_err, 4, cudaMemcpyDeviceToHost, ctx->stream));
-    NEO_CK(ctx, cudaStreamSynchronize(ctx->stream));
+    NEO_CK(ctx, ctx_d2h(ctx, &e, ctx->d_err, 4));
+    NEO_CK(ctx, ctx_sync(ctx));
     if (e) {
         NEO_CK(ctx, cudaMemsetAsync(ctx->d_err, 0, 4, ctx->stream));
         char buf[96];
@@ -61,7 +62,7 @@ extern "C" int neo_gpu_ctx_stream(const neo_gpu_ctx* ctx, void** stream) {
 extern "C" int neo_gpu_synchronize(neo_gpu_ctx* ctx) {
     if (!ctx) return NEO_ERR_ARG;
     cudaSetDevice(ctx->device);
-    NEO_CK(ctx, cudaStreamSynchronize(ctx->stream));
+    NEO_CK(ctx, ctx_sync(ctx));
     return NEO_OK;
 }
 
@@ -174,8 +175,8 @@ extern "C" int neo_gpu_decomp_b2(neo_gpu_ctx* ctx, const uint64_t* z, uint64_t m
     NEO_CK(ctx, cudaMemcpyAsync(dz.p, z, m * 8, cudaMemcpyHostToDevice, ctx->stream));
     decomp_b2_kernel<<<ceil_div(m, 256), 256, 0, ctx->stream>>>(dz.p, m, dZ.p);
     NEO_LAUNCHED(ctx);
-    NEO_CK(ctx, cudaMemcpyAsync(Z, dZ.p, (size_t)NEO_D * m, cudaMemcpyDeviceToHost, ctx->stream));
-    NEO_CK(ctx, cudaStreamSynchronize(ctx->stream));
+    NEO_CK(ctx, ctx_d2h(ctx, Z, dZ.p, (size_t)NEO_D * m));
+    NEO_CK(ctx, ctx_sync(ctx));
     return NEO_OK;
 }
 
@@ -258,8 +259,8 @@ extern "C" int neo_gpu_rlc_mix(neo_gpu_ctx* ctx, const int8_t* rho_coeffs, const
     NEO_CK(ctx, cudaMemcpyAsync(dZs.p, Zs, dZs.bytes(), cudaMemcpyHostToDevice, ctx->stream));
     int rc = rlc_mix_device(ctx, rho_coeffs, dZs.p, count, m, dmix.p, drot.p);
     if (rc) return rc;
-    NEO_CK(ctx, cudaMemcpyAsync(Zmix, dmix.p, dmix.bytes(), cudaMemcpyDeviceToHost, ctx->stream));
-    NEO_CK(ctx, cudaStreamSynchronize(ctx->stream));
+    NEO_CK(ctx, ctx_d2h(ctx, Zmix, dmix.p, dmix.bytes()));
+    NEO_CK(ctx, ctx_sync(ctx));
     return NEO_OK;
 }
 
@@ -317,9 +318,9 @@ extern "C" int neo_gpu_split_b(neo_gpu_ctx* ctx, const int32_t* Zmix, uint64_t l
     int rc = split_b_device(ctx, dmix.p, len, k, b, dpl.p, dfl.p);
     if (rc) return rc;
     uint32_t flags[2];
-    NEO_CK(ctx, cudaMemcpyAsync(flags, dfl.p, 8, cudaMemcpyDeviceToHost, ctx->stream));
-    NEO_CK(ctx, cudaMemcpyAsync(planes, dpl.p, (size_t)k * len, cudaMemcpyDeviceToHost, ctx->stream));
-    NEO_CK(ctx, cudaStreamSynchronize(ctx->stream));
+    NEO_CK(ctx, ctx_d2h(ctx, flags, dfl.p, 8));
+    NEO_CK(ctx, ctx_d2h(ctx, planes, dpl.p, (size_t)k * len));
+    NEO_CK(ctx, ctx_sync(ctx));
     if (flags[0]) return ctx->fail(NEO_ERR_INVARIANT, "DEC split: entry out of range for k_rho digits");
     for (uint32_t i = 0; i < k; i++) nonzero[i] = (flags[1] >> i) & 1;
     return NEO_OK;
@@ -445,8 +446,8 @@ extern "C" int neo_gpu_me_y(neo_gpu_ctx* ctx, const neo_ccs_desc* desc, const in
     NEO_CK(ctx, cudaMemcpyAsync(dr.p, r, ell_n * 16, cudaMemcpyHostToDevice, ctx->stream));
     if ((rc = launch_chi_table(ctx, dr.p, ell_n, dchi.p))) return rc;
     if ((rc = launch_me_y(ctx, ccs, dZ.p, n_w, m, dchi.p, ell_n, b, dvj.p, dy.p, dysc.p))) return rc;
-    NEO_CK(ctx, cudaMemcpyAsync(y, dy.p, dy.bytes(), cudaMemcpyDeviceToHost, ctx->stream));
-    NEO_CK(ctx, cudaMemcpyAsync(y_scalars, dysc.p, dysc.bytes(), cudaMemcpyDeviceToHost, ctx->stream));
-    NEO_CK(ctx, cudaStreamSynchronize(ctx->stream));
+    NEO_CK(ctx, ctx_d2h(ctx, y, dy.p, dy.bytes()));
+    NEO_CK(ctx, ctx_d2h(ctx, y_scalars, dysc.p, dysc.bytes()));
+    NEO_CK(ctx, ctx_sync(ctx));
     return NEO_OK;
 }

@@ -641,8 +641,8 @@ static int bus_openings(neo_gpu_shard* sh, const int8_t* d_Z, uint32_t n_w, std:
                                                                     sh->d_busw.p, sh->d_busy.p);
     NEO_LAUNCHED(ctx);
     y.resize((size_t)n_w * nb * NEO_D);
-    NEO_CK(ctx, cudaMemcpyAsync(y.data(), sh->d_busy.p, y.size() * sizeof(K), cudaMemcpyDeviceToHost, ctx->stream));
-    NEO_CK(ctx, cudaStreamSynchronize(ctx->stream));
+    NEO_CK(ctx, ctx_d2h(ctx, y.data(), sh->d_busy.p, y.size() * sizeof(K)));
+    NEO_CK(ctx, ctx_sync(ctx));
     ysc.assign((size_t)n_w * nb, gl::kzero());
     for (size_t q = 0; q < (size_t)n_w * nb; q++) {
         K s = gl::kzero();
@@ -753,8 +753,8 @@ static int rlc_dec_lane(neo_gpu_shard* sh, const char* lane, uint32_t idx, const
         NEO_CK(ctx, cudaMemcpyAsync(sh->d_mixv.p, cv.data(), cv.size() * 8, cudaMemcpyHostToDevice, ctx->stream));
         rot_mix_kernel<<<kappa, 64, 0, ctx->stream>>>(sh->d_rot.p, k, sh->d_mixv.p, kappa, 1, sh->d_mixo.p);
         NEO_LAUNCHED(ctx);
-        NEO_CK(ctx, cudaMemcpyAsync(c_parent.data(), sh->d_mixo.p, c_parent.size() * 8, cudaMemcpyDeviceToHost, ctx->stream));
-        NEO_CK(ctx, cudaStreamSynchronize(ctx->stream));
+        NEO_CK(ctx, ctx_d2h(ctx, c_parent.data(), sh->d_mixo.p, c_parent.size() * 8));
+        NEO_CK(ctx, ctx_sync(ctx));
         std::vector<K> yv((size_t)k * t * NEO_D);
         for (uint32_t i = 0; i < k; i++)
             for (uint32_t j = 0; j < t; j++)
@@ -763,8 +763,8 @@ static int rlc_dec_lane(neo_gpu_shard* sh, const char* lane, uint32_t idx, const
         NEO_CK(ctx, cudaMemcpyAsync(sh->d_mixv.p, yv.data(), yv.size() * 16, cudaMemcpyHostToDevice, ctx->stream));
         rot_mix_kernel<<<t * 2, 64, 0, ctx->stream>>>(sh->d_rot.p, k, sh->d_mixv.p, t, 2, sh->d_mixo.p);
         NEO_LAUNCHED(ctx);
-        NEO_CK(ctx, cudaMemcpyAsync(y_parent.data(), sh->d_mixo.p, y_parent.size() * 16, cudaMemcpyDeviceToHost, ctx->stream));
-        NEO_CK(ctx, cudaStreamSynchronize(ctx->stream));
+        NEO_CK(ctx, ctx_d2h(ctx, y_parent.data(), sh->d_mixo.p, y_parent.size() * 16));
+        NEO_CK(ctx, ctx_sync(ctx));
     }
     P.insert(P.end(), c_parent.begin(), c_parent.end());
     // Pi_DEC: split into k_rho planes, commit, child claims
@@ -776,12 +776,13 @@ static int rlc_dec_lane(neo_gpu_shard* sh, const char* lane, uint32_t idx, const
     std::vector<uint64_t> cc((size_t)sh->k_rho * kappa * NEO_D);
     std::vector<K> yc((size_t)sh->k_rho * t * NEO_D);
     std::vector<int8_t> Xc((size_t)sh->k_rho * NEO_D * sh->m_in);
-    NEO_CK(ctx, cudaMemcpyAsync(flags, sh->d_flags.p, 8, cudaMemcpyDeviceToHost, ctx->stream));
-    NEO_CK(ctx, cudaMemcpyAsync(cc.data(), sh->d_commits.p, cc.size() * 8, cudaMemcpyDeviceToHost, ctx->stream));
-    NEO_CK(ctx, cudaMemcpyAsync(yc.data(), sh->d_ychild.p, yc.size() * 16, cudaMemcpyDeviceToHost, ctx->stream));
+    NEO_CK(ctx, ctx_d2h(ctx, flags, sh->d_flags.p, 8));
+    NEO_CK(ctx, ctx_d2h(ctx, cc.data(), sh->d_commits.p, cc.size() * 8));
+    NEO_CK(ctx, ctx_d2h(ctx, yc.data(), sh->d_ychild.p, yc.size() * 16));
+    if (ctx->blocking) NEO_CK(ctx, ctx_sync(ctx));
     NEO_CK(ctx, cudaMemcpy2DAsync(Xc.data(), sh->m_in, d_planes, m, sh->m_in, (size_t)sh->k_rho * NEO_D,
                                   cudaMemcpyDeviceToHost, ctx->stream));
-    NEO_CK(ctx, cudaStreamSynchronize(ctx->stream));
+    NEO_CK(ctx, ctx_sync(ctx));
     if ((rc = check_device_error(ctx))) return rc;
     if (flags[0]) return ctx->fail(NEO_ERR_INVARIANT, "DEC split: Z_mix entry out of range for k_rho digits");
     std::vector<K> by, bsc;
@@ -884,10 +885,11 @@ static int fold_step_impl(neo_gpu_shard* sh, const uint64_t* z_host, const uint6
     mcs.c.resize((size_t)kappa * NEO_D);
     std::vector<uint64_t> x(sh->m_in);
     std::vector<int8_t> Xd((size_t)NEO_D * sh->m_in);
-    NEO_CK(ctx, cudaMemcpyAsync(mcs.c.data(), sh->d_commits.p, mcs.c.size() * 8, cudaMemcpyDeviceToHost, ctx->stream));
-    NEO_CK(ctx, cudaMemcpyAsync(x.data(), d_z, sh->m_in * 8, cudaMemcpyDeviceToHost, ctx->stream));
+    NEO_CK(ctx, ctx_d2h(ctx, mcs.c.data(), sh->d_commits.p, mcs.c.size() * 8));
+    NEO_CK(ctx, ctx_d2h(ctx, x.data(), d_z, sh->m_in * 8));
+    if (ctx->blocking) NEO_CK(ctx, ctx_sync(ctx));
     NEO_CK(ctx, cudaMemcpy2DAsync(Xd.data(), sh->m_in, sh->Zall.p, m, sh->m_in, NEO_D, cudaMemcpyDeviceToHost, ctx->stream));
-    NEO_CK(ctx, cudaStreamSynchronize(ctx->stream));
+    NEO_CK(ctx, ctx_sync(ctx));
     if ((rc = check_device_error(ctx))) return rc;
     for (auto& v : x) v = gl::canon(v);
     mcs.m_in = sh->m_in;
@@ -1075,9 +1077,8 @@ static int fold_step_impl(neo_gpu_shard* sh, const uint64_t* z_host, const uint6
                 const K* has = C + (size_t)(s.col0 + s.ea) * L;
                 // has_any_lookup: any nonzero gate in this step's bus column
                 std::vector<K> hg(sh->steps);
-                NEO_CK(ctx, cudaMemcpyAsync(hg.data(), has + sh->m_in, sh->steps * sizeof(K), cudaMemcpyDeviceToHost,
-                                            ctx->stream));
-                NEO_CK(ctx, cudaStreamSynchronize(ctx->stream));
+                NEO_CK(ctx, ctx_d2h(ctx, hg.data(), has + sh->m_in, sh->steps * sizeof(K)));
+                NEO_CK(ctx, ctx_sync(ctx));
                 bool any = false;
                 for (auto& g : hg) any |= !gl::kiszero(g);
                 if (!any) {
@@ -1377,9 +1378,9 @@ static int fold_step_impl(neo_gpu_shard* sh, const uint64_t* z_host, const uint6
                               sh->d_yvsc.p)))
             return rc;
         std::vector<K> yv((size_t)nv * t * NEO_D), yvsc((size_t)nv * t);
-        NEO_CK(ctx, cudaMemcpyAsync(yv.data(), sh->d_yv.p, yv.size() * sizeof(K), cudaMemcpyDeviceToHost, ctx->stream));
-        NEO_CK(ctx, cudaMemcpyAsync(yvsc.data(), sh->d_yvsc.p, yvsc.size() * sizeof(K), cudaMemcpyDeviceToHost, ctx->stream));
-        NEO_CK(ctx, cudaStreamSynchronize(ctx->stream));
+        NEO_CK(ctx, ctx_d2h(ctx, yv.data(), sh->d_yv.p, yv.size() * sizeof(K)));
+        NEO_CK(ctx, ctx_d2h(ctx, yvsc.data(), sh->d_yvsc.p, yvsc.size() * sizeof(K)));
+        NEO_CK(ctx, ctx_sync(ctx));
         std::vector<K> vby, vbsc;
         if ((rc = bus_openings(sh, sh->valwit.p, nv, vby, vbsc))) return rc;
         for (uint32_t v = 0; v < nv; v++) {
@@ -1434,7 +1435,7 @@ static int fold_step_impl(neo_gpu_shard* sh, const uint64_t* z_host, const uint6
                                     cudaMemcpyDeviceToDevice, ctx->stream));
         NEO_CK(ctx, cudaMemcpyAsync(sh->d_prev_cols.p, sh->d_cols.p, (size_t)nb * L * sizeof(K), cudaMemcpyDeviceToDevice,
                                     ctx->stream));
-        NEO_CK(ctx, cudaStreamSynchronize(ctx->stream));
+        NEO_CK(ctx, ctx_sync(ctx));
         sh->prev_c = mcs.c;
         sh->prev_X = mcs.X;
         sh->has_prev = true;

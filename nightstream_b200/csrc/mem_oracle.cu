@@ -390,8 +390,8 @@ int mem_round_values(neo_gpu_mem_oracle* o) {
     o->hvals.assign(npts, gl::kzero());
     if (o->len == 1) {
         std::vector<K> v(o->nf);
-        NEO_CK(ctx, cudaMemcpyAsync(v.data(), o->tab[o->cur].p, o->nf * sizeof(K), cudaMemcpyDeviceToHost, ctx->stream));
-        NEO_CK(ctx, cudaStreamSynchronize(ctx->stream));
+        NEO_CK(ctx, ctx_d2h(ctx, v.data(), o->tab[o->cur].p, o->nf * sizeof(K)));
+        NEO_CK(ctx, ctx_sync(ctx));
         K val;
         if (o->bitness) {
             K s = gl::kzero();
@@ -419,8 +419,8 @@ int mem_round_values(neo_gpu_mem_oracle* o) {
     NEO_LAUNCHED(ctx);
     mem_reduce_kernel<<<npts, 256, 0, ctx->stream>>>(o->partials.p, nb, o->vals.p);
     NEO_LAUNCHED(ctx);
-    NEO_CK(ctx, cudaMemcpyAsync(o->hvals.data(), o->vals.p, npts * sizeof(K), cudaMemcpyDeviceToHost, ctx->stream));
-    NEO_CK(ctx, cudaStreamSynchronize(ctx->stream));
+    NEO_CK(ctx, ctx_d2h(ctx, o->hvals.data(), o->vals.p, npts * sizeof(K)));
+    NEO_CK(ctx, ctx_sync(ctx));
     return NEO_OK;
 }
 
@@ -591,7 +591,7 @@ int mem_create(neo_gpu_ctx* ctx, int kind, uint32_t ell, const uint64_t* r_point
         claim_out[0] = o->claim.re;
         claim_out[1] = o->claim.im;
     }
-    NEO_CK(ctx, cudaStreamSynchronize(S));
+    NEO_CK(ctx, ctx_sync(ctx));
     *out = o;
     return NEO_OK;
 }
@@ -703,8 +703,8 @@ int addr_weights_device(neo_gpu_ctx* ctx, uint32_t ell, const K* d_rcycle, uint3
     NEO_LAUNCHED(ctx);
     mem_reduce_kernel<<<1, 256, 0, S>>>(part.p, nb, out1.p);
     NEO_LAUNCHED(ctx);
-    NEO_CK(ctx, cudaMemcpyAsync(claim, out1.p, sizeof(K), cudaMemcpyDeviceToHost, S));
-    NEO_CK(ctx, cudaStreamSynchronize(S));
+    NEO_CK(ctx, ctx_d2h(ctx, claim, out1.p, sizeof(K)));
+    NEO_CK(ctx, ctx_sync(ctx));
     return NEO_OK;
 }
 
@@ -1010,8 +1010,8 @@ int ta_values(neo_gpu_twist_addr* o) {
     NEO_LAUNCHED(ctx);
     mem_reduce_kernel<<<3, 256, 0, S>>>(o->partials.p, nb, o->vals.p);
     NEO_LAUNCHED(ctx);
-    NEO_CK(ctx, cudaMemcpyAsync(o->hvals.data(), o->vals.p, 3 * sizeof(K), cudaMemcpyDeviceToHost, S));
-    NEO_CK(ctx, cudaStreamSynchronize(S));
+    NEO_CK(ctx, ctx_d2h(ctx, o->hvals.data(), o->vals.p, 3 * sizeof(K)));
+    NEO_CK(ctx, ctx_sync(ctx));
     return NEO_OK;
 }
 
@@ -1067,8 +1067,8 @@ int ta_create(neo_gpu_ctx* ctx, int kind, uint32_t ell, const uint64_t* r_cycle,
     ta_count_kernel<<<nblk, TA_T, 0, S>>>(b.hr, b.hw, L, counts.p);
     NEO_LAUNCHED(ctx);
     std::vector<uint32_t> hc(nblk);
-    NEO_CK(ctx, cudaMemcpyAsync(hc.data(), counts.p, nblk * 4, cudaMemcpyDeviceToHost, S));
-    NEO_CK(ctx, cudaStreamSynchronize(S));
+    NEO_CK(ctx, ctx_d2h(ctx, hc.data(), counts.p, nblk * 4));
+    NEO_CK(ctx, ctx_sync(ctx));
     uint64_t E = 0;
     for (auto& c : hc) { uint32_t v = c; c = (uint32_t)E; E += v; }
     o->E = (uint32_t)E;
@@ -1104,7 +1104,7 @@ int ta_create(neo_gpu_ctx* ctx, int kind, uint32_t ell, const uint64_t* r_cycle,
         NEO_LAUNCHED(ctx);
     }
     o->tab_len = P;
-    NEO_CK(ctx, cudaStreamSynchronize(S));
+    NEO_CK(ctx, ctx_sync(ctx));
     *out = o;
     return NEO_OK;
 }

@@ -203,7 +203,7 @@ __attribute__((noinline)) static void permute_impl(const Poseidon2<W>& P, uint64
     const uint64_t mu0p1 = P.mu[0] + 1;  // mu_0 < q, so no wrap
     for (int r = 0; r < RP; r++) {
         const uint64_t x = sbox7(addq(st[0], P.rc_int[r]));
-        const uint64_t sum = addq(x, rest);
+        const uint64_t sum = red128((u128)x + rest);  // both lazily reduced: add in 128 bits
         st[0] = red128((u128)mu0p1 * x + rest);
         u128 nacc = 0;
 #pragma GCC unroll 16
