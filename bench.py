@@ -263,6 +263,31 @@ def cpu_baseline(args, ccs, z, pp, mem):
 BATCH_TWIST_ELL, BATCH_SHOUT_ELL = 10, 12
 
 
+def pp_setup_result(args, ctx, m, kappa=16, reps=3):
+    """Ajtai PP generation (setup_par from a 32-byte ChaCha8 seed) on the device:
+    wall time of neo_gpu_pp_generate (host seed derivation, device sampling,
+    tensor-core tile layout), and the same PP on the C oracle (OpenMP over the
+    chunk streams).  Replaces the bench's PP for this m; run it last."""
+    seed = bytes(range(32))
+    ctx.pp_generate(seed, kappa, m, 1)  # warm-up (allocation)
+    ts = []
+    for _ in range(reps):
+        t0 = time.perf_counter()
+        ctx.pp_generate(seed, kappa, m, 1)
+        ts.append(time.perf_counter() - t0)
+    dev_ms = min(ts) * 1e3
+    canon = kappa * m * 54 * 8
+    out = {"mode": "setup_par", "kappa": kappa, "m": m, "device_ms": dev_ms,
+           "canonical_bytes": canon, "device_gbs_canonical": canon / (dev_ms * 1e-3) / 1e9}
+    if not args.no_cpu_baseline:
+        import oracle
+        t0 = time.perf_counter()
+        oracle.pp_setup(seed, kappa, m, 1)
+        cpu_s = time.perf_counter() - t0
+        out.update({"cpu_ms": cpu_s * 1e3, "cpu_cores": os.cpu_count(), "cpu_kind": "port"})
+    return out
+
+
 def shard_mix(n_shards, lo, hi, seed, memory=True):
     """n_shards synthetic shards with log2(n) uniform in [lo, hi]; with memory,
     each carries a Twist memory of 2^10 cells and a 2^12-entry Shout table on
@@ -506,6 +531,7 @@ def run_ours(args, rank, world, local_rank):
                                          "(profiles/commit_tc_kernel_m16384_12planes.md)",
                        "launch_ms": commit_ms, "peak_source": peak_src, "algorithmic_ops_per_launch": ops}
     roofline = rounds_roofline(ctx, ccs, z, args.ell, stream)
+    pp_setup = pp_setup_result(args, ctx, m) if rank == 0 else None
 
     if rank == 0:
         out = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -513,6 +539,7 @@ def run_ours(args, rank, world, local_rank):
                "vs_baseline": None, "dtype": "u64 (F_q, K = F_q^2), int8 digits", "data": "synthetic",
                "config": config(args), "e2e": e2e, "gpu_launches": int(launches), "clocks": clk,
                "roofline": roofline, "roofline_commit": roofline_commit, "step_breakdown_ms": stats}
+        out["pp_setup"] = pp_setup
         if world == 1 and not args.no_cpu_baseline:
             out["cpu_baseline"] = cpu_baseline(args, ccs, z, pp, mem)
         if world == 1 and not args.no_batch:

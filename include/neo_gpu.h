@@ -67,6 +67,32 @@ int neo_gpu_synchronize(neo_gpu_ctx* ctx);
  * (crates/neo-ajtai/src/s_module.rs:23-222, types.rs:7-16). */
 int neo_gpu_pp_upload(neo_gpu_ctx* ctx, uint32_t kappa, uint64_t m, const uint64_t* coeffs);
 
+/* Generate M on the device from a 32-byte ChaCha8 seed and register it like
+ * neo_gpu_pp_upload.  mode NEO_PP_SETUP: setup(ChaCha8Rng::from_seed(seed),
+ * 54, kappa, m) -- one stream, coefficient order [kappa][m][54]
+ * (crates/neo-ajtai/src/commit.rs:133-157; FoldingSession::new_ajtai_seeded,
+ * crates/neo-fold/src/session.rs:1938-1951).  mode NEO_PP_SETUP_PAR:
+ * setup_par(ChaCha8Rng::from_seed(seed), 54, kappa, m) -- kappa row seeds,
+ * per row one seed per chunk of min(m, 2^15).max(1024) columns
+ * (commit.rs:159-225; seeded_pp_chunk_seeds, commit.rs:227-264;
+ * FoldingSession::new_ajtai, session.rs:1915-1931).  Coefficients are drawn by
+ * rejection (x < q) as sample_uniform_fq (commit.rs:21-30). */
+#define NEO_PP_SETUP 0
+#define NEO_PP_SETUP_PAR 1
+int neo_gpu_pp_generate(neo_gpu_ctx* ctx, const uint8_t* seed32, uint32_t kappa, uint64_t m, int mode);
+
+/* Copy words [first, first + count) of the registered PP of this m (layout
+ * [kappa][m][54], word (i*m + j)*54 + s) back to the host. */
+int neo_gpu_pp_download(neo_gpu_ctx* ctx, uint64_t m, uint64_t first, uint64_t count, uint64_t* out);
+
+/* The sampler under neo_gpu_pp_generate: for each stream s (ChaCha8Rng seeded
+ * with seeds[32*s .. 32*s+32]), the first counts[s] values x < bound of its
+ * next_u64() sequence, concatenated into out.  bound = q is
+ * sample_uniform_fq (crates/neo-ajtai/src/commit.rs:21-30); other bounds
+ * exercise the rejection path. */
+int neo_gpu_chacha8_sample(neo_gpu_ctx* ctx, const uint8_t* seeds, uint32_t n_streams, const uint64_t* counts,
+                           uint64_t bound, uint64_t* out);
+
 /* c = cf(M cf^{-1}(Z)) for n_vec digit matrices at once.
  * digits[(v*54 + r)*m + j] = Z_v[r][j] (row-major d x m, values in [-128,127]);
  * out[(v*kappa + i)*54 + r] = Commitment.data[i*54 + r] (column-major d x kappa,

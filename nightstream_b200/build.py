@@ -10,7 +10,7 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libneo_gpu.so")
-SOURCES = ["core.cu", "commit.cu", "commit_tc.cu", "ccs_oracle.cu", "fold.cu", "batch.cu", "mem_oracle.cu", "transcript.cpp", "transcript_capi.cpp"]
+SOURCES = ["core.cu", "commit.cu", "commit_tc.cu", "ccs_oracle.cu", "fold.cu", "batch.cu", "mem_oracle.cu", "pp_gen.cu", "transcript.cpp", "transcript_capi.cpp"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",

@@ -97,7 +97,7 @@ PPEntry* pp_lookup(int device, uint64_t m) {
 
 int launch_commit(neo_gpu_ctx* ctx, const int8_t* d_digits, uint32_t n_vec, uint64_t m, uint64_t* d_out) {
     PPEntry* pp = pp_lookup(ctx->device, m);
-    if (!pp) return ctx->fail(NEO_ERR_ARG, "commit: PP not loaded for this m");
+    if (!pp || !pp->kappa) return ctx->fail(NEO_ERR_ARG, "commit: PP not loaded for this m");
     if (pp->d_pp_limbs) {
         // tensor-core path (commit_tc.cu)
         uint32_t g, k, kb;
@@ -125,12 +125,11 @@ int launch_commit(neo_gpu_ctx* ctx, const int8_t* d_digits, uint32_t n_vec, uint
     return NEO_OK;
 }
 
-extern "C" int neo_gpu_pp_upload(neo_gpu_ctx* ctx, uint32_t kappa, uint64_t m, const uint64_t* coeffs) {
-    if (!ctx) return NEO_ERR_ARG;
-    if (!coeffs || kappa == 0 || m == 0 || kappa > 64) return ctx->fail(NEO_ERR_ARG, "pp_upload: bad args");
-    cudaSetDevice(ctx->device);
-    NEO_CK(ctx, ctx_sync(ctx));
-    std::lock_guard<std::mutex> lk(g_pp_mu);  // uploads are serialized; replacing a PP in use races (documented)
+std::mutex& pp_mutex() { return g_pp_mu; }
+
+// Registry slot for (ctx->device, m) with d_pp sized for kappa (caller holds
+// pp_mutex()).  The tensor-core tiles of a previous PP are dropped.
+int pp_slot(neo_gpu_ctx* ctx, uint32_t kappa, uint64_t m, PPEntry** out) {
     PPEntry*& slot = g_pp[{ctx->device, m}];
     if (!slot) {
         slot = new PPEntry();
@@ -139,13 +138,47 @@ extern "C" int neo_gpu_pp_upload(neo_gpu_ctx* ctx, uint32_t kappa, uint64_t m, c
     }
     PPEntry* pp = slot;
     const size_t n = (size_t)kappa * m * NEO_D;
-    if (pp->d_pp && pp->kappa != kappa) { cudaFree(pp->d_pp); pp->d_pp = nullptr; }
+    if (pp->d_pp && pp->kappa != kappa) { cudaFree(pp->d_pp); pp->d_pp = nullptr; pp->kappa = 0; }
     if (!pp->d_pp) NEO_CK(ctx, cudaMalloc(&pp->d_pp, n * 8));
-    NEO_CK(ctx, cudaMemcpy(pp->d_pp, coeffs, n * 8, cudaMemcpyHostToDevice));
-    pp->kappa = kappa;
     if (pp->d_pp_limbs) { cudaFree(pp->d_pp_limbs); pp->d_pp_limbs = nullptr; }
-    // tensor-core layout of the PP (byte limbs, pre-swizzled tiles) when the shape allows it
-    if (kappa <= 16 && m % 2 == 0) return tc_pp_prepare(ctx, pp);
+    *out = pp;
+    return NEO_OK;
+}
+
+// After d_pp holds the new PP: record kappa and build the tensor-core layout
+// (byte limbs, pre-swizzled tiles) when the shape allows it.
+int pp_finish(neo_gpu_ctx* ctx, PPEntry* pp, uint32_t kappa) {
+    pp->kappa = kappa;
+    if (kappa <= 16 && pp->m % 2 == 0) return tc_pp_prepare(ctx, pp);
+    return NEO_OK;
+}
+
+extern "C" int neo_gpu_pp_upload(neo_gpu_ctx* ctx, uint32_t kappa, uint64_t m, const uint64_t* coeffs) {
+    if (!ctx) return NEO_ERR_ARG;
+    if (!coeffs || kappa == 0 || m == 0 || kappa > 64) return ctx->fail(NEO_ERR_ARG, "pp_upload: bad args");
+    cudaSetDevice(ctx->device);
+    NEO_CK(ctx, ctx_sync(ctx));
+    std::lock_guard<std::mutex> lk(g_pp_mu);  // uploads are serialized; replacing a PP in use races (documented)
+    PPEntry* pp = nullptr;
+    int rc = pp_slot(ctx, kappa, m, &pp);
+    if (rc) return rc;
+    NEO_CK(ctx, cudaMemcpy(pp->d_pp, coeffs, (size_t)kappa * m * NEO_D * 8, cudaMemcpyHostToDevice));
+    return pp_finish(ctx, pp, kappa);
+}
+
+extern "C" int neo_gpu_pp_download(neo_gpu_ctx* ctx, uint64_t m, uint64_t first, uint64_t count, uint64_t* out) {
+    if (!ctx) return NEO_ERR_ARG;
+    if ((!out && count) || m == 0) return ctx->fail(NEO_ERR_ARG, "pp_download: bad args");
+    cudaSetDevice(ctx->device);
+    std::lock_guard<std::mutex> lk(g_pp_mu);
+    PPEntry* pp = nullptr;
+    auto it = g_pp.find({ctx->device, m});
+    if (it != g_pp.end()) pp = it->second;
+    if (!pp || !pp->d_pp || !pp->kappa) return ctx->fail(NEO_ERR_ARG, "pp_download: PP not loaded for this m");
+    const uint64_t total = (uint64_t)pp->kappa * m * NEO_D;
+    if (first > total || count > total - first) return ctx->fail(NEO_ERR_ARG, "pp_download: range outside the PP");
+    NEO_CK(ctx, ctx_sync(ctx));
+    if (count) NEO_CK(ctx, cudaMemcpy(out, pp->d_pp + first, count * 8, cudaMemcpyDeviceToHost));
     return NEO_OK;
 }
 
@@ -154,7 +187,7 @@ extern "C" int neo_gpu_commit(neo_gpu_ctx* ctx, const int8_t* digits, uint32_t n
     if (!digits || !out || n_vec == 0 || m == 0) return ctx->fail(NEO_ERR_ARG, "commit: bad args");
     cudaSetDevice(ctx->device);
     PPEntry* pp = pp_lookup(ctx->device, m);
-    if (!pp) return ctx->fail(NEO_ERR_ARG, "commit: PP not loaded for this m");
+    if (!pp || !pp->kappa) return ctx->fail(NEO_ERR_ARG, "commit: PP not loaded for this m");
     DevBuf<int8_t> dZ;
     DevBuf<uint64_t> dout;
     NEO_CK(ctx, dZ.alloc((size_t)n_vec * NEO_D * m));

@@ -93,6 +93,11 @@ struct PPEntry {
     uint8_t* d_pp_limbs = nullptr;  // tensor-core tiles: [m/2][128 rows][128 B], pre-swizzled
 };
 PPEntry* pp_lookup(int device, uint64_t m);
+// PP registry writes (commit.cu): pp_slot / pp_finish are called with pp_mutex() held
+#include <mutex>
+std::mutex& pp_mutex();
+int pp_slot(neo_gpu_ctx* ctx, uint32_t kappa, uint64_t m, PPEntry** out);
+int pp_finish(neo_gpu_ctx* ctx, PPEntry* pp, uint32_t kappa);
 
 // Owning device buffer (freed on scope exit).
 template <typename T>

@@ -29,6 +29,9 @@ SIGNATURES = {
     "neo_gpu_last_error": [P],
     "neo_gpu_kernel_launches": [P],
     "neo_gpu_pp_upload": [P, U32, U64, P],
+    "neo_gpu_pp_generate": [P, P, U32, U64, I],
+    "neo_gpu_pp_download": [P, U64, U64, U64, P],
+    "neo_gpu_chacha8_sample": [P, P, U32, P, U64, P],
     "neo_gpu_commit": [P, P, U32, U64, P],
     "neo_gpu_decomp_b2": [P, P, U64, P],
     "neo_gpu_rlc_mix": [P, P, P, U32, U64, P],
@@ -187,6 +190,37 @@ class Context:
         assert d == 54
         self.check(self.lib.neo_gpu_pp_upload(self.h, kappa, m, _p(pp)))
         self.kappa, self.m = kappa, m
+
+    PP_SETUP, PP_SETUP_PAR = 0, 1
+
+    def pp_generate(self, seed: bytes, kappa: int, m: int, mode: int = 1):
+        """Generate and register M on the device: mode 0 = setup, 1 = setup_par,
+        both from ChaCha8Rng::from_seed(seed)."""
+        if len(seed) != 32:
+            raise ValueError("seed must be 32 bytes")
+        sb = np.frombuffer(bytes(seed), np.uint8).copy()
+        self.check(self.lib.neo_gpu_pp_generate(self.h, _p(sb), kappa, m, mode))
+        self.kappa, self.m = kappa, m
+
+    def pp_download(self, m: int = None, kappa: int = None, first: int = 0, count: int = None) -> np.ndarray:
+        """Words [first, first + count) of the registered PP of this m; the whole
+        [kappa][m][54] array by default."""
+        m = self.m if m is None else m
+        kappa = self.kappa if kappa is None else kappa
+        whole = count is None
+        if whole:
+            count = kappa * m * 54 - first
+        out = np.empty(count, np.uint64)
+        self.check(self.lib.neo_gpu_pp_download(self.h, m, first, count, _p(out)))
+        return out.reshape(kappa, m, 54) if whole and first == 0 else out
+
+    def chacha8_sample(self, seeds, counts, bound: int) -> np.ndarray:
+        """Per 32-byte seed, the first counts[s] ChaCha8 next_u64() values < bound."""
+        sb = np.frombuffer(b"".join(bytes(x) for x in seeds), np.uint8).copy()
+        counts = _u64(counts)
+        out = np.empty(int(counts.sum()), np.uint64)
+        self.check(self.lib.neo_gpu_chacha8_sample(self.h, _p(sb), len(counts), _p(counts), int(bound), _p(out)))
+        return out
 
     def commit(self, digits: np.ndarray) -> np.ndarray:
         """digits [n_vec][54][m] (or [54][m]) -> commitments [n_vec][kappa][54]."""

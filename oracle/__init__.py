@@ -57,6 +57,8 @@ def lib():
             "or_me_y_at_r": [P, P, I, P, I, P, P],
             "or_poseidon2_permute": [P],
             "or_poseidon2_w16_permute": [P],
+            "or_chacha8_sample": [P, ctypes.c_uint32, P, ctypes.c_uint64, P],
+            "or_pp_setup": [P, ctypes.c_uint32, ctypes.c_uint64, I, P],
             "or_ccs_digest": [P, P],
             "or_tr_new": [ctypes.c_char_p],
             "or_tr_free": [P],
@@ -331,6 +333,26 @@ class Transcript:
         out = np.empty(8, np.uint64)
         lib().or_tr_state(self.h, out.ctypes.data)
         return out
+
+
+def chacha8_sample(seeds, counts, bound):
+    """Per stream (32-byte ChaCha8 seed) the first counts[s] next_u64() values
+    < bound (sample_uniform_fq for bound = q, crates/neo-ajtai/src/commit.rs:21-30)."""
+    seeds = np.ascontiguousarray(np.frombuffer(b"".join(seeds), np.uint8))
+    counts = u64(counts)
+    out = np.empty(int(counts.sum()), np.uint64)
+    lib().or_chacha8_sample(ptr(seeds), len(counts), ptr(counts), int(bound), ptr(out))
+    return out
+
+
+def pp_setup(seed: bytes, kappa: int, m: int, mode: int):
+    """Ajtai setup (mode 0, commit.rs:133-157) / setup_par (mode 1, commit.rs:159-225)
+    with ChaCha8Rng::from_seed(seed): PP as uint64 [kappa][m][54]."""
+    assert len(seed) == 32
+    sb = np.frombuffer(seed, np.uint8).copy()
+    out = np.empty((kappa, m, 54), np.uint64)
+    lib().or_pp_setup(ptr(sb), kappa, m, mode, ptr(out))
+    return out
 
 
 def ccs_digest(ccs):

@@ -1099,6 +1099,75 @@ static uint64_t cc_u64(or_chacha* c) {
     return lo | (hi << 32);
 }
 
+/* rand_core fill_bytes over a u32 block stream: whole words, little endian
+   (a partial last word is consumed). */
+static void cc_fill(or_chacha* c, uint8_t* out, size_t n) {
+    size_t i = 0;
+    while (i < n) {
+        if (c->idx >= 16) cc_refill(c);
+        uint32_t w = c->blk[c->idx++];
+        for (int b = 0; b < 4 && i < n; b++, i++) out[i] = (uint8_t)(w >> (8 * b));
+    }
+}
+static void cc_init(or_chacha* c, const uint8_t* seed) {
+    for (int i = 0; i < 8; i++)
+        c->key[i] = (uint32_t)seed[4*i] | ((uint32_t)seed[4*i+1] << 8) | ((uint32_t)seed[4*i+2] << 16) |
+                    ((uint32_t)seed[4*i+3] << 24);
+    c->ctr = 0; c->idx = 16;
+}
+
+/* sample_uniform_fq generalised to any bound (commit.rs:21-30): per stream the
+   first counts[s] next_u64() values < bound, concatenated into out. */
+void or_chacha8_sample(const uint8_t* seeds, uint32_t n_streams, const uint64_t* counts, uint64_t bound,
+                       uint64_t* out) {
+    uint64_t* offs = (uint64_t*)malloc(sizeof(uint64_t) * (n_streams + 1));
+    offs[0] = 0;
+    for (uint32_t s = 0; s < n_streams; s++) offs[s + 1] = offs[s] + counts[s];
+#pragma omp parallel for schedule(dynamic, 1)
+    for (int64_t s = 0; s < (int64_t)n_streams; s++) {
+        or_chacha c;
+        cc_init(&c, seeds + 32 * s);
+        uint64_t* o = out + offs[s];
+        for (uint64_t i = 0; i < counts[s]; i++) {
+            uint64_t x;
+            do { x = cc_u64(&c); } while (x >= bound);
+            o[i] = x;
+        }
+    }
+    free(offs);
+}
+
+/* Ajtai setup (commit.rs:133-157, mode 0) and setup_par (commit.rs:159-225,
+   mode 1) with rng = ChaCha8Rng::from_seed(seed): out[(i*m + j)*54 + s]. */
+void or_pp_setup(const uint8_t* seed, uint32_t kappa, uint64_t m, int mode, uint64_t* out) {
+    if (mode == 0) {
+        uint64_t n = (uint64_t)kappa * m * 54;
+        or_chacha8_sample(seed, 1, &n, Q, out);
+        return;
+    }
+    uint64_t chunk = m < (1u << 15) ? m : (1u << 15);
+    if (chunk < 1024) chunk = 1024;
+    uint64_t n_chunks = (m + chunk - 1) / chunk;
+    uint8_t* seeds = (uint8_t*)malloc(32 * (size_t)kappa * n_chunks);
+    uint64_t* counts = (uint64_t*)malloc(8 * (size_t)kappa * n_chunks);
+    uint8_t* rows = (uint8_t*)malloc(32 * (size_t)kappa);
+    or_chacha master;
+    cc_init(&master, seed);
+    for (uint32_t i = 0; i < kappa; i++) cc_fill(&master, rows + 32 * i, 32);
+    for (uint32_t i = 0; i < kappa; i++) {
+        or_chacha rr;
+        cc_init(&rr, rows + 32 * i);
+        for (uint64_t c = 0; c < n_chunks; c++) {
+            cc_fill(&rr, seeds + 32 * (i * n_chunks + c), 32);
+            uint64_t lo = c * chunk, hi = lo + chunk < m ? lo + chunk : m;
+            counts[i * n_chunks + c] = (hi - lo) * 54;
+        }
+    }
+    /* streams in (row, chunk) order are contiguous in the [kappa][m][54] layout */
+    or_chacha8_sample(seeds, (uint32_t)(kappa * n_chunks), counts, Q, out);
+    free(seeds); free(counts); free(rows);
+}
+
 static uint64_t P2_RCE[8][8], P2_RCI[22], P2_MU[8];
 static int p2_ready = 0;
 static void p2_init(void) {

@@ -119,6 +119,11 @@ void or_tr_challenge_fields(or_transcript* t, const char* label, size_t n, uint6
 void or_tr_digest32(or_transcript* t, uint8_t* out);
 void or_tr_state(const or_transcript* t, uint64_t* out);
 void or_poseidon2_w16_permute(uint64_t* st);
+
+/* Ajtai PP generation from ChaCha8 (crates/neo-ajtai/src/commit.rs:21-264) */
+void or_chacha8_sample(const uint8_t* seeds, uint32_t n_streams, const uint64_t* counts, uint64_t bound,
+                       uint64_t* out);
+void or_pp_setup(const uint8_t* seed, uint32_t kappa, uint64_t m, int mode, uint64_t* out);
 void or_ccs_digest(const or_ccs* s, uint64_t* out4);
 
 

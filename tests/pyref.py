@@ -179,3 +179,66 @@ def _ksum(it):
     for v in it:
         acc = kadd(acc, v)
     return acc
+
+
+class ChaCha8:
+    """ChaCha with 8 rounds as a counter-mode u32 stream (RFC 7539 block layout:
+    constants, 8 key words, 64-bit block counter in words 12-13, zero nonce)."""
+
+    M = 0xFFFFFFFF
+
+    def __init__(self, seed: bytes):
+        assert len(seed) == 32
+        self.key = [int.from_bytes(seed[4 * i:4 * i + 4], "little") for i in range(8)]
+        self.ctr = 0
+        self.buf = []
+
+    @staticmethod
+    def _rot(x, n):
+        return ((x << n) | (x >> (32 - n))) & ChaCha8.M
+
+    def _block(self):
+        s = [0x61707865, 0x3320646E, 0x79622D32, 0x6B206574] + self.key + [self.ctr & self.M, self.ctr >> 32, 0, 0]
+        x = list(s)
+
+        def qr(a, b, c, d):
+            x[a] = (x[a] + x[b]) & self.M; x[d] = self._rot(x[d] ^ x[a], 16)
+            x[c] = (x[c] + x[d]) & self.M; x[b] = self._rot(x[b] ^ x[c], 12)
+            x[a] = (x[a] + x[b]) & self.M; x[d] = self._rot(x[d] ^ x[a], 8)
+            x[c] = (x[c] + x[d]) & self.M; x[b] = self._rot(x[b] ^ x[c], 7)
+
+        for _ in range(4):
+            qr(0, 4, 8, 12); qr(1, 5, 9, 13); qr(2, 6, 10, 14); qr(3, 7, 11, 15)
+            qr(0, 5, 10, 15); qr(1, 6, 11, 12); qr(2, 7, 8, 13); qr(3, 4, 9, 14)
+        self.ctr += 1
+        self.buf = [(a + b) & self.M for a, b in zip(x, s)]
+
+    def next_u32(self):
+        if not self.buf:
+            self._block()
+        return self.buf.pop(0)
+
+    def next_u64(self):
+        lo = self.next_u32()
+        return lo | (self.next_u32() << 32)
+
+    def fill_bytes(self, n):
+        out = b""
+        while len(out) < n:
+            out += self.next_u32().to_bytes(4, "little")
+        return out[:n]
+
+
+def pp_par_streams(seed: bytes, kappa: int, m: int):
+    """setup_par partition: [(chunk seed, first column, columns)] in (row, chunk) order."""
+    chunk = max(min(m, 1 << 15), 1024)
+    n_chunks = (m + chunk - 1) // chunk
+    master = ChaCha8(seed)
+    rows = [master.fill_bytes(32) for _ in range(kappa)]
+    out = []
+    for rs in rows:
+        r = ChaCha8(rs)
+        for c in range(n_chunks):
+            lo = c * chunk
+            out.append((r.fill_bytes(32), lo, min(m, lo + chunk) - lo))
+    return out
