@@ -98,7 +98,7 @@ PPEntry* pp_lookup(int device, uint64_t m) {
 int launch_commit(neo_gpu_ctx* ctx, const int8_t* d_digits, uint32_t n_vec, uint64_t m, uint64_t* d_out) {
     PPEntry* pp = pp_lookup(ctx->device, m);
     if (!pp || !pp->kappa) return ctx->fail(NEO_ERR_ARG, "commit: PP not loaded for this m");
-    if (pp->d_pp_limbs) {
+    if (pp->tc) {
         // tensor-core path (commit_tc.cu)
         uint32_t g, k, kb;
         size_t need = tc_scratch_bytes(n_vec, m, &g, &k, &kb);
@@ -140,7 +140,7 @@ int pp_slot(neo_gpu_ctx* ctx, uint32_t kappa, uint64_t m, PPEntry** out) {
     const size_t n = (size_t)kappa * m * NEO_D;
     if (pp->d_pp && pp->kappa != kappa) { cudaFree(pp->d_pp); pp->d_pp = nullptr; pp->kappa = 0; }
     if (!pp->d_pp) NEO_CK(ctx, cudaMalloc(&pp->d_pp, n * 8));
-    if (pp->d_pp_limbs) { cudaFree(pp->d_pp_limbs); pp->d_pp_limbs = nullptr; }
+    pp->tc = false;  // the tiles (kept allocated: their size depends on m only) are rebuilt by pp_finish
     *out = pp;
     return NEO_OK;
 }
@@ -150,6 +150,7 @@ int pp_slot(neo_gpu_ctx* ctx, uint32_t kappa, uint64_t m, PPEntry** out) {
 int pp_finish(neo_gpu_ctx* ctx, PPEntry* pp, uint32_t kappa) {
     pp->kappa = kappa;
     if (kappa <= 16 && pp->m % 2 == 0) return tc_pp_prepare(ctx, pp);
+    if (pp->d_pp_limbs) { cudaFree(pp->d_pp_limbs); pp->d_pp_limbs = nullptr; }
     return NEO_OK;
 }
 

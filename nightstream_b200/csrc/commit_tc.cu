@@ -385,13 +385,14 @@ __global__ void commit_tc_reduce_kernel(const int32_t* __restrict__ partial, uin
 int tc_pp_prepare(neo_gpu_ctx* ctx, PPEntry* pp) {
     if (pp->kappa * 8 > 128) return ctx->fail(NEO_ERR_UNSUPPORTED, "tensor-core commit: kappa <= 16");
     if (pp->m % 2) return ctx->fail(NEO_ERR_UNSUPPORTED, "tensor-core commit: m must be even");
-    if (pp->d_pp_limbs) { cudaFree(pp->d_pp_limbs); pp->d_pp_limbs = nullptr; }
+    pp->tc = false;
     const uint64_t n_kb = pp->m / 2;
-    NEO_CK(ctx, cudaMalloc(&pp->d_pp_limbs, n_kb * TC_A_BYTES));
+    if (!pp->d_pp_limbs) NEO_CK(ctx, cudaMalloc(&pp->d_pp_limbs, n_kb * TC_A_BYTES));  // size depends on m only
     const uint64_t threads = n_kb * 128 * 8;
     pp_limbs_kernel<<<ceil_div(threads, 256), 256, 0, ctx->stream>>>(pp->d_pp, pp->kappa, pp->m, pp->d_pp_limbs);
     NEO_LAUNCHED(ctx);
     NEO_CK(ctx, ctx_sync(ctx));
+    pp->tc = true;
     return NEO_OK;
 }
 

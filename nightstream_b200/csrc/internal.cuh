@@ -91,6 +91,7 @@ struct PPEntry {
     uint32_t kappa = 0;
     uint64_t* d_pp = nullptr;       // [kappa][m][54] canonical u64
     uint8_t* d_pp_limbs = nullptr;  // tensor-core tiles: [m/2][128 rows][128 B], pre-swizzled
+    bool tc = false;                // d_pp_limbs holds the tiles of the current d_pp
 };
 PPEntry* pp_lookup(int device, uint64_t m);
 // PP registry writes (commit.cu): pp_slot / pp_finish are called with pp_mutex() held
