@@ -18,23 +18,35 @@
 //
 // A tiles are stored in HBM already in the 128B-swizzled K-major UMMA layout
 // (16 KB per K block, contiguous) and fetched with one cp.async.bulk each.
-// B tiles are built in shared memory by 4 warps: row (v,r) of K block kb is
-// F_{v,j}[80 - r + s] for s in [0,64), a contiguous window of the 144-byte
-// sequence F_{v,j}[w] = z_{v,j}[(80 - w) mod 81] precomputed per column.
+//
+// B is never materialised row by row.  With F_{v,j}[w] = z_{v,j}[(80 - w) mod 81]
+// (160 bytes per column, precomputed) the B row of output r is the window
+// F[r' + s], s < 64, with r' = 80 - r.  Writing r' = 16a + 8h + b, that window
+// is the 16-byte-aligned chunks a + k (k < 4) of the phase sequence
+// G_p[x] = F[x + p], p = 8h + b.  So the builders write, per column, the 16
+// phase sequences as 9 chunks of 16 bytes laid out [chunk][h][v][b] (9 KB),
+// and a no-swizzle K-major descriptor with 8-row-group stride 128 B and
+// K-chunk stride NV*256 B walks all rows (a, h, v, b) of all NV vectors: row
+// group g = (2a + h) NV + v sits at g*128 and its K chunk k at
+// (a + k) NV 256 = g-part + k*LBO.  Rows r' < 88 per vector (44 groups,
+// N = 256 + 96); r' in [81, 88) are computed and discarded.
 #include "internal.cuh"
 
 namespace {
 
 constexpr int TC_NV = 4;                    // vectors per CTA
-constexpr int TC_NROWS = TC_NV * 81;        // 324 B rows used
-constexpr int TC_NPAD = 336;                // MMA N total (multiple of 16, atoms of 8)
-constexpr int TC_N0 = 256, TC_N1 = TC_NPAD - 256;  // two MMAs per K step
+constexpr int TC_NPAD = 352;                // MMA N total: 44 groups of 8 rows, r' < 88 per vector
+constexpr int TC_N0 = 256, TC_N1 = TC_NPAD - 256;  // two MMAs per K step (N = 256, 96)
 constexpr int TC_ASTAGES = 6;               // A tiles + F sequences ring (bulk copies run ahead)
-constexpr int TC_BSTAGES = 2;               // B tiles ring (built by threads, overlaps MMA)
+constexpr int TC_BSTAGES = 4;               // B phase buffers ring (built by threads, overlaps MMA)
 constexpr int TC_A_BYTES = 128 * 128;       // 16 KB
-constexpr int TC_B_BYTES = TC_NPAD * 128;   // 42 KB
-constexpr int TC_FBYTES = 144;              // F sequence length (9 x 16 B)
-constexpr int TC_F_STAGE = 1280;            // NV x 2 columns x 144 B, padded (window reads overrun by 4 B)
+constexpr int TC_BCHUNKS = 9;               // 16-byte K chunks per column: a + k, a <= 5, k < 4
+constexpr int TC_BCOL_BYTES = TC_BCHUNKS * TC_NV * 256;  // [chunk][h][v][b][16 B] = 9 KB per column
+constexpr int TC_B_BYTES = 2 * TC_BCOL_BYTES;            // two columns per K block: 18 KB
+constexpr int TC_BLBO = TC_NV * 256;        // K-direction core-matrix stride (bytes)
+constexpr int TC_BSBO = 128;                // N-direction 8-row-group stride (bytes)
+constexpr int TC_FBYTES = 160;              // F sequence length (10 x 16 B)
+constexpr int TC_F_STAGE = TC_NV * 2 * TC_FBYTES;  // NV x 2 columns x 160 B
 constexpr int TC_SMEM_BYTES = TC_ASTAGES * (TC_A_BYTES + TC_F_STAGE) + TC_BSTAGES * TC_B_BYTES;
 constexpr int TC_BUILDERS = 256;            // 8 builder warps
 constexpr int TC_THREADS = 64 + TC_BUILDERS;  // warp0 producer, warp1 MMA, warps2-9 B build (2-5 epilogue)
@@ -43,8 +55,8 @@ constexpr uint32_t TC_SPIN_LIMIT = 1u << 22;  // ~0.3 s with the back-off below
 
 static_assert(TC_B_BYTES % 1024 == 0 && TC_A_BYTES % 1024 == 0, "stage buffers stay 1024-byte aligned");
 static_assert(TC_SMEM_BYTES + 1024 + 256 <= 232448, "shared memory budget");
-static_assert(TC_NV * 2 * TC_FBYTES + 16 <= TC_F_STAGE, "F staging holds the window overrun");
 static_assert(TC_NPAD % 16 == 0 && TC_N1 % 16 == 0 && TC_N1 >= 16, "MMA N constraints (M=128)");
+static_assert(TC_N0 == 32 * 8, "the first MMA covers row groups 0..31");
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
     return static_cast<uint32_t>(__cvta_generic_to_shared(p));
@@ -95,6 +107,17 @@ __device__ __forceinline__ uint64_t sw128_desc(uint32_t saddr) {
     return d;
 }
 
+// UMMA shared-memory descriptor: K-major, no swizzle: 8-row x 16-byte core
+// matrices, LBO between core matrices along K, SBO between 8-row groups.
+__device__ __forceinline__ uint64_t ns_desc(uint32_t saddr) {
+    uint64_t d = 0;
+    d |= (uint64_t)((saddr >> 4) & 0x3FFF);
+    d |= (uint64_t)((TC_BLBO >> 4) & 0x3FFF) << 16;
+    d |= (uint64_t)((TC_BSBO >> 4) & 0x3FFF) << 32;
+    d |= (uint64_t)1 << 46;  // descriptor version (sm_100); layout bits 61-63 = 0: no swizzle
+    return d;
+}
+
 // instruction descriptor: kind::i8, D = s32, A = u8 (K-major), B = s8 (K-major), M = 128
 __host__ __device__ constexpr uint32_t idesc_i8(int n) {
     return (2u << 4)            // c_format = S32
@@ -119,30 +142,40 @@ __device__ __forceinline__ void mma_commit(uint64_t* bar) {
 // ---------------------------------------------------------------------------
 // prep: PP -> pre-swizzled u8 limb tiles  PPL[kb][row][128 B]
 // ---------------------------------------------------------------------------
-__global__ void pp_limbs_kernel(const uint64_t* __restrict__ pp, uint32_t kappa, uint64_t m, uint8_t* __restrict__ ppl) {
-    // one thread per (kb, row, 16-byte chunk)
-    const uint64_t n_kb = m / 2;
-    const uint64_t tid = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
-    if (tid >= n_kb * 128 * 8) return;
-    const uint32_t c = tid & 7, row = (tid >> 3) & 127;
-    const uint64_t kb = tid >> 10;
-    const uint32_t i = row >> 3, l = row & 7;
-    uint8_t out[16];
+// One CTA per K block kb (columns 2kb, 2kb+1): thread (i, jj, g) loads the 8
+// coefficients s = 8g..8g+7 of M[i][2kb+jj] (one coalesced 64-byte run),
+// splits them into 8 byte planes l and stores each 8-byte piece at row
+// (i, l), K offset 64 jj + 8g of the swizzled tile in shared memory; the
+// 16 KB tile then goes out as 1024 contiguous 16-byte stores.
+__global__ void __launch_bounds__(256) pp_limbs_kernel(const uint64_t* __restrict__ pp, uint32_t kappa, uint64_t m,
+                                                       uint8_t* __restrict__ ppl) {
+    __shared__ __align__(16) uint8_t tile[TC_A_BYTES];
+    const uint64_t kb = blockIdx.x;
+    const uint32_t t = threadIdx.x;
+    const uint32_t i = t >> 4, jj = (t >> 3) & 1, g = t & 7;
+    uint64_t w[8];
 #pragma unroll
-    for (int b = 0; b < 16; b++) {
-        uint32_t k = c * 16 + b;
-        uint64_t j = kb * 2 + (k >> 6);
-        uint32_t s = k & 63;
-        uint8_t v = 0;
-        if (i < kappa && s < NEO_D) v = (uint8_t)(pp[((uint64_t)i * m + j) * NEO_D + s] >> (8 * l));
-        out[b] = v;
+    for (int e = 0; e < 8; e++) {
+        const uint32_t s_ = g * 8 + e;
+        w[e] = (i < kappa && s_ < NEO_D) ? pp[((uint64_t)i * m + kb * 2 + jj) * NEO_D + s_] : 0;
     }
-    uint32_t p = c ^ (row & 7);
-    uint4* dst = reinterpret_cast<uint4*>(ppl + kb * TC_A_BYTES + row * 128 + p * 16);
-    *dst = *reinterpret_cast<uint4*>(out);
+    const uint32_t k = jj * 64 + g * 8;  // K byte offset of this 8-byte piece
+#pragma unroll
+    for (int l = 0; l < 8; l++) {
+        uint64_t v = 0;
+#pragma unroll
+        for (int e = 0; e < 8; e++) v |= ((w[e] >> (8 * l)) & 0xFFull) << (8 * e);
+        const uint32_t row = i * 8 + l;
+        *reinterpret_cast<uint64_t*>(tile + row * 128 + ((((k >> 4) ^ (row & 7)) << 4) | (k & 15))) = v;
+    }
+    __syncthreads();
+    uint4* dst = reinterpret_cast<uint4*>(ppl + kb * TC_A_BYTES);
+    const uint4* src = reinterpret_cast<const uint4*>(tile);
+#pragma unroll
+    for (int q = 0; q < TC_A_BYTES / 16 / 256; q++) dst[t + 256 * q] = src[t + 256 * q];
 }
 
-// prep: F[v][j][w] = z_{v,j}[(80 - w) mod 81] (0 for indices >= 54), w < 144
+// prep: F[v][j][w] = z_{v,j}[(80 - w) mod 81] (0 for indices >= 54), w < 160
 __global__ void f_seq_kernel(const int8_t* __restrict__ digits, uint32_t n_vec, uint64_t m, uint8_t* __restrict__ F) {
     const uint64_t tid = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
     if (tid >= (uint64_t)n_vec * m) return;
@@ -186,7 +219,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1) commit_tc_kernel(const TcArgs a
     // 1024-align the tile buffers (dynamic smem base alignment is not guaranteed)
     uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
     uint8_t* sA = smem;                                        // [ASTAGES][16 KB]
-    uint8_t* sB = sA + TC_ASTAGES * TC_A_BYTES;                // [BSTAGES][42 KB]
+    uint8_t* sB = sA + TC_ASTAGES * TC_A_BYTES;                // [BSTAGES][18 KB]
     uint8_t* sF = sB + TC_BSTAGES * TC_B_BYTES;                // [ASTAGES][1280 B]
     uint64_t* bars = reinterpret_cast<uint64_t*>(sF + TC_ASTAGES * TC_F_STAGE);
     uint64_t* full_a = bars;                                   // [ASTAGES] A tile + F landed
@@ -218,12 +251,6 @@ __global__ void __launch_bounds__(TC_THREADS, 1) commit_tc_kernel(const TcArgs a
         mbar_init(done, 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
-    // zero the padding rows of every B stage once (never rewritten)
-    for (int s = 0; s < TC_BSTAGES; s++)
-        for (int x = threadIdx.x; x < (TC_NPAD - TC_NROWS) * 8; x += blockDim.x) {
-            int row = TC_NROWS + x / 8, c = x % 8;
-            *reinterpret_cast<uint4*>(sB + s * TC_B_BYTES + (row >> 3) * 1024 + (row & 7) * 128 + c * 16) = make_uint4(0, 0, 0, 0);
-        }
     if (warp == 1) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], 512;" ::"r"(smem_u32(tmem_slot)));
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
@@ -264,11 +291,12 @@ __global__ void __launch_bounds__(TC_THREADS, 1) commit_tc_kernel(const TcArgs a
                 asm volatile("tcgen05.fence::after_thread_sync;");
                 const uint32_t a0 = smem_u32(sA + sa * TC_A_BYTES), b0 = smem_u32(sB + sb * TC_B_BYTES);
 #pragma unroll
-                for (int k = 0; k < 4; k++) {  // 4 x 32-byte K steps inside the 128-byte swizzle atom
+                for (int k = 0; k < 4; k++) {  // 4 x 32-byte K steps: column k/2, s in [32(k%2), 32(k%2)+32)
                     const uint64_t ad = sw128_desc(a0 + 32 * k);
                     const uint32_t acc = (it > 0 || k > 0) ? 1u : 0u;
-                    mma_i8(tmem, ad, sw128_desc(b0 + 32 * k), id0, acc);
-                    mma_i8(tmem + TC_N0, ad, sw128_desc(b0 + (TC_N0 / 8) * 1024 + 32 * k), id1, acc);
+                    const uint32_t bcol = b0 + (k >> 1) * TC_BCOL_BYTES + (k & 1) * 2 * TC_BLBO;
+                    mma_i8(tmem, ad, ns_desc(bcol), id0, acc);
+                    mma_i8(tmem + TC_N0, ad, ns_desc(bcol + 32 * TC_BSBO), id1, acc);
                 }
                 mma_commit(&empty_a[sa]);  // tiles free once these MMAs complete
                 mma_commit(&empty_b[sb]);
@@ -277,43 +305,54 @@ __global__ void __launch_bounds__(TC_THREADS, 1) commit_tc_kernel(const TcArgs a
         }
     } else {
         // ---- B builders (warps 2..9) ----
+        // thread (part, column jj, vector vl, phase p = 8h + b) writes chunks c of
+        // G_p: chunk c = F[16c + p, 16c + p + 16) at [jj][c][h][vl][b]; part 0 the
+        // chunks 0..4, part 1 the chunks 5..8 (warp-uniform)
         const int bt = threadIdx.x - 64;
+        const int p = bt & 15, vl = (bt >> 4) & 3, jj = (bt >> 6) & 1, part = bt >> 7;
         for (uint32_t it = 0; it < nkb; it++) {
             const int sa = it % TC_ASTAGES, sb = it % TC_BSTAGES;
-            // F of this K block has landed, and the MMAs of K block it-2 released the B buffer
-            if (!mbar_wait(&full_a[sa], (it / TC_ASTAGES) & 1) ||
-                (it >= TC_BSTAGES && !mbar_wait(&empty_b[sb], ((it / TC_BSTAGES) & 1) ^ 1))) {
+            // F of this K block has landed, and the MMAs of K block it - BSTAGES released the B buffer;
+            // lane 0 waits for the warp, so every exit from this loop is warp-uniform
+            uint32_t st = 0;  // 0 go, 1 timed out, 2 another role aborted
+            if (lane == 0) {
+                if (!mbar_wait(&full_a[sa], (it / TC_ASTAGES) & 1) ||
+                    (it >= TC_BSTAGES && !mbar_wait(&empty_b[sb], ((it / TC_BSTAGES) & 1) ^ 1)))
+                    st = 1;
+                else if (s_abort)
+                    st = 2;
+            }
+            st = __shfl_sync(0xffffffffu, st, 0);
+            if (st == 1 && lane == 0) {
                 atomicOr(a.err, 4u);
                 s_abort = 1;
-                break;
             }
-            if (s_abort) break;
+            if (st) break;
             uint8_t* dstB = sB + sb * TC_B_BYTES;
             const uint8_t* srcF = sF + sa * TC_F_STAGE;
-            for (int task = bt; task < TC_NROWS * 2; task += TC_BUILDERS) {
-                const int half = task & 1, row = task >> 1;
-                const int vl = row / 81, r = row - vl * 81;
-                uint32_t out[16];
-                if ((uint32_t)vl < nvalid) {
-                    const int o = 80 - r;  // window start in F
-                    const uint32_t* src =
-                        reinterpret_cast<const uint32_t*>(srcF + (vl * 2 + half) * TC_FBYTES + (o & ~3));
-                    uint32_t w[17];
+            if ((uint32_t)vl < nvalid) {
+                const int c0 = part ? 5 : 0;
+                const int o = 16 * c0 + p;  // first F byte of this thread's chunks
+                const uint32_t* src = reinterpret_cast<const uint32_t*>(srcF + (vl * 2 + jj) * TC_FBYTES + (o & ~3));
+                const uint32_t sh = 8 * (o & 3);
+                uint8_t* dst = dstB + jj * TC_BCOL_BYTES + c0 * TC_BLBO + (p >> 3) * (TC_NV * 128) + vl * 128 + (p & 7) * 16;
+                uint32_t w[21];
+                if (part == 0) {  // 5 chunks: words [o/4, o/4 + 21) <= byte 96 of the 160-byte F
+#pragma unroll
+                    for (int q = 0; q < 21; q++) w[q] = src[q];
+#pragma unroll
+                    for (int c = 0; c < 5; c++)
+                        *reinterpret_cast<uint4*>(dst + c * TC_BLBO) =
+                            make_uint4(__funnelshift_r(w[4 * c], w[4 * c + 1], sh), __funnelshift_r(w[4 * c + 1], w[4 * c + 2], sh),
+                                       __funnelshift_r(w[4 * c + 2], w[4 * c + 3], sh), __funnelshift_r(w[4 * c + 3], w[4 * c + 4], sh));
+                } else {  // 4 chunks: words [o/4, o/4 + 17) end exactly at byte 160
 #pragma unroll
                     for (int q = 0; q < 17; q++) w[q] = src[q];
-                    const uint32_t sh = 8 * (o & 3);
 #pragma unroll
-                    for (int q = 0; q < 16; q++) out[q] = __funnelshift_r(w[q], w[q + 1], sh);
-                } else {
-#pragma unroll
-                    for (int q = 0; q < 16; q++) out[q] = 0;
-                }
-                uint8_t* rowp = dstB + (row >> 3) * 1024 + (row & 7) * 128;
-#pragma unroll
-                for (int c = 0; c < 4; c++) {
-                    const int chunk = half * 4 + c;
-                    *reinterpret_cast<uint4*>(rowp + ((chunk ^ (row & 7)) * 16)) =
-                        make_uint4(out[4 * c], out[4 * c + 1], out[4 * c + 2], out[4 * c + 3]);
+                    for (int c = 0; c < 4; c++)
+                        *reinterpret_cast<uint4*>(dst + c * TC_BLBO) =
+                            make_uint4(__funnelshift_r(w[4 * c], w[4 * c + 1], sh), __funnelshift_r(w[4 * c + 1], w[4 * c + 2], sh),
+                                       __funnelshift_r(w[4 * c + 2], w[4 * c + 3], sh), __funnelshift_r(w[4 * c + 3], w[4 * c + 4], sh));
                 }
             }
             asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
@@ -321,7 +360,9 @@ __global__ void __launch_bounds__(TC_THREADS, 1) commit_tc_kernel(const TcArgs a
             if (lane == 0) mbar_arrive(&full_b[sb]);
         }
         // ---- epilogue (warps 2..5 cover TMEM lane groups 2, 3, 0, 1): TMEM -> int32 partials ----
-        bool ok = nkb > 0 && !s_abort && mbar_wait(done, 0);
+        uint32_t okw = 0;  // lane 0 waits for the warp
+        if (lane == 0) okw = (nkb > 0 && !s_abort && mbar_wait(done, 0)) ? 1u : 0u;
+        const bool ok = __shfl_sync(0xffffffffu, okw, 0) != 0;
         if (nkb > 0 && !ok && warp < 6) atomicOr(a.err, 8u);
         asm volatile("tcgen05.fence::after_thread_sync;");
         const int lg = warp & 3;  // TMEM lane group this warp may access
@@ -366,7 +407,10 @@ __global__ void commit_tc_reduce_kernel(const int32_t* __restrict__ partial, uin
         int64_t acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
         for (uint32_t ks = 0; ks < n_ksplit; ks++) {
             const uint32_t cta = ks * n_groups + group;
-            const int32_t* p = partial + ((uint64_t)cta * 128 + i * 8) * TC_NPAD + vl * 81 + r;
+            // TMEM column of output row r: r' = 80 - r = 16a + 8h + b -> row group (2a + h) NV + vl
+            const int rp = 80 - r;
+            const int col = ((((rp >> 4) * 2 + ((rp >> 3) & 1)) * TC_NV + (int)vl) << 3) | (rp & 7);
+            const int32_t* p = partial + ((uint64_t)cta * 128 + i * 8) * TC_NPAD + col;
 #pragma unroll
             for (int l = 0; l < 8; l++) acc[l] += p[(uint64_t)l * TC_NPAD];
         }
@@ -388,8 +432,7 @@ int tc_pp_prepare(neo_gpu_ctx* ctx, PPEntry* pp) {
     pp->tc = false;
     const uint64_t n_kb = pp->m / 2;
     if (!pp->d_pp_limbs) NEO_CK(ctx, cudaMalloc(&pp->d_pp_limbs, n_kb * TC_A_BYTES));  // size depends on m only
-    const uint64_t threads = n_kb * 128 * 8;
-    pp_limbs_kernel<<<ceil_div(threads, 256), 256, 0, ctx->stream>>>(pp->d_pp, pp->kappa, pp->m, pp->d_pp_limbs);
+    pp_limbs_kernel<<<(unsigned)n_kb, 256, 0, ctx->stream>>>(pp->d_pp, pp->kappa, pp->m, pp->d_pp_limbs);
     NEO_LAUNCHED(ctx);
     NEO_CK(ctx, ctx_sync(ctx));
     pp->tc = true;
@@ -413,7 +456,7 @@ size_t tc_scratch_bytes(uint32_t n_vec, uint64_t m, uint32_t* n_groups_out, uint
     *n_groups_out = n_groups;
     *n_ksplit_out = n_ksplit;
     *kb_per_cta_out = kb_per_cta;
-    size_t f_bytes = (size_t)n_vec * m * TC_FBYTES + 64;  // window reads may run 4 bytes past the last F
+    size_t f_bytes = (size_t)n_vec * m * TC_FBYTES + 64;
     size_t p_bytes = (size_t)n_groups * n_ksplit * 128 * TC_NPAD * 4;
     return ((f_bytes + 255) & ~size_t(255)) + p_bytes + 256;
 }
