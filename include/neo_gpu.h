@@ -293,12 +293,31 @@ int neo_gpu_shard_create_mem(neo_gpu_ctx* ctx, const neo_ccs_desc* ccs, uint32_t
 /* Number of val-lane DEC children emitted so far (the reference's
  * val_lane_obligations, shard.rs:2548-2991). */
 int neo_gpu_shard_val_obligations(const neo_gpu_shard* sh, uint64_t* count);
+/* Replace the initial state of Twist instance mem_idx for the following fold
+ * steps: the MemInit of the next step's MemInstance, which for a trace split
+ * into chunks is the memory state at the end of the previous chunk
+ * (mem_init_from_state_map, crates/neo-memory/src/mem_init.rs:65-90).
+ * n_init = 0: MemInit::Zero; otherwise MemInit::Sparse in canonical form
+ * (addresses strictly increasing and < 2^ell_addr, mem_init.rs:26-60), else
+ * NEO_ERR_ARG.  The public init digest absorbed per step follows it. */
+int neo_gpu_shard_set_twist_init(neo_gpu_shard* sh, uint32_t mem_idx, uint64_t n_init, const uint64_t* init_addr,
+                                 const uint64_t* init_val);
 /* One fold step on the main lane (no Twist/Shout): witness build
  * (decomp + MCS commit, crates/neo-fold/src/session.rs:977-978), Pi_CCS
  * (batched time rounds + Ajtai rounds), ME outputs, Pi_RLC, Pi_DEC
  * (shard.rs:1803-2180, 1170-1331).  z: the step witness (m values, host).
- * proof: canonical dump of the step proof (see DESIGN.md for the word order);
- * pass NULL to query *proof_len. */
+ * proof: canonical dump of the step proof, in order: the MCS commitment
+ * (kappa*54), the initial sum T (K), [Shout address pre-time: claimed sums,
+ * active mask, round polynomials, r_addr], [per Twist: address round
+ * polynomials, r_addr, read / write finals], the batched time round
+ * polynomials (per round, per claim), the Ajtai round polynomials, the final
+ * running sum, the ME outputs' y (k x t x 54 K) and y_scalars (k x t K), [the
+ * bus openings of every output (bus_cols x 54 K + bus_cols K)], [Twist
+ * val-eval: claimed sums, round polynomials, r_val, CPU ME claims at r_val
+ * (y and y_scalars of (t + bus_cols) rows)], the main lane (k rhos x 54, the
+ * parent commitment, per DEC child its commitment, core y (t x 54 K) and bus
+ * y (bus_cols x 54 K)), [the val lane, same layout]; K = two words (re, im).
+ * Pass NULL to query *proof_len. */
 int neo_gpu_shard_fold_step(neo_gpu_shard* sh, const uint64_t* z, uint64_t* proof, uint64_t proof_cap,
                             uint64_t* proof_len);
 /* Same step with the witness already resident in device memory (d_z). */

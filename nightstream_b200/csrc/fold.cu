@@ -313,6 +313,27 @@ static void digest_fields(const char* label, const std::vector<uint64_t>& fs, ui
     h.digest32(out);
 }
 
+// MemInit of a Twist instance (crates/neo-memory/src/mem_init.rs): Sparse pairs
+// in canonical form (strictly increasing addresses < 2^ell_addr) or Zero, and
+// the public digest absorbed per step (digest_fields "twist/init/sparse" /
+// "twist/init/zero", memory_sidecar/memory.rs:86-124).  false: not canonical.
+static bool twist_set_init(TwistInst& ti, uint64_t n, const uint64_t* addr, const uint64_t* val) {
+    std::vector<uint64_t> a, v, fs;
+    for (uint64_t e = 0; e < n; e++) {
+        if (addr[e] >> ti.ea) return false;
+        if (e && addr[e] <= addr[e - 1]) return false;
+        a.push_back(addr[e]);
+        v.push_back(gl::canon(val[e]));
+        fs.push_back(addr[e]);
+        fs.push_back(gl::canon(val[e]));
+    }
+    ti.init_addr.swap(a);
+    ti.init_val.swap(v);
+    digest_fields(n ? "twist/init/sparse" : "twist/init/zero", fs, ti.digest);
+    return true;
+}
+
+
 extern "C" int neo_ccs_digest(const neo_ccs_desc* d, uint64_t* out4) {
     if (!d || !out4 || d->t == 0 || d->n == 0 || d->m == 0) return NEO_ERR_ARG;
     ccs_digest_words(d, out4);
@@ -382,16 +403,8 @@ static int shard_create_impl(neo_gpu_ctx* ctx, const neo_ccs_desc* desc, uint32_
             if (w.n_init && (!w.init_addr || !w.init_val)) return ctx->fail(NEO_ERR_ARG, "shard_create: Twist init is null");
             auto ti = std::make_unique<TwistInst>();
             ti->ea = w.ell_addr; ti->k = w.k; ti->d = w.d; ti->n_side = w.n_side; ti->ell = w.ell;
-            std::vector<uint64_t> fs;
-            for (uint64_t e = 0; e < w.n_init; e++) {
-                if (w.init_addr[e] >> w.ell_addr) return ctx->fail(NEO_ERR_ARG, "shard_create: Twist init address out of range");
-                ti->init_addr.push_back(w.init_addr[e]);
-                ti->init_val.push_back(gl::canon(w.init_val[e]));
-                fs.push_back(w.init_addr[e]);
-                fs.push_back(w.init_val[e]);
-            }
-            if (w.n_init) digest_fields("twist/init/sparse", fs, ti->digest);
-            else digest_fields("twist/init/zero", fs, ti->digest);
+            if (!twist_set_init(*ti, w.n_init, w.init_addr, w.init_val))
+                return ctx->fail(NEO_ERR_ARG, "shard_create: Twist init must have strictly increasing addresses < 2^ell_addr");
             ti->col0 = col;
             col += 2 * w.ell_addr + 5;
             sh->twist.push_back(std::move(ti));
@@ -1489,6 +1502,23 @@ extern "C" int neo_gpu_shard_ccs_digest(const neo_gpu_shard* sh, uint64_t* d4) {
 extern "C" int neo_gpu_shard_step_stats(const neo_gpu_shard* sh, double* out, uint32_t n) {
     if (!sh || !out) return NEO_ERR_ARG;
     for (uint32_t i = 0; i < n && i < 12; i++) out[i] = sh->stats[i];
+    return NEO_OK;
+}
+
+extern "C" int neo_gpu_shard_set_twist_init(neo_gpu_shard* sh, uint32_t mem_idx, uint64_t n_init,
+                                            const uint64_t* init_addr, const uint64_t* init_val) {
+    if (!sh) return NEO_ERR_ARG;
+    neo_gpu_ctx* ctx = sh->ctx;
+    if (mem_idx >= sh->twist.size()) return ctx->fail(NEO_ERR_ARG, "shard_set_twist_init: mem_idx out of range");
+    if (n_init && (!init_addr || !init_val)) return ctx->fail(NEO_ERR_ARG, "shard_set_twist_init: init is null");
+    TwistInst tmp;
+    tmp.ea = sh->twist[mem_idx]->ea;
+    if (!twist_set_init(tmp, n_init, init_addr, init_val))
+        return ctx->fail(NEO_ERR_ARG, "shard_set_twist_init: addresses must be strictly increasing and < 2^ell_addr");
+    TwistInst& ti = *sh->twist[mem_idx];
+    ti.init_addr.swap(tmp.init_addr);
+    ti.init_val.swap(tmp.init_val);
+    memcpy(ti.digest, tmp.digest, 32);
     return NEO_OK;
 }
 

@@ -53,6 +53,7 @@ SIGNATURES = {
     "neo_gpu_shard_create": [P, P, U32, U32, ctypes.c_char_p, P],
     "neo_gpu_shard_create_mem": [P, P, U32, U32, ctypes.c_char_p, P, P],
     "neo_gpu_shard_val_obligations": [P, P],
+    "neo_gpu_shard_set_twist_init": [P, U32, U64, P, P],
     "neo_gpu_shard_fold_step": [P, P, P, U64, P],
     "neo_gpu_shard_fold_step_device": [P, ctypes.c_void_p, P],
     "neo_gpu_shard_transcript_state": [P, P],
@@ -508,6 +509,15 @@ class Shard:
         out = np.zeros(12, np.float64)
         self.ctx.check(self.ctx.lib.neo_gpu_shard_step_stats(self.h, _p(out), 12))
         return {k: float(v) for k, v in zip(self.STAT_NAMES, out)}
+
+    def set_twist_init(self, mem_idx: int, init):
+        """MemInit of Twist instance mem_idx for the following steps: [(addr, value)]
+        with strictly increasing addresses (empty: MemInit::Zero)."""
+        a = np.array([int(x) for x, _ in init], np.uint64)
+        v = np.array([int(y) % 0xFFFFFFFF00000001 for _, y in init], np.uint64)
+        self.ctx.check(self.ctx.lib.neo_gpu_shard_set_twist_init(self.h, mem_idx, len(init),
+                                                                 _p(a) if len(init) else None,
+                                                                 _p(v) if len(init) else None))
 
     def val_obligations(self) -> int:
         c = ctypes.c_uint64()

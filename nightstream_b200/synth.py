@@ -36,9 +36,10 @@ def _uniform_fq(rng, shape):
         return v
 
 
-def make_r1cs(ell: int, seed: int, z_bits: int = 32, z: np.ndarray = None):
+def make_r1cs(ell: int, seed: int, z_bits: int = 32, z: np.ndarray = None, max_col: int = None):
     """Return (ccs, z) for a satisfied random R1CS with n = m = 2^ell
-    (z drawn here, or the given witness with z[0] = 1)."""
+    (z drawn here, or the given witness with z[0] = 1).  max_col: constraints
+    only touch columns < max_col (any values beyond stay satisfying)."""
     n = m = 1 << ell
     rng = np.random.default_rng(seed)
     if z is None:
@@ -47,13 +48,14 @@ def make_r1cs(ell: int, seed: int, z_bits: int = 32, z: np.ndarray = None):
     else:
         z = np.asarray(z, dtype=np.uint64).copy()
         rng.integers(0, 1 << z_bits, size=m, dtype=np.uint64)  # keep the stream aligned
-    a_cols = _distinct_cols(rng, n, m, 3)
-    b_cols = _distinct_cols(rng, n, m, 3)
-    c_cols = _distinct_cols(rng, n, m, 3)
+    mc = m if max_col is None else max_col
+    a_cols = _distinct_cols(rng, n, mc, 3)
+    b_cols = _distinct_cols(rng, n, mc, 3)
+    c_cols = _distinct_cols(rng, n, mc, 3)
     # the solved column must hold a nonzero witness value
     zero = z[c_cols[:, 2]] == 0
     while zero.any():
-        c_cols[zero, 2] = rng.integers(0, m, size=int(zero.sum()))
+        c_cols[zero, 2] = rng.integers(0, mc, size=int(zero.sum()))
         zero = z[c_cols[:, 2]] == 0
     a_vals = _uniform_fq(rng, (n, 3))
     b_vals = _uniform_fq(rng, (n, 3))
@@ -106,15 +108,30 @@ def memory_trace(steps: int, shout_ell, twist_ell, seed: int, table_len: int = N
     twist_ell: one int per instance (or a single int).  Returns the bus columns
     (values per step, Shout instances first then Twist, in the shared-bus
     column order) and the instance data."""
+    buses, mem, _ = memory_trace_chunks(1, steps, shout_ell, twist_ell, seed, table_len, init_cells, lookup_rate,
+                                        rw_rate)
+    return buses[0], mem
+
+
+def memory_trace_chunks(n_chunks: int, steps: int, shout_ell, twist_ell, seed: int, table_len: int = None,
+                        init_cells: int = 64, lookup_rate: float = 1.0, rw_rate: float = 1.0):
+    """A trace of n_chunks * steps steps (as memory_trace) split into fold
+    steps of `steps` trace steps.  Returns the per-chunk bus columns, the
+    instance data (with the initial state of chunk 0) and, per chunk, the
+    MemInit of every Twist instance: the nonzero cells at the chunk's start in
+    increasing address order (mem_init_from_state_map,
+    crates/neo-memory/src/mem_init.rs:65-90)."""
     rng = np.random.default_rng(seed)
     shout_ells = [shout_ell] if isinstance(shout_ell, int) else list(shout_ell)
     twist_ells = [twist_ell] if isinstance(twist_ell, int) else list(twist_ell)
+    S = n_chunks * steps
     cols, shout, twist = [], [], []
+    inits = [[] for _ in range(n_chunks)]
     for se in shout_ells:
         tl = table_len or (1 << se)
         table = rng.integers(0, 1 << 32, size=tl, dtype=np.uint64)
-        idx = rng.integers(0, tl, size=steps)
-        has = (rng.random(steps) < lookup_rate).astype(np.int64)
+        idx = rng.integers(0, tl, size=S)
+        has = (rng.random(S) < lookup_rate).astype(np.int64)
         idx = idx * has
         for b in range(se):
             cols.append((idx >> b) & 1)
@@ -128,15 +145,17 @@ def memory_trace(steps: int, shout_ell, twist_ell, seed: int, table_len: int = N
         mem = np.zeros(P, dtype=object)
         for a, v in init:
             mem[a] = v
-        ra = np.zeros(steps, np.int64)
-        wa = np.zeros(steps, np.int64)
-        hr = (rng.random(steps) < rw_rate).astype(np.int64)
-        hw = (rng.random(steps) < rw_rate).astype(np.int64)
-        rv = np.zeros(steps, dtype=object)
-        wv = rng.integers(0, 1 << 32, size=steps) * hw
-        inc = np.zeros(steps, dtype=object)
+        ra = np.zeros(S, np.int64)
+        wa = np.zeros(S, np.int64)
+        hr = (rng.random(S) < rw_rate).astype(np.int64)
+        hw = (rng.random(S) < rw_rate).astype(np.int64)
+        rv = np.zeros(S, dtype=object)
+        wv = rng.integers(0, 1 << 32, size=S) * hw
+        inc = np.zeros(S, dtype=object)
         pos = 0
-        for j in range(steps):
+        for j in range(S):
+            if j % steps == 0:
+                inits[j // steps].append([(a, int(mem[a])) for a in range(P) if mem[a] != 0])
             if rng.random() < 0.7:
                 pos = (pos + 4) % P
                 a_r = pos
@@ -157,7 +176,8 @@ def memory_trace(steps: int, shout_ell, twist_ell, seed: int, table_len: int = N
         cols += [hr, hw, wv, rv, inc]
         twist.append(dict(ell_addr=te, k=P, d=1, n_side=P, ell=te, init=init))
     bus = np.array([[int(v) % Q for v in c] for c in cols], dtype=np.uint64)
-    return bus, dict(steps=steps, shout=shout, twist=twist)
+    buses = [np.ascontiguousarray(bus[:, c * steps:(c + 1) * steps]) for c in range(n_chunks)]
+    return buses, dict(steps=steps, shout=shout, twist=twist), inits
 
 
 def make_memory_workload(ell: int, seed: int, steps: int, shout_ell, twist_ell, m_in: int = 1,
@@ -176,3 +196,26 @@ def make_memory_workload(ell: int, seed: int, steps: int, shout_ell, twist_ell, 
     z[base:] = bus.reshape(-1)
     ccs, z = make_r1cs(ell, seed, z=z)
     return ccs, z, mem
+
+
+def make_memory_workload_chunks(ell: int, seed: int, n_chunks: int, steps: int, shout_ell, twist_ell, m_in: int = 1,
+                                table_len: int = None, **trace_kw):
+    """A shard whose fold steps prove consecutive chunks of one trace: a
+    satisfied R1CS of n = m = 2^ell whose constraints avoid the bus region, and
+    per chunk a witness carrying that chunk's bus columns in its tail.
+    Returns (ccs, [z per chunk], mem, [Twist MemInits per chunk])."""
+    m = 1 << ell
+    buses, mem, inits = memory_trace_chunks(n_chunks, steps, shout_ell, twist_ell, seed + 1, table_len, **trace_kw)
+    rng = np.random.default_rng(seed + 2)
+    z = rng.integers(0, 1 << 32, size=m, dtype=np.uint64)
+    z[0] = 1
+    base = m - buses[0].shape[0] * steps
+    if base < m_in + 4 or m_in + steps > m:
+        raise ValueError("bus does not fit the witness")
+    ccs, z = make_r1cs(ell, seed, z=z, max_col=base)
+    zs = []
+    for bus in buses:
+        zc = z.copy()
+        zc[base:] = bus.reshape(-1)
+        zs.append(zc)
+    return ccs, zs, mem, inits

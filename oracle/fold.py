@@ -135,7 +135,8 @@ class OracleShard:
         self.step_idx = 0
         self.threads = threads
         self.mem = mem or dict(steps=0, shout=[], twist=[])
-        self.shout, self.twist = self.mem.get("shout", []), self.mem.get("twist", [])
+        self.shout = [dict(s) for s in self.mem.get("shout", [])]
+        self.twist = [dict(w) for w in self.mem.get("twist", [])]
         self.bus = BusLayout(self.m, m_in, self.mem.get("steps", 0), [s["ell_addr"] for s in self.shout],
                              [w["ell_addr"] for w in self.twist])
         for s in self.shout:
@@ -150,6 +151,22 @@ class OracleShard:
             else:
                 w["digest"] = digest_fields(b"twist/init/zero", [])
         self.prev = None     # previous step's MCS (c, Z) and decoded Twist columns
+
+    def set_twist_init(self, i, init):
+        """MemInit of Twist instance i for the following steps (mem_init.rs:26-90):
+        [(addr, value)] with strictly increasing addresses, [] = MemInit::Zero."""
+        init = [(int(a), int(v) % Q) for a, v in init]
+        if any(b[0] <= a[0] for a, b in zip(init, init[1:])):
+            raise ValueError("MemInit::Sparse must be strictly increasing by address")
+        w = self.twist[i]
+        w["init"] = init
+        if init:
+            fs = []
+            for a, v in init:
+                fs += [a, v]
+            w["digest"] = digest_fields(b"twist/init/sparse", fs)
+        else:
+            w["digest"] = digest_fields(b"twist/init/zero", [])
 
     def _k(self, label, v):
         self.tr.append_fields(label, np.array(v, np.uint64))

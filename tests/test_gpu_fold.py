@@ -62,6 +62,37 @@ def test_memory_fold_steps_match_oracle(ctx, ell, steps, chunk, shout_ell, twist
     g.close()
 
 
+@pytest.mark.parametrize("ell,chunks,chunk,shout_ell,twist_ell", [(12, 3, 32, 8, 6), (13, 3, 64, 10, 8)])
+def test_memory_multi_chunk_trace_matches_oracle(ctx, ell, chunks, chunk, shout_ell, twist_ell):
+    """Consecutive chunks of one trace, each step starting from the memory state
+    the previous chunk left (neo_gpu_shard_set_twist_init): every proof word and
+    the transcript state match the oracle; a stale init is rejected (the Twist
+    address-lane claim 0 fails at its first round, NEO_ERR_INVARIANT)."""
+    ccs, zs, mem, inits = synth.make_memory_workload_chunks(ell, 9, chunks, chunk, shout_ell, twist_ell)
+    pp = np.random.default_rng(ell + 3).integers(0, Q, size=(16, 1 << ell, 54), dtype=np.uint64)
+    ctx.pp_upload(pp)
+    g = gpu.Shard(ctx, ccs, m_in=1, k_rho=12, app_label=b"neo/test-chunks", mem=mem)
+    o = OracleShard(ccs, pp, m_in=1, k_rho=12, app_label=b"neo/test-chunks", mem=mem)
+    for c in range(chunks):
+        if c:
+            g.set_twist_init(0, inits[c][0])
+            o.set_twist_init(0, inits[c][0])
+        pg, po = g.fold_step(zs[c]), o.fold_step(zs[c])
+        assert np.array_equal(pg, po), f"chunk {c}: first mismatch at word {int(np.argmax(pg != po))}"
+        assert np.array_equal(g.transcript_state(), o.tr.state()), f"chunk {c}: transcript state"
+    g.close()
+    stale = gpu.Shard(ctx, ccs, m_in=1, k_rho=12, app_label=b"neo/test-chunks", mem=mem)
+    stale.fold_step(zs[0])
+    with pytest.raises(gpu.NeoGpuError) as e:
+        stale.fold_step(zs[1])
+    assert e.value.code == 3
+    with pytest.raises(gpu.NeoGpuError):
+        stale.set_twist_init(0, [(7, 1), (3, 2)])
+    with pytest.raises(gpu.NeoGpuError):
+        stale.set_twist_init(1, [])
+    stale.close()
+
+
 def test_memory_fold_rejects_bad_read(ctx):
     """A read value that disagrees with memory breaks the Twist checks: the
     prover stops with the invariant status instead of emitting a proof."""
