@@ -110,7 +110,8 @@ class OracleVerifier:
         self.val_obligations = []
         self.step_idx = 0
         self.mem = mem or dict(steps=0, shout=[], twist=[])
-        self.shout, self.twist = self.mem.get("shout", []), self.mem.get("twist", [])
+        self.shout = [dict(sd) for sd in self.mem.get("shout", [])]
+        self.twist = [dict(w) for w in self.mem.get("twist", [])]
         self.bus = BusLayout(self.m, m_in, self.mem.get("steps", 0), [s["ell_addr"] for s in self.shout],
                              [w["ell_addr"] for w in self.twist])
         self.shout_digest = [digest_fields(b"shout/table", [int(v) for v in s["table"]]) for s in self.shout]
@@ -124,8 +125,7 @@ class OracleVerifier:
                 self.twist_digest.append(digest_fields(b"twist/init/sparse", fs))
             else:
                 self.twist_digest.append(digest_fields(b"twist/init/zero", []))
-        if self.shout or self.twist:
-            raise NotImplementedError("memory sidecar verification")
+        self.prev = None  # previous step's MCS commitment, X and Twist MemInits (rollover)
 
     # ---------------------------------------------------------------- transcript --
     def _k(self, label, v):
@@ -342,23 +342,122 @@ class OracleVerifier:
             raise VerifyError(f"{lane.decode()} lane: DEC y check failed")
         return children
 
+    # ---------------------------------------------------------------- memory --
+    def set_twist_init(self, i, init):
+        """The public MemInit of Twist instance i for the following steps."""
+        init = [(int(a), int(v) % Q) for a, v in init]
+        if any(b[0] <= a[0] for a, b in zip(init, init[1:])):
+            raise VerifyError("MemInit::Sparse must be strictly increasing by address")
+        self.twist[i] = dict(self.twist[i], init=init)
+        fs = []
+        for a, v in init:
+            fs += [a, v]
+        self.twist_digest[i] = digest_fields(b"twist/init/sparse" if init else b"twist/init/zero", fs)
+
+    @staticmethod
+    def _init_at(init, r_addr):
+        """eval_init_at_r_addr (neo-memory/src/mem_init.rs:133-170)."""
+        acc = ZERO
+        for a, v in init:
+            chi = ONE
+            for bit, r in enumerate(r_addr):
+                chi = kmulp(chi, r if (a >> bit) & 1 else ksub(ONE, r))
+            acc = kadd(acc, kmulp((int(v) % Q, 0), chi))
+        return acc
+
+    @staticmethod
+    def _eq_bits(bits, u):
+        """eq_bits_prod with eq_bit_affine(b, u) = b (2u - 1) + (1 - u) (neo-memory/src/bit_ops.rs:6-20)."""
+        acc = ONE
+        for b, x in zip(bits, u):
+            acc = kmulp(acc, kadd(kmulp(b, ksub(kadd(x, x), ONE)), ksub(ONE, x)))
+        return acc
+
+    def _bitness_weights(self, r0, n, sep):
+        """bitness_weights (memory_sidecar/utils.rs:43-71): powers of r_cycle[0] + sep."""
+        base = ((r0[0] + sep) % Q, r0[1])
+        if base in (ZERO, ONE, (Q - 1, 0)):
+            base = ((base[0] + 1) % Q, base[1])
+        if base == ZERO:
+            base = ONE
+        out, cur = [], ONE
+        for _ in range(n):
+            out.append(cur)
+            cur = kmulp(cur, base)
+        return out
+
+    def _bitness_expected(self, chi, r0, opens, sep):
+        acc = ZERO
+        for w, b in zip(self._bitness_weights(r0, len(opens), sep), opens):
+            acc = kadd(acc, kmulp(w, kmulp(b, ksub(b, ONE))))
+        return kmulp(chi, acc)
+
+    @staticmethod
+    def _lt_eval(jp, j):
+        """lt_eval (neo-memory/src/mle.rs:7-24)."""
+        ell = len(j)
+        suffix = [ONE] * (ell + 1)
+        for i in range(ell - 1, -1, -1):
+            e = kadd(kmulp(ksub(ONE, jp[i]), ksub(ONE, j[i])), kmulp(jp[i], j[i]))
+            suffix[i] = kmulp(suffix[i + 1], e)
+        acc = ZERO
+        for i in range(ell):
+            acc = kadd(acc, kmulp(kmulp(ksub(ONE, jp[i]), j[i]), suffix[i + 1]))
+        return acc
+
+    def _bind_claim_sums(self, prefix, sums, labels):
+        """bind_batched_claim_sums (memory_sidecar/transcript.rs:12-26)."""
+        self.tr.append_message(prefix, le64(len(sums)))
+        for i, (sm, lab) in enumerate(zip(sums, labels)):
+            self.tr.append_message(b"addr_batch/label", lab)
+            self.tr.append_message(b"addr_batch/idx", le64(i))
+            self._k(b"addr_batch/claimed_sum", sm)
+
+    def _time_claim_plan(self):
+        """RouteATimeClaimPlan (memory_sidecar/claim_plan.rs:42-187): (label, degree, dynamic)."""
+        plan = [(b"ccs/time", self.d_sc, True)]
+        for s in self.shout:
+            plan += [(b"shout/value", 3, True), (b"shout/adapter", 2 + s["ell_addr"], True), (b"shout/bitness", 3, False)]
+        for w in self.twist:
+            plan += [(b"twist/read_check", 3 + w["ell_addr"], True), (b"twist/write_check", 3 + w["ell_addr"], True),
+                     (b"twist/bitness", 3, False)]
+        return plan
+
     # -------------------------------------------------------------- fold step --
     def verify_step(self, x, P):
-        """Check one step's proof words against the public input x = z[:m_in];
-        on success the verified DEC children become the accumulator."""
+        """Check one step's proof words against the public input x = z[:m_in]
+        (and the step's public memory instances); on success the verified DEC
+        children become the accumulator and the val-lane children are added to
+        val_obligations."""
         tr, t, ell_n, ell_d, d_sc = self.tr, self.t, self.ell_n, self.ell_d, self.d_sc
         idx, kappa, m_in = self.step_idx, self.kappa, self.m_in
+        bus, nb = self.bus, self.bus.bus_cols
         R = Reader(P)
         n_acc = len(self.acc)
         k = 1 + n_acc
-        d_pad = 1 << ell_d
         xv = [int(v) % Q for v in np.asarray(x, np.uint64).reshape(-1)][:m_in]
         c_mcs = R.take(kappa * D)
         Xm = [int(v) % Q for v in decomp_b2(np.array(xv, np.uint64)).astype(np.int64).reshape(-1)]
-        # absorb_step_memory (memory_sidecar/memory.rs:86-124), no instances
+        # absorb_step_memory (memory_sidecar/memory.rs:86-124)
         tr.append_message(b"step/absorb_memory_start")
-        tr.append_message(b"step/lut_count", le64(0))
-        tr.append_message(b"step/mem_count", le64(0))
+        tr.append_message(b"step/lut_count", le64(len(self.shout)))
+        for i, sd in enumerate(self.shout):
+            tr.append_message(b"step/lut_idx", le64(i))
+            tr.append_message(b"shout/k", le64(sd["k"]))
+            tr.append_message(b"shout/d", le64(sd["d"]))
+            tr.append_message(b"shout/n_side", le64(sd["n_side"]))
+            tr.append_message(b"shout/steps", le64(bus.chunk))
+            tr.append_message(b"shout/ell", le64(sd["ell"]))
+            tr.append_message(b"shout/table_digest", self.shout_digest[i])
+        tr.append_message(b"step/mem_count", le64(len(self.twist)))
+        for i, w in enumerate(self.twist):
+            tr.append_message(b"step/mem_idx", le64(i))
+            tr.append_message(b"twist/k", le64(w["k"]))
+            tr.append_message(b"twist/d", le64(w["d"]))
+            tr.append_message(b"twist/n_side", le64(w["n_side"]))
+            tr.append_message(b"twist/steps", le64(bus.chunk))
+            tr.append_message(b"twist/ell", le64(w["ell"]))
+            tr.append_message(b"twist/init_digest", self.twist_digest[i])
         tr.append_message(b"step/absorb_memory_done")
         # bind_header_and_instances_with_digest (engines/utils.rs:83-137)
         tr.append_message(b"phase/pi-ccs")
@@ -397,17 +496,84 @@ class OracleVerifier:
         if R.k() != T:
             raise VerifyError("initial sum mismatch: proof claims a different value than the public T")
         self._k(b"sumcheck/initial_sum", T)
-        self._sample_ext_point(b"route_a/r_cycle", b"route_a/cycle/0", b"route_a/cycle/1", ell_n)
-        # bind_batched_dynamic_claims (memory_sidecar/transcript.rs:37-63): the CCS claim alone
-        labels, degs, sums = [b"ccs/time"], [d_sc], [T]
-        tr.append_message(b"batched/dynamic_bind/len", le64(1))
-        tr.append_message(b"batched/dynamic_bind/claim_label", b"ccs/time")
-        tr.append_message(b"batched/dynamic_bind/claim_idx", le64(0))
-        tr.append_message(b"batched/dynamic_bind/degree_bound", le64(d_sc))
-        tr.append_message(b"batched/dynamic_bind/is_dynamic", bytes([1]))
-        self._k(b"batched/dynamic_bind/claimed_sum", T)
+        r_cycle = self._sample_ext_point(b"route_a/r_cycle", b"route_a/cycle/0", b"route_a/cycle/1", ell_n)
+
+        # ---- verify_shout_addr_pre_time (memory.rs:623-816) ----
+        shout_pre = []
+        r_addr_s = []
+        if self.shout:
+            ea = self.shout[0]["ell_addr"]
+            if any(sd["ell_addr"] != ea for sd in self.shout):
+                raise VerifyError("Shout: batched addr-pre requires uniform ell_addr")
+            sums = R.ks(len(self.shout))
+            active = R.take(1)[0]
+            if active >> len(self.shout):
+                raise VerifyError("shout_addr_pre active_mask has bits set out of range")
+            tr.append_message(b"shout/addr_pre_time/step_idx", le64(idx))
+            self._bind_claim_sums(b"shout/addr_pre_time/claimed_sums", sums, [b"shout/addr_pre"] * len(sums))
+            act = [i for i in range(len(self.shout)) if (active >> i) & 1]
+            if not act:
+                tr.append_message(b"shout/addr_pre_time/no_sumcheck", le64(idx))
+                r_addr_s = self._sample_ext_point(b"shout/addr_pre_time/no_sumcheck/r_addr",
+                                                  b"shout/addr_pre_time/no_sumcheck/r_addr/0",
+                                                  b"shout/addr_pre_time/no_sumcheck/r_addr/1", ea)
+                finals = []
+            else:
+                r_addr_s, finals = self._batched_ds(b"shout/addr_pre_time", idx, [b"shout/addr_pre"] * len(act),
+                                                    [2] * len(act), [sums[i] for i in act], ea, R)
+            if R.ks(ea) != r_addr_s:
+                raise VerifyError("shout_addr_pre r_addr mismatch: transcript-derived vs proof")
+            pos = 0
+            for i, sd in enumerate(self.shout):
+                is_active = i in act
+                fin = finals[pos] if is_active else ZERO
+                pos += 1 if is_active else 0
+                tab_eval = ZERO
+                if is_active:
+                    chi = chi_table(r_addr_s)
+                    for a, v in enumerate(list(sd["table"])[:1 << ea]):
+                        tab_eval = kadd(tab_eval, kmulp((int(v) % Q, 0), chi[a]))
+                shout_pre.append(dict(active=is_active, claim=sums[i], final=fin, table_eval=tab_eval))
+
+        # ---- verify_twist_addr_pre_time (memory.rs:818-903) ----
+        twist_pre = []
+        for i, w in enumerate(self.twist):
+            ea = w["ell_addr"]
+            labels = [b"twist/read_addr_pre", b"twist/write_addr_pre"]
+            tr.append_message(b"twist/addr_pre_time/claim_idx", le64(i))
+            self._bind_claim_sums(b"twist/addr_pre_time/claimed_sums", [ZERO, ZERO], labels)
+            r_addr, finals = self._batched_ds(b"twist/addr_pre_time", i, labels, [2, 2], [ZERO, ZERO], ea, R)
+            if R.ks(ea) != r_addr:
+                raise VerifyError("twist addr_pre r_addr mismatch: transcript-derived vs proof")
+            if R.ks(2) != finals:
+                raise VerifyError("twist addr_pre finals mismatch")
+            twist_pre.append(dict(r_addr=r_addr, read=finals[0], write=finals[1]))
+
+        # ---- verify_route_a_batched_time (route_a_time.rs:159-290) ----
+        plan = self._time_claim_plan()
+        labels = [p_[0] for p_ in plan]
+        degs = [p_[1] for p_ in plan]
+        # claimed sums: the CCS claim is the public T, static claims are 0, the
+        # dynamic memory claims are those of the proof's first round, p(0) + p(1)
+        first = Reader(R.P[R.i:R.i + sum(2 * (d + 1) for d in degs)])
+        sums = []
+        for (lab, deg, dyn) in plan:
+            co = first.ks(deg + 1)
+            p1 = ZERO
+            for c in co:
+                p1 = kadd(p1, c)
+            sums.append(kadd(co[0], p1) if dyn else ZERO)
+        sums[0] = T
+        tr.append_message(b"batched/dynamic_bind/len", le64(len(plan)))
+        for ci, (lab, deg, dyn) in enumerate(plan):
+            tr.append_message(b"batched/dynamic_bind/claim_label", lab)
+            tr.append_message(b"batched/dynamic_bind/claim_idx", le64(ci))
+            tr.append_message(b"batched/dynamic_bind/degree_bound", le64(deg))
+            tr.append_message(b"batched/dynamic_bind/is_dynamic", bytes([1 if dyn else 0]))
+            if dyn:
+                self._k(b"batched/dynamic_bind/claimed_sum", sums[ci])
         r_time, finals = self._batched_ds(b"shard/batched_time", idx, labels, degs, sums, ell_n, R)
-        # CCS Ajtai rounds (verify_sumcheck_rounds_ds with domain ccs/ajtai)
+        # ---- CCS Ajtai rounds (verify_sumcheck_rounds_ds with domain ccs/ajtai) ----
         running = finals[0]
         tr.append_message(b"sc/domain", b"ccs/ajtai")
         tr.append_message(b"sc/inst_idx", le64(idx))
@@ -430,9 +596,16 @@ class OracleVerifier:
         if R.k() != running:
             raise VerifyError("Pi_CCS sumcheck_final mismatch")
         fold_digest = tr.digest32()
-        # ME outputs (core rows) and the terminal identity
+        # ---- ME outputs (core rows + bus openings) and the Pi_CCS terminal identity ----
         y_out = [[R.ks(D) for _ in range(t)] for _ in range(k)]
         ysc_out = [R.ks(t) for _ in range(k)]
+        bus_y = []
+        for i in range(k):
+            rows = [R.ks(D) for _ in range(nb)]
+            bsc = R.ks(nb)
+            if self._yscalars(rows) != bsc:
+                raise VerifyError(f"ME output {i}: bus y_scalars do not recompose the bus y rows")
+            bus_y.append((rows, bsc))
         for i in range(k):
             if self._yscalars(y_out[i]) != ysc_out[i]:
                 raise VerifyError(f"Pi_CCS output {i}: y_scalars do not recompose y")
@@ -441,10 +614,115 @@ class OracleVerifier:
         if rhs != running:
             raise VerifyError("Pi_CCS terminal identity check failed")
         srcs = [dict(c=c_mcs, X=Xm)] + [dict(c=me["c"], X=me["X"]) for me in self.acc]
-        outs = [self._me(s["c"], s["X"], r_time, y_out[i], fold_digest) for i, s in enumerate(srcs)]
+        outs = [self._me(s_["c"], s_["X"], r_time, y_out[i] + bus_y[i][0], fold_digest) for i, s_ in enumerate(srcs)]
+
+        # ---- Twist val-eval batch (memory.rs:2088-2170) ----
+        has_prev = self.prev is not None
+        val_claims, r_val, vfin, vsums = [], [], [], []
+        if self.twist:
+            vplan = []
+            for i, w in enumerate(self.twist):
+                ea = w["ell_addr"]
+                vplan += [(b"twist/val_eval_lt", ea + 3, 0), (b"twist/val_eval_total", ea + 2, 1)]
+                if has_prev:
+                    vplan.append((b"twist/rollover_prev_total", ea + 2, 2))
+            vsums = R.ks(len(vplan))
+            tr.append_message(b"twist/val_eval/batch_start", le64(len(self.twist)))
+            tr.append_message(b"twist/val_eval/step_idx", le64(idx))
+            tr.append_message(b"twist/val_eval/claimed_sums_len", le64(len(vplan)))
+            for ci, ((lab, deg, tag), sm) in enumerate(zip(vplan, vsums)):
+                tr.append_message(b"twist/val_eval/claim_idx", le64(ci))
+                tr.append_message(b"twist/val_eval/claim_kind", bytes([tag]))
+                self._k(b"twist/val_eval/claimed_sum", sm)
+            r_val, vfin = self._batched_ds(b"twist/val_eval_batch", idx, [v[0] for v in vplan], [v[1] for v in vplan],
+                                           vsums, ell_n, R)
+            tr.append_message(b"twist/val_eval/batch_done")
+            if R.ks(ell_n) != r_val:
+                raise VerifyError("twist val-eval r_val mismatch")
+            # CPU ME claims at r_val (ts_common.rs:100-258): the current and previous MCS
+            fork = tr.clone_state()
+            fork.append_message(b"fork", b"cpu_bus/me_digest_val")
+            vdigest = fork.digest32()
+            vsrcs = [(c_mcs, Xm)] + ([(self.prev["c"], self.prev["X"])] if has_prev else [])
+            for c_, X_ in vsrcs:
+                rows = [R.ks(D) for _ in range(t + nb)]
+                ysc = R.ks(t + nb)
+                if self._yscalars(rows) != ysc:
+                    raise VerifyError("CPU ME(val): y_scalars do not recompose y")
+                val_claims.append(self._me(c_, X_, r_val, rows, vdigest))
+
+        # ---- verify_route_a_memory_step (memory.rs:1671-2380) ----
+        if self.shout or self.twist:
+            chi_c = keq(r_time, r_cycle)
+            o0 = bus_y[0][1]  # bus y_scalars of the MCS output at r_time
+            ci = 1
+            for i, (sd, sc) in enumerate(zip(self.shout, bus.shout)):
+                ea = sd["ell_addr"]
+                bits = [o0[c] for c in sc["addr_bits"]]
+                has, val = o0[sc["has_lookup"]], o0[sc["val"]]
+                pre = shout_pre[i]
+                if self._bitness_expected(chi_c, r_cycle[0], bits + [has], 0x5348_4F55_54 + i) != finals[ci + 2]:
+                    raise VerifyError("shout/bitness terminal value mismatch")
+                if kmulp(chi_c, kmulp(has, val)) != finals[ci]:
+                    raise VerifyError("shout value terminal value mismatch")
+                if kmulp(chi_c, kmulp(has, self._eq_bits(bits, r_addr_s))) != finals[ci + 1]:
+                    raise VerifyError("shout adapter terminal value mismatch")
+                if sums[ci] != pre["claim"]:
+                    raise VerifyError("shout value claimed sum != addr claimed sum")
+                if pre["active"]:
+                    if kmulp(pre["table_eval"], sums[ci + 1]) != pre["final"]:
+                        raise VerifyError("shout addr terminal value mismatch")
+                elif pre["claim"] != ZERO or sums[ci + 1] != ZERO or pre["final"] != ZERO:
+                    raise VerifyError("shout addr-pre skipped but a claim is nonzero")
+                ci += 3
+            lt = self._lt_eval(r_val, r_time) if self.twist else ZERO
+            per = 3 if has_prev else 2
+            for i, (w, tc) in enumerate(zip(self.twist, bus.twist)):
+                pre = twist_pre[i]
+                r_addr = pre["r_addr"]
+                ra = [o0[c] for c in tc["ra_bits"]]
+                wa = [o0[c] for c in tc["wa_bits"]]
+                hr, hw, wv, rv, inc = (o0[tc[n]] for n in ("has_read", "has_write", "wv", "rv", "inc"))
+                if sums[ci] != pre["read"] or sums[ci + 1] != pre["write"]:
+                    raise VerifyError("twist read/write check claimed sum != addr-pre final")
+                if self._bitness_expected(chi_c, r_cycle[0], ra + wa + [hr, hw], 0x5457_4953_54 + i) != finals[ci + 2]:
+                    raise VerifyError("twist/bitness terminal value mismatch")
+                claimed_val = kadd(self._init_at(w.get("init", []), r_addr), vsums[per * i])
+                exp_r = kmulp(chi_c, kmulp(hr, kmulp(ksub(claimed_val, rv), self._eq_bits(ra, r_addr))))
+                if exp_r != finals[ci]:
+                    raise VerifyError("twist/read_check terminal value mismatch")
+                exp_w = kmulp(chi_c, kmulp(hw, kmulp(ksub(ksub(wv, claimed_val), inc), self._eq_bits(wa, r_addr))))
+                if exp_w != finals[ci + 1]:
+                    raise VerifyError("twist/write_check terminal value mismatch")
+                # val-eval terminals against the CPU ME openings at r_val
+                ov = val_claims[0]["ysc"][t:]
+                inc_v = kmulp(ov[tc["has_write"]], kmulp(ov[tc["inc"]], self._eq_bits([ov[c] for c in tc["wa_bits"]],
+                                                                                     r_addr)))
+                if kmulp(inc_v, lt) != vfin[per * i]:
+                    raise VerifyError("twist/val_eval_lt terminal value mismatch")
+                if inc_v != vfin[per * i + 1]:
+                    raise VerifyError("twist/val_eval_total terminal value mismatch")
+                if has_prev:
+                    op = val_claims[1]["ysc"][t:]
+                    inc_p = kmulp(op[tc["has_write"]], kmulp(op[tc["inc"]],
+                                                             self._eq_bits([op[c] for c in tc["wa_bits"]], r_addr)))
+                    if inc_p != vfin[per * i + 2]:
+                        raise VerifyError("twist/rollover_prev_total terminal value mismatch")
+                    # Init_i(r_addr) == Init_{i-1}(r_addr) + PrevTotal(i)
+                    prev_init = self._init_at(self.prev["init"][i], r_addr)
+                    if self._init_at(w.get("init", []), r_addr) != kadd(prev_init, vsums[per * i + 2]):
+                        raise VerifyError("twist rollover init check failed")
+                ci += 3
+
+        # ---- main lane, val lane ----
         children = self._lane(b"main", idx, outs, r_time, fold_digest, R)
+        if val_claims:
+            tr.append_message(b"fold/val_lane_start", le64(idx))
+            self.val_obligations += self._lane(b"val", idx, val_claims, r_val, vdigest, R)
         tr.append_message(b"fold/step_done", le64(idx))
         R.done()
         self.acc = children
+        if self.twist:
+            self.prev = dict(c=c_mcs, X=Xm, init=[list(w.get("init", [])) for w in self.twist])
         self.step_idx += 1
         return True

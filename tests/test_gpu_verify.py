@@ -24,3 +24,20 @@ def test_verifier_accepts_gpu_proofs(ctx, ell):
     with pytest.raises(VerifyError):
         v.verify_step(z[:1], P)
     g.close()
+
+
+def test_verifier_accepts_gpu_memory_chunks(ctx):
+    """Three consecutive chunks of one trace proven by the CUDA library (one
+    Shout table of 2^10 entries, one Twist memory of 2^8 cells, 64 trace steps
+    per fold step) pass every memory-sidecar check of the verifier."""
+    ccs, zs, mem, inits = synth.make_memory_workload_chunks(13, 21, 3, 64, 10, 8)
+    ctx.pp_generate(bytes(range(1, 33)), 16, 1 << 13, 1)
+    g = gpu.Shard(ctx, ccs, m_in=1, k_rho=12, app_label=b"neo/gpu-verify-mem", mem=mem)
+    v = OracleVerifier(ccs, m_in=1, k_rho=12, kappa=16, app_label=b"neo/gpu-verify-mem", mem=mem)
+    for c in range(3):
+        if c:
+            g.set_twist_init(0, inits[c][0])
+            v.set_twist_init(0, inits[c][0])
+        assert v.verify_step(zs[c][:1], g.fold_step(zs[c]))
+    assert len(v.val_obligations) == g.val_obligations() == 36
+    g.close()
