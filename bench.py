@@ -64,16 +64,33 @@ def parse():
 MEM_TWIST_ELL, MEM_SHOUT_ELL = 12, 16
 
 
-def workload(args, rank):
-    """(ccs, z, pp, mem) of the benchmarked shard."""
-    from nightstream_b200 import synth
-    ell = args.ell
-    pp = np.random.default_rng(99 + rank).integers(0, Q, size=(16, 1 << ell, 54), dtype=np.uint64)
-    if args.workload == "memory":
-        ccs, z, mem = synth.make_memory_workload(ell, 1234 + rank, args.chunk, MEM_SHOUT_ELL, MEM_TWIST_ELL)
-        return ccs, z, pp, mem
-    ccs, z = synth.make_r1cs(ell, 1234 + rank)
-    return ccs, z, pp, None
+class Workload:
+    """The benchmarked shard: its CCS, PP, memory instances and, per fold step,
+    the witness and the Twist MemInits.  With memory the fold steps prove
+    consecutive chunks of one trace (at least 2^14 trace steps): chunk c's
+    witness carries chunk c's bus columns and its Twist memory starts from the
+    state chunk c-1 left.  Without memory every step reuses one witness."""
+
+    def __init__(self, args, rank, n_steps):
+        from nightstream_b200 import synth
+        ell = args.ell
+        self.pp = np.random.default_rng(99 + rank).integers(0, Q, size=(16, 1 << ell, 54), dtype=np.uint64)
+        if args.workload == "memory":
+            n = max(n_steps, (1 << 14) // args.chunk)
+            self.ccs, self.zs, self.mem, self.inits = synth.make_memory_workload_chunks(
+                ell, 1234 + rank, n, args.chunk, MEM_SHOUT_ELL, MEM_TWIST_ELL)
+        else:
+            self.ccs, z = synth.make_r1cs(ell, 1234 + rank)
+            self.zs, self.mem, self.inits = [z], None, None
+
+    def z(self, c):
+        return self.zs[c % len(self.zs)]
+
+    def prepare(self, shard, c):
+        """Set the MemInits of step c on a GPU shard or an oracle shard (c > 0)."""
+        if self.inits and c:
+            for i, init in enumerate(self.inits[c % len(self.zs)]):
+                shard.set_twist_init(i, init)
 
 
 def config(args):
@@ -81,8 +98,10 @@ def config(args):
     if args.workload == "memory":
         bus_cols = (MEM_SHOUT_ELL + 2) + (2 * MEM_TWIST_ELL + 5)
         return {
-            "workload": f"single shard with memory: steady-state fold step of an R1CS n=m=2^{ell} (k=13) carrying "
-                        f"the shared CPU bus of {args.chunk} trace steps per fold step; one Twist memory of "
+            "workload": f"single shard with memory: steady-state fold steps of an R1CS n=m=2^{ell} (k=13), each "
+                        f"proving the next chunk of {args.chunk} trace steps of one trace of >= 2^14 steps (the "
+                        f"chunk's shared CPU bus in the witness tail, its Twist memory starting from the state the "
+                        f"previous chunk left); one Twist memory of "
                         f"2^{MEM_TWIST_ELL} cells (1 read + 1 write per step, 70% stride-4 / 30% uniform "
                         f"addresses, 32-bit values), one Shout table of 2^{MEM_SHOUT_ELL} uniform 32-bit entries "
                         f"(uniform lookups); Route-A batched time claims + Twist val-eval + val lane",
@@ -247,13 +266,14 @@ def int8_peak_tops():
         return 2 * pk, f"2x measured bf16 (int8 GEMM unavailable: {type(ex).__name__})"
 
 
-def cpu_baseline(args, ccs, z, pp, mem):
+def cpu_baseline(args, wl):
     """One oracle fold step (C restatement, OpenMP on all host cores) after step 0."""
     from oracle.fold import OracleShard
-    sh = OracleShard(ccs, pp, m_in=1, k_rho=12, app_label=b"neo/bench", mem=mem)
-    sh.fold_step(z)  # step 0 (k = 1)
+    sh = OracleShard(wl.ccs, wl.pp, m_in=1, k_rho=12, app_label=b"neo/bench", mem=wl.mem)
+    sh.fold_step(wl.z(0))  # step 0 (k = 1)
+    wl.prepare(sh, 1)
     t0 = time.perf_counter()
-    sh.fold_step(z)
+    sh.fold_step(wl.z(1))
     dt = time.perf_counter() - t0
     return {"value": 1.0 / dt, "unit": UNIT, "cores": os.cpu_count(), "kind": "port",
             "sample": f"one steady-state fold step (k=13, {args.workload} workload) at n=m=2^{args.ell} on the C "
@@ -288,10 +308,12 @@ def pp_setup_result(args, ctx, m, kappa=16, reps=3):
     return out
 
 
-def shard_mix(n_shards, lo, hi, seed, memory=True):
+def shard_mix(n_shards, lo, hi, seed, steps, memory=True):
     """n_shards synthetic shards with log2(n) uniform in [lo, hi]; with memory,
     each carries a Twist memory of 2^10 cells and a 2^12-entry Shout table on
-    its shared CPU bus, min(1024, n/64) trace steps per fold step."""
+    its shared CPU bus, min(1024, n/64) trace steps per fold step, and its
+    `steps` fold steps prove consecutive chunks of one trace (per-step witness
+    and Twist MemInit).  Entries: (ell, ccs, witnesses, mem, inits)."""
     from nightstream_b200 import synth
     rng = np.random.default_rng(seed)
     ells = rng.integers(lo, hi + 1, size=n_shards)
@@ -300,10 +322,12 @@ def shard_mix(n_shards, lo, hi, seed, memory=True):
         ell = int(ell)
         if memory:
             chunk = min(1024, (1 << ell) // 64)
-            ccs, z, mem = synth.make_memory_workload(ell, seed * 1000 + i, chunk, BATCH_SHOUT_ELL, BATCH_TWIST_ELL)
+            ccs, zs, mem, inits = synth.make_memory_workload_chunks(ell, seed * 1000 + i, steps, chunk,
+                                                                    BATCH_SHOUT_ELL, BATCH_TWIST_ELL)
         else:
-            (ccs, z), mem = synth.make_r1cs(ell, seed * 1000 + i), None
-        out.append((ell, ccs, z, mem))
+            (ccs, z), mem, inits = synth.make_r1cs(ell, seed * 1000 + i), None, None
+            zs = [z] * steps
+        out.append((ell, ccs, zs, mem, inits))
     return out
 
 
@@ -318,7 +342,8 @@ def run_mix(mix, shards, steps, workers):
     from nightstream_b200 import gpu
     b = gpu.Batch(0, n_workers=workers)
     t0 = time.perf_counter()
-    ids = [b.submit(ccs, z, steps, app_label=b"neo/mix-%d" % i, mem=mem) for i, (ell, ccs, z, mem) in enumerate(shards)]
+    ids = [b.submit(ccs, zs, steps, app_label=b"neo/mix-%d" % i, mem=mem, inits=inits)
+           for i, (ell, ccs, zs, mem, inits) in enumerate(shards)]
     b.wait_all(3600)
     dt = time.perf_counter() - t0
     infos = [b.job_info(j) for j in ids]
@@ -331,7 +356,7 @@ def run_mix(mix, shards, steps, workers):
 def batched_result(args):
     from nightstream_b200 import gpu
     workers = args.workers or min(16, os.cpu_count() or 8)
-    shards = shard_mix(args.shards, 10, 16, 77)
+    shards = shard_mix(args.shards, 10, 16, 77, args.shard_steps)
     ctx = gpu.Context(0)
     upload_pps(ctx, [s[0] for s in shards])
     steps = args.shard_steps
@@ -368,7 +393,7 @@ def run_served(args):
     from nightstream_b200 import gpu
     workers = args.workers or min(16, os.cpu_count() or 8)
     n_req = args.shards
-    shards = shard_mix(n_req, 10, 18, 91)
+    shards = shard_mix(n_req, 10, 18, 91, args.shard_steps)
     ctx = gpu.Context(0)
     upload_pps(ctx, [s[0] for s in shards])
     rates = [2.0, 5.0, 10.0]
@@ -380,11 +405,11 @@ def run_served(args):
         t0 = time.perf_counter()
         ids = []
         t_next = t0
-        for i, (ell, ccs, z, mem) in enumerate(shards):
+        for i, (ell, ccs, zs, mem, inits) in enumerate(shards):
             t_next += gaps[i]
             while time.perf_counter() < t_next:
                 time.sleep(min(0.005, max(0.0, t_next - time.perf_counter())))
-            ids.append(b.submit(ccs, z, args.shard_steps, app_label=b"neo/req-%d" % i, mem=mem))
+            ids.append(b.submit(ccs, zs, args.shard_steps, app_label=b"neo/req-%d" % i, mem=mem, inits=inits))
         b.wait_all(3600)
         dt = time.perf_counter() - t0
         infos = [b.job_info(j) for j in ids]
@@ -408,20 +433,28 @@ def run_reference(args, rank, world):
     if rank != 0:
         return
     from oracle.fold import OracleShard
-    ccs, z, pp, mem = workload(args, 0)
-    sh = OracleShard(ccs, pp, m_in=1, k_rho=12, app_label=b"neo/bench", mem=mem)
-    sh.fold_step(z)
+    wl = Workload(args, 0, 2 + args.warmup + args.steps)
+    sh = OracleShard(wl.ccs, wl.pp, m_in=1, k_rho=12, app_label=b"neo/bench", mem=wl.mem)
+    c = 0
+
+    def step():
+        nonlocal c
+        wl.prepare(sh, c)
+        sh.fold_step(wl.z(c))
+        c += 1
+
+    step()
     t0 = time.perf_counter()
-    sh.fold_step(z)
+    step()
     est = time.perf_counter() - t0
     budget = 150.0
     warm = min(args.warmup, max(0, int(budget / 3 / est) - 1))
     steps = max(1, min(args.steps, int(budget / est)))
     for _ in range(warm):
-        sh.fold_step(z)
+        step()
     t0 = time.perf_counter()
     for _ in range(steps):
-        sh.fold_step(z)
+        step()
     dt = time.perf_counter() - t0
     value = steps / dt
     out = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": steps,
@@ -443,18 +476,29 @@ def run_ours(args, rank, world, local_rank):
     dist = None
     if world > 1:
         import torch.distributed as dist
-    ccs, z, pp, mem = workload(args, rank)
+    n_steps = 1 + args.warmup + 2 * args.steps
+    wl = Workload(args, rank, n_steps)
+    ccs, pp, mem = wl.ccs, wl.pp, wl.mem
     m = 1 << args.ell
     ctx = gpu.Context(local_rank)
     ctx.pp_upload(pp)
     shard = gpu.Shard(ctx, ccs, m_in=1, k_rho=12, app_label=b"neo/bench", mem=mem)
     stream = torch.cuda.ExternalStream(ctx.stream)
-    zt = torch.from_numpy(z.view(np.int64).copy()).cuda()
-    d_z = zt.data_ptr()
+    # every step's witness resident in HBM (one row per fold step)
+    zt = torch.from_numpy(np.stack([wl.z(c) for c in range(n_steps)]).view(np.int64).copy()).cuda()
+    z_ptr = lambda c: zt.data_ptr() + c * m * 8
+    cur = 0
+
+    def step_device():
+        nonlocal cur
+        wl.prepare(shard, cur)
+        shard.fold_step_device(z_ptr(cur))
+        cur += 1
+
     torch.cuda.synchronize()
-    shard.fold_step_device(d_z)  # step 0: k = 1 -> steady state afterwards
+    step_device()  # step 0: k = 1 -> steady state afterwards
     for _ in range(args.warmup):
-        shard.fold_step_device(d_z)
+        step_device()
     ctx.synchronize()
 
     def barrier():
@@ -469,7 +513,7 @@ def run_ours(args, rank, world, local_rank):
     torch.cuda.synchronize()
     ev0.record(stream)
     for _ in range(args.steps):
-        shard.fold_step_device(d_z)
+        step_device()
     ev1.record(stream)
     ev1.synchronize()
     torch.cuda.synchronize()
@@ -487,14 +531,15 @@ def run_ours(args, rank, world, local_rank):
     # end-to-end through the C ABI with host buffers: pinned z in, proof words out
     e2e = None
     if not args.no_e2e:
-        zp = torch.from_numpy(z.view(np.int64).copy()).pin_memory()
-        zh = zp.numpy().view(np.uint64)
-        proof = shard.fold_step(zh)  # sizes the proof buffer
+        zp = torch.from_numpy(np.stack([wl.z(c) for c in range(cur, cur + args.steps)]).view(np.int64).copy())
+        zh = zp.pin_memory().numpy().view(np.uint64)
         barrier()
         ctx.synchronize()
         ev0.record(stream)
-        for _ in range(args.steps):
-            proof = shard.fold_step(zh)
+        for i in range(args.steps):
+            wl.prepare(shard, cur)
+            proof = shard.fold_step(zh[i])
+            cur += 1
         ev1.record(stream)
         ev1.synchronize()
         ems = ev0.elapsed_time(ev1)
@@ -502,7 +547,7 @@ def run_ours(args, rank, world, local_rank):
             t = torch.tensor([ems], device="cuda")
             dist.all_reduce(t, op=dist.ReduceOp.MAX)
             ems = float(t.item())
-        e2e = {"value": world * args.steps / (ems * 1e-3), "unit": UNIT, "h2d_bytes_per_step": int(zh.nbytes),
+        e2e = {"value": world * args.steps / (ems * 1e-3), "unit": UNIT, "h2d_bytes_per_step": int(zh[0].nbytes),
                "d2h_bytes_per_step": int(proof.nbytes)}
 
     # dominant kernel roofline: the DEC batch commitment (12 digit planes, one launch pair)
@@ -530,7 +575,7 @@ def run_ours(args, rank, world, local_rank):
                        "traffic_source": "ncu dram__bytes_read+write of one 12-plane launch at m = 2^14, scaled by m "
                                          "(profiles/commit_tc_kernel_m16384_12planes.md)",
                        "launch_ms": commit_ms, "peak_source": peak_src, "algorithmic_ops_per_launch": ops}
-    roofline = rounds_roofline(ctx, ccs, z, args.ell, stream)
+    roofline = rounds_roofline(ctx, ccs, wl.z(0), args.ell, stream)
     pp_setup = pp_setup_result(args, ctx, m) if rank == 0 else None
 
     if rank == 0:
@@ -541,7 +586,7 @@ def run_ours(args, rank, world, local_rank):
                "roofline": roofline, "roofline_commit": roofline_commit, "step_breakdown_ms": stats}
         out["pp_setup"] = pp_setup
         if world == 1 and not args.no_cpu_baseline:
-            out["cpu_baseline"] = cpu_baseline(args, ccs, z, pp, mem)
+            out["cpu_baseline"] = cpu_baseline(args, wl)
         if world == 1 and not args.no_batch:
             out["batched"] = batched_result(args)
         print(json.dumps(out), flush=True)

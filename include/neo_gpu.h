@@ -353,6 +353,20 @@ int neo_gpu_batch_submit(neo_gpu_batch* b, const neo_ccs_desc* ccs, const uint64
 int neo_gpu_batch_submit_mem(neo_gpu_batch* b, const neo_ccs_desc* ccs, const neo_mem_desc* mem, const uint64_t* z,
                              uint32_t n_steps, uint32_t m_in, uint32_t k_rho, const char* app_label,
                              uint64_t* job_id);
+/* A request whose fold steps prove consecutive chunks of one trace: zs holds
+ * n_steps witnesses of ccs->m words (step s proves zs[s*m ..]) and inits the
+ * MemInit of every Twist instance before each step, row-major
+ * [n_steps][mem->n_twist] (row 0 unused: the instances' own init; NULL: keep
+ * them) -- what neo_gpu_shard_set_twist_init does between the steps of one
+ * shard.  mem may have no instances (then inits is ignored). */
+typedef struct {
+    uint64_t n_init;        /* 0: MemInit::Zero */
+    const uint64_t* addr;   /* strictly increasing, < 2^ell_addr */
+    const uint64_t* val;
+} neo_mem_init;
+int neo_gpu_batch_submit_chunks(neo_gpu_batch* b, const neo_ccs_desc* ccs, const neo_mem_desc* mem,
+                                const uint64_t* zs, const neo_mem_init* inits, uint32_t n_steps, uint32_t m_in,
+                                uint32_t k_rho, const char* app_label, uint64_t* job_id);
 /* Waits until every submitted request has finished (NEO_ERR_CUDA on timeout). */
 int neo_gpu_batch_wait_all(neo_gpu_batch* b, double timeout_ms);
 /* times3 = {submit->done ms, submit->admit ms, submit time since creation ms};

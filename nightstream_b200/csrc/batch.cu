@@ -91,8 +91,10 @@ struct Job {
     uint64_t id = 0;
     std::unique_ptr<CcsCopy> ccs;
     std::unique_ptr<MemCopy> mem;
-    std::vector<uint64_t> z;
+    std::vector<uint64_t> z;  // one witness (every step) or n_steps witnesses of m words
     uint32_t n_steps = 0, m_in = 1, k_rho = 12;
+    // per step s >= 1 and Twist instance: the MemInit set before step s (empty vector: none given)
+    std::vector<std::vector<std::pair<std::vector<uint64_t>, std::vector<uint64_t>>>> inits;
     std::string label;
     uint64_t footprint = 0;
     neo_gpu_shard* shard = nullptr;
@@ -201,9 +203,17 @@ static void worker_main(neo_gpu_batch* b, size_t wi) {
             rc = j->mem ? neo_gpu_shard_create_mem(w.ctx, &j->ccs->d, j->m_in, j->k_rho, j->label.c_str(), &j->mem->d,
                                                    &j->shard)
                         : neo_gpu_shard_create(w.ctx, &j->ccs->d, j->m_in, j->k_rho, j->label.c_str(), &j->shard);
+        if (rc == NEO_OK && j->steps_done > 0 && j->steps_done < j->inits.size()) {
+            auto& st = j->inits[j->steps_done];
+            for (uint32_t i = 0; rc == NEO_OK && i < st.size(); i++)
+                rc = neo_gpu_shard_set_twist_init(j->shard, i, st[i].first.size(), st[i].first.data(),
+                                                  st[i].second.data());
+        }
         if (rc == NEO_OK) {
             uint64_t len = 0;
-            rc = neo_gpu_shard_fold_step(j->shard, j->z.data(), nullptr, 0, &len);
+            const uint64_t m = j->ccs->d.m;
+            const uint64_t* zs = j->z.size() > m ? j->z.data() + (uint64_t)j->steps_done * m : j->z.data();
+            rc = neo_gpu_shard_fold_step(j->shard, zs, nullptr, 0, &len);
             if (rc == NEO_OK) j->steps_done++;
         }
         if (rc != NEO_OK || j->steps_done == j->n_steps) {
@@ -244,12 +254,24 @@ extern "C" int neo_gpu_batch_set_reserve(neo_gpu_batch* b, uint64_t bytes) {
 }
 
 static int submit_impl(neo_gpu_batch* b, const neo_ccs_desc* ccs, const neo_mem_desc* mem, const uint64_t* z,
-                       uint32_t n_steps, uint32_t m_in, uint32_t k_rho, const char* app_label, uint64_t* job_id) {
+                       uint32_t n_steps, uint32_t m_in, uint32_t k_rho, const char* app_label, uint64_t* job_id,
+                       bool per_step = false, const neo_mem_init* inits = nullptr) {
     if (!b || !ccs || !z || !app_label || !job_id || n_steps == 0 || ccs->m == 0) return NEO_ERR_ARG;
     auto j = std::make_unique<Job>();
     j->ccs = std::make_unique<CcsCopy>(ccs);
     if (mem && (mem->n_shout || mem->n_twist)) j->mem = std::make_unique<MemCopy>(mem);
-    j->z.assign(z, z + ccs->m);
+    j->z.assign(z, z + (per_step ? (uint64_t)n_steps : 1ull) * ccs->m);
+    const uint32_t n_twist = j->mem ? j->mem->d.n_twist : 0;
+    if (inits && n_twist) {
+        j->inits.resize(n_steps);
+        for (uint32_t st = 1; st < n_steps; st++)
+            for (uint32_t i = 0; i < n_twist; i++) {
+                const neo_mem_init& e = inits[(uint64_t)st * n_twist + i];
+                if (e.n_init && (!e.addr || !e.val)) return NEO_ERR_ARG;
+                j->inits[st].emplace_back(std::vector<uint64_t>(e.addr, e.addr + e.n_init),
+                                          std::vector<uint64_t>(e.val, e.val + e.n_init));
+            }
+    }
     j->n_steps = n_steps;
     j->m_in = m_in;
     j->k_rho = k_rho;
@@ -283,6 +305,12 @@ extern "C" int neo_gpu_batch_submit_mem(neo_gpu_batch* b, const neo_ccs_desc* cc
                                         const uint64_t* z, uint32_t n_steps, uint32_t m_in, uint32_t k_rho,
                                         const char* app_label, uint64_t* job_id) {
     return submit_impl(b, ccs, mem, z, n_steps, m_in, k_rho, app_label, job_id);
+}
+
+extern "C" int neo_gpu_batch_submit_chunks(neo_gpu_batch* b, const neo_ccs_desc* ccs, const neo_mem_desc* mem,
+                                           const uint64_t* zs, const neo_mem_init* inits, uint32_t n_steps,
+                                           uint32_t m_in, uint32_t k_rho, const char* app_label, uint64_t* job_id) {
+    return submit_impl(b, ccs, mem, zs, n_steps, m_in, k_rho, app_label, job_id, true, inits);
 }
 
 extern "C" int neo_gpu_batch_wait_all(neo_gpu_batch* b, double timeout_ms) {

@@ -63,6 +63,7 @@ SIGNATURES = {
     "neo_gpu_batch_set_reserve": [P, U64],
     "neo_gpu_batch_submit": [P, P, P, U32, U32, U32, ctypes.c_char_p, P],
     "neo_gpu_batch_wait_all": [P, ctypes.c_double],
+    "neo_gpu_batch_submit_chunks": [P, P, P, P, P, U32, U32, U32, ctypes.c_char_p, P],
     "neo_gpu_batch_submit_mem": [P, P, P, P, U32, U32, U32, ctypes.c_char_p, P],
     "neo_gpu_batch_job_info": [P, U64, P, P, P],
     "neo_gpu_batch_kernel_launches": [P],
@@ -434,6 +435,10 @@ class MemInstance(ctypes.Structure):
                 ("table_len", U64), ("n_init", U64), ("init_addr", P), ("init_val", P)]
 
 
+class MemInit(ctypes.Structure):
+    _fields_ = [("n_init", U64), ("addr", P), ("val", P)]
+
+
 class MemDesc(ctypes.Structure):
     _fields_ = [("steps", U64), ("n_shout", U32), ("shout", P), ("n_twist", U32), ("twist", P)]
 
@@ -617,11 +622,36 @@ class Batch:
             self.lib.neo_gpu_batch_set_reserve(self.h, reserve_bytes)
         self._descs = []
 
-    def submit(self, ccs, z: np.ndarray, n_steps: int, m_in: int = 1, k_rho: int = 12,
-               app_label: bytes = b"neo/shard", mem: dict = None) -> int:
+    def submit(self, ccs, z, n_steps: int, m_in: int = 1, k_rho: int = 12,
+               app_label: bytes = b"neo/shard", mem: dict = None, inits=None) -> int:
+        """z: one witness for every step, or a list of n_steps witnesses (consecutive
+        trace chunks) with inits[s][i] = the MemInit [(addr, value)] of Twist i
+        before step s (neo_gpu_batch_submit_chunks)."""
         desc = ccs.desc()
-        z = _u64(z)
         jid = ctypes.c_uint64()
+        if isinstance(z, (list, tuple)):
+            if len(z) != n_steps:
+                raise ValueError("one witness per step")
+            zs = np.ascontiguousarray(np.stack([_u64(v) for v in z]))
+            md = _mem_desc(mem) if mem else None
+            n_twist = len(mem.get("twist", [])) if mem else 0
+            arr, keep = None, []
+            if inits is not None and n_twist:
+                arr = (MemInit * (n_steps * n_twist))()
+                for s_ in range(1, n_steps):
+                    for i in range(n_twist):
+                        pairs = inits[s_][i]
+                        a = np.array([int(x) for x, _ in pairs], np.uint64)
+                        v = np.array([int(y) % 0xFFFFFFFF00000001 for _, y in pairs], np.uint64)
+                        keep += [a, v]
+                        e = arr[s_ * n_twist + i]
+                        e.n_init, e.addr, e.val = len(pairs), _p(a) if len(pairs) else None, _p(v) if len(pairs) else None
+            rc = self.lib.neo_gpu_batch_submit_chunks(self.h, ctypes.byref(desc), ctypes.byref(md) if md else None,
+                                                      _p(zs), arr, n_steps, m_in, k_rho, app_label, ctypes.byref(jid))
+            if rc:
+                raise NeoGpuError(rc, "batch submit")
+            return jid.value
+        z = _u64(z)
         if mem and (mem.get("shout") or mem.get("twist")):
             md = _mem_desc(mem)
             rc = self.lib.neo_gpu_batch_submit_mem(self.h, ctypes.byref(desc), ctypes.byref(md), _p(z), n_steps, m_in,

@@ -66,3 +66,43 @@ def test_batch_memory_shards_equal_oracle(ctx):
         assert info["status"] == 1, info
         assert np.array_equal(info["transcript_state"], expect[i]), f"memory shard {i} in the mix"
     mix.close()
+
+
+def test_batch_trace_chunks_equal_oracle(ctx):
+    """Memory shards whose fold steps prove consecutive chunks of one trace
+    (neo_gpu_batch_submit_chunks: per-step witness and Twist MemInit), mixed
+    with a main-lane shard, end in the oracle's transcript state."""
+    cfg = [(10, 16), (12, 32), (11, 16)]
+    steps = 3
+    shards = [synth.make_memory_workload_chunks(ell, 700 + i, steps, chunk, 8, 6) for i, (ell, chunk) in enumerate(cfg)]
+    ccs_m, z_m = synth.make_r1cs(11, 777)
+    for ell in sorted({c[0] for c in cfg} | {11}):
+        pp = np.random.default_rng(3000 + ell).integers(0, Q, size=(16, 1 << ell, 54), dtype=np.uint64)
+        ctx.pp_upload(pp)
+    expect = []
+    for i, (ccs, zs, mem, inits) in enumerate(shards):
+        ell = cfg[i][0]
+        pp = np.random.default_rng(3000 + ell).integers(0, Q, size=(16, 1 << ell, 54), dtype=np.uint64)
+        o = OracleShard(ccs, pp, app_label=b"neo/cbatch-%d" % i, mem=mem)
+        for c in range(steps):
+            if c:
+                o.set_twist_init(0, inits[c][0])
+            o.fold_step(zs[c])
+        expect.append(o.tr.state())
+    pp = np.random.default_rng(3011).integers(0, Q, size=(16, 1 << 11, 54), dtype=np.uint64)
+    o = OracleShard(ccs_m, np.random.default_rng(3000 + 11).integers(0, Q, size=(16, 1 << 11, 54), dtype=np.uint64),
+                    app_label=b"neo/cbatch-main")
+    for _ in range(steps):
+        o.fold_step(z_m)
+    expect_main = o.tr.state()
+    mix = gpu.Batch(0, n_workers=2)
+    ids = [mix.submit(ccs, zs, steps, app_label=b"neo/cbatch-%d" % i, mem=mem, inits=inits)
+           for i, (ccs, zs, mem, inits) in enumerate(shards)]
+    jm = mix.submit(ccs_m, [z_m] * steps, steps, app_label=b"neo/cbatch-main")
+    mix.wait_all(600)
+    for i, jid in enumerate(ids):
+        info = mix.job_info(jid)
+        assert info["status"] == 1, info
+        assert np.array_equal(info["transcript_state"], expect[i]), f"chunked memory shard {i}"
+    assert np.array_equal(mix.job_info(jm)["transcript_state"], expect_main)
+    mix.close()
