@@ -37,3 +37,21 @@ def test_transcript_distinct_labels_give_distinct_challenges():
 def test_ccs_digest_matches_oracle():
     ccs, _ = synth.make_r1cs(6, 3)
     assert np.array_equal(gpu.ccs_digest(ccs), O.ccs_digest(ccs))
+
+
+def test_ccs_digest_cache_returns_each_ccs_its_own_digest():
+    """The library keeps digests of CCSs it has seen (matched on an exact copy
+    of the matrices): repeated and interleaved lookups, and a CCS that differs
+    from a cached one in a single coefficient, all equal the oracle."""
+    import copy
+    from nightstream_b200 import synth
+    a, _ = synth.make_r1cs(9, 41)
+    b, _ = synth.make_r1cs(9, 42)
+    c = copy.deepcopy(a)
+    M = c.matrices[2]
+    M.vals = M.vals.copy()
+    M.vals[3] = (int(M.vals[3]) + 1) % ((1 << 64) - (1 << 32) + 1)
+    want = {k: O.ccs_digest(x) for k, x in (("a", a), ("b", b), ("c", c))}
+    for k, x in (("a", a), ("b", b), ("a", a), ("c", c), ("b", b), ("c", c), ("a", a)):
+        assert np.array_equal(gpu.ccs_digest(x), want[k]), k
+    assert not np.array_equal(want["a"], want["c"])
