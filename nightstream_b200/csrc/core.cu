@@ -33,7 +33,6 @@ extern "C" int neo_gpu_ctx_destroy(neo_gpu_ctx* ctx) {
     cudaStreamSynchronize(ctx->stream);
     if (ctx->scratch) cudaFree(ctx->scratch);
     if (ctx->d_err) cudaFree(ctx->d_err);
-    if (ctx->sync_ev) cudaEventDestroy(ctx->sync_ev);
     cudaStreamDestroy(ctx->stream);
     delete ctx;
     return NEO_OK;

@@ -865,7 +865,6 @@ static int rlc_dec_lane(neo_gpu_shard* sh, const char* lane, uint32_t idx, const
     NEO_CK(ctx, ctx_d2h(ctx, flags, sh->d_flags.p, 8));
     NEO_CK(ctx, ctx_d2h(ctx, cc.data(), sh->d_commits.p, cc.size() * 8));
     NEO_CK(ctx, ctx_d2h(ctx, yc.data(), sh->d_ychild.p, yc.size() * 16));
-    if (ctx->blocking) NEO_CK(ctx, ctx_sync(ctx));
     NEO_CK(ctx, cudaMemcpy2DAsync(Xc.data(), sh->m_in, d_planes, m, sh->m_in, (size_t)sh->k_rho * NEO_D,
                                   cudaMemcpyDeviceToHost, ctx->stream));
     NEO_CK(ctx, ctx_sync(ctx));
@@ -973,7 +972,6 @@ static int fold_step_impl(neo_gpu_shard* sh, const uint64_t* z_host, const uint6
     std::vector<int8_t> Xd((size_t)NEO_D * sh->m_in);
     NEO_CK(ctx, ctx_d2h(ctx, mcs.c.data(), sh->d_commits.p, mcs.c.size() * 8));
     NEO_CK(ctx, ctx_d2h(ctx, x.data(), d_z, sh->m_in * 8));
-    if (ctx->blocking) NEO_CK(ctx, ctx_sync(ctx));
     NEO_CK(ctx, cudaMemcpy2DAsync(Xd.data(), sh->m_in, sh->Zall.p, m, sh->m_in, NEO_D, cudaMemcpyDeviceToHost, ctx->stream));
     NEO_CK(ctx, ctx_sync(ctx));
     if ((rc = check_device_error(ctx))) return rc;

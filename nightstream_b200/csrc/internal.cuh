@@ -20,10 +20,6 @@ struct neo_gpu_ctx {
     uint32_t* d_err = nullptr;       // device error word (bounded-wait timeouts); 0 = ok
     void* scratch = nullptr;         // growable per-context scratch (stream-ordered use)
     size_t scratch_bytes = 0;
-    // blocking waits: the host thread sleeps in ctx_sync instead of spinning
-    // (worker threads of a batch leave the CPU to other shards' transcripts)
-    cudaEvent_t sync_ev = nullptr;
-    bool blocking = false;
     int fail(int code, const char* what, cudaError_t e = cudaSuccess) {
         char buf[512];
         if (e != cudaSuccess)
@@ -35,33 +31,12 @@ struct neo_gpu_ctx {
     }
 };
 
-// wait for the context's stream: a blocking-sync event when the context is
-// in blocking mode, a (spinning) stream synchronization otherwise
-inline cudaError_t ctx_sync(neo_gpu_ctx* c) {
-    if (c->blocking && c->sync_ev) {
-        cudaError_t e = cudaEventRecord(c->sync_ev, c->stream);
-        if (e != cudaSuccess) return e;
-        return cudaEventSynchronize(c->sync_ev);
-    }
-    return cudaStreamSynchronize(c->stream);
-}
-inline cudaError_t ctx_set_blocking(neo_gpu_ctx* c, bool on) {
-    if (on && !c->sync_ev) {
-        cudaError_t e = cudaEventCreateWithFlags(&c->sync_ev, cudaEventBlockingSync | cudaEventDisableTiming);
-        if (e != cudaSuccess) return e;
-    }
-    c->blocking = on;
-    return cudaSuccess;
-}
+// wait for the context's stream (a spinning stream synchronization: batch
+// workers that slept in blocking waits were measured no faster)
+inline cudaError_t ctx_sync(neo_gpu_ctx* c) { return cudaStreamSynchronize(c->stream); }
 
-// device -> pageable host copy on the context's stream; in blocking mode the
-// thread first sleeps until the stream's work is done, so the copy itself
-// (which waits for the stream) does not spin
+// device -> host copy on the context's stream
 inline cudaError_t ctx_d2h(neo_gpu_ctx* c, void* dst, const void* src, size_t bytes) {
-    if (c->blocking) {
-        cudaError_t e = ctx_sync(c);
-        if (e != cudaSuccess) return e;
-    }
     return cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, c->stream);
 }
 
