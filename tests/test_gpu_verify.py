@@ -41,3 +41,20 @@ def test_verifier_accepts_gpu_memory_chunks(ctx):
         assert v.verify_step(zs[c][:1], g.fold_step(zs[c]))
     assert len(v.val_obligations) == g.val_obligations() == 36
     g.close()
+
+
+def test_verifier_accepts_full_size_memory_chunks(ctx):
+    """The single-shard-with-memory workload at its full size: n = m = 2^16,
+    1024 trace steps per fold step, a Twist memory of 2^12 cells and a Shout
+    table of 2^16 entries; three consecutive chunks proven by the CUDA library
+    pass every check of the verifier restatement."""
+    ccs, zs, mem, inits = synth.make_memory_workload_chunks(16, 1234, 3, 1024, 16, 12)
+    ctx.pp_generate(bytes(range(7, 39)), 16, 1 << 16, 1)
+    g = gpu.Shard(ctx, ccs, m_in=1, k_rho=12, app_label=b"neo/full-verify", mem=mem)
+    v = OracleVerifier(ccs, m_in=1, k_rho=12, kappa=16, app_label=b"neo/full-verify", mem=mem)
+    for c in range(3):
+        if c:
+            g.set_twist_init(0, inits[c][0])
+            v.set_twist_init(0, inits[c][0])
+        assert v.verify_step(zs[c][:1], g.fold_step(zs[c]))
+    g.close()
