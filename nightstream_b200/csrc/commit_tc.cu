@@ -395,32 +395,49 @@ __global__ void __launch_bounds__(TC_THREADS, 1) commit_tc_kernel(const TcArgs a
     }
 }
 
-// c'_{v,i}[r] = sum_{ks} sum_l 2^(8l) D[ks][(i,l)][(v,r)] mod q, then fold 81 -> 54
-__global__ void commit_tc_reduce_kernel(const int32_t* __restrict__ partial, uint32_t n_groups, uint32_t n_ksplit,
-                                        uint32_t kappa, uint32_t n_vec, uint64_t* __restrict__ out) {
-    const uint32_t vi = blockIdx.x;  // v * kappa + i
-    const uint32_t v = vi / kappa, i = vi % kappa;
-    const uint32_t group = v / TC_NV, vl = v % TC_NV;
-    __shared__ uint64_t s_c[81];
-    const int r = threadIdx.x;
-    if (r < 81) {
-        int64_t acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-        for (uint32_t ks = 0; ks < n_ksplit; ks++) {
-            const uint32_t cta = ks * n_groups + group;
-            // TMEM column of output row r: r' = 80 - r = 16a + 8h + b -> row group (2a + h) NV + vl
-            const int rp = 80 - r;
-            const int col = ((((rp >> 4) * 2 + ((rp >> 3) & 1)) * TC_NV + (int)vl) << 3) | (rp & 7);
-            const int32_t* p = partial + ((uint64_t)cta * 128 + i * 8) * TC_NPAD + col;
+// c'_{v,i}[r] = sum_{ks} sum_l 2^(8l) D[ks][(i,l)][(v,r)] mod q, then fold 81 -> 54.
+// One block per (vector group, i): thread (col, half) sums the int32 partials
+// of TMEM column col over its half of the K splits for the 8 limb rows
+// (reads coalesced along the 352 columns), the halves meet in shared memory,
+// then each column is recombined mod q, mapped back to (v, r) and folded.
+constexpr int RED_THREADS = TC_NPAD * 2;
+__global__ void __launch_bounds__(RED_THREADS) commit_tc_reduce_kernel(const int32_t* __restrict__ partial,
+                                                                       uint32_t n_groups, uint32_t n_ksplit,
+                                                                       uint32_t kappa, uint32_t n_vec,
+                                                                       uint64_t* __restrict__ out) {
+    const uint32_t group = blockIdx.x / kappa, i = blockIdx.x % kappa;
+    const int col = threadIdx.x % TC_NPAD, half = threadIdx.x / TC_NPAD;
+    __shared__ int64_t s_acc[TC_NPAD][8];
+    __shared__ uint64_t s_c[TC_NV][81];
+    int64_t acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    const uint32_t ks0 = half ? n_ksplit / 2 : 0, ks1 = half ? n_ksplit : n_ksplit / 2;
+    for (uint32_t ks = ks0; ks < ks1; ks++) {
+        const int32_t* p = partial + ((uint64_t)(ks * n_groups + group) * 128 + i * 8) * TC_NPAD + col;
 #pragma unroll
-            for (int l = 0; l < 8; l++) acc[l] += p[(uint64_t)l * TC_NPAD];
-        }
-        uint64_t c = 0;
+        for (int l = 0; l < 8; l++) acc[l] += p[(uint64_t)l * TC_NPAD];
+    }
+    if (half) {
 #pragma unroll
-        for (int l = 0; l < 8; l++) c = gl::add(c, gl::mul(gl::from_i64(acc[l]), 1ULL << (8 * l)));
-        s_c[r] = c;
+        for (int l = 0; l < 8; l++) s_acc[col][l] = acc[l];
     }
     __syncthreads();
-    if (r < NEO_D) out[((uint64_t)v * kappa + i) * NEO_D + r] = gl::sub(s_c[r], r >= 27 ? s_c[r + 27] : s_c[r + 54]);
+    if (!half) {
+        uint64_t c = 0;
+#pragma unroll
+        for (int l = 0; l < 8; l++) c = gl::add(c, gl::mul(gl::from_i64(acc[l] + s_acc[col][l]), 1ULL << (8 * l)));
+        // column -> row group g = (2a + h) NV + v, row b; r' = 16a + 8h + b, r = 80 - r'
+        const int g = col >> 3, b = col & 7;
+        const int v = g % TC_NV, h = (g / TC_NV) & 1, a = g / (2 * TC_NV);
+        const int rp = 16 * a + 8 * h + b;
+        if (rp <= 80) s_c[v][80 - rp] = c;
+    }
+    __syncthreads();
+    for (int x = threadIdx.x; x < TC_NV * NEO_D; x += blockDim.x) {
+        const int v = x / NEO_D, r = x % NEO_D;
+        const uint32_t vg = group * TC_NV + v;
+        if (vg < n_vec)
+            out[((uint64_t)vg * kappa + i) * NEO_D + r] = gl::sub(s_c[v][r], r >= 27 ? s_c[v][r + 27] : s_c[v][r + 54]);
+    }
 }
 
 }  // namespace
@@ -485,7 +502,8 @@ int launch_commit_tc(neo_gpu_ctx* ctx, const PPEntry* pp, const int8_t* d_digits
     NEO_CK(ctx, cudaFuncSetAttribute(commit_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     commit_tc_kernel<<<n_groups * n_ksplit, TC_THREADS, smem, ctx->stream>>>(a);
     NEO_LAUNCHED(ctx);
-    commit_tc_reduce_kernel<<<n_vec * pp->kappa, 96, 0, ctx->stream>>>(partial, n_groups, n_ksplit, pp->kappa, n_vec,
+    commit_tc_reduce_kernel<<<n_groups * pp->kappa, RED_THREADS, 0, ctx->stream>>>(partial, n_groups, n_ksplit,
+                                                                                     pp->kappa, n_vec,
                                                                         d_out);
     NEO_LAUNCHED(ctx);
     return NEO_OK;
