@@ -337,9 +337,11 @@ int neo_gpu_shard_destroy(neo_gpu_shard* sh);
 /* No single reference function: the reference proves shards one at a time
  * (crates/neo-fold/src/shard.rs:2285 fold_shard_prove).  A batch owns
  * n_workers host threads, each with its own context (CUDA stream) on `device`.
- * Submitted shard-prove requests (CCS + witness + number of fold steps) are
- * admitted against free device memory, assigned to the least-loaded worker and
- * advanced one fold step at a time, round-robin, alongside earlier requests.
+ * Submitted shard-prove requests (CCS + witness + number of fold steps) wait
+ * in one FIFO queue; an idle worker starts the head request once its device
+ * footprint fits (free HBM when the engine was last idle, minus the running
+ * requests' footprints and the reserve) and proves it to completion.
+ * Destroying the batch lets running requests finish; queued ones never start.
  * PP for every m used must be uploaded first (any context on the device). */
 typedef struct neo_gpu_batch neo_gpu_batch;
 int neo_gpu_batch_create(int device, uint32_t n_workers, neo_gpu_batch** out);

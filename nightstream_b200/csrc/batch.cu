@@ -3,12 +3,19 @@
 // A zkVM run yields many shards of uneven size; each shard is an independent
 // fold-step chain (own transcript, own accumulator: crates/neo-fold/src/shard.rs:1725-2283).
 // The engine runs W worker threads, each with its own context (CUDA stream).
-// Requests are admitted against free HBM (cudaMemGetInfo minus what admitted
-// requests have reserved), assigned to the least-loaded worker, and every
-// worker advances its active shards one fold step at a time, round-robin.
-// Host-side Fiat-Shamir work of different shards thus runs in parallel and
-// their kernels overlap on the device; requests that arrive while others are
-// running join the rotation between steps (continuous batching).
+// Requests wait in one FIFO queue; an idle worker takes the request at its
+// head once its device footprint fits the HBM budget (free memory when the
+// engine was last idle, minus the footprints of running requests and a
+// margin) and proves it to completion.  Host-side Fiat-Shamir work of
+// different shards thus runs in parallel on W threads and their kernels
+// overlap on the device.  A step of one request is a single-threaded chain
+// (transcript, then kernels, then transcript), so a worker that interleaved
+// several requests would gain no throughput and only delay each of them:
+// run to completion keeps the latency of a request close to its own service
+// time plus its queueing.  Worker threads allocate shard buffers from the
+// device's memory pool, ordered on their own stream: cudaFree waits for the
+// whole device, so a worker freeing a finished shard would otherwise stall
+// every other worker's kernels.
 #include "internal.cuh"
 #include <atomic>
 #include <chrono>
@@ -108,9 +115,6 @@ struct Job {
 
 struct Worker {
     neo_gpu_ctx* ctx = nullptr;
-    std::vector<Job*> active;
-    std::deque<Job*> inbox;
-    uint64_t load = 0;  // outstanding work estimate (steps x m)
 };
 
 }  // namespace
@@ -121,9 +125,10 @@ struct neo_gpu_batch {
     std::vector<std::thread> threads;
     std::mutex mu;
     std::condition_variable cv_work, cv_done;
-    std::deque<Job*> pending;                 // not yet admitted (HBM)
+    std::deque<Job*> pending;                 // submitted, not yet started (FIFO)
     std::vector<std::unique_ptr<Job>> jobs;   // all jobs, by id
-    uint64_t reserved = 0;                    // bytes reserved by admitted, unfinished jobs
+    uint64_t reserved = 0;                    // footprints of the running jobs
+    uint64_t budget = 0;                      // free HBM when the engine was last idle, minus the margin
     uint64_t reserve_margin = 2ull << 30;     // headroom kept free on the device
     uint64_t unfinished = 0;
     bool stop = false;
@@ -142,27 +147,23 @@ static uint64_t shard_footprint(uint64_t m, uint32_t k_rho) {
     return zall + small + nc + commit_scratch + fold;
 }
 
-// caller holds b->mu
-static void admit_locked(neo_gpu_batch* b) {
-    while (!b->pending.empty()) {
-        Job* j = b->pending.front();
+// caller holds b->mu: may the head of the queue start now?
+static bool head_fits_locked(neo_gpu_batch* b) {
+    if (b->pending.empty()) return false;
+    if (b->reserved == 0) {
+        // idle engine: hand the pool's unused blocks back, refresh the budget; a
+        // request larger than it still runs alone
+        cudaMemPool_t pool;
+        if (cudaDeviceGetDefaultMemPool(&pool, b->device) == cudaSuccess) cudaMemPoolTrimTo(pool, 0);
         size_t free_b = 0, total_b = 0;
         if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) free_b = 0;
-        const uint64_t avail = free_b > b->reserved + b->reserve_margin ? free_b - b->reserved - b->reserve_margin : 0;
-        // always admit when nothing is running, so a large request cannot starve
-        if (j->footprint > avail && b->reserved > 0) break;
-        b->pending.pop_front();
-        b->reserved += j->footprint;
-        j->t_admit = bclock::now();
-        Worker* best = &b->workers[0];
-        for (auto& w : b->workers)
-            if (w.load < best->load) best = &w;
-        best->load += (uint64_t)j->n_steps * j->z.size();
-        best->inbox.push_back(j);
+        b->budget = free_b > b->reserve_margin ? free_b - b->reserve_margin : 0;
+        return true;
     }
+    return b->reserved + b->pending.front()->footprint <= b->budget;
 }
 
-static void finish_job(neo_gpu_batch* b, Worker& w, Job* j, int status, const char* err) {
+static void finish_job(neo_gpu_batch* b, Job* j, int status, const char* err) {
     if (j->shard) {
         neo_gpu_shard_transcript_state(j->shard, j->tr_state);
         neo_gpu_shard_destroy(j->shard);
@@ -173,56 +174,50 @@ static void finish_job(neo_gpu_batch* b, Worker& w, Job* j, int status, const ch
     if (err) j->error = err;
     j->t_done = bclock::now();
     b->reserved -= std::min(b->reserved, j->footprint);
-    const uint64_t work = (uint64_t)j->n_steps * j->z.size();
-    w.load -= std::min(w.load, work);
     b->unfinished--;
-    admit_locked(b);
     b->cv_work.notify_all();
     b->cv_done.notify_all();
 }
 
-static void worker_main(neo_gpu_batch* b, size_t wi) {
-    Worker& w = b->workers[wi];
-    cudaSetDevice(b->device);
-    size_t rr = 0;
-    for (;;) {
-        {
-            std::unique_lock<std::mutex> lk(b->mu);
-            b->cv_work.wait(lk, [&] { return b->stop || !w.inbox.empty() || !w.active.empty(); });
-            if (b->stop && w.inbox.empty() && w.active.empty()) return;
-            while (!w.inbox.empty()) {
-                w.active.push_back(w.inbox.front());
-                w.inbox.pop_front();
-            }
-        }
-        if (w.active.empty()) continue;
-        rr %= w.active.size();
-        Job* j = w.active[rr];
-        int rc = NEO_OK;
-        if (!j->shard)
-            rc = j->mem ? neo_gpu_shard_create_mem(w.ctx, &j->ccs->d, j->m_in, j->k_rho, j->label.c_str(), &j->mem->d,
-                                                   &j->shard)
-                        : neo_gpu_shard_create(w.ctx, &j->ccs->d, j->m_in, j->k_rho, j->label.c_str(), &j->shard);
-        if (rc == NEO_OK && j->steps_done > 0 && j->steps_done < j->inits.size()) {
+// every fold step of one request on this worker's context
+static void run_job(neo_gpu_batch* b, Worker& w, Job* j) {
+    int rc = j->mem ? neo_gpu_shard_create_mem(w.ctx, &j->ccs->d, j->m_in, j->k_rho, j->label.c_str(), &j->mem->d,
+                                               &j->shard)
+                    : neo_gpu_shard_create(w.ctx, &j->ccs->d, j->m_in, j->k_rho, j->label.c_str(), &j->shard);
+    const uint64_t m = j->ccs->d.m;
+    while (rc == NEO_OK && j->steps_done < j->n_steps) {
+        if (j->steps_done > 0 && j->steps_done < j->inits.size()) {
             auto& st = j->inits[j->steps_done];
             for (uint32_t i = 0; rc == NEO_OK && i < st.size(); i++)
                 rc = neo_gpu_shard_set_twist_init(j->shard, i, st[i].first.size(), st[i].first.data(),
                                                   st[i].second.data());
         }
-        if (rc == NEO_OK) {
-            uint64_t len = 0;
-            const uint64_t m = j->ccs->d.m;
-            const uint64_t* zs = j->z.size() > m ? j->z.data() + (uint64_t)j->steps_done * m : j->z.data();
-            rc = neo_gpu_shard_fold_step(j->shard, zs, nullptr, 0, &len);
-            if (rc == NEO_OK) j->steps_done++;
+        if (rc != NEO_OK) break;
+        uint64_t len = 0;
+        const uint64_t* zs = j->z.size() > m ? j->z.data() + (uint64_t)j->steps_done * m : j->z.data();
+        rc = neo_gpu_shard_fold_step(j->shard, zs, nullptr, 0, &len);
+        if (rc == NEO_OK) j->steps_done++;
+    }
+    std::string err = rc != NEO_OK ? std::string(neo_gpu_last_error(w.ctx)) : std::string();
+    finish_job(b, j, rc == NEO_OK ? 1 : -rc, rc != NEO_OK ? err.c_str() : nullptr);
+}
+
+static void worker_main(neo_gpu_batch* b, size_t wi) {
+    Worker& w = b->workers[wi];
+    cudaSetDevice(b->device);
+    g_alloc_stream = w.ctx->stream;  // this thread's shards allocate and free on its stream, from the pool
+    for (;;) {
+        Job* j = nullptr;
+        {
+            std::unique_lock<std::mutex> lk(b->mu);
+            b->cv_work.wait(lk, [&] { return b->stop || head_fits_locked(b); });
+            if (b->stop) return;
+            j = b->pending.front();
+            b->pending.pop_front();
+            b->reserved += j->footprint;
+            j->t_admit = bclock::now();
         }
-        if (rc != NEO_OK || j->steps_done == j->n_steps) {
-            std::string err = rc != NEO_OK ? std::string(neo_gpu_last_error(w.ctx)) : std::string();
-            w.active.erase(w.active.begin() + rr);
-            finish_job(b, w, j, rc == NEO_OK ? 1 : -rc, rc != NEO_OK ? err.c_str() : nullptr);
-        } else {
-            rr++;
-        }
+        run_job(b, w, j);
     }
 }
 
@@ -240,6 +235,14 @@ extern "C" int neo_gpu_batch_create(int device, uint32_t n_workers, neo_gpu_batc
             delete b;
             return rc;
         }
+    }
+    // freed shard buffers stay in the device's memory pool for the next request
+    // (returned to the driver only when the engine is idle, see head_fits_locked)
+    cudaMemPool_t pool;
+    cudaSetDevice(device);
+    if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
+        uint64_t keep = ~0ull;
+        cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
     }
     for (size_t i = 0; i < b->workers.size(); i++) b->threads.emplace_back(worker_main, b, i);
     *out = b;
@@ -291,7 +294,6 @@ static int submit_impl(neo_gpu_batch* b, const neo_ccs_desc* ccs, const neo_mem_
     b->pending.push_back(j.get());
     b->jobs.push_back(std::move(j));
     b->unfinished++;
-    admit_locked(b);
     b->cv_work.notify_all();
     return NEO_OK;
 }
@@ -346,12 +348,8 @@ extern "C" int neo_gpu_batch_destroy(neo_gpu_batch* b) {
         b->stop = true;
         b->cv_work.notify_all();
     }
-    for (auto& t : b->threads) t.join();
-    for (auto& w : b->workers) {
-        for (Job* j : w.active)
-            if (j->shard) neo_gpu_shard_destroy(j->shard);
-        neo_gpu_ctx_destroy(w.ctx);
-    }
+    for (auto& t : b->threads) t.join();  // running requests finish; queued ones never start
+    for (auto& w : b->workers) neo_gpu_ctx_destroy(w.ctx);
     delete b;
     return NEO_OK;
 }

@@ -27,6 +27,10 @@ extern "C" int neo_gpu_ctx_create(int device, neo_gpu_ctx** out) {
     return NEO_OK;
 }
 
+// Stream on which DevBuf allocations of this thread are made (stream-ordered,
+// from the device's memory pool) and later freed; null: cudaMalloc / cudaFree.
+thread_local cudaStream_t g_alloc_stream = nullptr;
+
 extern "C" int neo_gpu_ctx_destroy(neo_gpu_ctx* ctx) {
     if (!ctx) return NEO_ERR_ARG;
     cudaSetDevice(ctx->device);
@@ -109,18 +113,18 @@ int dev_ccs_upload(neo_gpu_ctx* ctx, const neo_ccs_desc* d, DevCcs& o) {
     NEO_CK(ctx, o.csc_ptr.alloc((size_t)d->t * (d->m + 1)));
     NEO_CK(ctx, o.csc_row.alloc(nn));
     NEO_CK(ctx, o.csc_val.alloc(nn));
-    NEO_CK(ctx, cudaMemcpy(o.csr_ptr.p, csr_ptr.data(), csr_ptr.size() * 8, cudaMemcpyHostToDevice));
-    NEO_CK(ctx, cudaMemcpy(o.csr_col.p, csr_col.data(), nn * 4, cudaMemcpyHostToDevice));
-    NEO_CK(ctx, cudaMemcpy(o.csr_val.p, csr_val.data(), nn * 8, cudaMemcpyHostToDevice));
+    NEO_CK(ctx, cudaMemcpyAsync(o.csr_ptr.p, csr_ptr.data(), csr_ptr.size() * 8, cudaMemcpyHostToDevice, ctx->stream));
+    NEO_CK(ctx, cudaMemcpyAsync(o.csr_col.p, csr_col.data(), nn * 4, cudaMemcpyHostToDevice, ctx->stream));
+    NEO_CK(ctx, cudaMemcpyAsync(o.csr_val.p, csr_val.data(), nn * 8, cudaMemcpyHostToDevice, ctx->stream));
     std::vector<uint64_t> csc_ptr((size_t)d->t * (d->m + 1), 0);
     for (uint32_t j = 0; j < d->t; j++)
         if (!o.is_identity[j]) memcpy(&csc_ptr[(size_t)j * (d->m + 1)], d->col_ptr + (size_t)j * (d->m + 1), (d->m + 1) * 8);
     std::vector<uint64_t> csc_val(nn, 0);
     if (nnz) for (uint64_t k = 0; k < nnz; k++) csc_val[k] = gl::canon(d->vals[k]);
-    NEO_CK(ctx, cudaMemcpy(o.csc_ptr.p, csc_ptr.data(), csc_ptr.size() * 8, cudaMemcpyHostToDevice));
+    NEO_CK(ctx, cudaMemcpyAsync(o.csc_ptr.p, csc_ptr.data(), csc_ptr.size() * 8, cudaMemcpyHostToDevice, ctx->stream));
     if (nnz) {
-        NEO_CK(ctx, cudaMemcpy(o.csc_row.p, d->row_idx, nnz * 4, cudaMemcpyHostToDevice));
-        NEO_CK(ctx, cudaMemcpy(o.csc_val.p, csc_val.data(), nnz * 8, cudaMemcpyHostToDevice));
+        NEO_CK(ctx, cudaMemcpyAsync(o.csc_row.p, d->row_idx, nnz * 4, cudaMemcpyHostToDevice, ctx->stream));
+        NEO_CK(ctx, cudaMemcpyAsync(o.csc_val.p, csc_val.data(), nnz * 8, cudaMemcpyHostToDevice, ctx->stream));
     }
     return NEO_OK;
 }

@@ -465,7 +465,7 @@ static int shard_create_impl(neo_gpu_ctx* ctx, const neo_ccs_desc* desc, uint32_
             std::vector<K> tk(P, gl::kzero());
             for (uint64_t a = 0; a < P && a < s.table_len; a++) tk[a] = gl::kfq(gl::canon(s.table[a]));
             NEO_CK(ctx, si->d_table.alloc(P));
-            NEO_CK(ctx, cudaMemcpy(si->d_table.p, tk.data(), P * sizeof(K), cudaMemcpyHostToDevice));
+            NEO_CK(ctx, cudaMemcpyAsync(si->d_table.p, tk.data(), P * sizeof(K), cudaMemcpyHostToDevice, ctx->stream));
             si->col0 = col;
             col += s.ell_addr + 2;
             sh->shout.push_back(std::move(si));

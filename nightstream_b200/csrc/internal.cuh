@@ -76,10 +76,15 @@ int pp_slot(neo_gpu_ctx* ctx, uint32_t kappa, uint64_t m, PPEntry** out);
 int pp_finish(neo_gpu_ctx* ctx, PPEntry* pp, uint32_t kappa);
 
 // Owning device buffer (freed on scope exit).
+// Stream of this thread's stream-ordered allocations (set by batch workers,
+// whose thread uses a single context); null: plain cudaMalloc / cudaFree.
+extern thread_local cudaStream_t g_alloc_stream;
+
 template <typename T>
 struct DevBuf {
     T* p = nullptr;
     size_t n = 0;
+    cudaStream_t s = nullptr;  // stream the allocation was ordered on (null: cudaMalloc)
     DevBuf() = default;
     DevBuf(const DevBuf&) = delete;
     DevBuf& operator=(const DevBuf&) = delete;
@@ -90,6 +95,8 @@ struct DevBuf {
         n = count;
         cap = count;
         if (count == 0) return cudaSuccess;
+        s = g_alloc_stream;
+        if (s) return cudaMallocAsync(reinterpret_cast<void**>(&p), count * sizeof(T), s);
         return cudaMalloc(&p, count * sizeof(T));
     }
     // keep the allocation when it is large enough (reused workspaces)
@@ -101,8 +108,12 @@ struct DevBuf {
         return alloc(count);
     }
     void release() {
-        if (p) cudaFree(p);
+        if (p) {
+            if (s) cudaFreeAsync(p, s);
+            else cudaFree(p);
+        }
         p = nullptr;
+        s = nullptr;
         n = 0;
         cap = 0;
     }
@@ -128,13 +139,18 @@ struct DevCcs {
 // Grow-only scratch owned by the context; valid until the next call that grows it.
 inline cudaError_t ctx_scratch(neo_gpu_ctx* ctx, size_t bytes, void** p) {
     if (bytes > ctx->scratch_bytes) {
+        const bool pooled = g_alloc_stream == ctx->stream;  // stream-ordered: no device-wide wait
         if (ctx->scratch) {
-            cudaStreamSynchronize(ctx->stream);
-            cudaFree(ctx->scratch);
+            if (pooled) {
+                cudaFreeAsync(ctx->scratch, ctx->stream);
+            } else {
+                cudaStreamSynchronize(ctx->stream);
+                cudaFree(ctx->scratch);
+            }
             ctx->scratch = nullptr;
             ctx->scratch_bytes = 0;
         }
-        cudaError_t e = cudaMalloc(&ctx->scratch, bytes);
+        cudaError_t e = pooled ? cudaMallocAsync(&ctx->scratch, bytes, ctx->stream) : cudaMalloc(&ctx->scratch, bytes);
         if (e != cudaSuccess) return e;
         ctx->scratch_bytes = bytes;
     }

@@ -732,7 +732,8 @@ extern "C" int neo_gpu_addr_lookup_weights(neo_gpu_ctx* ctx, uint32_t ell, const
     K cl;
     int rc = addr_weights_device(ctx, ell, dr.p, ell_addr, has.p, bits.p, tab.p, table_len, w.p, &cl, nullptr);
     if (rc) return rc;
-    NEO_CK(ctx, cudaMemcpy(weights, w.p, P * sizeof(K), cudaMemcpyDeviceToHost));
+    NEO_CK(ctx, ctx_d2h(ctx, weights, w.p, P * sizeof(K)));
+    NEO_CK(ctx, ctx_sync(ctx));
     claim[0] = cl.re;
     claim[1] = cl.im;
     return NEO_OK;
