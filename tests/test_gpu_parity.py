@@ -113,6 +113,27 @@ def test_ccs_oracle_all_rounds_match(ctx, ell, k, inputs):
     _run_both(ctx, ell, k, inputs)
 
 
+def test_ccs_oracle_wide_digits_match(ctx):
+    """Digit rows outside {-1,0,1} (a corrupted or non-decomposed witness) take
+    the general path of the digit-streaming rounds; the mix of general and
+    ternary rows still matches the oracle in every round."""
+    from nightstream_b200.gpu import GpuCcsOracle
+    ell, k = 10, 3
+    ccs, z, Z, ch, chals = ccs_case(ell, k, True, seed=23)
+    rng = np.random.default_rng(5)
+    Z = Z.copy()
+    mask = rng.random(Z.shape) < 0.05
+    Z[mask] = rng.integers(-7, 8, size=int(mask.sum())).astype(np.int8)
+    args = (ccs, Z, 2, ch["alpha"], ch["beta_a"], ch["beta_r"], ch["gamma"], ch["r_inputs"], ELL_D, ell, D_SC)
+    g = GpuCcsOracle(ctx, *args)
+    o = O.CcsOracle(*args)
+    for r in range(ell + ELL_D):
+        assert np.array_equal(g.evals_at(XS), o.evals_at(XS)), f"round {r}"
+        g.fold(chals[r])
+        o.fold(chals[r])
+    g.close()
+
+
 def test_ccs_oracle_steady_state_full_size(ctx):
     # k = 13 (1 MCS + 12 carried children), n = m = 2^16
     _run_both(ctx, 16, 13, True, seed=11)
