@@ -469,6 +469,24 @@ def run_reference(args, rank, world):
     print(json.dumps(out), flush=True)
 
 
+def max_over_ranks(ms, dist=None):
+    """The slowest rank's time: every rank takes part in one MAX all-reduce
+    (the only collective of a run; the ranks prove independent shards)."""
+    if not dist:
+        return ms
+    import torch
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([float(ms)], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_value(world, steps, ms):
+    """Whole-job fold-steps/s of `world` replicas, each proving `steps` steps of
+    its own shard in `ms` milliseconds (the slowest rank's)."""
+    return world * steps / (ms * 1e-3)
+
+
 def run_ours(args, rank, world, local_rank):
     import torch
     from nightstream_b200 import gpu
@@ -522,11 +540,8 @@ def run_ours(args, rank, world, local_rank):
     launches = ctx.kernel_launches - l0
     barrier()
     stats = shard.step_stats()
-    if dist:
-        t = torch.tensor([ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
-    value = world * args.steps / (ms * 1e-3)
+    ms = max_over_ranks(ms, dist)
+    value = replica_value(world, args.steps, ms)
 
     # end-to-end through the C ABI with host buffers: pinned z in, proof words out
     e2e = None
@@ -543,11 +558,8 @@ def run_ours(args, rank, world, local_rank):
         ev1.record(stream)
         ev1.synchronize()
         ems = ev0.elapsed_time(ev1)
-        if dist:
-            t = torch.tensor([ems], device="cuda")
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            ems = float(t.item())
-        e2e = {"value": world * args.steps / (ems * 1e-3), "unit": UNIT, "h2d_bytes_per_step": int(zh[0].nbytes),
+        ems = max_over_ranks(ems, dist)
+        e2e = {"value": replica_value(world, args.steps, ems), "unit": UNIT, "h2d_bytes_per_step": int(zh[0].nbytes),
                "d2h_bytes_per_step": int(proof.nbytes)}
 
     # dominant kernel roofline: the DEC batch commitment (12 digit planes, one launch pair)
