@@ -58,3 +58,25 @@ def test_verifier_accepts_full_size_memory_chunks(ctx):
             v.set_twist_init(0, inits[c][0])
         assert v.verify_step(zs[c][:1], g.fold_step(zs[c]))
     g.close()
+
+
+def test_verifier_accepts_large_shard_chunks(ctx):
+    """The large single shard: n = m = 2^20, 2^14 trace steps per fold step
+    (a 2^18-step trace folds in 16 steps), a Twist memory of 2^16 cells and a
+    Shout table of 2^20 entries (59 bus columns). Two consecutive chunks
+    proven by the CUDA library pass every check of the verifier restatement."""
+    import time
+    ccs, zs, mem, inits = synth.make_memory_workload_chunks(20, 4321, 2, 1 << 14, 20, 16)
+    ctx.pp_generate(bytes(range(3, 35)), 16, 1 << 20, 1)
+    g = gpu.Shard(ctx, ccs, m_in=1, k_rho=12, app_label=b"neo/large-verify", mem=mem)
+    v = OracleVerifier(ccs, m_in=1, k_rho=12, kappa=16, app_label=b"neo/large-verify", mem=mem)
+    for c in range(2):
+        if c:
+            g.set_twist_init(0, inits[c][0])
+            v.set_twist_init(0, inits[c][0])
+        t0 = time.perf_counter()
+        P = g.fold_step(zs[c])
+        t1 = time.perf_counter()
+        assert v.verify_step(zs[c][:1], P)
+        print(f"large shard chunk {c}: GPU fold step {1e3 * (t1 - t0):.0f} ms, verify {time.perf_counter() - t1:.1f} s")
+    g.close()
