@@ -104,28 +104,47 @@ const Poseidon2W16& digest_perm() {
 typedef unsigned __int128 u128;
 
 // Permutation arithmetic keeps lanes in [0, 2^64) (not necessarily < q) and
-// canonicalises once at the end. Corrections are masks, not branches: the
-// carries are data dependent, and a mispredicted branch per reduction costs
-// more than the whole multiply. State loops are fully unrolled so the eight
-// independent S-box chains of a full round overlap.
+// canonicalises once at the end. The transcript is one sequential chain of
+// permutations, so every reduction is written for latency:
+//  * a + b with carry: 2^64 = 2^32 - 1 (mod q), so the correction is the
+//    carry widened to 32 ones, which `sbb` on a 32-bit register produces
+//    directly (add, sbb, add);
+//  * lo - hi_hi borrows only when lo < hi_hi < 2^32, i.e. with probability
+//    about 2^-32 for a product, so it is a branch the predictor never misses
+//    instead of a mask on the critical path.
+// State loops are fully unrolled so the independent S-box chains of a full
+// round overlap.
+static inline __attribute__((always_inline)) uint64_t add_carry_fix(uint64_t a, uint64_t b) {
+#if defined(__x86_64__)
+    uint64_t adj;
+    __asm__("add %[b], %[a]\n\tsbb %k[adj], %k[adj]\n\tadd %[adj], %[a]"
+            : [a] "+r"(a), [adj] "=&r"(adj)
+            : [b] "r"(b)
+            : "cc");
+    return a;
+#else
+    uint64_t s;
+    const uint64_t c = __builtin_add_overflow(a, b, &s);
+    return s + (GL_EPS & (0 - c));
+#endif
+}
 static inline __attribute__((always_inline)) uint64_t red_nc(uint64_t lo, uint64_t hi) {
     // lo + 2^64 hi with 2^64 = 2^32 - 1 and 2^96 = -1 (mod q)
     const uint64_t hh = hi >> 32, hl = hi & GL_EPS;
     uint64_t t0;
-    const uint64_t br = __builtin_sub_overflow(lo, hh, &t0);
-    t0 -= GL_EPS & (0 - br);
-    const uint64_t t1 = (hl << 32) - hl;
-    uint64_t s;
-    const uint64_t c = __builtin_add_overflow(t0, t1, &s);
-    return s + (GL_EPS & (0 - c));
+    if (__builtin_expect(__builtin_sub_overflow(lo, hh, &t0), 0)) t0 -= GL_EPS;  // t0 >= 2^64 - 2^32 here
+    // t0 + hl (2^32 - 1); a carry leaves a sum below hl (2^32 - 1), so the
+    // correction cannot carry again
+    return add_carry_fix(t0, (hl << 32) - hl);
 }
 static inline __attribute__((always_inline)) uint64_t red128(u128 x) { return red_nc((uint64_t)x, (uint64_t)(x >> 64)); }
-static inline __attribute__((always_inline)) uint64_t mulq(uint64_t a, uint64_t b) { return red128((u128)a * b); }
-static inline __attribute__((always_inline)) uint64_t addq(uint64_t a, uint64_t b) {
-    uint64_t s;
-    const uint64_t c = __builtin_add_overflow(a, b, &s);
-    return s + (GL_EPS & (0 - c));
+// x with a high word below 2^32 (a sum of a few lanes): lo + hi (2^32 - 1)
+static inline __attribute__((always_inline)) uint64_t red_small(u128 x) {
+    const uint64_t hi = (uint64_t)(x >> 64);
+    return add_carry_fix((uint64_t)x, (hi << 32) - hi);
 }
+static inline __attribute__((always_inline)) uint64_t mulq(uint64_t a, uint64_t b) { return red128((u128)a * b); }
+static inline __attribute__((always_inline)) uint64_t addq(uint64_t a, uint64_t b) { return add_carry_fix(a, b); }
 static inline __attribute__((always_inline)) uint64_t canonq(uint64_t a) { return a >= GL_Q ? a - GL_Q : a; }
 
 static inline __attribute__((always_inline)) uint64_t sbox7(uint64_t x) {
@@ -162,7 +181,7 @@ static inline __attribute__((always_inline)) void external_layer(uint64_t* st) {
 #pragma GCC unroll 4
         for (int b = 0; b < W / 4; b++) s += y[4 * b + i];
 #pragma GCC unroll 4
-        for (int b = 0; b < W / 4; b++) st[4 * b + i] = red128(y[4 * b + i] + s);
+        for (int b = 0; b < W / 4; b++) st[4 * b + i] = red_small(y[4 * b + i] + s);  // < 2^72
     }
 }
 
@@ -195,24 +214,29 @@ __attribute__((noinline)) static void permute_impl(const Poseidon2<W>& P, uint64
     // Partial rounds: internal layer M_I x = sum(x) + mu_i * x_i.  Only lane 0
     // goes through the S-box, so with rest = Σ_{i>=1} x_i the new lane 0 is
     // (mu_0 + 1)·s + rest (one multiply-add after the S-box), while lanes
-    // 1..W-1 and the next rest are computed beside the next S-box chain.
+    // 1..W-1 and the next rest are computed beside the next S-box chain.  The
+    // next round's constant joins that multiply-add (x0 is the S-box input),
+    // which keeps a separate addition off the chain.
     u128 racc = 0;
 #pragma GCC unroll 16
     for (int i = 1; i < W; i++) racc += st[i];
-    uint64_t rest = red128(racc);
+    uint64_t rest = red_small(racc);
     const uint64_t mu0p1 = P.mu[0] + 1;  // mu_0 < q, so no wrap
+    uint64_t x0 = addq(st[0], P.rc_int[0]);
     for (int r = 0; r < RP; r++) {
-        const uint64_t x = sbox7(addq(st[0], P.rc_int[r]));
-        const uint64_t sum = red128((u128)x + rest);  // both lazily reduced: add in 128 bits
-        st[0] = red128((u128)mu0p1 * x + rest);
+        const uint64_t x = sbox7(x0);
+        const uint64_t sum = addq(x, rest);
+        const u128 addend = (u128)rest + (r + 1 < RP ? P.rc_int[r + 1] : 0);
+        x0 = red128((u128)mu0p1 * x + addend);  // < 2^128: mu0p1 < 2^64 - 2^32 + 2
         u128 nacc = 0;
 #pragma GCC unroll 16
         for (int i = 1; i < W; i++) {
             st[i] = red128((u128)P.mu[i] * st[i] + sum);
             nacc += st[i];
         }
-        rest = red128(nacc);
+        rest = red_small(nacc);
     }
+    st[0] = x0;
     for (int r = RF / 2; r < RF; r++) full_round<W>(st, P.rc_ext[r]);
 #pragma GCC unroll 16
     for (int i = 0; i < W; i++) st_io[i] = canonq(st[i]);
