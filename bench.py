@@ -54,6 +54,7 @@ def parse():
                     help="plain: one shard; batched: 64 uneven shards batched vs one at a time; "
                          "served: Poisson arrivals, p50/p99 latency")
     ap.add_argument("--shards", type=int, default=64)
+    ap.add_argument("--batch-reps", type=int, default=3, help="batched runs of the mix; the median is reported")
     ap.add_argument("--shard-steps", type=int, default=3)
     ap.add_argument("--workers", type=int, default=0, help="batch workers (0: min(16, host cores))")
     ap.add_argument("--no-batch", action="store_true",
@@ -362,15 +363,20 @@ def batched_result(args):
     steps = args.shard_steps
     total_steps = steps * len(shards)
     dt_plain, infos_plain, _ = run_mix(None, shards, steps, 1)
-    dt_b, infos_b, launches = run_mix(None, shards, steps, workers)
-    same = all(np.array_equal(a["transcript_state"], b["transcript_state"]) for a, b in zip(infos_plain, infos_b))
+    # the batched interval is ~1-2 s of host-bound work, so one run carries the
+    # host's jitter: report the median of `batch_reps` runs (each bit-checked)
+    runs = [run_mix(None, shards, steps, workers) for _ in range(max(1, args.batch_reps))]
+    same = all(np.array_equal(a["transcript_state"], b["transcript_state"])
+               for _, infos, _ in runs for a, b in zip(infos_plain, infos))
+    dt_b, infos_b, launches = sorted(runs, key=lambda r: r[0])[len(runs) // 2]
     lat = sorted(i["latency_ms"] for i in infos_b)
     ctx.close()
     return {"value": total_steps / dt_b, "plain_value": total_steps / dt_plain, "speedup": dt_plain / dt_b,
             "workers": workers, "shards": len(shards), "steps_per_shard": steps,
             "sizes_log2": [s[0] for s in shards], "bit_identical_to_plain": bool(same),
             "p50_ms": lat[len(lat) // 2], "p99_ms": lat[min(len(lat) - 1, int(0.99 * len(lat)))],
-            "gpu_launches": int(launches), "seconds": dt_b, "plain_seconds": dt_plain}
+            "gpu_launches": int(launches), "seconds": dt_b, "plain_seconds": dt_plain,
+            "runs_fold_steps_per_s": [total_steps / r[0] for r in runs]}
 
 
 def run_batched(args):
@@ -588,6 +594,8 @@ def run_ours(args, rank, world, local_rank):
                                          "(profiles/commit_tc_kernel_m16384_12planes.md)",
                        "launch_ms": commit_ms, "peak_source": peak_src, "algorithmic_ops_per_launch": ops}
     roofline = rounds_roofline(ctx, ccs, wl.z(0), args.ell, stream)
+    # the batched mix runs before the legs that use the host's OpenMP pool
+    batched = batched_result(args) if rank == 0 and world == 1 and not args.no_batch else None
     pp_setup = pp_setup_result(args, ctx, m) if rank == 0 else None
 
     if rank == 0:
@@ -599,8 +607,8 @@ def run_ours(args, rank, world, local_rank):
         out["pp_setup"] = pp_setup
         if world == 1 and not args.no_cpu_baseline:
             out["cpu_baseline"] = cpu_baseline(args, wl)
-        if world == 1 and not args.no_batch:
-            out["batched"] = batched_result(args)
+        if batched is not None:
+            out["batched"] = batched
         print(json.dumps(out), flush=True)
     shard.close()
     ctx.close()
