@@ -350,7 +350,8 @@ def run_mix(mix, shards, steps, workers):
     infos = [b.job_info(j) for j in ids]
     launches = b.kernel_launches
     b.close()
-    assert all(i["status"] == 1 for i in infos), [i["status"] for i in infos]
+    assert all(i["status"] == 1 for i in infos), [(j, i["status"], i.get("error")) for j, i in enumerate(infos)
+                                                  if i["status"] != 1]
     return dt, infos, launches
 
 

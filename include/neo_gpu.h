@@ -374,6 +374,9 @@ int neo_gpu_batch_wait_all(neo_gpu_batch* b, double timeout_ms);
 /* times3 = {submit->done ms, submit->admit ms, submit time since creation ms};
  * tr_state8 = final transcript state; status 1 = done, 0 = running, < 0 = -error. */
 int neo_gpu_batch_job_info(neo_gpu_batch* b, uint64_t job_id, double* times3, uint64_t* tr_state8, int* status);
+/* The error message of a failed request (empty while it runs or after it
+ * succeeded), NUL-terminated and truncated to cap bytes. */
+int neo_gpu_batch_job_error(neo_gpu_batch* b, uint64_t job_id, char* buf, uint64_t cap);
 uint64_t neo_gpu_batch_kernel_launches(const neo_gpu_batch* b);
 int neo_gpu_batch_destroy(neo_gpu_batch* b);
 

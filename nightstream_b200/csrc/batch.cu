@@ -341,6 +341,17 @@ extern "C" int neo_gpu_batch_job_info(neo_gpu_batch* b, uint64_t job_id, double*
     return NEO_OK;
 }
 
+extern "C" int neo_gpu_batch_job_error(neo_gpu_batch* b, uint64_t job_id, char* buf, uint64_t cap) {
+    if (!b || !buf || cap == 0) return NEO_ERR_ARG;
+    std::lock_guard<std::mutex> lk(b->mu);
+    if (job_id >= b->jobs.size()) return NEO_ERR_ARG;
+    const std::string& e = b->jobs[job_id]->error;
+    const size_t n = std::min<size_t>(e.size(), cap - 1);
+    memcpy(buf, e.data(), n);
+    buf[n] = 0;
+    return NEO_OK;
+}
+
 extern "C" int neo_gpu_batch_destroy(neo_gpu_batch* b) {
     if (!b) return NEO_ERR_ARG;
     {

@@ -977,7 +977,8 @@ static int ajtai_round(neo_gpu_ccs_oracle* o, const uint64_t* xs, uint32_t nx, u
     a.ysc = o->y_sc.p;
     a.ys_out = o->ys.p;
     size_t smem = (size_t)o->k * (1 + o->t) * NEO_D * sizeof(K);
-    NEO_CK(ctx, cudaFuncSetAttribute(ajtai_round_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    static SmemLimit limit;
+    NEO_CK(ctx, limit.at_least(ajtai_round_kernel, smem));
     ajtai_round_kernel<<<1, 512, smem, ctx->stream>>>(a);
     NEO_LAUNCHED(ctx);
     NEO_CK(ctx, ctx_d2h(ctx, ys, o->ys.p, nx * 16));

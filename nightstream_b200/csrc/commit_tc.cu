@@ -499,7 +499,8 @@ int launch_commit_tc(neo_gpu_ctx* ctx, const PPEntry* pp, const int8_t* d_digits
     a.kb_per_cta = kb_per_cta;
     a.n_kb = (uint32_t)(m / 2);
     const size_t smem = TC_SMEM_BYTES + 1024 /*align*/ + 256 /*barriers*/;
-    NEO_CK(ctx, cudaFuncSetAttribute(commit_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    static SmemLimit limit;
+    NEO_CK(ctx, limit.at_least(commit_tc_kernel, smem));
     commit_tc_kernel<<<n_groups * n_ksplit, TC_THREADS, smem, ctx->stream>>>(a);
     NEO_LAUNCHED(ctx);
     commit_tc_reduce_kernel<<<n_groups * pp->kappa, RED_THREADS, 0, ctx->stream>>>(partial, n_groups, n_ksplit,

@@ -243,7 +243,8 @@ int rlc_mix_device(neo_gpu_ctx* ctx, const int8_t* rho_coeffs_host, const int8_t
     }
     NEO_CK(ctx, cudaMemcpyAsync(d_rot_scratch, rot.data(), rot.size(), cudaMemcpyHostToDevice, ctx->stream));
     size_t smem = rot.size();
-    if (smem > 48 * 1024) NEO_CK(ctx, cudaFuncSetAttribute(rlc_mix_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    static SmemLimit limit;
+    if (smem > 48 * 1024) NEO_CK(ctx, limit.at_least(rlc_mix_kernel, smem));
     rlc_mix_kernel<<<ceil_div(m, 128), 128, smem, ctx->stream>>>(d_rot_scratch, d_Zs, count, m, d_Zmix);
     NEO_LAUNCHED(ctx);
     return NEO_OK;

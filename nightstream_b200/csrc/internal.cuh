@@ -191,3 +191,20 @@ int twist_addr_build_device(neo_gpu_ctx* ctx, int kind, uint32_t ell, const uint
                             const uint64_t* d_cols, neo_gpu_twist_addr** slot);
 
 inline unsigned ceil_div(uint64_t a, uint64_t b) { return (unsigned)((a + b - 1) / b); }
+
+// A kernel's dynamic shared-memory limit (cudaFuncAttributeMaxDynamicSharedMemorySize)
+// is a process-wide attribute of the function.  Host threads that set it to
+// their own launch's size would undo each other: a thread launching with 56 KB
+// fails ("too many resources requested for launch") when another thread set
+// 4 KB in between.  SmemLimit only ever raises the attribute, under a lock, so
+// every launch that follows its own at_least() call stays within the limit.
+struct SmemLimit {
+    std::mutex mu;
+    size_t cur = 48 * 1024;
+    template <typename Kernel>
+    cudaError_t at_least(Kernel* kernel, size_t bytes) {
+        std::lock_guard<std::mutex> lk(mu);
+        if (bytes > cur) cur = bytes;
+        return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)cur);
+    }
+};

@@ -66,6 +66,7 @@ SIGNATURES = {
     "neo_gpu_batch_submit_chunks": [P, P, P, P, P, U32, U32, U32, ctypes.c_char_p, P],
     "neo_gpu_batch_submit_mem": [P, P, P, P, U32, U32, U32, ctypes.c_char_p, P],
     "neo_gpu_batch_job_info": [P, U64, P, P, P],
+    "neo_gpu_batch_job_error": [P, U64, P, U64],
     "neo_gpu_batch_kernel_launches": [P],
     "neo_gpu_batch_destroy": [P],
     "neo_transcript_new": [ctypes.c_char_p, P],
@@ -673,8 +674,13 @@ class Batch:
         st = np.zeros(8, np.uint64)
         status = ctypes.c_int()
         self.lib.neo_gpu_batch_job_info(self.h, jid, _p(t), _p(st), ctypes.byref(status))
-        return {"latency_ms": float(t[0]), "queue_ms": float(t[1]), "submit_ms": float(t[2]),
+        info = {"latency_ms": float(t[0]), "queue_ms": float(t[1]), "submit_ms": float(t[2]),
                 "transcript_state": st, "status": status.value}
+        if status.value < 0:
+            buf = ctypes.create_string_buffer(512)
+            self.lib.neo_gpu_batch_job_error(self.h, jid, buf, 512)
+            info["error"] = buf.value.decode(errors="replace")
+        return info
 
     @property
     def kernel_launches(self) -> int:
