@@ -144,6 +144,9 @@ static inline __attribute__((always_inline)) uint64_t red_small(u128 x) {
     return add_carry_fix((uint64_t)x, (hi << 32) - hi);
 }
 static inline __attribute__((always_inline)) uint64_t mulq(uint64_t a, uint64_t b) { return red128((u128)a * b); }
+// a + b for any a < 2^64 and b < q (a round constant): with a carry the sum
+// a + b - 2^64 is below b < q = 2^64 - 2^32 + 1, so adding 2^32 - 1 cannot
+// carry again
 static inline __attribute__((always_inline)) uint64_t addq(uint64_t a, uint64_t b) { return add_carry_fix(a, b); }
 static inline __attribute__((always_inline)) uint64_t canonq(uint64_t a) { return a >= GL_Q ? a - GL_Q : a; }
 
@@ -225,7 +228,9 @@ __attribute__((noinline)) static void permute_impl(const Poseidon2<W>& P, uint64
     uint64_t x0 = addq(st[0], P.rc_int[0]);
     for (int r = 0; r < RP; r++) {
         const uint64_t x = sbox7(x0);
-        const uint64_t sum = addq(x, rest);
+        // both may lie in [q, 2^64), so the 65-bit sum goes through red_small
+        // (addq is exact only when one operand is below q)
+        const uint64_t sum = red_small((u128)x + rest);
         const u128 addend = (u128)rest + (r + 1 < RP ? P.rc_int[r + 1] : 0);
         x0 = red128((u128)mu0p1 * x + addend);  // < 2^128: mu0p1 < 2^64 - 2^32 + 2
         u128 nacc = 0;
