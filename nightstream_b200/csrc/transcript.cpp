@@ -1,6 +1,10 @@
 // transcript.cpp -- Poseidon2 width-8 permutation, ChaCha8 and the sponge.
 #include "transcript.h"
+#include <cstdlib>
 #include "gl.cuh"
+#if defined(__x86_64__)
+#include <immintrin.h>
+#endif
 
 namespace neo {
 
@@ -247,8 +251,157 @@ __attribute__((noinline)) static void permute_impl(const Poseidon2<W>& P, uint64
     for (int i = 0; i < W; i++) st_io[i] = canonq(st[i]);
 }
 
+#if defined(__x86_64__)
+// --------------------------------------------------- width 16 on AVX-512 --
+// The width-16 permutation (the CCS digest: a sponge over every nonzero of
+// the matrices, five entries per permutation) is throughput-bound in scalar
+// code: 16 independent S-boxes per full round and 15 linear lanes per
+// partial round.  With the state in two zmm registers (8 x u64 each) both
+// halves' multiply chains run side by side: full rounds do the S-boxes as
+// 32 x 32 -> 64-bit partial products and the external layer on 32-bit lane
+// halves (every intermediate fits 64 bits); partial rounds keep lane 0, the
+// S-box chain, in scalar registers and lanes 1..15 in the vectors, whose next
+// sum is sum_i mu_i x_i + 15 sum, so only lane 0's chain is serial.  Lanes
+// stay in [0, 2^64) as in the scalar code and the result is bit-identical to
+// it (1.5x faster on a Xeon with AVX-512).  Width 8 stays scalar: there the
+// vector multiply's latency outweighs its fewer instructions.
+#define NEO_AVX512 __attribute__((target("avx512f"), always_inline)) inline
+NEO_AVX512 static __m512i v_eps() { return _mm512_set1_epi64((long long)GL_EPS); }
+// (lo, hi) -> lo + 2^64 hi (mod q), the vector form of red_nc
+NEO_AVX512 static __m512i v_red(__m512i lo, __m512i hi) {
+    const __m512i eps = v_eps();
+    const __m512i hh = _mm512_srli_epi64(hi, 32), hl = _mm512_and_si512(hi, eps);
+    __m512i t0 = _mm512_sub_epi64(lo, hh);
+    t0 = _mm512_mask_sub_epi64(t0, _mm512_cmplt_epu64_mask(lo, hh), t0, eps);
+    const __m512i t1 = _mm512_sub_epi64(_mm512_slli_epi64(hl, 32), hl);
+    const __m512i s = _mm512_add_epi64(t0, t1);
+    return _mm512_mask_add_epi64(s, _mm512_cmplt_epu64_mask(s, t1), s, eps);
+}
+// a b (mod q) per lane from 32 x 32 -> 64 products: with a = ah 2^32 + al and
+// b = bh 2^32 + bl, t = ah bl + (al bl >> 32) and u = al bh + (t mod 2^32)
+// stay below 2^64, and a b = (al bl mod 2^32) + (u mod 2^32) 2^32
+// + (ah bh + t / 2^32 + u / 2^32) 2^64.
+NEO_AVX512 static __m512i v_mul(__m512i a, __m512i b, __m512i b_hi) {
+    const __m512i m32 = v_eps();
+    const __m512i a_hi = _mm512_srli_epi64(a, 32);
+    const __m512i ll = _mm512_mul_epu32(a, b);
+    const __m512i lh = _mm512_mul_epu32(a, b_hi);
+    const __m512i hl = _mm512_mul_epu32(a_hi, b);
+    const __m512i hh = _mm512_mul_epu32(a_hi, b_hi);
+    const __m512i t = _mm512_add_epi64(hl, _mm512_srli_epi64(ll, 32));
+    const __m512i u = _mm512_add_epi64(lh, _mm512_and_si512(t, m32));
+    const __m512i lo = _mm512_or_si512(_mm512_slli_epi64(u, 32), _mm512_and_si512(ll, m32));
+    const __m512i hi = _mm512_add_epi64(hh, _mm512_add_epi64(_mm512_srli_epi64(t, 32), _mm512_srli_epi64(u, 32)));
+    return v_red(lo, hi);
+}
+NEO_AVX512 static __m512i v_mul(__m512i a, __m512i b) { return v_mul(a, b, _mm512_srli_epi64(b, 32)); }
+// a + b with b < q in every lane (exact for the same reason as addq)
+NEO_AVX512 static __m512i v_add_small(__m512i a, __m512i b) {
+    const __m512i s = _mm512_add_epi64(a, b);
+    return _mm512_mask_add_epi64(s, _mm512_cmplt_epu64_mask(s, b), s, v_eps());
+}
+// block-local M4 on lanes < 2^32: lane i is sum_k C_k[i] x[(i + k) mod 4]
+// with C_0 = (5,6,5,6), C_1 = (7,1,7,1), C_2 = (1,1,1,1), C_3 = (3,4,3,4);
+// outputs < 16 * 2^32
+NEO_AVX512 static __m512i v_m4(__m512i v) {
+    const __m512i r1 = _mm512_permutexvar_epi64(_mm512_set_epi64(4, 7, 6, 5, 0, 3, 2, 1), v);
+    const __m512i r2 = _mm512_permutexvar_epi64(_mm512_set_epi64(5, 4, 7, 6, 1, 0, 3, 2), v);
+    const __m512i r3 = _mm512_permutexvar_epi64(_mm512_set_epi64(6, 5, 4, 7, 2, 1, 0, 3), v);
+    __m512i y = _mm512_mul_epu32(v, _mm512_set_epi64(6, 5, 6, 5, 6, 5, 6, 5));
+    y = _mm512_add_epi64(y, _mm512_mul_epu32(r1, _mm512_set_epi64(1, 7, 1, 7, 1, 7, 1, 7)));
+    y = _mm512_add_epi64(y, r2);
+    return _mm512_add_epi64(y, _mm512_mul_epu32(r3, _mm512_set_epi64(4, 3, 4, 3, 4, 3, 4, 3)));
+}
+// lo + hi 2^32 (mod q) for lo, hi < 2^40: hi = a 2^32 + b, a 2^64 = a (2^32 - 1)
+NEO_AVX512 static __m512i v_combine(__m512i lo, __m512i hi) {
+    const __m512i m32 = v_eps();
+    const __m512i a = _mm512_srli_epi64(hi, 32);
+    const __m512i base = _mm512_add_epi64(lo, _mm512_sub_epi64(_mm512_slli_epi64(a, 32), a));
+    const __m512i top = _mm512_slli_epi64(hi, 32);
+    const __m512i s2 = _mm512_add_epi64(base, top);
+    return _mm512_mask_add_epi64(s2, _mm512_cmplt_epu64_mask(s2, top), s2, m32);
+}
+// circ(2 M4, M4, M4, M4) with blocks 0, 1 in A and 2, 3 in B: the sum over
+// blocks is the 256-bit-half swap of A + B; outputs < 2^39 per lane half
+NEO_AVX512 static void v_external16(__m512i& A, __m512i& B) {
+    const __m512i m32 = v_eps();
+    const __m512i yal = v_m4(_mm512_and_si512(A, m32)), yah = v_m4(_mm512_srli_epi64(A, 32));
+    const __m512i ybl = v_m4(_mm512_and_si512(B, m32)), ybh = v_m4(_mm512_srli_epi64(B, 32));
+    __m512i sl = _mm512_add_epi64(yal, ybl), sh = _mm512_add_epi64(yah, ybh);
+    sl = _mm512_add_epi64(sl, _mm512_shuffle_i64x2(sl, sl, 0x4E));
+    sh = _mm512_add_epi64(sh, _mm512_shuffle_i64x2(sh, sh, 0x4E));
+    A = v_combine(_mm512_add_epi64(yal, sl), _mm512_add_epi64(yah, sh));
+    B = v_combine(_mm512_add_epi64(ybl, sl), _mm512_add_epi64(ybh, sh));
+}
+// sum of the 16 lanes of a and b (mod q): lane halves summed exactly
+NEO_AVX512 static uint64_t v_hsum2(__m512i a, __m512i b) {
+    const __m512i m32 = v_eps();
+    const uint64_t sl = (uint64_t)_mm512_reduce_add_epi64(_mm512_add_epi64(_mm512_and_si512(a, m32), _mm512_and_si512(b, m32)));
+    const uint64_t sh = (uint64_t)_mm512_reduce_add_epi64(_mm512_add_epi64(_mm512_srli_epi64(a, 32), _mm512_srli_epi64(b, 32)));
+    const uint64_t hi = sh >> 32, lo = sh & GL_EPS;
+    return add_carry_fix(sl + ((hi << 32) - hi), lo << 32);
+}
+NEO_AVX512 static void v_full16(__m512i& A, __m512i& B, const uint64_t* rc) {
+    const __m512i xa = v_add_small(A, _mm512_loadu_si512(rc)), xb = v_add_small(B, _mm512_loadu_si512(rc + 8));
+    const __m512i xa2 = v_mul(xa, xa), xb2 = v_mul(xb, xb);
+    A = v_mul(v_mul(xa2, xa), v_mul(xa2, xa2));
+    B = v_mul(v_mul(xb2, xb), v_mul(xb2, xb2));
+    v_external16(A, B);
+}
+__attribute__((target("avx512f"), noinline)) static void permute16_avx512(const Poseidon2<16>& P, uint64_t* st_io) {
+    __m512i A = _mm512_loadu_si512(st_io), B = _mm512_loadu_si512(st_io + 8);
+    v_external16(A, B);
+    for (int r = 0; r < 4; r++) v_full16(A, B, P.rc_ext[r]);
+    const __m512i muA = _mm512_maskz_loadu_epi64(0xFE, P.mu), muB = _mm512_loadu_si512(P.mu + 8);
+    const __m512i muA_hi = _mm512_srli_epi64(muA, 32), muB_hi = _mm512_srli_epi64(muB, 32);
+    uint64_t x0 = addq((uint64_t)_mm_cvtsi128_si64(_mm512_castsi512_si128(A)), P.rc_int[0]);
+    __m512i va = _mm512_maskz_mov_epi64(0xFE, A), vb = B;
+    uint64_t rest = v_hsum2(va, vb);
+    const uint64_t mu0p1 = P.mu[0] + 1;
+    for (int r = 0; r < 22; r++) {
+        const __m512i pa = v_mul(va, muA, muA_hi), pb = v_mul(vb, muB, muB_hi);
+        const uint64_t psum = v_hsum2(pa, pb);
+        const uint64_t x = sbox7(x0);
+        const uint64_t sum = canonq(red_small((u128)x + rest));
+        const u128 addend = (u128)rest + (r + 1 < 22 ? P.rc_int[r + 1] : 0);
+        x0 = red128((u128)mu0p1 * x + addend);
+        const __m512i bs = _mm512_set1_epi64((long long)sum);
+        va = v_add_small(pa, bs);
+        vb = v_add_small(pb, bs);
+        rest = red_small((u128)psum + red_small((u128)sum * 15));
+    }
+    A = _mm512_mask_set1_epi64(va, 0x01, (long long)x0);
+    B = vb;
+    for (int r = 4; r < 8; r++) v_full16(A, B, P.rc_ext[r]);
+    const __m512i q = _mm512_set1_epi64((long long)GL_Q);
+    A = _mm512_mask_sub_epi64(A, _mm512_cmpge_epu64_mask(A, q), A, q);
+    B = _mm512_mask_sub_epi64(B, _mm512_cmpge_epu64_mask(B, q), B, q);
+    _mm512_storeu_si512(st_io, A);
+    _mm512_storeu_si512(st_io + 8, B);
+}
+#undef NEO_AVX512
+
+// AVX-512F when the host has it, unless NEO_TRANSCRIPT_SCALAR is set (tests
+// compare both paths)
+static bool use_avx512() {
+    static const bool on = [] {
+        __builtin_cpu_init();
+        return __builtin_cpu_supports("avx512f") && !getenv("NEO_TRANSCRIPT_SCALAR");
+    }();
+    return on;
+}
+#endif
+
 template <int W>
 void Poseidon2<W>::permute(uint64_t* st_io) const {
+#if defined(__x86_64__)
+    if constexpr (W == 16) {
+        if (use_avx512()) {
+            permute16_avx512(*this, st_io);
+            return;
+        }
+    }
+#endif
     permute_impl<W>(*this, st_io);
 }
 

@@ -55,3 +55,23 @@ def test_ccs_digest_cache_returns_each_ccs_its_own_digest():
     for k, x in (("a", a), ("b", b), ("a", a), ("c", c), ("b", b), ("c", c), ("a", a)):
         assert np.array_equal(gpu.ccs_digest(x), want[k]), k
     assert not np.array_equal(want["a"], want["c"])
+
+
+def test_ccs_digest_simd_and_scalar_paths_match_oracle():
+    """The width-16 permutation behind the CCS digest has an AVX-512 path
+    (taken when the host has AVX-512F) and a scalar one (NEO_TRANSCRIPT_SCALAR
+    set): both give the oracle's digest, for a CCS whose digest takes some
+    ten thousand permutations."""
+    import os
+    import subprocess
+    import sys
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    code = ("import sys; sys.path.insert(0, %r); from nightstream_b200 import gpu, synth; "
+            "ccs, _ = synth.make_r1cs(12, 17); print(','.join(str(int(v)) for v in gpu.ccs_digest(ccs)))" % root)
+    ccs, _ = synth.make_r1cs(12, 17)
+    want = ",".join(str(int(v)) for v in O.ccs_digest(ccs))
+    for extra in ({}, {"NEO_TRANSCRIPT_SCALAR": "1"}):
+        env = {k: v for k, v in os.environ.items() if k != "NEO_TRANSCRIPT_SCALAR"}
+        env.update(extra)
+        out = subprocess.run([sys.executable, "-c", code], env=env, capture_output=True, text=True, check=True)
+        assert out.stdout.strip() == want, extra
