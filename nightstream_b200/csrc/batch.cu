@@ -181,24 +181,34 @@ static void finish_job(neo_gpu_batch* b, Job* j, int status, const char* err) {
 
 // every fold step of one request on this worker's context
 static void run_job(neo_gpu_batch* b, Worker& w, Job* j) {
-    int rc = j->mem ? neo_gpu_shard_create_mem(w.ctx, &j->ccs->d, j->m_in, j->k_rho, j->label.c_str(), &j->mem->d,
+    int rc = NEO_OK;
+    std::string err;  // a copy: finishing the request may overwrite the context's message
+    try {
+        rc = j->mem ? neo_gpu_shard_create_mem(w.ctx, &j->ccs->d, j->m_in, j->k_rho, j->label.c_str(), &j->mem->d,
                                                &j->shard)
                     : neo_gpu_shard_create(w.ctx, &j->ccs->d, j->m_in, j->k_rho, j->label.c_str(), &j->shard);
-    const uint64_t m = j->ccs->d.m;
-    while (rc == NEO_OK && j->steps_done < j->n_steps) {
-        if (j->steps_done > 0 && j->steps_done < j->inits.size()) {
-            auto& st = j->inits[j->steps_done];
-            for (uint32_t i = 0; rc == NEO_OK && i < st.size(); i++)
-                rc = neo_gpu_shard_set_twist_init(j->shard, i, st[i].first.size(), st[i].first.data(),
-                                                  st[i].second.data());
+        const uint64_t m = j->ccs->d.m;
+        while (rc == NEO_OK && j->steps_done < j->n_steps) {
+            if (j->steps_done > 0 && j->steps_done < j->inits.size()) {
+                auto& st = j->inits[j->steps_done];
+                for (uint32_t i = 0; rc == NEO_OK && i < st.size(); i++)
+                    rc = neo_gpu_shard_set_twist_init(j->shard, i, st[i].first.size(), st[i].first.data(),
+                                                      st[i].second.data());
+            }
+            if (rc != NEO_OK) break;
+            uint64_t len = 0;
+            const uint64_t* zs = j->z.size() > m ? j->z.data() + (uint64_t)j->steps_done * m : j->z.data();
+            rc = neo_gpu_shard_fold_step(j->shard, zs, nullptr, 0, &len);
+            if (rc == NEO_OK) j->steps_done++;
         }
-        if (rc != NEO_OK) break;
-        uint64_t len = 0;
-        const uint64_t* zs = j->z.size() > m ? j->z.data() + (uint64_t)j->steps_done * m : j->z.data();
-        rc = neo_gpu_shard_fold_step(j->shard, zs, nullptr, 0, &len);
-        if (rc == NEO_OK) j->steps_done++;
+        if (rc != NEO_OK) err = neo_gpu_last_error(w.ctx);
+    } catch (const std::bad_alloc&) {  // the request fails, the worker and the engine go on
+        rc = NEO_ERR_OOM;
+        err = "host allocation failed";
+    } catch (...) {
+        rc = NEO_ERR_INVARIANT;
+        err = "exception in the batch worker";
     }
-    std::string err = rc != NEO_OK ? std::string(neo_gpu_last_error(w.ctx)) : std::string();
     finish_job(b, j, rc == NEO_OK ? 1 : -rc, rc != NEO_OK ? err.c_str() : nullptr);
 }
 
@@ -221,7 +231,7 @@ static void worker_main(neo_gpu_batch* b, size_t wi) {
     }
 }
 
-extern "C" int neo_gpu_batch_create(int device, uint32_t n_workers, neo_gpu_batch** out) {
+static int neo_gpu_batch_create_impl_abi(int device, uint32_t n_workers, neo_gpu_batch** out) {
     if (!out || n_workers == 0 || n_workers > 256) return NEO_ERR_ARG;
     *out = nullptr;
     auto* b = new neo_gpu_batch();
@@ -248,13 +258,15 @@ extern "C" int neo_gpu_batch_create(int device, uint32_t n_workers, neo_gpu_batc
     *out = b;
     return NEO_OK;
 }
+extern "C" int neo_gpu_batch_create(int device, uint32_t n_workers, neo_gpu_batch** out) { NEO_ABI_GUARD(neo_gpu_batch_create_impl_abi(device, n_workers, out)) }
 
-extern "C" int neo_gpu_batch_set_reserve(neo_gpu_batch* b, uint64_t bytes) {
+static int neo_gpu_batch_set_reserve_impl_abi(neo_gpu_batch* b, uint64_t bytes) {
     if (!b) return NEO_ERR_ARG;
     std::lock_guard<std::mutex> lk(b->mu);
     b->reserve_margin = bytes;
     return NEO_OK;
 }
+extern "C" int neo_gpu_batch_set_reserve(neo_gpu_batch* b, uint64_t bytes) { NEO_ABI_GUARD(neo_gpu_batch_set_reserve_impl_abi(b, bytes)) }
 
 static int submit_impl(neo_gpu_batch* b, const neo_ccs_desc* ccs, const neo_mem_desc* mem, const uint64_t* z,
                        uint32_t n_steps, uint32_t m_in, uint32_t k_rho, const char* app_label, uint64_t* job_id,
@@ -298,33 +310,42 @@ static int submit_impl(neo_gpu_batch* b, const neo_ccs_desc* ccs, const neo_mem_
     return NEO_OK;
 }
 
-extern "C" int neo_gpu_batch_submit(neo_gpu_batch* b, const neo_ccs_desc* ccs, const uint64_t* z, uint32_t n_steps,
+static int neo_gpu_batch_submit_impl_abi(neo_gpu_batch* b, const neo_ccs_desc* ccs, const uint64_t* z, uint32_t n_steps,
                                     uint32_t m_in, uint32_t k_rho, const char* app_label, uint64_t* job_id) {
     return submit_impl(b, ccs, nullptr, z, n_steps, m_in, k_rho, app_label, job_id);
 }
+extern "C" int neo_gpu_batch_submit(neo_gpu_batch* b, const neo_ccs_desc* ccs, const uint64_t* z, uint32_t n_steps,
+                                    uint32_t m_in, uint32_t k_rho, const char* app_label, uint64_t* job_id) { NEO_ABI_GUARD(neo_gpu_batch_submit_impl_abi(b, ccs, z, n_steps, m_in, k_rho, app_label, job_id)) }
 
-extern "C" int neo_gpu_batch_submit_mem(neo_gpu_batch* b, const neo_ccs_desc* ccs, const neo_mem_desc* mem,
+static int neo_gpu_batch_submit_mem_impl_abi(neo_gpu_batch* b, const neo_ccs_desc* ccs, const neo_mem_desc* mem,
                                         const uint64_t* z, uint32_t n_steps, uint32_t m_in, uint32_t k_rho,
                                         const char* app_label, uint64_t* job_id) {
     return submit_impl(b, ccs, mem, z, n_steps, m_in, k_rho, app_label, job_id);
 }
+extern "C" int neo_gpu_batch_submit_mem(neo_gpu_batch* b, const neo_ccs_desc* ccs, const neo_mem_desc* mem,
+                                        const uint64_t* z, uint32_t n_steps, uint32_t m_in, uint32_t k_rho,
+                                        const char* app_label, uint64_t* job_id) { NEO_ABI_GUARD(neo_gpu_batch_submit_mem_impl_abi(b, ccs, mem, z, n_steps, m_in, k_rho, app_label, job_id)) }
 
-extern "C" int neo_gpu_batch_submit_chunks(neo_gpu_batch* b, const neo_ccs_desc* ccs, const neo_mem_desc* mem,
+static int neo_gpu_batch_submit_chunks_impl_abi(neo_gpu_batch* b, const neo_ccs_desc* ccs, const neo_mem_desc* mem,
                                            const uint64_t* zs, const neo_mem_init* inits, uint32_t n_steps,
                                            uint32_t m_in, uint32_t k_rho, const char* app_label, uint64_t* job_id) {
     return submit_impl(b, ccs, mem, zs, n_steps, m_in, k_rho, app_label, job_id, true, inits);
 }
+extern "C" int neo_gpu_batch_submit_chunks(neo_gpu_batch* b, const neo_ccs_desc* ccs, const neo_mem_desc* mem,
+                                           const uint64_t* zs, const neo_mem_init* inits, uint32_t n_steps,
+                                           uint32_t m_in, uint32_t k_rho, const char* app_label, uint64_t* job_id) { NEO_ABI_GUARD(neo_gpu_batch_submit_chunks_impl_abi(b, ccs, mem, zs, inits, n_steps, m_in, k_rho, app_label, job_id)) }
 
-extern "C" int neo_gpu_batch_wait_all(neo_gpu_batch* b, double timeout_ms) {
+static int neo_gpu_batch_wait_all_impl_abi(neo_gpu_batch* b, double timeout_ms) {
     if (!b) return NEO_ERR_ARG;
     std::unique_lock<std::mutex> lk(b->mu);
     bool ok = b->cv_done.wait_for(lk, std::chrono::duration<double, std::milli>(timeout_ms),
                                   [&] { return b->unfinished == 0; });
     return ok ? NEO_OK : NEO_ERR_CUDA;
 }
+extern "C" int neo_gpu_batch_wait_all(neo_gpu_batch* b, double timeout_ms) { NEO_ABI_GUARD(neo_gpu_batch_wait_all_impl_abi(b, timeout_ms)) }
 
 /* times3: [submit -> done ms, submit -> admit ms, submit time since batch creation ms] */
-extern "C" int neo_gpu_batch_job_info(neo_gpu_batch* b, uint64_t job_id, double* times3, uint64_t* tr_state8,
+static int neo_gpu_batch_job_info_impl_abi(neo_gpu_batch* b, uint64_t job_id, double* times3, uint64_t* tr_state8,
                                       int* status) {
     if (!b) return NEO_ERR_ARG;
     std::lock_guard<std::mutex> lk(b->mu);
@@ -340,8 +361,10 @@ extern "C" int neo_gpu_batch_job_info(neo_gpu_batch* b, uint64_t job_id, double*
     if (tr_state8) memcpy(tr_state8, j->tr_state, 64);
     return NEO_OK;
 }
+extern "C" int neo_gpu_batch_job_info(neo_gpu_batch* b, uint64_t job_id, double* times3, uint64_t* tr_state8,
+                                      int* status) { NEO_ABI_GUARD(neo_gpu_batch_job_info_impl_abi(b, job_id, times3, tr_state8, status)) }
 
-extern "C" int neo_gpu_batch_job_error(neo_gpu_batch* b, uint64_t job_id, char* buf, uint64_t cap) {
+static int neo_gpu_batch_job_error_impl_abi(neo_gpu_batch* b, uint64_t job_id, char* buf, uint64_t cap) {
     if (!b || !buf || cap == 0) return NEO_ERR_ARG;
     std::lock_guard<std::mutex> lk(b->mu);
     if (job_id >= b->jobs.size()) return NEO_ERR_ARG;
@@ -351,8 +374,9 @@ extern "C" int neo_gpu_batch_job_error(neo_gpu_batch* b, uint64_t job_id, char* 
     buf[n] = 0;
     return NEO_OK;
 }
+extern "C" int neo_gpu_batch_job_error(neo_gpu_batch* b, uint64_t job_id, char* buf, uint64_t cap) { NEO_ABI_GUARD(neo_gpu_batch_job_error_impl_abi(b, job_id, buf, cap)) }
 
-extern "C" int neo_gpu_batch_destroy(neo_gpu_batch* b) {
+static int neo_gpu_batch_destroy_impl_abi(neo_gpu_batch* b) {
     if (!b) return NEO_ERR_ARG;
     {
         std::lock_guard<std::mutex> lk(b->mu);
@@ -364,6 +388,7 @@ extern "C" int neo_gpu_batch_destroy(neo_gpu_batch* b) {
     delete b;
     return NEO_OK;
 }
+extern "C" int neo_gpu_batch_destroy(neo_gpu_batch* b) { NEO_ABI_GUARD(neo_gpu_batch_destroy_impl_abi(b)) }
 
 extern "C" uint64_t neo_gpu_batch_kernel_launches(const neo_gpu_batch* b) {
     if (!b) return 0;

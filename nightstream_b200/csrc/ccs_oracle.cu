@@ -618,7 +618,7 @@ static int oracle_init(neo_gpu_ctx* ctx, neo_gpu_ccs_oracle* o, const int8_t* d_
                        const K* alpha, const K* beta_a, const K* beta_r, K gamma, const K* r_inputs,
                        uint32_t ell_d, uint32_t ell_n, uint32_t d_sc);
 
-extern "C" int neo_gpu_ccs_oracle_create(neo_gpu_ctx* ctx, const neo_ccs_desc* desc, const int8_t* Z, uint32_t k,
+static int neo_gpu_ccs_oracle_create_impl_abi(neo_gpu_ctx* ctx, const neo_ccs_desc* desc, const int8_t* Z, uint32_t k,
                                          uint32_t b, const uint64_t* alpha, const uint64_t* beta_a,
                                          const uint64_t* beta_r, const uint64_t* gamma, const uint64_t* r_inputs,
                                          uint32_t ell_d, uint32_t ell_n, uint32_t d_sc, neo_gpu_ccs_oracle** out) {
@@ -644,6 +644,10 @@ extern "C" int neo_gpu_ccs_oracle_create(neo_gpu_ctx* ctx, const neo_ccs_desc* d
     *out = guard.release();
     return NEO_OK;
 }
+extern "C" int neo_gpu_ccs_oracle_create(neo_gpu_ctx* ctx, const neo_ccs_desc* desc, const int8_t* Z, uint32_t k,
+                                         uint32_t b, const uint64_t* alpha, const uint64_t* beta_a,
+                                         const uint64_t* beta_r, const uint64_t* gamma, const uint64_t* r_inputs,
+                                         uint32_t ell_d, uint32_t ell_n, uint32_t d_sc, neo_gpu_ccs_oracle** out) { NEO_ABI_GUARD(neo_gpu_ccs_oracle_create_impl_abi(ctx, desc, Z, k, b, alpha, beta_a, beta_r, gamma, r_inputs, ell_d, ell_n, d_sc, out)) }
 
 // Builds the oracle in *inout; an existing oracle is re-initialised in place so
 // its device workspaces are reused across fold steps.
@@ -986,7 +990,7 @@ static int ajtai_round(neo_gpu_ccs_oracle* o, const uint64_t* xs, uint32_t nx, u
     return NEO_OK;
 }
 
-extern "C" int neo_gpu_ccs_oracle_evals(neo_gpu_ccs_oracle* o, const uint64_t* xs, uint32_t nx, uint64_t* ys) {
+static int neo_gpu_ccs_oracle_evals_impl_abi(neo_gpu_ccs_oracle* o, const uint64_t* xs, uint32_t nx, uint64_t* ys) {
     if (!o) return NEO_ERR_ARG;
     neo_gpu_ctx* ctx = o->ctx;
     if (!xs || !ys || nx == 0 || nx > 16) return ctx->fail(NEO_ERR_ARG, "evals: bad args");
@@ -1009,8 +1013,9 @@ extern "C" int neo_gpu_ccs_oracle_evals(neo_gpu_ccs_oracle* o, const uint64_t* x
     }
     return ajtai_round(o, xs, nx, ys);
 }
+extern "C" int neo_gpu_ccs_oracle_evals(neo_gpu_ccs_oracle* o, const uint64_t* xs, uint32_t nx, uint64_t* ys) { NEO_ABI_GUARD(neo_gpu_ccs_oracle_evals_impl_abi(o, xs, nx, ys)) }
 
-extern "C" int neo_gpu_ccs_oracle_fold(neo_gpu_ccs_oracle* o, const uint64_t* r) {
+static int neo_gpu_ccs_oracle_fold_impl_abi(neo_gpu_ccs_oracle* o, const uint64_t* r) {
     if (!o) return NEO_ERR_ARG;
     if (!r) return o->ctx->fail(NEO_ERR_ARG, "fold: null r");
     K rr = gl::kmk(gl::canon(r[0]), gl::canon(r[1]));
@@ -1025,8 +1030,9 @@ extern "C" int neo_gpu_ccs_oracle_fold(neo_gpu_ccs_oracle* o, const uint64_t* r)
     o->round_idx++;
     return NEO_OK;
 }
+extern "C" int neo_gpu_ccs_oracle_fold(neo_gpu_ccs_oracle* o, const uint64_t* r) { NEO_ABI_GUARD(neo_gpu_ccs_oracle_fold_impl_abi(o, r)) }
 
-extern "C" int neo_gpu_ccs_oracle_row_rounds_device(neo_gpu_ccs_oracle* o, const uint64_t* chals, uint32_t n,
+static int neo_gpu_ccs_oracle_row_rounds_device_impl_abi(neo_gpu_ccs_oracle* o, const uint64_t* chals, uint32_t n,
                                                     uint64_t* d_coeffs) {
     if (!o) return NEO_ERR_ARG;
     neo_gpu_ctx* ctx = o->ctx;
@@ -1050,11 +1056,13 @@ extern "C" int neo_gpu_ccs_oracle_row_rounds_device(neo_gpu_ccs_oracle* o, const
     o->coeffs_valid = false;
     return NEO_OK;
 }
+extern "C" int neo_gpu_ccs_oracle_row_rounds_device(neo_gpu_ccs_oracle* o, const uint64_t* chals, uint32_t n,
+                                                    uint64_t* d_coeffs) { NEO_ABI_GUARD(neo_gpu_ccs_oracle_row_rounds_device_impl_abi(o, chals, n, d_coeffs)) }
 
 extern "C" uint32_t neo_gpu_ccs_oracle_num_rounds(const neo_gpu_ccs_oracle* o) { return o ? o->ell_n + o->ell_d : 0; }
 extern "C" uint32_t neo_gpu_ccs_oracle_degree_bound(const neo_gpu_ccs_oracle* o) { return o ? o->d_sc : 0; }
 
-extern "C" int neo_gpu_ccs_oracle_me_outputs(neo_gpu_ccs_oracle* o, uint64_t* y, uint64_t* y_scalars) {
+static int neo_gpu_ccs_oracle_me_outputs_impl_abi(neo_gpu_ccs_oracle* o, uint64_t* y, uint64_t* y_scalars) {
     if (!o) return NEO_ERR_ARG;
     neo_gpu_ctx* ctx = o->ctx;
     if (!y || !y_scalars) return ctx->fail(NEO_ERR_ARG, "me_outputs: null output");
@@ -1069,14 +1077,16 @@ extern "C" int neo_gpu_ccs_oracle_me_outputs(neo_gpu_ccs_oracle* o, uint64_t* y,
     NEO_CK(ctx, ctx_sync(ctx));
     return NEO_OK;
 }
+extern "C" int neo_gpu_ccs_oracle_me_outputs(neo_gpu_ccs_oracle* o, uint64_t* y, uint64_t* y_scalars) { NEO_ABI_GUARD(neo_gpu_ccs_oracle_me_outputs_impl_abi(o, y, y_scalars)) }
 
-extern "C" int neo_gpu_ccs_oracle_destroy(neo_gpu_ccs_oracle* o) {
+static int neo_gpu_ccs_oracle_destroy_impl_abi(neo_gpu_ccs_oracle* o) {
     if (!o) return NEO_ERR_ARG;
     cudaSetDevice(o->ctx->device);
     cudaStreamSynchronize(o->ctx->stream);
     delete o;
     return NEO_OK;
 }
+extern "C" int neo_gpu_ccs_oracle_destroy(neo_gpu_ccs_oracle* o) { NEO_ABI_GUARD(neo_gpu_ccs_oracle_destroy_impl_abi(o)) }
 
 // device view of v_j = M_j^T chi_r' for the fold step (child ME claims reuse it)
 int ccs_oracle_dev_vj(neo_gpu_ccs_oracle* o, const K** vj) {

@@ -154,7 +154,7 @@ int pp_finish(neo_gpu_ctx* ctx, PPEntry* pp, uint32_t kappa) {
     return NEO_OK;
 }
 
-extern "C" int neo_gpu_pp_upload(neo_gpu_ctx* ctx, uint32_t kappa, uint64_t m, const uint64_t* coeffs) {
+static int neo_gpu_pp_upload_impl_abi(neo_gpu_ctx* ctx, uint32_t kappa, uint64_t m, const uint64_t* coeffs) {
     if (!ctx) return NEO_ERR_ARG;
     if (!coeffs || kappa == 0 || m == 0 || kappa > 64) return ctx->fail(NEO_ERR_ARG, "pp_upload: bad args");
     cudaSetDevice(ctx->device);
@@ -166,8 +166,9 @@ extern "C" int neo_gpu_pp_upload(neo_gpu_ctx* ctx, uint32_t kappa, uint64_t m, c
     NEO_CK(ctx, cudaMemcpy(pp->d_pp, coeffs, (size_t)kappa * m * NEO_D * 8, cudaMemcpyHostToDevice));
     return pp_finish(ctx, pp, kappa);
 }
+extern "C" int neo_gpu_pp_upload(neo_gpu_ctx* ctx, uint32_t kappa, uint64_t m, const uint64_t* coeffs) { NEO_ABI_GUARD(neo_gpu_pp_upload_impl_abi(ctx, kappa, m, coeffs)) }
 
-extern "C" int neo_gpu_pp_download(neo_gpu_ctx* ctx, uint64_t m, uint64_t first, uint64_t count, uint64_t* out) {
+static int neo_gpu_pp_download_impl_abi(neo_gpu_ctx* ctx, uint64_t m, uint64_t first, uint64_t count, uint64_t* out) {
     if (!ctx) return NEO_ERR_ARG;
     if ((!out && count) || m == 0) return ctx->fail(NEO_ERR_ARG, "pp_download: bad args");
     cudaSetDevice(ctx->device);
@@ -182,8 +183,9 @@ extern "C" int neo_gpu_pp_download(neo_gpu_ctx* ctx, uint64_t m, uint64_t first,
     if (count) NEO_CK(ctx, cudaMemcpy(out, pp->d_pp + first, count * 8, cudaMemcpyDeviceToHost));
     return NEO_OK;
 }
+extern "C" int neo_gpu_pp_download(neo_gpu_ctx* ctx, uint64_t m, uint64_t first, uint64_t count, uint64_t* out) { NEO_ABI_GUARD(neo_gpu_pp_download_impl_abi(ctx, m, first, count, out)) }
 
-extern "C" int neo_gpu_commit(neo_gpu_ctx* ctx, const int8_t* digits, uint32_t n_vec, uint64_t m, uint64_t* out) {
+static int neo_gpu_commit_impl_abi(neo_gpu_ctx* ctx, const int8_t* digits, uint32_t n_vec, uint64_t m, uint64_t* out) {
     if (!ctx) return NEO_ERR_ARG;
     if (!digits || !out || n_vec == 0 || m == 0) return ctx->fail(NEO_ERR_ARG, "commit: bad args");
     cudaSetDevice(ctx->device);
@@ -201,14 +203,17 @@ extern "C" int neo_gpu_commit(neo_gpu_ctx* ctx, const int8_t* digits, uint32_t n
     NEO_CK(ctx, ctx_sync(ctx));
     return NEO_OK;
 }
+extern "C" int neo_gpu_commit(neo_gpu_ctx* ctx, const int8_t* digits, uint32_t n_vec, uint64_t m, uint64_t* out) { NEO_ABI_GUARD(neo_gpu_commit_impl_abi(ctx, digits, n_vec, m, out)) }
 
-extern "C" int neo_gpu_commit_device(neo_gpu_ctx* ctx, const int8_t* d_digits, uint32_t n_vec, uint64_t m,
+static int neo_gpu_commit_device_impl_abi(neo_gpu_ctx* ctx, const int8_t* d_digits, uint32_t n_vec, uint64_t m,
                                      uint64_t* d_out) {
     if (!ctx) return NEO_ERR_ARG;
     if (!d_digits || !d_out || n_vec == 0 || m == 0) return ctx->fail(NEO_ERR_ARG, "commit_device: bad args");
     cudaSetDevice(ctx->device);
     return launch_commit(ctx, d_digits, n_vec, m, d_out);
 }
+extern "C" int neo_gpu_commit_device(neo_gpu_ctx* ctx, const int8_t* d_digits, uint32_t n_vec, uint64_t m,
+                                     uint64_t* d_out) { NEO_ABI_GUARD(neo_gpu_commit_device_impl_abi(ctx, d_digits, n_vec, m, d_out)) }
 
 // ---------------------------------------------------------------------------
 // Allocation-free commitment.
@@ -234,7 +239,7 @@ std::mutex g_noalloc_mu;
 uint64_t* g_noalloc_ptr[NOALLOC_MAX_DEVICES] = {nullptr};
 }  // namespace
 
-extern "C" int neo_gpu_commit_noalloc(neo_gpu_ctx* ctx, const int8_t* d_digits, uint32_t n_vec, uint64_t m,
+static int neo_gpu_commit_noalloc_impl_abi(neo_gpu_ctx* ctx, const int8_t* d_digits, uint32_t n_vec, uint64_t m,
                                       uint64_t* d_out) {
     if (!ctx) return NEO_ERR_ARG;
     if (!d_digits || !d_out || n_vec == 0 || m == 0) return ctx->fail(NEO_ERR_ARG, "commit_noalloc: bad args");
@@ -280,3 +285,5 @@ extern "C" int neo_gpu_commit_noalloc(neo_gpu_ctx* ctx, const int8_t* d_digits, 
     NEO_LAUNCHED(ctx);
     return NEO_OK;
 }
+extern "C" int neo_gpu_commit_noalloc(neo_gpu_ctx* ctx, const int8_t* d_digits, uint32_t n_vec, uint64_t m,
+                                      uint64_t* d_out) { NEO_ABI_GUARD(neo_gpu_commit_noalloc_impl_abi(ctx, d_digits, n_vec, m, d_out)) }

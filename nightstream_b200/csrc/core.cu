@@ -5,7 +5,7 @@
 
 using gl::K;
 
-extern "C" int neo_gpu_ctx_create(int device, neo_gpu_ctx** out) {
+static int neo_gpu_ctx_create_impl_abi(int device, neo_gpu_ctx** out) {
     if (!out) return NEO_ERR_ARG;
     *out = nullptr;
     int ndev = 0;
@@ -26,12 +26,13 @@ extern "C" int neo_gpu_ctx_create(int device, neo_gpu_ctx** out) {
     *out = c;
     return NEO_OK;
 }
+extern "C" int neo_gpu_ctx_create(int device, neo_gpu_ctx** out) { NEO_ABI_GUARD(neo_gpu_ctx_create_impl_abi(device, out)) }
 
 // Stream on which DevBuf allocations of this thread are made (stream-ordered,
 // from the device's memory pool) and later freed; null: cudaMalloc / cudaFree.
 thread_local cudaStream_t g_alloc_stream = nullptr;
 
-extern "C" int neo_gpu_ctx_destroy(neo_gpu_ctx* ctx) {
+static int neo_gpu_ctx_destroy_impl_abi(neo_gpu_ctx* ctx) {
     if (!ctx) return NEO_ERR_ARG;
     cudaSetDevice(ctx->device);
     cudaStreamSynchronize(ctx->stream);
@@ -41,6 +42,7 @@ extern "C" int neo_gpu_ctx_destroy(neo_gpu_ctx* ctx) {
     delete ctx;
     return NEO_OK;
 }
+extern "C" int neo_gpu_ctx_destroy(neo_gpu_ctx* ctx) { NEO_ABI_GUARD(neo_gpu_ctx_destroy_impl_abi(ctx)) }
 
 extern "C" const char* neo_gpu_last_error(const neo_gpu_ctx* ctx) { return ctx ? ctx->err.c_str() : "null context"; }
 extern "C" uint64_t neo_gpu_kernel_launches(const neo_gpu_ctx* ctx) { return ctx ? ctx->launches : 0; }
@@ -57,17 +59,19 @@ int check_device_error(neo_gpu_ctx* ctx) {
     return NEO_OK;
 }
 
-extern "C" int neo_gpu_ctx_stream(const neo_gpu_ctx* ctx, void** stream) {
+static int neo_gpu_ctx_stream_impl_abi(const neo_gpu_ctx* ctx, void** stream) {
     if (!ctx || !stream) return NEO_ERR_ARG;
     *stream = (void*)ctx->stream;
     return NEO_OK;
 }
-extern "C" int neo_gpu_synchronize(neo_gpu_ctx* ctx) {
+extern "C" int neo_gpu_ctx_stream(const neo_gpu_ctx* ctx, void** stream) { NEO_ABI_GUARD(neo_gpu_ctx_stream_impl_abi(ctx, stream)) }
+static int neo_gpu_synchronize_impl_abi(neo_gpu_ctx* ctx) {
     if (!ctx) return NEO_ERR_ARG;
     cudaSetDevice(ctx->device);
     NEO_CK(ctx, ctx_sync(ctx));
     return NEO_OK;
 }
+extern "C" int neo_gpu_synchronize(neo_gpu_ctx* ctx) { NEO_ABI_GUARD(neo_gpu_synchronize_impl_abi(ctx)) }
 
 // ---------------------------------------------------------------------------
 // CCS upload: CSC as given, plus a CSR copy built on the host.
@@ -168,7 +172,7 @@ __global__ void decomp_b2_kernel(const uint64_t* __restrict__ z, uint64_t m, int
     }
 }
 
-extern "C" int neo_gpu_decomp_b2(neo_gpu_ctx* ctx, const uint64_t* z, uint64_t m, int8_t* Z) {
+static int neo_gpu_decomp_b2_impl_abi(neo_gpu_ctx* ctx, const uint64_t* z, uint64_t m, int8_t* Z) {
     if (!ctx || !z || !Z || m == 0) return ctx ? ctx->fail(NEO_ERR_ARG, "decomp: bad args") : NEO_ERR_ARG;
     cudaSetDevice(ctx->device);
     DevBuf<uint64_t> dz;
@@ -182,6 +186,7 @@ extern "C" int neo_gpu_decomp_b2(neo_gpu_ctx* ctx, const uint64_t* z, uint64_t m
     NEO_CK(ctx, ctx_sync(ctx));
     return NEO_OK;
 }
+extern "C" int neo_gpu_decomp_b2(neo_gpu_ctx* ctx, const uint64_t* z, uint64_t m, int8_t* Z) { NEO_ABI_GUARD(neo_gpu_decomp_b2_impl_abi(ctx, z, m, Z)) }
 
 // ---------------------------------------------------------------------------
 // Pi_RLC mix: Z_mix[:, c] = sum_i a_i(X) z_{i,c}(X) mod Phi_81 over the
@@ -250,7 +255,7 @@ int rlc_mix_device(neo_gpu_ctx* ctx, const int8_t* rho_coeffs_host, const int8_t
     return NEO_OK;
 }
 
-extern "C" int neo_gpu_rlc_mix(neo_gpu_ctx* ctx, const int8_t* rho_coeffs, const int8_t* Zs, uint32_t count,
+static int neo_gpu_rlc_mix_impl_abi(neo_gpu_ctx* ctx, const int8_t* rho_coeffs, const int8_t* Zs, uint32_t count,
                                uint64_t m, int32_t* Zmix) {
     if (!ctx) return NEO_ERR_ARG;
     if (!rho_coeffs || !Zs || !Zmix || count == 0 || count > 64 || m == 0) return ctx->fail(NEO_ERR_ARG, "rlc: bad args");
@@ -267,6 +272,8 @@ extern "C" int neo_gpu_rlc_mix(neo_gpu_ctx* ctx, const int8_t* rho_coeffs, const
     NEO_CK(ctx, ctx_sync(ctx));
     return NEO_OK;
 }
+extern "C" int neo_gpu_rlc_mix(neo_gpu_ctx* ctx, const int8_t* rho_coeffs, const int8_t* Zs, uint32_t count,
+                               uint64_t m, int32_t* Zmix) { NEO_ABI_GUARD(neo_gpu_rlc_mix_impl_abi(ctx, rho_coeffs, Zs, count, m, Zmix)) }
 
 // ---------------------------------------------------------------------------
 // Pi_DEC split (common.rs:75-268; balanced_divrem common.rs:44-58)
@@ -307,7 +314,7 @@ int split_b_device(neo_gpu_ctx* ctx, const int32_t* d_Zmix, uint64_t len, uint32
     return NEO_OK;
 }
 
-extern "C" int neo_gpu_split_b(neo_gpu_ctx* ctx, const int32_t* Zmix, uint64_t len, uint32_t k, uint32_t b,
+static int neo_gpu_split_b_impl_abi(neo_gpu_ctx* ctx, const int32_t* Zmix, uint64_t len, uint32_t k, uint32_t b,
                                int8_t* planes, uint8_t* nonzero) {
     if (!ctx) return NEO_ERR_ARG;
     if (!Zmix || !planes || !nonzero || len == 0) return ctx->fail(NEO_ERR_ARG, "split_b: bad args");
@@ -329,6 +336,8 @@ extern "C" int neo_gpu_split_b(neo_gpu_ctx* ctx, const int32_t* Zmix, uint64_t l
     for (uint32_t i = 0; i < k; i++) nonzero[i] = (flags[1] >> i) & 1;
     return NEO_OK;
 }
+extern "C" int neo_gpu_split_b(neo_gpu_ctx* ctx, const int32_t* Zmix, uint64_t len, uint32_t k, uint32_t b,
+                               int8_t* planes, uint8_t* nonzero) { NEO_ABI_GUARD(neo_gpu_split_b_impl_abi(ctx, Zmix, len, k, b, planes, nonzero)) }
 
 // ---------------------------------------------------------------------------
 // ME evaluations: v_j = M_j^T chi_r (CSC), y[w][j][rho] = sum_c Z_w[rho][c] v_j[c]
@@ -428,7 +437,7 @@ int launch_me_y(neo_gpu_ctx* ctx, const DevCcs& ccs, const int8_t* d_Z, uint32_t
     return NEO_OK;
 }
 
-extern "C" int neo_gpu_me_y(neo_gpu_ctx* ctx, const neo_ccs_desc* desc, const int8_t* Z, uint32_t n_w, uint32_t ell_n,
+static int neo_gpu_me_y_impl_abi(neo_gpu_ctx* ctx, const neo_ccs_desc* desc, const int8_t* Z, uint32_t n_w, uint32_t ell_n,
                             const uint64_t* r, uint32_t b, uint64_t* y, uint64_t* y_scalars) {
     if (!ctx) return NEO_ERR_ARG;
     if (!desc || !Z || !r || !y || !y_scalars || n_w == 0 || ell_n == 0 || ell_n > 30)
@@ -455,3 +464,5 @@ extern "C" int neo_gpu_me_y(neo_gpu_ctx* ctx, const neo_ccs_desc* desc, const in
     NEO_CK(ctx, ctx_sync(ctx));
     return NEO_OK;
 }
+extern "C" int neo_gpu_me_y(neo_gpu_ctx* ctx, const neo_ccs_desc* desc, const int8_t* Z, uint32_t n_w, uint32_t ell_n,
+                            const uint64_t* r, uint32_t b, uint64_t* y, uint64_t* y_scalars) { NEO_ABI_GUARD(neo_gpu_me_y_impl_abi(ctx, desc, Z, n_w, ell_n, r, b, y, y_scalars)) }

@@ -20,6 +20,7 @@
 // Pi_DEC writes the new children straight into slots 1..k_rho.  Bus columns
 // (the tail of z: cell (col, j) at bus_base + col * steps + j, time row
 // m_in + j) are decoded into dense K time columns d_cols[bus_cols][2^ell_n].
+#include <future>
 #include "internal.cuh"
 
 #include <list>
@@ -333,8 +334,43 @@ static void ccs_digest_words(const neo_ccs_desc* d, uint64_t* out4) {
     }
 }
 
+// Row-major (column, value) list of matrix j: columns ascending within a row
+// (the order of the dense scan the reference's digest follows).
+static std::vector<std::pair<uint64_t, uint64_t>> ccs_row_major(const neo_ccs_desc* d, uint32_t j,
+                                                                std::vector<uint64_t>& off) {
+    const uint64_t* cp = d->col_ptr + (size_t)j * (d->m + 1);
+    const uint64_t base = d->nnz_off[j], nnz = d->nnz_off[j + 1] - base;
+    off.assign(d->n + 1, 0);
+    for (uint64_t k = 0; k < nnz; k++) off[d->row_idx[base + k] + 1]++;
+    for (uint32_t r = 0; r < d->n; r++) off[r + 1] += off[r];
+    std::vector<std::pair<uint64_t, uint64_t>> ent(nnz);
+    std::vector<uint64_t> wp(off.begin(), off.end() - 1);
+    for (uint32_t c = 0; c < d->m; c++)
+        for (uint64_t k = cp[c]; k < cp[c + 1]; k++) ent[wp[d->row_idx[base + k]]++] = {c, d->vals[base + k]};
+    return ent;
+}
+
 static void ccs_digest_compute(const neo_ccs_desc* d, uint64_t* out4) {
     const neo::Poseidon2W16& P = neo::digest_perm();
+    // the sponge is one sequential chain; the row-major reorder of each sparse
+    // matrix runs on a helper thread meanwhile (matrix j is ready while the
+    // sponge absorbs matrices 0..j-1)
+    struct RowMajor {
+        std::vector<uint64_t> off;
+        std::vector<std::pair<uint64_t, uint64_t>> ent;
+    };
+    std::vector<RowMajor> rm(d->t);
+    std::vector<std::future<void>> ready(d->t);
+    for (uint32_t j = 0; j < d->t; j++)
+        if (!d->is_identity[j])
+        {
+            auto task = [d, j, &rm] { rm[j].ent = ccs_row_major(d, j, rm[j].off); };
+            try {
+                ready[j] = std::async(std::launch::async, task);
+            } catch (const std::system_error&) {  // no thread to spare: reorder when the sponge needs it
+                ready[j] = std::async(std::launch::deferred, task);
+            }
+        }
     uint64_t st[16] = {0};
     int ab = 0;
     const char* dom = "neo/ccs/matrices/v1";
@@ -356,18 +392,12 @@ static void ccs_digest_compute(const neo_ccs_desc* d, uint64_t* out4) {
         if (d->is_identity[j]) {
             for (uint64_t r = 0; r < d->n; r++) emit(r, r, 1);
         } else {
-            // row-major enumeration, columns ascending within a row
-            const uint64_t* cp = d->col_ptr + (size_t)j * (d->m + 1);
-            uint64_t base = d->nnz_off[j], nnz = d->nnz_off[j + 1] - base;
-            std::vector<uint64_t> off(d->n + 1, 0);
-            for (uint64_t k = 0; k < nnz; k++) off[d->row_idx[base + k] + 1]++;
-            for (uint32_t r = 0; r < d->n; r++) off[r + 1] += off[r];
-            std::vector<std::pair<uint64_t, uint64_t>> ent(nnz);
-            std::vector<uint64_t> wp(off.begin(), off.end() - 1);
-            for (uint32_t c = 0; c < d->m; c++)
-                for (uint64_t k = cp[c]; k < cp[c + 1]; k++) ent[wp[d->row_idx[base + k]]++] = {c, d->vals[base + k]};
+            ready[j].get();
+            const auto& off = rm[j].off;
+            const auto& ent = rm[j].ent;
             for (uint32_t r = 0; r < d->n; r++)
                 for (uint64_t e = off[r]; e < off[r + 1]; e++) emit(r, ent[e].first, ent[e].second);
+            rm[j] = RowMajor();
         }
         P.permute(st);
     }
@@ -407,11 +437,12 @@ static bool twist_set_init(TwistInst& ti, uint64_t n, const uint64_t* addr, cons
 }
 
 
-extern "C" int neo_ccs_digest(const neo_ccs_desc* d, uint64_t* out4) {
+static int neo_ccs_digest_impl_abi(const neo_ccs_desc* d, uint64_t* out4) {
     if (!d || !out4 || d->t == 0 || d->n == 0 || d->m == 0) return NEO_ERR_ARG;
     ccs_digest_words(d, out4);
     return NEO_OK;
 }
+extern "C" int neo_ccs_digest(const neo_ccs_desc* d, uint64_t* out4) { NEO_ABI_GUARD(neo_ccs_digest_impl_abi(d, out4)) }
 
 static int shard_create_impl(neo_gpu_ctx* ctx, const neo_ccs_desc* desc, uint32_t m_in, uint32_t k_rho,
                              const char* app_label, const neo_mem_desc* mem, neo_gpu_shard** out) {
@@ -524,17 +555,21 @@ static int shard_create_impl(neo_gpu_ctx* ctx, const neo_ccs_desc* desc, uint32_
     return NEO_OK;
 }
 
-extern "C" int neo_gpu_shard_create(neo_gpu_ctx* ctx, const neo_ccs_desc* desc, uint32_t m_in, uint32_t k_rho,
+static int neo_gpu_shard_create_impl_abi(neo_gpu_ctx* ctx, const neo_ccs_desc* desc, uint32_t m_in, uint32_t k_rho,
                                     const char* app_label, neo_gpu_shard** out) {
     return shard_create_impl(ctx, desc, m_in, k_rho, app_label, nullptr, out);
 }
+extern "C" int neo_gpu_shard_create(neo_gpu_ctx* ctx, const neo_ccs_desc* desc, uint32_t m_in, uint32_t k_rho,
+                                    const char* app_label, neo_gpu_shard** out) { NEO_ABI_GUARD(neo_gpu_shard_create_impl_abi(ctx, desc, m_in, k_rho, app_label, out)) }
 
-extern "C" int neo_gpu_shard_create_mem(neo_gpu_ctx* ctx, const neo_ccs_desc* desc, uint32_t m_in, uint32_t k_rho,
+static int neo_gpu_shard_create_mem_impl_abi(neo_gpu_ctx* ctx, const neo_ccs_desc* desc, uint32_t m_in, uint32_t k_rho,
                                         const char* app_label, const neo_mem_desc* mem, neo_gpu_shard** out) {
     return shard_create_impl(ctx, desc, m_in, k_rho, app_label, mem, out);
 }
+extern "C" int neo_gpu_shard_create_mem(neo_gpu_ctx* ctx, const neo_ccs_desc* desc, uint32_t m_in, uint32_t k_rho,
+                                        const char* app_label, const neo_mem_desc* mem, neo_gpu_shard** out) { NEO_ABI_GUARD(neo_gpu_shard_create_mem_impl_abi(ctx, desc, m_in, k_rho, app_label, mem, out)) }
 
-extern "C" int neo_gpu_shard_destroy(neo_gpu_shard* sh) {
+static int neo_gpu_shard_destroy_impl_abi(neo_gpu_shard* sh) {
     if (!sh) return NEO_ERR_ARG;
     cudaSetDevice(sh->ctx->device);
     cudaStreamSynchronize(sh->ctx->stream);
@@ -544,6 +579,7 @@ extern "C" int neo_gpu_shard_destroy(neo_gpu_shard* sh) {
     delete sh;
     return NEO_OK;
 }
+extern "C" int neo_gpu_shard_destroy(neo_gpu_shard* sh) { NEO_ABI_GUARD(neo_gpu_shard_destroy_impl_abi(sh)) }
 
 // ---------------------------------------------------------------------------
 // one fold step
@@ -1532,7 +1568,7 @@ static int fold_step_impl(neo_gpu_shard* sh, const uint64_t* z_host, const uint6
     return NEO_OK;
 }
 
-extern "C" int neo_gpu_shard_fold_step(neo_gpu_shard* sh, const uint64_t* z, uint64_t* proof, uint64_t proof_cap,
+static int neo_gpu_shard_fold_step_impl_abi(neo_gpu_shard* sh, const uint64_t* z, uint64_t* proof, uint64_t proof_cap,
                                        uint64_t* proof_len) {
     if (!sh) return NEO_ERR_ARG;
     if (!z) return sh->ctx->fail(NEO_ERR_ARG, "fold_step: null witness");
@@ -1546,9 +1582,11 @@ extern "C" int neo_gpu_shard_fold_step(neo_gpu_shard* sh, const uint64_t* z, uin
     }
     return NEO_OK;
 }
+extern "C" int neo_gpu_shard_fold_step(neo_gpu_shard* sh, const uint64_t* z, uint64_t* proof, uint64_t proof_cap,
+                                       uint64_t* proof_len) { NEO_ABI_GUARD(neo_gpu_shard_fold_step_impl_abi(sh, z, proof, proof_cap, proof_len)) }
 
 // Variant with the step witness already resident on the device (d_z: m words).
-extern "C" int neo_gpu_shard_fold_step_device(neo_gpu_shard* sh, const uint64_t* d_z, uint64_t* proof_len) {
+static int neo_gpu_shard_fold_step_device_impl_abi(neo_gpu_shard* sh, const uint64_t* d_z, uint64_t* proof_len) {
     if (!sh) return NEO_ERR_ARG;
     if (!d_z) return sh->ctx->fail(NEO_ERR_ARG, "fold_step_device: null witness");
     cudaSetDevice(sh->ctx->device);
@@ -1557,26 +1595,30 @@ extern "C" int neo_gpu_shard_fold_step_device(neo_gpu_shard* sh, const uint64_t*
     if (proof_len) *proof_len = sh->proof.size();
     return NEO_OK;
 }
+extern "C" int neo_gpu_shard_fold_step_device(neo_gpu_shard* sh, const uint64_t* d_z, uint64_t* proof_len) { NEO_ABI_GUARD(neo_gpu_shard_fold_step_device_impl_abi(sh, d_z, proof_len)) }
 
-extern "C" int neo_gpu_shard_transcript_state(const neo_gpu_shard* sh, uint64_t* st8) {
+static int neo_gpu_shard_transcript_state_impl_abi(const neo_gpu_shard* sh, uint64_t* st8) {
     if (!sh || !st8) return NEO_ERR_ARG;
     memcpy(st8, sh->tr->state(), 64);
     return NEO_OK;
 }
+extern "C" int neo_gpu_shard_transcript_state(const neo_gpu_shard* sh, uint64_t* st8) { NEO_ABI_GUARD(neo_gpu_shard_transcript_state_impl_abi(sh, st8)) }
 
-extern "C" int neo_gpu_shard_ccs_digest(const neo_gpu_shard* sh, uint64_t* d4) {
+static int neo_gpu_shard_ccs_digest_impl_abi(const neo_gpu_shard* sh, uint64_t* d4) {
     if (!sh || !d4) return NEO_ERR_ARG;
     memcpy(d4, sh->mat_digest, 32);
     return NEO_OK;
 }
+extern "C" int neo_gpu_shard_ccs_digest(const neo_gpu_shard* sh, uint64_t* d4) { NEO_ABI_GUARD(neo_gpu_shard_ccs_digest_impl_abi(sh, d4)) }
 
-extern "C" int neo_gpu_shard_step_stats(const neo_gpu_shard* sh, double* out, uint32_t n) {
+static int neo_gpu_shard_step_stats_impl_abi(const neo_gpu_shard* sh, double* out, uint32_t n) {
     if (!sh || !out) return NEO_ERR_ARG;
     for (uint32_t i = 0; i < n && i < 12; i++) out[i] = sh->stats[i];
     return NEO_OK;
 }
+extern "C" int neo_gpu_shard_step_stats(const neo_gpu_shard* sh, double* out, uint32_t n) { NEO_ABI_GUARD(neo_gpu_shard_step_stats_impl_abi(sh, out, n)) }
 
-extern "C" int neo_gpu_shard_set_twist_init(neo_gpu_shard* sh, uint32_t mem_idx, uint64_t n_init,
+static int neo_gpu_shard_set_twist_init_impl_abi(neo_gpu_shard* sh, uint32_t mem_idx, uint64_t n_init,
                                             const uint64_t* init_addr, const uint64_t* init_val) {
     if (!sh) return NEO_ERR_ARG;
     neo_gpu_ctx* ctx = sh->ctx;
@@ -1592,9 +1634,12 @@ extern "C" int neo_gpu_shard_set_twist_init(neo_gpu_shard* sh, uint32_t mem_idx,
     memcpy(ti.digest, tmp.digest, 32);
     return NEO_OK;
 }
+extern "C" int neo_gpu_shard_set_twist_init(neo_gpu_shard* sh, uint32_t mem_idx, uint64_t n_init,
+                                            const uint64_t* init_addr, const uint64_t* init_val) { NEO_ABI_GUARD(neo_gpu_shard_set_twist_init_impl_abi(sh, mem_idx, n_init, init_addr, init_val)) }
 
-extern "C" int neo_gpu_shard_val_obligations(const neo_gpu_shard* sh, uint64_t* count) {
+static int neo_gpu_shard_val_obligations_impl_abi(const neo_gpu_shard* sh, uint64_t* count) {
     if (!sh || !count) return NEO_ERR_ARG;
     *count = sh->val_obligations;
     return NEO_OK;
 }
+extern "C" int neo_gpu_shard_val_obligations(const neo_gpu_shard* sh, uint64_t* count) { NEO_ABI_GUARD(neo_gpu_shard_val_obligations_impl_abi(sh, count)) }

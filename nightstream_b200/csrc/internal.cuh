@@ -8,6 +8,7 @@
 #include <string>
 #include <vector>
 #include "../../include/neo_gpu.h"
+#include "abi_guard.h"
 #include "gl.cuh"
 
 #define NEO_D 54

@@ -598,13 +598,17 @@ int mem_create(neo_gpu_ctx* ctx, int kind, uint32_t ell, const uint64_t* r_point
 
 }  // namespace
 
-extern "C" int neo_gpu_mem_oracle_create(neo_gpu_ctx* ctx, int kind, uint32_t ell, const uint64_t* r_point,
+static int neo_gpu_mem_oracle_create_impl_abi(neo_gpu_ctx* ctx, int kind, uint32_t ell, const uint64_t* r_point,
                                          uint32_t ell_addr, const uint64_t* r_addr, const uint64_t* init_at_r_addr,
                                          uint32_t n_cols, const uint64_t* cols, const uint64_t* weights,
                                          uint64_t* claim, neo_gpu_mem_oracle** out) {
     return mem_create(ctx, kind, ell, r_point, ell_addr, r_addr, init_at_r_addr, n_cols, cols, false, weights, claim,
                       out);
 }
+extern "C" int neo_gpu_mem_oracle_create(neo_gpu_ctx* ctx, int kind, uint32_t ell, const uint64_t* r_point,
+                                         uint32_t ell_addr, const uint64_t* r_addr, const uint64_t* init_at_r_addr,
+                                         uint32_t n_cols, const uint64_t* cols, const uint64_t* weights,
+                                         uint64_t* claim, neo_gpu_mem_oracle** out) { NEO_ABI_GUARD(neo_gpu_mem_oracle_create_impl_abi(ctx, kind, ell, r_point, ell_addr, r_addr, init_at_r_addr, n_cols, cols, weights, claim, out)) }
 
 // Rebuild into *slot when it holds an oracle (its device buffers are kept),
 // create one otherwise; columns in device memory.  Fold steps call this every
@@ -618,7 +622,7 @@ int mem_oracle_build_device(neo_gpu_ctx* ctx, int kind, uint32_t ell, const uint
                       slot, true);
 }
 
-extern "C" int neo_gpu_mem_oracle_create_device(neo_gpu_ctx* ctx, int kind, uint32_t ell, const uint64_t* r_point,
+static int neo_gpu_mem_oracle_create_device_impl_abi(neo_gpu_ctx* ctx, int kind, uint32_t ell, const uint64_t* r_point,
                                                 uint32_t ell_addr, const uint64_t* r_addr,
                                                 const uint64_t* init_at_r_addr, uint32_t n_cols,
                                                 const uint64_t* d_cols, const uint64_t* weights, uint64_t* claim,
@@ -626,8 +630,13 @@ extern "C" int neo_gpu_mem_oracle_create_device(neo_gpu_ctx* ctx, int kind, uint
     return mem_create(ctx, kind, ell, r_point, ell_addr, r_addr, init_at_r_addr, n_cols, d_cols, true, weights, claim,
                       out);
 }
+extern "C" int neo_gpu_mem_oracle_create_device(neo_gpu_ctx* ctx, int kind, uint32_t ell, const uint64_t* r_point,
+                                                uint32_t ell_addr, const uint64_t* r_addr,
+                                                const uint64_t* init_at_r_addr, uint32_t n_cols,
+                                                const uint64_t* d_cols, const uint64_t* weights, uint64_t* claim,
+                                                neo_gpu_mem_oracle** out) { NEO_ABI_GUARD(neo_gpu_mem_oracle_create_device_impl_abi(ctx, kind, ell, r_point, ell_addr, r_addr, init_at_r_addr, n_cols, d_cols, weights, claim, out)) }
 
-extern "C" int neo_gpu_mem_oracle_evals(neo_gpu_mem_oracle* o, const uint64_t* xs, uint32_t nx, uint64_t* ys) {
+static int neo_gpu_mem_oracle_evals_impl_abi(neo_gpu_mem_oracle* o, const uint64_t* xs, uint32_t nx, uint64_t* ys) {
     if (!o) return NEO_ERR_ARG;
     if ((!xs || !ys) && nx) return o->ctx->fail(NEO_ERR_ARG, "mem_oracle_evals: null buffer");
     cudaSetDevice(o->ctx->device);
@@ -640,8 +649,9 @@ extern "C" int neo_gpu_mem_oracle_evals(neo_gpu_mem_oracle* o, const uint64_t* x
     }
     return NEO_OK;
 }
+extern "C" int neo_gpu_mem_oracle_evals(neo_gpu_mem_oracle* o, const uint64_t* xs, uint32_t nx, uint64_t* ys) { NEO_ABI_GUARD(neo_gpu_mem_oracle_evals_impl_abi(o, xs, nx, ys)) }
 
-extern "C" int neo_gpu_mem_oracle_fold(neo_gpu_mem_oracle* o, const uint64_t* r) {
+static int neo_gpu_mem_oracle_fold_impl_abi(neo_gpu_mem_oracle* o, const uint64_t* r) {
     if (!o) return NEO_ERR_ARG;
     if (!r) return o->ctx->fail(NEO_ERR_ARG, "mem_oracle_fold: null challenge");
     if (o->bit_idx >= o->ell) return NEO_OK;  // no rounds left: ignored, as in the reference
@@ -661,17 +671,19 @@ extern "C" int neo_gpu_mem_oracle_fold(neo_gpu_mem_oracle* o, const uint64_t* r)
     o->bit_idx++;
     return NEO_OK;
 }
+extern "C" int neo_gpu_mem_oracle_fold(neo_gpu_mem_oracle* o, const uint64_t* r) { NEO_ABI_GUARD(neo_gpu_mem_oracle_fold_impl_abi(o, r)) }
 
 extern "C" uint32_t neo_gpu_mem_oracle_num_rounds(const neo_gpu_mem_oracle* o) { return o ? o->ell - o->bit_idx : 0; }
 extern "C" uint32_t neo_gpu_mem_oracle_degree_bound(const neo_gpu_mem_oracle* o) { return o ? o->deg : 0; }
 
-extern "C" int neo_gpu_mem_oracle_destroy(neo_gpu_mem_oracle* o) {
+static int neo_gpu_mem_oracle_destroy_impl_abi(neo_gpu_mem_oracle* o) {
     if (!o) return NEO_OK;
     cudaSetDevice(o->ctx->device);
     cudaStreamSynchronize(o->ctx->stream);
     delete o;
     return NEO_OK;
 }
+extern "C" int neo_gpu_mem_oracle_destroy(neo_gpu_mem_oracle* o) { NEO_ABI_GUARD(neo_gpu_mem_oracle_destroy_impl_abi(o)) }
 
 // AddressLookupOracle weights from device columns: d_rcycle (ell K), d_has
 // (2^ell K), d_bits (A columns of 2^ell K), d_table (table_len K).  Writes
@@ -708,7 +720,7 @@ int addr_weights_device(neo_gpu_ctx* ctx, uint32_t ell, const K* d_rcycle, uint3
     return NEO_OK;
 }
 
-extern "C" int neo_gpu_addr_lookup_weights(neo_gpu_ctx* ctx, uint32_t ell, const uint64_t* r_cycle, uint32_t ell_addr,
+static int neo_gpu_addr_lookup_weights_impl_abi(neo_gpu_ctx* ctx, uint32_t ell, const uint64_t* r_cycle, uint32_t ell_addr,
                                            const uint64_t* has_lookup, const uint64_t* addr_bits,
                                            const uint64_t* table, uint64_t table_len, uint64_t* weights,
                                            uint64_t* claim) {
@@ -738,6 +750,10 @@ extern "C" int neo_gpu_addr_lookup_weights(neo_gpu_ctx* ctx, uint32_t ell, const
     claim[1] = cl.im;
     return NEO_OK;
 }
+extern "C" int neo_gpu_addr_lookup_weights(neo_gpu_ctx* ctx, uint32_t ell, const uint64_t* r_cycle, uint32_t ell_addr,
+                                           const uint64_t* has_lookup, const uint64_t* addr_bits,
+                                           const uint64_t* table, uint64_t table_len, uint64_t* weights,
+                                           uint64_t* claim) { NEO_ABI_GUARD(neo_gpu_addr_lookup_weights_impl_abi(ctx, ell, r_cycle, ell_addr, has_lookup, addr_bits, table, table_len, weights, claim)) }
 
 // ===========================================================================
 // Twist address-lane oracles (TwistReadCheckAddrOracleSparseTime /
@@ -1120,20 +1136,27 @@ int twist_addr_build_device(neo_gpu_ctx* ctx, int kind, uint32_t ell, const uint
     return ta_create(ctx, kind, ell, r_cycle, ell_addr, n_init, init_addr, init_val, d_cols, true, slot, true);
 }
 
-extern "C" int neo_gpu_twist_addr_create(neo_gpu_ctx* ctx, int kind, uint32_t ell, const uint64_t* r_cycle,
+static int neo_gpu_twist_addr_create_impl_abi(neo_gpu_ctx* ctx, int kind, uint32_t ell, const uint64_t* r_cycle,
                                          uint32_t ell_addr, uint64_t n_init, const uint64_t* init_addr,
                                          const uint64_t* init_val, const uint64_t* cols, neo_gpu_twist_addr** out) {
     return ta_create(ctx, kind, ell, r_cycle, ell_addr, n_init, init_addr, init_val, cols, false, out);
 }
+extern "C" int neo_gpu_twist_addr_create(neo_gpu_ctx* ctx, int kind, uint32_t ell, const uint64_t* r_cycle,
+                                         uint32_t ell_addr, uint64_t n_init, const uint64_t* init_addr,
+                                         const uint64_t* init_val, const uint64_t* cols, neo_gpu_twist_addr** out) { NEO_ABI_GUARD(neo_gpu_twist_addr_create_impl_abi(ctx, kind, ell, r_cycle, ell_addr, n_init, init_addr, init_val, cols, out)) }
 
-extern "C" int neo_gpu_twist_addr_create_device(neo_gpu_ctx* ctx, int kind, uint32_t ell, const uint64_t* r_cycle,
+static int neo_gpu_twist_addr_create_device_impl_abi(neo_gpu_ctx* ctx, int kind, uint32_t ell, const uint64_t* r_cycle,
                                                 uint32_t ell_addr, uint64_t n_init, const uint64_t* init_addr,
                                                 const uint64_t* init_val, const uint64_t* d_cols,
                                                 neo_gpu_twist_addr** out) {
     return ta_create(ctx, kind, ell, r_cycle, ell_addr, n_init, init_addr, init_val, d_cols, true, out);
 }
+extern "C" int neo_gpu_twist_addr_create_device(neo_gpu_ctx* ctx, int kind, uint32_t ell, const uint64_t* r_cycle,
+                                                uint32_t ell_addr, uint64_t n_init, const uint64_t* init_addr,
+                                                const uint64_t* init_val, const uint64_t* d_cols,
+                                                neo_gpu_twist_addr** out) { NEO_ABI_GUARD(neo_gpu_twist_addr_create_device_impl_abi(ctx, kind, ell, r_cycle, ell_addr, n_init, init_addr, init_val, d_cols, out)) }
 
-extern "C" int neo_gpu_twist_addr_evals(neo_gpu_twist_addr* o, const uint64_t* xs, uint32_t nx, uint64_t* ys) {
+static int neo_gpu_twist_addr_evals_impl_abi(neo_gpu_twist_addr* o, const uint64_t* xs, uint32_t nx, uint64_t* ys) {
     if (!o) return NEO_ERR_ARG;
     if ((!xs || !ys) && nx) return o->ctx->fail(NEO_ERR_ARG, "twist_addr_evals: null buffer");
     cudaSetDevice(o->ctx->device);
@@ -1147,8 +1170,9 @@ extern "C" int neo_gpu_twist_addr_evals(neo_gpu_twist_addr* o, const uint64_t* x
     }
     return NEO_OK;
 }
+extern "C" int neo_gpu_twist_addr_evals(neo_gpu_twist_addr* o, const uint64_t* xs, uint32_t nx, uint64_t* ys) { NEO_ABI_GUARD(neo_gpu_twist_addr_evals_impl_abi(o, xs, nx, ys)) }
 
-extern "C" int neo_gpu_twist_addr_fold(neo_gpu_twist_addr* o, const uint64_t* r) {
+static int neo_gpu_twist_addr_fold_impl_abi(neo_gpu_twist_addr* o, const uint64_t* r) {
     if (!o) return NEO_ERR_ARG;
     if (!r) return o->ctx->fail(NEO_ERR_ARG, "twist_addr_fold: null challenge");
     const uint32_t done = o->bit + (o->pending ? 1 : 0);
@@ -1162,16 +1186,18 @@ extern "C" int neo_gpu_twist_addr_fold(neo_gpu_twist_addr* o, const uint64_t* r)
     o->pending_r = kload_h(r);
     return NEO_OK;
 }
+extern "C" int neo_gpu_twist_addr_fold(neo_gpu_twist_addr* o, const uint64_t* r) { NEO_ABI_GUARD(neo_gpu_twist_addr_fold_impl_abi(o, r)) }
 
 extern "C" uint32_t neo_gpu_twist_addr_num_rounds(const neo_gpu_twist_addr* o) {
     return o ? o->A - o->bit - (o->pending ? 1 : 0) : 0;
 }
 extern "C" uint32_t neo_gpu_twist_addr_degree_bound(const neo_gpu_twist_addr* o) { return o ? 2 : 0; }
 
-extern "C" int neo_gpu_twist_addr_destroy(neo_gpu_twist_addr* o) {
+static int neo_gpu_twist_addr_destroy_impl_abi(neo_gpu_twist_addr* o) {
     if (!o) return NEO_OK;
     cudaSetDevice(o->ctx->device);
     cudaStreamSynchronize(o->ctx->stream);
     delete o;
     return NEO_OK;
 }
+extern "C" int neo_gpu_twist_addr_destroy(neo_gpu_twist_addr* o) { NEO_ABI_GUARD(neo_gpu_twist_addr_destroy_impl_abi(o)) }

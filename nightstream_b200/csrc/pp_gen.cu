@@ -235,7 +235,7 @@ int chacha8_sample_device(neo_gpu_ctx* ctx, const uint8_t* seeds, uint32_t n_str
     return NEO_OK;
 }
 
-extern "C" int neo_gpu_chacha8_sample(neo_gpu_ctx* ctx, const uint8_t* seeds, uint32_t n_streams,
+static int neo_gpu_chacha8_sample_impl_abi(neo_gpu_ctx* ctx, const uint8_t* seeds, uint32_t n_streams,
                                       const uint64_t* counts, uint64_t bound, uint64_t* out) {
     if (!ctx) return NEO_ERR_ARG;
     if ((n_streams && (!seeds || !counts)) || !out) return ctx->fail(NEO_ERR_ARG, "chacha8_sample: bad args");
@@ -255,8 +255,10 @@ extern "C" int neo_gpu_chacha8_sample(neo_gpu_ctx* ctx, const uint8_t* seeds, ui
     NEO_CK(ctx, ctx_sync(ctx));
     return NEO_OK;
 }
+extern "C" int neo_gpu_chacha8_sample(neo_gpu_ctx* ctx, const uint8_t* seeds, uint32_t n_streams,
+                                      const uint64_t* counts, uint64_t bound, uint64_t* out) { NEO_ABI_GUARD(neo_gpu_chacha8_sample_impl_abi(ctx, seeds, n_streams, counts, bound, out)) }
 
-extern "C" int neo_gpu_pp_generate(neo_gpu_ctx* ctx, const uint8_t* seed, uint32_t kappa, uint64_t m, int mode) {
+static int neo_gpu_pp_generate_impl_abi(neo_gpu_ctx* ctx, const uint8_t* seed, uint32_t kappa, uint64_t m, int mode) {
     if (!ctx) return NEO_ERR_ARG;
     if (!seed || kappa == 0 || kappa > 64 || m == 0) return ctx->fail(NEO_ERR_ARG, "pp_generate: bad args");
     if (mode != NEO_PP_SETUP && mode != NEO_PP_SETUP_PAR) return ctx->fail(NEO_ERR_ARG, "pp_generate: bad mode");
@@ -299,3 +301,4 @@ extern "C" int neo_gpu_pp_generate(neo_gpu_ctx* ctx, const uint8_t* seed, uint32
     if (rc) return rc;
     return pp_finish(ctx, pp, kappa);
 }
+extern "C" int neo_gpu_pp_generate(neo_gpu_ctx* ctx, const uint8_t* seed, uint32_t kappa, uint64_t m, int mode) { NEO_ABI_GUARD(neo_gpu_pp_generate_impl_abi(ctx, seed, kappa, m, mode)) }
