@@ -55,7 +55,38 @@ GL_HD uint64_t mulhi(uint64_t a, uint64_t b) {
 #endif
 }
 
-GL_HD uint64_t mul(uint64_t a, uint64_t b) { return reduce128(a * b, mulhi(a, b)); }
+#ifdef __CUDA_ARCH__
+// a b (mod q) on the device: the four 32 x 32 partial products of a b in one
+// carry chain (the two 64-bit halves of the product computed separately
+// would repeat the cross terms), then reduce128 on the limbs
+// (lo, r2 + 2^32 r3) with lo = r0 + 2^32 r1.
+__device__ __forceinline__ uint64_t mul_dev(uint64_t a, uint64_t b) {
+    const uint32_t a0 = (uint32_t)a, a1 = (uint32_t)(a >> 32), b0 = (uint32_t)b, b1 = (uint32_t)(b >> 32);
+    uint32_t r0, r1, r2, r3;
+    asm("{\n\t"
+        "mul.lo.u32 %0, %4, %6;\n\t"
+        "mul.hi.u32 %1, %4, %6;\n\t"
+        "mad.lo.cc.u32 %1, %4, %7, %1;\n\t"
+        "madc.hi.u32 %2, %4, %7, 0;\n\t"
+        "mad.lo.cc.u32 %1, %5, %6, %1;\n\t"
+        "madc.hi.cc.u32 %2, %5, %6, %2;\n\t"
+        "addc.u32 %3, 0, 0;\n\t"
+        "mad.lo.cc.u32 %2, %5, %7, %2;\n\t"
+        "madc.hi.u32 %3, %5, %7, %3;\n\t"
+        "}"
+        : "=r"(r0), "=r"(r1), "=r"(r2), "=r"(r3)
+        : "r"(a0), "r"(a1), "r"(b0), "r"(b1));
+    return reduce128(((uint64_t)r1 << 32) | r0, ((uint64_t)r3 << 32) | r2);
+}
+#endif
+
+GL_HD uint64_t mul(uint64_t a, uint64_t b) {
+#ifdef __CUDA_ARCH__
+    return mul_dev(a, b);
+#else
+    return reduce128(a * b, mulhi(a, b));
+#endif
+}
 
 GL_HD uint64_t from_i64(int64_t v) { return v >= 0 ? (uint64_t)v : GL_Q - (uint64_t)(-v); }
 
@@ -87,8 +118,17 @@ GL_HD K kneg(K a) { return kmk(neg(a.re), neg(a.im)); }
 GL_HD K kdbl(K a) { return kadd(a, a); }
 GL_HD bool kiszero(K a) { return (a.re | a.im) == 0; }
 
-// 7x mod q for x < q
-GL_HD uint64_t mul7(uint64_t x) { return mul_small(x, 7); }
+// 7x mod q for any x < 2^64, canonical: 7x = 8x - x as a 67-bit value
+// (lo, hi) with hi < 7, then lo + hi (2^32 - 1)
+GL_HD uint64_t mul7(uint64_t x) {
+    const uint64_t lo8 = x << 3;
+    const uint64_t lo = lo8 - x;
+    const uint64_t hi = (x >> 61) - (uint64_t)(lo8 < x);
+    const uint64_t t1 = (hi << 32) - hi;
+    uint64_t s = lo + t1;
+    s += (uint64_t)(s < t1) * GL_EPS;  // a carry leaves s < t1 < 2^35
+    return canon(s);
+}
 
 GL_HD K kmul(K a, K b) {
     uint64_t rr = add(mul(a.re, b.re), mul7(mul(a.im, b.im)));
