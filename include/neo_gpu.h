@@ -293,6 +293,19 @@ int neo_gpu_shard_create_mem(neo_gpu_ctx* ctx, const neo_ccs_desc* ccs, uint32_t
 /* Number of val-lane DEC children emitted so far (the reference's
  * val_lane_obligations, shard.rs:2548-2991). */
 int neo_gpu_shard_val_obligations(const neo_gpu_shard* sh, uint64_t* count);
+/* Checkpoint / resume: the state a shard carries from one fold step to the
+ * next (transcript position, step index, accumulator instances and their
+ * digit planes, the val lane's previous witness and commitment, Twist
+ * MemInits, the previous step's bus columns) as one byte string; buf == NULL
+ * only sets *len to its size (NEO_ERR_ARG when cap < *len).  A checkpoint
+ * restores into a shard created with the same CCS, m_in, k_rho and memory
+ * description, in any context or process (NEO_ERR_ARG otherwise, the shard
+ * unchanged); its next fold steps then equal the uninterrupted shard's bit
+ * for bit.  A serving loop evicts a shard's device state this way.  No
+ * counterpart in the reference, whose prover keeps this state in memory for
+ * the whole shard (crates/neo-fold/src/shard.rs:1725-2283). */
+int neo_gpu_shard_checkpoint(neo_gpu_shard* sh, uint8_t* buf, uint64_t cap, uint64_t* len);
+int neo_gpu_shard_restore(neo_gpu_shard* sh, const uint8_t* buf, uint64_t len);
 /* Replace the initial state of Twist instance mem_idx for the following fold
  * steps: the MemInit of the next step's MemInstance, which for a trace split
  * into chunks is the memory state at the end of the previous chunk

@@ -1643,3 +1643,212 @@ static int neo_gpu_shard_val_obligations_impl_abi(const neo_gpu_shard* sh, uint6
     return NEO_OK;
 }
 extern "C" int neo_gpu_shard_val_obligations(const neo_gpu_shard* sh, uint64_t* count) { NEO_ABI_GUARD(neo_gpu_shard_val_obligations_impl_abi(sh, count)) }
+
+// ------------------------------------------------------ checkpoint / resume --
+// The state a shard carries from one fold step to the next, as one byte
+// string: the transcript position, the step index, the accumulator (its ME
+// instances on the host and its digit planes, Zall slots 1..k), the val lane's
+// previous MCS witness, commitment and public input, its obligation count, the
+// Twist MemInits and the previous step's decoded bus columns (the rollover
+// claim).  Everything else a shard holds is either fixed at creation (CCS,
+// tables, buffers) or rebuilt every step (oracle workspaces).  A serving loop
+// evicts a shard's device state with it and restores it later, or resumes
+// after the process is restarted; the restored shard proves the next steps
+// exactly as the uninterrupted one would.
+namespace {
+constexpr uint64_t CKPT_MAGIC = 0x3154504B434F454EULL;  // "NEOCKPT1"
+constexpr uint64_t CKPT_VERSION = 1;
+
+// counts (dst == null) or writes the checkpoint
+struct CkptWriter {
+    uint8_t* dst = nullptr;
+    uint64_t n = 0;
+    neo_gpu_ctx* ctx = nullptr;
+    void put(const void* p, uint64_t bytes) {
+        if (dst && bytes) memcpy(dst + n, p, bytes);
+        n += bytes;
+    }
+    void u64(uint64_t v) { put(&v, 8); }
+    void u64s(const std::vector<uint64_t>& v) { u64(v.size()); put(v.data(), v.size() * 8); }
+    void ks(const std::vector<K>& v) { u64(v.size()); put(v.data(), v.size() * sizeof(K)); }
+    cudaError_t dev(const void* dptr, uint64_t bytes) {
+        u64(bytes);
+        cudaError_t e = cudaSuccess;
+        if (dst && bytes) e = cudaMemcpyAsync(dst + n, dptr, bytes, cudaMemcpyDeviceToHost, ctx->stream);
+        n += bytes;
+        return e;
+    }
+};
+
+struct CkptReader {
+    const uint8_t* p;
+    uint64_t left;
+    bool ok = true;
+    bool get(void* dst, uint64_t bytes) {
+        if (!ok || bytes > left) return ok = false;
+        if (bytes) memcpy(dst, p, bytes);
+        p += bytes;
+        left -= bytes;
+        return true;
+    }
+    uint64_t u64() {
+        uint64_t v = 0;
+        get(&v, 8);
+        return v;
+    }
+    template <typename T>
+    void vec(std::vector<T>& v) {
+        const uint64_t n = u64();
+        if (!ok || n > left / sizeof(T)) { ok = false; return; }
+        v.resize(n);
+        get(v.data(), n * sizeof(T));
+    }
+    // a device blob of exactly `bytes` (0 allowed when the shard has no such state yet)
+    const uint8_t* blob(uint64_t* bytes) {
+        *bytes = u64();
+        if (!ok || *bytes > left) { ok = false; return nullptr; }
+        const uint8_t* b = p;
+        p += *bytes;
+        left -= *bytes;
+        return b;
+    }
+};
+
+// header fields: the shard a checkpoint may be restored into
+void ckpt_header(const neo_gpu_shard* sh, uint64_t h[14]) {
+    h[0] = CKPT_MAGIC; h[1] = CKPT_VERSION; h[2] = sh->n; h[3] = sh->m; h[4] = sh->t; h[5] = sh->k_rho;
+    h[6] = sh->kappa; h[7] = sh->bus_cols; h[8] = sh->m_in; h[9] = sh->ell_n; h[10] = sh->shout.size();
+    h[11] = sh->twist.size(); h[12] = sh->steps; h[13] = sh->b;
+}
+
+int ckpt_write(neo_gpu_shard* sh, CkptWriter& w) {
+    neo_gpu_ctx* ctx = sh->ctx;
+    uint64_t h[14];
+    ckpt_header(sh, h);
+    for (uint64_t v : h) w.u64(v);
+    w.put(sh->mat_digest, 32);
+    uint64_t st[8], perms;
+    uint32_t absorbed;
+    sh->tr->save(st, &absorbed, &perms);
+    w.put(st, 64);
+    w.u64(absorbed);
+    w.u64(perms);
+    w.u64(sh->step_idx);
+    w.u64(sh->has_prev ? 1 : 0);
+    w.u64(sh->val_obligations);
+    w.u64(sh->acc.size());
+    for (const MeInst& me : sh->acc) {
+        w.u64s(me.c);
+        w.u64s(me.X);
+        w.ks(me.r);
+        w.ks(me.y);
+        w.ks(me.ysc);
+        w.u64(me.m_in);
+        w.put(me.digest, 32);
+    }
+    w.u64s(sh->prev_c);
+    w.u64s(sh->prev_X);
+    for (auto& ti : sh->twist) {
+        w.u64s(ti->init_addr);
+        w.u64s(ti->init_val);
+        w.put(ti->digest, 32);
+    }
+    const uint64_t plane = (uint64_t)NEO_D * sh->m;
+    NEO_CK(ctx, w.dev(sh->Zall.p + plane, sh->acc.size() * plane));
+    NEO_CK(ctx, w.dev(sh->valwit.p, sh->has_prev ? sh->valwit.bytes() : 0));
+    NEO_CK(ctx, w.dev(sh->d_prev_cols.p, sh->has_prev ? sh->d_prev_cols.bytes() : 0));
+    if (w.dst) NEO_CK(ctx, ctx_sync(ctx));
+    return NEO_OK;
+}
+}  // namespace
+
+static int neo_gpu_shard_checkpoint_impl_abi(neo_gpu_shard* sh, uint8_t* buf, uint64_t cap, uint64_t* len) {
+    if (!sh || !len) return NEO_ERR_ARG;
+    neo_gpu_ctx* ctx = sh->ctx;
+    cudaSetDevice(ctx->device);
+    CkptWriter count;
+    count.ctx = ctx;
+    int rc = ckpt_write(sh, count);
+    if (rc) return rc;
+    *len = count.n;
+    if (!buf) return NEO_OK;
+    if (cap < count.n) return ctx->fail(NEO_ERR_ARG, "shard_checkpoint: buffer too small (see *len)");
+    NEO_CK(ctx, ctx_sync(ctx));  // the last step's device work is part of the state
+    CkptWriter w;
+    w.dst = buf;
+    w.ctx = ctx;
+    return ckpt_write(sh, w);
+}
+extern "C" int neo_gpu_shard_checkpoint(neo_gpu_shard* sh, uint8_t* buf, uint64_t cap, uint64_t* len) { NEO_ABI_GUARD(neo_gpu_shard_checkpoint_impl_abi(sh, buf, cap, len)) }
+
+static int neo_gpu_shard_restore_impl_abi(neo_gpu_shard* sh, const uint8_t* buf, uint64_t len) {
+    if (!sh) return NEO_ERR_ARG;
+    neo_gpu_ctx* ctx = sh->ctx;
+    if (!buf) return ctx->fail(NEO_ERR_ARG, "shard_restore: null buffer");
+    cudaSetDevice(ctx->device);
+    CkptReader r{buf, len};
+    uint64_t want[14], got[14];
+    ckpt_header(sh, want);
+    for (auto& v : got) v = r.u64();
+    uint8_t dig[32];
+    r.get(dig, 32);
+    if (!r.ok || memcmp(got, want, sizeof want) || memcmp(dig, sh->mat_digest, 32))
+        return ctx->fail(NEO_ERR_ARG, "shard_restore: checkpoint of another shard shape, CCS or format");
+    uint64_t st[8];
+    r.get(st, 64);
+    const uint64_t absorbed = r.u64(), perms = r.u64(), step_idx = r.u64(), has_prev = r.u64(),
+                   val_obl = r.u64(), n_acc = r.u64();
+    if (!r.ok || n_acc > sh->k_rho || has_prev > 1 || step_idx > 0xFFFFFFFFull)
+        return ctx->fail(NEO_ERR_ARG, "shard_restore: malformed checkpoint");
+    std::vector<MeInst> acc(n_acc);
+    for (MeInst& me : acc) {
+        r.vec(me.c);
+        r.vec(me.X);
+        r.vec(me.r);
+        r.vec(me.y);
+        r.vec(me.ysc);
+        me.m_in = (uint32_t)r.u64();
+        r.get(me.digest, 32);
+        if (r.ok && (me.c.size() != (size_t)sh->kappa * NEO_D || me.r.size() != sh->ell_n))
+            return ctx->fail(NEO_ERR_ARG, "shard_restore: malformed accumulator instance");
+    }
+    std::vector<uint64_t> prev_c, prev_X;
+    r.vec(prev_c);
+    r.vec(prev_X);
+    std::vector<TwistInst> inits(sh->twist.size());
+    for (auto& ti : inits) {
+        r.vec(ti.init_addr);
+        r.vec(ti.init_val);
+        r.get(ti.digest, 32);
+        if (r.ok && ti.init_addr.size() != ti.init_val.size())
+            return ctx->fail(NEO_ERR_ARG, "shard_restore: malformed Twist init");
+    }
+    const uint64_t plane = (uint64_t)NEO_D * sh->m;
+    uint64_t zb, vb, pb;
+    const uint8_t* zsrc = r.blob(&zb);
+    const uint8_t* vsrc = r.blob(&vb);
+    const uint8_t* psrc = r.blob(&pb);
+    if (!r.ok || r.left || zb != n_acc * plane || vb != (has_prev ? sh->valwit.bytes() : 0) ||
+        pb != (has_prev ? sh->d_prev_cols.bytes() : 0))
+        return ctx->fail(NEO_ERR_ARG, "shard_restore: malformed checkpoint");
+    // everything validated: install
+    NEO_CK(ctx, ctx_sync(ctx));
+    if (zb) NEO_CK(ctx, cudaMemcpyAsync(sh->Zall.p + plane, zsrc, zb, cudaMemcpyHostToDevice, ctx->stream));
+    if (vb) NEO_CK(ctx, cudaMemcpyAsync(sh->valwit.p, vsrc, vb, cudaMemcpyHostToDevice, ctx->stream));
+    if (pb) NEO_CK(ctx, cudaMemcpyAsync(sh->d_prev_cols.p, psrc, pb, cudaMemcpyHostToDevice, ctx->stream));
+    NEO_CK(ctx, ctx_sync(ctx));
+    if (!sh->tr->restore(st, (uint32_t)absorbed, perms)) return ctx->fail(NEO_ERR_ARG, "shard_restore: bad transcript");
+    sh->step_idx = (uint32_t)step_idx;
+    sh->has_prev = has_prev != 0;
+    sh->val_obligations = val_obl;
+    sh->acc.swap(acc);
+    sh->prev_c.swap(prev_c);
+    sh->prev_X.swap(prev_X);
+    for (size_t i = 0; i < inits.size(); i++) {
+        sh->twist[i]->init_addr.swap(inits[i].init_addr);
+        sh->twist[i]->init_val.swap(inits[i].init_val);
+        memcpy(sh->twist[i]->digest, inits[i].digest, 32);
+    }
+    return NEO_OK;
+}
+extern "C" int neo_gpu_shard_restore(neo_gpu_shard* sh, const uint8_t* buf, uint64_t len) { NEO_ABI_GUARD(neo_gpu_shard_restore_impl_abi(sh, buf, len)) }

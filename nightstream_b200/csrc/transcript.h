@@ -73,6 +73,19 @@ class Transcript {
     void digest32(uint8_t out[32]);
     const uint64_t* state() const { return st_; }
     uint64_t permutations() const { return perms_; }
+    // the whole sponge position, for checkpointing a prover and resuming it
+    void save(uint64_t st[8], uint32_t* absorbed, uint64_t* perms) const {
+        memcpy(st, st_, sizeof st_);
+        *absorbed = (uint32_t)absorbed_;
+        *perms = perms_;
+    }
+    bool restore(const uint64_t st[8], uint32_t absorbed, uint64_t perms) {
+        if (absorbed > (uint32_t)RATE) return false;
+        memcpy(st_, st, sizeof st_);
+        absorbed_ = (int)absorbed;
+        perms_ = perms;
+        return true;
+    }
 
    private:
     void absorb_elem(uint64_t x);

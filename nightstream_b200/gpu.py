@@ -53,6 +53,8 @@ SIGNATURES = {
     "neo_gpu_shard_create": [P, P, U32, U32, ctypes.c_char_p, P],
     "neo_gpu_shard_create_mem": [P, P, U32, U32, ctypes.c_char_p, P, P],
     "neo_gpu_shard_val_obligations": [P, P],
+    "neo_gpu_shard_checkpoint": [P, P, U64, P],
+    "neo_gpu_shard_restore": [P, P, U64],
     "neo_gpu_shard_set_twist_init": [P, U32, U64, P, P],
     "neo_gpu_shard_fold_step": [P, P, P, U64, P],
     "neo_gpu_shard_fold_step_device": [P, ctypes.c_void_p, P],
@@ -534,6 +536,19 @@ class Shard:
         st = np.empty(8, np.uint64)
         self.ctx.check(self.ctx.lib.neo_gpu_shard_transcript_state(self.h, _p(st)))
         return st
+
+    def checkpoint(self) -> np.ndarray:
+        """The state carried to the next fold step, as bytes (neo_gpu_shard_checkpoint)."""
+        n = ctypes.c_uint64()
+        self.ctx.check(self.ctx.lib.neo_gpu_shard_checkpoint(self.h, None, 0, ctypes.byref(n)))
+        buf = np.empty(n.value, np.uint8)
+        self.ctx.check(self.ctx.lib.neo_gpu_shard_checkpoint(self.h, _p(buf), buf.size, ctypes.byref(n)))
+        return buf
+
+    def restore(self, buf: np.ndarray):
+        """Continue from a checkpoint of a shard with the same CCS, m_in, k_rho and memory."""
+        buf = np.ascontiguousarray(buf, np.uint8)
+        self.ctx.check(self.ctx.lib.neo_gpu_shard_restore(self.h, _p(buf), buf.size))
 
     def ccs_digest(self) -> np.ndarray:
         d = np.empty(4, np.uint64)
