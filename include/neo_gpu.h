@@ -28,7 +28,8 @@ enum {
     NEO_ERR_OOM = 2,        /* device allocation failed */
     NEO_ERR_INVARIANT = 3,  /* protocol invariant failed (reference: ProtocolError) */
     NEO_ERR_CUDA = 4,       /* CUDA runtime error */
-    NEO_ERR_UNSUPPORTED = 5 /* parameter outside what the kernels implement */
+    NEO_ERR_UNSUPPORTED = 5, /* parameter outside what the kernels implement */
+    NEO_ERR_CANCELLED = 6    /* a batched request cancelled by neo_gpu_batch_cancel */
 };
 
 typedef struct neo_gpu_ctx neo_gpu_ctx;
@@ -390,6 +391,10 @@ int neo_gpu_batch_job_info(neo_gpu_batch* b, uint64_t job_id, double* times3, ui
 /* The error message of a failed request (empty while it runs or after it
  * succeeded), NUL-terminated and truncated to cap bytes. */
 int neo_gpu_batch_job_error(neo_gpu_batch* b, uint64_t job_id, char* buf, uint64_t cap);
+/* Cancels a request: a queued one never starts, a running one stops before
+ * its next fold step (its device state is released); both finish with status
+ * -NEO_ERR_CANCELLED.  A finished request is left as it is. */
+int neo_gpu_batch_cancel(neo_gpu_batch* b, uint64_t job_id);
 uint64_t neo_gpu_batch_kernel_launches(const neo_gpu_batch* b);
 int neo_gpu_batch_destroy(neo_gpu_batch* b);
 

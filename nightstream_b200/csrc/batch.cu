@@ -17,6 +17,7 @@
 // whole device, so a worker freeing a finished shard would otherwise stall
 // every other worker's kernels.
 #include "internal.cuh"
+#include <algorithm>
 #include <atomic>
 #include <chrono>
 #include <condition_variable>
@@ -107,6 +108,7 @@ struct Job {
     neo_gpu_shard* shard = nullptr;
     uint32_t steps_done = 0;
     int status = 0;  // 0 pending/running, 1 done, <0 -(error code)
+    std::atomic<bool> cancel{false};  // checked by the worker before every fold step
     std::string error;
     bclock::time_point t_submit, t_admit, t_done;
     uint64_t tr_state[8] = {0};
@@ -189,6 +191,10 @@ static void run_job(neo_gpu_batch* b, Worker& w, Job* j) {
                     : neo_gpu_shard_create(w.ctx, &j->ccs->d, j->m_in, j->k_rho, j->label.c_str(), &j->shard);
         const uint64_t m = j->ccs->d.m;
         while (rc == NEO_OK && j->steps_done < j->n_steps) {
+            if (j->cancel.load(std::memory_order_relaxed)) {
+                rc = NEO_ERR_CANCELLED;
+                break;
+            }
             if (j->steps_done > 0 && j->steps_done < j->inits.size()) {
                 auto& st = j->inits[j->steps_done];
                 for (uint32_t i = 0; rc == NEO_OK && i < st.size(); i++)
@@ -201,7 +207,8 @@ static void run_job(neo_gpu_batch* b, Worker& w, Job* j) {
             rc = neo_gpu_shard_fold_step(j->shard, zs, nullptr, 0, &len);
             if (rc == NEO_OK) j->steps_done++;
         }
-        if (rc != NEO_OK) err = neo_gpu_last_error(w.ctx);
+        if (rc == NEO_ERR_CANCELLED) err = "cancelled";
+        else if (rc != NEO_OK) err = neo_gpu_last_error(w.ctx);
     } catch (const std::bad_alloc&) {  // the request fails, the worker and the engine go on
         rc = NEO_ERR_OOM;
         err = "host allocation failed";
@@ -375,6 +382,27 @@ static int neo_gpu_batch_job_error_impl_abi(neo_gpu_batch* b, uint64_t job_id, c
     return NEO_OK;
 }
 extern "C" int neo_gpu_batch_job_error(neo_gpu_batch* b, uint64_t job_id, char* buf, uint64_t cap) { NEO_ABI_GUARD(neo_gpu_batch_job_error_impl_abi(b, job_id, buf, cap)) }
+
+static int neo_gpu_batch_cancel_impl_abi(neo_gpu_batch* b, uint64_t job_id) {
+    if (!b) return NEO_ERR_ARG;
+    std::lock_guard<std::mutex> lk(b->mu);
+    if (job_id >= b->jobs.size()) return NEO_ERR_ARG;
+    Job* j = b->jobs[job_id].get();
+    auto it = std::find(b->pending.begin(), b->pending.end(), j);
+    if (it != b->pending.end()) {  // queued: finish it here, it never reaches a worker
+        b->pending.erase(it);
+        j->status = -NEO_ERR_CANCELLED;
+        j->error = "cancelled";
+        j->t_admit = j->t_done = bclock::now();
+        b->unfinished--;
+        b->cv_work.notify_all();  // the new head of the queue may fit now
+        b->cv_done.notify_all();
+    } else if (j->status == 0) {
+        j->cancel.store(true, std::memory_order_relaxed);  // running: stops before its next step
+    }
+    return NEO_OK;
+}
+extern "C" int neo_gpu_batch_cancel(neo_gpu_batch* b, uint64_t job_id) { NEO_ABI_GUARD(neo_gpu_batch_cancel_impl_abi(b, job_id)) }
 
 static int neo_gpu_batch_destroy_impl_abi(neo_gpu_batch* b) {
     if (!b) return NEO_ERR_ARG;

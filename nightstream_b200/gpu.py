@@ -20,7 +20,8 @@ U64 = ctypes.c_uint64
 I = ctypes.c_int
 
 NEO_OK = 0
-_ERRS = {1: "NEO_ERR_ARG", 2: "NEO_ERR_OOM", 3: "NEO_ERR_INVARIANT", 4: "NEO_ERR_CUDA", 5: "NEO_ERR_UNSUPPORTED"}
+_ERRS = {1: "NEO_ERR_ARG", 2: "NEO_ERR_OOM", 3: "NEO_ERR_INVARIANT", 4: "NEO_ERR_CUDA", 5: "NEO_ERR_UNSUPPORTED",
+         6: "NEO_ERR_CANCELLED"}
 
 # symbol -> argtypes; every function returns int unless listed in _RESTYPES
 SIGNATURES = {
@@ -69,6 +70,7 @@ SIGNATURES = {
     "neo_gpu_batch_submit_mem": [P, P, P, P, U32, U32, U32, ctypes.c_char_p, P],
     "neo_gpu_batch_job_info": [P, U64, P, P, P],
     "neo_gpu_batch_job_error": [P, U64, P, U64],
+    "neo_gpu_batch_cancel": [P, U64],
     "neo_gpu_batch_kernel_launches": [P],
     "neo_gpu_batch_destroy": [P],
     "neo_transcript_new": [ctypes.c_char_p, P],
@@ -625,7 +627,8 @@ def ccs_digest(ccs) -> np.ndarray:
 
 class Batch:
     """Many shard-prove requests on one GPU (neo_gpu_batch): n_workers host
-    threads, one CUDA stream each, HBM-based admission, round-robin fold steps."""
+    threads, one CUDA stream each; requests leave one FIFO queue when their
+    device footprint fits the HBM budget and are proven to completion."""
 
     def __init__(self, device: int = 0, n_workers: int = 8, reserve_bytes: int = None):
         self.lib = load()
@@ -678,6 +681,12 @@ class Batch:
         if rc:
             raise NeoGpuError(rc, "batch submit")
         return jid.value
+
+    def cancel(self, jid: int):
+        """A queued request never starts; a running one stops before its next step."""
+        rc = self.lib.neo_gpu_batch_cancel(self.h, jid)
+        if rc:
+            raise NeoGpuError(rc, "batch cancel")
 
     def wait_all(self, timeout_s: float = 3600.0):
         rc = self.lib.neo_gpu_batch_wait_all(self.h, timeout_s * 1e3)

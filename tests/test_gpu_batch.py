@@ -106,3 +106,36 @@ def test_batch_trace_chunks_equal_oracle(ctx):
         assert np.array_equal(info["transcript_state"], expect[i]), f"chunked memory shard {i}"
     assert np.array_equal(mix.job_info(jm)["transcript_state"], expect_main)
     mix.close()
+
+
+def test_batch_cancel_queued_and_running(ctx):
+    """neo_gpu_batch_cancel: queued requests never start, a running one stops
+    before its next fold step; all three end with NEO_ERR_CANCELLED while the
+    other requests complete in their solo transcript states."""
+    import time
+    ell = 10
+    ccs, z = synth.make_r1cs(ell, 700)
+    ctx.pp_upload(np.random.default_rng(3000 + ell).integers(0, Q, size=(16, 1 << ell, 54), dtype=np.uint64))
+    b = gpu.Batch(0, n_workers=1)
+    long_id = b.submit(ccs, z, 200, app_label=b"neo/cancel-long")  # seconds of work, runs first
+    ids = [b.submit(ccs, z, 2, app_label=b"neo/cancel-%d" % i) for i in range(4)]
+    b.cancel(ids[1])
+    b.cancel(ids[3])
+    time.sleep(0.3)
+    b.cancel(long_id)
+    t0 = time.perf_counter()
+    b.wait_all(600)
+    assert time.perf_counter() - t0 < 60  # far less than the 200 steps would take
+    info = {j: b.job_info(j) for j in [long_id] + ids}
+    for j in (long_id, ids[1], ids[3]):
+        assert info[j]["status"] == -6 and info[j]["error"] == "cancelled", (j, info[j]["status"])
+    assert info[ids[0]]["status"] == 1 and info[ids[2]]["status"] == 1
+    b.cancel(ids[0])  # finished: left as it is
+    assert b.job_info(ids[0])["status"] == 1
+    b.close()
+    solo = gpu.Batch(0, n_workers=1)
+    sids = [solo.submit(ccs, z, 2, app_label=b"neo/cancel-%d" % i) for i in (0, 2)]
+    solo.wait_all(600)
+    for sid, i in zip(sids, (0, 2)):
+        assert np.array_equal(solo.job_info(sid)["transcript_state"], info[ids[i]]["transcript_state"])
+    solo.close()
