@@ -192,30 +192,52 @@ extern "C" int neo_gpu_decomp_b2(neo_gpu_ctx* ctx, const uint64_t* z, uint64_t m
 // Pi_RLC mix: Z_mix[:, c] = sum_i a_i(X) z_{i,c}(X) mod Phi_81 over the
 // integers (all entries are small, so this equals the F_q computation of
 // optimized_engine/common.rs:1221-1379 with rot_from_coeffs common.rs:398-430).
-// One thread per column; rot matrices live in shared memory as int8.
+// Zmix = [rot_1 .. rot_k] (54 x 54k) times the stacked digit planes
+// (54k x m), exact in int32.  Each thread owns one column and RPT of the 54
+// output rows (small m uses fewer rows per thread so the grid still covers
+// the SMs).  Per input it issues the column's 54 digit loads together (one
+// memory latency per input instead of one per digit), packs them four to a
+// word and multiplies with dp4a against the rot rows, which sit in shared
+// memory as int8 rows padded to RLC_ROT_ROW = 64 bytes (zeros past k = 54)
+// and are read 16 bytes at a time.  Any split gives the same Zmix.
 // ---------------------------------------------------------------------------
+template <int RPT>
 __global__ void __launch_bounds__(128) rlc_mix_kernel(const int8_t* __restrict__ rot, const int8_t* __restrict__ Zs,
                                                       uint32_t count, uint64_t m, int32_t* __restrict__ Zmix) {
-    extern __shared__ int8_t s_rot[];  // [count][54][54] row-major rot(a_i)[r][k]
-    for (uint32_t x = threadIdx.x; x < count * NEO_D * NEO_D; x += blockDim.x) s_rot[x] = rot[x];
+    extern __shared__ int4 s_rot[];  // [count][54][64 B]
+    const uint32_t n16 = count * NEO_D * (RLC_ROT_ROW / 16);
+    const int4* g = reinterpret_cast<const int4*>(rot);
+    for (uint32_t x = threadIdx.x; x < n16; x += blockDim.x) s_rot[x] = g[x];
     __syncthreads();
-    uint64_t c = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+    const uint64_t c = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+    const int r0 = blockIdx.y * RPT;
     if (c >= m) return;
-    int32_t acc[NEO_D];
+    int32_t acc[RPT];
 #pragma unroll
-    for (int r = 0; r < NEO_D; r++) acc[r] = 0;
+    for (int r = 0; r < RPT; r++) acc[r] = 0;
     for (uint32_t i = 0; i < count; i++) {
-        const int8_t* Zi = Zs + (uint64_t)i * NEO_D * m;
-        const int8_t* R = s_rot + i * NEO_D * NEO_D;
-        for (int k = 0; k < NEO_D; k++) {
-            int z = Zi[(uint64_t)k * m + c];
-            if (z == 0) continue;
+        const int8_t* Zi = Zs + (uint64_t)i * NEO_D * m + c;
+        uint32_t zb[NEO_D];
 #pragma unroll
-            for (int r = 0; r < NEO_D; r++) acc[r] += z * (int)R[r * NEO_D + k];
+        for (int k = 0; k < NEO_D; k++) zb[k] = (uint8_t)Zi[(uint64_t)k * m];
+        int w[14];  // bytes 4j..4j+3 of the column (k = 54, 55 are zero)
+#pragma unroll
+        for (int j = 0; j < 13; j++) w[j] = (int)(zb[4 * j] | (zb[4 * j + 1] << 8) | (zb[4 * j + 2] << 16) | (zb[4 * j + 3] << 24));
+        w[13] = (int)(zb[52] | (zb[53] << 8));
+        const int4* R = s_rot + ((uint64_t)i * NEO_D + r0) * (RLC_ROT_ROW / 16);
+#pragma unroll
+        for (int r = 0; r < RPT; r++) {
+            const int4 q0 = R[4 * r], q1 = R[4 * r + 1], q2 = R[4 * r + 2], q3 = R[4 * r + 3];
+            int a = acc[r];
+            a = __dp4a(w[0], q0.x, a); a = __dp4a(w[1], q0.y, a); a = __dp4a(w[2], q0.z, a); a = __dp4a(w[3], q0.w, a);
+            a = __dp4a(w[4], q1.x, a); a = __dp4a(w[5], q1.y, a); a = __dp4a(w[6], q1.z, a); a = __dp4a(w[7], q1.w, a);
+            a = __dp4a(w[8], q2.x, a); a = __dp4a(w[9], q2.y, a); a = __dp4a(w[10], q2.z, a); a = __dp4a(w[11], q2.w, a);
+            a = __dp4a(w[12], q3.x, a); a = __dp4a(w[13], q3.y, a);  // q3.z, q3.w: the row's zero padding
+            acc[r] = a;
         }
     }
 #pragma unroll
-    for (int r = 0; r < NEO_D; r++) Zmix[(uint64_t)r * m + c] = acc[r];
+    for (int r = 0; r < RPT; r++) Zmix[(uint64_t)(r0 + r) * m + c] = acc[r];
 }
 
 // integer rot(a): column t = a X^t mod Phi_81 (commit.rs:46-54 recurrence)
@@ -246,13 +268,28 @@ int rlc_mix_device(neo_gpu_ctx* ctx, const int8_t* rho_coeffs_host, const int8_t
             rot_int8(rho_coeffs_host + i * NEO_D, rot.data() + (size_t)i * NEO_D * NEO_D);
         }
     }
-    NEO_CK(ctx, cudaMemcpyAsync(d_rot_scratch, rot.data(), rot.size(), cudaMemcpyHostToDevice, ctx->stream));
-    size_t smem = rot.size();
-    static SmemLimit limit;
-    if (smem > 48 * 1024) NEO_CK(ctx, limit.at_least(rlc_mix_kernel, smem));
-    rlc_mix_kernel<<<ceil_div(m, 128), 128, smem, ctx->stream>>>(d_rot_scratch, d_Zs, count, m, d_Zmix);
-    NEO_LAUNCHED(ctx);
-    return NEO_OK;
+    // rows padded to RLC_ROT_ROW bytes for the kernel's 16-byte shared loads
+    std::vector<int8_t> rot_pad((size_t)count * NEO_D * RLC_ROT_ROW, 0);
+    for (size_t row = 0; row < (size_t)count * NEO_D; row++)
+        memcpy(&rot_pad[row * RLC_ROT_ROW], &rot[row * NEO_D], NEO_D);
+    NEO_CK(ctx, cudaMemcpyAsync(d_rot_scratch, rot_pad.data(), rot_pad.size(), cudaMemcpyHostToDevice, ctx->stream));
+    NEO_CK(ctx, ctx_sync(ctx));  // rot_pad is pageable host memory that goes away on return
+    size_t smem = rot_pad.size();
+    // rows per thread: the most that still gives two waves of blocks over the SMs
+    const unsigned col_blocks = ceil_div(m, 128);
+    auto launch = [&](auto kernel, int rpt) -> int {
+        static SmemLimit limit[4];
+        SmemLimit& l = limit[rpt == 54 ? 0 : rpt == 18 ? 1 : rpt == 6 ? 2 : 3];
+        if (smem > 48 * 1024) NEO_CK(ctx, l.at_least(kernel, smem));
+        kernel<<<dim3(col_blocks, NEO_D / rpt), 128, smem, ctx->stream>>>(d_rot_scratch, d_Zs, count, m, d_Zmix);
+        NEO_LAUNCHED(ctx);
+        return NEO_OK;
+    };
+    const unsigned want = 2 * 148;
+    if (col_blocks >= want) return launch(rlc_mix_kernel<54>, 54);
+    if (col_blocks * 3 >= want) return launch(rlc_mix_kernel<18>, 18);
+    if (col_blocks * 9 >= want) return launch(rlc_mix_kernel<6>, 6);
+    return launch(rlc_mix_kernel<1>, 1);
 }
 
 static int neo_gpu_rlc_mix_impl_abi(neo_gpu_ctx* ctx, const int8_t* rho_coeffs, const int8_t* Zs, uint32_t count,
@@ -263,7 +300,7 @@ static int neo_gpu_rlc_mix_impl_abi(neo_gpu_ctx* ctx, const int8_t* rho_coeffs, 
     DevBuf<int8_t> dZs, drot;
     DevBuf<int32_t> dmix;
     NEO_CK(ctx, dZs.alloc((size_t)count * NEO_D * m));
-    NEO_CK(ctx, drot.alloc((size_t)count * NEO_D * NEO_D));
+    NEO_CK(ctx, drot.alloc((size_t)count * NEO_D * RLC_ROT_ROW));
     NEO_CK(ctx, dmix.alloc((size_t)NEO_D * m));
     NEO_CK(ctx, cudaMemcpyAsync(dZs.p, Zs, dZs.bytes(), cudaMemcpyHostToDevice, ctx->stream));
     int rc = rlc_mix_device(ctx, rho_coeffs, dZs.p, count, m, dmix.p, drot.p);

@@ -21,6 +21,7 @@
 // (the tail of z: cell (col, j) at bus_base + col * steps + j, time row
 // m_in + j) are decoded into dense K time columns d_cols[bus_cols][2^ell_n].
 #include <future>
+#include <nvtx3/nvToolsExt.h>
 #include "internal.cuh"
 
 #include <list>
@@ -76,24 +77,56 @@ static std::vector<uint8_t> le64(uint64_t v) {
 
 // out[v][r] = sum_i rot_i[r][k] * V_i[v][k]  over F_q, element stride `stride`
 // (Commitment mixing mix_rhos_commits and S-action on y vectors, common.rs:398-430).
-__global__ void rot_mix_kernel(const int8_t* __restrict__ rot, uint32_t count, const uint64_t* __restrict__ V,
-                               uint32_t nv, uint32_t stride, uint64_t* __restrict__ out) {
+// rot rows are RLC_ROT_ROW bytes apart (the RLC mix scratch).  A block
+// (64 x 16 threads) owns one output vector: thread (r, i) forms
+// sum_k rot_i[r][k] V_i[v][k] for 16 inputs at a time.  rot entries are small
+// integers, so the terms are summed exactly in 128 bits (positive and negative
+// coefficients apart) and reduced once; the per-input partials are then
+// added mod q in shared memory.
+__global__ void __launch_bounds__(1024) rot_mix_kernel(const int8_t* __restrict__ rot, uint32_t count,
+                                                       const uint64_t* __restrict__ V, uint32_t nv, uint32_t stride,
+                                                       uint64_t* __restrict__ out) {
+    __shared__ uint64_t xs[16][NEO_D];
+    __shared__ uint64_t part[16][NEO_D];
     const uint32_t v = blockIdx.x / stride, comp = blockIdx.x % stride;
-    const int r = threadIdx.x;
-    if (r >= NEO_D) return;
-    uint64_t acc = 0;
-    for (uint32_t i = 0; i < count; i++) {
-        const int8_t* R = rot + (size_t)i * NEO_D * NEO_D + r * NEO_D;
-        const uint64_t* x = V + (((size_t)i * nv + v) * NEO_D) * stride + comp;
-        for (int k = 0; k < NEO_D; k++) {
-            int c = R[k];
-            if (c == 0) continue;
-            uint64_t xv = x[(size_t)k * stride];
-            uint64_t p = c > 0 ? gl::mul_small(xv, (uint32_t)c) : gl::neg(gl::mul_small(xv, (uint32_t)(-c)));
-            acc = gl::add(acc, p);
+    const int r = threadIdx.x, ii = threadIdx.y;
+    const bool row = r < NEO_D;
+    uint64_t total = 0;
+    for (uint32_t i0 = 0; i0 < count; i0 += 16) {
+        const uint32_t i = i0 + ii;
+        const bool live = row && i < count;
+        if (live) xs[ii][r] = V[(((size_t)i * nv + v) * NEO_D + r) * stride + comp];
+        __syncthreads();
+        if (live) {
+            const int4* R4 = reinterpret_cast<const int4*>(rot + ((size_t)i * NEO_D + r) * RLC_ROT_ROW);
+            const int4 q[4] = {R4[0], R4[1], R4[2], R4[3]};
+            uint64_t pl = 0, ph = 0, nl = 0, nh = 0;  // < 54 * 4 * 2^64 < 2^72 each
+#pragma unroll
+            for (int k = 0; k < NEO_D; k++) {
+                const int4& w4 = q[k >> 4];
+                const int w = ((k >> 2) & 3) == 0 ? w4.x : ((k >> 2) & 3) == 1 ? w4.y : ((k >> 2) & 3) == 2 ? w4.z : w4.w;
+                const int c = (int)(int8_t)(w >> (8 * (k & 3)));
+                const uint64_t x = xs[ii][k];
+                const uint64_t a = (uint64_t)(c < 0 ? -c : c);
+                const uint64_t lo = x * a, hi = __umul64hi(x, a);
+                if (c > 0) {
+                    pl += lo;
+                    ph += hi + (pl < lo);
+                } else if (c < 0) {
+                    nl += lo;
+                    nh += hi + (nl < lo);
+                }
+            }
+            part[ii][r] = gl::sub(gl::reduce128(pl, ph), gl::reduce128(nl, nh));
+        } else if (row) {
+            part[ii][r] = 0;
         }
+        __syncthreads();
+        if (ii == 0 && row)
+            for (int j = 0; j < 16; j++) total = gl::add(total, part[j][r]);
+        __syncthreads();
     }
-    out[((size_t)v * NEO_D + r) * stride + comp] = acc;
+    if (ii == 0 && row) out[((size_t)v * NEO_D + r) * stride + comp] = total;
 }
 
 // child ME claims: y[w][j][rho] = sum_c P_w[rho][c] v_j[c] (zv_dot in core.cu uses the same math)
@@ -231,6 +264,44 @@ using hclock = std::chrono::steady_clock;
 static inline double ms_since(hclock::time_point t0) {
     return std::chrono::duration<double, std::milli>(hclock::now() - t0).count();
 }
+
+// NVTX ranges name a fold step and its phases (witness, bind, ccs_build,
+// time_rounds, ajtai_rounds, me_outputs, rlc_dec, val_lane) in the NVTX domain
+// "neo", for profilers: nsys timelines, ncu --nvtx --nvtx-include
+// "neo@fold_step/rlc_dec/".  With no tool attached a push or pop is one call
+// that returns.  Ranges still open when the step returns (an error path) are
+// closed here, so the thread's range stack stays balanced.
+namespace {
+nvtxDomainHandle_t nvtx_domain() {
+    static nvtxDomainHandle_t d = nvtxDomainCreateA("neo");
+    return d;
+}
+struct NvtxStep {
+    int depth = 0;
+    void push(const char* name) {
+        nvtxEventAttributes_t a = {};
+        a.version = NVTX_VERSION;
+        a.size = NVTX_EVENT_ATTRIB_STRUCT_SIZE;
+        a.messageType = NVTX_MESSAGE_TYPE_ASCII;
+        a.message.ascii = name;
+        nvtxDomainRangePushEx(nvtx_domain(), &a);
+        depth++;
+    }
+    void next(const char* name) {
+        pop();
+        push(name);
+    }
+    void pop() {
+        if (depth) {
+            nvtxDomainRangePop(nvtx_domain());
+            depth--;
+        }
+    }
+    ~NvtxStep() {
+        while (depth) pop();
+    }
+};
+}  // namespace
 
 static void header_params(neo_gpu_shard* sh) {
     // goldilocks_auto_r1cs_ccs (crates/neo-params/src/lib.rs:181-222) with
@@ -544,7 +615,7 @@ static int shard_create_impl(neo_gpu_ctx* ctx, const neo_ccs_desc* desc, uint32_
     NEO_CK(ctx, sh->Zall.alloc((size_t)(1 + k_rho) * NEO_D * m));
     NEO_CK(ctx, sh->d_z.alloc(m));
     NEO_CK(ctx, sh->d_mix.alloc((size_t)NEO_D * m));
-    NEO_CK(ctx, sh->d_rot.alloc((size_t)(1 + k_rho) * NEO_D * NEO_D));
+    NEO_CK(ctx, sh->d_rot.alloc((size_t)(1 + k_rho) * NEO_D * RLC_ROT_ROW));
     NEO_CK(ctx, sh->d_commits.alloc((size_t)(1 + k_rho) * sh->kappa * NEO_D));
     NEO_CK(ctx, sh->d_flags.alloc(2));
     NEO_CK(ctx, sh->d_ychild.alloc((size_t)k_rho * sh->t * NEO_D));
@@ -873,7 +944,7 @@ static int rlc_dec_lane(neo_gpu_shard* sh, const char* lane, uint32_t idx, const
         std::vector<uint64_t> cv((size_t)k * kappa * NEO_D);
         for (uint32_t i = 0; i < k; i++) memcpy(&cv[(size_t)i * kappa * NEO_D], ins[i].c.data(), kappa * NEO_D * 8);
         NEO_CK(ctx, cudaMemcpyAsync(sh->d_mixv.p, cv.data(), cv.size() * 8, cudaMemcpyHostToDevice, ctx->stream));
-        rot_mix_kernel<<<kappa, 64, 0, ctx->stream>>>(sh->d_rot.p, k, sh->d_mixv.p, kappa, 1, sh->d_mixo.p);
+        rot_mix_kernel<<<kappa, dim3(64, 16), 0, ctx->stream>>>(sh->d_rot.p, k, sh->d_mixv.p, kappa, 1, sh->d_mixo.p);
         NEO_LAUNCHED(ctx);
         NEO_CK(ctx, ctx_d2h(ctx, c_parent.data(), sh->d_mixo.p, c_parent.size() * 8));
         NEO_CK(ctx, ctx_sync(ctx));
@@ -883,7 +954,7 @@ static int rlc_dec_lane(neo_gpu_shard* sh, const char* lane, uint32_t idx, const
                 for (int rho = 0; rho < NEO_D; rho++) yv[((size_t)i * t + j) * NEO_D + rho] = ins[i].y[(size_t)j * d_pad + rho];
         // y vectors as [k][t][54] K = stride-2 F_q
         NEO_CK(ctx, cudaMemcpyAsync(sh->d_mixv.p, yv.data(), yv.size() * 16, cudaMemcpyHostToDevice, ctx->stream));
-        rot_mix_kernel<<<t * 2, 64, 0, ctx->stream>>>(sh->d_rot.p, k, sh->d_mixv.p, t, 2, sh->d_mixo.p);
+        rot_mix_kernel<<<t * 2, dim3(64, 16), 0, ctx->stream>>>(sh->d_rot.p, k, sh->d_mixv.p, t, 2, sh->d_mixo.p);
         NEO_LAUNCHED(ctx);
         NEO_CK(ctx, ctx_d2h(ctx, y_parent.data(), sh->d_mixo.p, y_parent.size() * 16));
         NEO_CK(ctx, ctx_sync(ctx));
@@ -983,6 +1054,9 @@ static int fold_step_impl(neo_gpu_shard* sh, const uint64_t* z_host, const uint6
     P.clear();
     int rc;
     const auto t_step = hclock::now();
+    NvtxStep nv;
+    nv.push("fold_step");
+    nv.push("witness");
     const uint64_t perms0 = tr.permutations();
     for (double& v : sh->stats) v = 0;
     auto t_ph = hclock::now();
@@ -1017,6 +1091,7 @@ static int fold_step_impl(neo_gpu_shard* sh, const uint64_t* z_host, const uint6
     for (size_t i = 0; i < Xd.size(); i++) mcs.X[i] = gl::from_i64(Xd[i]);
     P.insert(P.end(), mcs.c.begin(), mcs.c.end());
     sh->stats[1] = ms_since(t_ph);
+    nv.next("bind");
     t_ph = hclock::now();
 
     // ---- absorb_step_memory_witness (memory_sidecar/memory.rs:86-124) ----
@@ -1141,6 +1216,7 @@ static int fold_step_impl(neo_gpu_shard* sh, const uint64_t* z_host, const uint6
     std::vector<K> r_cycle = sample_ext_point(tr, "route_a/r_cycle", "route_a/cycle/0", "route_a/cycle/1", ell_n);
 
     sh->stats[2] = ms_since(t_ph);
+    nv.next("ccs_build");
     t_ph = hclock::now();
     // ---- Pi_CCS oracle over Zall slots 0..n_acc (workspace reused across steps) ----
     const K* rin = n_acc ? sh->acc[0].r.data() : nullptr;
@@ -1149,6 +1225,7 @@ static int fold_step_impl(neo_gpu_shard* sh, const uint64_t* z_host, const uint6
         return rc;
     neo_gpu_ccs_oracle* orc = sh->orc;
     sh->stats[3] = ms_since(t_ph);
+    nv.next("time_rounds");
     t_ph = hclock::now();
 
     // memory oracles are rebuilt every step into the shard's slots (device buffers kept)
@@ -1361,6 +1438,7 @@ static int fold_step_impl(neo_gpu_shard* sh, const uint64_t* z_host, const uint6
     if ((rc = run_batched_ds(sh, "shard/batched_time", idx, claims, ell_n, r_time, finals, P))) return rc;
     K running = finals[0];
     sh->stats[4] = ms_since(t_ph);
+    nv.next("ajtai_rounds");
     t_ph = hclock::now();
     // ---- Ajtai rounds: run_sumcheck_prover_ds("ccs/ajtai") ----
     auto bidx = le64(idx);
@@ -1389,6 +1467,7 @@ static int fold_step_impl(neo_gpu_shard* sh, const uint64_t* z_host, const uint6
     tr.digest32(fold_digest);
 
     sh->stats[5] = ms_since(t_ph);
+    nv.next("me_outputs");
     t_ph = hclock::now();
     // ---- ME outputs (oracle.rs:1955-2072) + bus openings at r_time (cpu_bus.rs:195-320) ----
     std::vector<K> y_eval((size_t)k * t * NEO_D), y_sc((size_t)k * t);
@@ -1426,6 +1505,7 @@ static int fold_step_impl(neo_gpu_shard* sh, const uint64_t* z_host, const uint6
         for (uint32_t c = 0; c < nb; c++) push_k(P, outs[i].ysc[t + c]);
     }
     sh->stats[6] = ms_since(t_ph);
+    nv.next("rlc_dec");
     t_ph = hclock::now();
 
     // ---- finalize_route_a_memory_prover (memory.rs:1284-1670): Twist val-eval batch + CPU ME claims at r_val ----
@@ -1536,6 +1616,7 @@ static int fold_step_impl(neo_gpu_shard* sh, const uint64_t* z_host, const uint6
                            children, P)))
         return rc;
     sh->stats[7] = ms_since(t_ph);
+    nv.next("val_lane");
     t_ph = hclock::now();
     // ---- val lane (shard.rs:2195-2252) ----
     if (!val_claims.empty()) {
@@ -1562,6 +1643,7 @@ static int fold_step_impl(neo_gpu_shard* sh, const uint64_t* z_host, const uint6
     }
     sh->step_idx++;
     sh->stats[8] = ms_since(t_ph);
+    nv.pop();
     sh->stats[10] = mem_ms;
     sh->stats[0] = ms_since(t_step);
     sh->stats[9] = (double)(tr.permutations() - perms0);

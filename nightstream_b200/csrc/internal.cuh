@@ -12,6 +12,8 @@
 #include "gl.cuh"
 
 #define NEO_D 54
+// bytes per rot(a) row in the RLC mix scratch: 54 int8 entries, zero padded
+constexpr int RLC_ROT_ROW = 64;
 
 struct neo_gpu_ctx {
     int device = 0;

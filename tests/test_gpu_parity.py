@@ -70,6 +70,18 @@ def test_rlc_mix_and_split_match_oracle(ctx):
     assert np.array_equal(ctx.rlc_mix(rho[:1], Zs[:1]), Zs[0].astype(np.int32))
 
 
+@pytest.mark.parametrize("count,m,wide", [(13, 100, False), (13, 1024, False), (2, 1024, True), (13, 8192, False), (13, 16384, False),
+                                          (13, 65536, False), (3, 65536, True)])
+def test_rlc_mix_every_grid_shape(ctx, count, m, wide):
+    """The mix splits a column's 54 output rows over 1, 3, 9 or 54 threads
+    depending on m (ragged m included); every shape equals the oracle, also
+    for digits outside {-1, 0, 1}."""
+    rng = np.random.default_rng(m + count)
+    rho = rng.integers(-2, 3, size=(count, 54)).astype(np.int8)
+    Zs = rng.integers(-7 if wide else -1, 8 if wide else 2, size=(count, 54, m)).astype(np.int8)
+    assert np.array_equal(ctx.rlc_mix(rho, Zs), O.rlc_mix(rho, Zs))
+
+
 def test_split_out_of_range_is_an_error(ctx):
     from nightstream_b200.gpu import NeoGpuError
     with pytest.raises(NeoGpuError) as e:
