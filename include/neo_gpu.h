@@ -56,6 +56,13 @@ typedef struct neo_ccs_desc {
 int neo_gpu_ctx_create(int device, neo_gpu_ctx** out);
 int neo_gpu_ctx_destroy(neo_gpu_ctx* ctx);
 const char* neo_gpu_last_error(const neo_gpu_ctx* ctx);
+/* Bounded device wait (health check and test of the failure path): a kernel
+ * polls a device flag at most spin_limit times (about 1 us apart, spin_limit
+ * <= 2^20); set_flag != 0 sets the flag first.  NEO_OK when the flag was
+ * seen; NEO_ERR_CUDA ("device wait timed out") when the wait ran out, with
+ * the context left usable -- the same path the commitment kernel's bounded
+ * mbarrier waits report through. */
+int neo_gpu_wait_probe(neo_gpu_ctx* ctx, uint32_t set_flag, uint32_t spin_limit);
 /* Number of kernels this context has launched so far (instrumentation). */
 uint64_t neo_gpu_kernel_launches(const neo_gpu_ctx* ctx);
 /* The context's CUDA stream (a cudaStream_t), for event timing by callers. */

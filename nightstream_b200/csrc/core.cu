@@ -59,6 +59,32 @@ int check_device_error(neo_gpu_ctx* ctx) {
     return NEO_OK;
 }
 
+// Bounded device wait: one thread polls *flag up to `limit` times (about
+// 1 us apart); a wait that runs out sets bit 0x10 of the context's error word
+// and returns, like the commitment kernel's bounded mbarrier waits.
+__global__ void wait_flag_kernel(const volatile uint32_t* flag, uint32_t limit, uint32_t* err) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    for (uint32_t it = 0; it < limit; it++) {
+        if (*flag) return;
+        __nanosleep(1000);
+    }
+    atomicOr(err, 0x10u);
+}
+
+static int neo_gpu_wait_probe_impl_abi(neo_gpu_ctx* ctx, uint32_t set_flag, uint32_t spin_limit) {
+    if (!ctx) return NEO_ERR_ARG;
+    if (spin_limit == 0 || spin_limit > (1u << 20)) return ctx->fail(NEO_ERR_ARG, "wait_probe: spin_limit in [1, 2^20]");
+    cudaSetDevice(ctx->device);
+    DevBuf<uint32_t> flag;
+    NEO_CK(ctx, flag.alloc(1));
+    NEO_CK(ctx, cudaMemsetAsync(flag.p, 0, 4, ctx->stream));
+    if (set_flag) NEO_CK(ctx, cudaMemsetAsync(flag.p, 0xFF, 4, ctx->stream));
+    wait_flag_kernel<<<1, 32, 0, ctx->stream>>>(flag.p, spin_limit, ctx->d_err);
+    NEO_LAUNCHED(ctx);
+    return check_device_error(ctx);  // synchronizes; a timeout is reported and cleared
+}
+extern "C" int neo_gpu_wait_probe(neo_gpu_ctx* ctx, uint32_t set_flag, uint32_t spin_limit) { NEO_ABI_GUARD(neo_gpu_wait_probe_impl_abi(ctx, set_flag, spin_limit)) }
+
 static int neo_gpu_ctx_stream_impl_abi(const neo_gpu_ctx* ctx, void** stream) {
     if (!ctx || !stream) return NEO_ERR_ARG;
     *stream = (void*)ctx->stream;

@@ -71,6 +71,7 @@ SIGNATURES = {
     "neo_gpu_batch_job_info": [P, U64, P, P, P],
     "neo_gpu_batch_job_error": [P, U64, P, U64],
     "neo_gpu_batch_cancel": [P, U64],
+    "neo_gpu_wait_probe": [P, U32, U32],
     "neo_gpu_batch_kernel_launches": [P],
     "neo_gpu_batch_destroy": [P],
     "neo_transcript_new": [ctypes.c_char_p, P],
@@ -174,6 +175,11 @@ class Context:
 
     def synchronize(self):
         self.check(self.lib.neo_gpu_synchronize(self.h))
+
+    def wait_probe(self, set_flag: bool, spin_limit: int = 1000):
+        """Bounded device wait on a flag (neo_gpu_wait_probe); raises NeoGpuError
+        (NEO_ERR_CUDA) when the wait runs out."""
+        self.check(self.lib.neo_gpu_wait_probe(self.h, 1 if set_flag else 0, spin_limit))
 
     def commit_device(self, d_digits: int, n_vec: int, m: int, d_out: int):
         self.check(self.lib.neo_gpu_commit_device(self.h, ctypes.c_void_p(d_digits), n_vec, m, ctypes.c_void_p(d_out)))
