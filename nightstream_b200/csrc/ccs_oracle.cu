@@ -448,33 +448,80 @@ __device__ K eq_lin_d(K a, K b) {
     return gl::kadd(gl::kmul(gl::ksub(gl::kone(), a), gl::ksub(gl::kone(), b)), gl::kmul(a, b));
 }
 
-__global__ void __launch_bounds__(512) ajtai_round_kernel(const AjtaiArgs a) {
-    extern __shared__ K s_y[];            // [nvec][54] prefolded
-    __shared__ K s_wb[64], s_wa[64];
-    const int nvec = a.k * (1 + a.t);     // vector q < k: NC (y[i][0]); then eval (i, jm)
-    const int j = a.j;
-    // prefix fold of every vector by bits 0..j-1 (fold_bit_inplace semantics)
-    for (int q = threadIdx.x; q < nvec; q += blockDim.x) {
-        const K* src = q < a.k ? a.y + ((uint64_t)q * a.t + 0) * NEO_D
-                               : a.y + (uint64_t)(q - a.k) * NEO_D;
-        K* dst = s_y + q * NEO_D;
-        for (int r = 0; r < NEO_D; r++) dst[r] = src[r];
-        for (int bb = 0; bb < j; bb++) {
-            int stride = 1 << bb, step = stride << 1;
-            for (int base = 0; base < NEO_D; base += step)
-                for (int off = 0; off < stride; off++) {
-                    int i0 = base + off;
-                    if (i0 >= NEO_D) break;
-                    int i1 = i0 + stride;
-                    K lo = dst[i0], hi = i1 < NEO_D ? dst[i1] : gl::kzero();
-                    dst[i0] = gl::klerp(lo, hi, a.ajtai_chals[bb]);
-                }
-        }
+// warp-wide sum of K values (lane 0 holds the total)
+__device__ __forceinline__ K warp_ksum(K v) {
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) {
+        K o;
+        o.re = __shfl_down_sync(0xffffffffu, (unsigned long long)v.re, off);
+        o.im = __shfl_down_sync(0xffffffffu, (unsigned long long)v.im, off);
+        v = gl::kadd(v, o);
     }
-    // tail weights chi(beta_a[j+1..]), chi(alpha[j+1..])
-    const int ntail = a.ell_d - j - 1;
-    const int tail_len = 1 << ntail;
-    for (int tt = threadIdx.x; tt < tail_len; tt += blockDim.x) {
+    return v;
+}
+
+// One Ajtai-phase round (oracle.rs:1659-1953): evaluations at xs of round j
+// over the 54 (padded to 2^ell_d) Ajtai coordinates.  Field arithmetic is
+// exact, so the work is reordered for parallelism without changing a bit:
+//  * the prefix fold by bits 0..j-1 of each vector is the weighted sum with
+//    the chi weights of those challenges (one thread per folded entry);
+//  * an evaluation vector's round value is linear in x, A + (B - A) x with
+//    A, B the tail-weighted sums of its lo / hi entries, so its gamma-weighted
+//    combination is formed once per round, not once per x;
+//  * x-independent products (gamma powers, prefix and row equalities, F') are
+//    separate threads' chains, and tail sums are warp reductions.
+__global__ void __launch_bounds__(512) ajtai_round_kernel(const AjtaiArgs a) {
+    extern __shared__ K s_dyn[];          // s_y [nvec][54] folded, then s_nc [nx][k]
+    __shared__ K s_wb[128], s_wa[128], s_w[128];
+    __shared__ K s_A[160], s_B[160];
+    __shared__ K s_gp[161];               // gamma^0..gamma^k
+    __shared__ K s_gkp[160];              // (gamma^k)^0..(gamma^k)^(t-1), t < k (1 + t) <= 160
+    __shared__ K s_fixed[8];              // ebp, eap, eq_br, eq_ri, fprime, SA, SB
+    __shared__ K s_ncsum[16];
+    const int nvec = a.k * (1 + a.t);     // vector q < k: NC (y[i][0]); then eval (i, jm)
+    K* s_y = s_dyn;
+    K* s_nc = s_dyn + nvec * NEO_D;
+    const int j = a.j, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nwarps = blockDim.x >> 5;
+    const int ntail = a.ell_d - j - 1, tail_len = 1 << ntail;
+    const int hs = 1 << (j + 1), stride = 1 << j;
+
+    // ---- 1. x-independent chains and weights ----
+    if (tid == 0) {
+        K g = gl::kone();
+        s_gp[0] = g;
+        for (int i = 0; i < a.k; i++) { g = gl::kmul(g, a.gamma); s_gp[i + 1] = g; }
+        K p = gl::kone();
+        for (int jm = 0; jm < a.t; jm++) { s_gkp[jm] = p; p = gl::kmul(p, g); }
+    } else if (tid == 1 || tid == 2) {
+        K e = gl::kone();
+        for (int i = 0; i < j; i++) e = gl::kmul(e, eq_lin_d(a.ajtai_chals[i], tid == 1 ? a.beta_a[i] : a.alpha[i]));
+        s_fixed[tid - 1] = e;  // ebp, eap
+    } else if (tid == 3 || tid == 4) {
+        K e = gl::kone();
+        if (tid == 3 || a.has_inputs)
+            for (int i = 0; i < a.ell_n; i++) e = gl::kmul(e, eq_lin_d(a.row_chals[i], tid == 3 ? a.beta_r[i] : a.r_in[i]));
+        s_fixed[tid - 1] = e;  // eq_br, eq_ri
+    } else if (tid == 5) {
+        // F' = f(m_vals), m_vals[j] = y_scalars[0][j] (z1 . v_j by linearity of recomposition)
+        K fprime = gl::kzero();
+        for (int tt = 0; tt < a.f.n_terms; tt++) {
+            K p = a.f.coeff[tt];
+            for (int vv = 0; vv < a.f.n_vars[tt]; vv++) {
+                K mv = a.ysc[a.fvar_j[a.f.var_pos[tt][vv]]];
+                for (int e = 0; e < a.f.var_exp[tt][vv]; e++) p = gl::kmul(p, mv);
+            }
+            fprime = gl::kadd(fprime, p);
+        }
+        s_fixed[4] = fprime;
+    } else if (tid >= 32 && tid < 32 + (1 << j)) {
+        // fold weight of offset b: prod over bits of (bit ? c : 1 - c)
+        const int b = tid - 32;
+        K w = gl::kone();
+        for (int i = 0; i < j; i++) w = gl::kmul(w, ((b >> i) & 1) ? a.ajtai_chals[i] : gl::ksub(gl::kone(), a.ajtai_chals[i]));
+        s_w[b] = w;
+    } else if (tid >= 160 && tid < 160 + tail_len) {
+        // tail weights chi(beta_a[j+1..]), chi(alpha[j+1..])
+        const int tt = tid - 160;
         K wb = gl::kone(), wa = gl::kone();
         for (int i = 0; i < ntail; i++) {
             int bit = (tt >> i) & 1;
@@ -486,76 +533,106 @@ __global__ void __launch_bounds__(512) ajtai_round_kernel(const AjtaiArgs a) {
         s_wa[tt] = wa;
     }
     __syncthreads();
-    const int hs = 1 << (j + 1), stride = 1 << j;
-    // per (x, vector) work item
-    __shared__ K s_val[16][160];
-    for (int w = threadIdx.x; w < a.nx * nvec; w += blockDim.x) {
-        int xi = w / nvec, q = w % nvec;
-        K x = a.xs[xi];
-        const K* v = s_y + q * NEO_D;
-        K acc = gl::kzero();
-        for (int tt = 0; tt < tail_len; tt++) {
-            int idx = tt * hs;
-            if (idx >= NEO_D) continue;
-            int i1 = idx + stride;
-            K lo = v[idx], hi = i1 < NEO_D ? v[i1] : gl::kzero();
-            K val = gl::klerp(lo, hi, x);
-            if (q < a.k) {
-                K y2 = gl::ksqr(val);
-                val = gl::kmul(val, gl::ksub(y2, gl::kone()));  // range product, b = 2
-                acc = gl::kadd(acc, gl::kmul(s_wb[tt], val));
+
+    // ---- 2. prefix fold by bits 0..j-1: entry i of the folded vector at s_y[q][i 2^j] ----
+    {
+        const int L = (NEO_D + stride - 1) >> j;
+        for (int w = tid; w < nvec * L; w += blockDim.x) {
+            const int q = w / L, i = w % L;
+            const K* src = q < a.k ? a.y + ((uint64_t)q * a.t + 0) * NEO_D : a.y + (uint64_t)(q - a.k) * NEO_D;
+            const int base = i << j;
+            K acc;
+            if (j == 0) {
+                acc = src[base];
             } else {
-                acc = gl::kadd(acc, gl::kmul(s_wa[tt], val));
+                acc = gl::kzero();
+                for (int b = 0; b < stride && base + b < NEO_D; b++) acc = gl::kadd(acc, gl::kmul(s_w[b], src[base + b]));
             }
+            s_y[q * NEO_D + base] = acc;
         }
-        s_val[xi][q] = acc;
     }
     __syncthreads();
-    if (threadIdx.x < a.nx) {
-        const int xi = threadIdx.x;
-        K x = a.xs[xi];
-        // gamma^k, prefix eqs
-        K gk = gl::kone();
-        for (int i = 0; i < a.k; i++) gk = gl::kmul(gk, a.gamma);
-        K ebp = gl::kone(), eap = gl::kone();
-        for (int i = 0; i < j; i++) {
-            ebp = gl::kmul(ebp, eq_lin_d(a.ajtai_chals[i], a.beta_a[i]));
-            eap = gl::kmul(eap, eq_lin_d(a.ajtai_chals[i], a.alpha[i]));
-        }
-        K eq_br = gl::kone(), eq_ri = gl::kone();
-        for (int i = 0; i < a.ell_n; i++) {
-            eq_br = gl::kmul(eq_br, eq_lin_d(a.row_chals[i], a.beta_r[i]));
-            if (a.has_inputs) eq_ri = gl::kmul(eq_ri, eq_lin_d(a.row_chals[i], a.r_in[i]));
-        }
-        K eq_beta = gl::kmul(eq_br, gl::kmul(ebp, eq_lin_d(x, a.beta_a[j])));
-        K eq_ar = a.has_inputs ? gl::kmul(eq_ri, gl::kmul(eap, eq_lin_d(x, a.alpha[j]))) : gl::kzero();
-        // F' = f(m_vals), m_vals[j] = y_scalars[0][j] (z1 . v_j by linearity of recomposition)
-        K fprime = gl::kzero();
-        for (int tt = 0; tt < a.f.n_terms; tt++) {
-            K p = a.f.coeff[tt];
-            for (int vv = 0; vv < a.f.n_vars[tt]; vv++) {
-                K mv = a.ysc[a.fvar_j[a.f.var_pos[tt][vv]]];
-                for (int e = 0; e < a.f.var_exp[tt][vv]; e++) p = gl::kmul(p, mv);
+
+    // ---- 3. tail sums: `seg` lanes per item (the tail length, at most 32),
+    //         32 / seg items per warp, segment sums by width-limited shuffles ----
+    const int n_nc = a.nx * a.k, n_items = n_nc + 2 * (nvec - a.k);
+    const int seg = tail_len < 32 ? tail_len : 32, per_warp = 32 / seg;
+    const int sub = lane % seg;
+    for (int base = warp * per_warp; base < n_items; base += nwarps * per_warp) {
+        const int item = base + lane / seg;
+        K part = gl::kzero();
+        if (item < n_nc) {
+            const int xi = item / a.k, q = item % a.k;
+            const K x = a.xs[xi];
+            const K* v = s_y + q * NEO_D;
+            for (int tt = sub; tt < tail_len; tt += seg) {
+                const int idx = tt * hs;
+                if (idx >= NEO_D) continue;
+                const int i1 = idx + stride;
+                K val = gl::klerp(v[idx], i1 < NEO_D ? v[i1] : gl::kzero(), x);
+                val = gl::kmul(val, gl::ksub(gl::ksqr(val), gl::kone()));  // range product, b = 2
+                part = gl::kadd(part, gl::kmul(s_wb[tt], val));
             }
-            fprime = gl::kadd(fprime, p);
+        } else if (item < n_items) {
+            const int e = item - n_nc, q = a.k + (e >> 1), hi_side = e & 1;
+            const K* v = s_y + q * NEO_D;
+            for (int tt = sub; tt < tail_len; tt += seg) {
+                const int idx = tt * hs;
+                if (idx >= NEO_D) continue;
+                const int pos = idx + (hi_side ? stride : 0);
+                if (pos < NEO_D) part = gl::kadd(part, gl::kmul(s_wa[tt], v[pos]));
+            }
         }
-        K nc_sum = gl::kzero(), g = a.gamma;
-        for (int i = 0; i < a.k; i++) {
-            nc_sum = gl::kadd(nc_sum, gl::kmul(g, s_val[xi][i]));
-            g = gl::kmul(g, a.gamma);
+        for (int off = seg >> 1; off > 0; off >>= 1) {
+            K o;
+            o.re = __shfl_down_sync(0xffffffffu, (unsigned long long)part.re, off, seg);
+            o.im = __shfl_down_sync(0xffffffffu, (unsigned long long)part.im, off, seg);
+            part = gl::kadd(part, o);
         }
-        K out = gl::kmul(eq_beta, gl::kadd(fprime, nc_sum));
+        if (sub == 0 && item < n_items) {
+            if (item < n_nc) {
+                s_nc[(item / a.k) * a.k + item % a.k] = part;
+            } else {
+                const int e = item - n_nc;
+                (e & 1 ? s_B : s_A)[a.k + (e >> 1)] = part;
+            }
+        }
+    }
+    __syncthreads();
+
+    // ---- 4. gamma-weighted combinations ----
+    if (warp == 0 || warp == 1) {
+        // S = sum_{jm, i >= 1} gamma^i (gamma^k)^jm X[k + i t + jm], X = A (warp 0) or B (warp 1)
+        const K* X = warp == 0 ? s_A : s_B;
+        const int nterm = (a.k - 1) * a.t;
+        K part = gl::kzero();
+        for (int u = lane; u < nterm; u += 32) {
+            const int i = 1 + u / a.t, jm = u % a.t;
+            part = gl::kadd(part, gl::kmul(gl::kmul(s_gp[i], s_gkp[jm]), X[a.k + i * a.t + jm]));
+        }
+        part = warp_ksum(part);
+        if (lane == 0) s_fixed[5 + warp] = part;
+    } else {
+        // nc_sum[x] = sum_i gamma^(i+1) nc[x][i], warps 2.. over the points
+        for (int xi = warp - 2; xi < a.nx; xi += nwarps - 2) {
+            K part = gl::kzero();
+            for (int i = lane; i < a.k; i += 32) part = gl::kadd(part, gl::kmul(s_gp[i + 1], s_nc[xi * a.k + i]));
+            part = warp_ksum(part);
+            if (lane == 0) s_ncsum[xi] = part;
+        }
+    }
+    __syncthreads();
+
+    // ---- 5. per evaluation point ----
+    if (tid < a.nx) {
+        const int xi = tid;
+        const K x = a.xs[xi];
+        const K gk = s_gp[a.k];
+        const K eq_beta = gl::kmul(s_fixed[2], gl::kmul(s_fixed[0], eq_lin_d(x, a.beta_a[j])));
+        const K eq_ar = a.has_inputs ? gl::kmul(s_fixed[3], gl::kmul(s_fixed[1], eq_lin_d(x, a.alpha[j]))) : gl::kzero();
+        K out = gl::kmul(eq_beta, gl::kadd(s_fixed[4], s_ncsum[xi]));
         if (a.k >= 2 && !gl::kiszero(eq_ar)) {
-            K inner = gl::kzero();
-            K gkj = gl::kone();
-            for (int jm = 0; jm < a.t; jm++) {
-                K gi = gl::kone();
-                for (int i = 1; i < a.k; i++) {
-                    gi = gl::kmul(gi, a.gamma);
-                    inner = gl::kadd(inner, gl::kmul(gl::kmul(gi, gkj), s_val[xi][a.k + i * a.t + jm]));
-                }
-                gkj = gl::kmul(gkj, gk);
-            }
+            const K inner = gl::klerp(s_fixed[5], s_fixed[6], x);
             out = gl::kadd(out, gl::kmul(eq_ar, gl::kmul(gk, inner)));
         }
         a.ys_out[xi] = out;
@@ -980,7 +1057,7 @@ static int ajtai_round(neo_gpu_ccs_oracle* o, const uint64_t* xs, uint32_t nx, u
     a.y = o->y_eval.p;
     a.ysc = o->y_sc.p;
     a.ys_out = o->ys.p;
-    size_t smem = (size_t)o->k * (1 + o->t) * NEO_D * sizeof(K);
+    size_t smem = ((size_t)o->k * (1 + o->t) * NEO_D + (size_t)nx * o->k) * sizeof(K);
     static SmemLimit limit;
     NEO_CK(ctx, limit.at_least(ajtai_round_kernel, smem));
     ajtai_round_kernel<<<1, 512, smem, ctx->stream>>>(a);
