@@ -336,7 +336,7 @@ static void header_params(neo_gpu_shard* sh) {
 
 // digest_ccs_matrices (crates/neo-reductions/src/engines/utils.rs:214-321)
 // The matrix digest is a sequential width-16 sponge over every nonzero
-// (O(nnz) permutations, 0.28 s at n = 2^16), computed once per CCS: the
+// (O(nnz) permutations, 0.17 s at n = 2^16), computed once per CCS: the
 // reference keeps it in ShardProverContext (shard.rs:2557-2560).  Shards
 // created for a CCS seen before (the same circuit proving many shards) reuse
 // it; entries are matched on an exact copy of the matrix data, least recently
