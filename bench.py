@@ -236,11 +236,11 @@ def rounds_roofline(ctx, ccs, z, ell, stream, reps=3):
             "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
             "traffic": ROUNDS_TRAFFIC_PER_ROW * m,
             "traffic_source": "ncu dram__bytes_read+write of the 16 row-round launches of one k = 13 step at "
-                              "2^16 rows, per row (profiles/ccs_round_kernel_ell16_k13.md)",
+                              "2^16 rows (ncu -k regex:ccs_ on bench.py --steps 1 --warmup 1), per row",
             "launch_ms": ms / ell, "sequence_ms": ms, "peak_source": src,
             "algorithmic_bytes_per_sequence": B,
             "note": "integer-ALU bound: the rounds stream int8 digit planes in rounds 0..4 and move far fewer "
-                    "bytes than B_ccs; see profiles/ccs_round_kernel_ell16_k13.md"}
+                    "bytes than B_ccs"}
 
 
 def int8_peak_tops():
@@ -591,8 +591,8 @@ def run_ours(args, rank, world, local_rank):
                                  "+ commit_tc_reduce_kernel)",
                        "bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TOPS", "frac": achieved / peak,
                        "traffic": COMMIT_TRAFFIC_PER_M * m if m >= 1 << 14 else None,
-                       "traffic_source": "ncu dram__bytes_read+write of one 12-plane launch at m = 2^14, scaled by m "
-                                         "(profiles/commit_tc_kernel_m16384_12planes.md)",
+                       "traffic_source": "ncu dram__bytes_read+write of one 12-plane commit_tc_kernel launch at "
+                                         "m = 2^14, scaled by m",
                        "launch_ms": commit_ms, "peak_source": peak_src, "algorithmic_ops_per_launch": ops}
     roofline = rounds_roofline(ctx, ccs, wl.z(0), args.ell, stream)
     # the batched mix runs before the legs that use the host's OpenMP pool
@@ -604,7 +604,11 @@ def run_ours(args, rank, world, local_rank):
                "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
                "vs_baseline": None, "dtype": "u64 (F_q, K = F_q^2), int8 digits", "data": "synthetic",
                "config": config(args), "e2e": e2e, "gpu_launches": int(launches), "clocks": clk,
-               "roofline": roofline, "roofline_commit": roofline_commit, "step_breakdown_ms": stats}
+               "roofline": roofline, "roofline_commit": roofline_commit}
+        perms = stats.pop("transcript_perms", None)
+        stats.pop("unused", None)
+        out["step_breakdown_ms"] = stats
+        out["transcript_permutations_per_step"] = int(perms) if perms is not None else None
         out["pp_setup"] = pp_setup
         if world == 1 and not args.no_cpu_baseline:
             out["cpu_baseline"] = cpu_baseline(args, wl)

@@ -244,9 +244,12 @@ static int neo_gpu_commit_noalloc_impl_abi(neo_gpu_ctx* ctx, const int8_t* d_dig
     if (!ctx) return NEO_ERR_ARG;
     if (!d_digits || !d_out || n_vec == 0 || m == 0) return ctx->fail(NEO_ERR_ARG, "commit_noalloc: bad args");
     PPEntry* pp = pp_lookup(ctx->device, m);
-    if (!pp) return ctx->fail(NEO_ERR_ARG, "commit_noalloc: PP not loaded for this m");
+    // kappa and the coefficient pointer are read once: a PP being generated or
+    // re-uploaded, or one whose generation failed, has kappa = 0 (no usable PP)
+    const uint32_t kappa = pp ? pp->kappa : 0;
+    const uint64_t* d_pp = pp ? pp->d_pp : nullptr;
+    if (!kappa || !d_pp) return ctx->fail(NEO_ERR_ARG, "commit_noalloc: PP not loaded for this m");
     if (ctx->device < 0 || ctx->device >= NOALLOC_MAX_DEVICES) return ctx->fail(NEO_ERR_UNSUPPORTED, "commit_noalloc: device index");
-    const uint32_t kappa = pp->kappa;
     const uint64_t per_chunk = (uint64_t)n_vec * kappa * 81;  // partial words needed per column chunk
     if (per_chunk > NOALLOC_SCRATCH_WORDS)
         return ctx->fail(NEO_ERR_ARG,
@@ -266,19 +269,21 @@ static int neo_gpu_commit_noalloc_impl_abi(neo_gpu_ctx* ctx, const int8_t* d_dig
         }
         scratch = g_noalloc_ptr[ctx->device];
     }
-    // same chunking rule as launch_commit, capped by the scratch capacity
+    // same chunking rule as launch_commit: about 1184 blocks in all, so
+    // n_chunks * kappa * n_vec stays near 1184 and, with 81 partial words per
+    // (chunk, row, vector), far inside the scratch once per_chunk fits
     uint32_t target_blocks = 148 * 8;
     uint32_t per = (uint32_t)((uint64_t)kappa * n_vec);
     uint64_t n_chunks = (target_blocks + per - 1) / per;
-    const uint64_t cap_chunks = NOALLOC_SCRATCH_WORDS / per_chunk;
-    if (n_chunks > cap_chunks) n_chunks = cap_chunks;
     uint64_t cols_per_block = (m + n_chunks - 1) / n_chunks;
     if (cols_per_block < CHUNK_COLS) cols_per_block = CHUNK_COLS;
-    n_chunks = (m + cols_per_block - 1) / cols_per_block;  // never grows past cap_chunks
+    n_chunks = (m + cols_per_block - 1) / cols_per_block;
+    if (n_chunks * per_chunk > NOALLOC_SCRATCH_WORDS)
+        return ctx->fail(NEO_ERR_INVARIANT, "commit_noalloc: partial sums exceed the fixed scratch");
     dim3 grid((uint32_t)n_chunks, kappa, n_vec);
     // every partial word a reduce reads is written by commit_partial_kernel first,
     // so the array needs no clearing between calls
-    commit_partial_kernel<<<grid, COMMIT_THREADS, 0, ctx->stream>>>(pp->d_pp, kappa, m, d_digits,
+    commit_partial_kernel<<<grid, COMMIT_THREADS, 0, ctx->stream>>>(d_pp, kappa, m, d_digits,
                                                                      (uint32_t)cols_per_block, scratch);
     NEO_LAUNCHED(ctx);
     commit_reduce_kernel<<<n_vec * kappa, 96, 0, ctx->stream>>>(scratch, (uint32_t)n_chunks, kappa, n_vec, d_out);
