@@ -639,6 +639,8 @@ __global__ void __launch_bounds__(512) ajtai_round_kernel(const AjtaiArgs a) {
     }
 }
 
+#include "ccs_fast.cuh"
+
 }  // namespace
 
 // ---------------------------------------------------------------------------
@@ -664,6 +666,13 @@ struct neo_gpu_ccs_oracle {
     int J = 0;
     DevBuf<K> wg, eqw, partials, coeffs, ys, scratch_k;
     DevBuf<K> d_chals;  // row challenges on the device (prefix χ tables of the streaming rounds)
+    // ternary-digit path (ccs_fast.cuh): E tables, the 8-row pattern histogram
+    bool fast = false;
+    DevBuf<K> E_all;            // E_j = chi_{beta_{j+1..}} at offset 2^ell - 2^(ell - j), j < ell
+    DevBuf<K> hist;             // [NPAT]
+    DevBuf<uint32_t> hist_part; // [hist blocks][NPAT][8]
+    DevBuf<uint32_t> tern_flag;
+    uint32_t hist_gx = 0, hist_gy = 0, hist_qc = 0;
     K gamma{}, gamma_to_k{};
     std::vector<K> alpha, beta_a, beta_r, r_in, row_chals, ajtai_chals;
     bool has_inputs = false, has_eval = false;
@@ -694,6 +703,7 @@ static K host_chi_mask(size_t mask, const std::vector<K>& pts) {
 static int oracle_init(neo_gpu_ctx* ctx, neo_gpu_ccs_oracle* o, const int8_t* d_Z, uint32_t k, uint32_t b,
                        const K* alpha, const K* beta_a, const K* beta_r, K gamma, const K* r_inputs,
                        uint32_t ell_d, uint32_t ell_n, uint32_t d_sc);
+static int fast_setup(neo_gpu_ccs_oracle* o);
 
 static int neo_gpu_ccs_oracle_create_impl_abi(neo_gpu_ctx* ctx, const neo_ccs_desc* desc, const int8_t* Z, uint32_t k,
                                          uint32_t b, const uint64_t* alpha, const uint64_t* beta_a,
@@ -901,7 +911,186 @@ static int oracle_init(neo_gpu_ctx* ctx, neo_gpu_ccs_oracle* o, const int8_t* d_
     NEO_CK(ctx, o->partials.ensure(max_blocks * (o->deg_max + 1)));
     NEO_CK(ctx, o->coeffs.ensure(MAX_DEG + 1));
     NEO_CK(ctx, o->ys.ensure(16));
+    // ternary digits (every witness the fold step builds: balanced base-2
+    // decomposition and split_b) take the pattern-histogram path; any other
+    // digit keeps the streaming kernels above
+    uint32_t h_bad = 1;
+    if (ell_n >= 3) {
+        NEO_CK(ctx, o->tern_flag.ensure(1));
+        NEO_CK(ctx, cudaMemsetAsync(o->tern_flag.p, 0, 4, ctx->stream));
+        const uint64_t nbytes = (uint64_t)nq * m;
+        ternary_check_kernel<<<148 * 4, 256, 0, ctx->stream>>>(reinterpret_cast<const uint4*>(o->Z), nbytes / 16,
+                                                              reinterpret_cast<const uint8_t*>(o->Z) + nbytes / 16 * 16,
+                                                              (uint32_t)(nbytes % 16), o->tern_flag.p);
+        NEO_LAUNCHED(ctx);
+        NEO_CK(ctx, ctx_d2h(ctx, &h_bad, o->tern_flag.p, 4));
+    }
     NEO_CK(ctx, ctx_sync(ctx));
+    o->fast = h_bad == 0;
+    if (o->fast) {
+        int rc2 = fast_setup(o);
+        if (rc2) return rc2;
+    }
+    return NEO_OK;
+}
+
+// Grid of the fast row kernel at round j: (pair, q chunk) threads, enough to
+// fill the GPU about twice when the pairs alone do not.
+static void fast_rows_grid(const neo_gpu_ccs_oracle* o, uint32_t j, uint64_t* pairs, uint32_t* n_chunk,
+                           uint32_t* q_chunk, uint32_t* blocks) {
+    const uint32_t nq = o->k * NEO_D;
+    *pairs = o->n_pad >> (j + 1);
+    uint32_t nc = 1;
+    if (j >= 3) {
+        const uint64_t target = 148ull * 2 * FR * 2;
+        nc = (uint32_t)std::min<uint64_t>(nq, std::max<uint64_t>(1, (target + *pairs - 1) / *pairs));
+    }
+    *q_chunk = (nq + nc - 1) / nc;
+    *n_chunk = (nq + *q_chunk - 1) / *q_chunk;
+    *blocks = (uint32_t)ceil_div(*pairs * *n_chunk, FR);
+}
+
+static int fast_setup(neo_gpu_ccs_oracle* o) {
+    neo_gpu_ctx* ctx = o->ctx;
+    const uint32_t ell = o->ell_n, nq = o->k * NEO_D;
+    // E_j = chi of beta_r[j+1..ell) for every row round (beta_r is in ws_bits[0..ell))
+    NEO_CK(ctx, o->E_all.ensure(o->n_pad));
+    for (uint32_t j = 0; j < ell; j++) {
+        const uint64_t off = o->n_pad - (o->n_pad >> j);
+        int rc = launch_chi_table(ctx, o->ws_bits.p + j + 1, ell - j - 1, o->E_all.p + off);
+        if (rc) return rc;
+    }
+    // histogram grid: a thread per 8-row block, q chunks so that ~2 blocks per SM
+    const uint32_t n_t8 = (uint32_t)(o->n_pad >> 3);
+    o->hist_gx = (uint32_t)ceil_div(n_t8, HIST_T);
+    uint32_t gy = std::max<uint32_t>(1, (296 + o->hist_gx - 1) / o->hist_gx);
+    o->hist_qc = std::max<uint32_t>(1, std::min<uint32_t>(HIST_MAX_Q, (nq + gy - 1) / gy));
+    o->hist_gy = (nq + o->hist_qc - 1) / o->hist_qc;
+    NEO_CK(ctx, o->hist_part.ensure((size_t)o->hist_gx * o->hist_gy * NPAT * HIST_LIMBS));
+    NEO_CK(ctx, o->hist.ensure(NPAT));
+    // partial records: the largest round
+    uint64_t recs = 0;
+    for (uint32_t j = 0; j < ell; j++) {
+        uint64_t pairs;
+        uint32_t nc, qc, blocks;
+        fast_rows_grid(o, j, &pairs, &nc, &qc, &blocks);
+        recs = std::max<uint64_t>(recs, blocks + ceil_div(pairs, FR) + ceil_div(NPAT, FR));
+    }
+    NEO_CK(ctx, o->partials.ensure(recs * REC));
+    static SmemLimit hist_smem;
+    NEO_CK(ctx, hist_smem.at_least(ccs_hist_kernel, (size_t)NPAT * HIST_LIMBS * 4 + HIST_MAX_Q * sizeof(K)));
+    return NEO_OK;
+}
+
+// One row round on the ternary-digit path; leaves deg_max + 1 coefficients in
+// coeffs_dst (device).  d_chals must hold r_0..r_{j-1}.
+static int fast_round_launch(neo_gpu_ccs_oracle* o, K* coeffs_dst) {
+    neo_gpu_ctx* ctx = o->ctx;
+    const uint32_t j = o->round_idx, ell = o->ell_n, nq = o->k * NEO_D;
+    const bool last = j + 1 == ell;
+    uint32_t nrec = 0;
+    if (j == 0) {
+        HistArgs h{};
+        h.Z = o->Z;
+        h.m = o->m;
+        h.nq = nq;
+        h.n_t8 = (uint32_t)(o->n_pad >> 3);
+        h.q_chunk = o->hist_qc;
+        h.wg = o->wg.p;
+        h.E8 = o->E_all.p + (o->n_pad - (o->n_pad >> 2));
+        h.partial = o->hist_part.p;
+        const size_t smem = (size_t)NPAT * HIST_LIMBS * 4 + (size_t)o->hist_qc * sizeof(K);
+        ccs_hist_kernel<<<dim3(o->hist_gx, o->hist_gy), HIST_T, smem, ctx->stream>>>(h);
+        NEO_LAUNCHED(ctx);
+        ccs_hist_reduce_kernel<<<ceil_div(NPAT, 32), 256, 0, ctx->stream>>>(o->hist_part.p, o->hist_gx * o->hist_gy,
+                                                                           o->hist.p);
+        NEO_LAUNCHED(ctx);
+    }
+    if (j <= 2) {
+        MomArgs ma{};
+        ma.H = o->hist.p;
+        ma.j = (int)j;
+        ma.chals = o->d_chals.p;
+        ma.beta1 = o->beta_r[1];
+        ma.beta2 = o->beta_r[2];
+        ma.partials = o->partials.p;
+        ma.part_off = 0;
+        const uint32_t nb = (uint32_t)ceil_div(NPAT, FR);
+        ccs_mom_round_kernel<<<nb, FR, 0, ctx->stream>>>(ma);
+        NEO_LAUNCHED(ctx);
+        nrec = nb;
+    }
+    FastRowArgs a{};
+    if (j == 0) {
+        a.small_in = o->small[0].p;
+        a.small_len_in = o->n_pad;
+        a.fold = 0;
+    } else {
+        a.small_in = o->small[o->small_cur].p;
+        a.small_len_in = o->n_pad >> (j - 1);
+        a.fold = 1;
+        a.r = o->row_chals[j - 1];
+        a.small_out = last ? nullptr : o->small[o->small_cur ^ 1].p;
+        a.small_len_out = o->n_pad >> j;
+    }
+    a.n_small = o->n_small;
+    a.idx_eqrin = o->idx_eqrin;
+    a.idx_eval = o->idx_eval;
+    a.f = o->f;
+    a.fdeg = o->deg_max - 1;
+    a.E = o->E_all.p + (o->n_pad - (o->n_pad >> j));
+    a.j = (int)j;
+    a.chals = o->d_chals.p;
+    a.Z = o->Z;
+    a.m = o->m;
+    a.wg = o->wg.p;
+    a.nq = nq;
+    a.partials = o->partials.p;
+    // small tables: one thread per pair
+    a.pairs = o->n_pad >> (j + 1);
+    a.part_off = nrec;
+    const uint32_t sblocks = (uint32_t)ceil_div(a.pairs, FR);
+    ccs_fast_small_kernel<<<sblocks, FR, 0, ctx->stream>>>(a);
+    NEO_LAUNCHED(ctx);
+    nrec += sblocks;
+    if (j >= 3) {
+        uint32_t nc, qc, blocks;
+        fast_rows_grid(o, j, &a.pairs, &nc, &qc, &blocks);
+        a.n_chunk = nc;
+        a.q_chunk = qc;
+        a.part_off = nrec;
+        if (j == 4 && !last) {
+            a.nc_out = o->nc[0].p;
+            a.nc_len_out = o->n_pad >> 4;
+            o->nc_cur = 0;
+        } else if (j >= 5) {
+            a.nc_in = o->nc[o->nc_cur].p;
+            a.nc_len_in = o->n_pad >> (j - 1);
+            if (!last) {
+                a.nc_out = o->nc[o->nc_cur ^ 1].p;
+                a.nc_len_out = o->n_pad >> j;
+            }
+        }
+        const size_t wsm = (size_t)nq * sizeof(K);
+        if (j == 3) ccs_fast_nc_kernel<3><<<blocks, FR, wsm, ctx->stream>>>(a);
+        else if (j == 4) ccs_fast_nc_kernel<4><<<blocks, FR, wsm, ctx->stream>>>(a);
+        else ccs_fast_nc_kernel<5><<<blocks, FR, wsm, ctx->stream>>>(a);
+        NEO_LAUNCHED(ctx);
+        nrec += blocks;
+    }
+    if (j > 0 && !last) o->small_cur ^= 1;
+    if (j >= 5 && !last) o->nc_cur ^= 1;
+    FastReduceArgs r{};
+    r.partials = o->partials.p;
+    r.nrec = nrec;
+    r.ncoef = o->deg_max + 1;
+    r.j = (int)j;
+    r.chals = o->d_chals.p;
+    for (uint32_t i = 0; i < ell && i < 32; i++) r.beta[i] = o->beta_r[i];
+    r.gamma_to_k = o->gamma_to_k;
+    r.coeffs_out = coeffs_dst;
+    ccs_fast_reduce_kernel<<<1, 256, 0, ctx->stream>>>(r);
+    NEO_LAUNCHED(ctx);
     return NEO_OK;
 }
 
@@ -909,6 +1098,7 @@ static int oracle_init(neo_gpu_ctx* ctx, neo_gpu_ccs_oracle* o, const int8_t* d_
 // leaves its deg_max + 1 coefficients in coeffs_dst (device); no host sync.
 // d_chals must hold the row challenges of the rounds already bound.
 static int row_round_launch(neo_gpu_ccs_oracle* o, K* coeffs_dst) {
+    if (o->fast) return fast_round_launch(o, coeffs_dst);
     neo_gpu_ctx* ctx = o->ctx;
     const uint32_t j = o->round_idx;
     const uint32_t nq = o->k * NEO_D;
@@ -1000,7 +1190,7 @@ static int row_round_launch(neo_gpu_ccs_oracle* o, K* coeffs_dst) {
 static int row_round(neo_gpu_ccs_oracle* o) {
     neo_gpu_ctx* ctx = o->ctx;
     const uint32_t j = o->round_idx;
-    if (j > 0 && (int)j <= o->J)
+    if (j > 0 && ((int)j <= o->J || o->fast))
         NEO_CK(ctx, cudaMemcpyAsync(o->d_chals.p, o->row_chals.data(), j * sizeof(K), cudaMemcpyHostToDevice,
                                     ctx->stream));
     int rc = row_round_launch(o, o->coeffs.p);

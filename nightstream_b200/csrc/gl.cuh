@@ -153,4 +153,58 @@ GL_HD K kinv(K a) {
 // a + (b - a) * r
 GL_HD K klerp(K a, K b, K r) { return kadd(a, kmul(ksub(b, a), r)); }
 
+#ifdef __CUDACC__
+// Unreduced sums of 64 x 64-bit products.  A 160-bit accumulator (five
+// 32-bit words, little-endian) adds each 128-bit product with three carry
+// chains and holds at least 2^32 products exactly; the sum is reduced mod q
+// once, when it is read.
+struct Acc160 {
+    uint32_t w0, w1, w2, w3, w4;
+};
+__device__ __forceinline__ void acc_zero(Acc160& a) { a.w0 = a.w1 = a.w2 = a.w3 = a.w4 = 0; }
+__device__ __forceinline__ void acc_mad(Acc160& a, uint64_t x, uint64_t y) {
+    const uint32_t x0 = (uint32_t)x, x1 = (uint32_t)(x >> 32), y0 = (uint32_t)y, y1 = (uint32_t)(y >> 32);
+    // x y = x0 y0 + (x0 y1 + x1 y0) 2^32 + x1 y1 2^64
+    asm("{\n\t"
+        "mad.lo.cc.u32 %0, %5, %7, %0;\n\t"
+        "madc.hi.cc.u32 %1, %5, %7, %1;\n\t"
+        "madc.lo.cc.u32 %2, %6, %8, %2;\n\t"
+        "madc.hi.cc.u32 %3, %6, %8, %3;\n\t"
+        "addc.u32 %4, %4, 0;\n\t"
+        "mad.lo.cc.u32 %1, %5, %8, %1;\n\t"
+        "madc.hi.cc.u32 %2, %5, %8, %2;\n\t"
+        "addc.cc.u32 %3, %3, 0;\n\t"
+        "addc.u32 %4, %4, 0;\n\t"
+        "mad.lo.cc.u32 %1, %6, %7, %1;\n\t"
+        "madc.hi.cc.u32 %2, %6, %7, %2;\n\t"
+        "addc.cc.u32 %3, %3, 0;\n\t"
+        "addc.u32 %4, %4, 0;\n\t"
+        "}"
+        : "+r"(a.w0), "+r"(a.w1), "+r"(a.w2), "+r"(a.w3), "+r"(a.w4)
+        : "r"(x0), "r"(x1), "r"(y0), "r"(y1));
+}
+// value mod q: 2^64 = 2^32 - 1, 2^96 = -1, 2^128 = -2^32 (mod q)
+__device__ __forceinline__ uint64_t acc_reduce(const Acc160& a) {
+    const uint64_t L = ((uint64_t)a.w1 << 32) | a.w0;
+    const uint64_t B = ((uint64_t)a.w2 << 32) - a.w2;
+    const uint64_t C = ((uint64_t)a.w4 << 32) | a.w3;
+    return sub(add(canon(L), canon(B)), canon(C));
+}
+// Unreduced sum of K products x y: re = sum (x.re y.re + (7 x.im) y.im),
+// im = sum (x.re y.im + x.im y.re), with 7 x.im (mod q) supplied by the
+// caller (it is shared by every product with the same x); 2^31 products at
+// most.
+struct KAcc {
+    Acc160 re, im;
+};
+__device__ __forceinline__ void kacc_zero(KAcc& a) { acc_zero(a.re); acc_zero(a.im); }
+__device__ __forceinline__ void kacc_mad(KAcc& a, K x, uint64_t x7im, K y) {
+    acc_mad(a.re, x.re, y.re);
+    acc_mad(a.re, x7im, y.im);
+    acc_mad(a.im, x.re, y.im);
+    acc_mad(a.im, x.im, y.re);
+}
+__device__ __forceinline__ K kacc_reduce(const KAcc& a) { return kmk(acc_reduce(a.re), acc_reduce(a.im)); }
+#endif
+
 }  // namespace gl
