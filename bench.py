@@ -57,6 +57,9 @@ def parse():
     ap.add_argument("--batch-reps", type=int, default=3, help="batched runs of the mix; the median is reported")
     ap.add_argument("--shard-steps", type=int, default=3)
     ap.add_argument("--workers", type=int, default=0, help="batch workers (0: min(16, host cores))")
+    ap.add_argument("--no-served", action="store_true", help="plain mode without the served (Poisson) sub-result")
+    ap.add_argument("--served-requests", type=int, default=24)
+    ap.add_argument("--no-large", action="store_true", help="plain mode without the 2^20 large-shard sub-result")
     ap.add_argument("--no-batch", action="store_true",
                     help="plain mode without the batched 64-shard memory mix (batched vs one-at-a-time) sub-result")
     return ap.parse_args()
@@ -395,15 +398,15 @@ def run_batched(args):
     print(json.dumps(out), flush=True)
 
 
-def run_served(args):
-    """Poisson arrivals of shard-prove requests (n log-uniform 2^10..2^18) at swept rates."""
+def served_result(args, n_req, rates=(2.0, 5.0, 10.0)):
+    """Poisson arrivals of shard-prove requests (n log-uniform 2^10..2^18, each
+    with a Twist memory and a Shout table) at each rate: p50 / p99 latency
+    (arrival to result), fold-steps/s over the run and the longest queue wait."""
     from nightstream_b200 import gpu
     workers = args.workers or min(16, os.cpu_count() or 8)
-    n_req = args.shards
     shards = shard_mix(n_req, 10, 18, 91, args.shard_steps)
     ctx = gpu.Context(0)
     upload_pps(ctx, [s[0] for s in shards])
-    rates = [2.0, 5.0, 10.0]
     res = []
     for lam in rates:
         rng = np.random.default_rng(int(lam * 100))
@@ -421,18 +424,58 @@ def run_served(args):
         dt = time.perf_counter() - t0
         infos = [b.job_info(j) for j in ids]
         b.close()
+        assert all(i["status"] == 1 for i in infos)
         lat = sorted(i["latency_ms"] for i in infos)
-        res.append({"rate_per_s": lam, "p50_ms": lat[len(lat) // 2], "p99_ms": lat[min(len(lat) - 1, int(0.99 * len(lat)))],
+        res.append({"rate_per_s": lam, "p50_ms": lat[len(lat) // 2],
+                    "p99_ms": lat[min(len(lat) - 1, int(0.99 * len(lat)))],
                     "fold_steps_per_s": n_req * args.shard_steps / dt, "max_queue_ms": max(i["queue_ms"] for i in infos)})
     ctx.close()
-    best = max(r["fold_steps_per_s"] for r in res)
-    out = {"metric": METRIC, "value": best, "unit": UNIT, "n_gpus": 1, "steps": n_req * args.shard_steps,
+    return {"requests": n_req, "steps_per_request": args.shard_steps, "workers": workers,
+            "sizes_log2": [s[0] for s in shards], "rates": res}
+
+
+def large_result(args, steps=3):
+    """The large single shard: n = m = 2^20, 2^14 trace steps per fold step, a
+    Twist memory of 2^16 cells and a Shout table of 2^20 entries (59 bus
+    columns), PP from setup_par on the device; steady-state fold steps through
+    the C ABI with the witness resident (CUDA events on the library stream)."""
+    import torch
+    from nightstream_b200 import gpu, synth
+    ell = 20
+    ccs, zs, mem, inits = synth.make_memory_workload_chunks(ell, 4321, steps + 1, 1 << 14, 20, 16)
+    ctx = gpu.Context(0)
+    ctx.pp_generate(bytes(range(3, 35)), 16, 1 << ell, 1)
+    sh = gpu.Shard(ctx, ccs, m_in=1, k_rho=12, app_label=b"neo/large", mem=mem)
+    zt = torch.from_numpy(np.stack(zs).view(np.int64).copy()).cuda()
+    stream = torch.cuda.ExternalStream(ctx.stream)
+    sh.fold_step_device(zt[0].data_ptr())  # step 0 (k = 1)
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ctx.synchronize()
+    ev0.record(stream)
+    for c in range(1, steps + 1):
+        sh.set_twist_init(0, inits[c][0])
+        sh.fold_step_device(zt[c].data_ptr())
+    ev1.record(stream)
+    ev1.synchronize()
+    ms = ev0.elapsed_time(ev1) / steps
+    stats = sh.step_stats()
+    sh.close()
+    ctx.close()
+    return {"workload": "n=m=2^20, 2^14 trace steps per fold step, Twist 2^16 cells, Shout 2^20 entries, k=13",
+            "steps": steps, "ms_per_step": ms, "fold_steps_per_s": 1e3 / ms,
+            "transcript_permutations_per_step": int(stats.get("transcript_perms", 0))}
+
+
+def run_served(args):
+    r = served_result(args, args.shards)
+    best = max(x["fold_steps_per_s"] for x in r["rates"])
+    out = {"metric": METRIC, "value": best, "unit": UNIT, "n_gpus": 1, "steps": r["requests"] * r["steps_per_request"],
            "warmup": 0, "ms_per_step": 1e3 / best, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
            "dtype": "u64 (F_q, K = F_q^2), int8 digits", "data": "synthetic",
-           "config": {"workload": f"served: {n_req} shard-prove requests, n=m=2^U, U uniform in [10,18], "
-                                  f"{args.shard_steps} fold steps each, Twist 2^10 cells + Shout 2^12 table per shard, "
-                                  f"Poisson arrivals, {workers} workers"},
-           "served": res}
+           "config": {"workload": f"served: {r['requests']} shard-prove requests, n=m=2^U, U uniform in [10,18], "
+                                  f"{r['steps_per_request']} fold steps each, Twist 2^10 cells + Shout 2^12 table per "
+                                  f"shard, Poisson arrivals, {r['workers']} workers"},
+           "served": r}
     print(json.dumps(out), flush=True)
 
 
@@ -597,6 +640,7 @@ def run_ours(args, rank, world, local_rank):
     roofline = rounds_roofline(ctx, ccs, wl.z(0), args.ell, stream)
     # the batched mix runs before the legs that use the host's OpenMP pool
     batched = batched_result(args) if rank == 0 and world == 1 and not args.no_batch else None
+    served = served_result(args, args.served_requests) if rank == 0 and world == 1 and not args.no_served else None
     pp_setup = pp_setup_result(args, ctx, m) if rank == 0 else None
 
     if rank == 0:
@@ -614,9 +658,14 @@ def run_ours(args, rank, world, local_rank):
             out["cpu_baseline"] = cpu_baseline(args, wl)
         if batched is not None:
             out["batched"] = batched
-        print(json.dumps(out), flush=True)
+        if served is not None:
+            out["served"] = served
     shard.close()
     ctx.close()
+    if rank == 0:
+        if world == 1 and not args.no_large:
+            out["large"] = large_result(args)
+        print(json.dumps(out), flush=True)
 
 
 def main():

@@ -37,6 +37,25 @@ constexpr int REC = MAX_DEG + 3;  // partial record: S coefficients [0, MAX_DEG)
 constexpr int FR = 256;           // threads per fast-row block
 constexpr uint32_t P4W = 0x1B090301u;  // base-3 weights 1, 3, 9, 27 for __dp4a
 
+// Out-of-line K products for code that runs once or a few times per warp
+// (serial roles, late rounds): every call site shares one copy of the
+// multiplication, so the instruction cache holds it; the hot streaming rounds
+// keep the inlined form (C = false).
+__device__ __noinline__ K kmul_n(K a, K b) { return gl::kmul(a, b); }
+__device__ __noinline__ K ksqr_n(K a) { return gl::ksqr(a); }
+template <bool C>
+__device__ __forceinline__ K kmul_c(K a, K b) {
+    if constexpr (C) return kmul_n(a, b);
+    else return gl::kmul(a, b);
+}
+template <bool C>
+__device__ __forceinline__ K ksqr_c(K a) {
+    if constexpr (C) return ksqr_n(a);
+    else return gl::ksqr(a);
+}
+template <bool C>
+__device__ __forceinline__ K klerp_c(K a, K b, K r) { return gl::kadd(a, kmul_c<C>(gl::ksub(b, a), r)); }
+
 // base-3 index of four ternary digits (bytes -1, 0, 1) and whether all four are ternary
 __device__ __forceinline__ uint32_t p4_index(uint32_t x) { return __dp4a(__vadd4(x, 0x01010101u), P4W, 0u); }
 __device__ __forceinline__ bool p4_ternary(uint32_t x) { return __vcmpgtu4(__vadd4(x, 0x01010101u), 0x02020202u) == 0; }
@@ -65,14 +84,16 @@ struct HistArgs {
     uint32_t q_chunk;  // q per block (<= HIST_MAX_Q)
     const K* wg;       // [nq]
     const K* E8;       // E_2, [n_t8]
-    uint32_t* partial; // [gridDim.y][gridDim.x][NPAT][HIST_LIMBS]
+    uint32_t* partial; // [gridDim.y][gridDim.x][HIST_LIMBS][NPAT]
 };
 
 // One thread per 8-row block t8, a range of q per block.  Each nonzero
 // (q, t8) adds +-E_2(t8) wg_q to its pattern's counters: eight 16-bit limbs
-// in u32 shared-memory counters (at most 65536 adds per block).
+// (re: 0..3, im: 4..7) in u32 shared-memory counters, at most 65536 adds per
+// block so no counter overflows.  The counters are limb-major, so the lanes
+// of a warp (random patterns) spread over the banks.
 __global__ void __launch_bounds__(HIST_T) ccs_hist_kernel(const HistArgs a) {
-    extern __shared__ uint32_t s_hist[];  // [NPAT][HIST_LIMBS], then wg of the block's q range
+    extern __shared__ uint32_t s_hist[];  // [HIST_LIMBS][NPAT], then wg of the block's q range
     K* s_wg = reinterpret_cast<K*>(s_hist + NPAT * HIST_LIMBS);
     const int tid = threadIdx.x;
     for (int i = tid; i < NPAT * HIST_LIMBS; i += HIST_T) s_hist[i] = 0;
@@ -84,8 +105,17 @@ __global__ void __launch_bounds__(HIST_T) ccs_hist_kernel(const HistArgs a) {
     if (t8 < a.n_t8) {
         const K e = a.E8[t8];
         const int8_t* zp = a.Z + (uint64_t)q0 * a.m + 8ull * t8;
-        for (uint32_t q = q0; q < q1; q++, zp += a.m) {
-            const uint2 v = *reinterpret_cast<const uint2*>(zp);
+        constexpr int BATCH = 8;  // loads in flight per thread
+        for (uint32_t qb = q0; qb < q1; qb += BATCH) {
+          uint2 vb[BATCH];
+#pragma unroll
+          for (int i = 0; i < BATCH; i++)
+              vb[i] = qb + i < q1 ? __ldg(reinterpret_cast<const uint2*>(zp + (uint64_t)(qb - q0 + i) * a.m))
+                                 : make_uint2(0, 0);
+#pragma unroll
+          for (int i = 0; i < BATCH; i++) {
+            const uint2 v = vb[i];
+            const uint32_t q = qb + i;
             if ((v.x | v.y) == 0) continue;
             const int P = (int)(p4_index(v.x) + 81u * p4_index(v.y));
             K w = gl::kmul(e, s_wg[q - q0]);
@@ -96,15 +126,12 @@ __global__ void __launch_bounds__(HIST_T) ccs_hist_kernel(const HistArgs a) {
                 idx = NPAT - 1 - P;  // the negated pattern 6560 - P
                 w = gl::kneg(w);
             }
-            uint32_t* h = s_hist + idx * HIST_LIMBS;
-            atomicAdd(h + 0, (uint32_t)(w.re & 0xFFFF));
-            atomicAdd(h + 1, (uint32_t)((w.re >> 16) & 0xFFFF));
-            atomicAdd(h + 2, (uint32_t)((w.re >> 32) & 0xFFFF));
-            atomicAdd(h + 3, (uint32_t)(w.re >> 48));
-            atomicAdd(h + 4, (uint32_t)(w.im & 0xFFFF));
-            atomicAdd(h + 5, (uint32_t)((w.im >> 16) & 0xFFFF));
-            atomicAdd(h + 6, (uint32_t)((w.im >> 32) & 0xFFFF));
-            atomicAdd(h + 7, (uint32_t)(w.im >> 48));
+#pragma unroll
+            for (int l = 0; l < 4; l++) {
+                atomicAdd(s_hist + l * NPAT + idx, (uint32_t)((w.re >> (16 * l)) & 0xFFFF));
+                atomicAdd(s_hist + (4 + l) * NPAT + idx, (uint32_t)((w.im >> (16 * l)) & 0xFFFF));
+            }
+          }
         }
     }
     __syncthreads();
@@ -113,65 +140,60 @@ __global__ void __launch_bounds__(HIST_T) ccs_hist_kernel(const HistArgs a) {
         reinterpret_cast<uint4*>(out)[i] = reinterpret_cast<const uint4*>(s_hist)[i];
 }
 
-// H[p] = sum over blocks of the limb counters, recombined mod q.  Block:
-// 32 patterns x 8 limbs (one thread each), summing nblk counters in u64
-// (each counter < 2^32; nblk <= 2^20 keeps the sum < 2^52).
-__global__ void __launch_bounds__(256) ccs_hist_reduce_kernel(const uint32_t* __restrict__ partial, uint32_t nblk,
-                                                              K* __restrict__ H) {
-    __shared__ uint64_t s[32][HIST_LIMBS];
-    const int tid = threadIdx.x;
-    const uint32_t p = blockIdx.x * 32 + tid / HIST_LIMBS;
-    const int l = tid % HIST_LIMBS;
+// H64[l][p] += the block counters of one slice of blocks; one thread per
+// counter, consecutive threads on consecutive counters.  Each sum stays below
+// 2^52 (2^20 blocks of counters < 2^32).
+constexpr int HIST_SUM_SLICE = 8;
+__global__ void __launch_bounds__(256) ccs_hist_sum_kernel(const uint32_t* __restrict__ partial, uint32_t nblk,
+                                                           unsigned long long* __restrict__ H64) {
+    const uint32_t i = blockIdx.x * 256 + threadIdx.x;
+    if (i >= NPAT * HIST_LIMBS) return;
+    const uint32_t b0 = blockIdx.y * HIST_SUM_SLICE, b1 = min(nblk, b0 + HIST_SUM_SLICE);
     uint64_t acc = 0;
-    if (p < NPAT) {
-        const uint32_t* src = partial + (uint64_t)p * HIST_LIMBS + l;
-        uint32_t b = 0;
-        for (; b + 4 <= nblk; b += 4) {
-            const uint64_t st = (uint64_t)NPAT * HIST_LIMBS;
-            acc += (uint64_t)src[b * st] + src[(b + 1) * st] + src[(b + 2) * st] + src[(b + 3) * st];
-        }
-        for (; b < nblk; b++) acc += src[(uint64_t)b * NPAT * HIST_LIMBS];
+    for (uint32_t b = b0; b < b1; b++) acc += __ldg(partial + (uint64_t)b * NPAT * HIST_LIMBS + i);
+    if (acc) atomicAdd(H64 + i, (unsigned long long)acc);
+}
+
+// H[p] from its eight limb sums (limb l has weight 2^(16 l); 2^0 .. 2^48 are canonical)
+__device__ __forceinline__ K hist_value(const unsigned long long* H64, int p) {
+    uint64_t re = 0, im = 0;
+#pragma unroll
+    for (int l = 0; l < 4; l++) {
+        const uint64_t pw = 1ull << (16 * l);
+        re = gl::add(re, gl::mul(gl::canon(H64[l * NPAT + p]), pw));
+        im = gl::add(im, gl::mul(gl::canon(H64[(4 + l) * NPAT + p]), pw));
     }
-    s[tid / HIST_LIMBS][l] = acc;
-    __syncthreads();
-    if (tid < 32 && blockIdx.x * 32 + tid < NPAT) {
-        // limb l has weight 2^(16 (l mod 4)); 2^0, 2^16, 2^32, 2^48 are canonical
-        uint64_t re = 0, im = 0;
-        for (int i = 0; i < 4; i++) {
-            const uint64_t pw = 1ull << (16 * i);
-            re = gl::add(re, gl::mul(gl::canon(s[tid][i]), pw));
-            im = gl::add(im, gl::mul(gl::canon(s[tid][4 + i]), pw));
-        }
-        H[blockIdx.x * 32 + tid] = gl::kmk(re, im);
-    }
+    return gl::kmk(re, im);
 }
 
 // coefficients of N(lo + (hi - lo) X) = c0 + c1 X + c2 X^2 + c3 X^3
+template <bool C = false>
 __device__ __forceinline__ void n_coeffs(K lo, K hi, K c[4]) {
     const K b = gl::ksub(hi, lo);
-    const K a2 = gl::ksqr(lo), b2 = gl::ksqr(b);
-    const K a2b = gl::kmul(a2, b), ab2 = gl::kmul(lo, b2);
-    c[0] = gl::ksub(gl::kmul(a2, lo), lo);
+    const K a2 = ksqr_c<C>(lo), b2 = ksqr_c<C>(b);
+    const K a2b = kmul_c<C>(a2, b), ab2 = kmul_c<C>(lo, b2);
+    c[0] = gl::ksub(kmul_c<C>(a2, lo), lo);
     c[1] = gl::ksub(gl::kadd(gl::kdbl(a2b), a2b), b);
     c[2] = gl::kadd(gl::kdbl(ab2), ab2);
-    c[3] = gl::kmul(b2, b);
+    c[3] = kmul_c<C>(b2, b);
 }
 
 __device__ __forceinline__ K eq_lin(K a, K b) {  // (1 - a)(1 - b) + a b
-    return gl::kadd(gl::kmul(gl::ksub(gl::kone(), a), gl::ksub(gl::kone(), b)), gl::kmul(a, b));
+    return gl::kadd(kmul_n(gl::ksub(gl::kone(), a), gl::ksub(gl::kone(), b)), kmul_n(a, b));
 }
 
 // chi_{pts[0..n)}(b)
 __device__ __forceinline__ K chi_of(const K* pts, int n, uint32_t b) {
     K w = gl::kone();
-    for (int i = 0; i < n; i++) w = gl::kmul(w, ((b >> i) & 1) ? pts[i] : gl::ksub(gl::kone(), pts[i]));
+    for (int i = 0; i < n; i++) w = kmul_n(w, ((b >> i) & 1) ? pts[i] : gl::ksub(gl::kone(), pts[i]));
     return w;
 }
 
 // block sum of v[0..n) into rec[0..n), zeros in rec[n..REC); n <= REC
-__device__ __forceinline__ void block_sum_rec(K* v, int n, K* rec) {
+__device__ __forceinline__ void block_sum_rec(const K* v, int n, K* rec) {
     __shared__ K s_red[FR / 32][REC];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll 1
     for (int d = 0; d < n; d++) {
         K x = v[d];
 #pragma unroll
@@ -182,28 +204,66 @@ __device__ __forceinline__ void block_sum_rec(K* v, int n, K* rec) {
     if (threadIdx.x < REC) {
         K x = gl::kzero();
         if ((int)threadIdx.x < n)
-            for (int w = 0; w < (int)(blockDim.x >> 5); w++) x = gl::kadd(x, s_red[w][threadIdx.x]);
-        rec[threadIdx.x] = x;
+            for (int w = 0; w < FR / 32; w++) x = gl::kadd(x, s_red[w][threadIdx.x]);
+        st_k(rec + threadIdx.x, x);
     }
 }
 
-struct MomArgs {
-    const K* H;        // [NPAT]
-    int j;             // 0, 1 or 2
-    const K* chals;    // device row challenges r_0..r_{j-1}
-    K beta1, beta2;    // beta_r[1], beta_r[2]
-    K* partials;       // records [part_off + blockIdx.x]
-    uint32_t part_off;
+// One row round is one launch of ccs_fast_round_kernel: its blocks take one
+// of three roles, in this order, and each writes one partial record:
+//   moment blocks (rounds 0..2): sum_P H[P] F_j(P, X), one thread per pattern;
+//   small-table blocks: fold the f-variable / eq_rin / eval tables, add
+//     E_j(t) f_t(X) to S and eq_rin_t(X) eval_t(X) to V, one thread per pair;
+//   NC blocks (rounds >= 3): E_j(t) sum_q wg_q N(y_{q,t}(X)) over a q chunk,
+//     one thread per (pair, chunk).
+// The last block to finish (an atomic ticket) sums the records and writes the
+// round's coefficients C_j eq(beta_j, X) S(X) + gamma^k V(X).
+struct FastRoundArgs {
+    int j;
+    uint32_t n_mom, n_small;     // blocks of the first two roles; the rest are NC blocks
+    // moments
+    const unsigned long long* H64;
+    K beta1, beta2;              // beta_r[1], beta_r[2]
+    // small tables: f variables at slots 1..n_fvar, eq_rin / eval at idx_eqrin / idx_eval
+    const K* small_in;
+    K* small_out;
+    uint64_t small_len_in, small_len_out;
+    int fold;
+    K r;                         // r_{j-1}
+    int n_small_tab;
+    int idx_eqrin, idx_eval;
+    FTerms f;
+    int fdeg;                    // degree of f (<= MAX_DEG - 1)
+    const K* E;                  // E_j [pairs]
+    uint64_t pairs;
+    // NC
+    const K* chals;              // device r_0..r_{j-1}
+    const int8_t* Z;             // [nq][m]
+    uint64_t m;
+    const K* nc_in;              // T_{j-1} [nq][nc_len_in] (rounds >= 5)
+    uint64_t nc_len_in;
+    K* nc_out;                   // T_j [nq][nc_len_out] (rounds 4.., null in the last round)
+    uint64_t nc_len_out;
+    const K* wg;                 // [nq]
+    uint32_t nq, q_chunk, n_chunk;
+    // reduction
+    K* partials;                 // [gridDim.x][REC]
+    unsigned int* ticket;        // zero between launches (atomicInc wraps it)
+    int ncoef;
+    K beta[32];                  // beta_r
+    K gamma_to_k;
+    K* Cs;                       // [ell]: C_j of each round (written by round j)
+    K* coeffs_out;               // [ncoef]
 };
 
-// Rounds 0..2: sum_P H[P] F_j(P, X) (one thread per canonical pattern).
-__global__ void __launch_bounds__(FR) ccs_mom_round_kernel(const MomArgs a) {
-    K c[REC];
-#pragma unroll
-    for (int d = 0; d < REC; d++) c[d] = gl::kzero();
-    const int p = blockIdx.x * FR + threadIdx.x;
+// The roles and the final reduction run as out-of-line functions with rolled
+// loops: a launch of a late round has few warps, and long straight-line
+// K-multiplication code there stalls on instruction fetch.
+__device__ __noinline__ void mom_role(const FastRoundArgs& a, uint32_t blk, K* rec) {
+    K c[4] = {gl::kzero(), gl::kzero(), gl::kzero(), gl::kzero()};
+    const int p = blk * FR + threadIdx.x;
     if (p < NPAT) {
-        const K h = a.H[p];
+        const K h = hist_value(a.H64, p);
         if (!gl::kiszero(h)) {
             int tr[8];
             int P = p + NPAT + 1;
@@ -211,12 +271,13 @@ __global__ void __launch_bounds__(FR) ccs_mom_round_kernel(const MomArgs a) {
             for (int i = 0; i < 8; i++) { tr[i] = P % 3 - 1; P /= 3; }
             K F[4] = {gl::kzero(), gl::kzero(), gl::kzero(), gl::kzero()};
             if (a.j == 0) {
-                // digits of pair s: lo = tr[2s], hi = tr[2s + 1]; weight chi_{beta1, beta2}(s)
+                // pair s: lo = tr[2s], hi = tr[2s + 1] (small integers); weight chi_{beta1, beta2}(s)
+#pragma unroll
                 for (int s = 0; s < 4; s++) {
                     const int lo = tr[2 * s], b = tr[2 * s + 1] - lo;
                     const int n1 = b * (3 * lo * lo - 1), n2 = 3 * lo * b * b, n3 = b * b * b;
                     if (!(n1 | n2 | n3)) continue;
-                    const K ws = gl::kmul((s & 1) ? a.beta1 : gl::ksub(gl::kone(), a.beta1),
+                    const K ws = kmul_n((s & 1) ? a.beta1 : gl::ksub(gl::kone(), a.beta1),
                                           (s & 2) ? a.beta2 : gl::ksub(gl::kone(), a.beta2));
                     F[1] = gl::kadd(F[1], gl::kscale_small(ws, n1));
                     F[2] = gl::kadd(F[2], gl::kscale_small(ws, n2));
@@ -234,65 +295,36 @@ __global__ void __launch_bounds__(FR) ccs_mom_round_kernel(const MomArgs a) {
                         if (dh) hi = dh > 0 ? gl::kadd(hi, w[b]) : gl::ksub(hi, w[b]);
                     }
                     K n[4];
-                    n_coeffs(lo, hi, n);
+                    n_coeffs<true>(lo, hi, n);
                     if (j == 1) {
                         const K ws = s ? a.beta2 : gl::ksub(gl::kone(), a.beta2);
-                        for (int d = 0; d < 4; d++) F[d] = gl::kadd(F[d], gl::kmul(ws, n[d]));
+                        for (int d = 0; d < 4; d++) F[d] = gl::kadd(F[d], kmul_n(ws, n[d]));
                     } else {
                         for (int d = 0; d < 4; d++) F[d] = n[d];
                     }
                 }
             }
-            for (int d = 0; d < 4; d++) c[d] = gl::kmul(h, F[d]);
+            for (int d = 0; d < 4; d++) c[d] = kmul_n(h, F[d]);
         }
     }
-    block_sum_rec(c, 4, a.partials + (uint64_t)(a.part_off + blockIdx.x) * REC);
+    block_sum_rec(c, 4, rec);
 }
 
-struct FastRowArgs {
-    // small tables: f variables at slots 1..n_fvar, eq_rin / eval at idx_eqrin / idx_eval
-    const K* small_in;
-    K* small_out;
-    uint64_t small_len_in, small_len_out;
-    int fold;
-    K r;               // r_{j-1} (fold)
-    int n_small;
-    int idx_eqrin, idx_eval;
-    FTerms f;
-    int fdeg;          // degree of f (<= MAX_DEG - 1)
-    const K* E;        // E_j [pairs]
-    // NC
-    int j;
-    const K* chals;    // device r_0..r_{j-1}
-    const int8_t* Z;   // [nq][m] (modes 3, 4)
-    uint64_t m;
-    const K* nc_in;    // mode 5: T_{j-1} [nq][nc_len_in]
-    uint64_t nc_len_in;
-    K* nc_out;         // modes 4, 5: T_j [nq][nc_len_out] (null in the last round)
-    uint64_t nc_len_out;
-    const K* wg;       // [nq]
-    uint32_t nq, q_chunk, n_chunk;
-    uint64_t pairs;
-    K* partials;
-    uint32_t part_off;
-};
-
-// Small tables of one row round: fold (rounds >= 1), f_t(X) and the eval
-// term, for every pair t (one thread each).  Adds E_j(t) f_t(X) to S and
-// eq_rin_t(X) eval_t(X) to V.
-__global__ void __launch_bounds__(FR) ccs_fast_small_kernel(const FastRowArgs a) {
+__device__ __noinline__ void small_role(const FastRoundArgs& a, uint32_t blk, K* rec) {
     K out[REC];
 #pragma unroll
     for (int d = 0; d < REC; d++) out[d] = gl::kzero();
-    const uint64_t t = blockIdx.x * (uint64_t)FR + threadIdx.x;
+    const uint64_t t = blk * (uint64_t)FR + threadIdx.x;
     if (t < a.pairs) {
         K lo_s[2 + MAX_FVAR + 2], hi_s[2 + MAX_FVAR + 2];
-        for (int s = 1; s < a.n_small; s++) {
+#pragma unroll
+        for (int s = 1; s < 2 + MAX_FVAR + 2; s++) {
+            if (s >= a.n_small_tab) break;
             K lo, hi;
             if (a.fold) {
                 const K* in = a.small_in + (uint64_t)s * a.small_len_in + 4 * t;
-                lo = gl::klerp(ld_k(in), ld_k(in + 1), a.r);
-                hi = gl::klerp(ld_k(in + 2), ld_k(in + 3), a.r);
+                lo = klerp_c<true>(ld_k(in), ld_k(in + 1), a.r);
+                hi = klerp_c<true>(ld_k(in + 2), ld_k(in + 3), a.r);
                 if (a.small_out) {
                     K* o = a.small_out + (uint64_t)s * a.small_len_out + 2 * t;
                     st_k(o, lo);
@@ -306,62 +338,59 @@ __global__ void __launch_bounds__(FR) ccs_fast_small_kernel(const FastRowArgs a)
             lo_s[s] = lo;
             hi_s[s] = hi;
         }
-        K S[MAX_DEG];
-#pragma unroll
+        // f_t(X) = sum_terms coeff prod_v (a_v + b_v X)^exp, degree <= fdeg
+        K S[MAX_DEG], tp[MAX_DEG];
+#pragma unroll 1
         for (int d = 0; d < MAX_DEG; d++) S[d] = gl::kzero();
+#pragma unroll 1
         for (int tt = 0; tt < a.f.n_terms; tt++) {
-            K tp[MAX_DEG];
-#pragma unroll
+#pragma unroll 1
             for (int d = 0; d < MAX_DEG; d++) tp[d] = gl::kzero();
             tp[0] = a.f.coeff[tt];
+            int deg = 0;  // degree of tp so far
+#pragma unroll 1
             for (int vv = 0; vv < a.f.n_vars[tt]; vv++) {
                 const int pos = a.f.var_pos[tt][vv];
                 const K av = lo_s[1 + pos], bv = gl::ksub(hi_s[1 + pos], av);
-                for (int e = 0; e < a.f.var_exp[tt][vv]; e++) {
-                    K prev = gl::kzero();
-#pragma unroll
-                    for (int d = 0; d < MAX_DEG; d++) {
-                        if (d <= a.fdeg) {
-                            const K old = tp[d];
-                            tp[d] = gl::kadd(gl::kmul(av, old), gl::kmul(bv, prev));
-                            prev = old;
-                        }
-                    }
+#pragma unroll 1
+                for (int e = 0; e < a.f.var_exp[tt][vv] && deg < a.fdeg; e++) {
+                    deg++;
+                    tp[deg] = kmul_n(bv, tp[deg - 1]);
+#pragma unroll 1
+                    for (int d = deg - 1; d >= 1; d--) tp[d] = gl::kadd(kmul_n(av, tp[d]), kmul_n(bv, tp[d - 1]));
+                    tp[0] = kmul_n(av, tp[0]);
                 }
             }
-#pragma unroll
-            for (int d = 0; d < MAX_DEG; d++) S[d] = gl::kadd(S[d], tp[d]);
+#pragma unroll 1
+            for (int d = 0; d <= deg; d++) S[d] = gl::kadd(S[d], tp[d]);
         }
         const K e = a.E[t];
+#pragma unroll 1
+        for (int d = 0; d <= a.fdeg; d++) S[d] = kmul_n(e, S[d]);
 #pragma unroll
-        for (int d = 0; d < MAX_DEG; d++)
-            if (d <= a.fdeg) out[d] = gl::kmul(e, S[d]);
+        for (int d = 0; d < MAX_DEG; d++) out[d] = d <= a.fdeg ? S[d] : gl::kzero();
         if (a.idx_eval >= 0) {
             const K r0 = lo_s[a.idx_eqrin], r1 = gl::ksub(hi_s[a.idx_eqrin], r0);
             const K v0 = lo_s[a.idx_eval], v1 = gl::ksub(hi_s[a.idx_eval], v0);
-            out[MAX_DEG] = gl::kmul(r0, v0);
-            out[MAX_DEG + 1] = gl::kadd(gl::kmul(r0, v1), gl::kmul(r1, v0));
-            out[MAX_DEG + 2] = gl::kmul(r1, v1);
+            out[MAX_DEG] = kmul_n(r0, v0);
+            out[MAX_DEG + 1] = gl::kadd(kmul_n(r0, v1), kmul_n(r1, v0));
+            out[MAX_DEG + 2] = kmul_n(r1, v1);
         }
     }
-    block_sum_rec(out, REC, a.partials + (uint64_t)(a.part_off + blockIdx.x) * REC);
+    block_sum_rec(out, REC, rec);
 }
 
-// NC term of row rounds >= 3: MODE 3 / 4 stream 16- / 32-row digit blocks,
-// MODE 5 folds the K table.  Thread = (pair t, q chunk c), t fastest; adds
-// E_j(t) sum_{q in chunk} wg_q N(y_{q,t}(X)) to S.
-template <int MODE>
-__global__ void __launch_bounds__(FR, 2) ccs_fast_nc_kernel(const FastRowArgs a) {
+template <int MODE, bool C>
+__device__ __forceinline__ void nc_role(const FastRoundArgs& a, uint32_t blk, K* rec, K* s_wg) {
     constexpr int NLUT = MODE == 3 ? 2 : (MODE == 4 ? 4 : 0);
     __shared__ K s_lut[NLUT ? NLUT * 81 : 1];
     __shared__ K s_w[16];
-    extern __shared__ K s_wg[];  // [nq]
-    const uint64_t gid = blockIdx.x * (uint64_t)FR + threadIdx.x;
+    const uint64_t gid = blk * (uint64_t)FR + threadIdx.x;
     const bool live = gid < a.pairs * a.n_chunk;
     const uint64_t t = live ? gid % a.pairs : 0;
     const uint32_t c = live ? (uint32_t)(gid / a.pairs) : 0;
     if constexpr (NLUT > 0) {
-        if (threadIdx.x < (1 << a.j)) s_w[threadIdx.x] = chi_of(a.chals, a.j, threadIdx.x);
+        if (threadIdx.x < (1u << a.j)) s_w[threadIdx.x] = chi_of(a.chals, a.j, threadIdx.x);
         __syncthreads();
         for (int e = threadIdx.x; e < NLUT * 81; e += FR) {
             const int g = e / 81;
@@ -378,24 +407,44 @@ __global__ void __launch_bounds__(FR, 2) ccs_fast_nc_kernel(const FastRowArgs a)
     for (uint32_t q = threadIdx.x; q < a.nq; q += FR) s_wg[q] = a.wg[q];
     __syncthreads();
 
-    K out[4];
-#pragma unroll
-    for (int d = 0; d < 4; d++) out[d] = gl::kzero();
+    K out[4] = {gl::kzero(), gl::kzero(), gl::kzero(), gl::kzero()};
     if (live) {
         gl::KAcc acc[4];
 #pragma unroll
         for (int d = 0; d < 4; d++) gl::kacc_zero(acc[d]);
         const uint32_t q0 = c * a.q_chunk, q1 = min(a.nq, q0 + a.q_chunk);
+        // the next q's inputs are loaded before the current one is evaluated
+        uint4 nv = make_uint4(0, 0, 0, 0), nu = make_uint4(0, 0, 0, 0);
+        ulonglong2 nx[4];
+        auto fetch = [&](uint32_t q) {
+            if (q >= q1) return;
+            if constexpr (MODE == 3) {
+                nv = __ldg(reinterpret_cast<const uint4*>(a.Z + (uint64_t)q * a.m + 16 * t));
+            } else if constexpr (MODE == 4) {
+                const uint4* zp = reinterpret_cast<const uint4*>(a.Z + (uint64_t)q * a.m + 32 * t);
+                nv = __ldg(zp);
+                nu = __ldg(zp + 1);
+            } else {
+                const ulonglong2* in = reinterpret_cast<const ulonglong2*>(a.nc_in + (uint64_t)q * a.nc_len_in + 4 * t);
+#pragma unroll
+                for (int i = 0; i < 4; i++) nx[i] = __ldg(in + i);
+            }
+        };
+        fetch(q0);
         for (uint32_t q = q0; q < q1; q++) {
+            const uint4 cv = nv, cu = nu;
+            ulonglong2 cx[4];
+#pragma unroll
+            for (int i = 0; i < 4; i++) cx[i] = nx[i];
+            fetch(q + 1);
             K lo, hi;
             if constexpr (MODE == 3) {
-                const uint4 v = __ldg(reinterpret_cast<const uint4*>(a.Z + (uint64_t)q * a.m + 16 * t));
+                const uint4 v = cv;
                 if ((v.x | v.y | v.z | v.w) == 0) continue;
                 lo = gl::kadd(s_lut[p4_index(v.x)], s_lut[81 + p4_index(v.y)]);
                 hi = gl::kadd(s_lut[p4_index(v.z)], s_lut[81 + p4_index(v.w)]);
             } else if constexpr (MODE == 4) {
-                const uint4* zp = reinterpret_cast<const uint4*>(a.Z + (uint64_t)q * a.m + 32 * t);
-                const uint4 v = __ldg(zp), u = __ldg(zp + 1);
+                const uint4 v = cv, u = cu;
                 const bool zero = (v.x | v.y | v.z | v.w | u.x | u.y | u.z | u.w) == 0;
                 if (zero) {
                     lo = hi = gl::kzero();
@@ -412,10 +461,10 @@ __global__ void __launch_bounds__(FR, 2) ccs_fast_nc_kernel(const FastRowArgs a)
                 }
                 if (zero) continue;
             } else {
-                const K* in = a.nc_in + (uint64_t)q * a.nc_len_in + 4 * t;
-                const K x0 = ld_k(in), x1 = ld_k(in + 1), x2 = ld_k(in + 2), x3 = ld_k(in + 3);
-                lo = gl::klerp(x0, x1, a.r);
-                hi = gl::klerp(x2, x3, a.r);
+                const K x0 = gl::kmk(cx[0].x, cx[0].y), x1 = gl::kmk(cx[1].x, cx[1].y);
+                const K x2 = gl::kmk(cx[2].x, cx[2].y), x3 = gl::kmk(cx[3].x, cx[3].y);
+                lo = klerp_c<C>(x0, x1, a.r);
+                hi = klerp_c<C>(x2, x3, a.r);
                 if (a.nc_out) {
                     K* o = a.nc_out + (uint64_t)q * a.nc_len_out + 2 * t;
                     st_k(o, lo);
@@ -424,7 +473,7 @@ __global__ void __launch_bounds__(FR, 2) ccs_fast_nc_kernel(const FastRowArgs a)
                 if (gl::kiszero(lo) && gl::kiszero(hi)) continue;
             }
             K n[4];
-            n_coeffs(lo, hi, n);
+            n_coeffs<C>(lo, hi, n);
             const K w = s_wg[q];
             const uint64_t w7 = gl::mul7(w.im);
 #pragma unroll
@@ -432,52 +481,81 @@ __global__ void __launch_bounds__(FR, 2) ccs_fast_nc_kernel(const FastRowArgs a)
         }
         const K e = a.E[t];
 #pragma unroll
-        for (int d = 0; d < 4; d++) out[d] = gl::kmul(e, gl::kacc_reduce(acc[d]));
+        for (int d = 0; d < 4; d++) out[d] = kmul_c<C>(e, gl::kacc_reduce(acc[d]));
     }
-    block_sum_rec(out, 4, a.partials + (uint64_t)(a.part_off + blockIdx.x) * REC);
+    block_sum_rec(out, 4, rec);
 }
 
-struct FastReduceArgs {
-    const K* partials;
-    uint32_t nrec;
-    int ncoef;          // deg_max + 1 coefficients written
-    int j;
-    const K* chals;     // device r_0..r_{j-1}
-    K beta[32];         // beta_r
-    K gamma_to_k;
-    K* coeffs_out;
-};
-
-// p_j(X) = C_j eq(beta_j, X) S(X) + gamma^k V(X), coefficients low -> high.
-__global__ void __launch_bounds__(256) ccs_fast_reduce_kernel(const FastReduceArgs a) {
-    __shared__ K s_sum[REC];
-    __shared__ K s_red[8];
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    for (int d = 0; d < REC; d++) {
-        K v = gl::kzero();
-        for (uint32_t b = threadIdx.x; b < a.nrec; b += blockDim.x) v = gl::kadd(v, a.partials[(uint64_t)b * REC + d]);
-        for (int o = 16; o > 0; o >>= 1) v = gl::kadd(v, shfl_xor_k(v, o));
-        if (lane == 0) s_red[warp] = v;
-        __syncthreads();
-        if (threadIdx.x == 0) {
-            K s = gl::kzero();
-            for (int w = 0; w < 8; w++) s = gl::kadd(s, s_red[w]);
-            s_sum[d] = s;
+// Sums the records of every block of the launch (run by the last block).
+__device__ __noinline__ void round_final_reduce(const FastRoundArgs& a) {
+    __shared__ K s_tot[FR / 32][REC];
+    K s[REC];
+#pragma unroll
+    for (int d = 0; d < REC; d++) s[d] = gl::kzero();
+    for (uint32_t r = threadIdx.x; r < gridDim.x; r += FR) {
+        const ulonglong2* p = reinterpret_cast<const ulonglong2*>(a.partials + (uint64_t)r * REC);
+#pragma unroll
+        for (int d = 0; d < REC; d++) {
+            const ulonglong2 v = __ldcg(p + d);
+            s[d] = gl::kadd(s[d], gl::kmk(v.x, v.y));
         }
-        __syncthreads();
     }
-    if (threadIdx.x == 0) {
-        K Cj = gl::kone();
-        for (int i = 0; i < a.j; i++) Cj = gl::kmul(Cj, eq_lin(a.beta[i], a.chals[i]));
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int d = 0; d < REC; d++) {
+        K x = s[d];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) x = gl::kadd(x, shfl_xor_k(x, o));
+        if (lane == 0) s_tot[warp][d] = x;
+    }
+    __syncthreads();
+    __shared__ K s_S[REC];
+    if (threadIdx.x < REC) {
+        K x = gl::kzero();
+#pragma unroll 1
+        for (int w = 0; w < FR / 32; w++) x = gl::kadd(x, s_tot[w][threadIdx.x]);
+        s_S[threadIdx.x] = x;
+    }
+    __syncthreads();
+    if (threadIdx.x < (unsigned)a.ncoef) {
+        // C_j eq(beta_j, X) = e0 + e1 X; coefficient d = e0 S_d + e1 S_{d-1} + gamma^k V_d
+        // C_j = C_{j-1} eq(beta_{j-1}, r_{j-1}), C_0 = 1; kept on the device per round
+        const K Cj = a.j == 0 ? gl::kone() : kmul_n(ld_k(a.Cs + a.j - 1), eq_lin(a.beta[a.j - 1], a.chals[a.j - 1]));
+        if (threadIdx.x == 0) st_k(a.Cs + a.j, Cj);
         const K bj = a.beta[a.j];
-        const K e0 = gl::kmul(Cj, gl::ksub(gl::kone(), bj));            // eq(beta_j, X) C_j = e0 + e1 X
-        const K e1 = gl::kmul(Cj, gl::ksub(gl::kdbl(bj), gl::kone()));
-        for (int d = 0; d < a.ncoef; d++) {
-            K v = gl::kzero();
-            if (d < MAX_DEG) v = gl::kmul(e0, s_sum[d]);
-            if (d >= 1 && d - 1 < MAX_DEG) v = gl::kadd(v, gl::kmul(e1, s_sum[d - 1]));
-            if (d < 3) v = gl::kadd(v, gl::kmul(a.gamma_to_k, s_sum[MAX_DEG + d]));
-            a.coeffs_out[d] = v;
-        }
+        const K e0 = kmul_n(Cj, gl::ksub(gl::kone(), bj));
+        const K e1 = kmul_n(Cj, gl::ksub(gl::kdbl(bj), gl::kone()));
+        const int d = threadIdx.x;
+        K v = gl::kzero();
+        if (d < MAX_DEG) v = kmul_n(e0, s_S[d]);
+        if (d >= 1 && d - 1 < MAX_DEG) v = gl::kadd(v, kmul_n(e1, s_S[d - 1]));
+        if (d < 3) v = gl::kadd(v, kmul_n(a.gamma_to_k, s_S[MAX_DEG + d]));
+        st_k(a.coeffs_out + d, v);
+    }
+}
+
+// MODE 0: rounds 0..2 (moment and small-table blocks); 3 / 4: stream 16- /
+// 32-row digit blocks; 5: fold the K table.
+template <int MODE, bool C>
+__global__ void __launch_bounds__(FR, 2) ccs_fast_round_kernel(const __grid_constant__ FastRoundArgs a) {
+    extern __shared__ K s_wg[];  // [nq] for NC blocks
+    const uint32_t b = blockIdx.x;
+    K* rec = a.partials + (uint64_t)b * REC;
+    if (b < a.n_mom) {
+        mom_role(a, b, rec);
+    } else if (b < a.n_mom + a.n_small) {
+        small_role(a, b - a.n_mom, rec);
+    } else {
+        if constexpr (MODE != 0) nc_role<MODE, C>(a, b - a.n_mom - a.n_small, rec, s_wg);
+    }
+    // the record is written by threads < REC; publish it, then take a ticket
+    __threadfence();
+    __syncthreads();
+    __shared__ unsigned int s_last;
+    if (threadIdx.x == 0) s_last = atomicInc(a.ticket, gridDim.x - 1) == gridDim.x - 1;
+    __syncthreads();
+    if (s_last) {
+        __threadfence();
+        round_final_reduce(a);
     }
 }

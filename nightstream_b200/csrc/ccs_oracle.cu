@@ -21,6 +21,7 @@
 //    makes them order-independent anyway).
 #include "internal.cuh"
 #include <algorithm>
+#include <cstdlib>
 #include <memory>
 
 using gl::K;
@@ -669,10 +670,13 @@ struct neo_gpu_ccs_oracle {
     // ternary-digit path (ccs_fast.cuh): E tables, the 8-row pattern histogram
     bool fast = false;
     DevBuf<K> E_all;            // E_j = chi_{beta_{j+1..}} at offset 2^ell - 2^(ell - j), j < ell
-    DevBuf<K> hist;             // [NPAT]
-    DevBuf<uint32_t> hist_part; // [hist blocks][NPAT][8]
+    DevBuf<uint64_t> hist64;    // [8][NPAT] limb sums of the pattern histogram
+    DevBuf<uint32_t> hist_part; // [hist blocks][8][NPAT]
     DevBuf<uint32_t> tern_flag;
+    DevBuf<uint32_t> ticket;    // last-block ticket of the fused round kernel
+    DevBuf<K> Cs;               // C_j = prod_{i<j} eq(beta_i, r_i) per row round
     uint32_t hist_gx = 0, hist_gy = 0, hist_qc = 0;
+    uint32_t compact_q = 8;     // q per thread below which the NC blocks use out-of-line K products
     K gamma{}, gamma_to_k{};
     std::vector<K> alpha, beta_a, beta_r, r_in, row_chals, ajtai_chals;
     bool has_inputs = false, has_eval = false;
@@ -934,24 +938,22 @@ static int oracle_init(neo_gpu_ctx* ctx, neo_gpu_ccs_oracle* o, const int8_t* d_
     return NEO_OK;
 }
 
-// Grid of the fast row kernel at round j: (pair, q chunk) threads, enough to
+// Grid of the NC blocks at round j >= 3: (pair, q chunk) threads, enough to
 // fill the GPU about twice when the pairs alone do not.
-static void fast_rows_grid(const neo_gpu_ccs_oracle* o, uint32_t j, uint64_t* pairs, uint32_t* n_chunk,
-                           uint32_t* q_chunk, uint32_t* blocks) {
+static void fast_nc_grid(const neo_gpu_ccs_oracle* o, uint32_t j, uint32_t* n_chunk, uint32_t* q_chunk,
+                         uint32_t* blocks) {
     const uint32_t nq = o->k * NEO_D;
-    *pairs = o->n_pad >> (j + 1);
-    uint32_t nc = 1;
-    if (j >= 3) {
-        const uint64_t target = 148ull * 2 * FR * 2;
-        nc = (uint32_t)std::min<uint64_t>(nq, std::max<uint64_t>(1, (target + *pairs - 1) / *pairs));
-    }
+    const uint64_t pairs = o->n_pad >> (j + 1);
+    const uint64_t target = 148ull * 2 * FR * 2;
+    const uint32_t nc = (uint32_t)std::min<uint64_t>(nq, std::max<uint64_t>(1, (target + pairs - 1) / pairs));
     *q_chunk = (nq + nc - 1) / nc;
     *n_chunk = (nq + *q_chunk - 1) / *q_chunk;
-    *blocks = (uint32_t)ceil_div(*pairs * *n_chunk, FR);
+    *blocks = (uint32_t)ceil_div(pairs * *n_chunk, FR);
 }
 
 static int fast_setup(neo_gpu_ccs_oracle* o) {
     neo_gpu_ctx* ctx = o->ctx;
+    if (const char* e = getenv("NEO_TUNE_CCS_COMPACT_Q")) o->compact_q = (uint32_t)strtoul(e, nullptr, 10);
     const uint32_t ell = o->ell_n, nq = o->k * NEO_D;
     // E_j = chi of beta_r[j+1..ell) for every row round (beta_r is in ws_bits[0..ell))
     NEO_CK(ctx, o->E_all.ensure(o->n_pad));
@@ -963,18 +965,25 @@ static int fast_setup(neo_gpu_ccs_oracle* o) {
     // histogram grid: a thread per 8-row block, q chunks so that ~2 blocks per SM
     const uint32_t n_t8 = (uint32_t)(o->n_pad >> 3);
     o->hist_gx = (uint32_t)ceil_div(n_t8, HIST_T);
-    uint32_t gy = std::max<uint32_t>(1, (296 + o->hist_gx - 1) / o->hist_gx);
+    uint32_t gy = std::max<uint32_t>(1, 296 / o->hist_gx);  // one wave of 2 blocks per SM when it fits
     o->hist_qc = std::max<uint32_t>(1, std::min<uint32_t>(HIST_MAX_Q, (nq + gy - 1) / gy));
     o->hist_gy = (nq + o->hist_qc - 1) / o->hist_qc;
     NEO_CK(ctx, o->hist_part.ensure((size_t)o->hist_gx * o->hist_gy * NPAT * HIST_LIMBS));
-    NEO_CK(ctx, o->hist.ensure(NPAT));
+    NEO_CK(ctx, o->hist64.ensure((size_t)NPAT * 8));
+    NEO_CK(ctx, o->ticket.ensure(1));
+    NEO_CK(ctx, o->Cs.ensure(ell));
+    NEO_CK(ctx, cudaMemsetAsync(o->ticket.p, 0, 4, ctx->stream));
     // partial records: the largest round
     uint64_t recs = 0;
     for (uint32_t j = 0; j < ell; j++) {
-        uint64_t pairs;
-        uint32_t nc, qc, blocks;
-        fast_rows_grid(o, j, &pairs, &nc, &qc, &blocks);
-        recs = std::max<uint64_t>(recs, blocks + ceil_div(pairs, FR) + ceil_div(NPAT, FR));
+        uint64_t r = ceil_div(o->n_pad >> (j + 1), FR);
+        if (j <= 2) r += ceil_div(NPAT, FR);
+        if (j >= 3) {
+            uint32_t nc, qc, blocks;
+            fast_nc_grid(o, j, &nc, &qc, &blocks);
+            r += blocks;
+        }
+        recs = std::max<uint64_t>(recs, r);
     }
     NEO_CK(ctx, o->partials.ensure(recs * REC));
     static SmemLimit hist_smem;
@@ -982,13 +991,13 @@ static int fast_setup(neo_gpu_ccs_oracle* o) {
     return NEO_OK;
 }
 
-// One row round on the ternary-digit path; leaves deg_max + 1 coefficients in
-// coeffs_dst (device).  d_chals must hold r_0..r_{j-1}.
+// One row round on the ternary-digit path (one launch; round 0 first builds
+// the pattern histogram); leaves deg_max + 1 coefficients in coeffs_dst
+// (device).  d_chals must hold r_0..r_{j-1}.
 static int fast_round_launch(neo_gpu_ccs_oracle* o, K* coeffs_dst) {
     neo_gpu_ctx* ctx = o->ctx;
     const uint32_t j = o->round_idx, ell = o->ell_n, nq = o->k * NEO_D;
     const bool last = j + 1 == ell;
-    uint32_t nrec = 0;
     if (j == 0) {
         HistArgs h{};
         h.Z = o->Z;
@@ -1002,25 +1011,19 @@ static int fast_round_launch(neo_gpu_ccs_oracle* o, K* coeffs_dst) {
         const size_t smem = (size_t)NPAT * HIST_LIMBS * 4 + (size_t)o->hist_qc * sizeof(K);
         ccs_hist_kernel<<<dim3(o->hist_gx, o->hist_gy), HIST_T, smem, ctx->stream>>>(h);
         NEO_LAUNCHED(ctx);
-        ccs_hist_reduce_kernel<<<ceil_div(NPAT, 32), 256, 0, ctx->stream>>>(o->hist_part.p, o->hist_gx * o->hist_gy,
-                                                                           o->hist.p);
+        NEO_CK(ctx, cudaMemsetAsync(o->hist64.p, 0, o->hist64.bytes(), ctx->stream));
+        const uint32_t nblk = o->hist_gx * o->hist_gy;
+        ccs_hist_sum_kernel<<<dim3((uint32_t)ceil_div(NPAT * HIST_LIMBS, 256), (uint32_t)ceil_div(nblk, HIST_SUM_SLICE)), 256, 0,
+                              ctx->stream>>>(o->hist_part.p, nblk,
+                                             reinterpret_cast<unsigned long long*>(o->hist64.p));
         NEO_LAUNCHED(ctx);
     }
-    if (j <= 2) {
-        MomArgs ma{};
-        ma.H = o->hist.p;
-        ma.j = (int)j;
-        ma.chals = o->d_chals.p;
-        ma.beta1 = o->beta_r[1];
-        ma.beta2 = o->beta_r[2];
-        ma.partials = o->partials.p;
-        ma.part_off = 0;
-        const uint32_t nb = (uint32_t)ceil_div(NPAT, FR);
-        ccs_mom_round_kernel<<<nb, FR, 0, ctx->stream>>>(ma);
-        NEO_LAUNCHED(ctx);
-        nrec = nb;
-    }
-    FastRowArgs a{};
+    FastRoundArgs a{};
+    a.j = (int)j;
+    a.n_mom = j <= 2 ? (uint32_t)ceil_div(NPAT, FR) : 0;
+    a.H64 = reinterpret_cast<const unsigned long long*>(o->hist64.p);
+    a.beta1 = o->beta_r[1];
+    a.beta2 = o->beta_r[2];
     if (j == 0) {
         a.small_in = o->small[0].p;
         a.small_len_in = o->n_pad;
@@ -1033,32 +1036,22 @@ static int fast_round_launch(neo_gpu_ccs_oracle* o, K* coeffs_dst) {
         a.small_out = last ? nullptr : o->small[o->small_cur ^ 1].p;
         a.small_len_out = o->n_pad >> j;
     }
-    a.n_small = o->n_small;
+    a.n_small_tab = o->n_small;
     a.idx_eqrin = o->idx_eqrin;
     a.idx_eval = o->idx_eval;
     a.f = o->f;
     a.fdeg = o->deg_max - 1;
     a.E = o->E_all.p + (o->n_pad - (o->n_pad >> j));
-    a.j = (int)j;
+    a.pairs = o->n_pad >> (j + 1);
+    a.n_small = (uint32_t)ceil_div(a.pairs, FR);
     a.chals = o->d_chals.p;
     a.Z = o->Z;
     a.m = o->m;
     a.wg = o->wg.p;
     a.nq = nq;
-    a.partials = o->partials.p;
-    // small tables: one thread per pair
-    a.pairs = o->n_pad >> (j + 1);
-    a.part_off = nrec;
-    const uint32_t sblocks = (uint32_t)ceil_div(a.pairs, FR);
-    ccs_fast_small_kernel<<<sblocks, FR, 0, ctx->stream>>>(a);
-    NEO_LAUNCHED(ctx);
-    nrec += sblocks;
+    uint32_t nc_blocks = 0;
     if (j >= 3) {
-        uint32_t nc, qc, blocks;
-        fast_rows_grid(o, j, &a.pairs, &nc, &qc, &blocks);
-        a.n_chunk = nc;
-        a.q_chunk = qc;
-        a.part_off = nrec;
+        fast_nc_grid(o, j, &a.n_chunk, &a.q_chunk, &nc_blocks);
         if (j == 4 && !last) {
             a.nc_out = o->nc[0].p;
             a.nc_len_out = o->n_pad >> 4;
@@ -1071,26 +1064,32 @@ static int fast_round_launch(neo_gpu_ccs_oracle* o, K* coeffs_dst) {
                 a.nc_len_out = o->n_pad >> j;
             }
         }
-        const size_t wsm = (size_t)nq * sizeof(K);
-        if (j == 3) ccs_fast_nc_kernel<3><<<blocks, FR, wsm, ctx->stream>>>(a);
-        else if (j == 4) ccs_fast_nc_kernel<4><<<blocks, FR, wsm, ctx->stream>>>(a);
-        else ccs_fast_nc_kernel<5><<<blocks, FR, wsm, ctx->stream>>>(a);
-        NEO_LAUNCHED(ctx);
-        nrec += blocks;
     }
+    a.partials = o->partials.p;
+    a.ticket = o->ticket.p;
+    a.ncoef = o->deg_max + 1;
+    for (uint32_t i = 0; i < ell && i < 32; i++) a.beta[i] = o->beta_r[i];
+    a.gamma_to_k = o->gamma_to_k;
+    a.Cs = o->Cs.p;
+    a.coeffs_out = coeffs_dst;
+    const uint32_t blocks = a.n_mom + a.n_small + nc_blocks;
+    const size_t wsm = j >= 3 ? (size_t)nq * sizeof(K) : 0;
+    // a thread that evaluates few q runs its K products out of line (compact code)
+    const bool compact = j >= 3 && a.q_chunk < o->compact_q;
+    if (j <= 2) ccs_fast_round_kernel<0, true><<<blocks, FR, 0, ctx->stream>>>(a);
+    else if (j == 3) {
+        if (compact) ccs_fast_round_kernel<3, true><<<blocks, FR, wsm, ctx->stream>>>(a);
+        else ccs_fast_round_kernel<3, false><<<blocks, FR, wsm, ctx->stream>>>(a);
+    } else if (j == 4) {
+        if (compact) ccs_fast_round_kernel<4, true><<<blocks, FR, wsm, ctx->stream>>>(a);
+        else ccs_fast_round_kernel<4, false><<<blocks, FR, wsm, ctx->stream>>>(a);
+    } else {
+        if (compact) ccs_fast_round_kernel<5, true><<<blocks, FR, wsm, ctx->stream>>>(a);
+        else ccs_fast_round_kernel<5, false><<<blocks, FR, wsm, ctx->stream>>>(a);
+    }
+    NEO_LAUNCHED(ctx);
     if (j > 0 && !last) o->small_cur ^= 1;
     if (j >= 5 && !last) o->nc_cur ^= 1;
-    FastReduceArgs r{};
-    r.partials = o->partials.p;
-    r.nrec = nrec;
-    r.ncoef = o->deg_max + 1;
-    r.j = (int)j;
-    r.chals = o->d_chals.p;
-    for (uint32_t i = 0; i < ell && i < 32; i++) r.beta[i] = o->beta_r[i];
-    r.gamma_to_k = o->gamma_to_k;
-    r.coeffs_out = coeffs_dst;
-    ccs_fast_reduce_kernel<<<1, 256, 0, ctx->stream>>>(r);
-    NEO_LAUNCHED(ctx);
     return NEO_OK;
 }
 

@@ -120,7 +120,8 @@ def _run_both(ctx, ell, k, inputs, seed=7):
     g.close()
 
 
-@pytest.mark.parametrize("ell,k,inputs", [(1, 1, False), (3, 2, True), (6, 1, False), (10, 13, True), (12, 3, True)])
+@pytest.mark.parametrize("ell,k,inputs", [(1, 1, False), (3, 2, True), (4, 2, True), (5, 3, False), (6, 1, False),
+                                          (10, 13, True), (12, 3, True)])
 def test_ccs_oracle_all_rounds_match(ctx, ell, k, inputs):
     _run_both(ctx, ell, k, inputs)
 

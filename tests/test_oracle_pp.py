@@ -42,3 +42,17 @@ def test_setup_par_partition(m):
     assert np.array_equal(pp.reshape(-1), ref)
     # row 0 of setup_par differs from setup (the stream is partitioned)
     assert not np.array_equal(pp[0], oracle.pp_setup(SEED, kappa, m, 0)[0])
+
+
+def test_chacha8_block_matches_published_vector():
+    """ChaCha with 8 rounds, 256-bit all-zero key, zero nonce and counter: the
+    first 64 keystream bytes of the published test vector TC1
+    (draft-strombergson-chacha-test-vectors-01, 8 rounds).  rand_chacha's
+    ChaCha8Rng::from_seed([0; 32]) returns these bytes as its first eight
+    next_u64 values (little-endian), so this pins the block function, the key
+    layout and the word order the PP sampler and the Poseidon2 constants use."""
+    tc1 = bytes.fromhex(
+        "3e00ef2f895f40d67f5bb8e81f09a5a12c840ec3ce9a7f3b181be188ef711a1e"
+        "984ce172b9216f419f445367456d5619314a42a3da86b001387bfdb80e0cfe42")
+    v = oracle.chacha8_sample([bytes(32)], [8], (1 << 64) - 1)
+    assert b"".join(int(x).to_bytes(8, "little") for x in v) == tc1
