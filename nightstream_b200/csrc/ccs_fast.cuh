@@ -83,15 +83,18 @@ struct HistArgs {
     uint32_t n_t8;     // m / 8
     uint32_t q_chunk;  // q per block (<= HIST_MAX_Q)
     const K* wg;       // [nq]
-    const K* E8;       // E_2, [n_t8]
-    uint32_t* partial; // [gridDim.y][gridDim.x][HIST_LIMBS][NPAT]
+    const K* Ew;       // split: E_3 [n_t8 / 2] (weight of block t8 is Ew[t8 >> 1]); else E_2 [n_t8]
+    int split;         // blockIdx.z = parity of t8: one histogram per parity
+    uint32_t* partial; // [gridDim.z][gridDim.y][gridDim.x][HIST_LIMBS][NPAT]
 };
 
 // One thread per 8-row block t8, a range of q per block.  Each nonzero
-// (q, t8) adds +-E_2(t8) wg_q to its pattern's counters: eight 16-bit limbs
+// (q, t8) adds +-w(t8) wg_q to its pattern's counters: eight 16-bit limbs
 // (re: 0..3, im: 4..7) in u32 shared-memory counters, at most 65536 adds per
 // block so no counter overflows.  The counters are limb-major, so the lanes
-// of a warp (random patterns) spread over the banks.
+// of a warp (random patterns) spread over the banks.  Split: the even and the
+// odd 8-row blocks (the lo and hi halves of the 16-row blocks of round 3)
+// fill separate histograms, weighted by E_3 of their 16-row block.
 __global__ void __launch_bounds__(HIST_T) ccs_hist_kernel(const HistArgs a) {
     extern __shared__ uint32_t s_hist[];  // [HIST_LIMBS][NPAT], then wg of the block's q range
     K* s_wg = reinterpret_cast<K*>(s_hist + NPAT * HIST_LIMBS);
@@ -101,9 +104,10 @@ __global__ void __launch_bounds__(HIST_T) ccs_hist_kernel(const HistArgs a) {
     const uint32_t q1 = min(a.nq, q0 + a.q_chunk);
     for (uint32_t q = q0 + tid; q < q1; q += HIST_T) s_wg[q - q0] = a.wg[q];
     __syncthreads();
-    const uint32_t t8 = blockIdx.x * HIST_T + tid;
+    const uint32_t u = blockIdx.x * HIST_T + tid;
+    const uint32_t t8 = a.split ? 2 * u + blockIdx.z : u;
     if (t8 < a.n_t8) {
-        const K e = a.E8[t8];
+        const K e = a.Ew[a.split ? (t8 >> 1) : t8];
         const int8_t* zp = a.Z + (uint64_t)q0 * a.m + 8ull * t8;
         constexpr int BATCH = 8;  // loads in flight per thread
         for (uint32_t qb = q0; qb < q1; qb += BATCH) {
@@ -135,28 +139,31 @@ __global__ void __launch_bounds__(HIST_T) ccs_hist_kernel(const HistArgs a) {
         }
     }
     __syncthreads();
-    uint32_t* out = a.partial + ((uint64_t)blockIdx.y * gridDim.x + blockIdx.x) * (NPAT * HIST_LIMBS);
+    uint32_t* out = a.partial +
+                    (((uint64_t)blockIdx.z * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x) * (NPAT * HIST_LIMBS);
     for (int i = tid; i < NPAT * HIST_LIMBS / 4; i += HIST_T)
         reinterpret_cast<uint4*>(out)[i] = reinterpret_cast<const uint4*>(s_hist)[i];
 }
 
-// H64[l][p] += the block counters of one slice of blocks; one thread per
-// counter, consecutive threads on consecutive counters.  Each sum stays below
-// 2^52 (2^20 blocks of counters < 2^32).
+// H64[z][l][p] += the block counters of one slice of the blocks of histogram
+// z; one thread per counter, consecutive threads on consecutive counters.
+// Each sum stays below 2^52 (2^20 blocks of counters < 2^32).
 constexpr int HIST_SUM_SLICE = 8;
 __global__ void __launch_bounds__(256) ccs_hist_sum_kernel(const uint32_t* __restrict__ partial, uint32_t nblk,
                                                            unsigned long long* __restrict__ H64) {
     const uint32_t i = blockIdx.x * 256 + threadIdx.x;
     if (i >= NPAT * HIST_LIMBS) return;
+    const uint32_t z = blockIdx.z;
     const uint32_t b0 = blockIdx.y * HIST_SUM_SLICE, b1 = min(nblk, b0 + HIST_SUM_SLICE);
+    const uint32_t* src = partial + (uint64_t)z * nblk * NPAT * HIST_LIMBS + i;
     uint64_t acc = 0;
-    for (uint32_t b = b0; b < b1; b++) acc += __ldg(partial + (uint64_t)b * NPAT * HIST_LIMBS + i);
-    if (acc) atomicAdd(H64 + i, (unsigned long long)acc);
+    for (uint32_t b = b0; b < b1; b++) acc += __ldg(src + (uint64_t)b * NPAT * HIST_LIMBS);
+    if (acc) atomicAdd(H64 + (uint64_t)z * NPAT * HIST_LIMBS + i, (unsigned long long)acc);
 }
 
 // H[p] from its eight limb sums (limb l has weight 2^(16 l); 2^0 .. 2^48 are canonical)
 __device__ __forceinline__ K hist_value(const unsigned long long* H64, int p) {
-    uint64_t re = 0, im = 0;
+    uint64_t re = 0, im = 0;  // H64 points at one histogram [HIST_LIMBS][NPAT]
 #pragma unroll
     for (int l = 0; l < 4; l++) {
         const uint64_t pw = 1ull << (16 * l);
@@ -222,8 +229,9 @@ struct FastRoundArgs {
     int j;
     uint32_t n_mom, n_small;     // blocks of the first two roles; the rest are NC blocks
     // moments
-    const unsigned long long* H64;
-    K beta1, beta2;              // beta_r[1], beta_r[2]
+    const unsigned long long* H64;  // [1 + split][HIST_LIMBS][NPAT]
+    int split;                   // H64 holds the even / odd 8-row-block histograms (weights E_3)
+    K beta1, beta2, beta3;       // beta_r[1..3] (beta3 only with split)
     // small tables: f variables at slots 1..n_fvar, eq_rin / eval at idx_eqrin / idx_eval
     const K* small_in;
     K* small_out;
@@ -263,7 +271,10 @@ __device__ __noinline__ void mom_role(const FastRoundArgs& a, uint32_t blk, K* r
     K c[4] = {gl::kzero(), gl::kzero(), gl::kzero(), gl::kzero()};
     const int p = blk * FR + threadIdx.x;
     if (p < NPAT) {
-        const K h = hist_value(a.H64, p);
+        // split: an 8-row block of parity z weighs E_2(t8) = eq(beta_3, z) E_3(t8 >> 1)
+        const K h = a.split ? gl::kadd(kmul_n(gl::ksub(gl::kone(), a.beta3), hist_value(a.H64, p)),
+                                       kmul_n(a.beta3, hist_value(a.H64 + NPAT * HIST_LIMBS, p)))
+                            : hist_value(a.H64, p);
         if (!gl::kiszero(h)) {
             int tr[8];
             int P = p + NPAT + 1;
@@ -380,6 +391,43 @@ __device__ __noinline__ void small_role(const FastRoundArgs& a, uint32_t blk, K*
     block_sum_rec(out, REC, rec);
 }
 
+// Round 3, separable part.  With lo, hi the K-linear forms of the even and
+// odd 8-row blocks of a 16-row block, N(lo + (hi - lo) X) has coefficients
+//   c0 = lo^3 - lo,                 c1 = 3 lo^2 hi - 3 lo^3 - hi + lo,
+//   c2 = 3 lo hi^2 - 6 lo^2 hi + 3 lo^3,   c3 = hi^3 - 3 lo hi^2 + 3 lo^2 hi - lo^3.
+// The terms in lo or hi alone are odd functions of one 8-row pattern, so they
+// come from the split histograms: SA_k = sum_P H_even[P] LV(P)^k and SB_k
+// with H_odd (LV(P) = sum_b chi_{r_0..r_2}(b) trit_b(P), E_3 already in H).
+// The NC blocks of round 3 add the cross terms lo^2 hi and lo hi^2.
+__device__ __noinline__ void sep_role(const FastRoundArgs& a, uint32_t blk, K* rec) {
+    __shared__ K s_w8[8];
+    if (threadIdx.x < 8) s_w8[threadIdx.x] = chi_of(a.chals, 3, threadIdx.x);
+    __syncthreads();
+    K c[4] = {gl::kzero(), gl::kzero(), gl::kzero(), gl::kzero()};
+    const int p = blk * FR + threadIdx.x;
+    if (p < NPAT) {
+        const K hA = hist_value(a.H64, p), hB = hist_value(a.H64 + NPAT * HIST_LIMBS, p);
+        if (!gl::kiszero(hA) || !gl::kiszero(hB)) {
+            int P = p + NPAT + 1;
+            K lv = gl::kzero();
+#pragma unroll 1
+            for (int i = 0; i < 8; i++) {
+                const int d = P % 3 - 1;
+                P /= 3;
+                if (d) lv = d > 0 ? gl::kadd(lv, s_w8[i]) : gl::ksub(lv, s_w8[i]);
+            }
+            const K l3 = kmul_n(ksqr_n(lv), lv);
+            const K sa1 = kmul_n(hA, lv), sa3 = kmul_n(hA, l3), sb1 = kmul_n(hB, lv), sb3 = kmul_n(hB, l3);
+            const K sa3x3 = gl::kadd(gl::kdbl(sa3), sa3);
+            c[0] = gl::ksub(sa3, sa1);
+            c[1] = gl::ksub(gl::ksub(sa1, sa3x3), sb1);
+            c[2] = sa3x3;
+            c[3] = gl::ksub(sb3, sa3);
+        }
+    }
+    block_sum_rec(c, 4, rec);
+}
+
 template <int MODE, bool C>
 __device__ __forceinline__ void nc_role(const FastRoundArgs& a, uint32_t blk, K* rec, K* s_wg) {
     constexpr int NLUT = MODE == 3 ? 2 : (MODE == 4 ? 4 : 0);
@@ -409,9 +457,10 @@ __device__ __forceinline__ void nc_role(const FastRoundArgs& a, uint32_t blk, K*
 
     K out[4] = {gl::kzero(), gl::kzero(), gl::kzero(), gl::kzero()};
     if (live) {
-        gl::KAcc acc[4];
+        constexpr int NACC = MODE == 3 ? 2 : 4;
+        gl::KAcc acc[NACC];
 #pragma unroll
-        for (int d = 0; d < 4; d++) gl::kacc_zero(acc[d]);
+        for (int d = 0; d < NACC; d++) gl::kacc_zero(acc[d]);
         const uint32_t q0 = c * a.q_chunk, q1 = min(a.nq, q0 + a.q_chunk);
         // the next q's inputs are loaded before the current one is evaluated
         uint4 nv = make_uint4(0, 0, 0, 0), nu = make_uint4(0, 0, 0, 0);
@@ -440,7 +489,7 @@ __device__ __forceinline__ void nc_role(const FastRoundArgs& a, uint32_t blk, K*
             K lo, hi;
             if constexpr (MODE == 3) {
                 const uint4 v = cv;
-                if ((v.x | v.y | v.z | v.w) == 0) continue;
+                if ((v.x | v.y) == 0 || (v.z | v.w) == 0) continue;  // a zero half zeroes both cross terms
                 lo = gl::kadd(s_lut[p4_index(v.x)], s_lut[81 + p4_index(v.y)]);
                 hi = gl::kadd(s_lut[p4_index(v.z)], s_lut[81 + p4_index(v.w)]);
             } else if constexpr (MODE == 4) {
@@ -472,16 +521,30 @@ __device__ __forceinline__ void nc_role(const FastRoundArgs& a, uint32_t blk, K*
                 }
                 if (gl::kiszero(lo) && gl::kiszero(hi)) continue;
             }
-            K n[4];
-            n_coeffs<C>(lo, hi, n);
             const K w = s_wg[q];
             const uint64_t w7 = gl::mul7(w.im);
+            if constexpr (MODE == 3) {
+                // cross terms only (the separable ones come from the split histograms)
+                gl::kacc_mad(acc[0], w, w7, kmul_c<C>(ksqr_c<C>(lo), hi));
+                gl::kacc_mad(acc[1], w, w7, kmul_c<C>(lo, ksqr_c<C>(hi)));
+            } else {
+                K n[4];
+                n_coeffs<C>(lo, hi, n);
 #pragma unroll
-            for (int d = 0; d < 4; d++) gl::kacc_mad(acc[d], w, w7, n[d]);
+                for (int d = 0; d < 4; d++) gl::kacc_mad(acc[d], w, w7, n[d]);
+            }
         }
         const K e = a.E[t];
+        if constexpr (MODE == 3) {
+            const K x21 = gl::kacc_reduce(acc[0]), x12 = gl::kacc_reduce(acc[1]);
+            const K x21x3 = gl::kadd(gl::kdbl(x21), x21), x12x3 = gl::kadd(gl::kdbl(x12), x12);
+            out[1] = kmul_c<C>(e, x21x3);
+            out[2] = kmul_c<C>(e, gl::ksub(x12x3, gl::kdbl(x21x3)));
+            out[3] = kmul_c<C>(e, gl::ksub(x21x3, x12x3));
+        } else {
 #pragma unroll
-        for (int d = 0; d < 4; d++) out[d] = kmul_c<C>(e, gl::kacc_reduce(acc[d]));
+            for (int d = 0; d < 4; d++) out[d] = kmul_c<C>(e, gl::kacc_reduce(acc[d]));
+        }
     }
     block_sum_rec(out, 4, rec);
 }
@@ -542,7 +605,8 @@ __global__ void __launch_bounds__(FR, 2) ccs_fast_round_kernel(const __grid_cons
     const uint32_t b = blockIdx.x;
     K* rec = a.partials + (uint64_t)b * REC;
     if (b < a.n_mom) {
-        mom_role(a, b, rec);
+        if constexpr (MODE == 3) sep_role(a, b, rec);
+        else mom_role(a, b, rec);
     } else if (b < a.n_mom + a.n_small) {
         small_role(a, b - a.n_mom, rec);
     } else {

@@ -676,7 +676,9 @@ struct neo_gpu_ccs_oracle {
     DevBuf<uint32_t> ticket;    // last-block ticket of the fused round kernel
     DevBuf<K> Cs;               // C_j = prod_{i<j} eq(beta_i, r_i) per row round
     uint32_t hist_gx = 0, hist_gy = 0, hist_qc = 0;
+    bool hist_split = false;
     uint32_t compact_q = 8;     // q per thread below which the NC blocks use out-of-line K products
+    uint64_t nc_threads = 148ull * 2 * 256 * 2;  // NC threads per round when the pairs alone are fewer
     K gamma{}, gamma_to_k{};
     std::vector<K> alpha, beta_a, beta_r, r_in, row_chals, ajtai_chals;
     bool has_inputs = false, has_eval = false;
@@ -944,7 +946,7 @@ static void fast_nc_grid(const neo_gpu_ccs_oracle* o, uint32_t j, uint32_t* n_ch
                          uint32_t* blocks) {
     const uint32_t nq = o->k * NEO_D;
     const uint64_t pairs = o->n_pad >> (j + 1);
-    const uint64_t target = 148ull * 2 * FR * 2;
+    const uint64_t target = o->nc_threads;
     const uint32_t nc = (uint32_t)std::min<uint64_t>(nq, std::max<uint64_t>(1, (target + pairs - 1) / pairs));
     *q_chunk = (nq + nc - 1) / nc;
     *n_chunk = (nq + *q_chunk - 1) / *q_chunk;
@@ -954,6 +956,7 @@ static void fast_nc_grid(const neo_gpu_ccs_oracle* o, uint32_t j, uint32_t* n_ch
 static int fast_setup(neo_gpu_ccs_oracle* o) {
     neo_gpu_ctx* ctx = o->ctx;
     if (const char* e = getenv("NEO_TUNE_CCS_COMPACT_Q")) o->compact_q = (uint32_t)strtoul(e, nullptr, 10);
+    if (const char* e = getenv("NEO_TUNE_CCS_NC_THREADS")) o->nc_threads = std::max<uint64_t>(1, strtoull(e, nullptr, 10));
     const uint32_t ell = o->ell_n, nq = o->k * NEO_D;
     // E_j = chi of beta_r[j+1..ell) for every row round (beta_r is in ws_bits[0..ell))
     NEO_CK(ctx, o->E_all.ensure(o->n_pad));
@@ -963,13 +966,16 @@ static int fast_setup(neo_gpu_ccs_oracle* o) {
         if (rc) return rc;
     }
     // histogram grid: a thread per 8-row block, q chunks so that ~2 blocks per SM
+    // split histograms (even / odd 8-row blocks) when round 3 exists
     const uint32_t n_t8 = (uint32_t)(o->n_pad >> 3);
-    o->hist_gx = (uint32_t)ceil_div(n_t8, HIST_T);
-    uint32_t gy = std::max<uint32_t>(1, 296 / o->hist_gx);  // one wave of 2 blocks per SM when it fits
+    o->hist_split = ell >= 4;
+    const uint32_t nz = o->hist_split ? 2 : 1;
+    o->hist_gx = (uint32_t)ceil_div(n_t8 / nz, HIST_T);
+    uint32_t gy = std::max<uint32_t>(1, 296 / (o->hist_gx * nz));  // one wave of 2 blocks per SM when it fits
     o->hist_qc = std::max<uint32_t>(1, std::min<uint32_t>(HIST_MAX_Q, (nq + gy - 1) / gy));
     o->hist_gy = (nq + o->hist_qc - 1) / o->hist_qc;
-    NEO_CK(ctx, o->hist_part.ensure((size_t)o->hist_gx * o->hist_gy * NPAT * HIST_LIMBS));
-    NEO_CK(ctx, o->hist64.ensure((size_t)NPAT * 8));
+    NEO_CK(ctx, o->hist_part.ensure((size_t)nz * o->hist_gx * o->hist_gy * NPAT * HIST_LIMBS));
+    NEO_CK(ctx, o->hist64.ensure((size_t)nz * NPAT * HIST_LIMBS));
     NEO_CK(ctx, o->ticket.ensure(1));
     NEO_CK(ctx, o->Cs.ensure(ell));
     NEO_CK(ctx, cudaMemsetAsync(o->ticket.p, 0, 4, ctx->stream));
@@ -977,7 +983,7 @@ static int fast_setup(neo_gpu_ccs_oracle* o) {
     uint64_t recs = 0;
     for (uint32_t j = 0; j < ell; j++) {
         uint64_t r = ceil_div(o->n_pad >> (j + 1), FR);
-        if (j <= 2) r += ceil_div(NPAT, FR);
+        if (j <= 3) r += ceil_div(NPAT, FR);
         if (j >= 3) {
             uint32_t nc, qc, blocks;
             fast_nc_grid(o, j, &nc, &qc, &blocks);
@@ -1006,24 +1012,29 @@ static int fast_round_launch(neo_gpu_ccs_oracle* o, K* coeffs_dst) {
         h.n_t8 = (uint32_t)(o->n_pad >> 3);
         h.q_chunk = o->hist_qc;
         h.wg = o->wg.p;
-        h.E8 = o->E_all.p + (o->n_pad - (o->n_pad >> 2));
+        const uint32_t jw = o->hist_split ? 3 : 2;  // E_3 per 16-row block, or E_2 per 8-row block
+        h.Ew = o->E_all.p + (o->n_pad - (o->n_pad >> jw));
+        h.split = o->hist_split;
         h.partial = o->hist_part.p;
+        const uint32_t nz = o->hist_split ? 2 : 1;
         const size_t smem = (size_t)NPAT * HIST_LIMBS * 4 + (size_t)o->hist_qc * sizeof(K);
-        ccs_hist_kernel<<<dim3(o->hist_gx, o->hist_gy), HIST_T, smem, ctx->stream>>>(h);
+        ccs_hist_kernel<<<dim3(o->hist_gx, o->hist_gy, nz), HIST_T, smem, ctx->stream>>>(h);
         NEO_LAUNCHED(ctx);
-        NEO_CK(ctx, cudaMemsetAsync(o->hist64.p, 0, o->hist64.bytes(), ctx->stream));
+        NEO_CK(ctx, cudaMemsetAsync(o->hist64.p, 0, (size_t)nz * NPAT * HIST_LIMBS * 8, ctx->stream));
         const uint32_t nblk = o->hist_gx * o->hist_gy;
-        ccs_hist_sum_kernel<<<dim3((uint32_t)ceil_div(NPAT * HIST_LIMBS, 256), (uint32_t)ceil_div(nblk, HIST_SUM_SLICE)), 256, 0,
-                              ctx->stream>>>(o->hist_part.p, nblk,
-                                             reinterpret_cast<unsigned long long*>(o->hist64.p));
+        ccs_hist_sum_kernel<<<dim3((uint32_t)ceil_div(NPAT * HIST_LIMBS, 256), (uint32_t)ceil_div(nblk, HIST_SUM_SLICE), nz),
+                              256, 0, ctx->stream>>>(o->hist_part.p, nblk,
+                                                     reinterpret_cast<unsigned long long*>(o->hist64.p));
         NEO_LAUNCHED(ctx);
     }
     FastRoundArgs a{};
     a.j = (int)j;
-    a.n_mom = j <= 2 ? (uint32_t)ceil_div(NPAT, FR) : 0;
+    a.n_mom = j <= 3 ? (uint32_t)ceil_div(NPAT, FR) : 0;  // moments (rounds 0..2), separable terms (round 3)
     a.H64 = reinterpret_cast<const unsigned long long*>(o->hist64.p);
+    a.split = o->hist_split;
     a.beta1 = o->beta_r[1];
     a.beta2 = o->beta_r[2];
+    if (o->hist_split) a.beta3 = o->beta_r[3];
     if (j == 0) {
         a.small_in = o->small[0].p;
         a.small_len_in = o->n_pad;
