@@ -128,6 +128,18 @@ int neo_gpu_commit_device(neo_gpu_ctx* ctx, const int8_t* d_digits, uint32_t n_v
  * is asynchronous on the context stream and allocates nothing. */
 int neo_gpu_commit_noalloc(neo_gpu_ctx* ctx, const int8_t* d_digits, uint32_t n_vec, uint64_t m, uint64_t* d_out);
 
+/* Commitment mixers (CommitMixers, crates/neo-fold/src/shard.rs:146-153), host
+ * buffers in and out.  Commitments are [kappa][54] F_q (Commitment::data,
+ * column-major, crates/neo-ajtai/src/types.rs:15-22).
+ * mix_rhos_commits: out = sum_i rho_i c_i with rhos[count][54][54] row-major
+ * F_q matrices (the S-action of Pi_RLC, common.rs:398-430); cs[count][kappa][54].
+ * combine_b_pows: out = sum_i b^i c_i (i from 0, the DEC parent check,
+ * shard.rs:1120). */
+int neo_gpu_mix_rhos_commits(neo_gpu_ctx* ctx, const uint64_t* rhos, const uint64_t* cs, uint32_t count,
+                             uint32_t kappa, uint64_t* out);
+int neo_gpu_combine_b_pows(neo_gpu_ctx* ctx, const uint64_t* cs, uint32_t count, uint32_t kappa, uint32_t b,
+                           uint64_t* out);
+
 /* Balanced base-2 decomposition z in F_q^m -> Z in {-1,0,1}^{54 x m}
  * row-major (crates/neo-ajtai/src/decomp.rs:118-158, DecompStyle::Balanced). */
 int neo_gpu_decomp_b2(neo_gpu_ctx* ctx, const uint64_t* z, uint64_t m, int8_t* Z);

@@ -50,6 +50,8 @@ SIGNATURES = {
     "neo_gpu_synchronize": [P],
     "neo_gpu_commit_device": [P, ctypes.c_void_p, U32, U64, ctypes.c_void_p],
     "neo_gpu_commit_noalloc": [P, ctypes.c_void_p, U32, U64, ctypes.c_void_p],
+    "neo_gpu_mix_rhos_commits": [P, P, P, U32, U32, P],
+    "neo_gpu_combine_b_pows": [P, P, U32, U32, U32, P],
     "neo_gpu_shard_step_stats": [P, P, U32],
     "neo_gpu_shard_create": [P, P, U32, U32, ctypes.c_char_p, P],
     "neo_gpu_shard_create_mem": [P, P, U32, U32, ctypes.c_char_p, P, P],
@@ -187,6 +189,23 @@ class Context:
     def commit_noalloc(self, d_digits: int, n_vec: int, m: int, d_out: int):
         """Commitment with the library's fixed device scratch (no allocation)."""
         self.check(self.lib.neo_gpu_commit_noalloc(self.h, ctypes.c_void_p(d_digits), n_vec, m, ctypes.c_void_p(d_out)))
+
+    def mix_rhos_commits(self, rhos: np.ndarray, cs: np.ndarray) -> np.ndarray:
+        """sum_i rho_i c_i: rhos [count][54][54] F_q, cs [count][kappa][54] -> [kappa][54]
+        (CommitMixers::mix_rhos_commits, crates/neo-fold/src/shard.rs:146-153)."""
+        rhos, cs = _u64(rhos), _u64(cs)
+        count, kappa = cs.shape[0], cs.shape[1]
+        out = np.empty((kappa, 54), np.uint64)
+        self.check(self.lib.neo_gpu_mix_rhos_commits(self.h, _p(rhos), _p(cs), count, kappa, _p(out)))
+        return out
+
+    def combine_b_pows(self, cs: np.ndarray, b: int) -> np.ndarray:
+        """sum_i b^i c_i over cs [count][kappa][54] (CommitMixers::combine_b_pows)."""
+        cs = _u64(cs)
+        count, kappa = cs.shape[0], cs.shape[1]
+        out = np.empty((kappa, 54), np.uint64)
+        self.check(self.lib.neo_gpu_combine_b_pows(self.h, _p(cs), count, kappa, b, _p(out)))
+        return out
 
     def close(self):
         if getattr(self, "h", None):

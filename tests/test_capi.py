@@ -34,3 +34,19 @@ def test_context_creation_fails_loudly_without_gpu():
     import pytest
     with pytest.raises(gpu.NeoGpuError):
         gpu.Context(0)
+
+
+def test_rust_bindings_cover_the_header():
+    """nightstream_b200/rust/neo-gpu-sys declares every entry point of
+    include/neo_gpu.h (the binding a Rust host such as the reference's shard
+    loop links against), with the same parameter count."""
+    import re
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    hdr = re.sub(r"/\*.*?\*/", "", open(os.path.join(root, "include", "neo_gpu.h")).read(), flags=re.S)
+    decl = {n: len([a for a in args.split(",") if a.strip() and a.strip() != "void"])
+            for n, args in re.findall(r"^(?:int|uint32_t|const char\*)\s+(neo_\w+)\s*\(([^;]*?)\)\s*;", hdr, re.M | re.S)}
+    rs = open(os.path.join(root, "nightstream_b200", "rust", "neo-gpu-sys", "src", "lib.rs")).read()
+    got = {n: len([a for a in args.split(",") if a.strip()])
+           for n, args in re.findall(r"pub fn (neo_\w+)\(([^)]*)\)", rs)}
+    assert decl, "no declarations parsed"
+    assert decl == got

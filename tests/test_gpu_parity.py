@@ -181,3 +181,22 @@ def test_row_rounds_device_matches_oracle(ctx):
     yo, yso = o.me_outputs()
     assert np.array_equal(yg, yo) and np.array_equal(ysg, yso)
     g.close()
+
+
+def test_commit_mixers_match_definition(ctx):
+    """CommitMixers on the device: sum_i rho_i c_i for general 54 x 54 F_q
+    matrices and sum_i b^i c_i, against the definition in Python integers."""
+    rng = np.random.default_rng(31)
+    count, kappa = 13, 16
+    rhos = rng.integers(0, Q, size=(count, 54, 54), dtype=np.uint64)
+    rhos[0] = O.rot_matrix(rng.integers(-2, 3, size=54).astype(np.int8))  # a Pi_RLC rho = rot(a), a in {-2..2}^54
+    cs = rng.integers(0, Q, size=(count, kappa, 54), dtype=np.uint64)
+    got = ctx.mix_rhos_commits(rhos, cs)
+    R = [[[int(x) for x in row] for row in m] for m in rhos]
+    C = [[[int(x) for x in col] for col in c] for c in cs]
+    want = [[sum(R[i][r][k] * C[i][c][k] for i in range(count) for k in range(54)) % Q for r in range(54)]
+            for c in range(kappa)]
+    assert np.array_equal(got, np.array(want, dtype=np.uint64))
+    got = ctx.combine_b_pows(cs[:12], 2)
+    want = [[sum(pow(2, i, Q) * C[i][c][r] for i in range(12)) % Q for r in range(54)] for c in range(kappa)]
+    assert np.array_equal(got, np.array(want, dtype=np.uint64))
