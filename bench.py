@@ -66,6 +66,7 @@ def parse():
 
 
 MEM_TWIST_ELL, MEM_SHOUT_ELL = 12, 16
+INT8_DATASHEET_TOPS = 4500.0  # B200 dense int8 tensor throughput, datasheet (TOPS)
 
 
 class Workload:
@@ -636,7 +637,9 @@ def run_ours(args, rank, world, local_rank):
                        "traffic": COMMIT_TRAFFIC_PER_M * m if m >= 1 << 14 else None,
                        "traffic_source": "ncu dram__bytes_read+write of one 12-plane commit_tc_kernel launch at "
                                          "m = 2^14, scaled by m",
-                       "launch_ms": commit_ms, "peak_source": peak_src, "algorithmic_ops_per_launch": ops}
+                       "launch_ms": commit_ms, "peak_source": peak_src, "algorithmic_ops_per_launch": ops,
+                       "frac_of_datasheet": achieved / INT8_DATASHEET_TOPS,
+                       "datasheet_peak": INT8_DATASHEET_TOPS}
     roofline = rounds_roofline(ctx, ccs, wl.z(0), args.ell, stream)
     # the batched mix runs before the legs that use the host's OpenMP pool
     batched = batched_result(args) if rank == 0 and world == 1 and not args.no_batch else None

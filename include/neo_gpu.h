@@ -195,6 +195,22 @@ uint32_t neo_gpu_ccs_oracle_degree_bound(const neo_gpu_ccs_oracle* o);
 int neo_gpu_ccs_oracle_me_outputs(neo_gpu_ccs_oracle* o, uint64_t* y, uint64_t* y_scalars);
 int neo_gpu_ccs_oracle_destroy(neo_gpu_ccs_oracle* o);
 
+/* Launch-shape autotuner of the Pi_CCS row rounds (no counterpart in the
+ * reference, whose oracle is CPU code): per shape (ell_n, k) the library keeps
+ * the NC-block thread count, the out-of-line threshold and the histogram block
+ * size that ran the row-round sequence fastest.  neo_gpu_ccs_autotune times
+ * every candidate on the caller's CCS and k ternary digit matrices
+ * Z[k][54][m] (n == m == 2^ell_n) with `reps` timed runs each and records the
+ * best; out3 = {nc_threads, compact_q, hist_items}.  Oracles created later for
+ * that shape use it.  neo_gpu_tune_save / neo_gpu_tune_load write / read the
+ * table as text lines "ccs <ell_n> <k> <nc_threads> <compact_q> <hist_items>";
+ * neo_gpu_tune_get reads one entry (NEO_ERR_ARG when the shape is untuned). */
+int neo_gpu_ccs_autotune(neo_gpu_ctx* ctx, const neo_ccs_desc* ccs, const int8_t* Z, uint32_t k, uint32_t reps,
+                         uint64_t* out3);
+int neo_gpu_tune_load(const char* path);
+int neo_gpu_tune_save(const char* path);
+int neo_gpu_tune_get(uint32_t ell_n, uint32_t k, uint64_t* out3);
+
 /* ---- Twist / Shout time-lane oracles (RoundOracle) ------------------- */
 /* The sparse-in-time oracles of crates/neo-memory/src/twist_oracle.rs, on
  * dense tables.  cols: n_cols K columns of 2^ell entries each (column-major,

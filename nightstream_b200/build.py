@@ -16,7 +16,7 @@ CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libneo_gpu.so")
 OBJDIR = os.path.join(HERE, "_build")
 SOURCES = ["core.cu", "commit.cu", "commit_tc.cu", "ccs_oracle.cu", "fold.cu", "batch.cu",
-           "mem_oracle.cu", "mixers.cu", "pp_gen.cu", "transcript.cpp", "transcript_capi.cpp"]
+           "mem_oracle.cu", "mixers.cu", "pp_gen.cu", "tune.cu", "transcript.cpp", "transcript_capi.cpp"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 CFLAGS = ARCH + [

@@ -20,6 +20,7 @@
 //    in a fixed order, so results are deterministic (exact F_q arithmetic
 //    makes them order-independent anyway).
 #include "internal.cuh"
+#include "tune.h"
 #include <algorithm>
 #include <cstdlib>
 #include <memory>
@@ -675,10 +676,12 @@ struct neo_gpu_ccs_oracle {
     DevBuf<uint32_t> tern_flag;
     DevBuf<uint32_t> ticket;    // last-block ticket of the fused round kernel
     DevBuf<K> Cs;               // C_j = prod_{i<j} eq(beta_i, r_i) per row round
+    HostBuf<K> h_chals;         // page-locked staging of the row challenges (async upload)
     uint32_t hist_gx = 0, hist_gy = 0, hist_qc = 0;
     bool hist_split = false;
     uint32_t compact_q = 8;     // q per thread below which the NC blocks use out-of-line K products
-    uint64_t nc_threads = 148ull * 2 * 256 * 2;  // NC threads per round when the pairs alone are fewer
+    uint64_t nc_threads = 148ull * 2 * 256;  // NC threads per round (one wave) when the pairs alone are fewer
+    uint32_t hist_items = 16384;              // target (q, 8-row block) items per histogram block
     K gamma{}, gamma_to_k{};
     std::vector<K> alpha, beta_a, beta_r, r_in, row_chals, ajtai_chals;
     bool has_inputs = false, has_eval = false;
@@ -955,6 +958,17 @@ static void fast_nc_grid(const neo_gpu_ccs_oracle* o, uint32_t j, uint32_t* n_ch
 
 static int fast_setup(neo_gpu_ccs_oracle* o) {
     neo_gpu_ctx* ctx = o->ctx;
+    // launch choices: defaults, the tuned table of this shape (tune.cu), then
+    // environment overrides
+    o->compact_q = 8;
+    o->nc_threads = 148ull * 2 * 256;
+    o->hist_items = 16384;
+    CcsTune tn;
+    if (tune_lookup(o->ell_n, o->k, &tn)) {
+        o->nc_threads = std::max<uint64_t>(1, tn.nc_threads);
+        o->compact_q = tn.compact_q;
+        o->hist_items = std::max<uint32_t>(1, tn.hist_items);
+    }
     if (const char* e = getenv("NEO_TUNE_CCS_COMPACT_Q")) o->compact_q = (uint32_t)strtoul(e, nullptr, 10);
     if (const char* e = getenv("NEO_TUNE_CCS_NC_THREADS")) o->nc_threads = std::max<uint64_t>(1, strtoull(e, nullptr, 10));
     const uint32_t ell = o->ell_n, nq = o->k * NEO_D;
@@ -971,7 +985,11 @@ static int fast_setup(neo_gpu_ccs_oracle* o) {
     o->hist_split = ell >= 4;
     const uint32_t nz = o->hist_split ? 2 : 1;
     o->hist_gx = (uint32_t)ceil_div(n_t8 / nz, HIST_T);
-    uint32_t gy = std::max<uint32_t>(1, 296 / (o->hist_gx * nz));  // one wave of 2 blocks per SM when it fits
+    // one wave of 2 blocks per SM when it fits, but at least ~16k items per
+    // block: a block zeroes, fills and writes out a 105 KB histogram
+    const uint64_t items = (uint64_t)nq * n_t8;
+    uint32_t gy = std::max<uint32_t>(1, 296 / (o->hist_gx * nz));
+    gy = std::min<uint32_t>(gy, std::max<uint64_t>(1, items / ((uint64_t)o->hist_gx * nz * o->hist_items)));
     o->hist_qc = std::max<uint32_t>(1, std::min<uint32_t>(HIST_MAX_Q, (nq + gy - 1) / gy));
     o->hist_gy = (nq + o->hist_qc - 1) / o->hist_qc;
     NEO_CK(ctx, o->hist_part.ensure((size_t)nz * o->hist_gx * o->hist_gy * NPAT * HIST_LIMBS));
@@ -1212,6 +1230,30 @@ static int row_round(neo_gpu_ccs_oracle* o) {
     return NEO_OK;
 }
 
+// Enqueues the current row round with its coefficients (deg_max + 1 K values)
+// written to d_dst on the device and no host sync (the batched sum-check
+// launches every claim of a round, then copies all values back at once).
+int ccs_oracle_round_launch(neo_gpu_ccs_oracle* o, K* d_dst, uint32_t* ncoef) {
+    neo_gpu_ctx* ctx = o->ctx;
+    const uint32_t j = o->round_idx;
+    if (j >= o->ell_n) return ctx->fail(NEO_ERR_ARG, "ccs round launch: not a row round");
+    if (j > 0 && ((int)j <= o->J || o->fast)) {
+        NEO_CK(ctx, o->h_chals.ensure(o->ell_n));
+        memcpy(o->h_chals.p, o->row_chals.data(), j * sizeof(K));
+        NEO_CK(ctx, cudaMemcpyAsync(o->d_chals.p, o->h_chals.p, j * sizeof(K), cudaMemcpyHostToDevice, ctx->stream));
+    }
+    int rc = row_round_launch(o, d_dst);
+    if (rc) return rc;
+    *ncoef = (uint32_t)o->deg_max + 1;
+    return NEO_OK;
+}
+
+// The coefficients of the round just launched, read back by the caller.
+void ccs_oracle_round_set(neo_gpu_ccs_oracle* o, const K* coeffs) {
+    o->h_coeffs.assign(coeffs, coeffs + o->deg_max + 1);
+    o->coeffs_valid = true;
+}
+
 static int ajtai_precompute(neo_gpu_ccs_oracle* o) {
     neo_gpu_ctx* ctx = o->ctx;
     NEO_CK(ctx, o->chi_r.ensure(o->n_pad));
@@ -1374,4 +1416,100 @@ int ccs_oracle_dev_vj(neo_gpu_ccs_oracle* o, const K** vj) {
     }
     *vj = o->vj.p;
     return NEO_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Autotuner of the ternary-digit row rounds (tune.cu): every candidate launch
+// choice runs the whole row-round sequence of the caller's CCS and witness
+// digits (random challenges); the fastest is recorded for (ell_n, k).
+// ---------------------------------------------------------------------------
+static uint64_t tune_mix(uint64_t& s) {
+    s += 0x9E3779B97F4A7C15ull;
+    uint64_t z = s;
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    return gl::canon(z ^ (z >> 31));
+}
+
+static int neo_gpu_ccs_autotune_impl_abi(neo_gpu_ctx* ctx, const neo_ccs_desc* desc, const int8_t* Z, uint32_t k,
+                                         uint32_t reps, uint64_t* best3) {
+    if (!ctx) return NEO_ERR_ARG;
+    if (!desc || !Z || !best3 || k == 0 || reps == 0) return ctx->fail(NEO_ERR_ARG, "ccs_autotune: bad args");
+    uint32_t ell_n = 0;
+    while ((1u << ell_n) < desc->n) ell_n++;
+    if (desc->n != desc->m || (1u << ell_n) != desc->n || ell_n < 3)
+        return ctx->fail(NEO_ERR_UNSUPPORTED, "ccs_autotune: needs n == m == 2^ell, ell >= 3");
+    NEO_CK(ctx, cudaSetDevice(ctx->device));
+    const uint32_t ell_d = 6, d_sc = 6;
+    uint64_t seed = 0x4E454F54554E45ull;
+    auto rk = [&](size_t n) {
+        std::vector<K> v(n);
+        for (auto& x : v) x = gl::kmk(tune_mix(seed), tune_mix(seed));
+        return v;
+    };
+    std::vector<K> al = rk(ell_d), ba = rk(ell_d), br = rk(ell_n), ri = rk(ell_n), g = rk(1), ch = rk(ell_n);
+    auto* o = new neo_gpu_ccs_oracle();
+    std::unique_ptr<neo_gpu_ccs_oracle> guard(o);
+    int rc = dev_ccs_upload(ctx, desc, o->own_ccs);
+    if (rc) return rc;
+    o->ccs = &o->own_ccs;
+    NEO_CK(ctx, o->own_Z.alloc((size_t)k * NEO_D * desc->m));
+    NEO_CK(ctx, cudaMemcpyAsync(o->own_Z.p, Z, o->own_Z.bytes(), cudaMemcpyHostToDevice, ctx->stream));
+    DevBuf<K> coeffs;
+    NEO_CK(ctx, coeffs.ensure((size_t)ell_n * (MAX_DEG + 1)));
+    cudaEvent_t e0, e1;
+    NEO_CK(ctx, cudaEventCreate(&e0));
+    NEO_CK(ctx, cudaEventCreate(&e1));
+    const uint64_t wave = 148ull * 2 * FR;
+    const uint64_t nts[3] = {wave / 2, wave, 2 * wave};
+    const uint32_t cqs[3] = {0, 8, 64}, his[3] = {8192, 16384, 65536};
+    CcsTune best{wave, 8, 16384};
+    float best_ms = 1e30f;
+    for (uint64_t nt : nts)
+        for (uint32_t cq : cqs)
+            for (uint32_t hi : his) {
+                CcsTune cand{nt, cq, hi};
+                float cand_ms = 1e30f;
+                for (uint32_t rep = 0; rep < reps + 1 && rc == 0; rep++) {
+                    tune_force(&cand);
+                    rc = oracle_init(ctx, o, o->own_Z.p, k, 2, al.data(), ba.data(), br.data(), g[0], ri.data(), ell_d,
+                                     ell_n, d_sc);
+                    tune_force(nullptr);
+                    if (rc) break;
+                    if (!o->fast) {
+                        rc = ctx->fail(NEO_ERR_UNSUPPORTED, "ccs_autotune: digits are not ternary");
+                        break;
+                    }
+                    o->row_chals.assign(ch.begin(), ch.end());
+                    NEO_CK(ctx, cudaMemcpyAsync(o->d_chals.p, ch.data(), ell_n * sizeof(K), cudaMemcpyHostToDevice,
+                                                ctx->stream));
+                    NEO_CK(ctx, cudaEventRecord(e0, ctx->stream));
+                    for (uint32_t j = 0; j < ell_n && rc == 0; j++) {
+                        o->round_idx = j;
+                        rc = row_round_launch(o, coeffs.p + (size_t)j * (MAX_DEG + 1));
+                    }
+                    NEO_CK(ctx, cudaEventRecord(e1, ctx->stream));
+                    NEO_CK(ctx, cudaEventSynchronize(e1));
+                    float ms = 0;
+                    NEO_CK(ctx, cudaEventElapsedTime(&ms, e0, e1));
+                    if (rep > 0 && ms < cand_ms) cand_ms = ms;  // the first run warms up
+                }
+                if (rc) break;
+                if (cand_ms < best_ms) {
+                    best_ms = cand_ms;
+                    best = cand;
+                }
+            }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (rc) return rc;
+    tune_store(ell_n, k, best);
+    best3[0] = best.nc_threads;
+    best3[1] = best.compact_q;
+    best3[2] = best.hist_items;
+    return NEO_OK;
+}
+extern "C" int neo_gpu_ccs_autotune(neo_gpu_ctx* ctx, const neo_ccs_desc* desc, const int8_t* Z, uint32_t k,
+                                    uint32_t reps, uint64_t* best3) {
+    NEO_ABI_GUARD(neo_gpu_ccs_autotune_impl_abi(ctx, desc, Z, k, reps, best3))
 }

@@ -227,6 +227,11 @@ __global__ void __launch_bounds__(256) bus_open_kernel(const int8_t* __restrict_
 struct neo_gpu_shard {
     neo_gpu_ctx* ctx = nullptr;
     DevCcs ccs;
+    // batched sum-check rounds: every claim's round values in one device array,
+    // read back with one copy per round (page-locked), and the partial sums of
+    // the multi-claim memory kernels
+    DevBuf<K> d_round, d_mpart;
+    HostBuf<K> h_round;
     uint32_t kappa = 16;
     uint32_t n = 0, m32 = 0, t = 0, ell_n = 0, ell_d = 6, d_sc = 6, k_rho = 12, b = 2, m_in = 1, lambda = 127;
     uint64_t m = 0;
@@ -659,12 +664,31 @@ int ccs_oracle_create_dev(neo_gpu_ctx* ctx, const DevCcs* ccs, const int8_t* d_Z
                           const K* alpha, const K* beta_a, const K* beta_r, K gamma, const K* r_inputs,
                           uint32_t ell_d, uint32_t ell_n, uint32_t d_sc, neo_gpu_ccs_oracle** out);
 int ccs_oracle_dev_vj(neo_gpu_ccs_oracle* o, const K** vj);
+int ccs_oracle_round_launch(neo_gpu_ccs_oracle* o, K* d_dst, uint32_t* ncoef);
+void ccs_oracle_round_set(neo_gpu_ccs_oracle* o, const K* coeffs);
+bool mem_round_multi_ok(const neo_gpu_mem_oracle* o);
+int mem_round_launch_multi(neo_gpu_ctx* ctx, neo_gpu_mem_oracle* const* os, int n, K* const* d_out,
+                           DevBuf<K>& partials);
 
 namespace {
 
 static void interpolate(const std::vector<K>& xs, const std::vector<K>& ys, std::vector<K>& co) {
-    // sumcheck.rs:74-118
+    // sumcheck.rs:74-118; the nodes here are always 0..n-1, whose Lagrange
+    // denominators 1 / prod_{j != i} (i - j) are computed once per n
     const size_t n = xs.size();
+    bool ints = true;
+    for (size_t i = 0; i < n; i++) ints &= xs[i].im == 0 && xs[i].re == i;
+    static thread_local std::vector<std::vector<K>> inv_den;
+    if (ints && inv_den.size() <= n) inv_den.resize(n + 1);
+    if (ints && inv_den[n].empty()) {
+        inv_den[n].resize(n);
+        for (size_t i = 0; i < n; i++) {
+            K den = gl::kone();
+            for (size_t j = 0; j < n; j++)
+                if (i != j) den = gl::kmul(den, gl::ksub(xs[i], xs[j]));
+            inv_den[n][i] = gl::kinv(den);
+        }
+    }
     co.assign(n, gl::kzero());
     std::vector<K> numer(n), next(n);
     for (size_t i = 0; i < n; i++) {
@@ -681,10 +705,15 @@ static void interpolate(const std::vector<K>& xs, const std::vector<K>& ys, std:
             numer.swap(next);
             cur++;
         }
-        K den = gl::kone();
-        for (size_t j = 0; j < n; j++)
-            if (i != j) den = gl::kmul(den, gl::ksub(xs[i], xs[j]));
-        K sc = gl::kmul(ys[i], gl::kinv(den));
+        K sc;
+        if (ints) {
+            sc = gl::kmul(ys[i], inv_den[n][i]);
+        } else {
+            K den = gl::kone();
+            for (size_t j = 0; j < n; j++)
+                if (i != j) den = gl::kmul(den, gl::ksub(xs[i], xs[j]));
+            sc = gl::kmul(ys[i], gl::kinv(den));
+        }
         for (size_t d = 0; d <= cur; d++) co[d] = gl::kadd(co[d], gl::kmul(sc, numer[d]));
     }
 }
@@ -731,7 +760,12 @@ struct Claim {
 };
 
 // run_batched_sumcheck_prover (sumcheck.rs:350-456) inside sc_start / sc_end
-// (sumcheck_ds.rs:11-19); round polynomials appended to P in claim order
+// (sumcheck_ds.rs:11-19); round polynomials appended to P in claim order.
+// Per round every claim is launched first -- the Pi_CCS claim writes its
+// coefficients, the memory claims their values at 0..deg (all of them in one
+// multi-claim fold / eval / reduce), into one device array -- then a single
+// copy and sync bring the round back; Twist address-lane claims (and memory
+// claims whose tables are exhausted) take the per-claim path.
 static int run_batched_ds(neo_gpu_shard* sh, const char* domain, uint64_t inst_idx, std::vector<Claim>& cl,
                           uint32_t rounds, std::vector<K>& chals, std::vector<K>& finals, std::vector<uint64_t>& P) {
     neo_gpu_ctx* ctx = sh->ctx;
@@ -742,16 +776,57 @@ static int run_batched_ds(neo_gpu_shard* sh, const char* domain, uint64_t inst_i
     std::vector<K> running(cl.size());
     for (size_t i = 0; i < cl.size(); i++) running[i] = cl[i].sum;
     std::vector<std::vector<K>> polys(cl.size());
+    // slots: MAX_SLOT K values per claim
+    constexpr uint32_t MAX_SLOT = 33;
+    NEO_CK(ctx, sh->d_round.ensure(cl.size() * MAX_SLOT));
+    NEO_CK(ctx, sh->h_round.ensure(cl.size() * MAX_SLOT));
     chals.clear();
+    std::vector<neo_gpu_mem_oracle*> mos;
+    std::vector<K*> mdst;
+    std::vector<uint32_t> kind(cl.size()), ncoef(cl.size());  // kind: 0 per-claim, 1 ccs, 2 multi memory
     for (uint32_t rd = 0; rd < rounds; rd++) {
         auto br = le64(rd);
         tr.append_message("batched/round_idx", br.data(), 8);
+        mos.clear();
+        mdst.clear();
+        for (size_t i = 0; i < cl.size(); i++) {
+            K* slot = sh->d_round.p + i * MAX_SLOT;
+            kind[i] = 0;
+            if (cl[i].ccs && cl[i].deg + 1 <= MAX_SLOT) {
+                int rc = ccs_oracle_round_launch(cl[i].ccs, slot, &ncoef[i]);
+                if (rc) return rc;
+                kind[i] = 1;
+            } else if (cl[i].mem && cl[i].deg + 1 <= MAX_SLOT && neo_gpu_mem_oracle_degree_bound(cl[i].mem) == cl[i].deg &&
+                       mem_round_multi_ok(cl[i].mem)) {
+                mos.push_back(cl[i].mem);
+                mdst.push_back(slot);
+                kind[i] = 2;
+            }
+        }
+        for (size_t i0 = 0; i0 < mos.size(); i0 += 24) {
+            const int nn = (int)std::min<size_t>(24, mos.size() - i0);
+            int rc = mem_round_launch_multi(ctx, mos.data() + i0, nn, mdst.data() + i0, sh->d_mpart);
+            if (rc) return rc;
+        }
+        NEO_CK(ctx, cudaMemcpyAsync(sh->h_round.p, sh->d_round.p, cl.size() * MAX_SLOT * sizeof(K),
+                                    cudaMemcpyDeviceToHost, ctx->stream));
+        NEO_CK(ctx, ctx_sync(ctx));
         for (size_t i = 0; i < cl.size(); i++) {
             const uint32_t np = cl[i].deg + 1;
             std::vector<K> xs(np), ys(np);
             for (uint32_t x = 0; x < np; x++) xs[x] = gl::kfq(x);
-            int rc = cl[i].evals(xs.data(), np, ys.data());
-            if (rc) return rc;
+            const K* h = sh->h_round.p + i * MAX_SLOT;
+            if (kind[i] == 1) {
+                // values at 0..deg from the coefficients (Horner, sumcheck.rs:48-60)
+                ccs_oracle_round_set(cl[i].ccs, h);
+                std::vector<K> co(h, h + ncoef[i]);
+                for (uint32_t x = 0; x < np; x++) ys[x] = poly_eval(co, xs[x]);
+            } else if (kind[i] == 2) {
+                for (uint32_t x = 0; x < np; x++) ys[x] = h[x];
+            } else {
+                int rc = cl[i].evals(xs.data(), np, ys.data());
+                if (rc) return rc;
+            }
             if (!keq(gl::kadd(ys[0], ys[1]), running[i]))
                 return ctx->fail(NEO_ERR_INVARIANT, ("batched sum-check " + cl[i].label + ": p(0)+p(1) != running sum").c_str());
             interpolate(xs, ys, polys[i]);

@@ -123,6 +123,30 @@ struct DevBuf {
     size_t bytes() const { return n * sizeof(T); }
 };
 
+// Page-locked host buffer: a cudaMemcpyAsync from or to it is queued on the
+// stream and does not wait for the stream's earlier work (a pageable source
+// makes the copy synchronous).  Reused across rounds; freed on scope exit.
+template <typename T>
+struct HostBuf {
+    T* p = nullptr;
+    size_t cap = 0;
+    HostBuf() = default;
+    HostBuf(const HostBuf&) = delete;
+    HostBuf& operator=(const HostBuf&) = delete;
+    ~HostBuf() {
+        if (p) cudaFreeHost(p);
+    }
+    cudaError_t ensure(size_t count) {
+        if (p && count <= cap) return cudaSuccess;
+        if (p) cudaFreeHost(p);
+        p = nullptr;
+        cap = 0;
+        cudaError_t e = cudaHostAlloc(reinterpret_cast<void**>(&p), (count ? count : 1) * sizeof(T), cudaHostAllocDefault);
+        if (e == cudaSuccess) cap = count;
+        return e;
+    }
+};
+
 // Device-side CCS copy in both CSR (row SpMV) and CSC (transposed SpMV) form.
 struct DevCcs {
     uint32_t n = 0, m = 0, t = 0;

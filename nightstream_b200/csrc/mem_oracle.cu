@@ -312,6 +312,155 @@ __global__ void __launch_bounds__(256) dot_kernel(const K* __restrict__ a, const
     }
 }
 
+// ---- all memory claims of one sum-check round in three launches ----------
+// A batched round (the Route-A time claims, the val-eval batch, the address
+// pre-time batches) evaluates every claim's round polynomial at x = 0..deg
+// before the transcript draws the next challenge.  These kernels fold, evaluate
+// and reduce the tables of up to MULTI_MAX claims together; the values land in
+// one device array that the host reads with a single copy.
+constexpr int MULTI_MAX = 24;
+constexpr int MX = 8;  // evaluation points per pass (thread-local accumulators)
+
+struct MultiClaim {
+    const K* tab;      // [nf][len] current tables
+    K* dst;            // fold destination [nf][len / 2] (fold kernel)
+    uint64_t len;
+    uint32_t nf, npts;
+    int bitness;
+    const K* w;        // bitness weights [nf - 1]
+    K r;               // fold challenge
+    uint32_t blk0;     // first block of this claim
+    uint32_t part0;    // first partial [npts][nblk]
+    uint32_t nblk;
+    K* out;            // values at x = 0..npts-1 (reduce kernel)
+};
+
+struct MultiArgs {
+    int n;
+    MultiClaim c[MULTI_MAX];
+    K* partials;
+};
+
+__device__ __forceinline__ int multi_claim_of(const MultiArgs& a, uint32_t blk) {
+    int c = 0;
+    while (c + 1 < a.n && blk >= a.c[c + 1].blk0) c++;
+    return c;
+}
+
+// fold every claim's tables by its challenge: dst[f][t] = lerp(tab[f][2t], tab[f][2t+1], r)
+__global__ void __launch_bounds__(256) mem_multi_fold_kernel(const __grid_constant__ MultiArgs a) {
+    const int ci = multi_claim_of(a, blockIdx.x);
+    const MultiClaim& c = a.c[ci];
+    const uint64_t half = c.len >> 1;
+    const uint64_t i = (uint64_t)(blockIdx.x - c.blk0) * 256 + threadIdx.x;
+    if (i >= half * c.nf) return;
+    const uint64_t f = i / half, t = i % half;
+    const K* s = c.tab + f * c.len + 2 * t;
+    c.dst[f * half + t] = gl::klerp(s[0], s[1], c.r);
+}
+
+// One thread per pair of one claim: the claim's factor pairs are read once per
+// MX points, the product (or the bitness sum) evaluated at those points with
+// additions along x, and each point reduced over the block.
+__global__ void __launch_bounds__(256) mem_multi_eval_kernel(const __grid_constant__ MultiArgs a) {
+    __shared__ K s_red[256 / 32][MX];
+    const int ci = multi_claim_of(a, blockIdx.x);
+    const MultiClaim& c = a.c[ci];
+    const uint32_t b = blockIdx.x - c.blk0;
+    const uint64_t pairs = c.len >> 1;
+    const uint64_t p = (uint64_t)b * 256 + threadIdx.x;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    // a pair whose gate factor (the first, or every bitness column) is zero on
+    // both children contributes nothing at any x
+    bool live = p < pairs;
+    if (live && !c.bitness) {
+        const K* s = c.tab + 2 * p;
+        live = !(gl::kiszero(s[0]) && gl::kiszero(s[1]));
+    }
+    for (uint32_t x0 = 0; x0 < c.npts; x0 += MX) {
+        K acc[MX];
+#pragma unroll
+        for (int i = 0; i < MX; i++) acc[i] = live ? (c.bitness ? gl::kzero() : gl::kone()) : gl::kzero();
+        if (live) {
+            if (!c.bitness) {
+                for (uint32_t f = 0; f < c.nf; f++) {
+                    const K* s = c.tab + (uint64_t)f * c.len + 2 * p;
+                    const K f0 = s[0], d = gl::ksub(s[1], f0);
+                    K v = gl::kadd(f0, gl::kscale_small(d, (int32_t)x0));
+#pragma unroll
+                    for (int i = 0; i < MX; i++) {
+                        acc[i] = gl::kmul(acc[i], v);
+                        v = gl::kadd(v, d);
+                    }
+                }
+            } else {
+                for (uint32_t f = 1; f < c.nf; f++) {
+                    const K* s = c.tab + (uint64_t)f * c.len + 2 * p;
+                    if (gl::kiszero(s[0]) && gl::kiszero(s[1])) continue;  // b(b - 1) = 0 at every x
+                    const K f0 = s[0], d = gl::ksub(s[1], f0), w = c.w[f - 1];
+                    K v = gl::kadd(f0, gl::kscale_small(d, (int32_t)x0));
+#pragma unroll
+                    for (int i = 0; i < MX; i++) {
+                        acc[i] = gl::kadd(acc[i], gl::kmul(w, gl::kmul(v, gl::ksub(v, gl::kone()))));
+                        v = gl::kadd(v, d);
+                    }
+                }
+                const K* s = c.tab + 2 * p;
+                const K f0 = s[0], d = gl::ksub(s[1], f0);
+                K v = gl::kadd(f0, gl::kscale_small(d, (int32_t)x0));
+#pragma unroll
+                for (int i = 0; i < MX; i++) {
+                    acc[i] = gl::kmul(acc[i], v);
+                    v = gl::kadd(v, d);
+                }
+            }
+        }
+        const bool any = __syncthreads_or(live);
+        if (!any) {
+            if (threadIdx.x < MX && x0 + threadIdx.x < c.npts)
+                a.partials[c.part0 + (uint64_t)(x0 + threadIdx.x) * c.nblk + b] = gl::kzero();
+            continue;
+        }
+#pragma unroll
+        for (int i = 0; i < MX; i++) {
+            K v = acc[i];
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) v = gl::kadd(v, shfl_xor_km(v, o));
+            if (lane == 0) s_red[warp][i] = v;
+        }
+        __syncthreads();
+        if (threadIdx.x < MX && x0 + threadIdx.x < c.npts) {
+            K v = gl::kzero();
+#pragma unroll
+            for (int w = 0; w < 256 / 32; w++) v = gl::kadd(v, s_red[w][threadIdx.x]);
+            a.partials[c.part0 + (uint64_t)(x0 + threadIdx.x) * c.nblk + b] = v;
+        }
+        __syncthreads();
+    }
+}
+
+// out[x] = sum of the claim's block partials at x; one block per (claim, x)
+__global__ void __launch_bounds__(256) mem_multi_reduce_kernel(const __grid_constant__ MultiArgs a) {
+    __shared__ K s_red[8];
+    uint32_t rest = blockIdx.x;
+    int ci = 0;
+    while (rest >= a.c[ci].npts) { rest -= a.c[ci].npts; ci++; }
+    const MultiClaim& c = a.c[ci];
+    const uint32_t x = rest;
+    K v = gl::kzero();
+    for (uint32_t b = threadIdx.x; b < c.nblk; b += 256) v = gl::kadd(v, a.partials[c.part0 + (uint64_t)x * c.nblk + b]);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = gl::kadd(v, shfl_xor_km(v, o));
+    if (lane == 0) s_red[warp] = v;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        K t = gl::kzero();
+        for (int w = 0; w < 8; w++) t = gl::kadd(t, s_red[w]);
+        c.out[x] = t;
+    }
+}
+
 inline K kload_h(const uint64_t* p) { return gl::kmk(p[0], p[1]); }
 
 }  // namespace
@@ -597,6 +746,82 @@ int mem_create(neo_gpu_ctx* ctx, int kind, uint32_t ell, const uint64_t* r_point
 }
 
 }  // namespace
+
+// True when the oracle's next round has at least one pair (its pending fold
+// applied): the rounds that mem_round_launch_multi evaluates.
+bool mem_round_multi_ok(const neo_gpu_mem_oracle* o) {
+    const uint64_t len = o->pending ? o->len >> 1 : o->len;
+    return len >= 2 && o->deg + 1 <= MEM_MAX_DEG + 1;
+}
+
+// The next round of n oracles: pending folds, then the values at x = 0..deg
+// of oracle i into d_out[i] (device), in three launches and without a host
+// sync.  Every oracle must satisfy mem_round_multi_ok; n <= MULTI_MAX.
+int mem_round_launch_multi(neo_gpu_ctx* ctx, neo_gpu_mem_oracle* const* os, int n, K* const* d_out,
+                           DevBuf<K>& partials) {
+    if (n <= 0) return NEO_OK;
+    if (n > MULTI_MAX) return ctx->fail(NEO_ERR_UNSUPPORTED, "mem_round_launch_multi: too many claims");
+    // folds
+    MultiArgs f{};
+    uint32_t blocks = 0;
+    for (int i = 0; i < n; i++) {
+        neo_gpu_mem_oracle* o = os[i];
+        if (!o->pending) continue;
+        MultiClaim& c = f.c[f.n++];
+        c.tab = o->tab[o->cur].p;
+        c.dst = o->tab[o->cur ^ 1].p;
+        c.len = o->len;
+        c.nf = o->nf;
+        c.r = o->pending_r;
+        c.blk0 = blocks;
+        blocks += (uint32_t)ceil_div((o->len >> 1) * o->nf, 256);
+    }
+    if (f.n) {
+        mem_multi_fold_kernel<<<blocks, 256, 0, ctx->stream>>>(f);
+        NEO_LAUNCHED(ctx);
+        for (int i = 0; i < n; i++) {
+            neo_gpu_mem_oracle* o = os[i];
+            if (!o->pending) continue;
+            o->cur ^= 1;
+            o->len >>= 1;
+            o->pending = false;
+        }
+    }
+    // evaluations
+    MultiArgs a{};
+    a.n = n;
+    blocks = 0;
+    uint64_t parts = 0;
+    uint32_t pts = 0;
+    for (int i = 0; i < n; i++) {
+        neo_gpu_mem_oracle* o = os[i];
+        if (o->len < 2) return ctx->fail(NEO_ERR_INVARIANT, "mem_round_launch_multi: no pairs left");
+        MultiClaim& c = a.c[i];
+        c.tab = o->tab[o->cur].p;
+        c.len = o->len;
+        c.nf = o->nf;
+        c.npts = o->deg + 1;
+        c.bitness = o->bitness;
+        c.w = o->w.p;
+        c.blk0 = blocks;
+        c.nblk = (uint32_t)ceil_div(o->len >> 1, 256);
+        c.part0 = (uint32_t)parts;
+        c.out = d_out[i];
+        blocks += c.nblk;
+        parts += (uint64_t)c.npts * c.nblk;
+        pts += c.npts;
+    }
+    if (parts > 0xFFFFFFFFull) return ctx->fail(NEO_ERR_UNSUPPORTED, "mem_round_launch_multi: too many partials");
+    NEO_CK(ctx, partials.ensure(parts));
+    a.partials = partials.p;
+    mem_multi_eval_kernel<<<blocks, 256, 0, ctx->stream>>>(a);
+    NEO_LAUNCHED(ctx);
+    mem_multi_reduce_kernel<<<pts, 256, 0, ctx->stream>>>(a);
+    NEO_LAUNCHED(ctx);
+    return NEO_OK;
+}
+
+
 
 static int neo_gpu_mem_oracle_create_impl_abi(neo_gpu_ctx* ctx, int kind, uint32_t ell, const uint64_t* r_point,
                                          uint32_t ell_addr, const uint64_t* r_addr, const uint64_t* init_at_r_addr,

@@ -51,6 +51,10 @@ SIGNATURES = {
     "neo_gpu_commit_device": [P, ctypes.c_void_p, U32, U64, ctypes.c_void_p],
     "neo_gpu_commit_noalloc": [P, ctypes.c_void_p, U32, U64, ctypes.c_void_p],
     "neo_gpu_mix_rhos_commits": [P, P, P, U32, U32, P],
+    "neo_gpu_ccs_autotune": [P, P, P, U32, U32, P],
+    "neo_gpu_tune_load": [ctypes.c_char_p],
+    "neo_gpu_tune_save": [ctypes.c_char_p],
+    "neo_gpu_tune_get": [U32, U32, P],
     "neo_gpu_combine_b_pows": [P, P, U32, U32, U32, P],
     "neo_gpu_shard_step_stats": [P, P, U32],
     "neo_gpu_shard_create": [P, P, U32, U32, ctypes.c_char_p, P],
@@ -115,6 +119,28 @@ _RESTYPES = {
 }
 
 _lib = None
+
+
+TUNE_FILE = os.path.join(os.path.dirname(os.path.abspath(__file__)), "tune_b200.txt")
+
+
+def tune_load(path: str = TUNE_FILE) -> bool:
+    """Load a launch-shape table (neo_gpu_tune_load); False when the file is absent."""
+    if not os.path.exists(path):
+        return False
+    return load().neo_gpu_tune_load(path.encode()) == 0
+
+
+def tune_save(path: str):
+    if load().neo_gpu_tune_save(path.encode()):
+        raise NeoGpuError(1, f"tune_save {path}")
+
+
+def tune_get(ell_n: int, k: int):
+    out = np.zeros(3, np.uint64)
+    if load().neo_gpu_tune_get(ell_n, k, _p(out)):
+        return None
+    return tuple(int(x) for x in out)
 
 
 class NeoGpuError(RuntimeError):
@@ -206,6 +232,16 @@ class Context:
         out = np.empty((kappa, 54), np.uint64)
         self.check(self.lib.neo_gpu_combine_b_pows(self.h, _p(cs), count, kappa, b, _p(out)))
         return out
+
+    def ccs_autotune(self, ccs, Z: np.ndarray, reps: int = 3):
+        """Time every launch choice of the Pi_CCS row rounds on this CCS and the
+        digit matrices Z [k][54][m]; the best is recorded for (ell_n, k) and
+        returned as (nc_threads, compact_q, hist_items)."""
+        Zs = _i8(Z)
+        desc = ccs.desc()
+        out = np.zeros(3, np.uint64)
+        self.check(self.lib.neo_gpu_ccs_autotune(self.h, ctypes.byref(desc), _p(Zs), Zs.shape[0], reps, _p(out)))
+        return tuple(int(x) for x in out)
 
     def close(self):
         if getattr(self, "h", None):

@@ -113,6 +113,10 @@ extern "C" {
     pub fn neo_gpu_ccs_oracle_degree_bound(o: *const neo_gpu_ccs_oracle) -> u32;
     pub fn neo_gpu_ccs_oracle_me_outputs(o: *mut neo_gpu_ccs_oracle, y: *mut u64, y_scalars: *mut u64) -> c_int;
     pub fn neo_gpu_ccs_oracle_destroy(o: *mut neo_gpu_ccs_oracle) -> c_int;
+    pub fn neo_gpu_ccs_autotune(ctx: *mut neo_gpu_ctx, ccs: *const neo_ccs_desc, Z: *const i8, k: u32, reps: u32, out3: *mut u64) -> c_int;
+    pub fn neo_gpu_tune_load(path: *const c_char) -> c_int;
+    pub fn neo_gpu_tune_save(path: *const c_char) -> c_int;
+    pub fn neo_gpu_tune_get(ell_n: u32, k: u32, out3: *mut u64) -> c_int;
     pub fn neo_gpu_mem_oracle_create(ctx: *mut neo_gpu_ctx, kind: c_int, ell: u32, r_point: *const u64, ell_addr: u32, r_addr: *const u64, init_at_r_addr: *const u64, n_cols: u32, cols: *const u64, weights: *const u64, claim: *mut u64, out: *mut *mut neo_gpu_mem_oracle) -> c_int;
     pub fn neo_gpu_mem_oracle_create_device(ctx: *mut neo_gpu_ctx, kind: c_int, ell: u32, r_point: *const u64, ell_addr: u32, r_addr: *const u64, init_at_r_addr: *const u64, n_cols: u32, d_cols: *const u64, weights: *const u64, claim: *mut u64, out: *mut *mut neo_gpu_mem_oracle) -> c_int;
     pub fn neo_gpu_mem_oracle_evals(o: *mut neo_gpu_mem_oracle, xs: *const u64, nx: u32, ys: *mut u64) -> c_int;

@@ -50,3 +50,16 @@ def test_rust_bindings_cover_the_header():
            for n, args in re.findall(r"pub fn (neo_\w+)\(([^)]*)\)", rs)}
     assert decl, "no declarations parsed"
     assert decl == got
+
+
+def test_tune_table_round_trip(tmp_path):
+    """The launch-shape table loads from and saves to its text form, without a GPU."""
+    p = tmp_path / "tune.txt"
+    p.write_text("ccs 18 13 75776 8 16384\nccs 10 3 37888 0 8192\nbogus line\n")
+    assert gpu.tune_load(str(p))
+    assert gpu.tune_get(18, 13) == (75776, 8, 16384)
+    assert gpu.tune_get(10, 3) == (37888, 0, 8192)
+    out = tmp_path / "out.txt"
+    gpu.tune_save(str(out))
+    lines = out.read_text().split("\n")
+    assert "ccs 18 13 75776 8 16384" in lines and "ccs 10 3 37888 0 8192" in lines

@@ -200,3 +200,15 @@ def test_commit_mixers_match_definition(ctx):
     got = ctx.combine_b_pows(cs[:12], 2)
     want = [[sum(pow(2, i, Q) * C[i][c][r] for i in range(12)) % Q for r in range(54)] for c in range(kappa)]
     assert np.array_equal(got, np.array(want, dtype=np.uint64))
+
+
+def test_autotuned_rounds_match_oracle(ctx):
+    """The autotuner picks launch choices for (ell_n, k) on a real shape; an
+    oracle created afterwards uses them and still equals the oracle in every
+    round."""
+    from nightstream_b200 import gpu
+    ell, k = 11, 4
+    ccs, z, Z, ch, chals = ccs_case(ell, k, True, seed=41)
+    best = ctx.ccs_autotune(ccs, Z, reps=1)
+    assert gpu.tune_get(ell, k) == best
+    _run_both(ctx, ell, k, True, seed=41)
