@@ -369,6 +369,19 @@ int neo_gpu_shard_set_twist_init(neo_gpu_shard* sh, uint32_t mem_idx, uint64_t n
  * Pass NULL to query *proof_len. */
 int neo_gpu_shard_fold_step(neo_gpu_shard* sh, const uint64_t* z, uint64_t* proof, uint64_t proof_cap,
                             uint64_t* proof_len);
+/* The last fold step's proof in the field order of the reference's StepProof
+ * (crates/neo-fold/src/shard_proof_types.rs:45-131) -- fold {ccs_out,
+ * ccs_proof, rlc_rhos (54 x 54 Mat<F>), rlc_parent, dec_children}, mem
+ * {cpu_me_claims_val, shout_addr_pre, per-Twist address proofs, the Twist
+ * val-eval batch}, batched_time {claimed_sums, degree_bounds, labels,
+ * round_polys[claim][round]}, val_fold -- as a canonical word dump: every Vec
+ * prefixed by its length, K = (re, im), F and integers one word, [u8; 32]
+ * digests four little-endian words, byte strings a length then 8 bytes per
+ * word, Option a 0 / 1 word then the value.  MeInstance = {c (d, kappa,
+ * data), X (rows, cols, data), r, y (rows of 2^ell_d K), y_scalars, m_in,
+ * fold_digest, c_step_coords, u_offset, u_len}.  out == NULL only sets *len.
+ * The field-by-field map is in INTEGRATION.md; oracle/verify.py reads it. */
+int neo_gpu_shard_step_proof(neo_gpu_shard* sh, uint64_t* out, uint64_t cap, uint64_t* len);
 /* Same step with the witness already resident in device memory (d_z). */
 int neo_gpu_shard_fold_step_device(neo_gpu_shard* sh, const uint64_t* d_z, uint64_t* proof_len);
 /* Transcript sponge state (8 words) and CCS matrix digest (4 words). */

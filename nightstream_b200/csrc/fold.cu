@@ -224,6 +224,42 @@ __global__ void __launch_bounds__(256) bus_open_kernel(const int8_t* __restrict_
 }  // namespace
 
 // ---------------------------------------------------------------------------
+// The last fold step in the field order of the reference's StepProof
+// (crates/neo-fold/src/shard_proof_types.rs:45-131): the pieces the
+// transcript-order proof dump interleaves, kept for neo_gpu_shard_step_proof.
+struct BatchRec {  // one batched sum-check (BatchedTimeProof-like)
+    std::vector<std::string> labels;
+    std::vector<uint32_t> degs;
+    std::vector<K> sums;
+    std::vector<std::vector<std::vector<K>>> polys;  // [claim][round][coefficient]
+    std::vector<K> chals, finals;
+};
+struct LaneRec {  // RlcDecProof
+    bool present = false;
+    std::vector<int8_t> rhos;  // [k][54] coefficients of rho_i = rot(a_i)
+    MeInst parent;
+    std::vector<MeInst> children;
+};
+struct StepRecord {
+    bool valid = false;
+    std::vector<MeInst> ccs_out;
+    std::vector<std::vector<K>> ajtai_polys;  // PiCcsProof::sumcheck_rounds (the Ajtai rounds)
+    std::vector<K> ajtai_chals;
+    K T{}, final_sum{};
+    std::vector<K> alpha, beta_a, beta_r;
+    K gamma{};
+    LaneRec main, val;
+    BatchRec time;
+    std::vector<MeInst> cpu_me_val;
+    bool has_shout = false;
+    std::vector<K> shout_sums;
+    uint64_t shout_active = 0;
+    BatchRec shout_pre;
+    std::vector<BatchRec> twist_pre;
+    bool has_val_eval = false;
+    BatchRec val_eval;
+};
+
 struct neo_gpu_shard {
     neo_gpu_ctx* ctx = nullptr;
     DevCcs ccs;
@@ -232,6 +268,7 @@ struct neo_gpu_shard {
     // the multi-claim memory kernels
     DevBuf<K> d_round, d_mpart;
     HostBuf<K> h_round;
+    StepRecord rec;  // the last step, for neo_gpu_shard_step_proof
     uint32_t kappa = 16;
     uint32_t n = 0, m32 = 0, t = 0, ell_n = 0, ell_d = 6, d_sc = 6, k_rho = 12, b = 2, m_in = 1, lambda = 127;
     uint64_t m = 0;
@@ -767,7 +804,8 @@ struct Claim {
 // copy and sync bring the round back; Twist address-lane claims (and memory
 // claims whose tables are exhausted) take the per-claim path.
 static int run_batched_ds(neo_gpu_shard* sh, const char* domain, uint64_t inst_idx, std::vector<Claim>& cl,
-                          uint32_t rounds, std::vector<K>& chals, std::vector<K>& finals, std::vector<uint64_t>& P) {
+                          uint32_t rounds, std::vector<K>& chals, std::vector<K>& finals, std::vector<uint64_t>& P,
+                          BatchRec* rec = nullptr) {
     neo_gpu_ctx* ctx = sh->ctx;
     neo::Transcript& tr = *sh->tr;
     auto bi = le64(inst_idx);
@@ -776,6 +814,15 @@ static int run_batched_ds(neo_gpu_shard* sh, const char* domain, uint64_t inst_i
     std::vector<K> running(cl.size());
     for (size_t i = 0; i < cl.size(); i++) running[i] = cl[i].sum;
     std::vector<std::vector<K>> polys(cl.size());
+    if (rec) {
+        *rec = BatchRec();
+        for (auto& c : cl) {
+            rec->labels.push_back(c.label);
+            rec->degs.push_back(c.deg);
+            rec->sums.push_back(c.sum);
+        }
+        rec->polys.assign(cl.size(), {});
+    }
     // slots: MAX_SLOT K values per claim
     constexpr uint32_t MAX_SLOT = 33;
     NEO_CK(ctx, sh->d_round.ensure(cl.size() * MAX_SLOT));
@@ -846,11 +893,16 @@ static int run_batched_ds(neo_gpu_shard* sh, const char* domain, uint64_t inst_i
             int rc = cl[i].fold(r);
             if (rc) return rc;
             for (auto& c : polys[i]) push_k(P, c);
+            if (rec) rec->polys[i].push_back(polys[i]);
         }
     }
     tr.append_message("sc/domain_end", domain);
     tr.append_message("sc/inst_idx_end", bi.data(), 8);
     finals = running;
+    if (rec) {
+        rec->chals = chals;
+        rec->finals = finals;
+    }
     return NEO_OK;
 }
 
@@ -962,7 +1014,8 @@ static std::vector<uint32_t> twist_val_ids(const TwistInst& w) {
 // from vj, bus rows from the planes), DEC public checks.
 static int rlc_dec_lane(neo_gpu_shard* sh, const char* lane, uint32_t idx, const std::vector<MeInst>& ins,
                         const int8_t* d_wits, int8_t* d_planes, const std::vector<K>& r, const K* d_vj,
-                        const uint8_t* digest, std::vector<MeInst>& children, std::vector<uint64_t>& P) {
+                        const uint8_t* digest, std::vector<MeInst>& children, std::vector<uint64_t>& P,
+                        LaneRec* rec = nullptr) {
     neo_gpu_ctx* ctx = sh->ctx;
     neo::Transcript& tr = *sh->tr;
     const uint32_t k = (uint32_t)ins.size(), t = sh->t, kappa = sh->kappa, nb = sh->bus_cols;
@@ -1108,6 +1161,30 @@ static int rlc_dec_lane(neo_gpu_shard* sh, const char* lane, uint32_t idx, const
         for (uint32_t c = 0; c < nb; c++)
             for (int rho = 0; rho < NEO_D; rho++) push_k(P, ch.y[(size_t)(t + c) * d_pad + rho]);
     }
+    if (rec) {
+        // the RLC parent: c from the mix; X, y and y_scalars recomposed from the
+        // children (sum_i b^i child_i, exact: DEC splits the parent's digits)
+        rec->present = true;
+        rec->rhos = rhos;
+        rec->children = children;
+        MeInst& pa = rec->parent;
+        pa = MeInst();
+        pa.c = c_parent;
+        pa.m_in = sh->m_in;
+        pa.r = r;
+        memcpy(pa.digest, digest, 32);
+        pa.X.assign((size_t)NEO_D * sh->m_in, 0);
+        pa.y.assign((size_t)(t + nb) * d_pad, gl::kzero());
+        pa.ysc.assign(t + nb, gl::kzero());
+        uint64_t pw = 1;
+        for (uint32_t i = 0; i < sh->k_rho; i++) {
+            const MeInst& ch = children[i];
+            for (size_t q = 0; q < pa.X.size(); q++) pa.X[q] = gl::add(pa.X[q], gl::mul(ch.X[q], pw));
+            for (size_t q = 0; q < pa.y.size(); q++) pa.y[q] = gl::kadd(pa.y[q], gl::kscale(ch.y[q], pw));
+            for (size_t q = 0; q < pa.ysc.size(); q++) pa.ysc[q] = gl::kadd(pa.ysc[q], gl::kscale(ch.ysc[q], pw));
+            pw = gl::mul(pw, sh->b);
+        }
+    }
     return NEO_OK;
 }
 
@@ -1127,6 +1204,8 @@ static int fold_step_impl(neo_gpu_shard* sh, const uint64_t* z_host, const uint6
     const bool has_mem = nb > 0;
     std::vector<uint64_t>& P = sh->proof;
     P.clear();
+    StepRecord& rec = sh->rec;
+    rec = StepRecord();
     int rc;
     const auto t_step = hclock::now();
     NvtxStep nv;
@@ -1287,6 +1366,11 @@ static int fold_step_impl(neo_gpu_shard* sh, const uint64_t* z_host, const uint6
     }
     absorb_k(tr, "sumcheck/initial_sum", T);
     push_k(P, T);
+    rec.alpha = alpha;
+    rec.beta_a = beta_a;
+    rec.beta_r = beta_r;
+    rec.gamma = gamma;
+    rec.T = T;
     // ---- r_cycle = sample_ext_point (neo-memory/src/ts_common.rs:22-37) ----
     std::vector<K> r_cycle = sample_ext_point(tr, "route_a/r_cycle", "route_a/cycle/0", "route_a/cycle/1", ell_n);
 
@@ -1384,6 +1468,9 @@ static int fold_step_impl(neo_gpu_shard* sh, const uint64_t* z_host, const uint6
                             std::vector<std::string>(sums.size(), "shout/addr_pre"));
             for (auto& s : sums) push_k(P, s);
             P.push_back(active);
+            rec.has_shout = true;
+            rec.shout_sums = sums;
+            rec.shout_active = active;
             if (active == 0) {
                 tr.append_message("shout/addr_pre_time/no_sumcheck", bi.data(), 8);
                 r_addr_s = sample_ext_point(tr, "shout/addr_pre_time/no_sumcheck/r_addr",
@@ -1391,8 +1478,10 @@ static int fold_step_impl(neo_gpu_shard* sh, const uint64_t* z_host, const uint6
                                             "shout/addr_pre_time/no_sumcheck/r_addr/1", ea);
             } else {
                 std::vector<K> fin;
-                if ((rc = run_batched_ds(sh, "shout/addr_pre_time", idx, ac, ea, r_addr_s, fin, P))) return rc;
+                if ((rc = run_batched_ds(sh, "shout/addr_pre_time", idx, ac, ea, r_addr_s, fin, P, &rec.shout_pre)))
+                    return rc;
             }
+            rec.shout_pre.chals = r_addr_s;
             for (auto& r : r_addr_s) push_k(P, r);
         }
         // ---- Twist address pre-time (memory.rs:232-428) ----
@@ -1419,7 +1508,9 @@ static int fold_step_impl(neo_gpu_shard* sh, const uint64_t* z_host, const uint6
             tc[0].label = labels[0]; tc[0].deg = 2; tc[0].sum = gl::kzero(); tc[0].ta = ro;
             tc[1].label = labels[1]; tc[1].deg = 2; tc[1].sum = gl::kzero(); tc[1].ta = wo;
             std::vector<K> fin;
-            if ((rc = run_batched_ds(sh, "twist/addr_pre_time", i, tc, w.ea, r_addr_t[i], fin, P))) return rc;
+            rec.twist_pre.emplace_back();
+            if ((rc = run_batched_ds(sh, "twist/addr_pre_time", i, tc, w.ea, r_addr_t[i], fin, P, &rec.twist_pre.back())))
+                return rc;
             for (auto& r : r_addr_t[i]) push_k(P, r);
             twist_read[i] = fin[0];
             twist_write[i] = fin[1];
@@ -1510,7 +1601,7 @@ static int fold_step_impl(neo_gpu_shard* sh, const uint64_t* z_host, const uint6
     }
     // ---- batched time sum-check (route_a_time.rs:28-152) ----
     std::vector<K> r_time, finals;
-    if ((rc = run_batched_ds(sh, "shard/batched_time", idx, claims, ell_n, r_time, finals, P))) return rc;
+    if ((rc = run_batched_ds(sh, "shard/batched_time", idx, claims, ell_n, r_time, finals, P, &rec.time))) return rc;
     K running = finals[0];
     sh->stats[4] = ms_since(t_ph);
     nv.next("ajtai_rounds");
@@ -1534,10 +1625,13 @@ static int fold_step_impl(neo_gpu_shard* sh, const uint64_t* z_host, const uint6
         running = poly_eval(co, r);
         if ((rc = neo_gpu_ccs_oracle_fold(orc, (const uint64_t*)&r))) return rc;
         for (auto& c : co) push_k(P, c);
+        rec.ajtai_polys.push_back(co);
+        rec.ajtai_chals.push_back(r);
     }
     tr.append_message("sc/domain_end", "ccs/ajtai");
     tr.append_message("sc/inst_idx_end", bidx.data(), 8);
     push_k(P, running);
+    rec.final_sum = running;
     uint8_t fold_digest[32];
     tr.digest32(fold_digest);
 
@@ -1572,6 +1666,7 @@ static int fold_step_impl(neo_gpu_shard* sh, const uint64_t* z_host, const uint6
         }
         memcpy(o.digest, fold_digest, 32);
     }
+    rec.ccs_out = outs;
     for (auto& v : y_eval) push_k(P, v);
     for (auto& v : y_sc) push_k(P, v);
     for (uint32_t i = 0; i < k && nb; i++) {
@@ -1635,7 +1730,8 @@ static int fold_step_impl(neo_gpu_shard* sh, const uint64_t* z_host, const uint6
             push_k(P, vcl[i].sum);
         }
         std::vector<K> fin;
-        if ((rc = run_batched_ds(sh, "twist/val_eval_batch", idx, vcl, ell_n, r_val, fin, P))) return rc;
+        rec.has_val_eval = true;
+        if ((rc = run_batched_ds(sh, "twist/val_eval_batch", idx, vcl, ell_n, r_val, fin, P, &rec.val_eval))) return rc;
         tr.append_message("twist/val_eval/batch_done", nullptr, 0);
         for (auto& r : r_val) push_k(P, r);
         // emit_me_claims_for_mats (neo-memory/src/ts_common.rs:100-258): fold digest of the fork
@@ -1680,6 +1776,7 @@ static int fold_step_impl(neo_gpu_shard* sh, const uint64_t* z_host, const uint6
             for (auto& s : me.ysc) push_k(P, s);
             val_claims.push_back(std::move(me));
         }
+        rec.cpu_me_val = val_claims;
         mem_ms += ms_since(t_mem);
     }
 
@@ -1688,7 +1785,7 @@ static int fold_step_impl(neo_gpu_shard* sh, const uint64_t* z_host, const uint6
     if ((rc = ccs_oracle_dev_vj(orc, &vj))) return rc;
     std::vector<MeInst> children;
     if ((rc = rlc_dec_lane(sh, "main", idx, outs, sh->Zall.p, sh->Zall.p + (size_t)NEO_D * m, r_time, vj, fold_digest,
-                           children, P)))
+                           children, P, &rec.main)))
         return rc;
     sh->stats[7] = ms_since(t_ph);
     nv.next("val_lane");
@@ -1699,7 +1796,7 @@ static int fold_step_impl(neo_gpu_shard* sh, const uint64_t* z_host, const uint6
         // v_j = M_j^T chi(r_val) is still in d_vj from the CPU ME claims
         std::vector<MeInst> vch;
         if ((rc = rlc_dec_lane(sh, "val", idx, val_claims, sh->valwit.p, sh->valplanes.p, r_val, sh->d_vj.p, vdigest, vch,
-                               P)))
+                               P, &rec.val)))
             return rc;
         sh->val_obligations += vch.size();
     }
@@ -1717,6 +1814,7 @@ static int fold_step_impl(neo_gpu_shard* sh, const uint64_t* z_host, const uint6
         sh->has_prev = true;
     }
     sh->step_idx++;
+    rec.valid = true;
     sh->stats[8] = ms_since(t_ph);
     nv.pop();
     sh->stats[10] = mem_ms;
@@ -1753,6 +1851,179 @@ static int neo_gpu_shard_fold_step_device_impl_abi(neo_gpu_shard* sh, const uint
     return NEO_OK;
 }
 extern "C" int neo_gpu_shard_fold_step_device(neo_gpu_shard* sh, const uint64_t* d_z, uint64_t* proof_len) { NEO_ABI_GUARD(neo_gpu_shard_fold_step_device_impl_abi(sh, d_z, proof_len)) }
+
+// ---------------------------------------------------------------------------
+// StepProof in struct order (crates/neo-fold/src/shard_proof_types.rs:45-131):
+// a canonical word dump, every Vec prefixed by its length, K = (re, im),
+// F and integers one word, [u8; 32] digests four little-endian words, byte
+// strings a length then 8 bytes per word, Option a 0 / 1 word then the value.
+// ---------------------------------------------------------------------------
+namespace {
+struct WordWriter {
+    std::vector<uint64_t> w;
+    void u(uint64_t v) { w.push_back(v); }
+    void k(K v) {
+        w.push_back(v.re);
+        w.push_back(v.im);
+    }
+    void fvec(const std::vector<uint64_t>& v) {
+        u(v.size());
+        w.insert(w.end(), v.begin(), v.end());
+    }
+    void kvec(const std::vector<K>& v) {
+        u(v.size());
+        for (auto& x : v) k(x);
+    }
+    void digest(const uint8_t* d) {
+        for (int i = 0; i < 4; i++) {
+            uint64_t x = 0;
+            for (int b = 0; b < 8; b++) x |= (uint64_t)d[8 * i + b] << (8 * b);
+            u(x);
+        }
+    }
+    void bytes(const std::string& s) {
+        u(s.size());
+        for (size_t i = 0; i < s.size(); i += 8) {
+            uint64_t x = 0;
+            for (size_t b = 0; b < 8 && i + b < s.size(); b++) x |= (uint64_t)(uint8_t)s[i + b] << (8 * b);
+            u(x);
+        }
+    }
+};
+
+// MeInstance (crates/neo-ccs/src/relations.rs:234-258): c, X, r, y, y_scalars,
+// m_in, fold_digest, c_step_coords (empty), u_offset, u_len (0)
+void write_me(WordWriter& W, const MeInst& me, uint32_t kappa, uint32_t d_pad) {
+    W.u(NEO_D);
+    W.u(kappa);
+    W.fvec(me.c);
+    W.u(NEO_D);
+    W.u(me.m_in);
+    W.fvec(me.X);
+    W.kvec(me.r);
+    const size_t rows = me.y.size() / d_pad;
+    W.u(rows);
+    for (size_t r = 0; r < rows; r++) {
+        W.u(d_pad);
+        for (uint32_t e = 0; e < d_pad; e++) W.k(me.y[r * d_pad + e]);
+    }
+    W.kvec(me.ysc);
+    W.u(me.m_in);
+    W.digest(me.digest);
+    W.u(0);
+    W.u(0);
+    W.u(0);
+}
+
+void write_mes(WordWriter& W, const std::vector<MeInst>& v, uint32_t kappa, uint32_t d_pad) {
+    W.u(v.size());
+    for (auto& me : v) write_me(W, me, kappa, d_pad);
+}
+
+// rho_i = rot(a_i): column j = cf(a_i X^j mod Phi_81) (X^54 = -X^27 - 1); the
+// identity when the lane mixes one instance (common.rs:557-562)
+void write_rhos(WordWriter& W, const std::vector<int8_t>& rhos, uint32_t k) {
+    W.u(k);
+    for (uint32_t i = 0; i < k; i++) {
+        int64_t R[NEO_D][NEO_D];
+        int64_t col[NEO_D];
+        for (int q = 0; q < NEO_D; q++) col[q] = rhos[(size_t)i * NEO_D + q];
+        for (int j = 0; j < NEO_D; j++) {
+            for (int q = 0; q < NEO_D; q++) R[q][j] = k == 1 ? (q == j) : col[q];
+            const int64_t last = col[NEO_D - 1];
+            for (int q = NEO_D - 1; q > 0; q--) col[q] = col[q - 1];
+            col[0] = -last;
+            col[27] -= last;
+        }
+        W.u(NEO_D);
+        W.u(NEO_D);
+        W.u((uint64_t)NEO_D * NEO_D);
+        for (int q = 0; q < NEO_D; q++)
+            for (int j = 0; j < NEO_D; j++) W.u(gl::from_i64(R[q][j]));
+    }
+}
+
+void write_polys(WordWriter& W, const std::vector<std::vector<std::vector<K>>>& polys) {
+    W.u(polys.size());
+    for (auto& claim : polys) {
+        W.u(claim.size());
+        for (auto& round : claim) W.kvec(round);
+    }
+}
+
+void write_lane(WordWriter& W, const LaneRec& L, uint32_t kappa, uint32_t d_pad) {
+    write_rhos(W, L.rhos, (uint32_t)(L.rhos.size() / NEO_D));
+    write_me(W, L.parent, kappa, d_pad);
+    write_mes(W, L.children, kappa, d_pad);
+}
+}  // namespace
+
+static int neo_gpu_shard_step_proof_impl_abi(neo_gpu_shard* sh, uint64_t* out, uint64_t cap, uint64_t* len) {
+    if (!sh || !len) return NEO_ERR_ARG;
+    const StepRecord& R = sh->rec;
+    if (!R.valid) return sh->ctx->fail(NEO_ERR_ARG, "step_proof: no completed fold step");
+    const uint32_t kappa = sh->kappa, d_pad = 1u << sh->ell_d;
+    WordWriter W;
+    // fold: FoldStep
+    write_mes(W, R.ccs_out, kappa, d_pad);
+    W.u(R.ajtai_polys.size());  // PiCcsProof::sumcheck_rounds
+    for (auto& co : R.ajtai_polys) W.kvec(co);
+    W.u(1);  // sc_initial_sum: Some(T)
+    W.k(R.T);
+    {
+        std::vector<K> ch = R.time.chals;  // sumcheck_challenges: r_time || alpha'
+        ch.insert(ch.end(), R.ajtai_chals.begin(), R.ajtai_chals.end());
+        W.kvec(ch);
+    }
+    W.kvec(R.alpha);  // challenges_public
+    W.kvec(R.beta_a);
+    W.kvec(R.beta_r);
+    W.k(R.gamma);
+    W.k(R.final_sum);  // sumcheck_final
+    W.u(0);            // header_digest: empty
+    W.u(0);            // _extra: None
+    write_lane(W, R.main, kappa, d_pad);
+    // mem: MemSidecarProof
+    write_mes(W, R.cpu_me_val, kappa, d_pad);
+    W.u(R.has_shout ? 1 : 0);  // shout_addr_pre
+    if (R.has_shout) {
+        W.kvec(R.shout_sums);
+        W.u(R.shout_active);
+        write_polys(W, R.shout_pre.polys);
+        W.kvec(R.shout_pre.chals);
+    }
+    W.u(R.twist_pre.size());  // proofs: one Twist proof per instance (tag 0)
+    for (auto& tp : R.twist_pre) {
+        W.u(0);
+        write_polys(W, tp.polys);
+        W.kvec(tp.chals);
+        W.kvec(tp.finals);
+    }
+    W.u(R.has_val_eval ? 1 : 0);  // Twist val-eval batch
+    if (R.has_val_eval) {
+        W.kvec(R.val_eval.sums);
+        write_polys(W, R.val_eval.polys);
+        W.kvec(R.val_eval.chals);
+    }
+    // batched_time: BatchedTimeProof
+    W.kvec(R.time.sums);
+    W.u(R.time.degs.size());
+    for (auto d : R.time.degs) W.u(d);
+    W.u(R.time.labels.size());
+    for (auto& l : R.time.labels) W.bytes(l);
+    write_polys(W, R.time.polys);
+    // val_fold: Option<RlcDecProof>
+    W.u(R.val.present ? 1 : 0);
+    if (R.val.present) write_lane(W, R.val, kappa, d_pad);
+    *len = W.w.size();
+    if (!out) return NEO_OK;
+    if (cap < W.w.size()) return sh->ctx->fail(NEO_ERR_ARG, "step_proof: buffer too small");
+    memcpy(out, W.w.data(), W.w.size() * 8);
+    return NEO_OK;
+}
+extern "C" int neo_gpu_shard_step_proof(neo_gpu_shard* sh, uint64_t* out, uint64_t cap, uint64_t* len) {
+    NEO_ABI_GUARD(neo_gpu_shard_step_proof_impl_abi(sh, out, cap, len))
+}
 
 static int neo_gpu_shard_transcript_state_impl_abi(const neo_gpu_shard* sh, uint64_t* st8) {
     if (!sh || !st8) return NEO_ERR_ARG;

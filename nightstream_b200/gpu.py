@@ -51,6 +51,7 @@ SIGNATURES = {
     "neo_gpu_commit_device": [P, ctypes.c_void_p, U32, U64, ctypes.c_void_p],
     "neo_gpu_commit_noalloc": [P, ctypes.c_void_p, U32, U64, ctypes.c_void_p],
     "neo_gpu_mix_rhos_commits": [P, P, P, U32, U32, P],
+    "neo_gpu_shard_step_proof": [P, P, U64, P],
     "neo_gpu_ccs_autotune": [P, P, P, U32, U32, P],
     "neo_gpu_tune_load": [ctypes.c_char_p],
     "neo_gpu_tune_save": [ctypes.c_char_p],
@@ -594,6 +595,14 @@ class Shard:
         c = ctypes.c_uint64()
         self.ctx.check(self.ctx.lib.neo_gpu_shard_val_obligations(self.h, ctypes.byref(c)))
         return int(c.value)
+
+    def step_proof(self) -> np.ndarray:
+        """The last fold step's proof in StepProof field order (neo_gpu_shard_step_proof)."""
+        n = ctypes.c_uint64()
+        self.ctx.check(self.ctx.lib.neo_gpu_shard_step_proof(self.h, None, 0, ctypes.byref(n)))
+        out = np.empty(n.value, np.uint64)
+        self.ctx.check(self.ctx.lib.neo_gpu_shard_step_proof(self.h, _p(out), n.value, ctypes.byref(n)))
+        return out
 
     def transcript_state(self) -> np.ndarray:
         st = np.empty(8, np.uint64)

@@ -139,6 +139,7 @@ extern "C" {
     pub fn neo_gpu_shard_restore(sh: *mut neo_gpu_shard, buf: *const u8, len: u64) -> c_int;
     pub fn neo_gpu_shard_set_twist_init(sh: *mut neo_gpu_shard, mem_idx: u32, n_init: u64, init_addr: *const u64, init_val: *const u64) -> c_int;
     pub fn neo_gpu_shard_fold_step(sh: *mut neo_gpu_shard, z: *const u64, proof: *mut u64, proof_cap: u64, proof_len: *mut u64) -> c_int;
+    pub fn neo_gpu_shard_step_proof(sh: *mut neo_gpu_shard, out: *mut u64, cap: u64, len: *mut u64) -> c_int;
     pub fn neo_gpu_shard_fold_step_device(sh: *mut neo_gpu_shard, d_z: *const u64, proof_len: *mut u64) -> c_int;
     pub fn neo_gpu_shard_transcript_state(sh: *const neo_gpu_shard, st8: *mut u64) -> c_int;
     pub fn neo_gpu_shard_ccs_digest(sh: *const neo_gpu_shard, d4: *mut u64) -> c_int;

@@ -146,9 +146,12 @@ class OracleVerifier:
         tr = self.tr
         running = list(sums)
         chals = []
+        self.last_polys = [[] for _ in degs]  # [claim][round][coefficient]
         for rd in range(n_rounds):
             tr.append_message(b"batched/round_idx", le64(rd))
             polys = [R.ks(deg + 1) for deg in degs]
+            for ci, co in enumerate(polys):
+                self.last_polys[ci].append(co)
             for ci, (lab, co) in enumerate(zip(labels, polys)):
                 p0, p1 = co[0], ZERO
                 for c in co:
@@ -249,7 +252,7 @@ class OracleVerifier:
         return kadd(kmulp(eq_beta, kadd(fp, nc)), kmulp(eq_ar, kmulp(gk, ev)))
 
     # ---------------------------------------------------------- RLC / DEC lane --
-    def _lane(self, lane, idx, ins, r, digest, R):
+    def _lane(self, lane, idx, ins, r, digest, R, rec=None):
         """verify_rlc_dec_lane (shard.rs:1333-1420): transcript binding, rho
         sampling, RLC public mix, DEC reconstruction; returns the children."""
         tr, t, kappa, m_in, nb = self.tr, self.t, self.kappa, self.m_in, self.bus.bus_cols
@@ -291,7 +294,9 @@ class OracleVerifier:
                         rhos[i, got] = A5[xv % 5]
                         got += 1
                 ctr += 1
-        if [centered(v) for v in R.take(k * D)] != [int(v) for v in rhos.reshape(-1)]:
+        proof_rhos = [centered(v) for v in R.take(k * D)]
+        # a lane of one instance uses rho = I; the struct-order proof does not carry its sampled vector
+        if not (k == 1 and getattr(self, "_rho_identity_free", False)) and proof_rhos != [int(v) for v in rhos.reshape(-1)]:
             raise VerifyError(f"{lane.decode()} lane: RLC rho mismatch (transcript vs proof)")
         Rs = [np.eye(D, dtype=np.int64)] if k == 1 else [rot_int(rhos[i]) for i in range(k)]
 
@@ -340,7 +345,30 @@ class OracleVerifier:
             raise VerifyError(f"{lane.decode()} lane: DEC commitment check failed")
         if ysum_re != y_re or ysum_im != y_im:
             raise VerifyError(f"{lane.decode()} lane: DEC y check failed")
+        if rec is not None:
+            parent_rows = [[(a, b) for a, b in zip(y_re[row], y_im[row])] for row in range(rows)]
+            rec.update(rhos=[list(v) for v in rhos], children=children,
+                       parent=self._me([v for col in c_parent for v in col],
+                                       [X_parent[j][rho] for rho in range(D) for j in range(m_in)], r, parent_rows,
+                                       digest))
         return children
+
+    def verify_step_struct(self, x, S):
+        """Check one step's proof in StepProof struct order (neo_gpu_shard_step_proof):
+        its proof-carried fields go through verify_step, and every field the
+        replay derives (ME claims' r, X, digests, the RLC parent, the public
+        challenges) must equal the struct's, word for word."""
+        from .step_proof import read_step, to_transcript_order, write_step
+        try:
+            f = read_step(S)
+            P, _ = to_transcript_order(f, self.t, self.bus.bus_cols, self.ell_n)
+        except (ValueError, IndexError, KeyError, TypeError) as e:
+            raise VerifyError(f"malformed struct-order proof: {e}")
+        rec = {}
+        self.verify_step(x, P, record=rec, _rho_identity_free=True)
+        if not np.array_equal(write_step(rec, self.kappa, 1 << self.ell_d), np.asarray(S, np.uint64)):
+            raise VerifyError("struct-order fields differ from the verifier's replay")
+        return True
 
     # ---------------------------------------------------------------- memory --
     def set_twist_init(self, i, init):
@@ -424,11 +452,14 @@ class OracleVerifier:
         return plan
 
     # -------------------------------------------------------------- fold step --
-    def verify_step(self, x, P):
+    def verify_step(self, x, P, record=None, _rho_identity_free=False):
         """Check one step's proof words against the public input x = z[:m_in]
         (and the step's public memory instances); on success the verified DEC
         children become the accumulator and the val-lane children are added to
-        val_obligations."""
+        val_obligations.  record (a dict) receives the step's fields in the
+        struct order of StepProof (oracle/step_proof.py)."""
+        rec = record if record is not None else {}
+        self._rho_identity_free = _rho_identity_free
         tr, t, ell_n, ell_d, d_sc = self.tr, self.t, self.ell_n, self.ell_d, self.d_sc
         idx, kappa, m_in = self.step_idx, self.kappa, self.m_in
         bus, nb = self.bus, self.bus.bus_cols
@@ -493,6 +524,8 @@ class OracleVerifier:
         gamma = ck()
         beta_a, beta_r = beta[:ell_d], beta[ell_d:]
         T = self._initial_sum(alpha, gamma, k)
+        rec.update(alpha=alpha, beta_a=beta_a, beta_r=beta_r, gamma=gamma, T=T, shout=None, twist=[], val_eval=None,
+                   val=None, cpu_me_val=[])
         if R.k() != T:
             raise VerifyError("initial sum mismatch: proof claims a different value than the public T")
         self._k(b"sumcheck/initial_sum", T)
@@ -521,6 +554,7 @@ class OracleVerifier:
             else:
                 r_addr_s, finals = self._batched_ds(b"shout/addr_pre_time", idx, [b"shout/addr_pre"] * len(act),
                                                     [2] * len(act), [sums[i] for i in act], ea, R)
+            rec["shout"] = dict(sums=sums, active=active, polys=self.last_polys if act else [], r_addr=r_addr_s)
             if R.ks(ea) != r_addr_s:
                 raise VerifyError("shout_addr_pre r_addr mismatch: transcript-derived vs proof")
             pos = 0
@@ -543,6 +577,7 @@ class OracleVerifier:
             tr.append_message(b"twist/addr_pre_time/claim_idx", le64(i))
             self._bind_claim_sums(b"twist/addr_pre_time/claimed_sums", [ZERO, ZERO], labels)
             r_addr, finals = self._batched_ds(b"twist/addr_pre_time", i, labels, [2, 2], [ZERO, ZERO], ea, R)
+            rec["twist"].append(dict(polys=self.last_polys, r_addr=r_addr, finals=finals))
             if R.ks(ea) != r_addr:
                 raise VerifyError("twist addr_pre r_addr mismatch: transcript-derived vs proof")
             if R.ks(2) != finals:
@@ -573,14 +608,18 @@ class OracleVerifier:
             if dyn:
                 self._k(b"batched/dynamic_bind/claimed_sum", sums[ci])
         r_time, finals = self._batched_ds(b"shard/batched_time", idx, labels, degs, sums, ell_n, R)
+        rec["time"] = dict(sums=list(sums), degs=list(degs), labels=list(labels), polys=self.last_polys)
+        rec["r_time"] = r_time
         # ---- CCS Ajtai rounds (verify_sumcheck_rounds_ds with domain ccs/ajtai) ----
         running = finals[0]
         tr.append_message(b"sc/domain", b"ccs/ajtai")
         tr.append_message(b"sc/inst_idx", le64(idx))
         self._k(b"sc/claimed_sum", running)
         alpha_p = []
+        rec["ajtai_polys"] = []
         for rd in range(ell_d):
             co = R.ks(d_sc + 1)
+            rec["ajtai_polys"].append(co)
             p1 = ZERO
             for c in co:
                 p1 = kadd(p1, c)
@@ -595,6 +634,7 @@ class OracleVerifier:
         tr.append_message(b"sc/inst_idx_end", le64(idx))
         if R.k() != running:
             raise VerifyError("Pi_CCS sumcheck_final mismatch")
+        rec["alpha_p"], rec["final"] = alpha_p, running
         fold_digest = tr.digest32()
         # ---- ME outputs (core rows + bus openings) and the Pi_CCS terminal identity ----
         y_out = [[R.ks(D) for _ in range(t)] for _ in range(k)]
@@ -615,6 +655,7 @@ class OracleVerifier:
             raise VerifyError("Pi_CCS terminal identity check failed")
         srcs = [dict(c=c_mcs, X=Xm)] + [dict(c=me["c"], X=me["X"]) for me in self.acc]
         outs = [self._me(s_["c"], s_["X"], r_time, y_out[i] + bus_y[i][0], fold_digest) for i, s_ in enumerate(srcs)]
+        rec["ccs_out"] = outs
 
         # ---- Twist val-eval batch (memory.rs:2088-2170) ----
         has_prev = self.prev is not None
@@ -636,6 +677,7 @@ class OracleVerifier:
                 self._k(b"twist/val_eval/claimed_sum", sm)
             r_val, vfin = self._batched_ds(b"twist/val_eval_batch", idx, [v[0] for v in vplan], [v[1] for v in vplan],
                                            vsums, ell_n, R)
+            rec["val_eval"] = dict(sums=vsums, polys=self.last_polys, r_val=r_val)
             tr.append_message(b"twist/val_eval/batch_done")
             if R.ks(ell_n) != r_val:
                 raise VerifyError("twist val-eval r_val mismatch")
@@ -650,6 +692,7 @@ class OracleVerifier:
                 if self._yscalars(rows) != ysc:
                     raise VerifyError("CPU ME(val): y_scalars do not recompose y")
                 val_claims.append(self._me(c_, X_, r_val, rows, vdigest))
+            rec["cpu_me_val"] = val_claims
 
         # ---- verify_route_a_memory_step (memory.rs:1671-2380) ----
         if self.shout or self.twist:
@@ -715,10 +758,12 @@ class OracleVerifier:
                 ci += 3
 
         # ---- main lane, val lane ----
-        children = self._lane(b"main", idx, outs, r_time, fold_digest, R)
+        rec["main"] = {}
+        children = self._lane(b"main", idx, outs, r_time, fold_digest, R, rec["main"])
         if val_claims:
             tr.append_message(b"fold/val_lane_start", le64(idx))
-            self.val_obligations += self._lane(b"val", idx, val_claims, r_val, vdigest, R)
+            rec["val"] = {}
+            self.val_obligations += self._lane(b"val", idx, val_claims, r_val, vdigest, R, rec["val"])
         tr.append_message(b"fold/step_done", le64(idx))
         R.done()
         self.acc = children

@@ -80,3 +80,31 @@ def test_verifier_accepts_large_shard_chunks(ctx):
         assert v.verify_step(zs[c][:1], P)
         print(f"large shard chunk {c}: GPU fold step {1e3 * (t1 - t0):.0f} ms, verify {time.perf_counter() - t1:.1f} s")
     g.close()
+
+
+@pytest.mark.parametrize("memory", [False, True])
+def test_step_proof_struct_order_matches_verifier(ctx, memory):
+    """neo_gpu_shard_step_proof (StepProof in struct order) equals, word for
+    word, the struct the verifier restatement derives from the transcript-order
+    proof, and verify_step_struct accepts it, step after step."""
+    from oracle.step_proof import write_step
+    if memory:
+        ccs, zs, mem, inits = synth.make_memory_workload_chunks(11, 6, 3, 32, 8, 6)
+    else:
+        ccs, z = synth.make_r1cs(10, 9)
+        zs, mem, inits = [z] * 3, None, None
+    ctx.pp_generate(bytes(range(9, 41)), 16, ccs.m, 1)
+    g = gpu.Shard(ctx, ccs, m_in=1, k_rho=12, app_label=b"neo/struct-gpu", mem=mem)
+    v1 = OracleVerifier(ccs, m_in=1, k_rho=12, kappa=16, app_label=b"neo/struct-gpu", mem=mem)
+    v2 = OracleVerifier(ccs, m_in=1, k_rho=12, kappa=16, app_label=b"neo/struct-gpu", mem=mem)
+    for c in range(3):
+        if c and inits:
+            for s_ in (g, v1, v2):
+                s_.set_twist_init(0, inits[c][0])
+        P = g.fold_step(zs[c])
+        S = g.step_proof()
+        rec = {}
+        assert v1.verify_step(zs[c][:1], P, record=rec)
+        assert np.array_equal(S, write_step(rec, 16, 64)), f"step {c}: first mismatch at word {int(np.argmax(S != write_step(rec, 16, 64)))}"
+        assert v2.verify_step_struct(zs[c][:1], S)
+    g.close()
