@@ -380,7 +380,10 @@ int neo_gpu_shard_fold_step(neo_gpu_shard* sh, const uint64_t* z, uint64_t* proo
  * word, Option a 0 / 1 word then the value.  MeInstance = {c (d, kappa,
  * data), X (rows, cols, data), r, y (rows of 2^ell_d K), y_scalars, m_in,
  * fold_digest, c_step_coords, u_offset, u_len}.  out == NULL only sets *len.
- * The field-by-field map is in INTEGRATION.md; oracle/verify.py reads it. */
+ * The CCS proof part is {sumcheck_rounds (the Ajtai rounds), Some(sc_initial_sum),
+ * sumcheck_challenges (r' || alpha'), alpha, beta_a, beta_r, gamma,
+ * sumcheck_final, header_digest (empty), _extra (None)}; a lane mixing one
+ * instance carries rho = I. */
 int neo_gpu_shard_step_proof(neo_gpu_shard* sh, uint64_t* out, uint64_t cap, uint64_t* len);
 /* Same step with the witness already resident in device memory (d_z). */
 int neo_gpu_shard_fold_step_device(neo_gpu_shard* sh, const uint64_t* d_z, uint64_t* proof_len);

@@ -256,7 +256,8 @@ struct StepRecord {
     uint64_t shout_active = 0;
     BatchRec shout_pre;
     std::vector<BatchRec> twist_pre;
-    bool has_val_eval = false;
+    uint32_t n_lut = 0;
+    bool has_val_eval = false, val_has_prev = false;
     BatchRec val_eval;
 };
 
@@ -1469,6 +1470,7 @@ static int fold_step_impl(neo_gpu_shard* sh, const uint64_t* z_host, const uint6
             for (auto& s : sums) push_k(P, s);
             P.push_back(active);
             rec.has_shout = true;
+            rec.n_lut = (uint32_t)sh->shout.size();
             rec.shout_sums = sums;
             rec.shout_active = active;
             if (active == 0) {
@@ -1731,6 +1733,7 @@ static int fold_step_impl(neo_gpu_shard* sh, const uint64_t* z_host, const uint6
         }
         std::vector<K> fin;
         rec.has_val_eval = true;
+        rec.val_has_prev = sh->has_prev;
         if ((rc = run_batched_ds(sh, "twist/val_eval_batch", idx, vcl, ell_n, r_val, fin, P, &rec.val_eval))) return rc;
         tr.append_message("twist/val_eval/batch_done", nullptr, 0);
         for (auto& r : r_val) push_k(P, r);
@@ -1985,25 +1988,42 @@ static int neo_gpu_shard_step_proof_impl_abi(neo_gpu_shard* sh, uint64_t* out, u
     write_lane(W, R.main, kappa, d_pad);
     // mem: MemSidecarProof
     write_mes(W, R.cpu_me_val, kappa, d_pad);
-    W.u(R.has_shout ? 1 : 0);  // shout_addr_pre
-    if (R.has_shout) {
-        W.kvec(R.shout_sums);
-        W.u(R.shout_active);
-        write_polys(W, R.shout_pre.polys);
-        W.kvec(R.shout_pre.chals);
-    }
-    W.u(R.twist_pre.size());  // proofs: one Twist proof per instance (tag 0)
-    for (auto& tp : R.twist_pre) {
+    // shout_addr_pre: ShoutAddrPreProof, empty without Shout instances
+    W.kvec(R.shout_sums);
+    W.u(R.shout_active);
+    write_polys(W, R.shout_pre.polys);
+    W.kvec(R.has_shout ? R.shout_pre.chals : std::vector<K>());
+    // proofs: Vec<MemOrLutProof>, the Shout entries first (memory.rs:1555-1569);
+    // enum tags in declaration order, Twist = 0, Shout = 1
+    W.u(R.n_lut + R.twist_pre.size());
+    for (uint32_t i = 0; i < R.n_lut; i++) {
+        W.u(1);  // ShoutProof { addr_pre: BatchedAddrProof::default() }
         W.u(0);
+        W.u(0);
+        W.u(0);
+    }
+    const uint32_t per_mem = R.val_has_prev ? 3 : 2;
+    for (size_t i = 0; i < R.twist_pre.size(); i++) {
+        const BatchRec& tp = R.twist_pre[i];
+        W.u(0);
+        W.kvec(tp.sums);  // addr_pre: claimed sums (zero), read / write rounds, r_addr
         write_polys(W, tp.polys);
         W.kvec(tp.chals);
-        W.kvec(tp.finals);
-    }
-    W.u(R.has_val_eval ? 1 : 0);  // Twist val-eval batch
-    if (R.has_val_eval) {
-        W.kvec(R.val_eval.sums);
-        write_polys(W, R.val_eval.polys);
-        W.kvec(R.val_eval.chals);
+        const size_t base = per_mem * i;  // val_eval: this instance's claims of the batch
+        const bool ve = R.has_val_eval && base + per_mem <= R.val_eval.sums.size();
+        W.u(ve ? 1 : 0);
+        if (!ve) continue;
+        for (uint32_t c = 0; c < per_mem; c++) {
+            if (c == 2) W.u(1);  // Some(claimed_prev_inc_sum_total)
+            W.k(R.val_eval.sums[base + c]);
+            if (c == 2) W.u(1);  // Some(rounds_prev_total)
+            W.u(R.val_eval.polys[base + c].size());
+            for (auto& rd : R.val_eval.polys[base + c]) W.kvec(rd);
+        }
+        if (per_mem == 2) {
+            W.u(0);
+            W.u(0);
+        }
     }
     // batched_time: BatchedTimeProof
     W.kvec(R.time.sums);

@@ -109,29 +109,44 @@ def write_step(rec, kappa, d_pad):
     W.u(0)
     W.lane(rec["main"], kappa, d_pad)
     W.mes(rec["cpu_me_val"], kappa, d_pad)
-    if rec.get("shout") is not None:
-        s = rec["shout"]
-        W.u(1)
+    # shout_addr_pre: ShoutAddrPreProof, empty without Shout instances
+    s = rec.get("shout")
+    if s is not None:
         W.kvec(s["sums"])
         W.u(s["active"])
         W.polys(s["polys"])
         W.kvec(s["r_addr"])
     else:
+        W.w += [0, 0, 0, 0]
+    # proofs: Vec<MemOrLutProof> (memory.rs:1555-1569), Shout entries first;
+    # enum tags in declaration order, Twist = 0, Shout = 1
+    n_lut = len(s["sums"]) if s is not None else 0
+    W.u(n_lut + len(rec["twist"]))
+    for _ in range(n_lut):
+        W.w += [1, 0, 0, 0]  # ShoutProof { addr_pre: BatchedAddrProof::default() }
+    v = rec.get("val_eval")
+    per = 3 if (v is not None and v.get("has_prev")) else 2
+    for i, tp in enumerate(rec["twist"]):
         W.u(0)
-    W.u(len(rec["twist"]))
-    for tp in rec["twist"]:
-        W.u(0)
+        W.kvec([(0, 0), (0, 0)])  # addr_pre: claimed sums (zero), read / write rounds, r_addr
         W.polys(tp["polys"])
         W.kvec(tp["r_addr"])
-        W.kvec(tp["finals"])
-    if rec.get("val_eval") is not None:
-        v = rec["val_eval"]
-        W.u(1)
-        W.kvec(v["sums"])
-        W.polys(v["polys"])
-        W.kvec(v["r_val"])
-    else:
-        W.u(0)
+        base = per * i
+        if v is None or base + per > len(v["sums"]):
+            W.u(0)
+            continue
+        W.u(1)  # val_eval: Some(TwistValEvalProof)
+        for c in range(per):
+            if c == 2:
+                W.u(1)
+            W.k(v["sums"][base + c])
+            if c == 2:
+                W.u(1)
+            W.u(len(v["polys"][base + c]))
+            for rd in v["polys"][base + c]:
+                W.kvec(rd)
+        if per == 2:
+            W.w += [0, 0]
     t = rec["time"]
     W.kvec(t["sums"])
     W.u(len(t["degs"]))
@@ -229,12 +244,44 @@ def read_step(S):
     f["extra"] = R.u()
     f["main"] = R.lane()
     f["cpu_me_val"] = R.mes()
-    f["shout"] = dict(sums=R.kvec(), active=R.u(), polys=R.polys(), r_addr=R.kvec()) if R.u() else None
+    sums, active, polys, r_addr = R.kvec(), R.u(), R.polys(), R.kvec()
+    f["shout"] = dict(sums=sums, active=active, polys=polys, r_addr=r_addr) if sums else None
+    if not sums and (active or polys or r_addr):
+        raise ValueError("shout_addr_pre must be empty when there are no Shout instances")
     f["twist"] = []
+    vsums, vpolys, has_prev, n_ve = [], [], None, 0
     for _ in range(R.u()):
         tag = R.u()
-        f["twist"].append(dict(tag=tag, polys=R.polys(), r_addr=R.kvec(), finals=R.kvec()))
-    f["val_eval"] = dict(sums=R.kvec(), polys=R.polys(), r_val=R.kvec()) if R.u() else None
+        cs, pol, ra = R.kvec(), R.polys(), R.kvec()
+        if tag == 1:
+            if f["twist"] or cs or pol or ra:
+                raise ValueError("a Shout proof entry must be empty and precede the Twist entries")
+            continue
+        if tag != 0:
+            raise ValueError(f"unknown MemOrLutProof tag {tag}")
+        if cs != [(0, 0), (0, 0)] or len(pol) != 2:
+            raise ValueError("Twist addr_pre must carry two zero claimed sums and two claims")
+        f["twist"].append(dict(polys=pol, r_addr=ra))
+        if R.u():
+            n_ve += 1
+            for c in range(3):
+                if c == 2:
+                    prev = R.u()
+                    if has_prev is None:
+                        has_prev = bool(prev)
+                    if bool(prev) != has_prev:
+                        raise ValueError("rollover claims on some Twist instances only")
+                    if not prev:
+                        if R.u():
+                            raise ValueError("rounds_prev_total without claimed_prev_inc_sum_total")
+                        break
+                vsums.append(R.k())
+                if c == 2 and not R.u():
+                    raise ValueError("claimed_prev_inc_sum_total without rounds_prev_total")
+                vpolys.append([R.kvec() for _ in range(R.u())])
+    if n_ve not in (0, len(f["twist"])):
+        raise ValueError("val_eval on some Twist instances only")
+    f["val_eval"] = dict(sums=vsums, polys=vpolys, has_prev=bool(has_prev)) if n_ve else None
     sums = R.kvec()
     degs = [R.u() for _ in range(R.u())]
     labels = [R.bytes_() for _ in range(R.u())]
@@ -256,9 +303,11 @@ def _round_major(polys, n_rounds):
 
 def to_transcript_order(f, t, nb, ell_n):
     """The transcript-order proof words (neo_gpu_shard_fold_step's dump) carried
-    by a struct-order step proof.  A lane that mixes one instance has rho = I;
-    its sampled coefficients are not part of the struct, and zeros stand in for
-    them (the verifier then accepts any sampled value, as it uses rho = I)."""
+    by a struct-order step proof, less the words the verifier derives itself
+    (Twist address finals, r_val), which the struct does not hold.  A lane that
+    mixes one instance has rho = I; its sampled coefficients are not part of the
+    struct, and zeros stand in for them (the verifier then accepts any sampled
+    value, as it uses rho = I).  verify_step(..., _struct=True) reads this."""
     P = []
     k = len(f["ccs_out"])
     P += list(f["ccs_out"][0]["c"])
@@ -271,9 +320,9 @@ def to_transcript_order(f, t, nb, ell_n):
         P += _round_major(s["polys"], len(s["r_addr"]) if s["polys"] else 0)
         for v in s["r_addr"]:
             P += list(v)
-    for tp in f["twist"]:
+    for tp in f["twist"]:  # the address finals are not in the struct: the verifier derives them
         P += _round_major(tp["polys"], len(tp["r_addr"]))
-        for v in tp["r_addr"] + tp["finals"]:
+        for v in tp["r_addr"]:
             P += list(v)
     P += _round_major(f["time"]["polys"], ell_n)
     for co in f["ajtai_polys"]:
@@ -298,9 +347,7 @@ def to_transcript_order(f, t, nb, ell_n):
         v = f["val_eval"]
         for x in v["sums"]:
             P += list(x)
-        P += _round_major(v["polys"], ell_n)
-        for x in v["r_val"]:
-            P += list(x)
+        P += _round_major(v["polys"], ell_n)  # r_val is transcript-derived, not in the struct
         for me in f["cpu_me_val"]:
             for j in range(t + nb):
                 for c in me["y"][j][:D]:

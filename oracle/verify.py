@@ -296,7 +296,7 @@ class OracleVerifier:
                 ctr += 1
         proof_rhos = [centered(v) for v in R.take(k * D)]
         # a lane of one instance uses rho = I; the struct-order proof does not carry its sampled vector
-        if not (k == 1 and getattr(self, "_rho_identity_free", False)) and proof_rhos != [int(v) for v in rhos.reshape(-1)]:
+        if not (k == 1 and getattr(self, "_struct", False)) and proof_rhos != [int(v) for v in rhos.reshape(-1)]:
             raise VerifyError(f"{lane.decode()} lane: RLC rho mismatch (transcript vs proof)")
         Rs = [np.eye(D, dtype=np.int64)] if k == 1 else [rot_int(rhos[i]) for i in range(k)]
 
@@ -365,7 +365,7 @@ class OracleVerifier:
         except (ValueError, IndexError, KeyError, TypeError) as e:
             raise VerifyError(f"malformed struct-order proof: {e}")
         rec = {}
-        self.verify_step(x, P, record=rec, _rho_identity_free=True)
+        self.verify_step(x, P, record=rec, _struct=True)
         if not np.array_equal(write_step(rec, self.kappa, 1 << self.ell_d), np.asarray(S, np.uint64)):
             raise VerifyError("struct-order fields differ from the verifier's replay")
         return True
@@ -452,14 +452,17 @@ class OracleVerifier:
         return plan
 
     # -------------------------------------------------------------- fold step --
-    def verify_step(self, x, P, record=None, _rho_identity_free=False):
+    def verify_step(self, x, P, record=None, _struct=False):
         """Check one step's proof words against the public input x = z[:m_in]
         (and the step's public memory instances); on success the verified DEC
         children become the accumulator and the val-lane children are added to
         val_obligations.  record (a dict) receives the step's fields in the
-        struct order of StepProof (oracle/step_proof.py)."""
+        struct order of StepProof (oracle/step_proof.py).  _struct: P was rebuilt
+        from a struct-order proof, which carries neither the words the verifier
+        derives itself (Twist address finals, r_val) nor a one-instance lane's
+        sampled rho."""
         rec = record if record is not None else {}
-        self._rho_identity_free = _rho_identity_free
+        self._struct = _struct
         tr, t, ell_n, ell_d, d_sc = self.tr, self.t, self.ell_n, self.ell_d, self.d_sc
         idx, kappa, m_in = self.step_idx, self.kappa, self.m_in
         bus, nb = self.bus, self.bus.bus_cols
@@ -580,7 +583,7 @@ class OracleVerifier:
             rec["twist"].append(dict(polys=self.last_polys, r_addr=r_addr, finals=finals))
             if R.ks(ea) != r_addr:
                 raise VerifyError("twist addr_pre r_addr mismatch: transcript-derived vs proof")
-            if R.ks(2) != finals:
+            if not _struct and R.ks(2) != finals:
                 raise VerifyError("twist addr_pre finals mismatch")
             twist_pre.append(dict(r_addr=r_addr, read=finals[0], write=finals[1]))
 
@@ -677,9 +680,9 @@ class OracleVerifier:
                 self._k(b"twist/val_eval/claimed_sum", sm)
             r_val, vfin = self._batched_ds(b"twist/val_eval_batch", idx, [v[0] for v in vplan], [v[1] for v in vplan],
                                            vsums, ell_n, R)
-            rec["val_eval"] = dict(sums=vsums, polys=self.last_polys, r_val=r_val)
+            rec["val_eval"] = dict(sums=vsums, polys=self.last_polys, r_val=r_val, has_prev=has_prev)
             tr.append_message(b"twist/val_eval/batch_done")
-            if R.ks(ell_n) != r_val:
+            if not _struct and R.ks(ell_n) != r_val:
                 raise VerifyError("twist val-eval r_val mismatch")
             # CPU ME claims at r_val (ts_common.rs:100-258): the current and previous MCS
             fork = tr.clone_state()

@@ -51,9 +51,11 @@ def test_struct_round_trip_and_verify(steps):
         f = read_step(S)
         assert len(f["ccs_out"]) == (1 if c == 0 else 13) and len(f["main"]["children"]) == 12
         P2, k = to_transcript_order(f, ccs.t, v.bus.bus_cols, v.ell_n)
-        if k == 1:
-            assert len(P2) == len(P)  # the one-instance lane's sampled rho words are not in the struct
-        else:
+        # words the verifier derives are not in the struct: per Twist instance
+        # its two address finals, and r_val of the val-eval batch
+        derived = 4 * len(f["twist"]) + (2 * v.ell_n if f["val_eval"] is not None else 0)
+        assert len(P2) == len(P) - derived
+        if k > 1 and not derived:  # (a one-instance lane's sampled rho is not in the struct either)
             assert np.array_equal(P2, np.asarray(P, np.uint64))
         if c and inits:
             v.set_twist_init(0, inits[c][0])
@@ -89,6 +91,25 @@ def test_struct_rejects_changed_derived_fields(steps):
             v.set_twist_init(0, inits[1][0])
         with pytest.raises(VerifyError):
             v.verify_step_struct(z[:1], S_bad)
+
+
+def test_struct_memory_fields(steps):
+    """The memory sidecar in MemSidecarProof order: Shout entries (empty
+    BatchedAddrProof) before one Twist entry per instance, each with zero
+    address claimed sums, read / write rounds, r_addr and its val-eval claims
+    (lt, total and, from the second step on, the rollover total)."""
+    ccs, mem, inits, out = steps
+    for c, (z, P, S) in enumerate(out):
+        f = read_step(S)
+        if mem is None:
+            assert f["shout"] is None and f["twist"] == [] and f["val_eval"] is None
+            continue
+        assert len(f["twist"]) == len(mem["twist"])
+        for tp in f["twist"]:
+            assert len(tp["polys"]) == 2 and all(len(cl) == len(tp["r_addr"]) for cl in tp["polys"])
+        ve = f["val_eval"]
+        assert ve is not None and ve["has_prev"] == (c > 0)
+        assert len(ve["sums"]) == (3 if c else 2) * len(mem["twist"]) == len(ve["polys"])
 
 
 def _rewrite(f):
