@@ -67,6 +67,9 @@ int neo_gpu_wait_probe(neo_gpu_ctx* ctx, uint32_t set_flag, uint32_t spin_limit)
 uint64_t neo_gpu_kernel_launches(const neo_gpu_ctx* ctx);
 /* The context's CUDA stream (a cudaStream_t), for event timing by callers. */
 int neo_gpu_ctx_stream(const neo_gpu_ctx* ctx, void** stream);
+/* Wait for the context's stream, then report and clear device-side errors: a
+ * timed-out bounded wait (NEO_ERR_CUDA) or commitment digits that broke
+ * NEO_COMMIT_SMALL_DIGITS (NEO_ERR_INVARIANT). */
 int neo_gpu_synchronize(neo_gpu_ctx* ctx);
 
 /* ---- Ajtai commitment (crates/neo-ajtai) ---------------------------- */
@@ -110,8 +113,22 @@ int neo_gpu_chacha8_sample(neo_gpu_ctx* ctx, const uint8_t* seeds, uint32_t n_st
 int neo_gpu_commit(neo_gpu_ctx* ctx, const int8_t* digits, uint32_t n_vec, uint64_t m, uint64_t* out);
 
 /* neo_gpu_commit with DEVICE pointers (digits and out already in HBM); the
- * call is asynchronous on the context stream. */
+ * call is asynchronous on the context stream.  (neo_gpu_commit checks the
+ * digits once and takes the faster small-digit tensor-core form when every
+ * |digit| <= 63; this call, which never synchronizes, takes the form valid for
+ * any int8 unless neo_gpu_commit_device_ex says the digits are small.) */
 int neo_gpu_commit_device(neo_gpu_ctx* ctx, const int8_t* d_digits, uint32_t n_vec, uint64_t m, uint64_t* d_out);
+
+/* neo_gpu_commit_device with flags.  NEO_COMMIT_SMALL_DIGITS: the caller
+ * guarantees |digit| <= 63 (balanced base-b digits, b <= 64, as
+ * decomp_b_row_major produces, crates/neo-ajtai/src/decomp.rs:118-158), so
+ * the product is taken mod Phi_81 directly on the tensor cores; a digit pair
+ * that breaks the guarantee is reported as NEO_ERR_INVARIANT by the next call
+ * that checks the context's device error word (neo_gpu_synchronize).
+ * Asynchronous on the context stream. */
+#define NEO_COMMIT_SMALL_DIGITS 1u
+int neo_gpu_commit_device_ex(neo_gpu_ctx* ctx, const int8_t* d_digits, uint32_t n_vec, uint64_t m, uint64_t* d_out,
+                             uint32_t flags);
 
 /* Allocation-free commitment (no counterpart in the reference).  Same result
  * as neo_gpu_commit_device, for callers that cannot allocate device memory

@@ -8,6 +8,7 @@
 // epilogue.  This file holds the CUDA-core kernel: split-K over column
 // chunks, exact F_q accumulation, then a cross-chunk reduction.
 #include "internal.cuh"
+#include <algorithm>
 
 using gl::K;
 
@@ -95,16 +96,18 @@ PPEntry* pp_lookup(int device, uint64_t m) {
     return it == g_pp.end() ? nullptr : it->second;
 }
 
-int launch_commit(neo_gpu_ctx* ctx, const int8_t* d_digits, uint32_t n_vec, uint64_t m, uint64_t* d_out) {
+int launch_commit(neo_gpu_ctx* ctx, const int8_t* d_digits, uint32_t n_vec, uint64_t m, uint64_t* d_out, int digits) {
     PPEntry* pp = pp_lookup(ctx->device, m);
     if (!pp || !pp->kappa) return ctx->fail(NEO_ERR_ARG, "commit: PP not loaded for this m");
     if (pp->tc) {
-        // tensor-core path (commit_tc.cu)
+        // tensor-core path (commit_tc.cu); scratch for every form the call may take
         uint32_t g, k, kb;
-        size_t need = tc_scratch_bytes(n_vec, m, &g, &k, &kb);
+        size_t need = 0;
+        if (digits != TC_DIGITS_ANY) need = tc_scratch_bytes(n_vec, m, true, &g, &k, &kb);
+        if (digits != TC_DIGITS_SMALL) need = std::max(need, tc_scratch_bytes(n_vec, m, false, &g, &k, &kb));
         void* scratch = nullptr;
         NEO_CK(ctx, ctx_scratch(ctx, need, &scratch));
-        return launch_commit_tc(ctx, pp, d_digits, n_vec, d_out, (uint8_t*)scratch, ctx->d_err);
+        return launch_commit_tc(ctx, pp, d_digits, n_vec, d_out, (uint8_t*)scratch, ctx->d_err, digits);
     }
     const uint32_t kappa = pp->kappa;
     // pick a chunking that fills the GPU: ~4 blocks per SM in total
@@ -210,10 +213,24 @@ static int neo_gpu_commit_device_impl_abi(neo_gpu_ctx* ctx, const int8_t* d_digi
     if (!ctx) return NEO_ERR_ARG;
     if (!d_digits || !d_out || n_vec == 0 || m == 0) return ctx->fail(NEO_ERR_ARG, "commit_device: bad args");
     cudaSetDevice(ctx->device);
-    return launch_commit(ctx, d_digits, n_vec, m, d_out);
+    return launch_commit(ctx, d_digits, n_vec, m, d_out, TC_DIGITS_ANY);
 }
 extern "C" int neo_gpu_commit_device(neo_gpu_ctx* ctx, const int8_t* d_digits, uint32_t n_vec, uint64_t m,
                                      uint64_t* d_out) { NEO_ABI_GUARD(neo_gpu_commit_device_impl_abi(ctx, d_digits, n_vec, m, d_out)) }
+
+static int neo_gpu_commit_device_ex_impl_abi(neo_gpu_ctx* ctx, const int8_t* d_digits, uint32_t n_vec, uint64_t m,
+                                             uint64_t* d_out, uint32_t flags) {
+    if (!ctx) return NEO_ERR_ARG;
+    if (!d_digits || !d_out || n_vec == 0 || m == 0 || (flags & ~(uint32_t)NEO_COMMIT_SMALL_DIGITS))
+        return ctx->fail(NEO_ERR_ARG, "commit_device_ex: bad args");
+    cudaSetDevice(ctx->device);
+    return launch_commit(ctx, d_digits, n_vec, m, d_out,
+                         (flags & NEO_COMMIT_SMALL_DIGITS) ? TC_DIGITS_SMALL : TC_DIGITS_ANY);
+}
+extern "C" int neo_gpu_commit_device_ex(neo_gpu_ctx* ctx, const int8_t* d_digits, uint32_t n_vec, uint64_t m,
+                                        uint64_t* d_out, uint32_t flags) {
+    NEO_ABI_GUARD(neo_gpu_commit_device_ex_impl_abi(ctx, d_digits, n_vec, m, d_out, flags))
+}
 
 // ---------------------------------------------------------------------------
 // Allocation-free commitment.

@@ -440,6 +440,291 @@ __global__ void __launch_bounds__(RED_THREADS) commit_tc_reduce_kernel(const int
     }
 }
 
+// ---------------------------------------------------------------------------
+// Small-digit form: the product taken mod Phi_81 directly.
+//
+// For digits |z| <= 63 the rotation matrix of z mod Phi_81 itself fits int8:
+// [X^r] X^s z(X) mod Phi_81 = z[r-s] - z[r+27-s]                 (r >= 27)
+//                             z[r-s] - z[r+54-s] + z[r+81-s]      (r < 27)
+// (X^54 = -X^27 - 1 and X^81 = 1 mod Phi_81; z[x] = 0 outside [0, 54)), and
+// at most two of the terms are nonzero for any (r, s).  With r' = 58 - r for
+// the rows r >= 27 and r' = 31 - r for the rows r < 27 (r' < 32, rows r' < 5
+// computed and discarded), row r is the window [r', r' + 64) of one of two
+// sequences per (vector, column):
+//   H_0[w] = z[58 - w] - z[85 - w],   H_1[w] = z[31 - w] - z[85 - w] + z[112 - w].
+// So the B operand keeps the phase-sequence layout of the cyclic form with
+// 64 rows per vector instead of 88: N = 64 NV, one MMA per 32-byte K step
+// (A read once), 1.40x the algorithmic MACs instead of 1.93x, and the output
+// needs no 81 -> 54 fold.  Row groups g = ((2a + h) 2 + seq) NV + v, r' =
+// 16a + 8h + b; phase chunks [chunk][h][seq][v][b][16 B], chunk < 5.
+constexpr int P8_HSEQ = 112;            // bytes per window sequence (w < 95 used)
+constexpr int P8_FBYTES = 2 * P8_HSEQ;  // both sequences of one (vector, column)
+
+template <int NV>
+struct P8 {
+    static constexpr int NPAD = 64 * NV;        // MMA N
+    static constexpr int LBO = 4 * NV * 128;    // K-direction core-matrix stride
+    static constexpr int BCOL = 5 * LBO;        // B bytes per column
+    static constexpr int B_BYTES = 2 * BCOL;    // two columns per K block
+    static constexpr int F_STAGE = NV * 2 * P8_FBYTES;
+    static constexpr int BUILDERS = NV >= 2 ? 64 * NV : 128;  // (column, vector, seq, phase); >= 4 epilogue warps
+    static constexpr int THREADS = 64 + BUILDERS;
+    static constexpr int ASTAGES = 6, BSTAGES = 4;
+    static constexpr int SMEM = ASTAGES * (TC_A_BYTES + F_STAGE) + BSTAGES * B_BYTES;
+    static constexpr uint32_t TMEM_COLS = NPAD <= 64 ? 64 : (NPAD <= 128 ? 128 : 256);
+    static_assert(NPAD <= 256 && NPAD % 16 == 0, "one MMA per K step (M = 128: N <= 256, N % 16 == 0)");
+    static_assert(B_BYTES % 1024 == 0, "B stages stay 1024-byte aligned");
+    static_assert(SMEM + 1024 + 256 <= 232448, "shared memory budget");
+};
+
+__device__ __forceinline__ uint64_t ns_desc_lbo(uint32_t saddr, uint32_t lbo) {
+    uint64_t d = 0;
+    d |= (uint64_t)((saddr >> 4) & 0x3FFF);
+    d |= (uint64_t)((lbo >> 4) & 0x3FFF) << 16;
+    d |= (uint64_t)((TC_BSBO >> 4) & 0x3FFF) << 32;
+    d |= (uint64_t)1 << 46;
+    return d;
+}
+
+// z[x], 0 outside [0, 54) (x is a compile-time constant after unrolling)
+__device__ __forceinline__ int zat(const int (&z)[NEO_D], int x) { return (x >= 0 && x < NEO_D) ? z[x] : 0; }
+
+// prep: the two window sequences of every (vector, column); a digit pair whose
+// window entry leaves int8 sets bit 16 of *err (the caller then takes the
+// cyclic form, or reports the error)
+__global__ void p8_seq_kernel(const int8_t* __restrict__ digits, uint32_t n_vec, uint64_t m, uint8_t* __restrict__ F,
+                              uint32_t* __restrict__ err) {
+    const uint64_t tid = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+    if (tid >= (uint64_t)n_vec * m) return;
+    const uint64_t v = tid / m, j = tid % m;
+    int z[NEO_D];
+    const int8_t* zv = digits + v * NEO_D * m + j;
+#pragma unroll
+    for (int x = 0; x < NEO_D; x++) z[x] = zv[(uint64_t)x * m];
+    uint4* dst = reinterpret_cast<uint4*>(F + tid * P8_FBYTES);
+    bool bad = false;
+#pragma unroll
+    for (int seq = 0; seq < 2; seq++) {
+#pragma unroll
+        for (int q = 0; q < P8_HSEQ / 16; q++) {
+            uint32_t w4[4];
+#pragma unroll
+            for (int e = 0; e < 4; e++) {
+                uint32_t word = 0;
+#pragma unroll
+                for (int b = 0; b < 4; b++) {
+                    const int w = q * 16 + e * 4 + b;
+                    const int h = seq == 0 ? zat(z, 58 - w) - zat(z, 85 - w)
+                                           : zat(z, 31 - w) - zat(z, 85 - w) + zat(z, 112 - w);
+                    bad |= h < -128 || h > 127;
+                    word |= (uint32_t)(uint8_t)(int8_t)h << (8 * b);
+                }
+                w4[e] = word;
+            }
+            dst[seq * (P8_HSEQ / 16) + q] = make_uint4(w4[0], w4[1], w4[2], w4[3]);
+        }
+    }
+    if (bad) atomicOr(err, 1u << 16);
+}
+
+template <int NV>
+__global__ void __launch_bounds__(P8<NV>::THREADS, 1) commit_p8_kernel(const TcArgs a) {
+    using S = P8<NV>;
+    extern __shared__ __align__(1024) uint8_t smem_raw[];
+    uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+    uint8_t* sA = smem;                                  // [ASTAGES][16 KB]
+    uint8_t* sB = sA + S::ASTAGES * TC_A_BYTES;          // [BSTAGES][B_BYTES]
+    uint8_t* sF = sB + S::BSTAGES * S::B_BYTES;          // [ASTAGES][F_STAGE]
+    uint64_t* bars = reinterpret_cast<uint64_t*>(sF + S::ASTAGES * S::F_STAGE);
+    uint64_t* full_a = bars;
+    uint64_t* empty_a = bars + S::ASTAGES;
+    uint64_t* full_b = bars + 2 * S::ASTAGES;
+    uint64_t* empty_b = full_b + S::BSTAGES;
+    uint64_t* done = empty_b + S::BSTAGES;
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(done + 1);
+    __shared__ int s_abort;
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const uint32_t cta = blockIdx.x;
+    const uint32_t group = cta % a.n_groups, ks = cta / a.n_groups;
+    const uint32_t kb0 = ks * a.kb_per_cta;
+    const uint32_t kb1 = min(a.n_kb, kb0 + a.kb_per_cta);
+    const uint32_t nkb = kb1 > kb0 ? kb1 - kb0 : 0;
+    const uint32_t nvalid = min((uint32_t)NV, a.n_vec - group * NV);
+
+    if (threadIdx.x == 0) {
+        s_abort = 0;
+        for (int s = 0; s < S::ASTAGES; s++) {
+            mbar_init(&full_a[s], 1);
+            mbar_init(&empty_a[s], 1);
+        }
+        for (int s = 0; s < S::BSTAGES; s++) {
+            mbar_init(&full_b[s], S::BUILDERS / 32);
+            mbar_init(&empty_b[s], 1);
+        }
+        mbar_init(done, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 1) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+                     "n"(S::TMEM_COLS));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;");
+    const uint32_t tmem = *tmem_slot;
+
+    if (warp == 0) {
+        // ---- producer: A tiles and window sequences ----
+        if (lane == 0) {
+            for (uint32_t it = 0; it < nkb; it++) {
+                const int s = it % S::ASTAGES;
+                const uint32_t ph = (it / S::ASTAGES) & 1;
+                if (it >= S::ASTAGES && !mbar_wait(&empty_a[s], ph ^ 1)) { atomicOr(a.err, 1u); s_abort = 1; break; }
+                if (s_abort) break;
+                const uint64_t kb = kb0 + it;
+                mbar_expect_tx(&full_a[s], TC_A_BYTES + nvalid * 2 * P8_FBYTES);
+                bulk_g2s(sA + s * TC_A_BYTES, a.ppl + kb * TC_A_BYTES, TC_A_BYTES, &full_a[s]);
+                for (uint32_t vl = 0; vl < nvalid; vl++)  // columns 2kb, 2kb+1 of vector vl: 448 contiguous bytes
+                    bulk_g2s(sF + s * S::F_STAGE + vl * 2 * P8_FBYTES,
+                             a.F + ((uint64_t)(group * NV + vl) * a.m + kb * 2) * P8_FBYTES, 2 * P8_FBYTES, &full_a[s]);
+            }
+        }
+    } else if (warp == 1) {
+        // ---- MMA issuer: one M = 128, N = 64 NV MMA per 32-byte K step ----
+        if (lane == 0) {
+            const uint32_t id = idesc_i8(S::NPAD);
+            for (uint32_t it = 0; it < nkb; it++) {
+                const int sa = it % S::ASTAGES, sb = it % S::BSTAGES;
+                if (!mbar_wait(&full_a[sa], (it / S::ASTAGES) & 1) || !mbar_wait(&full_b[sb], (it / S::BSTAGES) & 1)) {
+                    atomicOr(a.err, 2u);
+                    s_abort = 1;
+                    break;
+                }
+                asm volatile("tcgen05.fence::after_thread_sync;");
+                const uint32_t a0 = smem_u32(sA + sa * TC_A_BYTES), b0 = smem_u32(sB + sb * S::B_BYTES);
+#pragma unroll
+                for (int k = 0; k < 4; k++) {  // column k/2, s in [32(k%2), 32(k%2)+32): chunks 2(k%2), 2(k%2)+1
+                    const uint32_t acc = (it > 0 || k > 0) ? 1u : 0u;
+                    const uint32_t bcol = b0 + (k >> 1) * S::BCOL + (k & 1) * 2 * S::LBO;
+                    mma_i8(tmem, sw128_desc(a0 + 32 * k), ns_desc_lbo(bcol, S::LBO), id, acc);
+                }
+                mma_commit(&empty_a[sa]);
+                mma_commit(&empty_b[sb]);
+            }
+            mma_commit(done);
+        }
+    } else {
+        // ---- B builders: thread (column jj, vector v, seq, phase p = 8h + b)
+        // writes chunks c < 5 of G_p = H_seq[16c + p, 16c + p + 16) at
+        // [jj][c][h][seq][v][b]; the warp shares (jj, v), so lane groups of 8
+        // write 128 contiguous bytes ----
+        const int bt = threadIdx.x - 64;
+        const int p = bt & 15, seq = (bt >> 4) & 1, combo = bt >> 5;
+        const int v = combo % NV, jj = combo / NV;
+        for (uint32_t it = 0; it < nkb; it++) {
+            const int sa = it % S::ASTAGES, sb = it % S::BSTAGES;
+            uint32_t st = 0;  // 0 go, 1 timed out, 2 another role aborted (lane 0 waits for the warp)
+            if (lane == 0) {
+                if (!mbar_wait(&full_a[sa], (it / S::ASTAGES) & 1) ||
+                    (it >= S::BSTAGES && !mbar_wait(&empty_b[sb], ((it / S::BSTAGES) & 1) ^ 1)))
+                    st = 1;
+                else if (s_abort)
+                    st = 2;
+            }
+            st = __shfl_sync(0xffffffffu, st, 0);
+            if (st == 1 && lane == 0) {
+                atomicOr(a.err, 4u);
+                s_abort = 1;
+            }
+            if (st) break;
+            if (jj < 2 && (uint32_t)v < nvalid) {
+                const uint32_t* src = reinterpret_cast<const uint32_t*>(sF + sa * S::F_STAGE + (v * 2 + jj) * P8_FBYTES +
+                                                                        seq * P8_HSEQ) + (p >> 2);
+                const uint32_t sh = 8 * (p & 3);
+                uint8_t* dst = sB + sb * S::B_BYTES + jj * S::BCOL + (p >> 3) * (2 * NV * 128) + seq * (NV * 128) +
+                               v * 128 + (p & 7) * 16;
+                uint32_t w[21];  // words [p/4, p/4 + 21): bytes < 96 of the 112-byte sequence
+#pragma unroll
+                for (int q = 0; q < 21; q++) w[q] = src[q];
+#pragma unroll
+                for (int c = 0; c < 5; c++)
+                    *reinterpret_cast<uint4*>(dst + c * S::LBO) =
+                        make_uint4(__funnelshift_r(w[4 * c], w[4 * c + 1], sh), __funnelshift_r(w[4 * c + 1], w[4 * c + 2], sh),
+                                   __funnelshift_r(w[4 * c + 2], w[4 * c + 3], sh), __funnelshift_r(w[4 * c + 3], w[4 * c + 4], sh));
+            }
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&full_b[sb]);
+        }
+        // ---- epilogue (warps 2..5 cover TMEM lane groups 2, 3, 0, 1) ----
+        uint32_t okw = 0;
+        if (lane == 0) okw = (nkb > 0 && !s_abort && mbar_wait(done, 0)) ? 1u : 0u;
+        const bool ok = __shfl_sync(0xffffffffu, okw, 0) != 0;
+        if (nkb > 0 && !ok && warp < 6) atomicOr(a.err, 8u);
+        asm volatile("tcgen05.fence::after_thread_sync;");
+        const int lg = warp & 3;
+        const int row = lg * 32 + lane;
+        int32_t* dst = a.partial + ((uint64_t)cta * 128 + row) * S::NPAD;
+        for (int c0 = 0; c0 < (warp < 6 ? S::NPAD : 0); c0 += 16) {
+            uint32_t v16[16];
+            const uint32_t taddr = tmem + ((uint32_t)(lg * 32) << 16) + (uint32_t)c0;
+            asm volatile(
+                "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+                : "=r"(v16[0]), "=r"(v16[1]), "=r"(v16[2]), "=r"(v16[3]), "=r"(v16[4]), "=r"(v16[5]), "=r"(v16[6]),
+                  "=r"(v16[7]), "=r"(v16[8]), "=r"(v16[9]), "=r"(v16[10]), "=r"(v16[11]), "=r"(v16[12]), "=r"(v16[13]),
+                  "=r"(v16[14]), "=r"(v16[15])
+                : "r"(taddr));
+            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+            for (int q = 0; q < 16; q += 4)
+                *reinterpret_cast<int4*>(dst + c0 + q) =
+                    ok ? make_int4((int)v16[q], (int)v16[q + 1], (int)v16[q + 2], (int)v16[q + 3]) : make_int4(0, 0, 0, 0);
+        }
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;");
+    __syncthreads();
+    if (warp == 1) {
+        asm volatile("tcgen05.fence::after_thread_sync;");
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "n"(S::TMEM_COLS));
+    }
+}
+
+// c_{v,i}[r] = sum_{ks} sum_l 2^(8l) D[ks][(i,l)][col] mod q for the column
+// col of row r (no fold: the small-digit form computes mod Phi_81 directly).
+template <int NV>
+__global__ void __launch_bounds__(2 * P8<NV>::NPAD) commit_p8_reduce_kernel(const int32_t* __restrict__ partial,
+                                                                            uint32_t n_groups, uint32_t n_ksplit,
+                                                                            uint32_t kappa, uint32_t n_vec,
+                                                                            uint64_t* __restrict__ out) {
+    constexpr int NP = P8<NV>::NPAD;
+    const uint32_t group = blockIdx.x / kappa, i = blockIdx.x % kappa;
+    const int col = threadIdx.x % NP, half = threadIdx.x / NP;
+    __shared__ int64_t s_acc[NP][8];
+    int64_t acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    const uint32_t ks0 = half ? n_ksplit / 2 : 0, ks1 = half ? n_ksplit : n_ksplit / 2;
+    for (uint32_t ks = ks0; ks < ks1; ks++) {
+        const int32_t* pp = partial + ((uint64_t)(ks * n_groups + group) * 128 + i * 8) * NP + col;
+#pragma unroll
+        for (int l = 0; l < 8; l++) acc[l] += pp[(uint64_t)l * NP];
+    }
+    if (half) {
+#pragma unroll
+        for (int l = 0; l < 8; l++) s_acc[col][l] = acc[l];
+    }
+    __syncthreads();
+    if (half) return;
+    uint64_t c = 0;
+#pragma unroll
+    for (int l = 0; l < 8; l++) c = gl::add(c, gl::mul(gl::from_i64(acc[l] + s_acc[col][l]), 1ULL << (8 * l)));
+    const int g = col >> 3, b = col & 7;
+    const int v = g % NV, seq = (g / NV) & 1, h = (g / (2 * NV)) & 1, aa = g / (4 * NV);
+    const int rp = 16 * aa + 8 * h + b;
+    const uint32_t vg = group * NV + v;
+    if (rp >= 5 && vg < n_vec) out[((uint64_t)vg * kappa + i) * NEO_D + (seq ? 31 - rp : 58 - rp)] = c;
+}
+
 }  // namespace
 
 // ---------------------------------------------------------------------------
@@ -456,9 +741,15 @@ int tc_pp_prepare(neo_gpu_ctx* ctx, PPEntry* pp) {
     return NEO_OK;
 }
 
-size_t tc_scratch_bytes(uint32_t n_vec, uint64_t m, uint32_t* n_groups_out, uint32_t* n_ksplit_out,
+// Vectors per CTA: the cyclic form runs groups of 4; the small-digit form
+// runs a single vector alone (the MCS commitment: N = 64, no padding
+// vectors) and groups of 4 otherwise.
+static uint32_t tc_nv(uint32_t n_vec, bool small) { return small && n_vec == 1 ? 1 : 4; }
+
+size_t tc_scratch_bytes(uint32_t n_vec, uint64_t m, bool small, uint32_t* n_groups_out, uint32_t* n_ksplit_out,
                         uint32_t* kb_per_cta_out) {
-    const uint32_t n_groups = (n_vec + TC_NV - 1) / TC_NV;
+    const uint32_t nv = tc_nv(n_vec, small);
+    const uint32_t n_groups = (n_vec + nv - 1) / nv;
     const uint32_t n_kb = (uint32_t)(m / 2);
     // fill whole waves of 148 SMs (1 CTA per SM), at most TC_MAX_KB K blocks per CTA
     uint32_t waves = 1, n_ksplit;
@@ -473,39 +764,83 @@ size_t tc_scratch_bytes(uint32_t n_vec, uint64_t m, uint32_t* n_groups_out, uint
     *n_groups_out = n_groups;
     *n_ksplit_out = n_ksplit;
     *kb_per_cta_out = kb_per_cta;
-    size_t f_bytes = (size_t)n_vec * m * TC_FBYTES + 64;
-    size_t p_bytes = (size_t)n_groups * n_ksplit * 128 * TC_NPAD * 4;
-    return ((f_bytes + 255) & ~size_t(255)) + p_bytes + 256;
+    const size_t fb = small ? P8_FBYTES : TC_FBYTES, npad = small ? 64 * nv : TC_NPAD;
+    size_t f_bytes = (size_t)n_vec * m * fb + 64;
+    size_t p_bytes = (size_t)n_groups * n_ksplit * 128 * npad * 4;
+    return ((f_bytes + 255) & ~size_t(255)) + p_bytes + 256 /*flag*/ + 256;
+}
+
+template <int NV>
+static int launch_p8(neo_gpu_ctx* ctx, const TcArgs& a, uint32_t kappa, uint64_t* d_out) {
+    using S = P8<NV>;
+    const size_t smem = S::SMEM + 1024 /*align*/ + 256 /*barriers*/;
+    static SmemLimit limit;
+    NEO_CK(ctx, limit.at_least(commit_p8_kernel<NV>, smem));
+    commit_p8_kernel<NV><<<a.n_groups * a.n_ksplit, S::THREADS, smem, ctx->stream>>>(a);
+    NEO_LAUNCHED(ctx);
+    commit_p8_reduce_kernel<NV><<<a.n_groups * kappa, 2 * S::NPAD, 0, ctx->stream>>>(a.partial, a.n_groups, a.n_ksplit,
+                                                                                     kappa, a.n_vec, d_out);
+    NEO_LAUNCHED(ctx);
+    return NEO_OK;
 }
 
 int launch_commit_tc(neo_gpu_ctx* ctx, const PPEntry* pp, const int8_t* d_digits, uint32_t n_vec, uint64_t* d_out,
-                     uint8_t* scratch, uint32_t* d_err) {
+                     uint8_t* scratch, uint32_t* d_err, int digits) {
     const uint64_t m = pp->m;
+    TcArgs a;
+    a.ppl = pp->d_pp_limbs;
+    a.err = d_err;
+    a.m = m;
+    a.n_vec = n_vec;
+    a.n_kb = (uint32_t)(m / 2);
+    if (digits != TC_DIGITS_ANY) {
+        // small-digit form; for digits of unknown size the window sequences are
+        // built first and checked (one synchronisation), falling back to the
+        // cyclic form when an entry leaves int8
+        uint32_t n_groups, n_ksplit, kb_per_cta;
+        const size_t need = tc_scratch_bytes(n_vec, m, true, &n_groups, &n_ksplit, &kb_per_cta);
+        uint8_t* F = scratch;
+        const size_t f_end = ((size_t)n_vec * m * P8_FBYTES + 64 + 255) & ~size_t(255);
+        uint32_t* flag = reinterpret_cast<uint32_t*>(scratch + need - 512);
+        const bool known = digits == TC_DIGITS_SMALL;
+        if (!known) NEO_CK(ctx, cudaMemsetAsync(flag, 0, 4, ctx->stream));
+        p8_seq_kernel<<<ceil_div((uint64_t)n_vec * m, 128), 128, 0, ctx->stream>>>(d_digits, n_vec, m, F,
+                                                                                   known ? d_err : flag);
+        NEO_LAUNCHED(ctx);
+        bool ok = true;
+        if (!known) {
+            uint32_t h_flag = 0;
+            NEO_CK(ctx, ctx_d2h(ctx, &h_flag, flag, 4));
+            NEO_CK(ctx, ctx_sync(ctx));
+            ok = h_flag == 0;
+        }
+        if (ok) {
+            a.F = F;
+            a.partial = reinterpret_cast<int32_t*>(scratch + f_end);
+            a.n_groups = n_groups;
+            a.n_ksplit = n_ksplit;
+            a.kb_per_cta = kb_per_cta;
+            return tc_nv(n_vec, true) == 1 ? launch_p8<1>(ctx, a, pp->kappa, d_out) : launch_p8<4>(ctx, a, pp->kappa, d_out);
+        }
+    }
     uint32_t n_groups, n_ksplit, kb_per_cta;
-    tc_scratch_bytes(n_vec, m, &n_groups, &n_ksplit, &kb_per_cta);
+    tc_scratch_bytes(n_vec, m, false, &n_groups, &n_ksplit, &kb_per_cta);
     uint8_t* F = scratch;
     int32_t* partial = reinterpret_cast<int32_t*>(scratch + (((size_t)n_vec * m * TC_FBYTES + 64 + 255) & ~size_t(255)));
     f_seq_kernel<<<ceil_div((uint64_t)n_vec * m, 128), 128, 0, ctx->stream>>>(d_digits, n_vec, m, F);
     NEO_LAUNCHED(ctx);
-    TcArgs a;
-    a.ppl = pp->d_pp_limbs;
     a.F = F;
     a.partial = partial;
-    a.err = d_err;
-    a.m = m;
-    a.n_vec = n_vec;
     a.n_groups = n_groups;
     a.n_ksplit = n_ksplit;
     a.kb_per_cta = kb_per_cta;
-    a.n_kb = (uint32_t)(m / 2);
     const size_t smem = TC_SMEM_BYTES + 1024 /*align*/ + 256 /*barriers*/;
     static SmemLimit limit;
     NEO_CK(ctx, limit.at_least(commit_tc_kernel, smem));
     commit_tc_kernel<<<n_groups * n_ksplit, TC_THREADS, smem, ctx->stream>>>(a);
     NEO_LAUNCHED(ctx);
     commit_tc_reduce_kernel<<<n_groups * pp->kappa, RED_THREADS, 0, ctx->stream>>>(partial, n_groups, n_ksplit,
-                                                                                     pp->kappa, n_vec,
-                                                                        d_out);
+                                                                                     pp->kappa, n_vec, d_out);
     NEO_LAUNCHED(ctx);
     return NEO_OK;
 }

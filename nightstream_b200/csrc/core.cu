@@ -52,7 +52,11 @@ int check_device_error(neo_gpu_ctx* ctx) {
     NEO_CK(ctx, ctx_sync(ctx));
     if (e) {
         NEO_CK(ctx, cudaMemsetAsync(ctx->d_err, 0, 4, ctx->stream));
-        char buf[96];
+        char buf[128];
+        if (e == (1u << 16)) {  // set by the small-digit commitment form only
+            snprintf(buf, sizeof buf, "commitment digits outside [-63, 63] on the small-digit path");
+            return ctx->fail(NEO_ERR_INVARIANT, buf);
+        }
         snprintf(buf, sizeof buf, "device wait timed out (error bits 0x%x)", e);
         return ctx->fail(NEO_ERR_CUDA, buf);
     }
@@ -94,8 +98,7 @@ extern "C" int neo_gpu_ctx_stream(const neo_gpu_ctx* ctx, void** stream) { NEO_A
 static int neo_gpu_synchronize_impl_abi(neo_gpu_ctx* ctx) {
     if (!ctx) return NEO_ERR_ARG;
     cudaSetDevice(ctx->device);
-    NEO_CK(ctx, ctx_sync(ctx));
-    return NEO_OK;
+    return check_device_error(ctx);  // waits for the stream, then reports (and clears) device-side errors
 }
 extern "C" int neo_gpu_synchronize(neo_gpu_ctx* ctx) { NEO_ABI_GUARD(neo_gpu_synchronize_impl_abi(ctx)) }
 

@@ -1091,7 +1091,7 @@ static int rlc_dec_lane(neo_gpu_shard* sh, const char* lane, uint32_t idx, const
     P.insert(P.end(), c_parent.begin(), c_parent.end());
     // Pi_DEC: split into k_rho planes, commit, child claims
     if ((rc = split_b_device(ctx, sh->d_mix.p, (uint64_t)NEO_D * m, sh->k_rho, sh->b, d_planes, sh->d_flags.p))) return rc;
-    if ((rc = launch_commit(ctx, d_planes, sh->k_rho, m, sh->d_commits.p))) return rc;
+    if ((rc = launch_commit(ctx, d_planes, sh->k_rho, m, sh->d_commits.p, TC_DIGITS_SMALL))) return rc;  // planes in {-1, 0, 1}
     child_y_kernel<<<sh->k_rho * NEO_D, 256, 0, ctx->stream>>>(d_planes, m, t, d_vj, sh->d_ychild.p);
     NEO_LAUNCHED(ctx);
     uint32_t flags[2];
@@ -1225,7 +1225,7 @@ static int fold_step_impl(neo_gpu_shard* sh, const uint64_t* z_host, const uint6
     }
     decomp_b2_kernel<<<ceil_div(m, 256), 256, 0, ctx->stream>>>(d_z, m, sh->Zall.p);
     NEO_LAUNCHED(ctx);
-    if ((rc = launch_commit(ctx, sh->Zall.p, 1, m, sh->d_commits.p))) return rc;
+    if ((rc = launch_commit(ctx, sh->Zall.p, 1, m, sh->d_commits.p, TC_DIGITS_SMALL))) return rc;  // digits in {-1, 0, 1}
     if (has_mem) {
         bus_decode_kernel<<<ceil_div((uint64_t)nb * L, 256), 256, 0, ctx->stream>>>(d_z, sh->m_in, sh->bus_base, sh->steps,
                                                                                     nb, L, sh->d_cols.p);

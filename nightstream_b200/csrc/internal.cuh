@@ -191,11 +191,19 @@ int launch_chi_table(neo_gpu_ctx* ctx, const gl::K* d_bits, uint32_t nbits, gl::
 int launch_me_y(neo_gpu_ctx* ctx, const DevCcs& ccs, const int8_t* d_Z, uint32_t n_w, uint64_t m,
                 const gl::K* d_chi, uint32_t ell_n, uint32_t b, gl::K* d_vj_scratch, gl::K* d_y,
                 gl::K* d_ysc);
-int launch_commit(neo_gpu_ctx* ctx, const int8_t* d_digits, uint32_t n_vec, uint64_t m, uint64_t* d_out);
+// What the caller knows about the digits of a commitment: any int8
+// (TC_DIGITS_ANY: the cyclic tensor-core form), |digit| <= 63 by construction
+// (TC_DIGITS_SMALL: the small-digit form, a violation is reported through the
+// device error word), or nothing (TC_DIGITS_CHECK: the small-digit form after
+// one device check, else the cyclic form).
+enum { TC_DIGITS_ANY = 0, TC_DIGITS_SMALL = 1, TC_DIGITS_CHECK = 2 };
+int launch_commit(neo_gpu_ctx* ctx, const int8_t* d_digits, uint32_t n_vec, uint64_t m, uint64_t* d_out,
+                  int digits = TC_DIGITS_CHECK);
 int tc_pp_prepare(neo_gpu_ctx* ctx, PPEntry* pp);
-size_t tc_scratch_bytes(uint32_t n_vec, uint64_t m, uint32_t* n_groups, uint32_t* n_ksplit, uint32_t* kb_per_cta);
+size_t tc_scratch_bytes(uint32_t n_vec, uint64_t m, bool small, uint32_t* n_groups, uint32_t* n_ksplit,
+                        uint32_t* kb_per_cta);
 int launch_commit_tc(neo_gpu_ctx* ctx, const PPEntry* pp, const int8_t* d_digits, uint32_t n_vec, uint64_t* d_out,
-                     uint8_t* scratch, uint32_t* d_err);
+                     uint8_t* scratch, uint32_t* d_err, int digits);
 // reads and clears the device error word (synchronizes the stream)
 int check_device_error(neo_gpu_ctx* ctx);
 

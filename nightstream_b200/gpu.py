@@ -49,6 +49,7 @@ SIGNATURES = {
     "neo_gpu_ctx_stream": [P, P],
     "neo_gpu_synchronize": [P],
     "neo_gpu_commit_device": [P, ctypes.c_void_p, U32, U64, ctypes.c_void_p],
+    "neo_gpu_commit_device_ex": [P, ctypes.c_void_p, U32, U64, ctypes.c_void_p, U32],
     "neo_gpu_commit_noalloc": [P, ctypes.c_void_p, U32, U64, ctypes.c_void_p],
     "neo_gpu_mix_rhos_commits": [P, P, P, U32, U32, P],
     "neo_gpu_shard_step_proof": [P, P, U64, P],
@@ -162,6 +163,8 @@ def load(path: str = LIB_PATH):
             fn.argtypes = args
             fn.restype = _RESTYPES.get(name, I)
         _lib = L
+        if os.path.exists(TUNE_FILE):  # the launch-shape table measured on the target GPU (tune.py)
+            L.neo_gpu_tune_load(TUNE_FILE.encode())
     return _lib
 
 
@@ -210,8 +213,15 @@ class Context:
         (NEO_ERR_CUDA) when the wait runs out."""
         self.check(self.lib.neo_gpu_wait_probe(self.h, 1 if set_flag else 0, spin_limit))
 
-    def commit_device(self, d_digits: int, n_vec: int, m: int, d_out: int):
-        self.check(self.lib.neo_gpu_commit_device(self.h, ctypes.c_void_p(d_digits), n_vec, m, ctypes.c_void_p(d_out)))
+    def commit_device(self, d_digits: int, n_vec: int, m: int, d_out: int, small_digits: bool = False):
+        """Asynchronous commitment of device digits; small_digits: the caller
+        guarantees |digit| <= 63 (NEO_COMMIT_SMALL_DIGITS)."""
+        if small_digits:
+            self.check(self.lib.neo_gpu_commit_device_ex(self.h, ctypes.c_void_p(d_digits), n_vec, m,
+                                                         ctypes.c_void_p(d_out), 1))
+        else:
+            self.check(self.lib.neo_gpu_commit_device(self.h, ctypes.c_void_p(d_digits), n_vec, m,
+                                                      ctypes.c_void_p(d_out)))
 
     def commit_noalloc(self, d_digits: int, n_vec: int, m: int, d_out: int):
         """Commitment with the library's fixed device scratch (no allocation)."""

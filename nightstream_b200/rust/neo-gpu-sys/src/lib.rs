@@ -15,6 +15,7 @@ pub const NEO_ERR_INVARIANT: c_int = 3;
 pub const NEO_ERR_CUDA: c_int = 4;
 pub const NEO_ERR_UNSUPPORTED: c_int = 5;
 pub const NEO_ERR_CANCELLED: c_int = 6;
+pub const NEO_COMMIT_SMALL_DIGITS: u32 = 1;
 
 /// Memory-oracle kinds (include/neo_gpu.h, NEO_MEM_*).
 pub const NEO_MEM_SHOUT_VALUE: c_int = 0;
@@ -98,6 +99,7 @@ extern "C" {
     pub fn neo_gpu_chacha8_sample(ctx: *mut neo_gpu_ctx, seeds: *const u8, n_streams: u32, counts: *const u64, bound: u64, out: *mut u64) -> c_int;
     pub fn neo_gpu_commit(ctx: *mut neo_gpu_ctx, digits: *const i8, n_vec: u32, m: u64, out: *mut u64) -> c_int;
     pub fn neo_gpu_commit_device(ctx: *mut neo_gpu_ctx, d_digits: *const i8, n_vec: u32, m: u64, d_out: *mut u64) -> c_int;
+    pub fn neo_gpu_commit_device_ex(ctx: *mut neo_gpu_ctx, d_digits: *const i8, n_vec: u32, m: u64, d_out: *mut u64, flags: u32) -> c_int;
     pub fn neo_gpu_commit_noalloc(ctx: *mut neo_gpu_ctx, d_digits: *const i8, n_vec: u32, m: u64, d_out: *mut u64) -> c_int;
     pub fn neo_gpu_mix_rhos_commits(ctx: *mut neo_gpu_ctx, rhos: *const u64, cs: *const u64, count: u32, kappa: u32, out: *mut u64) -> c_int;
     pub fn neo_gpu_combine_b_pows(ctx: *mut neo_gpu_ctx, cs: *const u64, count: u32, kappa: u32, b: u32, out: *mut u64) -> c_int;

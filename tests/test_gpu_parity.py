@@ -49,6 +49,66 @@ def test_commit_int32_bound_extreme_pp(ctx):
     assert np.array_equal(got[0], O.commit_digits(pp, Z[0]))
 
 
+@pytest.mark.parametrize("n_vec", [1, 2, 4, 5])
+def test_commit_small_digit_form_extremes(ctx, n_vec):
+    """Digits with |z| <= 63 take the mod-Phi_81 tensor-core form, whose B
+    entries are differences of two digits: alternating +-63 (|entry| = 126,
+    the int8 limit of that form), constant +-63, random digits in [-63, 63]
+    and one digit of 64 (the call falls back to the cyclic form) all equal the
+    oracle, against PP limbs of 0xFF (the int32 bound of the partial sums)."""
+    m = 2048
+    pp = np.full((16, m, 54), (1 << 64) - (1 << 32), dtype=np.uint64)
+    pp[:, :, ::2] = np.uint64(0xFEFFFFFFFFFFFFFF)
+    pp[:, ::3] = _pp(16, m, 7)[:, ::3]
+    ctx.pp_upload(pp)
+    rng = np.random.default_rng(n_vec)
+    alt = np.where(np.arange(54)[:, None] % 2 == 0, 63, -63).astype(np.int8) * np.ones((1, m), np.int8)
+    cases = [np.stack([alt] * n_vec), np.full((n_vec, 54, m), -63, np.int8), np.full((n_vec, 54, m), 63, np.int8),
+             rng.integers(-63, 64, size=(n_vec, 54, m)).astype(np.int8)]
+    over = rng.integers(-63, 64, size=(n_vec, 54, m)).astype(np.int8)
+    over[-1, 53, m - 1] = 64
+    cases.append(over)
+    for Z in cases:
+        got = ctx.commit(Z)
+        for v in range(n_vec):
+            assert np.array_equal(got[v], O.commit_digits(pp, Z[v]))
+
+
+def test_commit_device_ex_small_digits(ctx):
+    """neo_gpu_commit_device_ex with NEO_COMMIT_SMALL_DIGITS (the form the fold
+    step uses for its ternary planes) equals the host commitment and the
+    any-int8 device form; digits that break the |z| <= 63 guarantee are
+    reported as NEO_ERR_INVARIANT at the next synchronisation, and the context
+    stays usable."""
+    import torch
+    from nightstream_b200.gpu import NeoGpuError
+    m, n_vec = 4096, 12
+    pp = _pp(16, m, 21)
+    ctx.pp_upload(pp)
+    Z = np.random.default_rng(8).integers(-1, 2, size=(n_vec, 54, m)).astype(np.int8)
+    want = ctx.commit(Z)
+    d = torch.from_numpy(Z).cuda()
+    out = torch.zeros((n_vec, 16, 54), dtype=torch.int64, device="cuda")
+    torch.cuda.synchronize()
+    for small in (True, False, True):
+        out.zero_()
+        torch.cuda.synchronize()
+        ctx.commit_device(d.data_ptr(), n_vec, m, out.data_ptr(), small_digits=small)
+        ctx.synchronize()
+        assert np.array_equal(out.cpu().numpy().view(np.uint64), want)
+    bad = Z.copy()
+    bad[3, 10, 100] = 100
+    db = torch.from_numpy(bad).cuda()
+    torch.cuda.synchronize()
+    ctx.commit_device(db.data_ptr(), n_vec, m, out.data_ptr(), small_digits=True)
+    with pytest.raises(NeoGpuError) as e:
+        ctx.synchronize()
+    assert e.value.code == 3
+    ctx.commit_device(d.data_ptr(), n_vec, m, out.data_ptr(), small_digits=True)
+    ctx.synchronize()
+    assert np.array_equal(out.cpu().numpy().view(np.uint64), want)
+
+
 def test_decomp_matches_oracle(ctx):
     rng = np.random.default_rng(3)
     z = np.concatenate([rng.integers(0, 1 << 32, size=5000, dtype=np.uint64),
