@@ -50,9 +50,10 @@ def parse():
     ap.add_argument("--chunk", type=int, default=1024, help="trace steps per fold step (memory workload)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--mode", default="plain", choices=["plain", "batched", "served"],
+    ap.add_argument("--mode", default="plain", choices=["plain", "batched", "served", "rounds", "commit"],
                     help="plain: one shard; batched: 64 uneven shards batched vs one at a time; "
-                         "served: Poisson arrivals, p50/p99 latency")
+                         "served: Poisson arrivals, p50/p99 latency; rounds / commit: the Pi_CCS row-round "
+                         "sequence or the commitment alone at --ell (--steps timed repetitions)")
     ap.add_argument("--shards", type=int, default=64)
     ap.add_argument("--batch-reps", type=int, default=3, help="batched runs of the mix; the median is reported")
     ap.add_argument("--shard-steps", type=int, default=3)
@@ -245,6 +246,61 @@ def rounds_roofline(ctx, ccs, z, ell, stream, reps=3):
             "algorithmic_bytes_per_sequence": B,
             "note": "integer-ALU bound: the rounds stream int8 digit planes in rounds 0..4 and move far fewer "
                     "bytes than B_ccs"}
+
+
+def commit_roofline(ctx, m, stream, n_vec=12, reps=5):
+    """The DEC batch commitment (n_vec ternary digit planes in one call, the
+    small-digit tensor-core form) timed with CUDA events on the library
+    stream; the PP limb tiles (537 MB at m = 2^16) exceed L2, so consecutive
+    launches stream them from HBM."""
+    import torch
+    digits = torch.randint(-1, 2, (n_vec, 54, m), dtype=torch.int8, device="cuda")
+    outc = torch.empty((n_vec, 16, 54), dtype=torch.int64, device="cuda")
+    torch.cuda.synchronize()
+    for _ in range(2):
+        ctx.commit_device(digits.data_ptr(), n_vec, m, outc.data_ptr(), small_digits=True)
+    ctx.synchronize()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    for _ in range(reps):
+        ctx.commit_device(digits.data_ptr(), n_vec, m, outc.data_ptr(), small_digits=True)
+    ev1.record(stream)
+    ev1.synchronize()
+    commit_ms = ev0.elapsed_time(ev1) / reps
+    ops = 746496 * m * n_vec  # 2 * 8 limbs * kappa * d^2 * m per commitment
+    peak, peak_src = int8_peak_tops()
+    achieved = ops / (commit_ms * 1e-3) / 1e12
+    nv = 4 if n_vec > 1 else 1
+    return {"kernel": f"Ajtai commit, {n_vec} digit plane(s) per call, small-digit form (p8_seq_kernel + "
+                      f"commit_p8_kernel<{nv}>: tcgen05 kind::i8, N = {64 * nv}, + commit_p8_reduce_kernel<{nv}>)",
+            "bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TOPS", "frac": achieved / peak,
+            "traffic": COMMIT_TRAFFIC_PER_M * m if m >= 1 << 14 and n_vec == 12 else None,
+            "traffic_source": "ncu dram__bytes_read+write of one 12-plane commit_p8_kernel<4> launch at "
+                              "m = 2^14, scaled by m",
+            "launch_ms": commit_ms, "peak_source": peak_src, "algorithmic_ops_per_launch": ops,
+            "frac_of_datasheet": achieved / INT8_DATASHEET_TOPS,
+            "datasheet_peak": INT8_DATASHEET_TOPS}
+
+
+def run_kernel_mode(args):
+    """--mode rounds / commit: one kernel family alone at --ell (profiling and
+    tuning; prints one JSON line)."""
+    import torch
+    from nightstream_b200 import gpu, synth
+    ctx = gpu.Context(0)
+    stream = torch.cuda.ExternalStream(ctx.stream)
+    m = 1 << args.ell
+    if args.mode == "rounds":
+        ccs, z = synth.make_r1cs(args.ell, 3)
+        out = rounds_roofline(ctx, ccs, z, args.ell, stream, reps=args.steps)
+    else:
+        ctx.pp_upload(np.random.default_rng(1).integers(0, Q, size=(16, m, 54), dtype=np.uint64))
+        out = {"planes12": commit_roofline(ctx, m, stream, 12, args.steps),
+               "mcs1": commit_roofline(ctx, m, stream, 1, args.steps)}
+    out["mode"] = args.mode
+    out["ell"] = args.ell
+    print(json.dumps(out), flush=True)
+    ctx.close()
 
 
 def int8_peak_tops():
@@ -621,33 +677,7 @@ def run_ours(args, rank, world, local_rank):
         e2e = {"value": replica_value(world, args.steps, ems), "unit": UNIT, "h2d_bytes_per_step": int(zh[0].nbytes),
                "d2h_bytes_per_step": int(proof.nbytes)}
 
-    # dominant kernel roofline: the DEC batch commitment (12 digit planes, one launch pair)
-    n_vec = 12
-    digits = torch.randint(-1, 2, (n_vec, 54, m), dtype=torch.int8, device="cuda")
-    outc = torch.empty((n_vec, 16, 54), dtype=torch.int64, device="cuda")
-    torch.cuda.synchronize()
-    for _ in range(2):
-        ctx.commit_device(digits.data_ptr(), n_vec, m, outc.data_ptr(), small_digits=True)
-    ctx.synchronize()
-    reps = 5
-    ev0.record(stream)
-    for _ in range(reps):
-        ctx.commit_device(digits.data_ptr(), n_vec, m, outc.data_ptr(), small_digits=True)
-    ev1.record(stream)
-    ev1.synchronize()
-    commit_ms = ev0.elapsed_time(ev1) / reps
-    ops = 746496 * m * n_vec  # 2 * 8 limbs * kappa * d^2 * m per commitment
-    peak, peak_src = int8_peak_tops()
-    achieved = ops / (commit_ms * 1e-3) / 1e12
-    roofline_commit = {"kernel": "Ajtai commit, 12 DEC planes per launch, small-digit form (p8_seq_kernel + "
-                                 "commit_p8_kernel<4>: tcgen05 kind::i8, N = 256, + commit_p8_reduce_kernel<4>)",
-                       "bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TOPS", "frac": achieved / peak,
-                       "traffic": COMMIT_TRAFFIC_PER_M * m if m >= 1 << 14 else None,
-                       "traffic_source": "ncu dram__bytes_read+write of one 12-plane commit_tc_kernel launch at "
-                                         "m = 2^14, scaled by m",
-                       "launch_ms": commit_ms, "peak_source": peak_src, "algorithmic_ops_per_launch": ops,
-                       "frac_of_datasheet": achieved / INT8_DATASHEET_TOPS,
-                       "datasheet_peak": INT8_DATASHEET_TOPS}
+    roofline_commit = commit_roofline(ctx, m, stream)
     roofline = rounds_roofline(ctx, ccs, wl.z(0), args.ell, stream)
     # the batched mix runs before the legs that use the host's OpenMP pool
     batched = batched_result(args) if rank == 0 and world == 1 and not args.no_batch else None
@@ -699,6 +729,9 @@ def main():
         elif args.mode == "served":
             if rank == 0:
                 run_served(args)
+        elif args.mode in ("rounds", "commit"):
+            if rank == 0:
+                run_kernel_mode(args)
         else:
             run_ours(args, rank, world, local_rank)
     finally:

@@ -122,9 +122,11 @@ int neo_gpu_commit_device(neo_gpu_ctx* ctx, const int8_t* d_digits, uint32_t n_v
 /* neo_gpu_commit_device with flags.  NEO_COMMIT_SMALL_DIGITS: the caller
  * guarantees |digit| <= 63 (balanced base-b digits, b <= 64, as
  * decomp_b_row_major produces, crates/neo-ajtai/src/decomp.rs:118-158), so
- * the product is taken mod Phi_81 directly on the tensor cores; a digit pair
- * that breaks the guarantee is reported as NEO_ERR_INVARIANT by the next call
- * that checks the context's device error word (neo_gpu_synchronize).
+ * the product is taken mod Phi_81 directly on the tensor cores, whose operand
+ * entries are sums of two digits.  Digits outside the guarantee whose sums
+ * leave int8 (the result would be wrong) are reported as NEO_ERR_INVARIANT by
+ * the next call that checks the context's device error word
+ * (neo_gpu_synchronize); otherwise the result is exact.
  * Asynchronous on the context stream. */
 #define NEO_COMMIT_SMALL_DIGITS 1u
 int neo_gpu_commit_device_ex(neo_gpu_ctx* ctx, const int8_t* d_digits, uint32_t n_vec, uint64_t m, uint64_t* d_out,

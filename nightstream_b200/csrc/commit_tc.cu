@@ -469,7 +469,13 @@ struct P8 {
     static constexpr int F_STAGE = NV * 2 * P8_FBYTES;
     static constexpr int BUILDERS = NV >= 2 ? 64 * NV : 128;  // (column, vector, seq, phase); >= 4 epilogue warps
     static constexpr int THREADS = 64 + BUILDERS;
-    static constexpr int ASTAGES = 6, BSTAGES = 4;
+#ifndef P8_ASTAGES
+#define P8_ASTAGES 6
+#endif
+#ifndef P8_BSTAGES
+#define P8_BSTAGES 4
+#endif
+    static constexpr int ASTAGES = P8_ASTAGES, BSTAGES = P8_BSTAGES;
     static constexpr int SMEM = ASTAGES * (TC_A_BYTES + F_STAGE) + BSTAGES * B_BYTES;
     static constexpr uint32_t TMEM_COLS = NPAD <= 64 ? 64 : (NPAD <= 128 ? 128 : 256);
     static_assert(NPAD <= 256 && NPAD % 16 == 0, "one MMA per K step (M = 128: N <= 256, N % 16 == 0)");

@@ -331,7 +331,8 @@ struct MultiClaim {
     K r;               // fold challenge
     uint32_t blk0;     // first block of this claim
     uint32_t part0;    // first partial [npts][nblk]
-    uint32_t nblk;
+    uint32_t nblk;     // blocks of 256 pairs
+    uint32_t ppt;      // evaluation points per thread (1, 2, 4 or MX): blocks = ceil(npts / ppt) * nblk
     K* out;            // values at x = 0..npts-1 (reduce kernel)
 };
 
@@ -359,16 +360,62 @@ __global__ void __launch_bounds__(256) mem_multi_fold_kernel(const __grid_consta
     c.dst[f * half + t] = gl::klerp(s[0], s[1], c.r);
 }
 
-// One thread per pair of one claim: the claim's factor pairs are read once per
-// MX points, the product (or the bitness sum) evaluated at those points with
-// additions along x, and each point reduced over the block.
+// Values of one pair at x = x0 .. x0 + PPT - 1: the product of the claim's
+// affine factors (or the gated bitness sum), additions along x.
+template <int PPT>
+__device__ __forceinline__ void multi_eval_points(const MultiClaim& c, uint64_t p, uint32_t x0, K* acc) {
+#pragma unroll
+    for (int i = 0; i < PPT; i++) acc[i] = c.bitness ? gl::kzero() : gl::kone();
+    if (!c.bitness) {
+        for (uint32_t f = 0; f < c.nf; f++) {
+            const K* s = c.tab + (uint64_t)f * c.len + 2 * p;
+            const K f0 = s[0], d = gl::ksub(s[1], f0);
+            K v = gl::kadd(f0, gl::kscale_small(d, (int32_t)x0));
+#pragma unroll
+            for (int i = 0; i < PPT; i++) {
+                acc[i] = gl::kmul(acc[i], v);
+                v = gl::kadd(v, d);
+            }
+        }
+        return;
+    }
+    for (uint32_t f = 1; f < c.nf; f++) {
+        const K* s = c.tab + (uint64_t)f * c.len + 2 * p;
+        if (gl::kiszero(s[0]) && gl::kiszero(s[1])) continue;  // b(b - 1) = 0 at every x
+        const K f0 = s[0], d = gl::ksub(s[1], f0), w = c.w[f - 1];
+        K v = gl::kadd(f0, gl::kscale_small(d, (int32_t)x0));
+#pragma unroll
+        for (int i = 0; i < PPT; i++) {
+            acc[i] = gl::kadd(acc[i], gl::kmul(w, gl::kmul(v, gl::ksub(v, gl::kone()))));
+            v = gl::kadd(v, d);
+        }
+    }
+    const K* s = c.tab + 2 * p;
+    const K f0 = s[0], d = gl::ksub(s[1], f0);
+    K v = gl::kadd(f0, gl::kscale_small(d, (int32_t)x0));
+#pragma unroll
+    for (int i = 0; i < PPT; i++) {
+        acc[i] = gl::kmul(acc[i], v);
+        v = gl::kadd(v, d);
+    }
+}
+
+// Block (point group g, pair block pb) of one claim: thread t takes pair
+// pb * 256 + t at the claim's ppt points x0 = g * ppt ..; each point is
+// reduced over the block into partials[x][pb].  A claim with many pairs
+// takes MX points per thread (its factor pairs read once per MX points); one
+// with few pairs (the late rounds) takes fewer, so that its point groups run
+// side by side instead of one thread walking every point.
 __global__ void __launch_bounds__(256) mem_multi_eval_kernel(const __grid_constant__ MultiArgs a) {
     __shared__ K s_red[256 / 32][MX];
     const int ci = multi_claim_of(a, blockIdx.x);
     const MultiClaim& c = a.c[ci];
     const uint32_t b = blockIdx.x - c.blk0;
+    const uint32_t g = b / c.nblk, pb = b % c.nblk;
+    const uint32_t x0 = g * c.ppt;
+    const uint32_t np = min(c.ppt, c.npts - x0);
     const uint64_t pairs = c.len >> 1;
-    const uint64_t p = (uint64_t)b * 256 + threadIdx.x;
+    const uint64_t p = (uint64_t)pb * 256 + threadIdx.x;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     // a pair whose gate factor (the first, or every bitness column) is zero on
     // both children contributes nothing at any x
@@ -377,65 +424,36 @@ __global__ void __launch_bounds__(256) mem_multi_eval_kernel(const __grid_consta
         const K* s = c.tab + 2 * p;
         live = !(gl::kiszero(s[0]) && gl::kiszero(s[1]));
     }
-    for (uint32_t x0 = 0; x0 < c.npts; x0 += MX) {
-        K acc[MX];
+    K acc[MX];
 #pragma unroll
-        for (int i = 0; i < MX; i++) acc[i] = live ? (c.bitness ? gl::kzero() : gl::kone()) : gl::kzero();
-        if (live) {
-            if (!c.bitness) {
-                for (uint32_t f = 0; f < c.nf; f++) {
-                    const K* s = c.tab + (uint64_t)f * c.len + 2 * p;
-                    const K f0 = s[0], d = gl::ksub(s[1], f0);
-                    K v = gl::kadd(f0, gl::kscale_small(d, (int32_t)x0));
-#pragma unroll
-                    for (int i = 0; i < MX; i++) {
-                        acc[i] = gl::kmul(acc[i], v);
-                        v = gl::kadd(v, d);
-                    }
-                }
-            } else {
-                for (uint32_t f = 1; f < c.nf; f++) {
-                    const K* s = c.tab + (uint64_t)f * c.len + 2 * p;
-                    if (gl::kiszero(s[0]) && gl::kiszero(s[1])) continue;  // b(b - 1) = 0 at every x
-                    const K f0 = s[0], d = gl::ksub(s[1], f0), w = c.w[f - 1];
-                    K v = gl::kadd(f0, gl::kscale_small(d, (int32_t)x0));
-#pragma unroll
-                    for (int i = 0; i < MX; i++) {
-                        acc[i] = gl::kadd(acc[i], gl::kmul(w, gl::kmul(v, gl::ksub(v, gl::kone()))));
-                        v = gl::kadd(v, d);
-                    }
-                }
-                const K* s = c.tab + 2 * p;
-                const K f0 = s[0], d = gl::ksub(s[1], f0);
-                K v = gl::kadd(f0, gl::kscale_small(d, (int32_t)x0));
-#pragma unroll
-                for (int i = 0; i < MX; i++) {
-                    acc[i] = gl::kmul(acc[i], v);
-                    v = gl::kadd(v, d);
-                }
-            }
+    for (int i = 0; i < MX; i++) acc[i] = gl::kzero();
+    if (live) {
+        switch (c.ppt) {
+            case 1: multi_eval_points<1>(c, p, x0, acc); break;
+            case 2: multi_eval_points<2>(c, p, x0, acc); break;
+            case 4: multi_eval_points<4>(c, p, x0, acc); break;
+            default: multi_eval_points<MX>(c, p, x0, acc); break;
         }
-        const bool any = __syncthreads_or(live);
-        if (!any) {
-            if (threadIdx.x < MX && x0 + threadIdx.x < c.npts)
-                a.partials[c.part0 + (uint64_t)(x0 + threadIdx.x) * c.nblk + b] = gl::kzero();
-            continue;
-        }
+    }
+    const bool any = __syncthreads_or(live);
+    if (!any) {
+        if (threadIdx.x < np) a.partials[c.part0 + (uint64_t)(x0 + threadIdx.x) * c.nblk + pb] = gl::kzero();
+        return;
+    }
 #pragma unroll
-        for (int i = 0; i < MX; i++) {
-            K v = acc[i];
+    for (int i = 0; i < MX; i++) {
+        if ((uint32_t)i >= np) break;
+        K v = acc[i];
 #pragma unroll
-            for (int o = 16; o > 0; o >>= 1) v = gl::kadd(v, shfl_xor_km(v, o));
-            if (lane == 0) s_red[warp][i] = v;
-        }
-        __syncthreads();
-        if (threadIdx.x < MX && x0 + threadIdx.x < c.npts) {
-            K v = gl::kzero();
+        for (int o = 16; o > 0; o >>= 1) v = gl::kadd(v, shfl_xor_km(v, o));
+        if (lane == 0) s_red[warp][i] = v;
+    }
+    __syncthreads();
+    if (threadIdx.x < np) {
+        K v = gl::kzero();
 #pragma unroll
-            for (int w = 0; w < 256 / 32; w++) v = gl::kadd(v, s_red[w][threadIdx.x]);
-            a.partials[c.part0 + (uint64_t)(x0 + threadIdx.x) * c.nblk + b] = v;
-        }
-        __syncthreads();
+        for (int w = 0; w < 256 / 32; w++) v = gl::kadd(v, s_red[w][threadIdx.x]);
+        a.partials[c.part0 + (uint64_t)(x0 + threadIdx.x) * c.nblk + pb] = v;
     }
 }
 
@@ -805,9 +823,13 @@ int mem_round_launch_multi(neo_gpu_ctx* ctx, neo_gpu_mem_oracle* const* os, int 
         c.w = o->w.p;
         c.blk0 = blocks;
         c.nblk = (uint32_t)ceil_div(o->len >> 1, 256);
+        // points per thread: MX while the pairs fill the GPU, fewer for the
+        // small tables of the late rounds (their point groups run in parallel)
+        const uint64_t pairs = o->len >> 1;
+        c.ppt = pairs >= 8192 ? MX : (pairs >= 1024 ? 4 : (pairs >= 256 ? 2 : 1));
         c.part0 = (uint32_t)parts;
         c.out = d_out[i];
-        blocks += c.nblk;
+        blocks += c.nblk * (uint32_t)ceil_div(c.npts, c.ppt);
         parts += (uint64_t)c.npts * c.nblk;
         pts += c.npts;
     }

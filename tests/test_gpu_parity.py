@@ -77,9 +77,9 @@ def test_commit_small_digit_form_extremes(ctx, n_vec):
 def test_commit_device_ex_small_digits(ctx):
     """neo_gpu_commit_device_ex with NEO_COMMIT_SMALL_DIGITS (the form the fold
     step uses for its ternary planes) equals the host commitment and the
-    any-int8 device form; digits that break the |z| <= 63 guarantee are
-    reported as NEO_ERR_INVARIANT at the next synchronisation, and the context
-    stays usable."""
+    any-int8 device form; digits that break the |z| <= 63 guarantee so that
+    a window entry leaves int8 are reported as NEO_ERR_INVARIANT at the next
+    synchronisation, and the context stays usable."""
     import torch
     from nightstream_b200.gpu import NeoGpuError
     m, n_vec = 4096, 12
@@ -97,7 +97,8 @@ def test_commit_device_ex_small_digits(ctx):
         ctx.synchronize()
         assert np.array_equal(out.cpu().numpy().view(np.uint64), want)
     bad = Z.copy()
-    bad[3, 10, 100] = 100
+    bad[3, 10, 100] = 100  # rows 10 and 37 (27 apart) meet in one window entry: 100 - (-100) leaves int8
+    bad[3, 37, 100] = -100
     db = torch.from_numpy(bad).cuda()
     torch.cuda.synchronize()
     ctx.commit_device(db.data_ptr(), n_vec, m, out.data_ptr(), small_digits=True)
