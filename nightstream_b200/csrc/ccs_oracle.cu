@@ -681,6 +681,8 @@ struct neo_gpu_ccs_oracle {
     bool hist_split = false;
     uint32_t compact_q = 8;     // q per thread below which the NC blocks use out-of-line K products
     uint64_t nc_threads = 148ull * 2 * 256;  // NC threads per round (one wave) when the pairs alone are fewer
+    uint64_t late_pairs = 0;                 // rounds with fewer pairs than this use late_threads NC threads
+    uint64_t late_threads = 256;
     uint32_t hist_items = 16384;              // target (q, 8-row block) items per histogram block
     K gamma{}, gamma_to_k{};
     std::vector<K> alpha, beta_a, beta_r, r_in, row_chals, ajtai_chals;
@@ -949,7 +951,7 @@ static void fast_nc_grid(const neo_gpu_ccs_oracle* o, uint32_t j, uint32_t* n_ch
                          uint32_t* blocks) {
     const uint32_t nq = o->k * NEO_D;
     const uint64_t pairs = o->n_pad >> (j + 1);
-    const uint64_t target = o->nc_threads;
+    const uint64_t target = pairs < o->late_pairs ? o->late_threads : o->nc_threads;
     const uint32_t nc = (uint32_t)std::min<uint64_t>(nq, std::max<uint64_t>(1, (target + pairs - 1) / pairs));
     *q_chunk = (nq + nc - 1) / nc;
     *n_chunk = (nq + *q_chunk - 1) / *q_chunk;
@@ -971,14 +973,12 @@ static int fast_setup(neo_gpu_ccs_oracle* o) {
     }
     if (const char* e = getenv("NEO_TUNE_CCS_COMPACT_Q")) o->compact_q = (uint32_t)strtoul(e, nullptr, 10);
     if (const char* e = getenv("NEO_TUNE_CCS_NC_THREADS")) o->nc_threads = std::max<uint64_t>(1, strtoull(e, nullptr, 10));
+    if (const char* e = getenv("NEO_TUNE_CCS_LATE_PAIRS")) o->late_pairs = strtoull(e, nullptr, 10);
+    if (const char* e = getenv("NEO_TUNE_CCS_LATE_THREADS")) o->late_threads = std::max<uint64_t>(1, strtoull(e, nullptr, 10));
     const uint32_t ell = o->ell_n, nq = o->k * NEO_D;
     // E_j = chi of beta_r[j+1..ell) for every row round (beta_r is in ws_bits[0..ell))
     NEO_CK(ctx, o->E_all.ensure(o->n_pad));
-    for (uint32_t j = 0; j < ell; j++) {
-        const uint64_t off = o->n_pad - (o->n_pad >> j);
-        int rc = launch_chi_table(ctx, o->ws_bits.p + j + 1, ell - j - 1, o->E_all.p + off);
-        if (rc) return rc;
-    }
+    if (int rc = launch_suffix_chi_tables(ctx, o->ws_bits.p, ell, o->E_all.p)) return rc;
     // histogram grid: a thread per 8-row block, q chunks so that ~2 blocks per SM
     // split histograms (even / odd 8-row blocks) when round 3 exists
     const uint32_t n_t8 = (uint32_t)(o->n_pad >> 3);

@@ -629,10 +629,12 @@ __global__ void __launch_bounds__(P8<NV>::THREADS, 1) commit_p8_kernel(const TcA
         const int bt = threadIdx.x - 64;
         const int p = bt & 15, seq = (bt >> 4) & 1, combo = bt >> 5;
         const int v = combo % NV, jj = combo / NV;
+        const bool active = jj < 2 && (uint32_t)v < nvalid;
         for (uint32_t it = 0; it < nkb; it++) {
-            const int sa = it % S::ASTAGES, sb = it % S::BSTAGES;
+            const int sb = it % S::BSTAGES;
             uint32_t st = 0;  // 0 go, 1 timed out, 2 another role aborted (lane 0 waits for the warp)
             if (lane == 0) {
+                const int sa = it % S::ASTAGES;
                 if (!mbar_wait(&full_a[sa], (it / S::ASTAGES) & 1) ||
                     (it >= S::BSTAGES && !mbar_wait(&empty_b[sb], ((it / S::BSTAGES) & 1) ^ 1)))
                     st = 1;
@@ -645,15 +647,16 @@ __global__ void __launch_bounds__(P8<NV>::THREADS, 1) commit_p8_kernel(const TcA
                 s_abort = 1;
             }
             if (st) break;
-            if (jj < 2 && (uint32_t)v < nvalid) {
+            if (active) {
+                const int sa = it % S::ASTAGES;
                 const uint32_t* src = reinterpret_cast<const uint32_t*>(sF + sa * S::F_STAGE + (v * 2 + jj) * P8_FBYTES +
                                                                         seq * P8_HSEQ) + (p >> 2);
-                const uint32_t sh = 8 * (p & 3);
-                uint8_t* dst = sB + sb * S::B_BYTES + jj * S::BCOL + (p >> 3) * (2 * NV * 128) + seq * (NV * 128) +
-                               v * 128 + (p & 7) * 16;
                 uint32_t w[21];  // words [p/4, p/4 + 21): bytes < 96 of the 112-byte sequence
 #pragma unroll
                 for (int q = 0; q < 21; q++) w[q] = src[q];
+                const uint32_t sh = 8 * (p & 3);
+                uint8_t* dst = sB + sb * S::B_BYTES + jj * S::BCOL + (p >> 3) * (2 * NV * 128) + seq * (NV * 128) +
+                               v * 128 + (p & 7) * 16;
 #pragma unroll
                 for (int c = 0; c < 5; c++)
                     *reinterpret_cast<uint4*>(dst + c * S::LBO) =

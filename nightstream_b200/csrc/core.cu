@@ -184,6 +184,31 @@ int launch_chi_table(neo_gpu_ctx* ctx, const K* d_bits, uint32_t nbits, K* d_out
     return NEO_OK;
 }
 
+// The tables chi(bits[j+1..nbits)) of every j < nbits in one launch: table j
+// (2^(nbits-j-1) entries) sits at n - n/2^j, n = 2^nbits, so an index's
+// leading one bits give its j.
+__global__ void suffix_chi_kernel(const K* __restrict__ bits, uint32_t nbits, K* __restrict__ out) {
+    const uint64_t n = 1ULL << nbits;
+    const uint64_t idx = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+    if (idx + 1 >= n) return;
+    const uint32_t j = __clzll(~(idx << (64 - nbits)));  // leading ones of the nbits-bit index
+    const uint64_t local = idx - (n - (n >> j));
+    K w = gl::kone();
+    for (uint32_t i = 0; i + j + 1 < nbits; i++) {
+        const K b = bits[j + 1 + i];
+        w = gl::kmul(w, ((local >> i) & 1) ? b : gl::ksub(gl::kone(), b));
+    }
+    out[idx] = w;
+}
+
+int launch_suffix_chi_tables(neo_gpu_ctx* ctx, const K* d_bits, uint32_t nbits, K* d_out) {
+    if (nbits == 0) return NEO_OK;
+    const uint64_t n = 1ULL << nbits;
+    suffix_chi_kernel<<<ceil_div(n - 1, 256), 256, 0, ctx->stream>>>(d_bits, nbits, d_out);
+    NEO_LAUNCHED(ctx);
+    return NEO_OK;
+}
+
 // ---------------------------------------------------------------------------
 // decomp_b (b = 2, balanced) (crates/neo-ajtai/src/decomp.rs:118-158)
 // ---------------------------------------------------------------------------

@@ -705,6 +705,7 @@ int ccs_oracle_dev_vj(neo_gpu_ccs_oracle* o, const K** vj);
 int ccs_oracle_round_launch(neo_gpu_ccs_oracle* o, K* d_dst, uint32_t* ncoef);
 void ccs_oracle_round_set(neo_gpu_ccs_oracle* o, const K* coeffs);
 bool mem_round_multi_ok(const neo_gpu_mem_oracle* o);
+int ta_round_launch(neo_gpu_twist_addr* o, K* d_dst, bool* launched);
 int mem_round_launch_multi(neo_gpu_ctx* ctx, neo_gpu_mem_oracle* const* os, int n, K* const* d_out,
                            DevBuf<K>& partials);
 
@@ -801,9 +802,9 @@ struct Claim {
 // (sumcheck_ds.rs:11-19); round polynomials appended to P in claim order.
 // Per round every claim is launched first -- the Pi_CCS claim writes its
 // coefficients, the memory claims their values at 0..deg (all of them in one
-// multi-claim fold / eval / reduce), into one device array -- then a single
-// copy and sync bring the round back; Twist address-lane claims (and memory
-// claims whose tables are exhausted) take the per-claim path.
+// multi-claim fold and eval), the Twist address-lane claims theirs at 0, 1,
+// 2, into one device array -- then a single copy and sync bring the round
+// back; claims whose tables are exhausted take the per-claim path.
 static int run_batched_ds(neo_gpu_shard* sh, const char* domain, uint64_t inst_idx, std::vector<Claim>& cl,
                           uint32_t rounds, std::vector<K>& chals, std::vector<K>& finals, std::vector<uint64_t>& P,
                           BatchRec* rec = nullptr) {
@@ -849,6 +850,11 @@ static int run_batched_ds(neo_gpu_shard* sh, const char* domain, uint64_t inst_i
                 mos.push_back(cl[i].mem);
                 mdst.push_back(slot);
                 kind[i] = 2;
+            } else if (cl[i].ta && cl[i].deg == 2) {
+                bool launched = false;
+                int rc = ta_round_launch(cl[i].ta, slot, &launched);
+                if (rc) return rc;
+                if (launched) kind[i] = 2;  // values at 0, 1, 2 in the slot
             }
         }
         for (size_t i0 = 0; i0 < mos.size(); i0 += 24) {

@@ -188,6 +188,8 @@ int dev_ccs_upload(neo_gpu_ctx* ctx, const neo_ccs_desc* desc, DevCcs& out);
 
 // Kernels callable from several translation units.
 int launch_chi_table(neo_gpu_ctx* ctx, const gl::K* d_bits, uint32_t nbits, gl::K* d_out);
+// chi(bits[j+1..nbits)) for every j < nbits, table j at 2^nbits - 2^(nbits-j), in one launch
+int launch_suffix_chi_tables(neo_gpu_ctx* ctx, const gl::K* d_bits, uint32_t nbits, gl::K* d_out);
 int launch_me_y(neo_gpu_ctx* ctx, const DevCcs& ccs, const int8_t* d_Z, uint32_t n_w, uint64_t m,
                 const gl::K* d_chi, uint32_t ell_n, uint32_t b, gl::K* d_vj_scratch, gl::K* d_y,
                 gl::K* d_ysc);

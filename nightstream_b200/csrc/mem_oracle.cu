@@ -20,6 +20,7 @@
 // requested points on the host. fold(r) is one pass over every factor.
 // All arithmetic is exact in F_q / K, so values equal the reference's.
 #include "internal.cuh"
+#include <algorithm>
 
 using gl::K;
 
@@ -40,9 +41,10 @@ __device__ __forceinline__ K eq_bit_affine(K bit, K u) {
     return gl::kadd(gl::kmul(bit, gl::ksub(gl::kdbl(u), gl::kone())), gl::ksub(gl::kone(), u));
 }
 
-__global__ void eqbit_kernel(K* __restrict__ col, uint64_t len, K u) {
-    uint64_t t = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
-    if (t < len) col[t] = eq_bit_affine(col[t], u);
+// columns b < A of [A][len], in place: col_b[t] = eq_bit_affine(col_b[t], u_b)
+__global__ void eqbit_kernel(K* __restrict__ cols, uint64_t len, uint32_t A, const K* __restrict__ u) {
+    const uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+    if (i < len * A) cols[i] = eq_bit_affine(cols[i], u[i / len]);
 }
 
 // inc_terms(t) = has_write(t)·inc(t)·Π_b eq_bit_affine(wa_b(t), r_addr_b)
@@ -312,12 +314,13 @@ __global__ void __launch_bounds__(256) dot_kernel(const K* __restrict__ a, const
     }
 }
 
-// ---- all memory claims of one sum-check round in three launches ----------
+// ---- all memory claims of one sum-check round in two launches ------------
 // A batched round (the Route-A time claims, the val-eval batch, the address
 // pre-time batches) evaluates every claim's round polynomial at x = 0..deg
-// before the transcript draws the next challenge.  These kernels fold, evaluate
-// and reduce the tables of up to MULTI_MAX claims together; the values land in
-// one device array that the host reads with a single copy.
+// before the transcript draws the next challenge.  These kernels fold, then
+// evaluate and reduce (each claim's last block sums its partials) the tables
+// of up to MULTI_MAX claims together; the values land in one device array
+// that the host reads with a single copy.
 constexpr int MULTI_MAX = 24;
 constexpr int MX = 8;  // evaluation points per pass (thread-local accumulators)
 
@@ -331,10 +334,13 @@ struct MultiClaim {
     K r;               // fold challenge
     uint32_t blk0;     // first block of this claim
     uint32_t part0;    // first partial [npts][nblk]
-    uint32_t nblk;     // blocks of 256 pairs
+    uint32_t nblk;     // partial columns per point: pair blocks of 256 pairs x column chunks
     uint32_t ppt;      // evaluation points per thread (1, 2, 4 or MX): blocks = ceil(npts / ppt) * nblk
-    K* out;            // values at x = 0..npts-1 (reduce kernel)
+    uint32_t nchunk;   // bitness: column chunks of BIT_CHUNK columns (1 otherwise)
+    K* out;            // values at x = 0..npts-1
+    unsigned int* ticket;  // the claim's block counter (zero between launches)
 };
+constexpr uint32_t BIT_CHUNK = 4;  // bitness columns per thread
 
 struct MultiArgs {
     int n;
@@ -361,15 +367,23 @@ __global__ void __launch_bounds__(256) mem_multi_fold_kernel(const __grid_consta
 }
 
 // Values of one pair at x = x0 .. x0 + PPT - 1: the product of the claim's
-// affine factors (or the gated bitness sum), additions along x.
+// affine factors (a factor zero on both children zeroes every point), or for
+// a bitness claim chi(x) times the weighted b(b - 1) sum over the columns of
+// chunk ch, additions along x.
 template <int PPT>
-__device__ __forceinline__ void multi_eval_points(const MultiClaim& c, uint64_t p, uint32_t x0, K* acc) {
-#pragma unroll
-    for (int i = 0; i < PPT; i++) acc[i] = c.bitness ? gl::kzero() : gl::kone();
+__device__ __forceinline__ void multi_eval_points(const MultiClaim& c, uint64_t p, uint32_t x0, uint32_t ch, K* acc) {
     if (!c.bitness) {
+#pragma unroll
+        for (int i = 0; i < PPT; i++) acc[i] = gl::kone();
         for (uint32_t f = 0; f < c.nf; f++) {
             const K* s = c.tab + (uint64_t)f * c.len + 2 * p;
-            const K f0 = s[0], d = gl::ksub(s[1], f0);
+            const K f0 = s[0], f1 = s[1];
+            if (gl::kiszero(f0) && gl::kiszero(f1)) {
+#pragma unroll
+                for (int i = 0; i < PPT; i++) acc[i] = gl::kzero();
+                return;
+            }
+            const K d = gl::ksub(f1, f0);
             K v = gl::kadd(f0, gl::kscale_small(d, (int32_t)x0));
 #pragma unroll
             for (int i = 0; i < PPT; i++) {
@@ -379,17 +393,35 @@ __device__ __forceinline__ void multi_eval_points(const MultiClaim& c, uint64_t 
         }
         return;
     }
-    for (uint32_t f = 1; f < c.nf; f++) {
-        const K* s = c.tab + (uint64_t)f * c.len + 2 * p;
-        if (gl::kiszero(s[0]) && gl::kiszero(s[1])) continue;  // b(b - 1) = 0 at every x
-        const K f0 = s[0], d = gl::ksub(s[1], f0), w = c.w[f - 1];
-        K v = gl::kadd(f0, gl::kscale_small(d, (int32_t)x0));
+#pragma unroll
+    for (int i = 0; i < PPT; i++) acc[i] = gl::kzero();
+    const uint32_t f_lo = 1 + ch * BIT_CHUNK, f_hi = min(c.nf, f_lo + BIT_CHUNK);
+    // the chunk's column pairs are loaded together (one memory round trip)
+    K b0[BIT_CHUNK], b1[BIT_CHUNK];
+#pragma unroll
+    for (uint32_t u = 0; u < BIT_CHUNK; u++) {
+        if (f_lo + u < f_hi) {
+            const K* s = c.tab + (uint64_t)(f_lo + u) * c.len + 2 * p;
+            b0[u] = s[0];
+            b1[u] = s[1];
+        } else {
+            b0[u] = b1[u] = gl::kzero();
+        }
+    }
+    bool any = false;
+#pragma unroll
+    for (uint32_t u = 0; u < BIT_CHUNK; u++) {
+        if (gl::kiszero(b0[u]) && gl::kiszero(b1[u])) continue;  // b(b - 1) = 0 at every x
+        any = true;
+        const K d = gl::ksub(b1[u], b0[u]), w = c.w[f_lo + u - 1];
+        K v = gl::kadd(b0[u], gl::kscale_small(d, (int32_t)x0));
 #pragma unroll
         for (int i = 0; i < PPT; i++) {
             acc[i] = gl::kadd(acc[i], gl::kmul(w, gl::kmul(v, gl::ksub(v, gl::kone()))));
             v = gl::kadd(v, d);
         }
     }
+    if (!any) return;
     const K* s = c.tab + 2 * p;
     const K f0 = s[0], d = gl::ksub(s[1], f0);
     K v = gl::kadd(f0, gl::kscale_small(d, (int32_t)x0));
@@ -400,84 +432,95 @@ __device__ __forceinline__ void multi_eval_points(const MultiClaim& c, uint64_t 
     }
 }
 
-// Block (point group g, pair block pb) of one claim: thread t takes pair
-// pb * 256 + t at the claim's ppt points x0 = g * ppt ..; each point is
-// reduced over the block into partials[x][pb].  A claim with many pairs
-// takes MX points per thread (its factor pairs read once per MX points); one
-// with few pairs (the late rounds) takes fewer, so that its point groups run
-// side by side instead of one thread walking every point.
+// Block (point group g, partial column r) of one claim: r = ch * (pair
+// blocks) + pair block pb; thread t takes pair pb * 256 + t (bitness: its
+// column chunk ch) at the claim's ppt points x0 = g * ppt ..; each point is
+// reduced over the block into partials[x][r].  A claim with many pairs takes
+// MX points per thread (its factor pairs read once per MX points); one with
+// few pairs (the late rounds) takes fewer, so that its point groups run side
+// by side instead of one thread walking every point.
 __global__ void __launch_bounds__(256) mem_multi_eval_kernel(const __grid_constant__ MultiArgs a) {
     __shared__ K s_red[256 / 32][MX];
     const int ci = multi_claim_of(a, blockIdx.x);
     const MultiClaim& c = a.c[ci];
     const uint32_t b = blockIdx.x - c.blk0;
-    const uint32_t g = b / c.nblk, pb = b % c.nblk;
+    const uint32_t g = b / c.nblk, pb = b % c.nblk;  // pb: the partial column
+    const uint32_t nbp = c.nblk / c.nchunk;          // pair blocks
+    const uint32_t ch = pb / nbp;
     const uint32_t x0 = g * c.ppt;
     const uint32_t np = min(c.ppt, c.npts - x0);
     const uint64_t pairs = c.len >> 1;
-    const uint64_t p = (uint64_t)pb * 256 + threadIdx.x;
+    const uint64_t p = (uint64_t)(pb % nbp) * 256 + threadIdx.x;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    // a pair whose gate factor (the first, or every bitness column) is zero on
-    // both children contributes nothing at any x
+    // a product whose gate factor (factor 1: has_lookup / has_read /
+    // has_write behind chi; factor 0 where no chi leads) is zero on both
+    // children contributes nothing at any x
     bool live = p < pairs;
     if (live && !c.bitness) {
-        const K* s = c.tab + 2 * p;
-        live = !(gl::kiszero(s[0]) && gl::kiszero(s[1]));
+        const K* s0 = c.tab + 2 * p;
+        const K* s1 = c.tab + (c.nf > 1 ? c.len : 0) + 2 * p;
+        live = !(gl::kiszero(s0[0]) && gl::kiszero(s0[1])) && !(gl::kiszero(s1[0]) && gl::kiszero(s1[1]));
     }
     K acc[MX];
 #pragma unroll
     for (int i = 0; i < MX; i++) acc[i] = gl::kzero();
     if (live) {
         switch (c.ppt) {
-            case 1: multi_eval_points<1>(c, p, x0, acc); break;
-            case 2: multi_eval_points<2>(c, p, x0, acc); break;
-            case 4: multi_eval_points<4>(c, p, x0, acc); break;
-            default: multi_eval_points<MX>(c, p, x0, acc); break;
+            case 1: multi_eval_points<1>(c, p, x0, ch, acc); break;
+            case 2: multi_eval_points<2>(c, p, x0, ch, acc); break;
+            case 4: multi_eval_points<4>(c, p, x0, ch, acc); break;
+            default: multi_eval_points<MX>(c, p, x0, ch, acc); break;
         }
     }
     const bool any = __syncthreads_or(live);
     if (!any) {
         if (threadIdx.x < np) a.partials[c.part0 + (uint64_t)(x0 + threadIdx.x) * c.nblk + pb] = gl::kzero();
-        return;
-    }
+    } else {
 #pragma unroll
-    for (int i = 0; i < MX; i++) {
-        if ((uint32_t)i >= np) break;
-        K v = acc[i];
+        for (int i = 0; i < MX; i++) {
+            if ((uint32_t)i >= np) break;
+            K v = acc[i];
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) v = gl::kadd(v, shfl_xor_km(v, o));
+            if (lane == 0) s_red[warp][i] = v;
+        }
+        __syncthreads();
+        if (threadIdx.x < np) {
+            K v = gl::kzero();
+#pragma unroll
+            for (int w = 0; w < 256 / 32; w++) v = gl::kadd(v, s_red[w][threadIdx.x]);
+            a.partials[c.part0 + (uint64_t)(x0 + threadIdx.x) * c.nblk + pb] = v;
+        }
+    }
+    // the claim's last block to finish sums its partials (ticket, no waits)
+    __threadfence();
+    __syncthreads();
+    __shared__ unsigned int s_last;
+    const uint32_t claim_blocks = c.nblk * ((c.npts + c.ppt - 1) / c.ppt);
+    if (threadIdx.x == 0) s_last = atomicInc(c.ticket, claim_blocks - 1) == claim_blocks - 1;
+    __syncthreads();
+    if (!s_last) return;
+    __threadfence();
+    for (uint32_t x = 0; x < c.npts; x++) {
+        K v = gl::kzero();
+        for (uint32_t r = threadIdx.x; r < c.nblk; r += 256) {
+            const ulonglong2 u = __ldcg(reinterpret_cast<const ulonglong2*>(a.partials + c.part0 + (uint64_t)x * c.nblk + r));
+            v = gl::kadd(v, gl::kmk(u.x, u.y));
+        }
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) v = gl::kadd(v, shfl_xor_km(v, o));
-        if (lane == 0) s_red[warp][i] = v;
-    }
-    __syncthreads();
-    if (threadIdx.x < np) {
-        K v = gl::kzero();
+        if (lane == 0) s_red[warp][0] = v;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            K t = gl::kzero();
 #pragma unroll
-        for (int w = 0; w < 256 / 32; w++) v = gl::kadd(v, s_red[w][threadIdx.x]);
-        a.partials[c.part0 + (uint64_t)(x0 + threadIdx.x) * c.nblk + pb] = v;
+            for (int w = 0; w < 256 / 32; w++) t = gl::kadd(t, s_red[w][0]);
+            c.out[x] = t;
+        }
+        __syncthreads();
     }
 }
 
-// out[x] = sum of the claim's block partials at x; one block per (claim, x)
-__global__ void __launch_bounds__(256) mem_multi_reduce_kernel(const __grid_constant__ MultiArgs a) {
-    __shared__ K s_red[8];
-    uint32_t rest = blockIdx.x;
-    int ci = 0;
-    while (rest >= a.c[ci].npts) { rest -= a.c[ci].npts; ci++; }
-    const MultiClaim& c = a.c[ci];
-    const uint32_t x = rest;
-    K v = gl::kzero();
-    for (uint32_t b = threadIdx.x; b < c.nblk; b += 256) v = gl::kadd(v, a.partials[c.part0 + (uint64_t)x * c.nblk + b]);
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) v = gl::kadd(v, shfl_xor_km(v, o));
-    if (lane == 0) s_red[warp] = v;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        K t = gl::kzero();
-        for (int w = 0; w < 8; w++) t = gl::kadd(t, s_red[w]);
-        c.out[x] = t;
-    }
-}
 
 inline K kload_h(const uint64_t* p) { return gl::kmk(p[0], p[1]); }
 
@@ -669,11 +712,12 @@ int mem_create(neo_gpu_ctx* ctx, int kind, uint32_t ell, const uint64_t* r_point
             return fail(ctx->fail(NEO_ERR_OOM, "mem_oracle: r_addr"));
     }
     auto eqbits = [&](uint32_t f0, uint32_t c0) -> int {
-        for (uint32_t b = 0; b < A; b++) {
+        if (!A) return NEO_OK;
+        if (!r_addr) return ctx->fail(NEO_ERR_ARG, "mem_oracle: address bits without r_addr");
+        for (uint32_t b = 0; b < A; b++)
             if (put(f0 + b, c0 + b)) return ctx->fail(NEO_ERR_CUDA, "mem_oracle: column upload");
-            eqbit_kernel<<<ceil_div(L, 256), 256, 0, S>>>(T + (size_t)(f0 + b) * L, L, kload_h(r_addr + 2 * b));
-            NEO_LAUNCHED(ctx);
-        }
+        eqbit_kernel<<<ceil_div(L * A, 256), 256, 0, S>>>(T + (size_t)f0 * L, L, A, dra.p);  // all A columns at once
+        NEO_LAUNCHED(ctx);
         return NEO_OK;
     };
     int rc = NEO_OK;
@@ -773,7 +817,7 @@ bool mem_round_multi_ok(const neo_gpu_mem_oracle* o) {
 }
 
 // The next round of n oracles: pending folds, then the values at x = 0..deg
-// of oracle i into d_out[i] (device), in three launches and without a host
+// of oracle i into d_out[i] (device), in two launches and without a host
 // sync.  Every oracle must satisfy mem_round_multi_ok; n <= MULTI_MAX.
 int mem_round_launch_multi(neo_gpu_ctx* ctx, neo_gpu_mem_oracle* const* os, int n, K* const* d_out,
                            DevBuf<K>& partials) {
@@ -810,7 +854,6 @@ int mem_round_launch_multi(neo_gpu_ctx* ctx, neo_gpu_mem_oracle* const* os, int 
     a.n = n;
     blocks = 0;
     uint64_t parts = 0;
-    uint32_t pts = 0;
     for (int i = 0; i < n; i++) {
         neo_gpu_mem_oracle* o = os[i];
         if (o->len < 2) return ctx->fail(NEO_ERR_INVARIANT, "mem_round_launch_multi: no pairs left");
@@ -822,23 +865,35 @@ int mem_round_launch_multi(neo_gpu_ctx* ctx, neo_gpu_mem_oracle* const* os, int 
         c.bitness = o->bitness;
         c.w = o->w.p;
         c.blk0 = blocks;
-        c.nblk = (uint32_t)ceil_div(o->len >> 1, 256);
+        c.nchunk = o->bitness ? std::max<uint32_t>(1, (uint32_t)ceil_div(o->nf - 1, BIT_CHUNK)) : 1;
+        c.nblk = (uint32_t)ceil_div(o->len >> 1, 256) * c.nchunk;
         // points per thread: MX while the pairs fill the GPU, fewer for the
-        // small tables of the late rounds (their point groups run in parallel)
+        // small tables of the late rounds (their point groups run in parallel),
+        // never more than the claim's points rounded up to a power of two
         const uint64_t pairs = o->len >> 1;
-        c.ppt = pairs >= 8192 ? MX : (pairs >= 1024 ? 4 : (pairs >= 256 ? 2 : 1));
+        uint32_t ppt = pairs >= 8192 ? MX : (pairs >= 1024 ? 4 : (pairs >= 256 ? 2 : 1));
+        while (ppt > 1 && ppt / 2 >= c.npts) ppt /= 2;
+        c.ppt = ppt;
         c.part0 = (uint32_t)parts;
         c.out = d_out[i];
         blocks += c.nblk * (uint32_t)ceil_div(c.npts, c.ppt);
         parts += (uint64_t)c.npts * c.nblk;
-        pts += c.npts;
     }
     if (parts > 0xFFFFFFFFull) return ctx->fail(NEO_ERR_UNSUPPORTED, "mem_round_launch_multi: too many partials");
-    NEO_CK(ctx, partials.ensure(parts));
+    // the claims' tickets sit behind the partials (MULTI_MAX counters in
+    // MULTI_TICKET_K entries); they return to zero after every launch, so
+    // they are cleared only when the buffer is (re)allocated
+    constexpr size_t MULTI_TICKET_K = (MULTI_MAX * sizeof(unsigned int) + sizeof(K) - 1) / sizeof(K);
+    const K* before = partials.p;
+    const size_t cap_before = partials.cap;
+    NEO_CK(ctx, partials.ensure(std::max<uint64_t>(parts, cap_before > MULTI_TICKET_K ? cap_before - MULTI_TICKET_K : 0) +
+                                MULTI_TICKET_K));
+    unsigned int* tickets = reinterpret_cast<unsigned int*>(partials.p + (partials.cap - MULTI_TICKET_K));
+    if (partials.p != before || partials.cap != cap_before)
+        NEO_CK(ctx, cudaMemsetAsync(tickets, 0, MULTI_TICKET_K * sizeof(K), ctx->stream));
+    for (int i = 0; i < n; i++) a.c[i].ticket = tickets + i;
     a.partials = partials.p;
     mem_multi_eval_kernel<<<blocks, 256, 0, ctx->stream>>>(a);
-    NEO_LAUNCHED(ctx);
-    mem_multi_reduce_kernel<<<pts, 256, 0, ctx->stream>>>(a);
     NEO_LAUNCHED(ctx);
     return NEO_OK;
 }
@@ -1246,15 +1301,19 @@ int ta_apply_fold(neo_gpu_twist_addr* o) {
     return NEO_OK;
 }
 
-int ta_values(neo_gpu_twist_addr* o) {
+// The round's values at x = 0, 1, 2 into d_dst (device), without a host sync
+// (the pending fold applied first); no events: zeros.
+int ta_values_launch(neo_gpu_twist_addr* o, K* d_dst) {
     neo_gpu_ctx* ctx = o->ctx;
     cudaStream_t S = ctx->stream;
     if (o->pending) {
         int rc = ta_apply_fold(o);
         if (rc) return rc;
     }
-    o->hvals.assign(3, gl::kzero());
-    if (o->E == 0) return NEO_OK;
+    if (o->E == 0) {
+        NEO_CK(ctx, cudaMemsetAsync(d_dst, 0, 3 * sizeof(K), S));
+        return NEO_OK;
+    }
     ta_prep_kernel<<<ceil_div(o->E, 256), 256, 0, S>>>(o->hw.p, o->inc.p, o->wa.p, o->wpw.p, o->E, o->bit, o->wkey.p,
                                                      o->wdelta.p);
     NEO_LAUNCHED(ctx);
@@ -1272,8 +1331,15 @@ int ta_values(neo_gpu_twist_addr* o) {
     a.partials = o->partials.p;
     ta_eval_kernel<<<dim3(nbx, nbx), TA_T, 0, S>>>(a);
     NEO_LAUNCHED(ctx);
-    mem_reduce_kernel<<<3, 256, 0, S>>>(o->partials.p, nb, o->vals.p);
+    mem_reduce_kernel<<<3, 256, 0, S>>>(o->partials.p, nb, d_dst);
     NEO_LAUNCHED(ctx);
+    return NEO_OK;
+}
+
+int ta_values(neo_gpu_twist_addr* o) {
+    neo_gpu_ctx* ctx = o->ctx;
+    o->hvals.assign(3, gl::kzero());
+    if (int rc = ta_values_launch(o, o->vals.p)) return rc;
     NEO_CK(ctx, ctx_d2h(ctx, o->hvals.data(), o->vals.p, 3 * sizeof(K)));
     NEO_CK(ctx, ctx_sync(ctx));
     return NEO_OK;
@@ -1402,6 +1468,18 @@ extern "C" int neo_gpu_twist_addr_create_device(neo_gpu_ctx* ctx, int kind, uint
                                                 uint32_t ell_addr, uint64_t n_init, const uint64_t* init_addr,
                                                 const uint64_t* init_val, const uint64_t* d_cols,
                                                 neo_gpu_twist_addr** out) { NEO_ABI_GUARD(neo_gpu_twist_addr_create_device_impl_abi(ctx, kind, ell, r_cycle, ell_addr, n_init, init_addr, init_val, d_cols, out)) }
+
+// The next round of a Twist address-lane oracle into d_dst[0..3) (device),
+// without a host sync; false (nothing launched) once every address bit is
+// bound, when the value no longer depends on x.
+int ta_round_launch(neo_gpu_twist_addr* o, K* d_dst, bool* launched) {
+    *launched = false;
+    if (o->bit + (o->pending ? 1 : 0) >= o->A) return NEO_OK;
+    cudaSetDevice(o->ctx->device);
+    if (int rc = ta_values_launch(o, d_dst)) return rc;
+    *launched = true;
+    return NEO_OK;
+}
 
 static int neo_gpu_twist_addr_evals_impl_abi(neo_gpu_twist_addr* o, const uint64_t* xs, uint32_t nx, uint64_t* ys) {
     if (!o) return NEO_ERR_ARG;
