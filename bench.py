@@ -170,14 +170,21 @@ class Clocks:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
-# DRAM bytes (read + write) of one 12-plane commit_tc launch per witness column,
-# from an ncu capture at m = 2^14 (166.56 MB / 16384); the tiles scale with m.
-COMMIT_TRAFFIC_PER_M = 166.56e6 / 16384
+# DRAM bytes (read + write) of one 12-plane commit_p8_kernel<4> launch per
+# witness column, from an ncu capture at m = 2^14 (182.1 MB / 16384: the PP
+# limb tiles once plus the window sequences once); the tiles scale with m.
+COMMIT_TRAFFIC_PER_M = 182.1e6 / 16384
 
 
-# DRAM bytes (read + write) of the 16 row-round launches of one k = 13 step,
-# per row, from an ncu capture at 2^16 rows (347.2 MB / 65536).
-ROUNDS_TRAFFIC_PER_ROW = 347.22e6 / 65536
+# DRAM bytes (read + write) of the 18 launches of one 16-round Pi_CCS sequence
+# (k = 13), per row, from an ncu capture at 2^16 rows (248.5 MB / 65536).
+ROUNDS_TRAFFIC_PER_ROW = 248.5e6 / 65536
+
+# Integer-ALU ceiling of the sequence's largest launch (round 3, the cross
+# terms), from ncu --set full at 2^16 rows, k = 13: ALU pipe and issue-slot
+# utilisation.
+ROUNDS_ALU = {"kernel": "ccs_fast_round_kernel<3,0> (round 3)", "alu_pipe_frac": 0.669, "issue_active_frac": 0.579,
+              "source": "ncu --set full -k regex:ccs_fast_round_kernel -s 3 -c 1 on bench.py --mode rounds --ell 16"}
 
 
 def measured_peaks():
@@ -236,16 +243,18 @@ def rounds_roofline(ctx, ccs, z, ell, stream, reps=3):
     if not peak:
         peak, src = 6650.0, "fallback 6.65 TB/s"
     achieved = B / (ms * 1e-3) / 1e9
-    return {"kernel": f"Pi_CCS time rounds: ccs_round_kernel<0..5> + reduce_eval_kernel, {ell} rounds, k = {k}, "
-                      f"{launches} launches per sequence",
+    return {"kernel": f"Pi_CCS time rounds, ternary-digit path: ccs_hist_kernel + ccs_hist_sum_kernel + "
+                      f"ccs_fast_round_kernel<MODE>, {ell} rounds, k = {k}, {launches} launches per sequence",
             "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
             "traffic": ROUNDS_TRAFFIC_PER_ROW * m,
-            "traffic_source": "ncu dram__bytes_read+write of the 16 row-round launches of one k = 13 step at "
-                              "2^16 rows (ncu -k regex:ccs_ on bench.py --steps 1 --warmup 1), per row",
+            "traffic_source": "ncu dram__bytes_read+write of the 18 launches of one sequence at 2^16 rows, "
+                              "k = 13 (ncu --cache-control none -k regex:ccs_ on bench.py --mode rounds --ell 16), "
+                              "per row",
+            "alu": ROUNDS_ALU,
             "launch_ms": ms / ell, "sequence_ms": ms, "peak_source": src,
             "algorithmic_bytes_per_sequence": B,
-            "note": "integer-ALU bound: the rounds stream int8 digit planes in rounds 0..4 and move far fewer "
-                    "bytes than B_ccs"}
+            "note": "integer-ALU bound (alu): rounds 0..4 read int8 digit planes and the whole sequence moves "
+                    "0.16x B_ccs"}
 
 
 def commit_roofline(ctx, m, stream, n_vec=12, reps=5):
