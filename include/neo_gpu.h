@@ -406,6 +406,49 @@ int neo_gpu_shard_fold_step(neo_gpu_shard* sh, const uint64_t* z, uint64_t* proo
 int neo_gpu_shard_step_proof(neo_gpu_shard* sh, uint64_t* out, uint64_t cap, uint64_t* len);
 /* Same step with the witness already resident in device memory (d_z). */
 int neo_gpu_shard_fold_step_device(neo_gpu_shard* sh, const uint64_t* d_z, uint64_t* proof_len);
+
+/* The memory events of one chunk of a VM trace, per step j < steps: Shout
+ * instance i (in neo_mem_desc order) looked up key[j] with value val[j] when
+ * has_lookup[j] = 1; Twist instance i read rv[j] at ra[j] (has_read[j] = 1) and
+ * wrote wv[j] at wa[j] (has_write[j] = 1).  Flags are 0 or 1; addresses and
+ * values of inactive ports are ignored. */
+typedef struct neo_shout_events {
+    const uint8_t* has_lookup;
+    const uint64_t* key;
+    const uint64_t* val;
+} neo_shout_events;
+typedef struct neo_twist_events {
+    const uint8_t* has_read;
+    const uint64_t* ra;
+    const uint64_t* rv;
+    const uint8_t* has_write;
+    const uint64_t* wa;
+    const uint64_t* wv;
+} neo_twist_events;
+typedef struct neo_trace_chunk {
+    uint64_t steps;                 /* <= the shard's steps per fold step (and <= 16384) */
+    const neo_shout_events* shout;  /* one per Shout instance */
+    const neo_twist_events* twist;  /* one per Twist instance */
+} neo_trace_chunk;
+/* One fold step built from a trace chunk on the device (the witness build of
+ * R1csCpu::build_ccs_chunks with the shared CPU bus,
+ * crates/neo-memory/src/cpu/r1cs_adapter.rs:372-650): z = z_cpu (the CPU
+ * witness, z_cpu_len <= the bus base words) padded with zeros, the bus tail
+ * written from the events (address bits least-significant first, flags,
+ * values; bus cell (col, j) at bus_base + col*steps + j,
+ * crates/neo-memory/src/cpu/bus_layout.rs:59-81), and each Twist write's
+ * increment inc = wv - (the value at wa before the write) from a memory
+ * state the shard keeps in device memory across chunks; then the step
+ * proceeds as neo_gpu_shard_fold_step.  The step's Twist MemInit is that
+ * state at the chunk's start (mem_init_from_state_map,
+ * crates/neo-memory/src/mem_init.rs:65-90): after a successful step the
+ * shard sets the next step's MemInit from it, so no
+ * neo_gpu_shard_set_twist_init is needed between trace steps (one given
+ * replaces the state).  An address >= 2^ell_addr, a flag other than 0 / 1 or
+ * too many steps is NEO_ERR_ARG. */
+int neo_gpu_shard_fold_step_trace(neo_gpu_shard* sh, const uint64_t* z_cpu, uint64_t z_cpu_len,
+                                  const neo_trace_chunk* trace, uint64_t* proof, uint64_t proof_cap,
+                                  uint64_t* proof_len);
 /* Transcript sponge state (8 words) and CCS matrix digest (4 words). */
 int neo_gpu_shard_transcript_state(const neo_gpu_shard* sh, uint64_t* st8);
 int neo_gpu_shard_ccs_digest(const neo_gpu_shard* sh, uint64_t* d4);

@@ -67,6 +67,10 @@ struct TwistInst {
     std::vector<uint64_t> init_addr, init_val;  // MemInit::Sparse (empty: MemInit::Zero)
     uint8_t digest[32] = {0};
     uint32_t col0 = 0;  // ra col0.., wa col0+ea.., has_read +2ea, has_write +2ea+1, wv +2, rv +3, inc +4
+    // trace steps (neo_gpu_shard_fold_step_trace): the memory, dense over
+    // 2^ea cells in device memory, at the start of the next chunk
+    DevBuf<uint64_t> d_state;
+    bool state_valid = false;
 };
 
 static std::vector<uint8_t> le64(uint64_t v) {
@@ -269,6 +273,8 @@ struct neo_gpu_shard {
     // the multi-claim memory kernels
     DevBuf<K> d_round, d_mpart;
     HostBuf<K> h_round;
+    DevBuf<uint64_t> d_events;  // a trace chunk's packed events (neo_gpu_shard_fold_step_trace)
+    HostBuf<uint64_t> h_events;
     StepRecord rec;  // the last step, for neo_gpu_shard_step_proof
     uint32_t kappa = 16;
     uint32_t n = 0, m32 = 0, t = 0, ell_n = 0, ell_d = 6, d_sc = 6, k_rho = 12, b = 2, m_in = 1, lambda = 127;
@@ -1862,6 +1868,245 @@ static int neo_gpu_shard_fold_step_device_impl_abi(neo_gpu_shard* sh, const uint
 extern "C" int neo_gpu_shard_fold_step_device(neo_gpu_shard* sh, const uint64_t* d_z, uint64_t* proof_len) { NEO_ABI_GUARD(neo_gpu_shard_fold_step_device_impl_abi(sh, d_z, proof_len)) }
 
 // ---------------------------------------------------------------------------
+// Trace chunk -> witness on the device (R1csCpu::build_ccs_chunks with the
+// shared CPU bus, crates/neo-memory/src/cpu/r1cs_adapter.rs:372-650).
+// Events arrive packed, per step j < S: Shout instance i at 3 S i words
+// [has_lookup | key | val], then Twist instance i at 3 S n_shout + 6 S i
+// [has_read | ra | rv | has_write | wa | wv].
+namespace {
+
+constexpr uint32_t TRACE_MAX_STEPS = 16384;  // the increment sort's keys fit shared memory
+constexpr int TRACE_J_BITS = 15;
+
+__global__ void trace_state_init_kernel(uint64_t* __restrict__ state, uint64_t n, const uint64_t* __restrict__ addr,
+                                        const uint64_t* __restrict__ val) {
+    const uint64_t e = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+    if (e < n) state[addr[e]] = val[e];
+}
+
+// Shout bus cells of step j: address bits (least significant first), has_lookup, val
+__global__ void trace_shout_bus_kernel(uint64_t* __restrict__ z, uint64_t bus_base, uint64_t cap, uint64_t S,
+                                       uint32_t col0, uint32_t ea, const uint64_t* __restrict__ ev) {
+    const uint64_t j = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+    if (j >= S || !ev[j]) return;
+    const uint64_t key = ev[S + j];
+    for (uint32_t b = 0; b < ea; b++) z[bus_base + (uint64_t)(col0 + b) * cap + j] = (key >> b) & 1;
+    z[bus_base + (uint64_t)(col0 + ea) * cap + j] = 1;
+    z[bus_base + (uint64_t)(col0 + ea + 1) * cap + j] = gl::canon(ev[2 * S + j]);
+}
+
+// Twist bus cells of step j: ra bits, wa bits, has_read, has_write, wv, rv
+// (the increment comes from trace_twist_inc_kernel)
+__global__ void trace_twist_bus_kernel(uint64_t* __restrict__ z, uint64_t bus_base, uint64_t cap, uint64_t S,
+                                       uint32_t col0, uint32_t ea, const uint64_t* __restrict__ ev) {
+    const uint64_t j = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+    if (j >= S) return;
+    auto cell = [&](uint32_t col) -> uint64_t& { return z[bus_base + (uint64_t)col * cap + j]; };
+    if (ev[j]) {
+        const uint64_t ra = ev[S + j];
+        for (uint32_t b = 0; b < ea; b++) cell(col0 + b) = (ra >> b) & 1;
+        cell(col0 + 2 * ea) = 1;
+        cell(col0 + 2 * ea + 3) = gl::canon(ev[2 * S + j]);
+    }
+    if (ev[3 * S + j]) {
+        const uint64_t wa = ev[4 * S + j];
+        for (uint32_t b = 0; b < ea; b++) cell(col0 + ea + b) = (wa >> b) & 1;
+        cell(col0 + 2 * ea + 1) = 1;
+        cell(col0 + 2 * ea + 2) = gl::canon(ev[5 * S + j]);
+    }
+}
+
+// inc_at_write_addr of every write of one Twist instance and the memory after
+// the chunk (one block): the writes sorted by (address, step) in shared
+// memory; a write's previous value is the write before it in that order when
+// it has the same address, else the memory at the chunk's start.  All reads
+// of the memory happen before the barrier, the updates (the last write of
+// each address) after it.
+__global__ void __launch_bounds__(1024) trace_twist_inc_kernel(uint64_t* __restrict__ z, uint64_t bus_base,
+                                                               uint64_t cap, uint64_t S, uint32_t n_sort,
+                                                               uint32_t inc_col, const uint64_t* __restrict__ ev,
+                                                               uint64_t* __restrict__ state) {
+    extern __shared__ uint64_t keys[];
+    const uint64_t NONE = ~0ull;
+    const uint64_t* has_w = ev + 3 * S;
+    const uint64_t* wa = ev + 4 * S;
+    const uint64_t* wv = ev + 5 * S;
+    for (uint32_t i = threadIdx.x; i < n_sort; i += blockDim.x)
+        keys[i] = (i < S && has_w[i]) ? (wa[i] << TRACE_J_BITS) | i : NONE;
+    __syncthreads();
+    for (uint32_t k = 2; k <= n_sort; k <<= 1)  // bitonic sort, ascending
+        for (uint32_t h = k >> 1; h > 0; h >>= 1) {
+            for (uint32_t i = threadIdx.x; i < n_sort; i += blockDim.x) {
+                const uint32_t l = i ^ h;
+                if (l > i) {
+                    const uint64_t a = keys[i], b = keys[l];
+                    if ((a > b) == ((i & k) == 0)) {
+                        keys[i] = b;
+                        keys[l] = a;
+                    }
+                }
+            }
+            __syncthreads();
+        }
+    const uint64_t jmask = (1ull << TRACE_J_BITS) - 1;
+    for (uint32_t i = threadIdx.x; i < n_sort; i += blockDim.x) {
+        const uint64_t key = keys[i];
+        if (key == NONE) continue;
+        const uint64_t j = key & jmask, addr = key >> TRACE_J_BITS;
+        const bool same = i > 0 && keys[i - 1] != NONE && (keys[i - 1] >> TRACE_J_BITS) == addr;
+        const uint64_t old = same ? gl::canon(wv[keys[i - 1] & jmask]) : state[addr];
+        z[bus_base + (uint64_t)inc_col * cap + j] = gl::sub(gl::canon(wv[j]), old);
+    }
+    __syncthreads();
+    for (uint32_t i = threadIdx.x; i < n_sort; i += blockDim.x) {
+        const uint64_t key = keys[i];
+        if (key == NONE) continue;
+        const uint64_t addr = key >> TRACE_J_BITS;
+        const bool last = i + 1 == n_sort || keys[i + 1] == NONE || (keys[i + 1] >> TRACE_J_BITS) != addr;
+        if (last) state[addr] = gl::canon(wv[key & jmask]);
+    }
+}
+
+}  // namespace
+
+static int neo_gpu_shard_fold_step_trace_impl_abi(neo_gpu_shard* sh, const uint64_t* z_cpu, uint64_t z_cpu_len,
+                                                  const neo_trace_chunk* trc, uint64_t* proof, uint64_t proof_cap,
+                                                  uint64_t* proof_len) {
+    if (!sh) return NEO_ERR_ARG;
+    neo_gpu_ctx* ctx = sh->ctx;
+    if (!trc || (z_cpu_len && !z_cpu)) return ctx->fail(NEO_ERR_ARG, "fold_step_trace: null argument");
+    if (sh->steps == 0) return ctx->fail(NEO_ERR_ARG, "fold_step_trace: the shard has no memory instances");
+    if (z_cpu_len > sh->bus_base) return ctx->fail(NEO_ERR_ARG, "fold_step_trace: CPU witness overlaps the bus tail");
+    const uint64_t S = trc->steps;
+    if (S > sh->steps || S > TRACE_MAX_STEPS) return ctx->fail(NEO_ERR_ARG, "fold_step_trace: too many steps");
+    const size_t ns = sh->shout.size(), nt = sh->twist.size();
+    if ((ns && !trc->shout) || (nt && !trc->twist)) return ctx->fail(NEO_ERR_ARG, "fold_step_trace: missing events");
+    cudaSetDevice(ctx->device);
+    cudaStream_t st = ctx->stream;
+    // validate and pack the events (the reference's build errors: bad flags,
+    // Twist addresses outside the memory)
+    const size_t words = (3 * ns + 6 * nt) * S;
+    NEO_CK(ctx, sh->h_events.ensure(words ? words : 1));
+    uint64_t* h = sh->h_events.p;
+    auto flag = [](const uint8_t* f, uint64_t j, bool* ok) -> uint64_t {
+        const uint8_t v = f ? f[j] : 0;
+        if (v > 1) *ok = false;
+        return v;
+    };
+    bool ok = true;
+    for (size_t i = 0; i < ns && ok; i++) {
+        const neo_shout_events& e = trc->shout[i];
+        uint64_t* o = h + 3 * S * i;
+        for (uint64_t j = 0; j < S; j++) {
+            o[j] = flag(e.has_lookup, j, &ok);
+            if (o[j] && (!e.key || !e.val)) ok = false;
+            o[S + j] = o[j] && ok ? e.key[j] & ((1ull << sh->shout[i]->ea) - 1) : 0;
+            o[2 * S + j] = o[j] && ok ? e.val[j] : 0;
+        }
+    }
+    for (size_t i = 0; i < nt && ok; i++) {
+        const neo_twist_events& e = trc->twist[i];
+        const uint32_t ea = sh->twist[i]->ea;
+        uint64_t* o = h + 3 * S * ns + 6 * S * i;
+        for (uint64_t j = 0; j < S && ok; j++) {
+            o[j] = flag(e.has_read, j, &ok);
+            o[3 * S + j] = flag(e.has_write, j, &ok);
+            if ((o[j] && (!e.ra || !e.rv)) || (o[3 * S + j] && (!e.wa || !e.wv))) ok = false;
+            if (!ok) break;
+            o[S + j] = o[j] ? e.ra[j] : 0;
+            o[2 * S + j] = o[j] ? e.rv[j] : 0;
+            o[4 * S + j] = o[3 * S + j] ? e.wa[j] : 0;
+            o[5 * S + j] = o[3 * S + j] ? e.wv[j] : 0;
+            if ((o[S + j] >> ea) || (o[4 * S + j] >> ea))
+                return ctx->fail(NEO_ERR_ARG, "fold_step_trace: Twist address outside the memory");
+        }
+    }
+    if (!ok) return ctx->fail(NEO_ERR_ARG, "fold_step_trace: malformed events (flag not 0/1 or null array)");
+    // the memories at the chunk's start, rebuilt from the MemInit when stale
+    for (size_t i = 0; i < nt; i++) {
+        TwistInst& ti = *sh->twist[i];
+        if (ti.state_valid) continue;
+        const uint64_t cells = 1ull << ti.ea;
+        NEO_CK(ctx, ti.d_state.ensure(cells));
+        NEO_CK(ctx, cudaMemsetAsync(ti.d_state.p, 0, cells * 8, st));
+        const uint64_t n = ti.init_addr.size();
+        if (n) {
+            DevBuf<uint64_t> da, dv;
+            NEO_CK(ctx, da.alloc(n));
+            NEO_CK(ctx, dv.alloc(n));
+            NEO_CK(ctx, cudaMemcpyAsync(da.p, ti.init_addr.data(), n * 8, cudaMemcpyHostToDevice, st));
+            NEO_CK(ctx, cudaMemcpyAsync(dv.p, ti.init_val.data(), n * 8, cudaMemcpyHostToDevice, st));
+            trace_state_init_kernel<<<ceil_div(n, 256), 256, 0, st>>>(ti.d_state.p, n, da.p, dv.p);
+            NEO_LAUNCHED(ctx);
+            NEO_CK(ctx, ctx_sync(ctx));  // the staging buffers go out of scope
+        }
+        ti.state_valid = true;
+    }
+    // z = CPU witness, zeros, then the bus tail from the events
+    const uint64_t m = sh->m;
+    NEO_CK(ctx, cudaMemsetAsync(sh->d_z.p, 0, m * 8, st));
+    if (z_cpu_len) NEO_CK(ctx, cudaMemcpyAsync(sh->d_z.p, z_cpu, z_cpu_len * 8, cudaMemcpyHostToDevice, st));
+    if (words) {
+        NEO_CK(ctx, sh->d_events.ensure(words));
+        NEO_CK(ctx, cudaMemcpyAsync(sh->d_events.p, h, words * 8, cudaMemcpyHostToDevice, st));
+    }
+    if (S) {
+        for (size_t i = 0; i < ns; i++) {
+            trace_shout_bus_kernel<<<ceil_div(S, 256), 256, 0, st>>>(sh->d_z.p, sh->bus_base, sh->steps, S,
+                                                                     sh->shout[i]->col0, sh->shout[i]->ea,
+                                                                     sh->d_events.p + 3 * S * i);
+            NEO_LAUNCHED(ctx);
+        }
+        uint32_t n_sort = 1;
+        while (n_sort < S) n_sort <<= 1;
+        static SmemLimit inc_smem;
+        NEO_CK(ctx, inc_smem.at_least(trace_twist_inc_kernel, (size_t)n_sort * 8));
+        for (size_t i = 0; i < nt; i++) {
+            const TwistInst& ti = *sh->twist[i];
+            const uint64_t* ev = sh->d_events.p + 3 * S * ns + 6 * S * i;
+            trace_twist_bus_kernel<<<ceil_div(S, 256), 256, 0, st>>>(sh->d_z.p, sh->bus_base, sh->steps, S, ti.col0,
+                                                                     ti.ea, ev);
+            NEO_LAUNCHED(ctx);
+            trace_twist_inc_kernel<<<1, 1024, (size_t)n_sort * 8, st>>>(sh->d_z.p, sh->bus_base, sh->steps, S, n_sort,
+                                                                       ti.col0 + 2 * ti.ea + 4, ev, ti.d_state.p);
+            NEO_LAUNCHED(ctx);
+        }
+    }
+    int rc = fold_step_impl(sh, nullptr, sh->d_z.p);
+    if (rc) {
+        for (auto& ti : sh->twist) ti->state_valid = false;  // the memory advanced; the MemInit did not
+        return rc;
+    }
+    // the next step's MemInit: the nonzero cells of each memory, by address
+    for (size_t i = 0; i < nt; i++) {
+        TwistInst& ti = *sh->twist[i];
+        const uint64_t cells = 1ull << ti.ea;
+        std::vector<uint64_t> dense(cells), a, v;
+        NEO_CK(ctx, ctx_d2h(ctx, dense.data(), ti.d_state.p, cells * 8));
+        NEO_CK(ctx, ctx_sync(ctx));
+        for (uint64_t c = 0; c < cells; c++)
+            if (dense[c]) {
+                a.push_back(c);
+                v.push_back(dense[c]);
+            }
+        if (!twist_set_init(ti, a.size(), a.data(), v.data()))
+            return ctx->fail(NEO_ERR_INVARIANT, "fold_step_trace: memory state is not a valid MemInit");
+        ti.state_valid = true;
+    }
+    if (proof_len) *proof_len = sh->proof.size();
+    if (proof) {
+        if (proof_cap < sh->proof.size()) return ctx->fail(NEO_ERR_ARG, "fold_step_trace: proof buffer too small");
+        memcpy(proof, sh->proof.data(), sh->proof.size() * 8);
+    }
+    return NEO_OK;
+}
+extern "C" int neo_gpu_shard_fold_step_trace(neo_gpu_shard* sh, const uint64_t* z_cpu, uint64_t z_cpu_len,
+                                             const neo_trace_chunk* trace, uint64_t* proof, uint64_t proof_cap,
+                                             uint64_t* proof_len) {
+    NEO_ABI_GUARD(neo_gpu_shard_fold_step_trace_impl_abi(sh, z_cpu, z_cpu_len, trace, proof, proof_cap, proof_len))
+}
+
+// ---------------------------------------------------------------------------
 // StepProof in struct order (crates/neo-fold/src/shard_proof_types.rs:45-131):
 // a canonical word dump, every Vec prefixed by its length, K = (re, im),
 // F and integers one word, [u8; 32] digests four little-endian words, byte
@@ -2086,6 +2331,7 @@ static int neo_gpu_shard_set_twist_init_impl_abi(neo_gpu_shard* sh, uint32_t mem
     ti.init_addr.swap(tmp.init_addr);
     ti.init_val.swap(tmp.init_val);
     memcpy(ti.digest, tmp.digest, 32);
+    ti.state_valid = false;  // a trace step rebuilds its memory from this MemInit
     return NEO_OK;
 }
 extern "C" int neo_gpu_shard_set_twist_init(neo_gpu_shard* sh, uint32_t mem_idx, uint64_t n_init,
@@ -2302,6 +2548,7 @@ static int neo_gpu_shard_restore_impl_abi(neo_gpu_shard* sh, const uint8_t* buf,
         sh->twist[i]->init_addr.swap(inits[i].init_addr);
         sh->twist[i]->init_val.swap(inits[i].init_val);
         memcpy(sh->twist[i]->digest, inits[i].digest, 32);
+        sh->twist[i]->state_valid = false;
     }
     return NEO_OK;
 }

@@ -67,6 +67,7 @@ SIGNATURES = {
     "neo_gpu_shard_set_twist_init": [P, U32, U64, P, P],
     "neo_gpu_shard_fold_step": [P, P, P, U64, P],
     "neo_gpu_shard_fold_step_device": [P, ctypes.c_void_p, P],
+    "neo_gpu_shard_fold_step_trace": [P, P, U64, P, P, U64, P],
     "neo_gpu_shard_transcript_state": [P, P],
     "neo_gpu_shard_ccs_digest": [P, P],
     "neo_gpu_shard_destroy": [P],
@@ -549,6 +550,19 @@ def _mem_desc(mem: dict) -> MemDesc:
     return md
 
 
+class _ShoutEvents(ctypes.Structure):
+    _fields_ = [("has_lookup", ctypes.c_void_p), ("key", ctypes.c_void_p), ("val", ctypes.c_void_p)]
+
+
+class _TwistEvents(ctypes.Structure):
+    _fields_ = [("has_read", ctypes.c_void_p), ("ra", ctypes.c_void_p), ("rv", ctypes.c_void_p),
+                ("has_write", ctypes.c_void_p), ("wa", ctypes.c_void_p), ("wv", ctypes.c_void_p)]
+
+
+class _TraceChunk(ctypes.Structure):
+    _fields_ = [("steps", ctypes.c_uint64), ("shout", ctypes.c_void_p), ("twist", ctypes.c_void_p)]
+
+
 class Shard:
     """Shard prover with a device-resident accumulator (neo_gpu_shard)."""
 
@@ -577,6 +591,39 @@ class Shard:
             self._cap = 1 << 20
         out = np.empty(self._cap, np.uint64)
         self.ctx.check(self.ctx.lib.neo_gpu_shard_fold_step(self.h, _p(z), _p(out), self._cap, ctypes.byref(n)))
+        return out[: n.value].copy()
+
+    def fold_step_trace(self, z_cpu: np.ndarray, shout=(), twist=()) -> np.ndarray:
+        """One fold step built on the device from a trace chunk
+        (neo_gpu_shard_fold_step_trace): z_cpu the CPU witness (at most the bus
+        base words), shout[i] = (has_lookup, key, val) and twist[i] = (has_read,
+        ra, rv, has_write, wa, wv) per step; returns the step-proof words."""
+        z = _u64(z_cpu)
+        keep = []
+
+        def arr(a, dt):
+            a = np.ascontiguousarray(a, dtype=dt)
+            keep.append(a)
+            return a.ctypes.data_as(ctypes.c_void_p)
+
+        steps = 0
+        sh_ev = (_ShoutEvents * max(1, len(shout)))()
+        for i, (has, key, val) in enumerate(shout):
+            steps = len(has)
+            sh_ev[i] = _ShoutEvents(arr(has, np.uint8), arr(key, np.uint64), arr(val, np.uint64))
+        tw_ev = (_TwistEvents * max(1, len(twist)))()
+        for i, (hr, ra, rv, hw, wa, wv) in enumerate(twist):
+            steps = len(hr)
+            tw_ev[i] = _TwistEvents(arr(hr, np.uint8), arr(ra, np.uint64), arr(rv, np.uint64), arr(hw, np.uint8),
+                                    arr(wa, np.uint64), arr(wv, np.uint64))
+        chunk = _TraceChunk(steps, ctypes.cast(sh_ev, ctypes.c_void_p), ctypes.cast(tw_ev, ctypes.c_void_p))
+        n = ctypes.c_uint64()
+        if self._cap == 0:
+            self._cap = 1 << 20
+        out = np.empty(self._cap, np.uint64)
+        self.ctx.check(self.ctx.lib.neo_gpu_shard_fold_step_trace(self.h, _p(z) if z.size else None, z.size,
+                                                                  ctypes.byref(chunk), _p(out), self._cap,
+                                                                  ctypes.byref(n)))
         return out[: n.value].copy()
 
     def fold_step_device(self, d_z_ptr: int) -> int:

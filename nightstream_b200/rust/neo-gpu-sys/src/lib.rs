@@ -78,6 +78,36 @@ pub struct neo_mem_desc {
     pub twist: *const neo_mem_instance,
 }
 
+/// One Shout instance's events of a trace chunk (include/neo_gpu.h).
+#[repr(C)]
+#[derive(Clone, Copy)]
+pub struct neo_shout_events {
+    pub has_lookup: *const u8,
+    pub key: *const u64,
+    pub val: *const u64,
+}
+
+/// One Twist instance's events of a trace chunk.
+#[repr(C)]
+#[derive(Clone, Copy)]
+pub struct neo_twist_events {
+    pub has_read: *const u8,
+    pub ra: *const u64,
+    pub rv: *const u64,
+    pub has_write: *const u8,
+    pub wa: *const u64,
+    pub wv: *const u64,
+}
+
+/// The memory events of one trace chunk (neo_gpu_shard_fold_step_trace).
+#[repr(C)]
+#[derive(Clone, Copy)]
+pub struct neo_trace_chunk {
+    pub steps: u64,
+    pub shout: *const neo_shout_events,
+    pub twist: *const neo_twist_events,
+}
+
 #[repr(C)]
 #[derive(Clone, Copy)]
 pub struct neo_mem_init {
@@ -143,6 +173,7 @@ extern "C" {
     pub fn neo_gpu_shard_fold_step(sh: *mut neo_gpu_shard, z: *const u64, proof: *mut u64, proof_cap: u64, proof_len: *mut u64) -> c_int;
     pub fn neo_gpu_shard_step_proof(sh: *mut neo_gpu_shard, out: *mut u64, cap: u64, len: *mut u64) -> c_int;
     pub fn neo_gpu_shard_fold_step_device(sh: *mut neo_gpu_shard, d_z: *const u64, proof_len: *mut u64) -> c_int;
+    pub fn neo_gpu_shard_fold_step_trace(sh: *mut neo_gpu_shard, z_cpu: *const u64, z_cpu_len: u64, trace: *const neo_trace_chunk, proof: *mut u64, proof_cap: u64, proof_len: *mut u64) -> c_int;
     pub fn neo_gpu_shard_transcript_state(sh: *const neo_gpu_shard, st8: *mut u64) -> c_int;
     pub fn neo_gpu_shard_ccs_digest(sh: *const neo_gpu_shard, d4: *mut u64) -> c_int;
     pub fn neo_gpu_shard_step_stats(sh: *const neo_gpu_shard, out: *mut f64, n: u32) -> c_int;
