@@ -685,6 +685,33 @@ def run_ours(args, rank, world, local_rank):
         ems = max_over_ranks(ems, dist)
         e2e = {"value": replica_value(world, args.steps, ems), "unit": UNIT, "h2d_bytes_per_step": int(zh[0].nbytes),
                "d2h_bytes_per_step": int(proof.nbytes)}
+        if wl.mem is not None:
+            # the same steps from trace chunks (neo_gpu_shard_fold_step_trace): the
+            # CPU witness and the chunk's memory events in; the bus tail, the Twist
+            # increments and the next MemInit are computed on the device
+            from nightstream_b200 import synth
+            n_chunks = len(wl.zs)
+            chunks = []
+            for i in range(args.steps):
+                c = cur + i
+                base, sev, tev = synth.trace_events(wl.z(c), wl.mem, m)
+                zc = torch.from_numpy(wl.z(c)[:base].view(np.int64).copy()).pin_memory().numpy().view(np.uint64)
+                chunks.append((c, zc, sev, tev))
+            h2d = int(chunks[0][1].nbytes) + sum(int(a.nbytes) for ev in chunks[0][2] + chunks[0][3] for a in ev)
+            barrier()
+            ctx.synchronize()
+            ev0.record(stream)
+            for i, (c, zc, sev, tev) in enumerate(chunks):
+                if i == 0 or c % n_chunks == 0:  # the trace restarts: its memory from the chunk's MemInit
+                    wl.prepare(shard, c)
+                proof = shard.fold_step_trace(zc, sev, tev)
+            ev1.record(stream)
+            ev1.synchronize()
+            tms = max_over_ranks(ev0.elapsed_time(ev1), dist)
+            cur += args.steps
+            e2e["trace"] = {"value": replica_value(world, args.steps, tms), "unit": UNIT, "h2d_bytes_per_step": h2d,
+                            "d2h_bytes_per_step": int(proof.nbytes),
+                            "api": "neo_gpu_shard_fold_step_trace (CPU witness + trace events in)"}
 
     roofline_commit = commit_roofline(ctx, m, stream)
     roofline = rounds_roofline(ctx, ccs, wl.z(0), args.ell, stream)

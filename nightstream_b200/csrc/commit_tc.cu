@@ -472,6 +472,9 @@ struct P8 {
 #ifndef P8_ASTAGES
 #define P8_ASTAGES 6
 #endif
+#ifndef P8_CTAS_PER_SM
+#define P8_CTAS_PER_SM 1
+#endif
 #ifndef P8_BSTAGES
 #define P8_BSTAGES 4
 #endif
@@ -480,7 +483,8 @@ struct P8 {
     static constexpr uint32_t TMEM_COLS = NPAD <= 64 ? 64 : (NPAD <= 128 ? 128 : 256);
     static_assert(NPAD <= 256 && NPAD % 16 == 0, "one MMA per K step (M = 128: N <= 256, N % 16 == 0)");
     static_assert(B_BYTES % 1024 == 0, "B stages stay 1024-byte aligned");
-    static_assert(SMEM + 1024 + 256 <= 232448, "shared memory budget");
+    static_assert(SMEM + 1024 + 256 <= 232448 / P8_CTAS_PER_SM - 1024 * (P8_CTAS_PER_SM - 1), "shared memory budget");
+    static_assert(P8_CTAS_PER_SM == 1 || TMEM_COLS * P8_CTAS_PER_SM <= 512, "TMEM columns of the resident CTAs");
 };
 
 __device__ __forceinline__ uint64_t ns_desc_lbo(uint32_t saddr, uint32_t lbo) {
@@ -534,7 +538,7 @@ __global__ void p8_seq_kernel(const int8_t* __restrict__ digits, uint32_t n_vec,
 }
 
 template <int NV>
-__global__ void __launch_bounds__(P8<NV>::THREADS, 1) commit_p8_kernel(const TcArgs a) {
+__global__ void __launch_bounds__(P8<NV>::THREADS, P8_CTAS_PER_SM) commit_p8_kernel(const TcArgs a) {
     using S = P8<NV>;
     extern __shared__ __align__(1024) uint8_t smem_raw[];
     uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
@@ -763,7 +767,8 @@ size_t tc_scratch_bytes(uint32_t n_vec, uint64_t m, bool small, uint32_t* n_grou
     // fill whole waves of 148 SMs (1 CTA per SM), at most TC_MAX_KB K blocks per CTA
     uint32_t waves = 1, n_ksplit;
     for (;; waves++) {
-        n_ksplit = (148 * waves) / n_groups;  // n_groups * n_ksplit <= whole waves of 148 CTAs
+        // n_groups * n_ksplit <= whole waves of 148 SMs x the CTAs one SM holds
+        n_ksplit = (148 * (small ? P8_CTAS_PER_SM : 1) * waves) / n_groups;
         if (n_ksplit == 0) n_ksplit = 1;
         if (n_ksplit > n_kb) n_ksplit = n_kb;
         if ((n_kb + n_ksplit - 1) / n_ksplit <= TC_MAX_KB) break;

@@ -180,6 +180,38 @@ def memory_trace_chunks(n_chunks: int, steps: int, shout_ell, twist_ell, seed: i
     return buses, dict(steps=steps, shout=shout, twist=twist), inits
 
 
+def trace_events(z: np.ndarray, mem: dict, m: int):
+    """The memory events a witness's shared-CPU-bus tail encodes, in the form
+    neo_gpu_shard_fold_step_trace takes: (bus_base, shout, twist) with
+    shout[i] = (has_lookup, key, val) and twist[i] = (has_read, ra, rv,
+    has_write, wa, wv) per trace step (column order of the bus: per Shout
+    [addr bits, has_lookup, val], per Twist [ra bits, wa bits, has_read,
+    has_write, wv, rv, inc])."""
+    steps = mem["steps"]
+    widths = [sd["ell_addr"] + 2 for sd in mem["shout"]] + [2 * td["ell_addr"] + 5 for td in mem["twist"]]
+    base = m - sum(widths) * steps
+    bus = np.asarray(z, np.uint64)[base:].reshape(sum(widths), steps)
+
+    def bits(rows):
+        out = np.zeros(steps, np.uint64)
+        for b in range(rows.shape[0]):
+            out |= rows[b].astype(np.uint64) << np.uint64(b)
+        return out
+
+    shout, twist, col = [], [], 0
+    for sd in mem["shout"]:
+        e = sd["ell_addr"]
+        shout.append((bus[col + e].astype(np.uint8), bits(bus[col:col + e]), bus[col + e + 1].copy()))
+        col += e + 2
+    for td in mem["twist"]:
+        e = td["ell_addr"]
+        t = bus[col:col + 2 * e + 5]
+        twist.append((t[2 * e].astype(np.uint8), bits(t[:e]), t[2 * e + 3].copy(), t[2 * e + 1].astype(np.uint8),
+                      bits(t[e:2 * e]), t[2 * e + 2].copy()))
+        col += 2 * e + 5
+    return base, shout, twist
+
+
 def make_memory_workload(ell: int, seed: int, steps: int, shout_ell, twist_ell, m_in: int = 1,
                          table_len: int = None, **trace_kw):
     """Single shard with memory: a satisfied R1CS of n = m = 2^ell whose witness
