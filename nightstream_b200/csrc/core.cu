@@ -37,6 +37,7 @@ static int neo_gpu_ctx_destroy_impl_abi(neo_gpu_ctx* ctx) {
     cudaSetDevice(ctx->device);
     cudaStreamSynchronize(ctx->stream);
     if (ctx->scratch) cudaFree(ctx->scratch);
+    if (ctx->chi_cache) cudaFree(ctx->chi_cache);
     if (ctx->d_err) cudaFree(ctx->d_err);
     cudaStreamDestroy(ctx->stream);
     delete ctx;

@@ -712,6 +712,8 @@ int ccs_oracle_round_launch(neo_gpu_ccs_oracle* o, K* d_dst, uint32_t* ncoef);
 void ccs_oracle_round_set(neo_gpu_ccs_oracle* o, const K* coeffs);
 bool mem_round_multi_ok(const neo_gpu_mem_oracle* o);
 int ta_round_launch(neo_gpu_twist_addr* o, K* d_dst, bool* launched);
+int mem_claims_multi(neo_gpu_ctx* ctx, neo_gpu_mem_oracle* const* os, int n, K* claims, DevBuf<K>& partials,
+                     DevBuf<K>& d_slots, HostBuf<K>& h_slots);
 int mem_round_launch_multi(neo_gpu_ctx* ctx, neo_gpu_mem_oracle* const* os, int n, K* const* d_out,
                            DevBuf<K>& partials);
 
@@ -1535,24 +1537,31 @@ static int fold_step_impl(neo_gpu_shard* sh, const uint64_t* z_host, const uint6
         for (size_t i = 0; i < sh->shout.size(); i++) {
             const ShoutInst& s = *sh->shout[i];
             neo_gpu_mem_oracle *vo = nullptr, *ao = nullptr, *bo = nullptr;
-            K vc, ac_, bc;
+            K vc{}, ac_{};
             // value: [has_lookup, val] are adjacent bus columns
             if ((rc = mb(&vo, NEO_MEM_SHOUT_VALUE, ell_n, (const uint64_t*)r_cycle.data(),
                                                        0, nullptr, nullptr, 2, (const uint64_t*)(C + (size_t)(s.col0 + s.ea) * L),
-                                                       nullptr, (uint64_t*)&vc)))
+                                                       nullptr, nullptr)))
                 return rc;
             std::vector<uint32_t> ids = {s.col0 + s.ea};
             for (uint32_t b = 0; b < s.ea; b++) ids.push_back(s.col0 + b);
             if ((rc = assemble(sh, C, ids))) return rc;
             if ((rc = mb(&ao, NEO_MEM_SHOUT_ADAPTER, ell_n, (const uint64_t*)r_cycle.data(),
                                                        s.ea, (const uint64_t*)r_addr_s.data(), nullptr, 1 + s.ea,
-                                                       (const uint64_t*)sh->d_asm.p, nullptr, (uint64_t*)&ac_)))
+                                                       (const uint64_t*)sh->d_asm.p, nullptr, nullptr)))
                 return rc;
+            {  // both claims from one evaluation of round 0
+                neo_gpu_mem_oracle* g2[2] = {vo, ao};
+                K c2[2];
+                if ((rc = mem_claims_multi(ctx, g2, 2, c2, sh->d_mpart, sh->d_round, sh->h_round))) return rc;
+                vc = c2[0];
+                ac_ = c2[1];
+            }
             // bitness over [addr_bits..., has_lookup] (adjacent columns)
             auto bw = bitness_weights(r_cycle[0], s.ea + 1, 0x53484F5554ULL + i);
             if ((rc = mb(&bo, NEO_MEM_BITNESS, ell_n, (const uint64_t*)r_cycle.data(), 0,
                                                        nullptr, nullptr, s.ea + 1, (const uint64_t*)(C + (size_t)s.col0 * L),
-                                                       (const uint64_t*)bw.data(), (uint64_t*)&bc)))
+                                                       (const uint64_t*)bw.data(), nullptr)))  // claim 0 by construction
                 return rc;
             Claim cv, ca, cb;
             cv.label = "shout/value"; cv.deg = 3; cv.sum = vc; cv.mem = vo;
@@ -1704,15 +1713,15 @@ static int fold_step_impl(neo_gpu_shard* sh, const uint64_t* z_host, const uint6
         for (size_t i = 0; i < sh->twist.size(); i++) {
             const TwistInst& w = *sh->twist[i];
             neo_gpu_mem_oracle *lo = nullptr, *to = nullptr, *po = nullptr;
-            K lc, tc_, pc;
+            K lc{}, tc_{}, pc{};  // set below from one evaluation of the batch's round 0
             if ((rc = assemble(sh, C, twist_val_ids(w)))) return rc;
             if ((rc = mb(&lo, NEO_MEM_VAL_EVAL, ell_n, (const uint64_t*)r_time.data(), w.ea,
                                                        (const uint64_t*)r_addr_t[i].data(), nullptr, 2 + w.ea,
-                                                       (const uint64_t*)sh->d_asm.p, nullptr, (uint64_t*)&lc)))
+                                                       (const uint64_t*)sh->d_asm.p, nullptr, nullptr)))
                 return rc;
             if ((rc = mb(&to, NEO_MEM_TOTAL_INC, ell_n, nullptr, w.ea,
                                                        (const uint64_t*)r_addr_t[i].data(), nullptr, 2 + w.ea,
-                                                       (const uint64_t*)sh->d_asm.p, nullptr, (uint64_t*)&tc_)))
+                                                       (const uint64_t*)sh->d_asm.p, nullptr, nullptr)))
                 return rc;
             Claim c1, c2;
             c1.label = "twist/val_eval_lt"; c1.deg = w.ea + 3; c1.sum = lc; c1.mem = lo;
@@ -1723,12 +1732,24 @@ static int fold_step_impl(neo_gpu_shard* sh, const uint64_t* z_host, const uint6
                 if ((rc = assemble(sh, sh->d_prev_cols.p, twist_val_ids(w)))) return rc;
                 if ((rc = mb(&po, NEO_MEM_TOTAL_INC, ell_n, nullptr, w.ea,
                                                            (const uint64_t*)r_addr_t[i].data(), nullptr, 2 + w.ea,
-                                                           (const uint64_t*)sh->d_asm.p, nullptr, (uint64_t*)&pc)))
+                                                           (const uint64_t*)sh->d_asm.p, nullptr, nullptr)))
                     return rc;
                 Claim c3;
                 c3.label = "twist/rollover_prev_total"; c3.deg = w.ea + 2; c3.sum = pc; c3.mem = po;
                 vcl.push_back(c3); tags.push_back(2);
             }
+        }
+        {  // every val-eval claim from one evaluation of round 0
+            std::vector<neo_gpu_mem_oracle*> vos;
+            for (auto& c : vcl) vos.push_back(c.mem);
+            std::vector<K> vs(vos.size());
+            for (size_t i0 = 0; i0 < vos.size(); i0 += 24) {
+                const int nn = (int)std::min<size_t>(24, vos.size() - i0);
+                if ((rc = mem_claims_multi(ctx, vos.data() + i0, nn, vs.data() + i0, sh->d_mpart, sh->d_round,
+                                           sh->h_round)))
+                    return rc;
+            }
+            for (size_t i = 0; i < vcl.size(); i++) vcl[i].sum = vs[i];
         }
         auto bn = le64(sh->twist.size());
         tr.append_message("twist/val_eval/batch_start", bn.data(), 8);

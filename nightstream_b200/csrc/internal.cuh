@@ -23,6 +23,11 @@ struct neo_gpu_ctx {
     uint32_t* d_err = nullptr;       // device error word (bounded-wait timeouts); 0 = ok
     void* scratch = nullptr;         // growable per-context scratch (stream-ordered use)
     size_t scratch_bytes = 0;
+    // the last chi table a memory oracle built (the time-lane oracles of a
+    // step share their point): key = ell then the point's words
+    void* chi_cache = nullptr;
+    size_t chi_cache_bytes = 0;
+    std::vector<uint64_t> chi_key;
     int fail(int code, const char* what, cudaError_t e = cudaSuccess) {
         char buf[512];
         if (e != cudaSuccess)

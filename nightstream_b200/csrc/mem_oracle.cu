@@ -314,19 +314,19 @@ __global__ void __launch_bounds__(256) dot_kernel(const K* __restrict__ a, const
     }
 }
 
-// ---- all memory claims of one sum-check round in two launches ------------
+// ---- all memory claims of one sum-check round in one launch --------------
 // A batched round (the Route-A time claims, the val-eval batch, the address
 // pre-time batches) evaluates every claim's round polynomial at x = 0..deg
-// before the transcript draws the next challenge.  These kernels fold, then
-// evaluate and reduce (each claim's last block sums its partials) the tables
-// of up to MULTI_MAX claims together; the values land in one device array
-// that the host reads with a single copy.
+// before the transcript draws the next challenge.  One kernel folds (the
+// pending challenge), evaluates and reduces (each claim's last block sums its
+// partials) the tables of up to MULTI_MAX claims together; the values land in
+// one device array that the host reads with a single copy.
 constexpr int MULTI_MAX = 24;
 constexpr int MX = 8;  // evaluation points per pass (thread-local accumulators)
 
 struct MultiClaim {
-    const K* tab;      // [nf][len] current tables
-    K* dst;            // fold destination [nf][len / 2] (fold kernel)
+    const K* tab;      // [nf][len] current tables (written by this launch when src is set)
+    const K* src;      // a pending fold: [nf][2 len] tables before binding r, else null
     uint64_t len;
     uint32_t nf, npts;
     int bitness;
@@ -354,30 +354,52 @@ __device__ __forceinline__ int multi_claim_of(const MultiArgs& a, uint32_t blk) 
     return c;
 }
 
-// fold every claim's tables by its challenge: dst[f][t] = lerp(tab[f][2t], tab[f][2t+1], r)
-__global__ void __launch_bounds__(256) mem_multi_fold_kernel(const __grid_constant__ MultiArgs a) {
-    const int ci = multi_claim_of(a, blockIdx.x);
-    const MultiClaim& c = a.c[ci];
-    const uint64_t half = c.len >> 1;
-    const uint64_t i = (uint64_t)(blockIdx.x - c.blk0) * 256 + threadIdx.x;
-    if (i >= half * c.nf) return;
-    const uint64_t f = i / half, t = i % half;
-    const K* s = c.tab + f * c.len + 2 * t;
-    c.dst[f * half + t] = gl::klerp(s[0], s[1], c.r);
+// Factor f of pair p in the current round: (f0, f1) = the entries 2p, 2p+1.
+// With a pending fold they are lerp(src[4p], src[4p+1], r) and lerp(src[4p+2],
+// src[4p+3], r) -- computed here unless this thread wrote them already.
+__device__ __forceinline__ void multi_factor(const MultiClaim& c, uint32_t f, uint64_t p, bool from_tab, K& f0, K& f1) {
+    if (c.src && !from_tab) {
+        const K* o = c.src + (uint64_t)f * (2 * c.len) + 4 * p;
+        f0 = gl::klerp(o[0], o[1], c.r);
+        f1 = gl::klerp(o[2], o[3], c.r);
+        return;
+    }
+    const K* s = c.tab + (uint64_t)f * c.len + 2 * p;
+    f0 = s[0];
+    f1 = s[1];
+}
+
+// The pending fold of the factors this thread owns (point group 0: every
+// factor, or for a bitness claim its column chunk and, in chunk 0, chi).
+__device__ __forceinline__ void multi_fold_owned(const MultiClaim& c, uint64_t p, uint32_t ch) {
+    K* t = const_cast<K*>(c.tab);
+    auto one = [&](uint32_t f) {
+        const K* o = c.src + (uint64_t)f * (2 * c.len) + 4 * p;
+        t[(uint64_t)f * c.len + 2 * p] = gl::klerp(o[0], o[1], c.r);
+        t[(uint64_t)f * c.len + 2 * p + 1] = gl::klerp(o[2], o[3], c.r);
+    };
+    if (!c.bitness) {
+        for (uint32_t f = 0; f < c.nf; f++) one(f);
+        return;
+    }
+    if (ch == 0) one(0);
+    const uint32_t f_lo = 1 + ch * BIT_CHUNK, f_hi = min(c.nf, f_lo + BIT_CHUNK);
+    for (uint32_t f = f_lo; f < f_hi; f++) one(f);
 }
 
 // Values of one pair at x = x0 .. x0 + PPT - 1: the product of the claim's
 // affine factors (a factor zero on both children zeroes every point), or for
 // a bitness claim chi(x) times the weighted b(b - 1) sum over the columns of
-// chunk ch, additions along x.
+// chunk ch, additions along x.  own: this thread folded its factors already.
 template <int PPT>
-__device__ __forceinline__ void multi_eval_points(const MultiClaim& c, uint64_t p, uint32_t x0, uint32_t ch, K* acc) {
+__device__ __forceinline__ void multi_eval_points(const MultiClaim& c, uint64_t p, uint32_t x0, uint32_t ch, bool own,
+                                                  K* acc) {
     if (!c.bitness) {
 #pragma unroll
         for (int i = 0; i < PPT; i++) acc[i] = gl::kone();
         for (uint32_t f = 0; f < c.nf; f++) {
-            const K* s = c.tab + (uint64_t)f * c.len + 2 * p;
-            const K f0 = s[0], f1 = s[1];
+            K f0, f1;
+            multi_factor(c, f, p, own, f0, f1);
             if (gl::kiszero(f0) && gl::kiszero(f1)) {
 #pragma unroll
                 for (int i = 0; i < PPT; i++) acc[i] = gl::kzero();
@@ -400,13 +422,8 @@ __device__ __forceinline__ void multi_eval_points(const MultiClaim& c, uint64_t 
     K b0[BIT_CHUNK], b1[BIT_CHUNK];
 #pragma unroll
     for (uint32_t u = 0; u < BIT_CHUNK; u++) {
-        if (f_lo + u < f_hi) {
-            const K* s = c.tab + (uint64_t)(f_lo + u) * c.len + 2 * p;
-            b0[u] = s[0];
-            b1[u] = s[1];
-        } else {
-            b0[u] = b1[u] = gl::kzero();
-        }
+        if (f_lo + u < f_hi) multi_factor(c, f_lo + u, p, own, b0[u], b1[u]);
+        else b0[u] = b1[u] = gl::kzero();
     }
     bool any = false;
 #pragma unroll
@@ -422,8 +439,9 @@ __device__ __forceinline__ void multi_eval_points(const MultiClaim& c, uint64_t 
         }
     }
     if (!any) return;
-    const K* s = c.tab + 2 * p;
-    const K f0 = s[0], d = gl::ksub(s[1], f0);
+    K f0, f1;
+    multi_factor(c, 0, p, own && ch == 0, f0, f1);
+    const K d = gl::ksub(f1, f0);
     K v = gl::kadd(f0, gl::kscale_small(d, (int32_t)x0));
 #pragma unroll
     for (int i = 0; i < PPT; i++) {
@@ -456,20 +474,24 @@ __global__ void __launch_bounds__(256) mem_multi_eval_kernel(const __grid_consta
     // has_write behind chi; factor 0 where no chi leads) is zero on both
     // children contributes nothing at any x
     bool live = p < pairs;
+    // a pending fold: point group 0 writes the folded tables of its pairs
+    const bool own = c.src && g == 0;
+    if (live && own) multi_fold_owned(c, p, ch);
     if (live && !c.bitness) {
-        const K* s0 = c.tab + 2 * p;
-        const K* s1 = c.tab + (c.nf > 1 ? c.len : 0) + 2 * p;
-        live = !(gl::kiszero(s0[0]) && gl::kiszero(s0[1])) && !(gl::kiszero(s1[0]) && gl::kiszero(s1[1]));
+        K a0, a1, b0, b1;
+        multi_factor(c, 0, p, own, a0, a1);
+        multi_factor(c, c.nf > 1 ? 1 : 0, p, own, b0, b1);
+        live = !(gl::kiszero(a0) && gl::kiszero(a1)) && !(gl::kiszero(b0) && gl::kiszero(b1));
     }
     K acc[MX];
 #pragma unroll
     for (int i = 0; i < MX; i++) acc[i] = gl::kzero();
     if (live) {
         switch (c.ppt) {
-            case 1: multi_eval_points<1>(c, p, x0, ch, acc); break;
-            case 2: multi_eval_points<2>(c, p, x0, ch, acc); break;
-            case 4: multi_eval_points<4>(c, p, x0, ch, acc); break;
-            default: multi_eval_points<MX>(c, p, x0, ch, acc); break;
+            case 1: multi_eval_points<1>(c, p, x0, ch, own, acc); break;
+            case 2: multi_eval_points<2>(c, p, x0, ch, own, acc); break;
+            case 4: multi_eval_points<4>(c, p, x0, ch, own, acc); break;
+            default: multi_eval_points<MX>(c, p, x0, ch, own, acc); break;
         }
     }
     const bool any = __syncthreads_or(live);
@@ -654,7 +676,8 @@ K lagrange_at(const std::vector<K>& v, K x) {
 
 int mem_create(neo_gpu_ctx* ctx, int kind, uint32_t ell, const uint64_t* r_point, uint32_t A, const uint64_t* r_addr,
                const uint64_t* init, uint32_t n_cols, const uint64_t* cols, bool cols_on_device,
-               const uint64_t* weights, uint64_t* claim_out, neo_gpu_mem_oracle** out, bool reuse = false) {
+               const uint64_t* weights, uint64_t* claim_out, neo_gpu_mem_oracle** out, bool reuse = false,
+               bool lazy = false) {
     if (!ctx || !out) return NEO_ERR_ARG;
     if (!reuse) *out = nullptr;
     if (kind < NEO_MEM_SHOUT_VALUE || kind > NEO_MEM_PRODUCT) return ctx->fail(NEO_ERR_ARG, "mem_oracle: unknown kind");
@@ -721,9 +744,29 @@ int mem_create(neo_gpu_ctx* ctx, int kind, uint32_t ell, const uint64_t* r_point
         return NEO_OK;
     };
     int rc = NEO_OK;
-    if (chi) {
-        rc = launch_chi_table(ctx, dpt.p, ell, T);  // factor 0 = χ_{r_cycle}
-        if (rc) return fail(rc);
+    if (chi) {  // factor 0 = χ_{r_cycle}, copied when the previous oracle built it for the same point
+        std::vector<uint64_t> key(1, ell);
+        key.insert(key.end(), r_point, r_point + 2 * (size_t)ell);
+        const size_t bytes = L * sizeof(K);
+        if (ctx->chi_cache && ctx->chi_key == key && ctx->chi_cache_bytes >= bytes) {
+            if (cudaMemcpyAsync(T, ctx->chi_cache, bytes, cudaMemcpyDeviceToDevice, S))
+                return fail(ctx->fail(NEO_ERR_CUDA, "mem_oracle: chi copy"));
+        } else {
+            rc = launch_chi_table(ctx, dpt.p, ell, T);
+            if (rc) return fail(rc);
+            if (ctx->chi_cache_bytes < bytes) {
+                cudaStreamSynchronize(S);  // the old cache may still be read by an earlier copy
+                if (ctx->chi_cache) cudaFree(ctx->chi_cache);
+                ctx->chi_cache = nullptr;
+                ctx->chi_cache_bytes = 0;
+                ctx->chi_key.clear();
+                if (cudaMalloc(&ctx->chi_cache, bytes)) return fail(ctx->fail(NEO_ERR_OOM, "mem_oracle: chi cache"));
+                ctx->chi_cache_bytes = bytes;
+            }
+            if (cudaMemcpyAsync(ctx->chi_cache, T, bytes, cudaMemcpyDeviceToDevice, S))
+                return fail(ctx->fail(NEO_ERR_CUDA, "mem_oracle: chi cache copy"));
+            ctx->chi_key = key;
+        }
     }
     cudaError_t ce = cudaSuccess;
     switch (kind) {
@@ -794,15 +837,19 @@ int mem_create(neo_gpu_ctx* ctx, int kind, uint32_t ell, const uint64_t* r_point
     }
     if (ce) return fail(ctx->fail(ce == cudaErrorMemoryAllocation ? NEO_ERR_OOM : NEO_ERR_CUDA, "mem_oracle: build", ce));
     if (rc) return fail(rc);
-    // claim = Σ over the hypercube = p_0(0) + p_0(1)  (the constructors' sums)
-    rc = mem_round_values(o);
-    if (rc) return fail(rc);
-    o->claim = ell ? gl::kadd(o->hvals[0], o->hvals[1]) : o->hvals[0];
-    if (claim_out) {
-        claim_out[0] = o->claim.re;
-        claim_out[1] = o->claim.im;
+    // claim = Σ over the hypercube = p_0(0) + p_0(1)  (the constructors' sums);
+    // a lazy build (the shard: no claim asked for, or claims computed for a
+    // group by mem_claims_multi) skips it
+    if (!lazy) {
+        rc = mem_round_values(o);
+        if (rc) return fail(rc);
+        o->claim = ell ? gl::kadd(o->hvals[0], o->hvals[1]) : o->hvals[0];
+        if (claim_out) {
+            claim_out[0] = o->claim.re;
+            claim_out[1] = o->claim.im;
+        }
+        NEO_CK(ctx, ctx_sync(ctx));
     }
-    NEO_CK(ctx, ctx_sync(ctx));
     *out = o;
     return NEO_OK;
 }
@@ -817,47 +864,28 @@ bool mem_round_multi_ok(const neo_gpu_mem_oracle* o) {
 }
 
 // The next round of n oracles: pending folds, then the values at x = 0..deg
-// of oracle i into d_out[i] (device), in two launches and without a host
+// of oracle i into d_out[i] (device), in one launch and without a host
 // sync.  Every oracle must satisfy mem_round_multi_ok; n <= MULTI_MAX.
 int mem_round_launch_multi(neo_gpu_ctx* ctx, neo_gpu_mem_oracle* const* os, int n, K* const* d_out,
                            DevBuf<K>& partials) {
     if (n <= 0) return NEO_OK;
     if (n > MULTI_MAX) return ctx->fail(NEO_ERR_UNSUPPORTED, "mem_round_launch_multi: too many claims");
-    // folds
-    MultiArgs f{};
+    MultiArgs a{};
+    a.n = n;
     uint32_t blocks = 0;
+    uint64_t parts = 0;
     for (int i = 0; i < n; i++) {
         neo_gpu_mem_oracle* o = os[i];
-        if (!o->pending) continue;
-        MultiClaim& c = f.c[f.n++];
-        c.tab = o->tab[o->cur].p;
-        c.dst = o->tab[o->cur ^ 1].p;
-        c.len = o->len;
-        c.nf = o->nf;
-        c.r = o->pending_r;
-        c.blk0 = blocks;
-        blocks += (uint32_t)ceil_div((o->len >> 1) * o->nf, 256);
-    }
-    if (f.n) {
-        mem_multi_fold_kernel<<<blocks, 256, 0, ctx->stream>>>(f);
-        NEO_LAUNCHED(ctx);
-        for (int i = 0; i < n; i++) {
-            neo_gpu_mem_oracle* o = os[i];
-            if (!o->pending) continue;
+        MultiClaim& c = a.c[i];
+        c.src = nullptr;
+        if (o->pending) {  // the evaluation launch applies the fold (point group 0 writes the tables)
+            c.src = o->tab[o->cur].p;
+            c.r = o->pending_r;
             o->cur ^= 1;
             o->len >>= 1;
             o->pending = false;
         }
-    }
-    // evaluations
-    MultiArgs a{};
-    a.n = n;
-    blocks = 0;
-    uint64_t parts = 0;
-    for (int i = 0; i < n; i++) {
-        neo_gpu_mem_oracle* o = os[i];
         if (o->len < 2) return ctx->fail(NEO_ERR_INVARIANT, "mem_round_launch_multi: no pairs left");
-        MultiClaim& c = a.c[i];
         c.tab = o->tab[o->cur].p;
         c.len = o->len;
         c.nf = o->nf;
@@ -900,6 +928,39 @@ int mem_round_launch_multi(neo_gpu_ctx* ctx, neo_gpu_mem_oracle* const* os, int 
 
 
 
+// Claims (sums over the hypercube, p_0(0) + p_0(1)) of n lazily built oracles:
+// one multi-claim evaluation of their round 0, one copy and one sync;
+// oracles the multi-claim kernel cannot take are evaluated one by one.
+int mem_claims_multi(neo_gpu_ctx* ctx, neo_gpu_mem_oracle* const* os, int n, K* claims, DevBuf<K>& partials,
+                     DevBuf<K>& d_slots, HostBuf<K>& h_slots) {
+    constexpr uint32_t SLOT = MEM_MAX_DEG + 1;
+    bool multi = n > 0 && n <= MULTI_MAX;
+    for (int i = 0; i < n && multi; i++) multi = mem_round_multi_ok(os[i]) && !os[i]->pending && os[i]->ell > 0;
+    if (!multi) {
+        for (int i = 0; i < n; i++) {
+            neo_gpu_mem_oracle* o = os[i];
+            if (int rc = mem_round_values(o)) return rc;
+            o->claim = o->ell ? gl::kadd(o->hvals[0], o->hvals[1]) : o->hvals[0];
+            claims[i] = o->claim;
+        }
+        NEO_CK(ctx, ctx_sync(ctx));
+        return NEO_OK;
+    }
+    NEO_CK(ctx, d_slots.ensure((size_t)n * SLOT));
+    NEO_CK(ctx, h_slots.ensure((size_t)n * SLOT));
+    std::vector<K*> dst(n);
+    for (int i = 0; i < n; i++) dst[i] = d_slots.p + (size_t)i * SLOT;
+    if (int rc = mem_round_launch_multi(ctx, os, n, dst.data(), partials)) return rc;
+    NEO_CK(ctx, cudaMemcpyAsync(h_slots.p, d_slots.p, (size_t)n * SLOT * sizeof(K), cudaMemcpyDeviceToHost, ctx->stream));
+    NEO_CK(ctx, ctx_sync(ctx));
+    for (int i = 0; i < n; i++) {
+        const K* v = h_slots.p + (size_t)i * SLOT;
+        os[i]->claim = gl::kadd(v[0], v[1]);
+        claims[i] = os[i]->claim;
+    }
+    return NEO_OK;
+}
+
 static int neo_gpu_mem_oracle_create_impl_abi(neo_gpu_ctx* ctx, int kind, uint32_t ell, const uint64_t* r_point,
                                          uint32_t ell_addr, const uint64_t* r_addr, const uint64_t* init_at_r_addr,
                                          uint32_t n_cols, const uint64_t* cols, const uint64_t* weights,
@@ -921,7 +982,7 @@ int mem_oracle_build_device(neo_gpu_ctx* ctx, int kind, uint32_t ell, const uint
                             const uint64_t* d_cols, const uint64_t* weights, uint64_t* claim,
                             neo_gpu_mem_oracle** slot) {
     return mem_create(ctx, kind, ell, r_point, ell_addr, r_addr, init_at_r_addr, n_cols, d_cols, true, weights, claim,
-                      slot, true);
+                      slot, true, claim == nullptr);
 }
 
 static int neo_gpu_mem_oracle_create_device_impl_abi(neo_gpu_ctx* ctx, int kind, uint32_t ell, const uint64_t* r_point,
@@ -1145,31 +1206,17 @@ __global__ void ta_build_kernel(const TaBuild a) {
     }
 }
 
-// per round: write keys and deltas
-__global__ void ta_prep_kernel(const K* __restrict__ hw, const K* __restrict__ inc, const uint32_t* __restrict__ wa,
-                               const K* __restrict__ wpw, uint32_t E, uint32_t bit, uint32_t* __restrict__ wkey,
-                               K* __restrict__ wdelta) {
-    uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
-    if (j >= E) return;
-    K h = hw[j];
-    if (gl::kiszero(h)) {
-        wkey[j] = 0xFFFFFFFFu;
-        wdelta[j] = gl::kzero();
-        return;
-    }
-    wkey[j] = bit >= 32 ? 0u : (wa[j] >> bit);
-    wdelta[j] = gl::kmul(gl::kmul(inc[j], h), wpw[j]);
-}
-
+// one round of the address lane: a block (query block x, event block y) adds
+// the earlier writes of event block y to its queries' memory values
 struct TaEval {
     int kind;  // 0 read, 1 write
     uint32_t E, bit;
     const K *eq, *hr, *rv, *hw, *inc, *wv, *rpw, *wpw;
     const uint32_t *ra, *wa;
-    const uint32_t* wkey;
-    const K* wdelta;
     const K* init_tab;  // folded initial memory, >= 2 entries
-    K* partials;        // [3][gridDim.x]
+    K* partials;        // [3][gridDim.x * gridDim.y]
+    K* out;             // the round's values at x = 0, 1, 2 (the last block sums the partials)
+    unsigned int* ticket;
 };
 
 // grid.x: query events i in tiles of TA_T; grid.y: earlier-event chunks j of
@@ -1199,8 +1246,12 @@ __global__ void __launch_bounds__(TA_T) ta_eval_kernel(const TaEval a) {
     if (j0 < i_end) {  // block-uniform: some query of this block has earlier events in the chunk
         const uint32_t j = j0 + threadIdx.x;
         if (j < a.E) {
-            s_key[threadIdx.x] = a.wkey[j];
-            s_d[threadIdx.x] = a.wdelta[j];
+            // the write event's key (its address block at this bit) and delta
+            // inc * has_write * address weight; no write: a key nothing matches
+            const K h = a.hw[j];
+            const bool w = !gl::kiszero(h);
+            s_key[threadIdx.x] = !w ? 0xFFFFFFFFu : (a.bit >= 32 ? 0u : (a.wa[j] >> a.bit));
+            s_d[threadIdx.x] = w ? gl::kmul(gl::kmul(a.inc[j], h), a.wpw[j]) : gl::kzero();
         }
         __syncthreads();
         if (q && i > j0) {
@@ -1238,21 +1289,54 @@ __global__ void __launch_bounds__(TA_T) ta_eval_kernel(const TaEval a) {
         if (lane == 0) s_red[x][warp] = v;
     }
     __syncthreads();
+    const uint64_t nb = (uint64_t)gridDim.x * gridDim.y;
     if (threadIdx.x < 3) {
         K s = gl::kzero();
         for (int w = 0; w < TA_T / 32; w++) s = gl::kadd(s, s_red[threadIdx.x][w]);
-        const uint64_t nb = (uint64_t)gridDim.x * gridDim.y;
         a.partials[(uint64_t)threadIdx.x * nb + (uint64_t)blockIdx.y * gridDim.x + blockIdx.x] = s;
+    }
+    // the last block to finish sums the partials (ticket, no waits)
+    __threadfence();
+    __syncthreads();
+    __shared__ unsigned int s_last;
+    if (threadIdx.x == 0) s_last = atomicInc(a.ticket, (unsigned int)(nb - 1)) == nb - 1;
+    __syncthreads();
+    if (!s_last) return;
+    __threadfence();
+    for (int x = 0; x < 3; x++) {
+        K v = gl::kzero();
+        for (uint64_t b = threadIdx.x; b < nb; b += TA_T) {
+            const ulonglong2 u = __ldcg(reinterpret_cast<const ulonglong2*>(a.partials + (uint64_t)x * nb + b));
+            v = gl::kadd(v, gl::kmk(u.x, u.y));
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v = gl::kadd(v, shfl_xor_km(v, o));
+        if (lane == 0) s_red[0][warp] = v;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            K t = gl::kzero();
+            for (int w = 0; w < TA_T / 32; w++) t = gl::kadd(t, s_red[0][w]);
+            a.out[x] = t;
+        }
+        __syncthreads();
     }
 }
 
+// One round's fold of the address lane: threads j < E fold the events'
+// address weights by the bound bit, the next `half` fold the initial-memory
+// table on its low address bit.
 __global__ void ta_fold_kernel(const uint32_t* __restrict__ ra, const uint32_t* __restrict__ wa, K* __restrict__ rpw,
-                               K* __restrict__ wpw, uint32_t E, uint32_t bit, K r, int kind) {
-    uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
-    if (j >= E) return;
-    const K omr = gl::ksub(gl::kone(), r);
-    if (kind == 0) rpw[j] = gl::kmul(rpw[j], ((ra[j] >> bit) & 1) ? r : omr);
-    wpw[j] = gl::kmul(wpw[j], ((wa[j] >> bit) & 1) ? r : omr);
+                               K* __restrict__ wpw, uint32_t E, uint32_t bit, K r, int kind, const K* __restrict__ tab,
+                               K* __restrict__ tab_out, uint64_t half) {
+    const uint64_t j = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+    if (j < E) {
+        const K omr = gl::ksub(gl::kone(), r);
+        if (kind == 0) rpw[j] = gl::kmul(rpw[j], ((ra[j] >> bit) & 1) ? r : omr);
+        wpw[j] = gl::kmul(wpw[j], ((wa[j] >> bit) & 1) ? r : omr);
+    } else if (j - E < half) {
+        const uint64_t p = j - E;
+        tab_out[p] = gl::klerp(tab[2 * p], tab[2 * p + 1], r);
+    }
 }
 
 __global__ void scatter_init_kernel(const uint64_t* __restrict__ addr, const K* __restrict__ val, uint64_t n,
@@ -1267,8 +1351,9 @@ struct neo_gpu_twist_addr {
     neo_gpu_ctx* ctx = nullptr;
     int kind = 0;
     uint32_t A = 0, bit = 0, E = 0;
-    DevBuf<K> eq, hr, rv, hw, inc, wv, rpw, wpw, wdelta, tab[2], partials, vals;
-    DevBuf<uint32_t> ra, wa, wkey;
+    DevBuf<K> eq, hr, rv, hw, inc, wv, rpw, wpw, tab[2], partials, vals;
+    DevBuf<uint32_t> ra, wa;
+    DevBuf<unsigned int> ticket;     // ta_eval_kernel's block counter (returns to zero after every launch)
     DevBuf<K> dcols, dr, dv;         // build workspace, kept for reuse
     DevBuf<uint32_t> counts;
     DevBuf<uint64_t> da;
@@ -1284,16 +1369,14 @@ namespace {
 int ta_apply_fold(neo_gpu_twist_addr* o) {
     neo_gpu_ctx* ctx = o->ctx;
     cudaStream_t S = ctx->stream;
-    if (o->E) {
-        ta_fold_kernel<<<ceil_div(o->E, 256), 256, 0, S>>>(o->ra.p, o->wa.p, o->rpw.p, o->wpw.p, o->E, o->bit,
-                                                         o->pending_r, o->kind);
+    // the events' address weights and the initial-memory table, one launch
+    const uint64_t half = o->tab_len >> 1;
+    const uint64_t n = o->E + half;
+    if (n) {
+        ta_fold_kernel<<<ceil_div(n, 256), 256, 0, S>>>(o->ra.p, o->wa.p, o->rpw.p, o->wpw.p, o->E, o->bit, o->pending_r,
+                                                       o->kind, o->tab[o->cur].p, o->tab[o->cur ^ 1].p, half);
         NEO_LAUNCHED(ctx);
     }
-    // fold the initial-memory table on its low address bit
-    const uint64_t half = o->tab_len >> 1;
-    mem_fold_kernel<<<ceil_div(half ? half : 1, 256), 256, 0, S>>>(o->tab[o->cur].p, o->tab_len, o->tab[o->cur ^ 1].p, 1,
-                                                                   o->pending_r);
-    NEO_LAUNCHED(ctx);
     o->cur ^= 1;
     o->tab_len = half;
     o->bit++;
@@ -1314,9 +1397,6 @@ int ta_values_launch(neo_gpu_twist_addr* o, K* d_dst) {
         NEO_CK(ctx, cudaMemsetAsync(d_dst, 0, 3 * sizeof(K), S));
         return NEO_OK;
     }
-    ta_prep_kernel<<<ceil_div(o->E, 256), 256, 0, S>>>(o->hw.p, o->inc.p, o->wa.p, o->wpw.p, o->E, o->bit, o->wkey.p,
-                                                     o->wdelta.p);
-    NEO_LAUNCHED(ctx);
     const uint32_t nbx = ceil_div(o->E, TA_T);
     const uint32_t nb = nbx * nbx;
     NEO_CK(ctx, o->partials.ensure((size_t)3 * nb));
@@ -1326,12 +1406,11 @@ int ta_values_launch(neo_gpu_twist_addr* o, K* d_dst) {
     a.bit = o->bit;
     a.eq = o->eq.p; a.hr = o->hr.p; a.rv = o->rv.p; a.hw = o->hw.p; a.inc = o->inc.p; a.wv = o->wv.p;
     a.rpw = o->rpw.p; a.wpw = o->wpw.p; a.ra = o->ra.p; a.wa = o->wa.p;
-    a.wkey = o->wkey.p; a.wdelta = o->wdelta.p;
     a.init_tab = o->tab[o->cur].p;
     a.partials = o->partials.p;
+    a.out = d_dst;
+    a.ticket = o->ticket.p;
     ta_eval_kernel<<<dim3(nbx, nbx), TA_T, 0, S>>>(a);
-    NEO_LAUNCHED(ctx);
-    mem_reduce_kernel<<<3, 256, 0, S>>>(o->partials.p, nb, d_dst);
     NEO_LAUNCHED(ctx);
     return NEO_OK;
 }
@@ -1404,10 +1483,11 @@ int ta_create(neo_gpu_ctx* ctx, int kind, uint32_t ell, const uint64_t* r_cycle,
     o->E = (uint32_t)E;
     const size_t ecap = E ? E : 1;
     if (o->eq.ensure(ecap) || o->hr.ensure(ecap) || o->rv.ensure(ecap) || o->hw.ensure(ecap) || o->inc.ensure(ecap) ||
-        o->wv.ensure(ecap) || o->rpw.ensure(ecap) || o->wpw.ensure(ecap) || o->wdelta.ensure(ecap) ||
-        o->ra.ensure(ecap) || o->wa.ensure(ecap) || o->wkey.ensure(ecap) || o->vals.ensure(3) ||
+        o->wv.ensure(ecap) || o->rpw.ensure(ecap) || o->wpw.ensure(ecap) ||
+        o->ra.ensure(ecap) || o->wa.ensure(ecap) || o->vals.ensure(3) || o->ticket.ensure(1) ||
         o->tab[0].ensure(P + 1) || o->tab[1].ensure(P / 2 + 1))
         return fail(ctx->fail(NEO_ERR_OOM, "twist_addr: event arrays"));
+    NEO_CK(ctx, cudaMemsetAsync(o->ticket.p, 0, sizeof(unsigned int), S));
     NEO_CK(ctx, cudaMemcpyAsync(counts.p, hc.data(), nblk * 4, cudaMemcpyHostToDevice, S));
     b.r_cycle = dr.p; b.ell = ell; b.A = A; b.L = L; b.offs = counts.p;
     b.eq = o->eq.p; b.ehr = o->hr.p; b.erv = o->rv.p; b.ehw = o->hw.p; b.einc = o->inc.p; b.ewv = o->wv.p;
