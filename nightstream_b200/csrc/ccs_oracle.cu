@@ -404,6 +404,61 @@ __global__ void eval_u_kernel(const int8_t* __restrict__ Z, uint64_t m, uint32_t
     u[c] = acc;
 }
 
+// u[c] of eval_u_kernel for ternary digit rows: the rows of instances 1..k-1
+// taken in pairs (q, q+1), whose 9 signed weight sums +-w[q] +- w[q+1] sit in
+// shared memory (the weights are the same for every column).  Thread = column,
+// blockIdx.y = a range of row pairs: one table entry per row pair added
+// unreduced in 128 bits; the last block of a column block (ticket) adds the
+// ranges' partials.
+constexpr uint32_t EU_MAX_PAIRS = 324;  // k <= 13
+constexpr uint32_t EU_SPLIT = 8;
+__global__ void __launch_bounds__(256) eval_u_pair_kernel(const int8_t* __restrict__ Z, uint64_t m, uint32_t k,
+                                                          const K* __restrict__ w, K* __restrict__ partials,
+                                                          unsigned int* __restrict__ tickets, K* __restrict__ u) {
+    __shared__ K tab[EU_MAX_PAIRS / EU_SPLIT + 1][9];
+    const uint32_t np = (k - 1) * NEO_D / 2;
+    const uint32_t per = (np + gridDim.y - 1) / gridDim.y;
+    const uint32_t g0 = blockIdx.y * per, g1 = min(np, g0 + per);
+    for (uint32_t i = threadIdx.x; i < (g1 > g0 ? g1 - g0 : 0) * 9; i += blockDim.x) {
+        const uint32_t g = g0 + i / 9, e = i % 9, q = NEO_D + 2 * g;
+        const K a = w[q], b = w[q + 1];
+        const uint32_t d0 = e % 3, d1 = e / 3;
+        K s2 = d0 == 0 ? gl::kneg(a) : (d0 == 2 ? a : gl::kzero());
+        tab[i / 9][e] = d1 == 0 ? gl::ksub(s2, b) : (d1 == 2 ? gl::kadd(s2, b) : s2);
+    }
+    __syncthreads();
+    const uint64_t c = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+    if (c < m) {
+        uint64_t lo0 = 0, hi0 = 0, lo1 = 0, hi1 = 0;
+        for (uint32_t g = g0; g < g1; g++) {
+            const uint64_t q = NEO_D + 2 * (uint64_t)g;
+            const int d0 = Z[q * m + c], d1 = Z[(q + 1) * m + c];
+            const K x = tab[g - g0][(uint32_t)(d0 + 1) + 3u * (uint32_t)(d1 + 1)];
+            lo0 += x.re;
+            hi0 += lo0 < x.re;
+            lo1 += x.im;
+            hi1 += lo1 < x.im;
+        }
+        K r;
+        r.re = gl::add(gl::canon(lo0), hi0 * 0xFFFFFFFFull);
+        r.im = gl::add(gl::canon(lo1), hi1 * 0xFFFFFFFFull);
+        partials[(uint64_t)blockIdx.y * m + c] = r;
+    }
+    __threadfence();
+    __syncthreads();
+    __shared__ unsigned int s_last;
+    if (threadIdx.x == 0) s_last = atomicInc(tickets + blockIdx.x, gridDim.y - 1) == gridDim.y - 1;
+    __syncthreads();
+    if (!s_last || c >= m) return;
+    __threadfence();
+    K a = gl::kzero();
+    for (uint32_t sp = 0; sp < gridDim.y; sp++) {
+        const ulonglong2 v = __ldcg(reinterpret_cast<const ulonglong2*>(partials + (uint64_t)sp * m + c));
+        a = gl::kadd(a, gl::kmk(v.x, v.y));
+    }
+    u[c] = a;
+}
+
 // eval[r] = sum_j coef_j (M_j u)[r]
 __global__ void eval_tbl_kernel(const uint64_t* __restrict__ row_ptr, const uint32_t* __restrict__ col,
                                 const uint64_t* __restrict__ val, const uint64_t* __restrict__ nnz_off,
@@ -694,7 +749,8 @@ struct neo_gpu_ccs_oracle {
     bool have_pre = false;
     DevBuf<K> chi_r, vj, y_eval, y_sc;
     // build temporaries, kept across re-initialisations
-    DevBuf<K> ws_bits, ws_w, ws_coef, ws_u;
+    DevBuf<K> ws_bits, ws_w, ws_coef, ws_u, ws_upart;  // ws_upart: eval_u_pair_kernel partials
+    DevBuf<unsigned int> ws_uticket;
     DevBuf<uint64_t> ws_z1, ws_nnzoff;
     DevBuf<uint8_t> ws_isid;
 };
@@ -797,6 +853,23 @@ static int oracle_init(neo_gpu_ctx* ctx, neo_gpu_ccs_oracle* o, const int8_t* d_
     o->has_inputs = r_inputs != nullptr;
     if (o->has_inputs) o->r_in.assign(r_inputs, r_inputs + ell_n);
     o->has_eval = o->has_inputs && k >= 2;
+    // every digit in {-1, 0, 1}?  Ternary digits (every witness the fold step
+    // builds: balanced base-2 decomposition and split_b) take the
+    // pattern-histogram row rounds and the pair-table kernels; any other digit
+    // keeps the streaming kernels
+    uint32_t h_bad = 1;
+    if (ell_n >= 3) {
+        NEO_CK(ctx, o->tern_flag.ensure(1));
+        NEO_CK(ctx, cudaMemsetAsync(o->tern_flag.p, 0, 4, ctx->stream));
+        const uint64_t nbytes = (uint64_t)k * NEO_D * cc.m;
+        ternary_check_kernel<<<148 * 4, 256, 0, ctx->stream>>>(reinterpret_cast<const uint4*>(o->Z), nbytes / 16,
+                                                              reinterpret_cast<const uint8_t*>(o->Z) + nbytes / 16 * 16,
+                                                              (uint32_t)(nbytes % 16), o->tern_flag.p);
+        NEO_LAUNCHED(ctx);
+        NEO_CK(ctx, ctx_d2h(ctx, &h_bad, o->tern_flag.p, 4));
+    }
+    NEO_CK(ctx, ctx_sync(ctx));
+    o->fast = h_bad == 0;
     struct { uint32_t n, m, n_terms; const uint32_t* f_exps; const uint64_t* f_coeff; } dd{
         cc.n, cc.m, cc.n_terms, cc.f_exps.data(), cc.f_coeff.data()};
     const auto* desc = &dd;
@@ -895,7 +968,16 @@ static int oracle_init(neo_gpu_ctx* ctx, neo_gpu_ccs_oracle* o, const int8_t* d_
         NEO_CK(ctx, du.ensure(m));
         NEO_CK(ctx, cudaMemcpyAsync(dw.p, w.data(), nq * 16, cudaMemcpyHostToDevice, ctx->stream));
         NEO_CK(ctx, cudaMemcpyAsync(dcoef.p, coef.data(), t * 16, cudaMemcpyHostToDevice, ctx->stream));
-        eval_u_kernel<<<ceil_div(m, 256), 256, 0, ctx->stream>>>(o->Z, m, k, dw.p, du.p);
+        if (o->fast && (k - 1) * NEO_D / 2 <= EU_MAX_PAIRS) {  // ternary digits (checked above)
+            const uint32_t cb = (uint32_t)ceil_div(m, 256);
+            NEO_CK(ctx, o->ws_upart.ensure((size_t)EU_SPLIT * m));
+            NEO_CK(ctx, o->ws_uticket.ensure(cb));
+            NEO_CK(ctx, cudaMemsetAsync(o->ws_uticket.p, 0, cb * sizeof(unsigned int), ctx->stream));
+            eval_u_pair_kernel<<<dim3(cb, EU_SPLIT), 256, 0, ctx->stream>>>(o->Z, m, k, dw.p, o->ws_upart.p,
+                                                                         o->ws_uticket.p, du.p);
+        } else {
+            eval_u_kernel<<<ceil_div(m, 256), 256, 0, ctx->stream>>>(o->Z, m, k, dw.p, du.p);
+        }
         NEO_LAUNCHED(ctx);
         DevBuf<uint8_t>& isid = o->ws_isid;
         NEO_CK(ctx, isid.ensure(t));
@@ -922,23 +1004,7 @@ static int oracle_init(neo_gpu_ctx* ctx, neo_gpu_ccs_oracle* o, const int8_t* d_
     NEO_CK(ctx, o->partials.ensure(max_blocks * (o->deg_max + 1)));
     NEO_CK(ctx, o->coeffs.ensure(MAX_DEG + 1));
     NEO_CK(ctx, o->ys.ensure(16));
-    // ternary digits (every witness the fold step builds: balanced base-2
-    // decomposition and split_b) take the pattern-histogram path; any other
-    // digit keeps the streaming kernels above
-    uint32_t h_bad = 1;
-    if (ell_n >= 3) {
-        NEO_CK(ctx, o->tern_flag.ensure(1));
-        NEO_CK(ctx, cudaMemsetAsync(o->tern_flag.p, 0, 4, ctx->stream));
-        const uint64_t nbytes = (uint64_t)nq * m;
-        ternary_check_kernel<<<148 * 4, 256, 0, ctx->stream>>>(reinterpret_cast<const uint4*>(o->Z), nbytes / 16,
-                                                              reinterpret_cast<const uint8_t*>(o->Z) + nbytes / 16 * 16,
-                                                              (uint32_t)(nbytes % 16), o->tern_flag.p);
-        NEO_LAUNCHED(ctx);
-        NEO_CK(ctx, ctx_d2h(ctx, &h_bad, o->tern_flag.p, 4));
-    }
-    NEO_CK(ctx, ctx_sync(ctx));
-    o->fast = h_bad == 0;
-    if (o->fast) {
+    if (o->fast) {  // the pattern-histogram row rounds
         int rc2 = fast_setup(o);
         if (rc2) return rc2;
     }
@@ -1265,7 +1331,8 @@ static int ajtai_precompute(neo_gpu_ccs_oracle* o) {
     NEO_CK(ctx, cudaMemcpyAsync(dbits.p, o->row_chals.data(), o->ell_n * 16, cudaMemcpyHostToDevice, ctx->stream));
     int rc = launch_chi_table(ctx, dbits.p, o->ell_n, o->chi_r.p);
     if (rc) return rc;
-    rc = launch_me_y(ctx, *o->ccs, o->Z, o->k, o->m, o->chi_r.p, o->ell_n, o->b, o->vj.p, o->y_eval.p, o->y_sc.p);
+    rc = launch_me_y(ctx, *o->ccs, o->Z, o->k, o->m, o->chi_r.p, o->ell_n, o->b, o->vj.p, o->y_eval.p, o->y_sc.p,
+                     o->fast);  // fast: every digit checked ternary at creation
     if (rc) return rc;
     NEO_CK(ctx, ctx_sync(ctx));
     o->have_pre = true;

@@ -496,6 +496,117 @@ __global__ void __launch_bounds__(256) zv_dot_kernel(const int8_t* __restrict__ 
     }
 }
 
+// y[row][j] = sum_c Z[row][c] v[j][c] for ternary digit rows (the ME
+// outputs y = Z M_j^T chi_r of compute_y_from_Z_and_r,
+// crates/neo-reductions/src/common.rs:582-650, for many rows at once).  A
+// block holds 128 rows (one per thread) and a range of columns; per chunk of
+// 64 columns the 9 signed sums (d0 v[c] + d1 v[c+1], d in {-1,0,1}) of every
+// column pair are tabulated in shared memory once for the block's rows, and a
+// row adds one table entry per pair (index from its two digits), summed
+// unreduced in 128 bits.  v is read once per 128 rows instead of once per row.
+// The last block of a row group (ticket) adds the column ranges' partials.
+constexpr int ZR_ROWS = 128, ZR_CHUNK = 64, ZR_TMAX = 4;
+constexpr int ZR_TPAD = 5;  // entry stride 80 B: the 9 entries of a pair fall on distinct bank groups
+__global__ void __launch_bounds__(ZR_ROWS) zrows_kernel(const int8_t* __restrict__ Z, uint32_t R, uint64_t m,
+                                                        uint32_t t, const K* __restrict__ v, uint64_t cols_per_split,
+                                                        K* __restrict__ partials, unsigned int* __restrict__ tickets,
+                                                        K* __restrict__ y) {
+    __shared__ K tab[ZR_CHUNK / 2][9][ZR_TPAD];
+    const uint32_t row = blockIdx.x * ZR_ROWS + threadIdx.x;
+    const uint64_t c_lo = blockIdx.y * cols_per_split, c_hi = min(m, c_lo + cols_per_split);
+    uint64_t lo[2 * ZR_TMAX], hi[2 * ZR_TMAX];
+#pragma unroll
+    for (int i = 0; i < 2 * ZR_TMAX; i++) lo[i] = hi[i] = 0;
+    for (uint64_t c0 = c_lo; c0 < c_hi; c0 += ZR_CHUNK) {
+        const uint32_t np = (uint32_t)(min((uint64_t)ZR_CHUNK, c_hi - c0) / 2);  // column pairs of this chunk
+        __syncthreads();  // the previous chunk's table is no longer read
+        for (uint32_t i = threadIdx.x; i < np * 9 * t; i += ZR_ROWS) {
+            const uint32_t j = i % t, e = (i / t) % 9, g = i / (9 * t);
+            const K a = v[(uint64_t)j * m + c0 + 2 * g], b = v[(uint64_t)j * m + c0 + 2 * g + 1];
+            const uint32_t d0 = e % 3, d1 = e / 3;  // digit + 1
+            K s = d0 == 0 ? gl::kneg(a) : (d0 == 2 ? a : gl::kzero());
+            s = d1 == 0 ? gl::ksub(s, b) : (d1 == 2 ? gl::kadd(s, b) : s);
+            tab[g][e][j] = s;
+        }
+        __syncthreads();
+        if (row >= R) continue;
+        const uint4* zr = reinterpret_cast<const uint4*>(Z + (uint64_t)row * m + c0);
+        for (uint32_t g0 = 0; g0 < np; g0 += 8) {  // 16 digits per load
+            const uint4 zz = __ldg(zr + g0 / 8);
+            const uint32_t w[4] = {zz.x, zz.y, zz.z, zz.w};
+#pragma unroll
+            for (int k = 0; k < 8; k++) {
+                const uint32_t word = w[k >> 1] >> (16 * (k & 1));
+                const int d0 = (int8_t)(word & 0xFF), d1 = (int8_t)((word >> 8) & 0xFF);
+                const uint32_t e = (uint32_t)(d0 + 1) + 3u * (uint32_t)(d1 + 1);  // entry 4 (both zero) is zero
+#pragma unroll
+                for (int j = 0; j < ZR_TMAX; j++) {
+                    if (j >= (int)t) break;
+                    const K x = tab[g0 + k][e][j];
+                    uint64_t s0 = lo[2 * j] + x.re;
+                    hi[2 * j] += s0 < x.re;
+                    lo[2 * j] = s0;
+                    uint64_t s1 = lo[2 * j + 1] + x.im;
+                    hi[2 * j + 1] += s1 < x.im;
+                    lo[2 * j + 1] = s1;
+                }
+            }
+        }
+    }
+    // lo + 2^64 hi (mod q) with 2^64 = 2^32 - 1; hi < 2^16
+    if (row < R) {
+#pragma unroll
+        for (int j = 0; j < ZR_TMAX; j++) {
+            if (j >= (int)t) break;
+            K r;
+            r.re = gl::add(gl::canon(lo[2 * j]), hi[2 * j] * 0xFFFFFFFFull);
+            r.im = gl::add(gl::canon(lo[2 * j + 1]), hi[2 * j + 1] * 0xFFFFFFFFull);
+            partials[((uint64_t)blockIdx.y * R + row) * t + j] = r;
+        }
+    }
+    __threadfence();
+    __syncthreads();
+    __shared__ unsigned int s_last;
+    if (threadIdx.x == 0) s_last = atomicInc(tickets + blockIdx.x, gridDim.y - 1) == gridDim.y - 1;
+    __syncthreads();
+    if (!s_last || row >= R) return;
+    __threadfence();
+    for (uint32_t j = 0; j < t; j++) {
+        K a = gl::kzero();
+        for (uint32_t sp = 0; sp < gridDim.y; sp++) {
+            const ulonglong2 u = __ldcg(reinterpret_cast<const ulonglong2*>(partials + ((uint64_t)sp * R + row) * t + j));
+            a = gl::kadd(a, gl::kmk(u.x, u.y));
+        }
+        const uint32_t w = row / NEO_D, rho = row % NEO_D;
+        y[((uint64_t)w * t + j) * NEO_D + rho] = a;
+    }
+}
+
+// y of R ternary digit rows (layout [w][t][54], row = w * 54 + rho); false
+// when the shape does not suit zrows_kernel (the caller keeps its kernel)
+int launch_zrows(neo_gpu_ctx* ctx, const int8_t* d_Z, uint32_t R, uint64_t m, uint32_t t, const K* d_v, K* d_y,
+                 bool* done) {
+    *done = false;
+    if (t == 0 || t > ZR_TMAX || m % ZR_CHUNK || R == 0) return NEO_OK;
+    const uint32_t groups = (R + ZR_ROWS - 1) / ZR_ROWS;
+    const uint64_t chunks = m / ZR_CHUNK;
+    // about 8 blocks of 128 rows per SM (latency-bound loop: occupancy hides it)
+    uint64_t splits = std::min<uint64_t>(chunks, std::max<uint64_t>(1, (8 * 148 + groups - 1) / groups));
+    const uint64_t cps = ((chunks + splits - 1) / splits) * ZR_CHUNK;
+    splits = (m + cps - 1) / cps;
+    const size_t part_bytes = (size_t)splits * R * t * sizeof(K);
+    void* scratch = nullptr;
+    NEO_CK(ctx, ctx_scratch(ctx, part_bytes + 256 + groups * sizeof(unsigned int), &scratch));
+    K* partials = reinterpret_cast<K*>(scratch);
+    unsigned int* tickets = reinterpret_cast<unsigned int*>(reinterpret_cast<uint8_t*>(scratch) + part_bytes + 256);
+    NEO_CK(ctx, cudaMemsetAsync(tickets, 0, groups * sizeof(unsigned int), ctx->stream));
+    zrows_kernel<<<dim3(groups, (uint32_t)splits), ZR_ROWS, 0, ctx->stream>>>(d_Z, R, m, t, d_v, cps, partials, tickets,
+                                                                               d_y);
+    NEO_LAUNCHED(ctx);
+    *done = true;
+    return NEO_OK;
+}
+
 __global__ void y_scalars_kernel(const K* __restrict__ y, uint32_t count, uint32_t b, K* __restrict__ ysc) {
     uint32_t q = blockIdx.x * blockDim.x + threadIdx.x;  // (w, j)
     if (q >= count) return;
@@ -509,7 +620,7 @@ __global__ void y_scalars_kernel(const K* __restrict__ y, uint32_t count, uint32
 }
 
 int launch_me_y(neo_gpu_ctx* ctx, const DevCcs& ccs, const int8_t* d_Z, uint32_t n_w, uint64_t m, const K* d_chi,
-                uint32_t ell_n, uint32_t b, K* d_vj, K* d_y, K* d_ysc) {
+                uint32_t ell_n, uint32_t b, K* d_vj, K* d_y, K* d_ysc, bool ternary) {
     uint64_t n_sz = 1ULL << ell_n;
     for (uint32_t j = 0; j < ccs.t; j++) {
         matT_chi_kernel<<<ceil_div(m, 256), 256, 0, ctx->stream>>>(
@@ -517,11 +628,16 @@ int launch_me_y(neo_gpu_ctx* ctx, const DevCcs& ccs, const int8_t* d_Z, uint32_t
             ccs.is_identity[j], ccs.n, (uint32_t)m, n_sz, d_chi, d_vj + (size_t)j * m);
         NEO_LAUNCHED(ctx);
     }
-    if (ccs.t <= 4)
-        zv_dot_kernel<4><<<n_w * NEO_D, 256, 0, ctx->stream>>>(d_Z, m, ccs.t, d_vj, d_y);
-    else
-        zv_dot_kernel<16><<<n_w * NEO_D, 256, 0, ctx->stream>>>(d_Z, m, ccs.t, d_vj, d_y);
-    NEO_LAUNCHED(ctx);
+    bool done = false;
+    if (ternary)
+        if (int rc = launch_zrows(ctx, d_Z, n_w * NEO_D, m, ccs.t, d_vj, d_y, &done)) return rc;
+    if (!done) {
+        if (ccs.t <= 4)
+            zv_dot_kernel<4><<<n_w * NEO_D, 256, 0, ctx->stream>>>(d_Z, m, ccs.t, d_vj, d_y);
+        else
+            zv_dot_kernel<16><<<n_w * NEO_D, 256, 0, ctx->stream>>>(d_Z, m, ccs.t, d_vj, d_y);
+        NEO_LAUNCHED(ctx);
+    }
     if (d_ysc) {
         y_scalars_kernel<<<ceil_div(n_w * ccs.t, 64), 64, 0, ctx->stream>>>(d_y, n_w * ccs.t, b, d_ysc);
         NEO_LAUNCHED(ctx);

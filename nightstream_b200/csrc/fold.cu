@@ -1106,8 +1106,14 @@ static int rlc_dec_lane(neo_gpu_shard* sh, const char* lane, uint32_t idx, const
     // Pi_DEC: split into k_rho planes, commit, child claims
     if ((rc = split_b_device(ctx, sh->d_mix.p, (uint64_t)NEO_D * m, sh->k_rho, sh->b, d_planes, sh->d_flags.p))) return rc;
     if ((rc = launch_commit(ctx, d_planes, sh->k_rho, m, sh->d_commits.p, TC_DIGITS_SMALL))) return rc;  // planes in {-1, 0, 1}
-    child_y_kernel<<<sh->k_rho * NEO_D, 256, 0, ctx->stream>>>(d_planes, m, t, d_vj, sh->d_ychild.p);
-    NEO_LAUNCHED(ctx);
+    {  // children's y at r: the planes are ternary
+        bool done = false;
+        if ((rc = launch_zrows(ctx, d_planes, sh->k_rho * NEO_D, m, t, d_vj, sh->d_ychild.p, &done))) return rc;
+        if (!done) {
+            child_y_kernel<<<sh->k_rho * NEO_D, 256, 0, ctx->stream>>>(d_planes, m, t, d_vj, sh->d_ychild.p);
+            NEO_LAUNCHED(ctx);
+        }
+    }
     uint32_t flags[2];
     std::vector<uint64_t> cc((size_t)sh->k_rho * kappa * NEO_D);
     std::vector<K> yc((size_t)sh->k_rho * t * NEO_D);
@@ -1782,7 +1788,7 @@ static int fold_step_impl(neo_gpu_shard* sh, const uint64_t* z_host, const uint6
         if ((rc = upload_point(sh, r_val))) return rc;
         if ((rc = launch_chi_table(ctx, sh->d_r.p, ell_n, sh->d_chi.p))) return rc;
         if ((rc = launch_me_y(ctx, sh->ccs, sh->valwit.p, nv, m, sh->d_chi.p, ell_n, sh->b, sh->d_vj.p, sh->d_yv.p,
-                              sh->d_yvsc.p)))
+                              sh->d_yvsc.p, true)))
             return rc;
         std::vector<K> yv((size_t)nv * t * NEO_D), yvsc((size_t)nv * t);
         NEO_CK(ctx, ctx_d2h(ctx, yv.data(), sh->d_yv.p, yv.size() * sizeof(K)));

@@ -197,7 +197,11 @@ int launch_chi_table(neo_gpu_ctx* ctx, const gl::K* d_bits, uint32_t nbits, gl::
 int launch_suffix_chi_tables(neo_gpu_ctx* ctx, const gl::K* d_bits, uint32_t nbits, gl::K* d_out);
 int launch_me_y(neo_gpu_ctx* ctx, const DevCcs& ccs, const int8_t* d_Z, uint32_t n_w, uint64_t m,
                 const gl::K* d_chi, uint32_t ell_n, uint32_t b, gl::K* d_vj_scratch, gl::K* d_y,
-                gl::K* d_ysc);
+                gl::K* d_ysc, bool ternary = false);
+// y[row][j] = sum_c Z[row][c] v[j][c] of R ternary digit rows (y layout [w][t][54]); *done = false
+// (nothing launched) when m % 64 != 0 or t > 4
+int launch_zrows(neo_gpu_ctx* ctx, const int8_t* d_Z, uint32_t R, uint64_t m, uint32_t t, const gl::K* d_v,
+                 gl::K* d_y, bool* done);
 // What the caller knows about the digits of a commitment: any int8
 // (TC_DIGITS_ANY: the cyclic tensor-core form), |digit| <= 63 by construction
 // (TC_DIGITS_SMALL: the small-digit form, a violation is reported through the
