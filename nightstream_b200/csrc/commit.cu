@@ -103,8 +103,8 @@ int launch_commit(neo_gpu_ctx* ctx, const int8_t* d_digits, uint32_t n_vec, uint
         // tensor-core path (commit_tc.cu); scratch for every form the call may take
         uint32_t g, k, kb;
         size_t need = 0;
-        if (digits != TC_DIGITS_ANY) need = tc_scratch_bytes(n_vec, m, true, &g, &k, &kb);
-        if (digits != TC_DIGITS_SMALL) need = std::max(need, tc_scratch_bytes(n_vec, m, false, &g, &k, &kb));
+        if (digits != TC_DIGITS_ANY) need = tc_scratch_bytes(n_vec, m, true, pp->kappa, &g, &k, &kb);
+        if (digits != TC_DIGITS_SMALL) need = std::max(need, tc_scratch_bytes(n_vec, m, false, pp->kappa, &g, &k, &kb));
         void* scratch = nullptr;
         NEO_CK(ctx, ctx_scratch(ctx, need, &scratch));
         return launch_commit_tc(ctx, pp, d_digits, n_vec, d_out, (uint8_t*)scratch, ctx->d_err, digits);

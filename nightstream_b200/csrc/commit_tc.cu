@@ -497,40 +497,56 @@ __device__ __forceinline__ int zat(const int (&z)[NEO_D], int x) { return (x >= 
 
 // prep: the two window sequences of every (vector, column); a digit pair whose
 // window entry leaves int8 sets bit 16 of *err (the caller then takes the
-// cyclic form, or reports the error)
-__global__ void p8_seq_kernel(const int8_t* __restrict__ digits, uint32_t n_vec, uint64_t m, uint8_t* __restrict__ F,
-                              uint32_t* __restrict__ err) {
-    const uint64_t tid = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
-    if (tid >= (uint64_t)n_vec * m) return;
-    const uint64_t v = tid / m, j = tid % m;
-    int z[NEO_D];
-    const int8_t* zv = digits + v * NEO_D * m + j;
+// cyclic form, or reports the error).  A block's 128 outputs are contiguous
+// (28 KB), so each thread writes its 224 bytes into shared memory (pitch 240 B:
+// an odd count of 16-byte chunks keeps a store phase on eight bank groups) and
+// the block copies them out with consecutive 16-byte stores.
+constexpr int P8_SEQ_THREADS = 128;
+constexpr int P8_SEQ_PITCH = P8_FBYTES + 16;
+__global__ void __launch_bounds__(P8_SEQ_THREADS) p8_seq_kernel(const int8_t* __restrict__ digits, uint32_t n_vec,
+                                                                uint64_t m, uint8_t* __restrict__ F,
+                                                                uint32_t* __restrict__ err) {
+    __shared__ __align__(16) uint8_t s_out[P8_SEQ_THREADS * P8_SEQ_PITCH];
+    const uint64_t total = (uint64_t)n_vec * m;
+    const uint64_t base = (uint64_t)blockIdx.x * P8_SEQ_THREADS;
+    const uint64_t tid = base + threadIdx.x;
+    if (tid < total) {
+        const uint64_t v = tid / m, j = tid % m;
+        int z[NEO_D];
+        const int8_t* zv = digits + v * NEO_D * m + j;
 #pragma unroll
-    for (int x = 0; x < NEO_D; x++) z[x] = zv[(uint64_t)x * m];
-    uint4* dst = reinterpret_cast<uint4*>(F + tid * P8_FBYTES);
-    bool bad = false;
+        for (int x = 0; x < NEO_D; x++) z[x] = zv[(uint64_t)x * m];
+        uint4* dst = reinterpret_cast<uint4*>(s_out + threadIdx.x * P8_SEQ_PITCH);
+        bool bad = false;
 #pragma unroll
-    for (int seq = 0; seq < 2; seq++) {
+        for (int seq = 0; seq < 2; seq++) {
 #pragma unroll
-        for (int q = 0; q < P8_HSEQ / 16; q++) {
-            uint32_t w4[4];
+            for (int q = 0; q < P8_HSEQ / 16; q++) {
+                uint32_t w4[4];
 #pragma unroll
-            for (int e = 0; e < 4; e++) {
-                uint32_t word = 0;
+                for (int e = 0; e < 4; e++) {
+                    uint32_t word = 0;
 #pragma unroll
-                for (int b = 0; b < 4; b++) {
-                    const int w = q * 16 + e * 4 + b;
-                    const int h = seq == 0 ? zat(z, 58 - w) - zat(z, 85 - w)
-                                           : zat(z, 31 - w) - zat(z, 85 - w) + zat(z, 112 - w);
-                    bad |= h < -128 || h > 127;
-                    word |= (uint32_t)(uint8_t)(int8_t)h << (8 * b);
+                    for (int b = 0; b < 4; b++) {
+                        const int w = q * 16 + e * 4 + b;
+                        const int h = seq == 0 ? zat(z, 58 - w) - zat(z, 85 - w)
+                                               : zat(z, 31 - w) - zat(z, 85 - w) + zat(z, 112 - w);
+                        bad |= h < -128 || h > 127;
+                        word |= (uint32_t)(uint8_t)(int8_t)h << (8 * b);
+                    }
+                    w4[e] = word;
                 }
-                w4[e] = word;
+                dst[seq * (P8_HSEQ / 16) + q] = make_uint4(w4[0], w4[1], w4[2], w4[3]);
             }
-            dst[seq * (P8_HSEQ / 16) + q] = make_uint4(w4[0], w4[1], w4[2], w4[3]);
         }
+        if (bad) atomicOr(err, 1u << 16);
     }
-    if (bad) atomicOr(err, 1u << 16);
+    __syncthreads();
+    const uint32_t cnt = (uint32_t)min((uint64_t)P8_SEQ_THREADS, total - base);
+    constexpr uint32_t CH = P8_FBYTES / 16;  // 14 chunks per output
+    uint4* out = reinterpret_cast<uint4*>(F + base * P8_FBYTES);
+    for (uint32_t k = threadIdx.x; k < cnt * CH; k += P8_SEQ_THREADS)
+        out[k] = *reinterpret_cast<const uint4*>(s_out + (k / CH) * P8_SEQ_PITCH + (k % CH) * 16);
 }
 
 template <int NV>
@@ -649,11 +665,26 @@ __global__ void __launch_bounds__(P8<NV>::THREADS, P8<NV>::CTAS) commit_p8_kerne
             if (st) break;
             if (active) {
                 const int sa = it % S::ASTAGES;
-                const uint32_t* src = reinterpret_cast<const uint32_t*>(sF + sa * S::F_STAGE + (v * 2 + jj) * P8_FBYTES +
-                                                                        seq * P8_HSEQ) + (p >> 2);
-                uint32_t w[21];  // words [p/4, p/4 + 21): bytes < 96 of the 112-byte sequence
+                // bytes [0, 96) of the sequence as six 16-byte loads (the warp's
+                // two sequences: one wavefront each), then words [p/4, p/4 + 21)
+                // selected in registers
+                const uint4* src = reinterpret_cast<const uint4*>(sF + sa * S::F_STAGE + (v * 2 + jj) * P8_FBYTES +
+                                                                  seq * P8_HSEQ);
+                uint32_t u[24];
 #pragma unroll
-                for (int q = 0; q < 21; q++) w[q] = src[q];
+                for (int q = 0; q < 6; q++) {
+                    const uint4 t = src[q];
+                    u[4 * q] = t.x;
+                    u[4 * q + 1] = t.y;
+                    u[4 * q + 2] = t.z;
+                    u[4 * q + 3] = t.w;
+                }
+                uint32_t x[22];
+#pragma unroll
+                for (int q = 0; q < 22; q++) x[q] = (p & 8) ? u[q + 2] : u[q];
+                uint32_t w[21];
+#pragma unroll
+                for (int q = 0; q < 21; q++) w[q] = (p & 4) ? x[q + 1] : x[q];
                 const uint32_t sh = 8 * (p & 3);
                 uint8_t* dst = sB + sb * S::B_BYTES + jj * S::BCOL + (p >> 3) * (2 * NV * 128) + seq * (NV * 128) +
                                v * 128 + (p & 7) * 16;
@@ -702,22 +733,55 @@ __global__ void __launch_bounds__(P8<NV>::THREADS, P8<NV>::CTAS) commit_p8_kerne
 
 // c_{v,i}[r] = sum_{ks} sum_l 2^(8l) D[ks][(i,l)][col] mod q for the column
 // col of row r (no fold: the small-digit form computes mod Phi_81 directly).
+// Block (group·kappa + i, y) sums the K splits [y n/S, (y+1) n/S) of row i
+// (its two halves take alternate splits) into int64 slice sums; the last block
+// of a row (ticket) adds the S slices and reduces mod q.  With S slices per row
+// the grid fills the GPU even for a single vector (kappa rows).
 template <int NV>
 __global__ void __launch_bounds__(2 * P8<NV>::NPAD) commit_p8_reduce_kernel(const int32_t* __restrict__ partial,
                                                                             uint32_t n_groups, uint32_t n_ksplit,
                                                                             uint32_t kappa, uint32_t n_vec,
+                                                                            int64_t* __restrict__ slices,
+                                                                            uint32_t* __restrict__ tickets,
                                                                             uint64_t* __restrict__ out) {
     constexpr int NP = P8<NV>::NPAD;
-    const uint32_t group = blockIdx.x / kappa, i = blockIdx.x % kappa;
+    const uint32_t row = blockIdx.x, S = gridDim.y, y = blockIdx.y;
+    const uint32_t group = row / kappa, i = row % kappa;
     const int col = threadIdx.x % NP, half = threadIdx.x / NP;
     __shared__ int64_t s_acc[NP][8];
+    __shared__ bool s_last;
     int64_t acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-    const uint32_t ks0 = half ? n_ksplit / 2 : 0, ks1 = half ? n_ksplit : n_ksplit / 2;
-    for (uint32_t ks = ks0; ks < ks1; ks++) {
+    const uint32_t ks0 = (uint32_t)((uint64_t)y * n_ksplit / S), ks1 = (uint32_t)((uint64_t)(y + 1) * n_ksplit / S);
+    for (uint32_t ks = ks0 + half; ks < ks1; ks += 2) {
         const int32_t* pp = partial + ((uint64_t)(ks * n_groups + group) * 128 + i * 8) * NP + col;
 #pragma unroll
         for (int l = 0; l < 8; l++) acc[l] += pp[(uint64_t)l * NP];
     }
+    if (half) {
+#pragma unroll
+        for (int l = 0; l < 8; l++) s_acc[col][l] = acc[l];
+    }
+    __syncthreads();
+    int64_t* mine = slices + ((uint64_t)row * S + y) * 8 * NP;
+    if (!half) {
+#pragma unroll
+        for (int l = 0; l < 8; l++) mine[l * NP + col] = acc[l] + s_acc[col][l];
+    }
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) s_last = atomicInc(tickets + row, S - 1) == S - 1;
+    __syncthreads();
+    if (!s_last) return;
+    __threadfence();
+    // last block: half h adds the slices y = h, h + 2, ...
+#pragma unroll
+    for (int l = 0; l < 8; l++) acc[l] = 0;
+    for (uint32_t yy = half; yy < S; yy += 2) {
+        const int64_t* sl = slices + ((uint64_t)row * S + yy) * 8 * NP + col;
+#pragma unroll
+        for (int l = 0; l < 8; l++) acc[l] += __ldcg(sl + l * NP);
+    }
+    __syncthreads();
     if (half) {
 #pragma unroll
         for (int l = 0; l < 8; l++) s_acc[col][l] = acc[l];
@@ -755,8 +819,15 @@ int tc_pp_prepare(neo_gpu_ctx* ctx, PPEntry* pp) {
 // vectors) and groups of 4 otherwise.
 static uint32_t tc_nv(uint32_t n_vec, bool small) { return small && n_vec == 1 ? 1 : 4; }
 
-size_t tc_scratch_bytes(uint32_t n_vec, uint64_t m, bool small, uint32_t* n_groups_out, uint32_t* n_ksplit_out,
-                        uint32_t* kb_per_cta_out) {
+// K-split slices per row of the small-digit reduce: about two blocks per SM
+static uint32_t p8_slices(uint32_t n_groups, uint32_t kappa, uint32_t n_ksplit) {
+    const uint32_t rows = n_groups * kappa;
+    uint32_t s = (2 * 148 + rows - 1) / rows;
+    return std::max(1u, std::min(s, n_ksplit));
+}
+
+size_t tc_scratch_bytes(uint32_t n_vec, uint64_t m, bool small, uint32_t kappa, uint32_t* n_groups_out,
+                        uint32_t* n_ksplit_out, uint32_t* kb_per_cta_out) {
     const uint32_t nv = tc_nv(n_vec, small);
     const uint32_t n_groups = (n_vec + nv - 1) / nv;
     const uint32_t n_kb = (uint32_t)(m / 2);
@@ -777,19 +848,27 @@ size_t tc_scratch_bytes(uint32_t n_vec, uint64_t m, bool small, uint32_t* n_grou
     const size_t fb = small ? P8_FBYTES : TC_FBYTES, npad = small ? 64 * nv : TC_NPAD;
     size_t f_bytes = (size_t)n_vec * m * fb + 64;
     size_t p_bytes = (size_t)n_groups * n_ksplit * 128 * npad * 4;
-    return ((f_bytes + 255) & ~size_t(255)) + p_bytes + 256 /*flag*/ + 256;
+    // small form: the reduce's int64 slice sums and one ticket per row
+    size_t r_bytes = small ? (size_t)n_groups * kappa * p8_slices(n_groups, kappa, n_ksplit) * 8 * npad * 8 +
+                                 (((size_t)n_groups * kappa * 4 + 255) & ~size_t(255))
+                           : 0;
+    return ((f_bytes + 255) & ~size_t(255)) + p_bytes + r_bytes + 256 /*flag*/ + 256;
 }
 
 template <int NV>
-static int launch_p8(neo_gpu_ctx* ctx, const TcArgs& a, uint32_t kappa, uint64_t* d_out) {
+static int launch_p8(neo_gpu_ctx* ctx, const TcArgs& a, uint32_t kappa, uint8_t* red, uint64_t* d_out) {
     using S = P8<NV>;
     const size_t smem = S::SMEM + 1024 /*align*/ + 256 /*barriers*/;
     static SmemLimit limit;
     NEO_CK(ctx, limit.at_least(commit_p8_kernel<NV>, smem));
+    const uint32_t rows = a.n_groups * kappa, ns = p8_slices(a.n_groups, kappa, a.n_ksplit);
+    int64_t* slices = reinterpret_cast<int64_t*>(red);
+    uint32_t* tickets = reinterpret_cast<uint32_t*>(red + (size_t)rows * ns * 8 * S::NPAD * 8);
+    NEO_CK(ctx, cudaMemsetAsync(tickets, 0, (size_t)rows * 4, ctx->stream));
     commit_p8_kernel<NV><<<a.n_groups * a.n_ksplit, S::THREADS, smem, ctx->stream>>>(a);
     NEO_LAUNCHED(ctx);
-    commit_p8_reduce_kernel<NV><<<a.n_groups * kappa, 2 * S::NPAD, 0, ctx->stream>>>(a.partial, a.n_groups, a.n_ksplit,
-                                                                                     kappa, a.n_vec, d_out);
+    commit_p8_reduce_kernel<NV><<<dim3(rows, ns), 2 * S::NPAD, 0, ctx->stream>>>(
+        a.partial, a.n_groups, a.n_ksplit, kappa, a.n_vec, slices, tickets, d_out);
     NEO_LAUNCHED(ctx);
     return NEO_OK;
 }
@@ -808,14 +887,14 @@ int launch_commit_tc(neo_gpu_ctx* ctx, const PPEntry* pp, const int8_t* d_digits
         // built first and checked (one synchronisation), falling back to the
         // cyclic form when an entry leaves int8
         uint32_t n_groups, n_ksplit, kb_per_cta;
-        const size_t need = tc_scratch_bytes(n_vec, m, true, &n_groups, &n_ksplit, &kb_per_cta);
+        const size_t need = tc_scratch_bytes(n_vec, m, true, pp->kappa, &n_groups, &n_ksplit, &kb_per_cta);
         uint8_t* F = scratch;
         const size_t f_end = ((size_t)n_vec * m * P8_FBYTES + 64 + 255) & ~size_t(255);
         uint32_t* flag = reinterpret_cast<uint32_t*>(scratch + need - 512);
         const bool known = digits == TC_DIGITS_SMALL;
         if (!known) NEO_CK(ctx, cudaMemsetAsync(flag, 0, 4, ctx->stream));
-        p8_seq_kernel<<<ceil_div((uint64_t)n_vec * m, 128), 128, 0, ctx->stream>>>(d_digits, n_vec, m, F,
-                                                                                   known ? d_err : flag);
+        p8_seq_kernel<<<ceil_div((uint64_t)n_vec * m, P8_SEQ_THREADS), P8_SEQ_THREADS, 0, ctx->stream>>>(
+            d_digits, n_vec, m, F, known ? d_err : flag);
         NEO_LAUNCHED(ctx);
         bool ok = true;
         if (!known) {
@@ -830,11 +909,13 @@ int launch_commit_tc(neo_gpu_ctx* ctx, const PPEntry* pp, const int8_t* d_digits
             a.n_groups = n_groups;
             a.n_ksplit = n_ksplit;
             a.kb_per_cta = kb_per_cta;
-            return tc_nv(n_vec, true) == 1 ? launch_p8<1>(ctx, a, pp->kappa, d_out) : launch_p8<4>(ctx, a, pp->kappa, d_out);
+            uint8_t* red = scratch + f_end + (size_t)n_groups * n_ksplit * 128 * 64 * tc_nv(n_vec, true) * 4;
+            return tc_nv(n_vec, true) == 1 ? launch_p8<1>(ctx, a, pp->kappa, red, d_out)
+                                           : launch_p8<4>(ctx, a, pp->kappa, red, d_out);
         }
     }
     uint32_t n_groups, n_ksplit, kb_per_cta;
-    tc_scratch_bytes(n_vec, m, false, &n_groups, &n_ksplit, &kb_per_cta);
+    tc_scratch_bytes(n_vec, m, false, pp->kappa, &n_groups, &n_ksplit, &kb_per_cta);
     uint8_t* F = scratch;
     int32_t* partial = reinterpret_cast<int32_t*>(scratch + (((size_t)n_vec * m * TC_FBYTES + 64 + 255) & ~size_t(255)));
     f_seq_kernel<<<ceil_div((uint64_t)n_vec * m, 128), 128, 0, ctx->stream>>>(d_digits, n_vec, m, F);

@@ -211,8 +211,8 @@ enum { TC_DIGITS_ANY = 0, TC_DIGITS_SMALL = 1, TC_DIGITS_CHECK = 2 };
 int launch_commit(neo_gpu_ctx* ctx, const int8_t* d_digits, uint32_t n_vec, uint64_t m, uint64_t* d_out,
                   int digits = TC_DIGITS_CHECK);
 int tc_pp_prepare(neo_gpu_ctx* ctx, PPEntry* pp);
-size_t tc_scratch_bytes(uint32_t n_vec, uint64_t m, bool small, uint32_t* n_groups, uint32_t* n_ksplit,
-                        uint32_t* kb_per_cta);
+size_t tc_scratch_bytes(uint32_t n_vec, uint64_t m, bool small, uint32_t kappa, uint32_t* n_groups,
+                        uint32_t* n_ksplit, uint32_t* kb_per_cta);
 int launch_commit_tc(neo_gpu_ctx* ctx, const PPEntry* pp, const int8_t* d_digits, uint32_t n_vec, uint64_t* d_out,
                      uint8_t* scratch, uint32_t* d_err, int digits);
 // reads and clears the device error word (synchronizes the stream)
