@@ -263,8 +263,10 @@ __attribute__((noinline)) static void permute_impl(const Poseidon2<W>& P, uint64
 // S-box chain, in scalar registers and lanes 1..15 in the vectors, whose next
 // sum is sum_i mu_i x_i + 15 sum, so only lane 0's chain is serial.  Lanes
 // stay in [0, 2^64) as in the scalar code and the result is bit-identical to
-// it (1.5x faster on a Xeon with AVX-512).  Width 8 stays scalar: there the
-// vector multiply's latency outweighs its fewer instructions.
+// it (1.5x faster on a Xeon with AVX-512).  Width 8 keeps its full rounds
+// scalar (eight S-box chains whose latency the vector multiply would lengthen)
+// and moves lanes 1..7 of its partial rounds into one vector, beside lane 0's
+// scalar chain (permute8_avx512).
 #define NEO_AVX512 __attribute__((target("avx512f"), always_inline)) inline
 NEO_AVX512 static __m512i v_eps() { return _mm512_set1_epi64((long long)GL_EPS); }
 // (lo, hi) -> lo + 2^64 hi (mod q), the vector form of red_nc
@@ -341,6 +343,14 @@ NEO_AVX512 static uint64_t v_hsum2(__m512i a, __m512i b) {
     const uint64_t hi = sh >> 32, lo = sh & GL_EPS;
     return add_carry_fix(sl + ((hi << 32) - hi), lo << 32);
 }
+// sum of the 8 lanes of a (mod q)
+NEO_AVX512 static uint64_t v_hsum1(__m512i a) {
+    const __m512i m32 = v_eps();
+    const uint64_t sl = (uint64_t)_mm512_reduce_add_epi64(_mm512_and_si512(a, m32));
+    const uint64_t sh = (uint64_t)_mm512_reduce_add_epi64(_mm512_srli_epi64(a, 32));
+    const uint64_t hi = sh >> 32, lo = sh & GL_EPS;
+    return add_carry_fix(sl + ((hi << 32) - hi), lo << 32);
+}
 NEO_AVX512 static void v_full16(__m512i& A, __m512i& B, const uint64_t* rc) {
     const __m512i xa = v_add_small(A, _mm512_loadu_si512(rc)), xb = v_add_small(B, _mm512_loadu_si512(rc + 8));
     const __m512i xa2 = v_mul(xa, xa), xb2 = v_mul(xb, xb);
@@ -379,6 +389,38 @@ __attribute__((target("avx512f"), noinline)) static void permute16_avx512(const 
     _mm512_storeu_si512(st_io, A);
     _mm512_storeu_si512(st_io + 8, B);
 }
+// width 8: scalar full rounds; in the partial rounds lanes 1..7 in one vector
+// (lane 0 masked to zero), whose products mu_i x_i do not wait for lane 0's
+// S-box, so only that chain is serial (the scalar partial round is bound by
+// the throughput of the seven scalar lane updates instead).  Bit-identical to
+// permute_impl<8>.
+__attribute__((target("avx512f"), noinline)) static void permute8_avx512(const Poseidon2<8>& P, uint64_t* st_io) {
+    uint64_t st[8];
+#pragma GCC unroll 8
+    for (int i = 0; i < 8; i++) st[i] = st_io[i];
+    external_layer<8>(st);
+    for (int r = 0; r < 4; r++) full_round<8>(st, P.rc_ext[r]);
+    const __m512i mu = _mm512_maskz_loadu_epi64(0xFE, P.mu), mu_hi = _mm512_srli_epi64(mu, 32);
+    __m512i v = _mm512_maskz_loadu_epi64(0xFE, st);
+    uint64_t rest = v_hsum1(v);
+    uint64_t x0 = addq(st[0], P.rc_int[0]);
+    const uint64_t mu0p1 = P.mu[0] + 1;
+    for (int r = 0; r < 22; r++) {
+        const __m512i p = v_mul(v, mu, mu_hi);
+        const uint64_t psum = v_hsum1(p);
+        const uint64_t x = sbox7(x0);
+        const uint64_t sum = canonq(red_small((u128)x + rest));
+        const u128 addend = (u128)rest + (r + 1 < 22 ? P.rc_int[r + 1] : 0);
+        x0 = red128((u128)mu0p1 * x + addend);
+        v = _mm512_maskz_mov_epi64(0xFE, v_add_small(p, _mm512_set1_epi64((long long)sum)));
+        rest = red_small((u128)psum + red_small((u128)sum * 7));
+    }
+    _mm512_storeu_si512(st, v);
+    st[0] = x0;
+    for (int r = 4; r < 8; r++) full_round<8>(st, P.rc_ext[r]);
+#pragma GCC unroll 8
+    for (int i = 0; i < 8; i++) st_io[i] = canonq(st[i]);
+}
 #undef NEO_AVX512
 
 // AVX-512F when the host has it, unless NEO_TRANSCRIPT_SCALAR is set (tests
@@ -395,11 +437,12 @@ static bool use_avx512() {
 template <int W>
 void Poseidon2<W>::permute(uint64_t* st_io) const {
 #if defined(__x86_64__)
-    if constexpr (W == 16) {
-        if (use_avx512()) {
+    if (use_avx512()) {
+        if constexpr (W == 16)
             permute16_avx512(*this, st_io);
-            return;
-        }
+        else
+            permute8_avx512(*this, st_io);
+        return;
     }
 #endif
     permute_impl<W>(*this, st_io);

@@ -75,3 +75,45 @@ def test_ccs_digest_simd_and_scalar_paths_match_oracle():
         env.update(extra)
         out = subprocess.run([sys.executable, "-c", code], env=env, capture_output=True, text=True, check=True)
         assert out.stdout.strip() == want, extra
+
+
+def _drive_many(tr):
+    """3000 absorbs of 23 random, edge-value (q - 1 - small) or small field
+    elements with a challenge every 50: about 20 k permutations."""
+    q = (1 << 64) - (1 << 32) + 1
+    rng = np.random.default_rng(11)
+    out = []
+    for i in range(3000):
+        kind = i % 3
+        if kind == 0:
+            vals = [int(v) for v in rng.integers(0, q, size=23, dtype=np.uint64)]
+        elif kind == 1:
+            vals = [q - 1 - int(v) for v in rng.integers(0, 4, size=23)]
+        else:
+            vals = [int(v) for v in rng.integers(0, 16, size=23)]
+        tr.append_fields(b"y_elem", vals)
+        if i % 50 == 0:
+            out.append(int(tr.challenge_field(b"chal")))
+    return out + [int(v) for v in tr.state()]
+
+
+def test_transcript_simd_and_scalar_paths_match_oracle():
+    """The width-8 transcript permutation has an AVX-512 path (lanes 1..7 of
+    the partial rounds in one vector; taken when the host has AVX-512F) and a
+    scalar one (NEO_TRANSCRIPT_SCALAR set): both follow the oracle's sponge
+    through about twenty thousand permutations of random, edge-value and
+    small-value absorbs."""
+    import os
+    import subprocess
+    import sys
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+    code = ("import sys; sys.path.insert(0, %r); sys.path.insert(0, %r); import test_transcript as T; "
+            "from nightstream_b200 import gpu; print(','.join(map(str, T._drive_many(gpu.HostTranscript(b'neo/simd')))))"
+            % (root, os.path.join(root, "tests")))
+    want = ",".join(map(str, _drive_many(O.Transcript(b"neo/simd"))))
+    for extra in ({}, {"NEO_TRANSCRIPT_SCALAR": "1"}):
+        env = {k: v for k, v in os.environ.items() if k != "NEO_TRANSCRIPT_SCALAR"}
+        env.update(extra)
+        out = subprocess.run([sys.executable, "-c", code], env=env, capture_output=True, text=True, check=True)
+        assert out.stdout.strip() == want, extra
