@@ -51,7 +51,8 @@ constexpr int TC_SMEM_BYTES = TC_ASTAGES * (TC_A_BYTES + TC_F_STAGE) + TC_BSTAGE
 constexpr int TC_BUILDERS = 256;            // 8 builder warps
 constexpr int TC_THREADS = 64 + TC_BUILDERS;  // warp0 producer, warp1 MMA, warps2-9 B build (2-5 epilogue)
 constexpr int TC_MAX_KB = 512;              // K blocks per CTA (int32 overflow bound)
-constexpr uint32_t TC_SPIN_LIMIT = 1u << 22;  // ~0.3 s with the back-off below
+constexpr uint32_t TC_SPIN_LIMIT = 1u << 22;       // wait attempts (each suspends at most a hardware limit)
+constexpr uint64_t TC_WAIT_NS = 500ull * 1000 * 1000;  // 0.5 s of global time per wait
 
 static_assert(TC_B_BYTES % 1024 == 0 && TC_A_BYTES % 1024 == 0, "stage buffers stay 1024-byte aligned");
 static_assert(TC_SMEM_BYTES + 1024 + 256 <= 232448, "shared memory budget");
@@ -73,18 +74,31 @@ __device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
                  "r"(bytes)
                  : "memory");
 }
-// bounded wait on phase parity (non-blocking test + back-off); false on timeout
+// bounded wait on phase parity; false on timeout.  mbarrier.try_wait suspends
+// the thread until the phase completes or a hardware time limit passes, so a
+// waiting warp does not keep polling shared memory; the wait gives up after
+// TC_WAIT_NS of global time or TC_SPIN_LIMIT attempts, whichever comes first.
+__device__ __forceinline__ uint64_t globaltimer_ns() {
+    uint64_t t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
 __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
-    uint32_t addr = smem_u32(bar);
+    const uint32_t addr = smem_u32(bar);
+    uint64_t t0 = 0;
     for (uint32_t it = 0; it < TC_SPIN_LIMIT; it++) {
         uint32_t done;
         asm volatile(
-            "{\n\t.reg .pred p;\n\tmbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n\t}"
+            "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n\t}"
             : "=r"(done)
             : "r"(addr), "r"(parity)
             : "memory");
         if (done) return true;
-        if (it > 256) __nanosleep(64);
+        const uint64_t t = globaltimer_ns();
+        if (it == 0)
+            t0 = t;
+        else if (t - t0 > TC_WAIT_NS)
+            return false;
     }
     return false;
 }
@@ -467,7 +481,9 @@ struct P8 {
     static constexpr int BCOL = 5 * LBO;        // B bytes per column
     static constexpr int B_BYTES = 2 * BCOL;    // two columns per K block
     static constexpr int F_STAGE = NV * 2 * P8_FBYTES;
-    static constexpr int BUILDERS = NV >= 2 ? 64 * NV : 128;  // (column, vector, seq, phase); >= 4 epilogue warps
+    // (column, vector, seq, phase pair) for NV <= 4; at least the 4 epilogue warps
+    static constexpr int BUILDERS = 128;
+    static_assert(NV <= 4, "one builder thread per (column, vector, seq, phase pair)");
     static constexpr int THREADS = 64 + BUILDERS;
     // groups of 4 vectors run two CTAs per SM (3 A stages, 2 B buffers each):
     // while one waits on its rings the other issues MMAs (0.47 instead of
@@ -638,12 +654,14 @@ __global__ void __launch_bounds__(P8<NV>::THREADS, P8<NV>::CTAS) commit_p8_kerne
             mma_commit(done);
         }
     } else {
-        // ---- B builders: thread (column jj, vector v, seq, phase p = 8h + b)
-        // writes chunks c < 5 of G_p = H_seq[16c + p, 16c + p + 16) at
-        // [jj][c][h][seq][v][b]; the warp shares (jj, v), so lane groups of 8
-        // write 128 contiguous bytes ----
+        // ---- B builders: thread (column jj, vector v, seq, b < 8) writes the
+        // chunks c < 5 of both phases p = b + 8h (h = 0, 1), G_p = H_seq[16c + p,
+        // 16c + p + 16), at [jj][c][h][seq][v][b]; the two phases share the
+        // words [b/4, b/4 + 23) of the sequence, read once.  A warp covers two
+        // (jj, v) pairs and both sequences, so each store phase writes whole
+        // 128-byte rows and the loads touch eight distinct words ----
         const int bt = threadIdx.x - 64;
-        const int p = bt & 15, seq = (bt >> 4) & 1, combo = bt >> 5;
+        const int b = bt & 7, seq = (bt >> 3) & 1, combo = bt >> 4;
         const int v = combo % NV, jj = combo / NV;
         const bool active = jj < 2 && (uint32_t)v < nvalid;
         for (uint32_t it = 0; it < nkb; it++) {
@@ -665,34 +683,22 @@ __global__ void __launch_bounds__(P8<NV>::THREADS, P8<NV>::CTAS) commit_p8_kerne
             if (st) break;
             if (active) {
                 const int sa = it % S::ASTAGES;
-                // bytes [0, 96) of the sequence as six 16-byte loads (the warp's
-                // two sequences: one wavefront each), then words [p/4, p/4 + 21)
-                // selected in registers
-                const uint4* src = reinterpret_cast<const uint4*>(sF + sa * S::F_STAGE + (v * 2 + jj) * P8_FBYTES +
-                                                                  seq * P8_HSEQ);
-                uint32_t u[24];
+                const uint32_t* src = reinterpret_cast<const uint32_t*>(sF + sa * S::F_STAGE + (v * 2 + jj) * P8_FBYTES +
+                                                                        seq * P8_HSEQ) + (b >> 2);
+                uint32_t w[23];  // bytes < 96 of the 112-byte sequence
 #pragma unroll
-                for (int q = 0; q < 6; q++) {
-                    const uint4 t = src[q];
-                    u[4 * q] = t.x;
-                    u[4 * q + 1] = t.y;
-                    u[4 * q + 2] = t.z;
-                    u[4 * q + 3] = t.w;
-                }
-                uint32_t x[22];
+                for (int q = 0; q < 23; q++) w[q] = src[q];
+                const uint32_t sh = 8 * (b & 3);
+                uint8_t* dst = sB + sb * S::B_BYTES + jj * S::BCOL + seq * (NV * 128) + v * 128 + b * 16;
 #pragma unroll
-                for (int q = 0; q < 22; q++) x[q] = (p & 8) ? u[q + 2] : u[q];
-                uint32_t w[21];
+                for (int h = 0; h < 2; h++)
 #pragma unroll
-                for (int q = 0; q < 21; q++) w[q] = (p & 4) ? x[q + 1] : x[q];
-                const uint32_t sh = 8 * (p & 3);
-                uint8_t* dst = sB + sb * S::B_BYTES + jj * S::BCOL + (p >> 3) * (2 * NV * 128) + seq * (NV * 128) +
-                               v * 128 + (p & 7) * 16;
-#pragma unroll
-                for (int c = 0; c < 5; c++)
-                    *reinterpret_cast<uint4*>(dst + c * S::LBO) =
-                        make_uint4(__funnelshift_r(w[4 * c], w[4 * c + 1], sh), __funnelshift_r(w[4 * c + 1], w[4 * c + 2], sh),
-                                   __funnelshift_r(w[4 * c + 2], w[4 * c + 3], sh), __funnelshift_r(w[4 * c + 3], w[4 * c + 4], sh));
+                    for (int c = 0; c < 5; c++) {
+                        const int o = 4 * c + 2 * h;
+                        *reinterpret_cast<uint4*>(dst + h * (2 * NV * 128) + c * S::LBO) =
+                            make_uint4(__funnelshift_r(w[o], w[o + 1], sh), __funnelshift_r(w[o + 1], w[o + 2], sh),
+                                       __funnelshift_r(w[o + 2], w[o + 3], sh), __funnelshift_r(w[o + 3], w[o + 4], sh));
+                    }
             }
             asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
             __syncwarp();
