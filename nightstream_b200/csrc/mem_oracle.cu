@@ -523,23 +523,19 @@ __global__ void __launch_bounds__(256) mem_multi_eval_kernel(const __grid_consta
     __syncthreads();
     if (!s_last) return;
     __threadfence();
-    for (uint32_t x = 0; x < c.npts; x++) {
+    // one warp per point: the points' sums run side by side (a claim of the
+    // late rounds has one partial per point, so this tail is a few load
+    // latencies instead of one block-wide reduction per point)
+    for (uint32_t x = warp; x < c.npts; x += 256 / 32) {
         K v = gl::kzero();
-        for (uint32_t r = threadIdx.x; r < c.nblk; r += 256) {
+#pragma unroll 4
+        for (uint32_t r = lane; r < c.nblk; r += 32) {
             const ulonglong2 u = __ldcg(reinterpret_cast<const ulonglong2*>(a.partials + c.part0 + (uint64_t)x * c.nblk + r));
             v = gl::kadd(v, gl::kmk(u.x, u.y));
         }
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) v = gl::kadd(v, shfl_xor_km(v, o));
-        if (lane == 0) s_red[warp][0] = v;
-        __syncthreads();
-        if (threadIdx.x == 0) {
-            K t = gl::kzero();
-#pragma unroll
-            for (int w = 0; w < 256 / 32; w++) t = gl::kadd(t, s_red[w][0]);
-            c.out[x] = t;
-        }
-        __syncthreads();
+        if (lane == 0) c.out[x] = v;
     }
 }
 
@@ -1303,22 +1299,17 @@ __global__ void __launch_bounds__(TA_T) ta_eval_kernel(const TaEval a) {
     __syncthreads();
     if (!s_last) return;
     __threadfence();
-    for (int x = 0; x < 3; x++) {
+    // the points x < 3 split over the block's warps, side by side
+    for (int x = warp; x < 3; x += TA_T / 32) {
         K v = gl::kzero();
-        for (uint64_t b = threadIdx.x; b < nb; b += TA_T) {
+#pragma unroll 4
+        for (uint64_t b = lane; b < nb; b += 32) {
             const ulonglong2 u = __ldcg(reinterpret_cast<const ulonglong2*>(a.partials + (uint64_t)x * nb + b));
             v = gl::kadd(v, gl::kmk(u.x, u.y));
         }
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) v = gl::kadd(v, shfl_xor_km(v, o));
-        if (lane == 0) s_red[0][warp] = v;
-        __syncthreads();
-        if (threadIdx.x == 0) {
-            K t = gl::kzero();
-            for (int w = 0; w < TA_T / 32; w++) t = gl::kadd(t, s_red[0][w]);
-            a.out[x] = t;
-        }
-        __syncthreads();
+        if (lane == 0) a.out[x] = v;
     }
 }
 
