@@ -371,21 +371,32 @@ extern "C" int neo_gpu_rlc_mix(neo_gpu_ctx* ctx, const int8_t* rho_coeffs, const
 // Pi_DEC split (common.rs:75-268; balanced_divrem common.rs:44-58)
 // flags[0] = out-of-range error, flags[1 + i] = plane i nonzero
 // ---------------------------------------------------------------------------
+// Z_mix entries are int32, so the digits come from 32-bit arithmetic; b = 2
+// (the fold step's base) takes the balanced remainder and an exact shift
+// instead of a division.
+template <bool B2>
 __global__ void split_b_kernel(const int32_t* __restrict__ Zmix, uint64_t len, uint32_t k, int32_t b,
                                int8_t* __restrict__ planes, uint32_t* __restrict__ flags) {
     uint64_t idx = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
     uint32_t nz_mask = 0;
     if (idx < len) {
-        int64_t v = Zmix[idx];
+        int32_t v = Zmix[idx];
+        // b^k, saturated once it exceeds every int32 (the check is then moot)
         int64_t B = 1;
-        for (uint32_t i = 0; i < k; i++) B *= b;
-        if (v >= B || v <= -B) atomicOr(&flags[0], 1u);
-        int64_t half = b / 2;
+        for (uint32_t i = 0; i < k && B <= INT32_MAX; i++) B *= b;
+        if ((int64_t)v >= B || (int64_t)v <= -B) atomicOr(&flags[0], 1u);
+        const int32_t half = b / 2;
         for (uint32_t i = 0; i < k; i++) {
-            int64_t r = v % b;
-            int64_t q = (v - r) / b;
-            if (r > half) { r -= b; q += 1; }
-            else if (r < -half) { r += b; q -= 1; }
+            int32_t r, q;
+            if (B2) {  // v % 2 in {-1, 0, 1} (sign of v), v - r even
+                r = (v & 1) ? (v < 0 ? -1 : 1) : 0;
+                q = (v - r) >> 1;
+            } else {
+                r = v % b;
+                q = (v - r) / b;
+                if (r > half) { r -= b; q += 1; }
+                else if (r < -half) { r += b; q -= 1; }
+            }
             planes[(uint64_t)i * len + idx] = (int8_t)r;
             if (r) nz_mask |= 1u << i;
             v = q;
@@ -401,7 +412,10 @@ int split_b_device(neo_gpu_ctx* ctx, const int32_t* d_Zmix, uint64_t len, uint32
                    uint32_t* d_flags) {
     if (k == 0 || k > 31 || b < 2 || b > 64) return ctx->fail(NEO_ERR_UNSUPPORTED, "split_b: k/b out of range");
     NEO_CK(ctx, cudaMemsetAsync(d_flags, 0, 2 * sizeof(uint32_t), ctx->stream));
-    split_b_kernel<<<ceil_div(len, 256), 256, 0, ctx->stream>>>(d_Zmix, len, k, (int32_t)b, d_planes, d_flags);
+    if (b == 2)
+        split_b_kernel<true><<<ceil_div(len, 256), 256, 0, ctx->stream>>>(d_Zmix, len, k, 2, d_planes, d_flags);
+    else
+        split_b_kernel<false><<<ceil_div(len, 256), 256, 0, ctx->stream>>>(d_Zmix, len, k, (int32_t)b, d_planes, d_flags);
     NEO_LAUNCHED(ctx);
     return NEO_OK;
 }
@@ -504,13 +518,17 @@ __global__ void __launch_bounds__(256) zv_dot_kernel(const int8_t* __restrict__ 
 // column pair are tabulated in shared memory once for the block's rows, and a
 // row adds one table entry per pair (index from its two digits), summed
 // unreduced in 128 bits.  v is read once per 128 rows instead of once per row.
-// The last block of a row group (ticket) adds the column ranges' partials.
+// Each block adds its column range's sums into per-(row, j) 64-bit
+// accumulators with atomics (a wrap past 2^64 counted apart: exact and
+// order-free), so the last block of a row group (ticket) only reduces them,
+// instead of summing every column range's partial one after the other.
 constexpr int ZR_ROWS = 128, ZR_CHUNK = 64, ZR_TMAX = 4;
 constexpr int ZR_TPAD = 5;  // entry stride 80 B: the 9 entries of a pair fall on distinct bank groups
 __global__ void __launch_bounds__(ZR_ROWS) zrows_kernel(const int8_t* __restrict__ Z, uint32_t R, uint64_t m,
                                                         uint32_t t, const K* __restrict__ v, uint64_t cols_per_split,
-                                                        K* __restrict__ partials, unsigned int* __restrict__ tickets,
-                                                        K* __restrict__ y) {
+                                                        unsigned long long* __restrict__ acc_lo,
+                                                        unsigned int* __restrict__ acc_wrap,
+                                                        unsigned int* __restrict__ tickets, K* __restrict__ y) {
     __shared__ K tab[ZR_CHUNK / 2][9][ZR_TPAD];
     const uint32_t row = blockIdx.x * ZR_ROWS + threadIdx.x;
     const uint64_t c_lo = blockIdx.y * cols_per_split, c_hi = min(m, c_lo + cols_per_split);
@@ -553,15 +571,17 @@ __global__ void __launch_bounds__(ZR_ROWS) zrows_kernel(const int8_t* __restrict
             }
         }
     }
-    // lo + 2^64 hi (mod q) with 2^64 = 2^32 - 1; hi < 2^16
+    // lo + 2^64 hi (mod q) with 2^64 = 2^32 - 1; hi < 2^16; then into the
+    // row's accumulators (a component whose add wraps past 2^64 counts one wrap)
     if (row < R) {
 #pragma unroll
-        for (int j = 0; j < ZR_TMAX; j++) {
-            if (j >= (int)t) break;
-            K r;
-            r.re = gl::add(gl::canon(lo[2 * j]), hi[2 * j] * 0xFFFFFFFFull);
-            r.im = gl::add(gl::canon(lo[2 * j + 1]), hi[2 * j + 1] * 0xFFFFFFFFull);
-            partials[((uint64_t)blockIdx.y * R + row) * t + j] = r;
+        for (int j = 0; j < 2 * ZR_TMAX; j++) {
+            if (j >= 2 * (int)t) break;
+            const uint64_t c = gl::add(gl::canon(lo[j]), hi[j] * 0xFFFFFFFFull);
+            if (c == 0) continue;
+            const uint64_t at = (uint64_t)row * 2 * t + j;  // [row][j / 2][re, im]
+            const unsigned long long old = atomicAdd(acc_lo + at, (unsigned long long)c);
+            if (old + c < old) atomicAdd(acc_wrap + at, 1u);
         }
     }
     __threadfence();
@@ -571,14 +591,16 @@ __global__ void __launch_bounds__(ZR_ROWS) zrows_kernel(const int8_t* __restrict
     __syncthreads();
     if (!s_last || row >= R) return;
     __threadfence();
+    const uint32_t w = row / NEO_D, rho = row % NEO_D;
     for (uint32_t j = 0; j < t; j++) {
-        K a = gl::kzero();
-        for (uint32_t sp = 0; sp < gridDim.y; sp++) {
-            const ulonglong2 u = __ldcg(reinterpret_cast<const ulonglong2*>(partials + ((uint64_t)sp * R + row) * t + j));
-            a = gl::kadd(a, gl::kmk(u.x, u.y));
+        uint64_t c[2];
+#pragma unroll
+        for (int e = 0; e < 2; e++) {
+            const uint64_t at = (uint64_t)row * 2 * t + 2 * j + e;
+            // lo + 2^64 wraps (mod q); wraps < 2^32, so wraps (2^32 - 1) < 2^64
+            c[e] = gl::add(gl::canon(__ldcg(acc_lo + at)), gl::canon((uint64_t)__ldcg(acc_wrap + at) * 0xFFFFFFFFull));
         }
-        const uint32_t w = row / NEO_D, rho = row % NEO_D;
-        y[((uint64_t)w * t + j) * NEO_D + rho] = a;
+        y[((uint64_t)w * t + j) * NEO_D + rho] = gl::kmk(c[0], c[1]);
     }
 }
 
@@ -594,14 +616,17 @@ int launch_zrows(neo_gpu_ctx* ctx, const int8_t* d_Z, uint32_t R, uint64_t m, ui
     uint64_t splits = std::min<uint64_t>(chunks, std::max<uint64_t>(1, (8 * 148 + groups - 1) / groups));
     const uint64_t cps = ((chunks + splits - 1) / splits) * ZR_CHUNK;
     splits = (m + cps - 1) / cps;
-    const size_t part_bytes = (size_t)splits * R * t * sizeof(K);
+    // accumulators [R][t][2] (64-bit sums, then 32-bit wrap counts) and the
+    // row groups' tickets, cleared together
+    const size_t n_acc = (size_t)R * t * 2;
+    const size_t lo_bytes = n_acc * 8, wrap_bytes = n_acc * 4;
     void* scratch = nullptr;
-    NEO_CK(ctx, ctx_scratch(ctx, part_bytes + 256 + groups * sizeof(unsigned int), &scratch));
-    K* partials = reinterpret_cast<K*>(scratch);
-    unsigned int* tickets = reinterpret_cast<unsigned int*>(reinterpret_cast<uint8_t*>(scratch) + part_bytes + 256);
-    NEO_CK(ctx, cudaMemsetAsync(tickets, 0, groups * sizeof(unsigned int), ctx->stream));
-    zrows_kernel<<<dim3(groups, (uint32_t)splits), ZR_ROWS, 0, ctx->stream>>>(d_Z, R, m, t, d_v, cps, partials, tickets,
-                                                                               d_y);
+    NEO_CK(ctx, ctx_scratch(ctx, lo_bytes + wrap_bytes + groups * sizeof(unsigned int), &scratch));
+    uint8_t* sb = reinterpret_cast<uint8_t*>(scratch);
+    NEO_CK(ctx, cudaMemsetAsync(sb, 0, lo_bytes + wrap_bytes + groups * sizeof(unsigned int), ctx->stream));
+    zrows_kernel<<<dim3(groups, (uint32_t)splits), ZR_ROWS, 0, ctx->stream>>>(
+        d_Z, R, m, t, d_v, cps, reinterpret_cast<unsigned long long*>(sb),
+        reinterpret_cast<unsigned int*>(sb + lo_bytes), reinterpret_cast<unsigned int*>(sb + lo_bytes + wrap_bytes), d_y);
     NEO_LAUNCHED(ctx);
     *done = true;
     return NEO_OK;

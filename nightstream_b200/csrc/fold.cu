@@ -196,33 +196,36 @@ __global__ void bus_weights_kernel(const K* __restrict__ r, uint32_t ell, uint32
 
 // bus openings y[w][c][rho] = Σ_j χ_r(m_in + j) Z_w[rho][bus_base + c*steps + j]
 // (append_bus_openings_to_me_instance, cpu_bus.rs:195-320); block per (c, rho), grid.y witnesses
-__global__ void __launch_bounds__(256) bus_open_kernel(const int8_t* __restrict__ Z, uint64_t m, uint64_t bus_base,
-                                                       uint64_t steps, uint32_t ncols, const K* __restrict__ w,
-                                                       K* __restrict__ y) {
-    const uint32_t c = blockIdx.x / NEO_D, rho = blockIdx.x % NEO_D, wi = blockIdx.y;
-    const int8_t* zr = Z + ((uint64_t)wi * NEO_D + rho) * m + bus_base + (uint64_t)c * steps;
+// One warp per (witness, bus column, digit row): y = sum_j Z[row][bus_base +
+// c steps + j] w[j] over the chunk's steps (lanes stride the steps; the
+// weights are shared by every item and stay in L1/L2), a warp reduction, no
+// block barrier.  items = n_w * ncols * 54.
+constexpr int BUS_OPEN_WARPS = 8;
+__global__ void __launch_bounds__(32 * BUS_OPEN_WARPS) bus_open_kernel(const int8_t* __restrict__ Z, uint64_t m,
+                                                                      uint64_t bus_base, uint64_t steps, uint32_t ncols,
+                                                                      uint64_t items, const K* __restrict__ w,
+                                                                      K* __restrict__ y) {
+    const uint64_t item = (uint64_t)blockIdx.x * BUS_OPEN_WARPS + (threadIdx.x >> 5);
+    if (item >= items) return;  // warp-uniform
+    const int lane = threadIdx.x & 31;
+    const uint32_t rho = (uint32_t)(item % NEO_D);
+    const uint32_t c = (uint32_t)((item / NEO_D) % ncols);
+    const uint64_t wi = item / ((uint64_t)NEO_D * ncols);
+    const int8_t* zr = Z + (wi * NEO_D + rho) * m + bus_base + (uint64_t)c * steps;
     K acc = gl::kzero();
-    for (uint64_t j = threadIdx.x; j < steps; j += blockDim.x) {
-        int z = zr[j];
+    for (uint64_t j = lane; j < steps; j += 32) {
+        const int z = zr[j];
         if (z == 1) acc = gl::kadd(acc, w[j]);
         else if (z == -1) acc = gl::ksub(acc, w[j]);
         else if (z != 0) acc = gl::kadd(acc, gl::kscale_small(w[j], z));
     }
-    __shared__ K red[8];
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     for (int o = 16; o > 0; o >>= 1) {
         K b;
         b.re = __shfl_xor_sync(0xffffffffu, acc.re, o);
         b.im = __shfl_xor_sync(0xffffffffu, acc.im, o);
         acc = gl::kadd(acc, b);
     }
-    if (lane == 0) red[warp] = acc;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        K s = gl::kzero();
-        for (int u = 0; u < 8; u++) s = gl::kadd(s, red[u]);
-        y[((uint64_t)wi * ncols + c) * NEO_D + rho] = s;
-    }
+    if (lane == 0) y[(wi * ncols + c) * NEO_D + rho] = acc;
 }
 
 }  // namespace
@@ -972,8 +975,9 @@ static int bus_openings(neo_gpu_shard* sh, const int8_t* d_Z, uint32_t n_w, std:
     bus_weights_kernel<<<ceil_div(sh->steps, 256), 256, 0, ctx->stream>>>(sh->d_r.p, sh->ell_n, sh->m_in, sh->steps,
                                                                           sh->d_busw.p);
     NEO_LAUNCHED(ctx);
-    bus_open_kernel<<<dim3(nb * NEO_D, n_w), 256, 0, ctx->stream>>>(d_Z, sh->m, sh->bus_base, sh->steps, nb,
-                                                                    sh->d_busw.p, sh->d_busy.p);
+    const uint64_t items = (uint64_t)n_w * nb * NEO_D;
+    bus_open_kernel<<<(unsigned)ceil_div(items, BUS_OPEN_WARPS), 32 * BUS_OPEN_WARPS, 0, ctx->stream>>>(
+        d_Z, sh->m, sh->bus_base, sh->steps, nb, items, sh->d_busw.p, sh->d_busy.p);
     NEO_LAUNCHED(ctx);
     y.resize((size_t)n_w * nb * NEO_D);
     NEO_CK(ctx, ctx_d2h(ctx, y.data(), sh->d_busy.p, y.size() * sizeof(K)));
