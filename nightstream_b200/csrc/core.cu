@@ -403,9 +403,16 @@ __global__ void split_b_kernel(const int32_t* __restrict__ Zmix, uint64_t len, u
         }
         if (v != 0) atomicOr(&flags[0], 1u);
     }
-    // warp-aggregate the nonzero plane mask
+    // block-aggregate the nonzero plane mask; one atomic per block, and none
+    // once every plane it saw is already flagged (a single address that every
+    // warp hit serialised the kernel)
     for (int o = 16; o > 0; o >>= 1) nz_mask |= __shfl_xor_sync(0xffffffffu, nz_mask, o);
-    if ((threadIdx.x & 31) == 0 && nz_mask) atomicOr(&flags[1], nz_mask);
+    __shared__ uint32_t s_mask;
+    if (threadIdx.x == 0) s_mask = 0;
+    __syncthreads();
+    if ((threadIdx.x & 31) == 0 && nz_mask) atomicOr(&s_mask, nz_mask);
+    __syncthreads();
+    if (threadIdx.x == 0 && s_mask && (s_mask & ~__ldcg(flags + 1))) atomicOr(&flags[1], s_mask);
 }
 
 int split_b_device(neo_gpu_ctx* ctx, const int32_t* d_Zmix, uint64_t len, uint32_t k, uint32_t b, int8_t* d_planes,
